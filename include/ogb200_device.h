@@ -1,0 +1,138 @@
+/*
+ * ogb200_device.h -- status-returning device API of libogb200 (no OpenGraph
+ * counterpart: this is the layer under the drop-in symbols of ogb200.h).
+ *
+ * Every function returns 0 on success or a nonzero status (see
+ * OGB_ERR_*), with a message in ogb_last_error().  Pointers named d_* are
+ * device pointers of the current CUDA device; `stream` is a cudaStream_t
+ * (NULL = the library stream).  Nothing here exits the process.
+ */
+#ifndef OGB200_DEVICE_H
+#define OGB200_DEVICE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OGB_OK 0
+#define OGB_ERR_CUDA 1
+#define OGB_ERR_ARG 2
+#define OGB_ERR_SPIN 3
+#define OGB_ERR_RANGE 4
+#define OGB_ERR_NOMEM 5
+#define OGB_ERR_UNSUPPORTED 6
+
+typedef struct ogb_graph ogb_graph; /* device-resident CSR, both directions */
+
+/* One direction of a device CSR (the device image of struct Vertex plus the
+ * sorted edge arrays of struct EdgeList). */
+typedef struct ogb_csr_view
+{
+    uint32_t num_vertices;
+    uint32_t num_edges;
+    uint32_t *src;        /* sorted source ids (E)                    */
+    uint32_t *dst;        /* neighbour ids (E)                        */
+    float *weight;        /* E, or NULL when unweighted               */
+    uint32_t *out_degree; /* V                                        */
+    uint32_t *in_degree;  /* V                                        */
+    uint32_t *edges_idx;  /* V, 0 for vertices without edges          */
+} ogb_csr_view;
+
+typedef struct ogb_bfs_info
+{
+    uint32_t iteration;        /* BFSStats.iteration                    */
+    uint32_t processed_nodes;  /* BFSStats.processed_nodes              */
+    uint32_t td_steps;
+    uint32_t bu_steps;
+    uint32_t reached;          /* vertices with a parent               */
+    uint32_t levels;           /* steps recorded in the level trace     */
+    uint64_t reached_out_edges;/* sum of out-degrees of reached vertices */
+    uint64_t edges_examined;   /* edges read by the steps               */
+    double ms;                 /* device time of the traversal          */
+} ogb_bfs_info;
+
+/* One step of the BFS level trace (ogb_bfs_trace). */
+typedef struct ogb_bfs_level
+{
+    uint32_t direction;  /* 0 top-down, 1 bottom-up */
+    uint32_t discovered;
+    uint32_t frontier;
+    uint32_t mf;
+    uint32_t mu;
+    uint32_t pad;
+    uint64_t edges;
+    float ms;
+    float pad2;
+} ogb_bfs_level;
+
+typedef struct ogb_pr_info
+{
+    uint32_t iterations;     /* PageRankStats.iterations              */
+    uint32_t executed;       /* iterations actually run               */
+    uint32_t activeVertices; /* of the last iteration                 */
+    uint32_t converged;      /* 1 if an iteration had no active vertex */
+    double error_total;      /* of the last iteration                 */
+    double ms;               /* device time, init to normalization    */
+} ogb_pr_info;
+
+const char *ogb_last_error(void);
+/* 1 when this build's struct layouts are the WEIGHTED=1 ones. */
+int ogb_weighted_layout(void);
+/* Silence the reference-style progress tables printed by ogb200.h calls. */
+void ogb_set_quiet(int quiet);
+
+int ogb_graph_create(ogb_graph **g);
+void ogb_graph_destroy(ogb_graph *g);
+/* Sort (SORT_TYPE semantics) and build both CSR directions from device edge
+ * arrays; all ids < V <= 2^30.  Inputs are read only.  d_w may be NULL. */
+int ogb_graph_build(ogb_graph *g, const uint32_t *d_src, const uint32_t *d_dst, const float *d_w,
+                    uint32_t num_edges, uint32_t num_vertices, uint32_t sort_type, void *stream);
+int ogb_graph_view(ogb_graph *g, int inverse, ogb_csr_view *view);
+/* The device copy the drop-in layer keeps for a host GraphCSR (uploaded on
+ * first use); NULL with an error message when it cannot be made. */
+ogb_graph *ogb_graph_of(const void *graphCSR);
+
+/* Stable device sort of an edge list with SORT_TYPE semantics. */
+int ogb_sort_edges(const uint32_t *d_src, const uint32_t *d_dst, const float *d_w, uint32_t num_edges,
+                   uint32_t sort_type, uint32_t *d_out_src, uint32_t *d_out_dst, float *d_out_w, void *stream);
+
+/* BFS from root; mode 0 pull, 1 push, 2 direction-optimized.  d_parents
+ * (int32) and d_distances (u32) hold V entries each. */
+int ogb_bfs(ogb_graph *g, uint32_t root, uint32_t mode, int32_t *d_parents, uint32_t *d_distances,
+            ogb_bfs_info *info, void *stream);
+/* Level trace of the last ogb_bfs on g (up to max_levels entries). */
+int ogb_bfs_trace(ogb_graph *g, ogb_bfs_level *levels, uint32_t max_levels, uint32_t *count);
+
+/* PageRank; mode 0 pull, 1 push.  d_ranks receives V normalized ranks;
+ * d_init (may be NULL) replaces the uniform unnormalized start 1-0.85. */
+int ogb_pagerank(ogb_graph *g, uint32_t mode, uint32_t max_iterations, double epsilon, float *d_ranks,
+                 const float *d_init, ogb_pr_info *info, void *stream);
+/* Per-iteration L1 error and active count of the last ogb_pagerank on g. */
+int ogb_pagerank_history(ogb_graph *g, double *errors, uint32_t *active, uint32_t max_entries, uint32_t *count);
+
+/* ---- synthetic inputs (host, multi-threaded, deterministic) ------------- */
+
+/* RMAT (a, b, c; d = 1-a-b-c) with 2^scale vertices and edge_factor*2^scale
+ * edges, counter-based RNG keyed by seed, ids relabelled by a seeded random
+ * permutation when permute != 0.  Weights (if w != NULL) uniform in [1,256). */
+int ogb_generate_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, double a, double b, double c,
+                      int permute, uint32_t *src, uint32_t *dst, float *w);
+/* Erdos-Renyi: num_edges uniform (src, dst) pairs over num_vertices ids. */
+int ogb_generate_uniform(uint32_t num_vertices, uint64_t num_edges, uint64_t seed, uint32_t *src, uint32_t *dst,
+                         float *w);
+/* side x side 4-neighbour grid (both directions) plus, per vertex with
+ * probability p, one shortcut to a random vertex.  Returns the edge count in
+ * *num_edges; call with src == NULL to get the capacity needed. */
+int ogb_generate_grid(uint32_t side, double p, uint64_t seed, uint32_t *src, uint32_t *dst, float *w,
+                      uint64_t *num_edges);
+/* Write {u32 src, u32 dst[, f32 w]} records (the reference .bin / .wbin). */
+int ogb_write_edge_file(const char *path, const uint32_t *src, const uint32_t *dst, const float *w,
+                        uint64_t num_edges);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OGB200_DEVICE_H */

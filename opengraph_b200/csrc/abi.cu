@@ -1,0 +1,1287 @@
+// abi.cu -- the OpenGraph C API over the device hot path (drop-in layer).
+//
+// Compiled twice: OGB200_WEIGHTED=0 -> libogb200.so, =1 -> libogb200_w.so.
+// Host structs keep the reference layouts (ogb200.h); sorting, CSR mapping,
+// BFS and PageRank run on the GPU.  A GraphCSR made by graphCSRPreProcessingStep
+// keeps its device copy in a side table keyed by the GraphCSR pointer, so the
+// algorithms do not upload it again; graphCSRFree drops it.  A GraphCSR built
+// elsewhere (for example by the reference's own CPU code) is uploaded on its
+// first use.
+//
+// Observable behaviour follows the reference: progress tables on stdout in the
+// reference's format, err(1)-style exits on I/O errors, NULL for unsupported
+// variants.  CUDA failures print the CUDA error and exit(1).
+#include <err.h>
+#include <fcntl.h>
+#include <stdarg.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <sys/time.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/ogb200.h"
+#include "../../include/ogb200_device.h"
+#include "graph.cuh"
+
+using namespace ogb;
+
+// ------------------------------------------------------------------ misc ----
+
+static int g_quiet = -1;
+
+static bool quiet() {
+  if (g_quiet < 0) {
+    const char* e = getenv("OGB200_QUIET");
+    g_quiet = (e && *e && *e != '0') ? 1 : 0;
+  }
+  return g_quiet == 1;
+}
+
+static void say(const char* fmt, ...) {
+  if (quiet()) return;
+  va_list ap;
+  va_start(ap, fmt);
+  vprintf(fmt, ap);
+  va_end(ap);
+}
+
+static void print_msg_time(const char* msg, double t) {
+  say(" -----------------------------------------------------\n");
+  say("| %-51s | \n", msg);
+  say(" -----------------------------------------------------\n");
+  say("| %-51f | \n", t);
+  say(" -----------------------------------------------------\n");
+}
+
+static double now_s() {
+  struct timeval tv;
+  gettimeofday(&tv, nullptr);
+  return tv.tv_sec + tv.tv_usec / 1e6;
+}
+
+// Allocation as the reference's my_malloc (128-byte aligned, free()-able).
+static void* host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (posix_memalign(&p, 128, bytes ? bytes : 128) != 0 || !p) {
+    fprintf(stderr, "Error, aligned_alloc!\n");
+    exit(EXIT_FAILURE);
+  }
+  return p;
+}
+
+[[noreturn]] static void die_status(const char* where, int st) {
+  fprintf(stderr, "ogb200: %s failed (status %d): %s\n", where, st, ogb::last_error());
+  exit(1);
+}
+
+#define OGB_MUST(call)                     \
+  do {                                     \
+    int _st = (call);                      \
+    if (_st != ::ogb::OK) die_status(#call, _st); \
+  } while (0)
+
+// Host <-> device copies of malloc'd (pageable) arrays run through a pinned
+// bounce buffer in chunks, double-buffered, with the host-side memcpy split
+// over threads.
+namespace {
+struct Bounce {
+  static constexpr size_t kChunk = 32u << 20;
+  void* h[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  std::mutex mu;
+  int init() {
+    if (h[0]) return OK;
+    for (int i = 0; i < 2; i++) {
+      OGB_CUDA(cudaMallocHost(&h[i], kChunk));
+      OGB_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
+    }
+    return OK;
+  }
+};
+Bounce& bounce() {
+  static Bounce b;
+  return b;
+}
+
+void par_memcpy(void* dst, const void* src, size_t n) {
+  const size_t kMin = 4u << 20;
+  unsigned nt = std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
+  if (n < kMin || nt == 1) {
+    memcpy(dst, src, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t chunk = (n + nt - 1) / nt;
+  for (unsigned t = 0; t < nt; t++) {
+    const size_t lo = t * chunk;
+    if (lo >= n) break;
+    const size_t len = std::min(chunk, n - lo);
+    th.emplace_back([=] { memcpy((char*)dst + lo, (const char*)src + lo, len); });
+  }
+  for (auto& x : th) x.join();
+}
+}  // namespace
+
+static int h2d(void* d, const void* h, size_t n, cudaStream_t s) {
+  if (!n) return OK;
+  Bounce& b = bounce();
+  std::lock_guard<std::mutex> lk(b.mu);
+  OGB_TRY(b.init());
+  size_t off = 0;
+  int i = 0;
+  while (off < n) {
+    const size_t len = std::min(Bounce::kChunk, n - off);
+    OGB_CUDA(cudaEventSynchronize(b.ev[i]));
+    par_memcpy(b.h[i], (const char*)h + off, len);
+    OGB_CUDA(cudaMemcpyAsync((char*)d + off, b.h[i], len, cudaMemcpyHostToDevice, s));
+    OGB_CUDA(cudaEventRecord(b.ev[i], s));
+    off += len;
+    i ^= 1;
+  }
+  OGB_CUDA(cudaStreamSynchronize(s));
+  return OK;
+}
+
+static int d2h(void* h, const void* d, size_t n, cudaStream_t s) {
+  if (!n) return OK;
+  Bounce& b = bounce();
+  std::lock_guard<std::mutex> lk(b.mu);
+  OGB_TRY(b.init());
+  // pipeline: copy chunk k+1 on the GPU while the host drains chunk k
+  size_t off = 0, pend_off = 0, pend_len = 0;
+  int i = 0, pend = -1;
+  while (off < n || pend >= 0) {
+    if (off < n) {
+      const size_t len = std::min(Bounce::kChunk, n - off);
+      OGB_CUDA(cudaMemcpyAsync(b.h[i], (const char*)d + off, len, cudaMemcpyDeviceToHost, s));
+      OGB_CUDA(cudaEventRecord(b.ev[i], s));
+      if (pend >= 0) {
+        OGB_CUDA(cudaEventSynchronize(b.ev[pend]));
+        par_memcpy((char*)h + pend_off, b.h[pend], pend_len);
+      }
+      pend = i;
+      pend_off = off;
+      pend_len = len;
+      off += len;
+      i ^= 1;
+    } else {
+      OGB_CUDA(cudaEventSynchronize(b.ev[pend]));
+      par_memcpy((char*)h + pend_off, b.h[pend], pend_len);
+      pend = -1;
+    }
+  }
+  return OK;
+}
+
+// ---------------------------------------------------------- device mirror ---
+
+struct ogb_graph {
+  DevGraph g;
+};
+
+namespace {
+struct MirrorEntry {
+  ogb_graph* dg;
+  const void* fwd_dst;   // host pointers the copy was made from
+  const void* inv_dst;
+  uint32_t V, E;
+};
+std::mutex g_mirror_mu;
+std::unordered_map<const GraphCSR*, MirrorEntry> g_mirrors;
+
+int upload_graph(const GraphCSR* h, ogb_graph* dg, cudaStream_t s) {
+  DevGraph& g = dg->g;
+  const uint32_t V = h->num_vertices, E = h->num_edges;
+  if (!h->vertices || !h->sorted_edges_array || !h->inverse_vertices || !h->inverse_sorted_edges_array)
+    return fail(ERR_ARG, "GraphCSR without both directions");
+  g.V = V;
+  g.E = E;
+  g.weighted = false;
+  for (int dir = 0; dir < 2; dir++) {
+    DevCSR& c = dir ? g.inv : g.fwd;
+    const Vertex* hv = dir ? h->inverse_vertices : h->vertices;
+    const EdgeList* he = dir ? h->inverse_sorted_edges_array : h->sorted_edges_array;
+    OGB_TRY(c.dst.alloc((size_t)E * 4 + 4));
+    OGB_TRY(c.out_degree.alloc((size_t)V * 4 + 4));
+    OGB_TRY(c.in_degree.alloc((size_t)V * 4 + 4));
+    OGB_TRY(c.edges_idx.alloc((size_t)V * 4 + 4));
+    OGB_TRY(c.rows.alloc((size_t)V * 8 + 8));
+    OGB_TRY(h2d(c.dst.p, he->edges_array_dest, (size_t)E * 4, s));
+    OGB_TRY(h2d(c.out_degree.p, hv->out_degree, (size_t)V * 4, s));
+    OGB_TRY(h2d(c.in_degree.p, hv->in_degree, (size_t)V * 4, s));
+    OGB_TRY(h2d(c.edges_idx.p, hv->edges_idx, (size_t)V * 4, s));
+    OGB_TRY(csr_pack_rows(c, V, s));
+  }
+  OGB_CUDA(cudaStreamSynchronize(s));
+  return OK;
+}
+}  // namespace
+
+static ogb_graph* mirror_of(const GraphCSR* h, int* status) {
+  std::lock_guard<std::mutex> lk(g_mirror_mu);
+  auto it = g_mirrors.find(h);
+  if (it != g_mirrors.end()) {
+    const MirrorEntry& m = it->second;
+    if (m.V == h->num_vertices && m.E == h->num_edges && m.fwd_dst == h->sorted_edges_array->edges_array_dest &&
+        m.inv_dst == h->inverse_sorted_edges_array->edges_array_dest) {
+      *status = OK;
+      return m.dg;
+    }
+    delete m.dg;
+    g_mirrors.erase(it);
+  }
+  ogb_graph* dg = new ogb_graph();
+  int st = upload_graph(h, dg, lib_stream());
+  if (st != OK) {
+    delete dg;
+    *status = st;
+    return nullptr;
+  }
+  g_mirrors[h] = {dg, h->sorted_edges_array->edges_array_dest, h->inverse_sorted_edges_array->edges_array_dest,
+                  h->num_vertices, h->num_edges};
+  *status = OK;
+  return dg;
+}
+
+static void mirror_set(const GraphCSR* h, ogb_graph* dg) {
+  std::lock_guard<std::mutex> lk(g_mirror_mu);
+  auto it = g_mirrors.find(h);
+  if (it != g_mirrors.end()) {
+    if (it->second.dg != dg) delete it->second.dg;
+    g_mirrors.erase(it);
+  }
+  g_mirrors[h] = {dg, h->sorted_edges_array->edges_array_dest, h->inverse_sorted_edges_array->edges_array_dest,
+                  h->num_vertices, h->num_edges};
+}
+
+static void mirror_drop(const GraphCSR* h) {
+  std::lock_guard<std::mutex> lk(g_mirror_mu);
+  auto it = g_mirrors.find(h);
+  if (it != g_mirrors.end()) {
+    delete it->second.dg;
+    g_mirrors.erase(it);
+  }
+}
+
+// ------------------------------------------------------------ RNG (MT) -----
+// Mersenne Twister MT19937 (Matsumoto & Nishimura, ACM TOMACS 8(1), 1998)
+// with the 1999 "sgenrand" seeding by the linear congruential map
+// x -> 69069 x + 1 that the reference uses (mt19937.c:54-67), so that root
+// draws and generated weights match it bit for bit.
+
+extern "C" void initializeMersenneState(mt19937state* m, unsigned long seed) {
+  unsigned long x = seed;
+  for (int i = 0; i < 624; i++) {
+    unsigned long hi = x & 0xffff0000UL;
+    x = 69069UL * x + 1UL;
+    unsigned long lo = (x & 0xffff0000UL) >> 16;
+    x = 69069UL * x + 1UL;
+    m->mt[i] = hi | lo;
+  }
+  m->mti = 624;
+}
+
+extern "C" unsigned long generateRandInt(mt19937state* m) {
+  const unsigned long upper = 0x80000000UL, lower = 0x7fffffffUL, twist = 0x9908b0dfUL;
+  if (m->mti >= 624) {
+    for (int k = 0; k < 624; k++) {
+      const unsigned long y = (m->mt[k] & upper) | (m->mt[(k + 1) % 624] & lower);
+      m->mt[k] = m->mt[(k + 397) % 624] ^ (y >> 1) ^ ((y & 1UL) ? twist : 0UL);
+    }
+    m->mti = 0;
+  }
+  unsigned long y = m->mt[m->mti++];
+  y ^= y >> 11;
+  y ^= (y << 7) & 0x9d2c5680UL;
+  y ^= (y << 15) & 0xefc60000UL;
+  y ^= y >> 18;
+  return y;
+}
+
+extern "C" float generateRandFloat(mt19937state* m) {
+  return ((float)generateRandInt(m)) * 2.3283064370807974e-10;
+}
+
+// ------------------------------------------------------------ edge lists ---
+
+extern "C" struct EdgeList* newEdgeList(uint32_t num_edges) {
+  EdgeList* e = (EdgeList*)host_alloc(sizeof(EdgeList));
+  e->edges_array_src = (uint32_t*)host_alloc((size_t)num_edges * 4);
+  e->edges_array_dest = (uint32_t*)host_alloc((size_t)num_edges * 4);
+  memset(e->edges_array_src, 0, (size_t)num_edges * 4);
+  memset(e->edges_array_dest, 0, (size_t)num_edges * 4);
+#if OGB200_WEIGHTED
+  e->edges_array_weight = (float*)host_alloc((size_t)num_edges * 4);
+  memset(e->edges_array_weight, 0, (size_t)num_edges * 4);
+  e->max_weight = 0;
+#endif
+  e->mask_array = nullptr;
+  e->label_array = nullptr;
+  e->inverse_label_array = nullptr;
+  e->num_edges = num_edges;
+  e->num_vertices = 0;
+  e->avg_degree = 0;
+  return e;
+}
+
+extern "C" void freeEdgeList(struct EdgeList* e) {
+  if (!e) return;
+  free(e->edges_array_src);
+  free(e->edges_array_dest);
+  free(e->mask_array);
+  free(e->label_array);
+  free(e->inverse_label_array);
+#if OGB200_WEIGHTED
+  free(e->edges_array_weight);
+#endif
+  free(e);
+}
+
+static void alloc_labels(EdgeList* e, uint32_t V) {
+  e->mask_array = (uint32_t*)host_alloc((size_t)V * 4);
+  e->label_array = (uint32_t*)host_alloc((size_t)V * 4);
+  e->inverse_label_array = (uint32_t*)host_alloc((size_t)V * 4);
+  for (uint32_t i = 0; i < V; i++) {
+    e->mask_array[i] = 0;
+    e->label_array[i] = i;
+    e->inverse_label_array[i] = i;
+  }
+}
+
+// readEdgeListsbin (edgeList.c:336-594): records of 8 bytes, or 12 when
+// weighted (the weight is read in the WEIGHTED layout and skipped in the
+// other); the WEIGHTED layout without file weights draws them from MT19937
+// seeded 27491095 in edge order.  symmetric appends the reversed copy.
+extern "C" struct EdgeList* readEdgeListsbin(const char* fname, uint8_t inverse, uint32_t symmetric,
+                                             uint32_t weighted) {
+  int fd = open(fname, O_RDONLY);
+  if (fd == -1) err(1, "open: %s", fname);
+  struct stat fs;
+  if (fstat(fd, &fs) == -1) err(1, "stat: %s", fname);
+  const size_t rec = weighted ? 12 : 8;
+  const uint32_t num_edges = (uint32_t)((uint64_t)fs.st_size / rec);
+  const uint32_t total = symmetric ? num_edges * 2 : num_edges;
+  EdgeList* e = newEdgeList(total);
+  const uint32_t* buf = nullptr;
+  if (fs.st_size > 0) {
+    void* addr = mmap(nullptr, fs.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
+    if (addr == MAP_FAILED) {
+      close(fd);
+      err(1, "mmap: %s", fname);
+    }
+    buf = (const uint32_t*)addr;
+  }
+  const uint32_t stride = (uint32_t)(rec / 4);
+#if OGB200_WEIGHTED
+  mt19937state* mt = nullptr;
+  if (!weighted) {
+    mt = (mt19937state*)host_alloc(sizeof(mt19937state));
+    initializeMersenneState(mt, 27491095);
+  }
+  float max_weight = 0;
+#endif
+  // parse in parallel (no weight draws), V = max id + 1
+  const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<uint32_t> vmax(nt, 0);
+  std::vector<std::thread> th;
+  const uint32_t chunk = (num_edges + nt - 1) / std::max(1u, nt);
+  for (unsigned t = 0; t < nt; t++) {
+    th.emplace_back([&, t] {
+      const uint64_t lo = (uint64_t)t * chunk, hi = std::min<uint64_t>(num_edges, lo + chunk);
+      uint32_t m = 0;
+      for (uint64_t i = lo; i < hi; i++) {
+        uint32_t s = buf[stride * i + 0], d = buf[stride * i + 1];
+        if (inverse) std::swap(s, d);
+        e->edges_array_src[i] = s;
+        e->edges_array_dest[i] = d;
+        if (symmetric) {
+          e->edges_array_src[i + num_edges] = d;
+          e->edges_array_dest[i + num_edges] = s;
+        }
+        m = std::max(m, std::max(s, d));
+#if OGB200_WEIGHTED
+        if (weighted) {
+          float wt;
+          memcpy(&wt, &buf[stride * i + 2], 4);
+          e->edges_array_weight[i] = wt;
+          if (symmetric) e->edges_array_weight[i + num_edges] = wt;
+        }
+#endif
+      }
+      vmax[t] = m;
+    });
+  }
+  for (auto& x : th) x.join();
+  uint32_t num_vertices = 0;
+  for (uint32_t m : vmax) num_vertices = std::max(num_vertices, m);
+#if OGB200_WEIGHTED
+  for (uint32_t i = 0; i < num_edges; i++) {
+    if (!weighted) {
+      e->edges_array_weight[i] = generateRandFloat(mt);
+      if (symmetric) e->edges_array_weight[i + num_edges] = e->edges_array_weight[i];
+    }
+    max_weight = std::max(max_weight, e->edges_array_weight[i]);
+  }
+  e->max_weight = max_weight;
+  free(mt);
+#endif
+  e->num_vertices = num_vertices + 1;
+  e->avg_degree = e->num_edges / e->num_vertices;
+  alloc_labels(e, e->num_vertices);
+  if (buf) munmap((void*)buf, fs.st_size);
+  close(fd);
+  return e;
+}
+
+// readEdgeListsMem (edgeList.c:597-745): copy of the list, src/dst swapped
+// when inverse; label arrays copied when present.
+extern "C" struct EdgeList* readEdgeListsMem(struct EdgeList* m, uint8_t inverse, uint32_t symmetric,
+                                             uint32_t weighted) {
+  (void)symmetric;
+  (void)weighted;
+  const uint32_t E = m->num_edges, V = m->num_vertices;
+  EdgeList* e = newEdgeList(E);
+  auto copy_arr = [&](uint32_t* src) -> uint32_t* {
+    if (!src) return nullptr;
+    uint32_t* d = (uint32_t*)host_alloc((size_t)V * 4);
+    memcpy(d, src, (size_t)V * 4);
+    return d;
+  };
+  e->mask_array = copy_arr(m->mask_array);
+  e->label_array = copy_arr(m->label_array);
+  e->inverse_label_array = copy_arr(m->inverse_label_array);
+  par_memcpy(inverse ? e->edges_array_src : e->edges_array_dest, m->edges_array_dest, (size_t)E * 4);
+  par_memcpy(inverse ? e->edges_array_dest : e->edges_array_src, m->edges_array_src, (size_t)E * 4);
+#if OGB200_WEIGHTED
+  par_memcpy(e->edges_array_weight, m->edges_array_weight, (size_t)E * 4);
+  e->max_weight = m->max_weight;
+#endif
+  e->num_vertices = V;
+  if (V) e->avg_degree = E / V;
+  return e;
+}
+
+// ---------------------------------------------------------------- sorting ---
+
+// Sort the arrays of a host edge list on the device (in place).
+// lex: by (src, dst); by_dst: by dst only.
+static int sort_host_list(EdgeList* e, bool lex, bool by_dst) {
+  const uint32_t E = e->num_edges;
+  if (E == 0) return OK;
+  cudaStream_t s = lib_stream();
+  DevBuf in_s, in_d, in_w, out_s, out_d, out_w;
+  SortWorkspace ws;
+  const bool w =
+#if OGB200_WEIGHTED
+      e->edges_array_weight != nullptr;
+#else
+      false;
+#endif
+  OGB_TRY(in_s.alloc((size_t)E * 4));
+  OGB_TRY(in_d.alloc((size_t)E * 4));
+  OGB_TRY(out_s.alloc((size_t)E * 4));
+  OGB_TRY(out_d.alloc((size_t)E * 4));
+  if (w) {
+    OGB_TRY(in_w.alloc((size_t)E * 4));
+    OGB_TRY(out_w.alloc((size_t)E * 4));
+  }
+  OGB_TRY(h2d(in_s.p, e->edges_array_src, (size_t)E * 4, s));
+  OGB_TRY(h2d(in_d.p, e->edges_array_dest, (size_t)E * 4, s));
+#if OGB200_WEIGHTED
+  if (w) OGB_TRY(h2d(in_w.p, e->edges_array_weight, (size_t)E * 4, s));
+#endif
+  KV in{in_s.as<uint32_t>(), in_d.as<uint32_t>(), w ? in_w.as<uint32_t>() : nullptr};
+  KV out{out_s.as<uint32_t>(), out_d.as<uint32_t>(), w ? out_w.as<uint32_t>() : nullptr};
+  if (by_dst) {
+    KV in2{in.v0, in.k, in.v1}, out2{out.v0, out.k, out.v1};
+    OGB_TRY(sort_pairs(in2, out2, E, ws, s));
+  } else if (lex) {
+    OGB_TRY(sort_pairs_lex(in, out, E, ws, s));
+  } else {
+    OGB_TRY(sort_pairs(in, out, E, ws, s));
+  }
+  OGB_TRY(sort_check(ws, s));
+  OGB_TRY(d2h(e->edges_array_src, out_s.p, (size_t)E * 4, s));
+  OGB_TRY(d2h(e->edges_array_dest, out_d.p, (size_t)E * 4, s));
+#if OGB200_WEIGHTED
+  if (w) OGB_TRY(d2h(e->edges_array_weight, out_w.p, (size_t)E * 4, s));
+#endif
+  return OK;
+}
+
+extern "C" struct EdgeList* radixSortEdgesBySource(struct EdgeList* e) {
+  OGB_MUST(sort_host_list(e, false, false));
+  return e;
+}
+extern "C" struct EdgeList* radixSortEdgesBySourceAndDestination(struct EdgeList* e) {
+  OGB_MUST(sort_host_list(e, true, false));
+  return e;
+}
+extern "C" struct EdgeList* countSortEdgesBySource(struct EdgeList* e) {
+  OGB_MUST(sort_host_list(e, false, false));
+  return e;
+}
+extern "C" struct EdgeList* countSortEdgesByDestination(struct EdgeList* e) {
+  OGB_MUST(sort_host_list(e, false, true));
+  return e;
+}
+extern "C" struct EdgeList* countSortEdgesBySourceAndDestination(struct EdgeList* e) {
+  OGB_MUST(sort_host_list(e, true, false));
+  return e;
+}
+
+// sortRunAlgorithms (sortRun.c:26-63).
+extern "C" struct EdgeList* sortRunAlgorithms(struct EdgeList* e, uint32_t sort) {
+  const double t0 = now_s();
+  const char* msg;
+  switch (sort) {
+    case 1:
+      e = radixSortEdgesBySourceAndDestination(e);
+      msg = "Radix Sort Edges By Source/Dest (Seconds)";
+      break;
+    case 2:
+      e = countSortEdgesBySource(e);
+      msg = "Count Sort Edges By Source (Seconds)";
+      break;
+    case 3:
+      e = countSortEdgesBySourceAndDestination(e);
+      msg = "Count Sort Edges By Source/Dest (Seconds)";
+      break;
+    default:
+      e = radixSortEdgesBySource(e);
+      msg = "Radix Sort Edges By Source (Seconds)";
+      break;
+  }
+  print_msg_time(msg, now_s() - t0);
+  return e;
+}
+
+// removeDulpicatesSelfLoopEdges (edgeList.c:138-211) on the device: drop
+// self loops, then drop every edge equal to the last kept one.  In the
+// WEIGHTED layout the reference passes kept weights through a uint32
+// temporary, i.e. truncates them to integers; that is reproduced.
+int dedup_device(const uint32_t* s, const uint32_t* d, const uint32_t* w, uint32_t E, uint32_t* os, uint32_t* od,
+                 uint32_t* ow, int truncate_weights, uint32_t* out_count, cudaStream_t st);
+
+extern "C" struct EdgeList* removeDulpicatesSelfLoopEdges(struct EdgeList* e) {
+  const uint32_t E = e->num_edges;
+  cudaStream_t s = lib_stream();
+  DevBuf a_s, a_d, a_w, b_s, b_d, b_w;
+  const bool w =
+#if OGB200_WEIGHTED
+      e->edges_array_weight != nullptr;
+#else
+      false;
+#endif
+  OGB_MUST(a_s.alloc((size_t)E * 4 + 4));
+  OGB_MUST(a_d.alloc((size_t)E * 4 + 4));
+  OGB_MUST(b_s.alloc((size_t)E * 4 + 4));
+  OGB_MUST(b_d.alloc((size_t)E * 4 + 4));
+  if (w) {
+    OGB_MUST(a_w.alloc((size_t)E * 4 + 4));
+    OGB_MUST(b_w.alloc((size_t)E * 4 + 4));
+  }
+  OGB_MUST(h2d(a_s.p, e->edges_array_src, (size_t)E * 4, s));
+  OGB_MUST(h2d(a_d.p, e->edges_array_dest, (size_t)E * 4, s));
+#if OGB200_WEIGHTED
+  if (w) OGB_MUST(h2d(a_w.p, e->edges_array_weight, (size_t)E * 4, s));
+#endif
+  uint32_t kept = 0;
+  OGB_MUST(dedup_device(a_s.as<uint32_t>(), a_d.as<uint32_t>(), w ? a_w.as<uint32_t>() : nullptr, E,
+                        b_s.as<uint32_t>(), b_d.as<uint32_t>(), w ? b_w.as<uint32_t>() : nullptr, 1, &kept, s));
+  EdgeList* t = newEdgeList(E);
+  OGB_MUST(d2h(t->edges_array_src, b_s.p, (size_t)kept * 4, s));
+  OGB_MUST(d2h(t->edges_array_dest, b_d.p, (size_t)kept * 4, s));
+#if OGB200_WEIGHTED
+  if (w) OGB_MUST(d2h(t->edges_array_weight, b_w.p, (size_t)kept * 4, s));
+  t->max_weight = e->max_weight;
+#endif
+  t->num_edges = kept;
+  t->num_vertices = e->num_vertices;
+  t->avg_degree = t->num_vertices ? t->num_edges / t->num_vertices : 0;
+  const uint32_t V = e->num_vertices;
+  t->mask_array = (uint32_t*)host_alloc((size_t)V * 4);
+  t->label_array = (uint32_t*)host_alloc((size_t)V * 4);
+  t->inverse_label_array = (uint32_t*)host_alloc((size_t)V * 4);
+  memcpy(t->mask_array, e->mask_array, (size_t)V * 4);
+  memcpy(t->label_array, e->label_array, (size_t)V * 4);
+  memcpy(t->inverse_label_array, e->inverse_label_array, (size_t)V * 4);
+  freeEdgeList(e);
+  return t;
+}
+
+// -------------------------------------------------------------------- CSR ---
+
+extern "C" struct Vertex* newVertexArray(uint32_t V) {
+  Vertex* v = (Vertex*)host_alloc(sizeof(Vertex));
+  v->out_degree = (uint32_t*)host_alloc((size_t)V * 4);
+  v->in_degree = (uint32_t*)host_alloc((size_t)V * 4);
+  v->edges_idx = (uint32_t*)host_alloc((size_t)V * 4);
+  memset(v->out_degree, 0, (size_t)V * 4);
+  memset(v->in_degree, 0, (size_t)V * 4);
+  memset(v->edges_idx, 0, (size_t)V * 4);
+  return v;
+}
+
+extern "C" void freeVertexArray(struct Vertex* v) {
+  if (!v) return;
+  free(v->edges_idx);
+  free(v->out_degree);
+  free(v->in_degree);
+  free(v);
+}
+
+extern "C" struct GraphCSR* graphCSRNew(uint32_t V, uint32_t E, uint8_t inverse) {
+  GraphCSR* g = (GraphCSR*)host_alloc(sizeof(GraphCSR));
+  g->num_vertices = V;
+  g->num_edges = E;
+  g->avg_degree = V ? E / V : 0;
+  g->sorted_edges_array = nullptr;
+  g->inverse_sorted_edges_array = nullptr;
+#if OGB200_WEIGHTED
+  g->max_weight = 0;
+#endif
+  g->vertices = newVertexArray(V);
+  g->inverse_vertices = inverse ? newVertexArray(V) : nullptr;
+  return g;
+}
+
+// mapVerticesWithInOutDegree (vertex.c:204-325) on the device for one host
+// direction: out_degree and edges_idx of that direction, in_degree of the
+// other (when it exists).
+extern "C" struct GraphCSR* mapVerticesWithInOutDegree(struct GraphCSR* graph, uint8_t inverse) {
+  EdgeList* e = inverse ? graph->inverse_sorted_edges_array : graph->sorted_edges_array;
+  Vertex* hv = inverse ? graph->inverse_vertices : graph->vertices;
+  Vertex* other = inverse ? graph->vertices : graph->inverse_vertices;
+  const uint32_t V = graph->num_vertices, E = graph->num_edges;
+  cudaStream_t s = lib_stream();
+  DevCSR c, o;
+  DevBuf err;
+  OGB_MUST(c.src.alloc((size_t)E * 4 + 4));
+  OGB_MUST(c.out_degree.alloc((size_t)V * 4 + 4));
+  OGB_MUST(c.edges_idx.alloc((size_t)V * 4 + 4));
+  OGB_MUST(c.rows.alloc((size_t)V * 8 + 8));
+  OGB_MUST(o.in_degree.alloc((size_t)V * 4 + 4));
+  OGB_MUST(err.alloc(16));
+  OGB_MUST(h2d(c.src.p, e->edges_array_src, (size_t)E * 4, s));
+  if (cudaMemsetAsync(err.p, 0, 16, s) != cudaSuccess) die_status("memset", ERR_CUDA);
+  OGB_MUST(csr_map(c, o, V, E, err.as<uint32_t>(), s));
+  uint32_t h_err = 0;
+  OGB_MUST(d2h(&h_err, err.p, 4, s));
+  if (h_err) {
+    fprintf(stderr, "ogb200: mapVerticesWithInOutDegree: a source id is >= num_vertices (%u)\n", V);
+    exit(1);
+  }
+  OGB_MUST(d2h(hv->out_degree, c.out_degree.p, (size_t)V * 4, s));
+  OGB_MUST(d2h(hv->edges_idx, c.edges_idx.p, (size_t)V * 4, s));
+  if (other) OGB_MUST(d2h(other->in_degree, o.in_degree.p, (size_t)V * 4, s));
+  return graph;
+}
+
+extern "C" struct GraphCSR* graphCSRAssignEdgeList(struct GraphCSR* graphCSR, struct EdgeList* edgeList,
+                                                   uint8_t inverse) {
+  if (inverse)
+    graphCSR->inverse_sorted_edges_array = edgeList;
+  else
+    graphCSR->sorted_edges_array = edgeList;
+#if OGB200_WEIGHTED
+  graphCSR->max_weight = edgeList->max_weight;
+#endif
+  return mapVerticesWithInOutDegree(graphCSR, inverse);
+}
+
+static void print_max_degree(const Vertex* v, uint32_t V, bool in) {
+  uint32_t best = 0, idx = 0;
+  for (uint32_t i = 0; i < V; i++) {
+    best = std::max(best, v->out_degree[i]);
+    if (v->out_degree[i] == best) idx = i;
+  }
+  say(" -----------------------------------------------------\n");
+  if (!in) {
+    say("| %-15s | %-15s | %-15s | \n", "Node", "*max_out_degree", "in_degree");
+    say(" -----------------------------------------------------\n");
+    say("| %-15u | %-15u | %-15u | \n", idx, V ? v->out_degree[idx] : 0, V ? v->in_degree[idx] : 0);
+  } else {
+    say("| %-15s | %-15s | %-15s | \n", "Node", "out_degree", "*max_in_degree");
+    say(" -----------------------------------------------------\n");
+    say("| %-15u | %-15u | %-15u | \n", idx, V ? v->in_degree[idx] : 0, V ? v->out_degree[idx] : 0);
+  }
+  say(" -----------------------------------------------------\n");
+}
+
+// graphCSRPrint (graphCSR.c:66-104).
+extern "C" void graphCSRPrint(struct GraphCSR* g) {
+  if (quiet()) return;
+  say(" -----------------------------------------------------\n");
+  say("| %-51s | \n", "GraphCSR Properties");
+  say(" -----------------------------------------------------\n");
+#if OGB200_WEIGHTED
+  say("| %-51s | \n", "WEIGHTED");
+  say("| %-51s | \n", "MAX WEIGHT");
+  say("| %-51f | \n", g->max_weight);
+#else
+  say("| %-51s | \n", "UN-WEIGHTED");
+#endif
+  say("| %-51s | \n", "DIRECTED");
+  say(" -----------------------------------------------------\n");
+  say("| %-51s | \n", "Average Degree (D)");
+  say("| %-51u | \n", g->avg_degree);
+  say(" -----------------------------------------------------\n");
+  say("| %-51s | \n", "Number of Vertices (V)");
+  say("| %-51u | \n", g->num_vertices);
+  say(" -----------------------------------------------------\n");
+  say("| %-51s | \n", "Number of Edges (E)");
+  say("| %-51u | \n", g->num_edges);
+  say(" -----------------------------------------------------\n");
+  print_max_degree(g->vertices, g->num_vertices, false);
+  if (g->inverse_vertices) print_max_degree(g->inverse_vertices, g->num_vertices, true);
+}
+
+// Reorder/mask stages of the reference (reorder.c) are outside this
+// library; in a link with the reference objects their definitions are used.
+extern "C" struct EdgeList* reorderGraphProcess(struct EdgeList*, struct Arguments*) __attribute__((weak));
+extern "C" struct EdgeList* maskGraphProcess(struct EdgeList*, struct Arguments*) __attribute__((weak));
+
+// Download the device CSR into freshly allocated host structs.
+static int download_graph(DevGraph& g, GraphCSR* h, EdgeList* fwd_list, EdgeList* inv_list, cudaStream_t s) {
+  const uint32_t V = g.V, E = g.E;
+  for (int dir = 0; dir < 2; dir++) {
+    DevCSR& c = dir ? g.inv : g.fwd;
+    EdgeList* e = dir ? inv_list : fwd_list;
+    Vertex* v = dir ? h->inverse_vertices : h->vertices;
+    OGB_TRY(d2h(e->edges_array_src, c.src.p, (size_t)E * 4, s));
+    OGB_TRY(d2h(e->edges_array_dest, c.dst.p, (size_t)E * 4, s));
+#if OGB200_WEIGHTED
+    if (g.weighted) OGB_TRY(d2h(e->edges_array_weight, c.w.p, (size_t)E * 4, s));
+#endif
+    OGB_TRY(d2h(v->out_degree, c.out_degree.p, (size_t)V * 4, s));
+    OGB_TRY(d2h(v->in_degree, c.in_degree.p, (size_t)V * 4, s));
+    OGB_TRY(d2h(v->edges_idx, c.edges_idx.p, (size_t)V * 4, s));
+  }
+  return OK;
+}
+
+// graphCSRPreProcessingStep (graphCSR.c:164-248): read, sort, [dedup],
+// [reorder/mask through the reference], CSR both directions.  The whole
+// build runs on the device from one upload; the host struct receives the
+// results, and the device copy stays for the algorithms.
+extern "C" struct GraphCSR* graphCSRPreProcessingStep(struct Arguments* arguments) {
+  double t0 = now_s();
+  EdgeList* edges = readEdgeListsbin(arguments->fnameb, 0, arguments->symmetric, arguments->weighted);
+  print_msg_time("Read Edge List From File (Seconds)", now_s() - t0);
+
+  const bool host_stages = arguments->lmode || arguments->lmode_l2 || arguments->lmode_l3 || arguments->mmode;
+  if (host_stages) {
+    // Relabelling stages need the reference's reorder code on host lists.
+    if (!reorderGraphProcess || !maskGraphProcess) {
+      fprintf(stderr, "ogb200: reorder/mask modes (-l/-L/-O/-M) need the reference's reorder.c in the link\n");
+      exit(1);
+    }
+    edges = sortRunAlgorithms(edges, arguments->sort);
+    if (arguments->dflag) {
+      t0 = now_s();
+      edges = removeDulpicatesSelfLoopEdges(edges);
+      print_msg_time("Removing duplicate edges (Seconds)", now_s() - t0);
+    }
+    uint32_t modes[3] = {arguments->lmode, arguments->lmode_l2, arguments->lmode_l3};
+    for (int i = 0; i < 3; i++) {
+      arguments->lmode = modes[i];
+      if (arguments->lmode) {
+        edges = reorderGraphProcess(edges, arguments);
+        edges = sortRunAlgorithms(edges, arguments->sort);
+      }
+    }
+    if (arguments->mmode) edges = maskGraphProcess(edges, arguments);
+  }
+
+  cudaStream_t s = lib_stream();
+  ogb_graph* dg = new ogb_graph();
+  DevGraph& g = dg->g;
+  uint32_t E = edges->num_edges;
+  const uint32_t V = edges->num_vertices;
+#if OGB200_WEIGHTED
+  const bool w = edges->edges_array_weight != nullptr;
+#else
+  const bool w = false;
+#endif
+  OGB_MUST(g.input_src.alloc((size_t)E * 4 + 4));
+  OGB_MUST(g.input_dst.alloc((size_t)E * 4 + 4));
+  if (w) OGB_MUST(g.input_w.alloc((size_t)E * 4 + 4));
+  OGB_MUST(h2d(g.input_src.p, edges->edges_array_src, (size_t)E * 4, s));
+  OGB_MUST(h2d(g.input_dst.p, edges->edges_array_dest, (size_t)E * 4, s));
+#if OGB200_WEIGHTED
+  if (w) OGB_MUST(h2d(g.input_w.p, edges->edges_array_weight, (size_t)E * 4, s));
+#endif
+  const float* in_w = w ? g.input_w.as<float>() : nullptr;
+
+  if (!host_stages && arguments->dflag) {
+    // sort, dedup on the device, then the CSR build re-sorts (a no-op order)
+    t0 = now_s();
+    KV in{g.input_src.as<uint32_t>(), g.input_dst.as<uint32_t>(), w ? g.input_w.as<uint32_t>() : nullptr};
+    DevBuf ss, sd, sw;
+    OGB_MUST(ss.alloc((size_t)E * 4 + 4));
+    OGB_MUST(sd.alloc((size_t)E * 4 + 4));
+    if (w) OGB_MUST(sw.alloc((size_t)E * 4 + 4));
+    KV out{ss.as<uint32_t>(), sd.as<uint32_t>(), w ? sw.as<uint32_t>() : nullptr};
+    const bool lex = arguments->sort == 1 || arguments->sort == 3;
+    OGB_MUST(lex ? sort_pairs_lex(in, out, E, g.sort_ws, s) : sort_pairs(in, out, E, g.sort_ws, s));
+    OGB_MUST(sort_check(g.sort_ws, s));
+    print_msg_time("Radix Sort Edges By Source (Seconds)", now_s() - t0);
+    t0 = now_s();
+    uint32_t kept = 0;
+    OGB_MUST(dedup_device(out.k, out.v0, out.v1, E, in.k, in.v0, in.v1, 1, &kept, s));
+    print_msg_time("Removing duplicate edges (Seconds)", now_s() - t0);
+    E = kept;
+    // host list mirrors the deduplicated sorted list
+    edges->num_edges = E;
+    edges->avg_degree = V ? E / V : 0;
+  }
+
+  t0 = now_s();
+  OGB_MUST(graph_build(g, g.input_src.as<uint32_t>(), g.input_dst.as<uint32_t>(), in_w, E, V, arguments->sort, s));
+  OGB_MUST(graph_check(g, s));
+  const double t_build = now_s() - t0;
+  g.input_src.release();
+  g.input_dst.release();
+  g.input_w.release();
+
+  GraphCSR* h = graphCSRNew(V, E, 1);
+  EdgeList* inv = newEdgeList(E);
+  inv->num_vertices = V;
+  inv->avg_degree = V ? E / V : 0;
+  auto copy_arr = [&](uint32_t* src) -> uint32_t* {
+    if (!src) return nullptr;
+    uint32_t* d = (uint32_t*)host_alloc((size_t)V * 4);
+    memcpy(d, src, (size_t)V * 4);
+    return d;
+  };
+  inv->mask_array = copy_arr(edges->mask_array);
+  inv->label_array = copy_arr(edges->label_array);
+  inv->inverse_label_array = copy_arr(edges->inverse_label_array);
+#if OGB200_WEIGHTED
+  inv->max_weight = edges->max_weight;
+  h->max_weight = edges->max_weight;
+  if (!w) {
+    free(inv->edges_array_weight);
+    inv->edges_array_weight = nullptr;
+  }
+#endif
+  t0 = now_s();
+  OGB_MUST(download_graph(g, h, edges, inv, s));
+  h->sorted_edges_array = edges;
+  h->inverse_sorted_edges_array = inv;
+  print_msg_time("Radix Sort + CSR both directions on GPU (Seconds)", t_build);
+  print_msg_time("Copy GraphCSR to host (Seconds)", now_s() - t0);
+  // the device copy no longer needs the sorted src arrays
+  mirror_set(h, dg);
+  graphCSRPrint(h);
+  return h;
+}
+
+extern "C" void graphCSRFree(struct GraphCSR* g) {
+  if (!g) return;
+  mirror_drop(g);
+  freeVertexArray(g->vertices);
+  freeEdgeList(g->sorted_edges_array);
+  freeVertexArray(g->inverse_vertices);
+  freeEdgeList(g->inverse_sorted_edges_array);
+  free(g);
+}
+
+// -------------------------------------------------------------------- BFS ---
+
+extern "C" struct BFSStats* newBFSStatsGraphCSR(struct GraphCSR* graph) {
+  const uint32_t V = graph->num_vertices;
+  BFSStats* st = (BFSStats*)host_alloc(sizeof(BFSStats));
+  st->distances = (uint32_t*)host_alloc((size_t)V * 4);
+  st->distances_DualOrder = (uint32_t*)host_alloc((size_t)V * 4);
+  st->parents = (int*)host_alloc((size_t)V * 4);
+  st->parents_DualOrder = (int*)host_alloc((size_t)V * 4);
+  st->processed_nodes = 0;
+  st->iteration = 0;
+  st->num_vertices = V;
+  st->time_total = 0.0;
+  for (uint32_t v = 0; v < V; v++) {
+    st->distances[v] = 0;
+    const uint32_t d = graph->vertices->out_degree[v];
+    st->parents[v] = d ? -(int)d : -1;
+    st->parents_DualOrder[v] = st->parents[v];
+  }
+  return st;
+}
+
+extern "C" void freeBFSStats(struct BFSStats* st) {
+  if (!st) return;
+  free(st->distances);
+  free(st->parents);
+  free(st->distances_DualOrder);
+  free(st->parents_DualOrder);
+  free(st);
+}
+
+static BfsResult g_last_bfs;  // level trace of the last drop-in BFS
+
+static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, uint32_t mode, const char* title,
+                                   bool bitmap_nf) {
+  BFSStats* st = newBFSStatsGraphCSR(graph);
+  const uint32_t V = graph->num_vertices;
+  // The reference checks source > V (BFS.c:482); source == V would index
+  // past the label array there, so it is rejected here too.
+  if (a->source < 0 || (uint32_t)a->source >= V) {
+    say(" -----------------------------------------------------\n");
+    say("| %-51s | \n", "ERROR!! CHECK SOURCE RANGE");
+    say(" -----------------------------------------------------\n");
+    return st;
+  }
+  const uint32_t* labels = graph->sorted_edges_array ? graph->sorted_edges_array->label_array : nullptr;
+  a->source = labels ? (int)labels[a->source] : a->source;
+  say(" -----------------------------------------------------\n");
+  say("| %-51s | \n", title);
+  say(" -----------------------------------------------------\n");
+  say("| %-51u | \n", (uint32_t)a->source);
+  say(" -----------------------------------------------------\n");
+  say("| %-15s | %-15s | %-15s | \n", "Iteration", "Nodes", "Time (Seconds)");
+  say(" -----------------------------------------------------\n");
+  int status = OK;
+  ogb_graph* dg = mirror_of(graph, &status);
+  if (!dg) die_status("device copy of GraphCSR", status);
+  cudaStream_t s = lib_stream();
+  DevBuf d_par, d_dist;
+  OGB_MUST(d_par.alloc((size_t)V * 4 + 4));
+  OGB_MUST(d_dist.alloc((size_t)V * 4 + 4));
+  BfsResult& r = g_last_bfs;
+  const double t0 = now_s();
+  OGB_MUST(bfs_run(dg->g, (uint32_t)a->source, mode, d_par.as<int32_t>(), d_dist.as<uint32_t>(), &r, !quiet(),
+                   bitmap_nf, s));
+  const double t_trav = now_s() - t0;
+  OGB_MUST(d2h(st->parents, d_par.p, (size_t)V * 4, s));
+  OGB_MUST(d2h(st->distances, d_dist.p, (size_t)V * 4, s));
+  st->processed_nodes = r.processed_nodes;
+  st->iteration = r.iteration;
+  st->time_total = t_trav;
+  if (!quiet()) {
+    say("| %s %-12u | %-15u | %-15f | \n", mode == BFS_PULL ? "BU" : "TD", 0u, 1u, 0.0);
+    for (int i = 0; i < r.nlevels; i++) {
+      const BfsLevel& L = r.levels[i];
+      say("| %s %-12u | %-15u | %-15f | \n", L.direction ? "BU" : "TD", (uint32_t)(i + 1), L.discovered,
+          L.ms / 1000.0);
+    }
+    say(" -----------------------------------------------------\n");
+    say("| %-15s | %-15u | %-15f | \n", "No OverHead", st->processed_nodes, r.ms / 1000.0);
+    say(" -----------------------------------------------------\n");
+    say(" -----------------------------------------------------\n");
+    say("| %-15s | %-15u | %-15f | \n", "total", st->processed_nodes, st->time_total);
+    say(" -----------------------------------------------------\n");
+  }
+  return st;
+}
+
+extern "C" struct BFSStats* breadthFirstSearchPullGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  return bfs_dropin(a, g, BFS_PULL, "Starting BFS PULL/BU (SOURCE NODE)", false);
+}
+extern "C" struct BFSStats* breadthFirstSearchPushGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  return bfs_dropin(a, g, BFS_PUSH, "Starting BFS PUSH/TD (SOURCE NODE)", false);
+}
+extern "C" struct BFSStats* breadthFirstSearchDirectionOptimizedGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  return bfs_dropin(a, g, BFS_DO, "Starting BFS PUSH/PULL(SOURCE NODE)", false);
+}
+extern "C" struct BFSStats* breadthFirstSearchPushBitmapGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  return bfs_dropin(a, g, BFS_PUSH, "Starting BFS PUSH/Bitmap (SOURCE NODE)", false);
+}
+extern "C" struct BFSStats* breadthFirstSearchPushDirectionOptimizedBitmapGraphCSR(struct Arguments* a,
+                                                                                   struct GraphCSR* g) {
+  return bfs_dropin(a, g, BFS_DO, "Starting BFS PUSH/PULL Bitmap (SOURCE NODE)", true);
+}
+
+// breadthFirstSearchGraphCSR (BFS.c:238-268).
+extern "C" struct BFSStats* breadthFirstSearchGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  switch (a->pushpull) {
+    case 0:
+      return breadthFirstSearchPullGraphCSR(a, g);
+    case 1:
+      return breadthFirstSearchPushGraphCSR(a, g);
+    case 2:
+      return breadthFirstSearchDirectionOptimizedGraphCSR(a, g);
+    case 3:
+      return breadthFirstSearchPushBitmapGraphCSR(a, g);
+    case 4:
+      return breadthFirstSearchPushDirectionOptimizedBitmapGraphCSR(a, g);
+    default:
+      return breadthFirstSearchDirectionOptimizedGraphCSR(a, g);
+  }
+}
+
+// Single-level steps over host state (BFS.c:639-754).
+int bfs_td_step_host(ogb::DevGraph& g, const uint32_t* q, uint32_t qsize, int32_t* parents, uint32_t* distances,
+                     uint32_t* next_q, uint32_t* next_size, uint32_t* mf, cudaStream_t s);
+int bfs_bu_step_host(ogb::DevGraph& g, const uint32_t* bm_cur, uint32_t* bm_next, int32_t* parents,
+                     uint32_t* distances, uint32_t* nf, cudaStream_t s);
+
+extern "C" uint32_t topDownStepGraphCSR(struct GraphCSR* graph, struct ArrayQueue* q, struct ArrayQueue** local,
+                                        struct BFSStats* stats) {
+  (void)local;
+  int status = OK;
+  ogb_graph* dg = mirror_of(graph, &status);
+  if (!dg) die_status("device copy of GraphCSR", status);
+  uint32_t next_size = 0, mf = 0;
+  OGB_MUST(bfs_td_step_host(dg->g, q->queue + q->head, q->tail - q->head, stats->parents, stats->distances,
+                            q->queue + q->tail_next, &next_size, &mf, lib_stream()));
+  q->tail_next += next_size;
+  return mf;
+}
+
+extern "C" uint32_t bottomUpStepGraphCSR(struct GraphCSR* graph, struct Bitmap* cur, struct Bitmap* next,
+                                         struct BFSStats* stats) {
+  int status = OK;
+  ogb_graph* dg = mirror_of(graph, &status);
+  if (!dg) die_status("device copy of GraphCSR", status);
+  uint32_t nf = 0;
+  OGB_MUST(bfs_bu_step_host(dg->g, cur->bitarray, next->bitarray, stats->parents, stats->distances, &nf,
+                            lib_stream()));
+  return nf;
+}
+
+// --------------------------------------------------------------- PageRank ---
+
+extern "C" struct PageRankStats* newPageRankStatsGraphCSR(struct GraphCSR* graph) {
+  const uint32_t V = graph->num_vertices;
+  PageRankStats* st = (PageRankStats*)host_alloc(sizeof(PageRankStats));
+  st->damp = 0.85f;
+  st->base_pr = 1.0f - st->damp;
+  st->iterations = 0;
+  st->num_vertices = V;
+  st->time_total = 0.0;
+  st->error_total = 0.0;
+  st->activeVertices = 0;
+  st->realRanks = (uint32_t*)host_alloc((size_t)V * 4);
+  st->pageRanks = (float*)host_alloc((size_t)V * 4);
+  for (uint32_t v = 0; v < V; v++) {
+    st->pageRanks[v] = st->base_pr;
+    st->realRanks[v] = v;
+  }
+  return st;
+}
+
+extern "C" void freePageRankStats(struct PageRankStats* st) {
+  if (!st) return;
+  free(st->realRanks);
+  free(st->pageRanks);
+  free(st);
+}
+
+static struct PageRankStats* pr_dropin(struct Arguments* a, struct GraphCSR* graph, uint32_t mode,
+                                       const char* title) {
+  PageRankStats* st = newPageRankStatsGraphCSR(graph);
+  say(" -----------------------------------------------------\n");
+  say("| %-51s | \n", title);
+  say(" -----------------------------------------------------\n");
+  say("| %-51.13lf | \n", a->epsilon);
+  say(" -----------------------------------------------------\n");
+  say("| %-10s | %-8s | %-15s | %-9s | \n", "Iteration", "Active", "Error", "Time (S)");
+  say(" -----------------------------------------------------\n");
+  int status = OK;
+  ogb_graph* dg = mirror_of(graph, &status);
+  if (!dg) die_status("device copy of GraphCSR", status);
+  cudaStream_t s = lib_stream();
+  const uint32_t V = graph->num_vertices;
+  DevBuf d_pr;
+  OGB_MUST(d_pr.alloc((size_t)V * 4 + 4));
+  static PrResult r;
+  const double t0 = now_s();
+  OGB_MUST(pagerank_run(dg->g, mode, a->iterations, a->epsilon, d_pr.as<float>(), nullptr, &r, s));
+  OGB_MUST(d2h(st->pageRanks, d_pr.p, (size_t)V * 4, s));
+  st->time_total = now_s() - t0;
+  st->iterations = r.iterations;
+  st->error_total = r.error_total;
+  st->activeVertices = r.activeVertices;
+  if (!quiet()) {
+    const double per = r.executed ? (r.ms / 1000.0) / r.executed : 0.0;
+    for (uint32_t i = 0; i < r.executed && i < 1024; i++)
+      say("| %-10u | %-8u | %-15.13lf | %-9f | \n", i, r.active_hist[i], r.err_hist[i], per);
+    double sum = 0.0;
+    for (uint32_t v = 0; v < V; v++) sum += st->pageRanks[v];
+    say(" -----------------------------------------------------\n");
+    say("| %-10s | %-8s | %-15s | %-9s | \n", "Iterations", "PR Sum", "Error", "Time (S)");
+    say(" -----------------------------------------------------\n");
+    say("| %-10u | %-8lf | %-15.13lf | %-9f | \n", st->iterations, sum, st->error_total, st->time_total);
+    say(" -----------------------------------------------------\n");
+  }
+  return st;
+}
+
+extern "C" struct PageRankStats* pageRankPullGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  return pr_dropin(a, g, PR_PULL, "Starting Page Rank Pull (tolerance/epsilon)");
+}
+extern "C" struct PageRankStats* pageRankPushGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  return pr_dropin(a, g, PR_PUSH, "Starting Page Rank Push (tolerance/epsilon)");
+}
+
+// pageRankGraphCSR (pageRank.c:871-936): pull and push are provided; the
+// fixed-point, quantized and data-driven variants are not part of this
+// library.
+extern "C" struct PageRankStats* pageRankGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  switch (a->pushpull) {
+    case 0:
+      return pageRankPullGraphCSR(a, g);
+    case 1:
+      return pageRankPushGraphCSR(a, g);
+    default:
+      if (a->pushpull > 13) return pageRankPullGraphCSR(a, g);
+      say(" -----------------------------------------------------\n");
+      say("| %-51s | \n", "PR variant not provided by ogb200 (use 0 or 1)");
+      say(" -----------------------------------------------------\n");
+      return nullptr;
+  }
+}
+
+// ------------------------------------------------------------------ roots ---
+
+// generateRandomRootGraphCSR (graphRun.c:537-556).
+extern "C" uint32_t generateRandomRootGraphCSR(mt19937state* mt, struct GraphCSR* graph) {
+  const uint32_t* labels = graph->sorted_edges_array ? graph->sorted_edges_array->label_array : nullptr;
+  for (;;) {
+    const uint32_t source = (uint32_t)generateRandInt(mt);
+    if (source < graph->num_vertices) {
+      const uint32_t t = labels ? labels[source] : source;
+      if (graph->vertices->out_degree[t] > graph->avg_degree) return source;
+    }
+  }
+}
+
+// ------------------------------------------------------------- device API ---
+
+extern "C" const char* ogb_last_error(void) { return ogb::last_error(); }
+extern "C" int ogb_weighted_layout(void) { return OGB200_WEIGHTED; }
+extern "C" void ogb_set_quiet(int q) { g_quiet = q ? 1 : 0; }
+
+extern "C" int ogb_graph_create(ogb_graph** g) {
+  if (!g) return fail(ERR_ARG, "null");
+  *g = new ogb_graph();
+  return OK;
+}
+
+extern "C" void ogb_graph_destroy(ogb_graph* g) { delete g; }
+
+static cudaStream_t as_stream(void* s) { return s ? (cudaStream_t)s : lib_stream(); }
+
+extern "C" int ogb_graph_build(ogb_graph* g, const uint32_t* d_src, const uint32_t* d_dst, const float* d_w,
+                               uint32_t E, uint32_t V, uint32_t sort_type, void* stream) {
+  if (!g) return fail(ERR_ARG, "null graph");
+  if (E && (!d_src || !d_dst)) return fail(ERR_ARG, "null edge arrays");
+  cudaStream_t s = as_stream(stream);
+  OGB_TRY(graph_build(g->g, d_src, d_dst, d_w, E, V, sort_type, s));
+  return graph_check(g->g, s);
+}
+
+extern "C" int ogb_graph_view(ogb_graph* g, int inverse, ogb_csr_view* v) {
+  if (!g || !v) return fail(ERR_ARG, "null");
+  DevCSR& c = inverse ? g->g.inv : g->g.fwd;
+  v->num_vertices = g->g.V;
+  v->num_edges = g->g.E;
+  v->src = c.d_src();
+  v->dst = c.d_dst();
+  v->weight = c.d_w();
+  v->out_degree = c.d_out_degree();
+  v->in_degree = c.d_in_degree();
+  v->edges_idx = c.d_edges_idx();
+  return OK;
+}
+
+extern "C" ogb_graph* ogb_graph_of(const void* graphCSR) {
+  int st = OK;
+  return mirror_of((const GraphCSR*)graphCSR, &st);
+}
+
+extern "C" int ogb_sort_edges(const uint32_t* d_src, const uint32_t* d_dst, const float* d_w, uint32_t E,
+                              uint32_t sort_type, uint32_t* o_src, uint32_t* o_dst, float* o_w, void* stream) {
+  cudaStream_t s = as_stream(stream);
+  static SortWorkspace* ws = new SortWorkspace();
+  KV in{const_cast<uint32_t*>(d_src), const_cast<uint32_t*>(d_dst), (uint32_t*)(d_w)};
+  KV out{o_src, o_dst, (uint32_t*)o_w};
+  if (d_w && !o_w) return fail(ERR_ARG, "weighted sort needs an output weight array");
+  if (!d_w) out.v1 = nullptr;
+  const bool lex = sort_type == 1 || sort_type == 3;
+  OGB_TRY(lex ? sort_pairs_lex(in, out, E, *ws, s) : sort_pairs(in, out, E, *ws, s));
+  return sort_check(*ws, s);
+}
+
+extern "C" int ogb_bfs(ogb_graph* g, uint32_t root, uint32_t mode, int32_t* d_parents, uint32_t* d_distances,
+                       ogb_bfs_info* info, void* stream) {
+  if (!g || !d_parents || !d_distances) return fail(ERR_ARG, "null");
+  if (mode > 2) return fail(ERR_ARG, "bfs mode %u", mode);
+  static thread_local BfsResult r;
+  OGB_TRY(bfs_run(g->g, root, mode, d_parents, d_distances, &r, false, false, as_stream(stream)));
+  g->g.bfs_last_levels = r.nlevels;
+  if (info) {
+    info->iteration = r.iteration;
+    info->processed_nodes = r.processed_nodes;
+    info->td_steps = r.td_steps;
+    info->bu_steps = r.bu_steps;
+    info->reached = r.reached;
+    info->levels = (uint32_t)r.nlevels;
+    info->reached_out_edges = r.reached_out_edges;
+    info->edges_examined = r.edges_examined;
+    info->ms = r.ms;
+  }
+  memcpy(g->g.bfs_trace, r.levels, sizeof(r.levels[0]) * std::min(r.nlevels, 512));
+  return OK;
+}
+
+extern "C" int ogb_bfs_trace(ogb_graph* g, ogb_bfs_level* levels, uint32_t max_levels, uint32_t* count) {
+  if (!g) return fail(ERR_ARG, "null");
+  const uint32_t n = std::min<uint32_t>(max_levels, (uint32_t)g->g.bfs_last_levels);
+  for (uint32_t i = 0; i < n; i++) {
+    const BfsLevel& L = g->g.bfs_trace[i];
+    levels[i].direction = L.direction;
+    levels[i].discovered = L.discovered;
+    levels[i].frontier = L.frontier;
+    levels[i].mf = L.mf;
+    levels[i].mu = L.mu;
+    levels[i].pad = 0;
+    levels[i].edges = L.edges;
+    levels[i].ms = L.ms;
+    levels[i].pad2 = 0;
+  }
+  if (count) *count = n;
+  return OK;
+}
+
+extern "C" int ogb_pagerank(ogb_graph* g, uint32_t mode, uint32_t max_iters, double eps, float* d_ranks,
+                            const float* d_init, ogb_pr_info* info, void* stream) {
+  if (!g || !d_ranks) return fail(ERR_ARG, "null");
+  if (mode > 1) return fail(ERR_ARG, "pagerank mode %u", mode);
+  static thread_local PrResult r;
+  OGB_TRY(pagerank_run(g->g, mode, max_iters, eps, d_ranks, d_init, &r, as_stream(stream)));
+  g->g.pr_last_executed = r.executed;
+  memcpy(g->g.pr_err_hist, r.err_hist, sizeof(double) * std::min<uint32_t>(r.executed, 1024));
+  memcpy(g->g.pr_active_hist, r.active_hist, sizeof(uint32_t) * std::min<uint32_t>(r.executed, 1024));
+  if (info) {
+    info->iterations = r.iterations;
+    info->executed = r.executed;
+    info->activeVertices = r.activeVertices;
+    info->converged = r.converged;
+    info->error_total = r.error_total;
+    info->ms = r.ms;
+  }
+  return OK;
+}
+
+extern "C" int ogb_pagerank_history(ogb_graph* g, double* errors, uint32_t* active, uint32_t max_entries,
+                                    uint32_t* count) {
+  if (!g) return fail(ERR_ARG, "null");
+  const uint32_t n = std::min<uint32_t>(max_entries, g->g.pr_last_executed);
+  for (uint32_t i = 0; i < n; i++) {
+    if (errors) errors[i] = g->g.pr_err_hist[i];
+    if (active) active[i] = g->g.pr_active_hist[i];
+  }
+  if (count) *count = n;
+  return OK;
+}

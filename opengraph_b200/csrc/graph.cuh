@@ -1,0 +1,142 @@
+// graph.cuh -- device-resident GraphCSR (both directions) and the entry
+// points of the hot-path modules (build, BFS, PageRank).
+#pragma once
+#include "common.cuh"
+#include "sort.cuh"
+
+namespace ogb {
+
+// One direction of a CSR on the device.  Field meaning follows the
+// reference's struct Vertex + struct EdgeList (vertex.h:13-18,
+// edgeList.h:8-23): src/dst/w are the sorted edge arrays, edges_idx the first
+// edge of each vertex (0 when it has none), out_degree the run length;
+// rows packs {edges_idx, out_degree} for one 8-byte load per vertex.
+struct DevCSR {
+  DevBuf src, dst, w;
+  DevBuf out_degree, in_degree, edges_idx;
+  DevBuf rows;  // uint2 per vertex
+  uint32_t* d_src() const { return src.as<uint32_t>(); }
+  uint32_t* d_dst() const { return dst.as<uint32_t>(); }
+  float* d_w() const { return w.as<float>(); }
+  uint32_t* d_out_degree() const { return out_degree.as<uint32_t>(); }
+  uint32_t* d_in_degree() const { return in_degree.as<uint32_t>(); }
+  uint32_t* d_edges_idx() const { return edges_idx.as<uint32_t>(); }
+  uint2* d_rows() const { return rows.as<uint2>(); }
+};
+
+struct BfsWork;  // bfs.cu
+struct PrWork;   // pagerank.cu
+void bfs_work_free(BfsWork* w);
+void pr_work_free(PrWork* w);
+
+struct BfsLevel {
+  uint32_t direction;  // 0 top-down, 1 bottom-up
+  uint32_t discovered; // vertices discovered by this step
+  uint32_t frontier;   // frontier size entering the step
+  uint32_t mf, mu;     // switch state after the step (top-down) / entering it
+  uint64_t edges;      // edges examined by the step
+  float ms;            // device time of the step (when timed)
+};
+
+struct DevGraph {
+  uint32_t V = 0;
+  uint32_t E = 0;
+  bool weighted = false;
+  uint32_t sort_type = 0;
+  DevCSR fwd, inv;
+  SortWorkspace sort_ws;
+  DevBuf input_src, input_dst, input_w;  // staging of host uploads
+  DevBuf err;                            // u32 error word of the build kernels
+  BfsWork* bfs = nullptr;
+  PrWork* pr = nullptr;
+  // traces of the last BFS / PageRank run through the device API
+  int bfs_last_levels = 0;
+  BfsLevel bfs_trace[512];
+  uint32_t pr_last_executed = 0;
+  double pr_err_hist[1024];
+  uint32_t pr_active_hist[1024];
+  ~DevGraph();
+};
+
+// Sort the device edge list (in_src, in_dst[, in_w]) with SORT_TYPE
+// semantics (0/2 by src, 1/3 by (src, dst)) and build both CSR directions.
+// All ids must be < V <= 2^30.  Inputs are not modified.
+int graph_build(DevGraph& g, const uint32_t* in_src, const uint32_t* in_dst, const float* in_w,
+                uint32_t E, uint32_t V, uint32_t sort_type, cudaStream_t s);
+
+// Fill the per-vertex arrays of one direction from its sorted src array
+// (the reference's mapVerticesWithInOutDegree, vertex.c:204-325), and the
+// in_degree array of the other direction.
+int csr_map(DevCSR& c, DevCSR& other, uint32_t V, uint32_t E, uint32_t* d_err, cudaStream_t s);
+
+// Rebuild the packed rows of one direction from edges_idx/out_degree (used
+// after an upload of a host GraphCSR).
+int csr_pack_rows(DevCSR& c, uint32_t V, cudaStream_t s);
+
+int sort_check(SortWorkspace& ws, cudaStream_t stream);
+int graph_check(DevGraph& g, cudaStream_t s);
+
+// ---- BFS -------------------------------------------------------------------
+enum BfsMode : uint32_t { BFS_PULL = 0, BFS_PUSH = 1, BFS_DO = 2 };
+
+
+
+struct BfsResult {
+  uint32_t iteration = 0;        // BFSStats.iteration
+  uint32_t processed_nodes = 0;  // BFSStats.processed_nodes
+  uint32_t td_steps = 0, bu_steps = 0;
+  uint64_t edges_examined = 0;
+  uint64_t reached_out_edges = 0;  // sum of out-degrees of reached vertices
+  uint32_t reached = 0;
+  double ms = 0.0;
+  int nlevels = 0;
+  BfsLevel levels[512];
+};
+
+// Direction switch policy: plain rule (alpha/beta) unless a policy callback
+// is installed (learned switch).  Returns 1 for bottom-up.
+struct BfsSwitchState {
+  uint32_t nf, nf_prev, mf, mu, n, E, level, direction;
+};
+
+// Run one BFS from `root` on the device graph; parents/distances are device
+// arrays of V entries.  bu_entry_nf selects the nf value at the start of a
+// bottom-up phase: 0 as the array-queue DO-BFS (BFS.c:550-551), or the
+// frontier size as the bitmap DO-BFS.
+int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_t* distances,
+            BfsResult* res, bool time_levels, bool bu_entry_nf_frontier, cudaStream_t s);
+
+}  // namespace ogb
+
+// One top-down / bottom-up level over HOST state (the reference's
+// topDownStepGraphCSR / bottomUpStepGraphCSR signatures): host arrays are
+// copied in, the level runs on the device, results are copied back.
+int bfs_td_step_host(ogb::DevGraph& g, const uint32_t* q, uint32_t qsize, int32_t* parents, uint32_t* distances,
+                     uint32_t* next_q, uint32_t* next_size, uint32_t* mf, cudaStream_t s);
+int bfs_bu_step_host(ogb::DevGraph& g, const uint32_t* bm_cur, uint32_t* bm_next, int32_t* parents,
+                     uint32_t* distances, uint32_t* nf, cudaStream_t s);
+
+namespace ogb {
+
+// ---- PageRank ----------------------------------------------------------------
+struct PrResult {
+  uint32_t iterations = 0;       // PageRankStats.iterations
+  uint32_t executed = 0;         // iterations actually run
+  uint32_t activeVertices = 0;
+  double error_total = 0.0;
+  double ms = 0.0;
+  int converged = 0;
+  double err_hist[1024];
+  uint32_t active_hist[1024];
+};
+
+enum PrMode : uint32_t { PR_PULL = 0, PR_PUSH = 1 };
+
+// PageRank with the reference semantics (pageRank.c:939-1186): unnormalized
+// start at 1-d, stop when no vertex changes by >= epsilon or after
+// max_iters, ranks divided by V at the end.  `ranks` is a device array of V
+// floats; `init` (optional, device) replaces the uniform start.
+int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon, float* ranks,
+                 const float* init, PrResult* res, cudaStream_t s);
+
+}  // namespace ogb

@@ -1,0 +1,350 @@
+/*
+ * og_oracle.c -- CPU restatement of the OpenGraph CSR hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (see og_oracle.h).  Written from the reference's
+ * algorithm, not its code: sequential, one pass per digit-free counting sort,
+ * explicit integer types.  Built with -ffp-contract=off semantics kept by
+ * hand (every float product and sum is a separate statement).
+ */
+#include "og_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------ sort -- */
+
+/* Stable counting sort by one u32 key (keys need not be dense: a 16-bit LSD
+ * two-pass counting sort keeps memory bounded). */
+static void sort_by_key(uint32_t E, const uint32_t *key, const uint32_t *pa, const uint32_t *pb,
+                        uint32_t *okey, uint32_t *oa, uint32_t *ob)
+{
+    uint32_t *k1 = malloc((size_t)E * 4 + 4), *a1 = malloc((size_t)E * 4 + 4), *b1 = malloc((size_t)E * 4 + 4);
+    uint64_t *cnt = malloc(sizeof(uint64_t) * 65537);
+    const uint32_t *ik = key, *ia = pa, *ib = pb;
+    uint32_t *tk = k1, *ta = a1, *tb = b1;
+    for (int pass = 0; pass < 2; pass++)
+    {
+        const int sh = pass * 16;
+        if (pass == 1)
+        {
+            tk = okey; ta = oa; tb = ob;
+        }
+        memset(cnt, 0, sizeof(uint64_t) * 65537);
+        for (uint32_t i = 0; i < E; i++) cnt[((ik[i] >> sh) & 0xFFFF) + 1]++;
+        for (int d = 0; d < 65536; d++) cnt[d + 1] += cnt[d];
+        for (uint32_t i = 0; i < E; i++)
+        {
+            const uint64_t p = cnt[(ik[i] >> sh) & 0xFFFF]++;
+            tk[p] = ik[i];
+            ta[p] = ia[i];
+            if (ib) tb[p] = ib[i];
+        }
+        ik = k1; ia = a1; ib = pb ? b1 : NULL;
+    }
+    free(k1); free(a1); free(b1); free(cnt);
+}
+
+void orc_sort(uint32_t E, const uint32_t *src, const uint32_t *dst, const float *w, int mode,
+              uint32_t *osrc, uint32_t *odst, float *ow)
+{
+    const uint32_t *wb = (const uint32_t *)w;
+    uint32_t *owb = (uint32_t *)ow;
+    if (mode == 0)
+    {
+        sort_by_key(E, src, dst, wb, osrc, odst, owb);
+    }
+    else if (mode == 2)
+    {
+        sort_by_key(E, dst, src, wb, odst, osrc, owb);
+    }
+    else
+    {
+        /* by dst first, then stably by src: lexicographic (src, dst) */
+        uint32_t *ts = malloc((size_t)E * 4 + 4), *td = malloc((size_t)E * 4 + 4), *tw = w ? malloc((size_t)E * 4 + 4) : NULL;
+        sort_by_key(E, dst, src, wb, td, ts, tw);
+        sort_by_key(E, ts, td, tw, osrc, odst, owb);
+        free(ts); free(td); free(tw);
+    }
+}
+
+int orc_csr_map(uint32_t E, uint32_t V, const uint32_t *s, uint32_t *out_degree, uint32_t *edges_idx)
+{
+    memset(out_degree, 0, (size_t)V * 4);
+    memset(edges_idx, 0, (size_t)V * 4);
+    for (uint32_t i = 0; i < E; i++)
+    {
+        if (s[i] >= V) return -1;
+        if (i == 0 || s[i] != s[i - 1]) edges_idx[s[i]] = i;
+        out_degree[s[i]]++;
+    }
+    return 0;
+}
+
+int orc_build(uint32_t E, uint32_t V, const uint32_t *src, const uint32_t *dst, const float *w, int sort_type,
+              uint32_t *f_src, uint32_t *f_dst, float *f_w, uint32_t *f_outdeg, uint32_t *f_indeg, uint32_t *f_idx,
+              uint32_t *i_src, uint32_t *i_dst, float *i_w, uint32_t *i_outdeg, uint32_t *i_indeg, uint32_t *i_idx)
+{
+    const int mode = (sort_type == 1 || sort_type == 3) ? 1 : 0;
+    orc_sort(E, src, dst, w, mode, f_src, f_dst, w ? f_w : NULL);
+    if (orc_csr_map(E, V, f_src, f_outdeg, f_idx)) return -1;
+    /* inverse list = sorted forward list with src/dst swapped, sorted again */
+    orc_sort(E, f_dst, f_src, w ? f_w : NULL, mode, i_src, i_dst, w ? i_w : NULL);
+    if (orc_csr_map(E, V, i_src, i_outdeg, i_idx)) return -1;
+    memcpy(i_indeg, f_outdeg, (size_t)V * 4);
+    memcpy(f_indeg, i_outdeg, (size_t)V * 4);
+    return 0;
+}
+
+uint32_t orc_dedup(uint32_t E, const uint32_t *s, const uint32_t *d, const float *w, uint32_t *os, uint32_t *od,
+                   float *ow, int truncate_w)
+{
+    uint32_t n = 0;
+    for (uint32_t i = 0; i < E; i++)
+    {
+        if (s[i] == d[i]) continue;
+        if (n > 0 && os[n - 1] == s[i] && od[n - 1] == d[i]) continue;
+        os[n] = s[i];
+        od[n] = d[i];
+        if (w) ow[n] = truncate_w ? (float)(uint32_t)w[i] : w[i];
+        n++;
+    }
+    return n;
+}
+
+/* ------------------------------------------------------------------- BFS -- */
+
+int orc_bfs(uint32_t V, uint32_t E, const uint32_t *f_outdeg, const uint32_t *f_idx, const uint32_t *f_dst,
+            const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, uint32_t root, int mode,
+            int bu_entry_nf_frontier, int32_t *parents, uint32_t *dist, orc_bfs_stats *st, uint8_t *dirs,
+            uint32_t max_dirs)
+{
+    if (root >= V) return -1;
+    for (uint32_t v = 0; v < V; v++)
+    {
+        parents[v] = f_outdeg[v] ? -(int32_t)f_outdeg[v] : -1;
+        dist[v] = 0;
+    }
+    uint32_t *q = malloc((size_t)V * 4 + 4), *nq = malloc((size_t)V * 4 + 4);
+    uint8_t *cur = calloc(V + 1, 1), *nxt = calloc(V + 1, 1);
+    uint32_t qn = 1, step = 0;
+    q[0] = root;
+    parents[root] = (int32_t)root;
+    uint32_t mu = E, mf = f_outdeg[root], nf = 0, nf_prev = 0;
+    const uint32_t alpha = 15, beta = 18;
+    orc_bfs_stats s = {1, 1, 0, 0, 0, 0};
+    while (qn > 0)
+    {
+        const int bu = (mode == 0) || (mode == 2 && mf > mu / alpha);
+        if (bu)
+        {
+            memset(cur, 0, V);
+            for (uint32_t i = 0; i < qn; i++) cur[q[i]] = 1;
+            nf = bu_entry_nf_frontier ? qn : 0;
+            do
+            {
+                nf_prev = nf;
+                nf = 0;
+                memset(nxt, 0, V);
+                for (uint32_t v = 0; v < V; v++)
+                {
+                    if (parents[v] >= 0) continue;
+                    for (uint32_t j = i_idx[v]; j < i_idx[v] + i_outdeg[v]; j++)
+                    {
+                        const uint32_t u = i_dst[j] & 0x3FFFFFFFu;
+                        if (cur[u])
+                        {
+                            parents[v] = (int32_t)u;
+                            dist[v] = dist[u] + 1;
+                            nxt[v] = 1;
+                            nf++;
+                            break;
+                        }
+                    }
+                }
+                uint8_t *t = cur; cur = nxt; nxt = t;
+                s.iteration++;
+                s.processed_nodes += nf;
+                s.bu_steps++;
+                if (dirs && step < max_dirs) dirs[step] = 1;
+                step++;
+            } while (mode == 0 ? (nf > 0) : ((nf > nf_prev) || (nf > V / beta)));
+            qn = 0;
+            for (uint32_t v = 0; v < V; v++)
+                if (cur[v]) q[qn++] = v;
+            mf = 1;
+        }
+        else
+        {
+            mu -= mf;
+            mf = 0;
+            uint32_t nn = 0;
+            for (uint32_t i = 0; i < qn; i++)
+            {
+                const uint32_t v = q[i];
+                for (uint32_t j = f_idx[v]; j < f_idx[v] + f_outdeg[v]; j++)
+                {
+                    const uint32_t u = f_dst[j] & 0x3FFFFFFFu;
+                    if (parents[u] < 0)
+                    {
+                        mf += (uint32_t)(-parents[u]);
+                        parents[u] = (int32_t)v;
+                        dist[u] = dist[v] + 1;
+                        nq[nn++] = u;
+                    }
+                }
+            }
+            uint32_t *t = q; q = nq; nq = t;
+            qn = nn;
+            s.iteration++;
+            s.processed_nodes += nn;
+            s.td_steps++;
+            if (dirs && step < max_dirs) dirs[step] = 0;
+            step++;
+        }
+    }
+    for (uint32_t v = 0; v < V; v++)
+        if (parents[v] >= 0)
+        {
+            s.reached++;
+            s.reached_out_edges += f_outdeg[v];
+        }
+    if (st) *st = s;
+    free(q); free(nq); free(cur); free(nxt);
+    return 0;
+}
+
+/* -------------------------------------------------------------- PageRank -- */
+
+uint32_t orc_pagerank(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_idx, const uint32_t *f_dst,
+                      const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, int mode,
+                      uint32_t max_iters, double epsilon, const float *init, float *pr,
+                      uint32_t *iterations_out, double *error_out, double *err_hist, uint32_t *active_hist)
+{
+    const float damp = 0.85f;
+    const float base_pr = 1.0f - damp;
+    float *contrib = malloc((size_t)V * 4 + 4), *next = calloc((size_t)V + 1, 4);
+    for (uint32_t v = 0; v < V; v++) pr[v] = init ? init[v] : base_pr;
+    uint32_t it, executed = 0;
+    double error_total = 0.0;
+    for (it = 0; it < max_iters; it++)
+    {
+        error_total = 0.0;
+        uint32_t active = 0;
+        for (uint32_t v = 0; v < V; v++)
+            contrib[v] = f_outdeg[v] ? pr[v] / (float)f_outdeg[v] : 0.0f;
+        if (mode == 0)
+        {
+            for (uint32_t v = 0; v < V; v++)
+            {
+                float s = 0.0f;
+                for (uint32_t j = i_idx[v]; j < i_idx[v] + i_outdeg[v]; j++) s += contrib[i_dst[j] & 0x3FFFFFFFu];
+                next[v] = s;
+            }
+        }
+        else
+        {
+            for (uint32_t v = 0; v < V; v++)
+                for (uint32_t j = f_idx[v]; j < f_idx[v] + f_outdeg[v]; j++) next[f_dst[j] & 0x3FFFFFFFu] += contrib[v];
+        }
+        for (uint32_t v = 0; v < V; v++)
+        {
+            const float prev = pr[v];
+            const float scaled = damp * next[v];
+            const float nv = base_pr + scaled;
+            pr[v] = nv;
+            next[v] = 0.0f;
+            const float diff = nv - prev;
+            const double e = fabs((double)diff);
+            error_total += e / V;
+            if (e >= epsilon) active++;
+        }
+        if (err_hist) err_hist[executed] = error_total;
+        if (active_hist) active_hist[executed] = active;
+        executed++;
+        if (active == 0) break;
+    }
+    for (uint32_t v = 0; v < V; v++) pr[v] = pr[v] / (float)V;
+    if (iterations_out) *iterations_out = it;
+    if (error_out) *error_out = error_total;
+    free(contrib);
+    free(next);
+    return executed;
+}
+
+void orc_pagerank_f64(uint32_t V, const uint32_t *f_outdeg, const uint32_t *i_outdeg, const uint32_t *i_idx,
+                      const uint32_t *i_dst, uint32_t iters, const double *init, double *pr)
+{
+    const double damp = 0.85, base_pr = 1.0 - damp;
+    double *contrib = malloc((size_t)V * 8 + 8);
+    for (uint32_t v = 0; v < V; v++) pr[v] = init ? init[v] : base_pr;
+    for (uint32_t it = 0; it < iters; it++)
+    {
+        for (uint32_t v = 0; v < V; v++) contrib[v] = f_outdeg[v] ? pr[v] / f_outdeg[v] : 0.0;
+        for (uint32_t v = 0; v < V; v++)
+        {
+            double s = 0.0;
+            for (uint32_t j = i_idx[v]; j < i_idx[v] + i_outdeg[v]; j++) s += contrib[i_dst[j] & 0x3FFFFFFFu];
+            pr[v] = base_pr + damp * s;
+        }
+    }
+    for (uint32_t v = 0; v < V; v++) pr[v] /= V;
+    free(contrib);
+}
+
+/* ------------------------------------------------------------------ roots -- */
+
+/* MT19937 (Matsumoto & Nishimura 1998) with the LCG seeding x -> 69069x + 1. */
+typedef struct { uint32_t mt[624]; int mti; } orc_mt;
+
+static void orc_mt_seed(orc_mt *m, uint32_t seed)
+{
+    uint64_t x = seed; /* the reference keeps 64-bit state; only the low 32 bits matter */
+    for (int i = 0; i < 624; i++)
+    {
+        uint32_t hi = (uint32_t)(x & 0xffff0000u);
+        x = 69069u * x + 1u;
+        uint32_t lo = (uint32_t)((x & 0xffff0000u) >> 16);
+        x = 69069u * x + 1u;
+        m->mt[i] = hi | lo;
+    }
+    m->mti = 624;
+}
+
+static uint32_t orc_mt_next(orc_mt *m)
+{
+    if (m->mti >= 624)
+    {
+        for (int k = 0; k < 624; k++)
+        {
+            uint32_t y = (m->mt[k] & 0x80000000u) | (m->mt[(k + 1) % 624] & 0x7fffffffu);
+            m->mt[k] = m->mt[(k + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+        }
+        m->mti = 0;
+    }
+    uint32_t y = m->mt[m->mti++];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    return y;
+}
+
+void orc_random_roots(uint32_t seed, uint32_t V, uint32_t avg_degree, const uint32_t *out_degree, uint32_t n,
+                      uint32_t *roots)
+{
+    orc_mt m;
+    orc_mt_seed(&m, seed);
+    for (uint32_t k = 0; k < n; k++)
+    {
+        for (;;)
+        {
+            const uint32_t s = orc_mt_next(&m);
+            if (s < V && out_degree[s] > avg_degree)
+            {
+                roots[k] = s;
+                break;
+            }
+        }
+    }
+}

@@ -1,0 +1,84 @@
+/*
+ * og_oracle.h -- CPU restatement of the OpenGraph CSR hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker that tests/, __graft_entry__.smoke()
+ * and bench.py's CPU-baseline leg compare the GPU library against.  Nothing in
+ * opengraph_b200/ links, loads or calls it.
+ *
+ * Sequential, plain-array restatement of the reference functions cited at
+ * each entry point (paths relative to the OpenGraph tree).  Pinned against
+ * the reference's own build (oracle/_ref) by tests/test_oracle.py, and
+ * against the committed fixtures under tests/golden/.
+ */
+#ifndef OG_ORACLE_H
+#define OG_ORACLE_H
+
+#include <stdint.h>
+
+/* Stable sort of (src, dst[, w]) -- mode 0: by src (radixsort.c:231-278,
+ * countsort.c:28-140), 1: by (src, dst) (radixsort.c:282-335,
+ * countsort.c:262-270), 2: by dst (countsort.c:143-259).  w may be NULL. */
+void orc_sort(uint32_t E, const uint32_t *src, const uint32_t *dst, const float *w, int mode,
+              uint32_t *osrc, uint32_t *odst, float *ow);
+
+/* mapVerticesWithInOutDegree (vertex.c:204-325) for one direction: run
+ * lengths and run starts of the sorted src array (edges_idx = 0 for vertices
+ * without edges).  Returns -1 if a source id is >= V. */
+int orc_csr_map(uint32_t E, uint32_t V, const uint32_t *sorted_src, uint32_t *out_degree, uint32_t *edges_idx);
+
+/* graphCSRPreProcessingStep's sort + map + inverse (graphCSR.c:164-248)
+ * without file I/O: f_* forward arrays, i_* inverse arrays (E or V each);
+ * in_degree arrays are the other direction's out_degree (vertex.c:291-311).
+ * sort_type as SORT_TYPE (0/2 by src, 1/3 by (src,dst)).  w may be NULL, then
+ * f_w/i_w are ignored. */
+int orc_build(uint32_t E, uint32_t V, const uint32_t *src, const uint32_t *dst, const float *w, int sort_type,
+              uint32_t *f_src, uint32_t *f_dst, float *f_w, uint32_t *f_outdeg, uint32_t *f_indeg, uint32_t *f_idx,
+              uint32_t *i_src, uint32_t *i_dst, float *i_w, uint32_t *i_outdeg, uint32_t *i_indeg, uint32_t *i_idx);
+
+/* removeDulpicatesSelfLoopEdges (edgeList.c:138-211) on a sorted list;
+ * truncate_w reproduces the WEIGHTED layout's uint32 temporary.  Returns the
+ * kept count. */
+uint32_t orc_dedup(uint32_t E, const uint32_t *s, const uint32_t *d, const float *w, uint32_t *os, uint32_t *od,
+                   float *ow, int truncate_w);
+
+typedef struct orc_bfs_stats
+{
+    uint32_t iteration;       /* BFSStats.iteration       */
+    uint32_t processed_nodes; /* BFSStats.processed_nodes */
+    uint32_t td_steps;
+    uint32_t bu_steps;
+    uint32_t reached;
+    uint64_t reached_out_edges;
+} orc_bfs_stats;
+
+/* BFS over both CSRs (BFS.c:281-754): mode 0 pull, 1 push, 2 direction-
+ * optimized (alpha 15, beta 18).  bu_entry_nf_frontier = 0 follows the
+ * array-queue DO-BFS (nf = 0 entering bottom-up), 1 the bitmap variant.
+ * Top-down parents are the first discoverer in queue order.  dirs (may be
+ * NULL) receives the direction of each step (0 TD, 1 BU), up to max_dirs. */
+int orc_bfs(uint32_t V, uint32_t E, const uint32_t *f_outdeg, const uint32_t *f_idx, const uint32_t *f_dst,
+            const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, uint32_t root, int mode,
+            int bu_entry_nf_frontier, int32_t *parents, uint32_t *dist, orc_bfs_stats *st, uint8_t *dirs,
+            uint32_t max_dirs);
+
+/* PageRank fp32 (pageRank.c:939-1186): mode 0 pull (sequential sums in CSR
+ * order), 1 push (sequential scatter in vertex order).  init (may be NULL)
+ * replaces the start 1-0.85f.  ranks receives the normalized ranks;
+ * err_hist/active_hist (may be NULL) one entry per executed iteration.
+ * Returns the number of executed iterations. */
+uint32_t orc_pagerank(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_idx, const uint32_t *f_dst,
+                      const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, int mode,
+                      uint32_t max_iters, double epsilon, const float *init, float *ranks,
+                      uint32_t *iterations_out, double *error_out, double *err_hist, uint32_t *active_hist);
+
+/* The same pull iteration in double precision throughout (the FP64 oracle the
+ * fp32 error is stated against).  Runs exactly `iters` iterations. */
+void orc_pagerank_f64(uint32_t V, const uint32_t *f_outdeg, const uint32_t *i_outdeg, const uint32_t *i_idx,
+                      const uint32_t *i_dst, uint32_t iters, const double *init, double *ranks);
+
+/* generateRandomRootGraphCSR (graphRun.c:537-556) with MT19937 seeded as
+ * initializeMersenneState (mt19937.c:54-67): n roots drawn in sequence. */
+void orc_random_roots(uint32_t seed, uint32_t V, uint32_t avg_degree, const uint32_t *out_degree, uint32_t n,
+                      uint32_t *roots);
+
+#endif

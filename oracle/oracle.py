@@ -1,0 +1,214 @@
+"""Oracle of the OpenGraph CSR hot path -- TEST INFRASTRUCTURE ONLY.
+
+Two checkers, both CPU:
+
+* ``Oracle``: the project's C restatement (``og_oracle.c`` -> ``liboracle.so``),
+  sequential and deterministic, every function citing the reference lines it
+  restates;
+* ``Reference``: the reference's own OpenMP code compiled from its sources by
+  ``oracle/Makefile`` into ``oracle/_ref/libogref{,_w}.so`` (git-ignored build
+  output that travels with the tree).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, as the checker or the timed CPU baseline; the product
+(``opengraph_b200``) never imports it.
+"""
+from __future__ import annotations
+
+import contextlib
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+REFERENCE_SRC = "/root/reference/00_graph_bench"
+
+u32 = C.c_uint32
+vp = C.c_void_p
+
+
+def build(ref: bool = True) -> None:
+    """make the restatement (and, when the reference sources exist, _ref)."""
+    targets = ["oracle"]
+    if ref and os.path.isdir(REFERENCE_SRC):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", HERE, "-j8", *targets], check=True)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class Oracle:
+    def __init__(self, path: str | None = None):
+        path = path or os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build(ref=False)
+        d = C.CDLL(path)
+        self.d = d
+        d.orc_sort.argtypes = [u32, vp, vp, vp, C.c_int, vp, vp, vp]
+        d.orc_csr_map.argtypes = [u32, u32, vp, vp, vp]
+        d.orc_csr_map.restype = C.c_int
+        d.orc_build.argtypes = [u32, u32, vp, vp, vp, C.c_int] + [vp] * 12
+        d.orc_build.restype = C.c_int
+        d.orc_dedup.argtypes = [u32, vp, vp, vp, vp, vp, vp, C.c_int]
+        d.orc_dedup.restype = u32
+        d.orc_bfs.argtypes = [u32, u32, vp, vp, vp, vp, vp, vp, u32, C.c_int, C.c_int, vp, vp, vp, vp, u32]
+        d.orc_bfs.restype = C.c_int
+        d.orc_pagerank.argtypes = [u32, vp, vp, vp, vp, vp, vp, C.c_int, u32, C.c_double, vp, vp, vp, vp, vp, vp]
+        d.orc_pagerank.restype = u32
+        d.orc_pagerank_f64.argtypes = [u32, vp, vp, vp, vp, u32, vp, vp]
+        d.orc_random_roots.argtypes = [u32, u32, u32, vp, u32, vp]
+
+    def sort(self, src, dst, w=None, mode: int = 0):
+        E = len(src)
+        os_, od = np.empty(E, np.uint32), np.empty(E, np.uint32)
+        ow = np.empty(E, np.float32) if w is not None else None
+        self.d.orc_sort(E, _p(src), _p(dst), _p(w), mode, _p(os_), _p(od), _p(ow))
+        return os_, od, ow
+
+    def build(self, src, dst, V: int, sort_type: int = 0, w=None) -> dict:
+        E = len(src)
+        r = {k: np.empty(E, np.uint32) for k in ("f_src", "f_dst", "i_src", "i_dst")}
+        r.update({k: np.empty(V, np.uint32) for k in ("f_outdeg", "f_indeg", "f_idx", "i_outdeg", "i_indeg",
+                                                        "i_idx")})
+        if w is not None:
+            r["f_w"], r["i_w"] = np.empty(E, np.float32), np.empty(E, np.float32)
+        st = self.d.orc_build(E, V, _p(src), _p(dst), _p(w), sort_type, _p(r["f_src"]), _p(r["f_dst"]),
+                              _p(r.get("f_w")), _p(r["f_outdeg"]), _p(r["f_indeg"]), _p(r["f_idx"]),
+                              _p(r["i_src"]), _p(r["i_dst"]), _p(r.get("i_w")), _p(r["i_outdeg"]),
+                              _p(r["i_indeg"]), _p(r["i_idx"]))
+        if st:
+            raise ValueError("oracle build: an id is >= V")
+        r["num_vertices"], r["num_edges"] = V, E
+        return r
+
+    def dedup(self, s, d, w=None, truncate_w: bool = False):
+        E = len(s)
+        os_, od = np.empty(E, np.uint32), np.empty(E, np.uint32)
+        ow = np.empty(E, np.float32) if w is not None else None
+        n = self.d.orc_dedup(E, _p(s), _p(d), _p(w), _p(os_), _p(od), _p(ow), 1 if truncate_w else 0)
+        return os_[:n], od[:n], (ow[:n] if ow is not None else None)
+
+    def bfs(self, g: dict, root: int, mode: int = 2, bitmap_nf: bool = False):
+        V, E = g["num_vertices"], g["num_edges"]
+        par, dist = np.empty(V, np.int32), np.empty(V, np.uint32)
+
+        class St(C.Structure):
+            _fields_ = [("iteration", u32), ("processed_nodes", u32), ("td_steps", u32), ("bu_steps", u32),
+                        ("reached", u32), ("reached_out_edges", C.c_uint64)]
+        st = St()
+        dirs = np.zeros(4096, np.uint8)
+        r = self.d.orc_bfs(V, E, _p(g["f_outdeg"]), _p(g["f_idx"]), _p(g["f_dst"]), _p(g["i_outdeg"]),
+                           _p(g["i_idx"]), _p(g["i_dst"]), root, mode, 1 if bitmap_nf else 0, _p(par), _p(dist),
+                           C.addressof(st), _p(dirs), len(dirs))
+        if r:
+            raise ValueError("oracle bfs: bad root")
+        stats = {f: getattr(st, f) for f, _ in St._fields_}
+        nsteps = stats["td_steps"] + stats["bu_steps"]
+        stats["dirs"] = dirs[:min(nsteps, len(dirs))].copy()
+        return par, dist, stats
+
+    def pagerank(self, g: dict, mode: int = 0, max_iters: int = 20, epsilon: float = 1e-4, init=None):
+        V = g["num_vertices"]
+        ranks = np.empty(V, np.float32)
+        it, err = u32(), C.c_double()
+        eh = np.zeros(max(max_iters, 1), np.float64)
+        ah = np.zeros(max(max_iters, 1), np.uint32)
+        n = self.d.orc_pagerank(V, _p(g["f_outdeg"]), _p(g["f_idx"]), _p(g["f_dst"]), _p(g["i_outdeg"]),
+                                _p(g["i_idx"]), _p(g["i_dst"]), mode, max_iters, epsilon, _p(init), _p(ranks),
+                                C.byref(it), C.byref(err), _p(eh), _p(ah))
+        return ranks, {"iterations": it.value, "error_total": err.value, "executed": n, "err_hist": eh[:n],
+                       "active_hist": ah[:n]}
+
+    def pagerank_f64(self, g: dict, iters: int, init=None):
+        V = g["num_vertices"]
+        ranks = np.empty(V, np.float64)
+        self.d.orc_pagerank_f64(V, _p(g["f_outdeg"]), _p(g["i_outdeg"]), _p(g["i_idx"]), _p(g["i_dst"]), iters,
+                                _p(init), _p(ranks))
+        return ranks
+
+    def random_roots(self, V: int, avg_degree: int, out_degree, n: int, seed: int = 27491095):
+        roots = np.empty(n, np.uint32)
+        self.d.orc_random_roots(seed, V, avg_degree, _p(out_degree), n, _p(roots))
+        return roots
+
+
+@contextlib.contextmanager
+def silenced_stdout():
+    """Send the C library's stdout (fd 1) to /dev/null for the duration."""
+    libc = C.CDLL(None)
+    libc.fflush(None)
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    try:
+        yield
+    finally:
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+
+
+class Reference:
+    """The reference's own CPU build (oracle/_ref), bound with the same struct
+    layouts as the product (layouts checked by tests/test_abi.py)."""
+
+    def __init__(self, weighted: bool = False):
+        import opengraph_b200 as og
+        self.og = og
+        self.weighted = weighted
+        path = os.path.join(REF_DIR, "libogref_w.so" if weighted else "libogref.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.d = C.CDLL(path)
+        EL = og.EdgeListW if weighted else og.EdgeList
+        G = og.GraphCSRW if weighted else og.GraphCSR
+        self.EdgeList, self.GraphCSR = EL, G
+        for name, res, args in og._api(EL, G):
+            if hasattr(self.d, name):
+                fn = getattr(self.d, name)
+                fn.restype, fn.argtypes = res, args
+                setattr(self, name, fn)
+
+    @staticmethod
+    def available(weighted: bool = False) -> bool:
+        return os.path.exists(os.path.join(REF_DIR, "libogref_w.so" if weighted else "libogref.so"))
+
+    def arguments(self, **kw):
+        a = self.og.default_arguments(**kw)
+        self.initializeMersenneState(C.byref(a.mt19937var), 27491095)
+        return a
+
+    def build_graph(self, path: str, sort: int = 0, dflag: int = 0, weighted_file: bool = False, quiet=True):
+        a = self.arguments(fnameb=path, sort=sort, dflag=dflag, weighted=1 if weighted_file else 0)
+        self._keep = a
+        with (silenced_stdout() if quiet else contextlib.nullcontext()):
+            g = self.graphCSRPreProcessingStep(C.byref(a))
+        return g
+
+    def bfs(self, g, root: int, pushpull: int = 2, quiet=True):
+        a = self.arguments(source=root, pushpull=pushpull)
+        with (silenced_stdout() if quiet else contextlib.nullcontext()):
+            st = self.breadthFirstSearchGraphCSR(C.byref(a), g)
+        s = st.contents
+        V = s.num_vertices
+        out = (self.og.as_numpy(s.parents, V, np.int32), self.og.as_numpy(s.distances, V, np.uint32),
+               {"processed_nodes": s.processed_nodes, "iteration": s.iteration, "time_total": s.time_total})
+        self.freeBFSStats(st)
+        return out
+
+    def pagerank(self, g, pushpull: int = 0, iterations: int = 20, epsilon: float = 1e-4, quiet=True):
+        a = self.arguments(pushpull=pushpull, iterations=iterations, epsilon=epsilon)
+        with (silenced_stdout() if quiet else contextlib.nullcontext()):
+            st = self.pageRankGraphCSR(C.byref(a), g)
+        s = st.contents
+        V = s.num_vertices
+        out = (self.og.as_numpy(s.pageRanks, V, np.float32),
+               {"iterations": s.iterations, "error_total": s.error_total, "time_total": s.time_total})
+        self.freePageRankStats(st)
+        return out
