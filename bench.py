@@ -1,0 +1,455 @@
+"""Benchmark of the B200 CSR hot path on RMAT scale 22 (edge factor 16,
+uint32 ids, float32 weights in [1,256), seeded synthetic data).
+
+A timed step is one sweep of direction-optimized BFS from 64 seeded random
+roots with out-degree > 0, each search timed on the device (CUDA events),
+with L2 flushed between searches.  value = Graph500 GTEPS of the sweep (sum of
+out-degrees of reached vertices over search time), summed over ranks.
+
+Also measured on the same resident graph, outside the step loop: the GPU
+radix sort + CSR build (both directions, weighted), PageRank pull and push to
+1e-6 L1 (max 100 iterations: iteration GTEPS and time-to-tolerance).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank owns one GPU and its own 64 roots (independent
+units: weak scaling); rank 0 prints one JSON line.  --impl reference times the
+reference's own OpenMP BFS (built from its sources into oracle/_ref) on the
+host cores on a bounded sample of the same roots.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SCALE, EDGE_FACTOR, SEED, NROOTS = 22, 16, 0, 64
+PR_TOL, PR_MAX = 1e-6, 100
+METRIC = "BFS & PR-iteration GTEPS on 1 B200 (%HBM roofline); PR time-to-1e-6, learned vs plain"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def bfs_bytes(trace, V: int) -> tuple[float, dict]:
+    """Algorithmic bytes of one search from its level trace.
+    TD level: 12|F| + 8 E_F + 12|N|;  BU level: 4V + 8U + 4 E_scan + 12|N|
+    (U = unvisited vertices entering the level; bitmap probes cached)."""
+    total, per_dir = 0.0, {"td": 0.0, "bu": 0.0}
+    visited = 1
+    for L in trace:
+        if L["direction"] == 0:
+            b = 12 * L["frontier"] + 8 * L["edges"] + 12 * L["discovered"]
+            per_dir["td"] += b
+        else:
+            U = V - visited
+            b = 4 * V + 8 * U + 4 * L["edges"] + 12 * L["discovered"]
+            per_dir["bu"] += b
+        total += b
+        visited += L["discovered"]
+    return total, per_dir
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import opengraph_b200 as og
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    lib = og.load(True)  # the weighted layout: configs carry float32 weights
+    lib.quiet(True)
+    hbm_peak, peak_kind = peaks()
+
+    # ---- inputs: RMAT-22, resident in HBM --------------------------------
+    s, d, w = og.generate_rmat(SCALE, EDGE_FACTOR, SEED, weighted=True)
+    V = 1 << SCALE
+    E = len(s)
+    ts = torch.from_numpy(s.view(np.int32)).to(dev)
+    td = torch.from_numpy(d.view(np.int32)).to(dev)
+    tw = torch.from_numpy(w).to(dev)
+    g = lib.device_graph()
+    g.build(ts, td, V, 0, weight=tw)
+    torch.cuda.synchronize()
+    f = g.view(False)
+    outdeg = f.out_degree.cpu().numpy().view(np.uint32)
+    rng = np.random.default_rng(1000 + rank)
+    cand = np.nonzero(outdeg > 0)[0]
+    roots = [int(x) for x in rng.choice(cand, size=NROOTS, replace=False)]
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    par = torch.empty(V, dtype=torch.int32, device=dev)
+    dis = torch.empty(V, dtype=torch.int32, device=dev)
+    lib.ogb_set_level_timing(1)
+
+    def sweep():
+        tot_ms, tot_edges, launches = 0.0, 0, 0
+        traces = []
+        for r in roots:
+            flush.zero_()
+            torch.cuda.synchronize()
+            info = g.bfs(r, par, dis, mode=2)
+            tot_ms += info["ms"]
+            tot_edges += info["reached_out_edges"]
+            launches += info["launches"]
+            traces.append(g.bfs_trace())
+        return tot_ms, tot_edges, launches, traces
+
+    for _ in range(args.warmup):
+        sweep()
+    clocks = ClockSampler(local)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    step_ms, edges_total, launches_total, traces = [], 0, 0, None
+    for _ in range(args.steps):
+        ms, ed, la, traces = sweep()
+        step_ms.append(ms)
+        edges_total += ed
+        launches_total += la
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    my_ms = sum(step_ms)
+    if ws > 1:
+        t = torch.tensor([my_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e = torch.tensor([edges_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(e, op=dist.ReduceOp.SUM)
+        max_ms, all_edges = float(t.item()), float(e.item())
+    else:
+        max_ms, all_edges = my_ms, float(edges_total)
+    gteps = all_edges / (max_ms / 1e3) / 1e9
+
+    # ---- roofline of the dominant BFS kernel (bottom-up steps) -----------
+    bu_bytes = bu_ms = td_bytes = td_ms = 0.0
+    for tr in traces:
+        _, per = bfs_bytes(tr, V)
+        bu_bytes += per["bu"]
+        td_bytes += per["td"]
+        bu_ms += sum(L["ms"] for L in tr if L["direction"] == 1)
+        td_ms += sum(L["ms"] for L in tr if L["direction"] == 0)
+    all_bytes = sum(bfs_bytes(tr, V)[0] for tr in traces)
+    sweep_ms = step_ms[-1]
+    bu_gbs = bu_bytes / (bu_ms / 1e3) / 1e9 if bu_ms else 0.0
+
+    # ---- e2e: the reference-facing C-ABI call with host buffers ----------
+    e2e = e2e_dropin(lib, og, s, d, w, roots, rank, dev)
+
+    extra = {}
+    if rank == 0 and not args.skip_stages:
+        extra = stages(lib, og, g, ts, td, tw, V, E, dev, hbm_peak)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.skip_cpu:
+        cpu = cpu_baseline(og, s, d, w, roots[:args.cpu_roots])
+
+    g.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC,
+        "value": round(gteps, 3),
+        "unit": "GTEPS",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(max_ms / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32",
+        "data": "synthetic (seeded RMAT generator)",
+        "config": {"workload": f"RMAT scale {SCALE} (V={V}, E={E}), a/b/c/d=.57/.19/.19/.05, permuted ids, "
+                               f"float32 weights; DO-BFS from {NROOTS} seeded random roots with out-degree>0 "
+                               "per rank, each search timed individually",
+                   "global_batch": NROOTS * ws, "seq_len": None, "parallelism": f"replicas{ws}",
+                   "l2": "flushed (256 MB write) before every search",
+                   "step": f"{NROOTS} DO-BFS searches"},
+        "roofline": {"bound": "hbm", "kernel": "bfs_bu (bottom-up steps)", "achieved": round(bu_gbs, 1),
+                     "peak": hbm_peak, "unit": "GB/s", "frac": round(bu_gbs / hbm_peak, 4),
+                     "peak_kind": peak_kind, "traffic": None,
+                     "bfs_all_kernels_gbs": round(all_bytes / (sweep_ms / 1e3) / 1e9, 1),
+                     "bu_share_of_search_time": round(bu_ms / sweep_ms, 3) if sweep_ms else None,
+                     "td_gbs": round(td_bytes / (td_ms / 1e3) / 1e9, 1) if td_ms else None},
+        "e2e": e2e,
+        "gpu_launches": int(launches_total),
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
+def e2e_dropin(lib, og, s, d, w, roots, rank, dev):
+    """BFS through breadthFirstSearchGraphCSR on a host GraphCSR (built by
+    graphCSRPreProcessingStep from a .wbin file): per call, the stats arrays
+    are host malloc'd and parents/distances are copied device -> host."""
+    import torch
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, f"rmat{SCALE}_{rank}.wbin")
+    og.write_edge_file(path, s, d, w)
+    a = og.default_arguments(fnameb=path, sort=0, weighted=1, pushpull=2)
+    lib.initializeMersenneState(C.byref(a.mt19937var), 27491095)
+    gh = lib.graphCSRPreProcessingStep(C.byref(a))
+    V = gh.contents.num_vertices
+    # warm-up
+    for r in roots[:3]:
+        a.source = r
+        lib.freeBFSStats(lib.breadthFirstSearchGraphCSR(C.byref(a), gh))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for r in roots:
+        a.source = r
+        lib.freeBFSStats(lib.breadthFirstSearchGraphCSR(C.byref(a), gh))
+    t1 = time.perf_counter()
+    # traversed edges of these roots (the same searches, run on the device copy)
+    g = og.DeviceGraph(lib, handle=lib.ogb_graph_of(C.cast(gh, C.c_void_p)), owned=False)
+    pt = torch.empty(V, dtype=torch.int32, device=dev)
+    dt = torch.empty(V, dtype=torch.int32, device=dev)
+    edges = sum(g.bfs(r, pt, dt, mode=2)["reached_out_edges"] for r in roots)
+    lib.graphCSRFree(gh)
+    os.remove(path)
+    n = len(roots)
+    return {"value": round(edges / (t1 - t0) / 1e9, 3), "unit": "GTEPS", "h2d_bytes_per_step": 0,
+            "d2h_bytes_per_step": int(n * 8 * V), "calls_per_step": n,
+            "api": "breadthFirstSearchGraphCSR(pushpull=2) on a graphCSRPreProcessingStep GraphCSR"}
+
+
+def stages(lib, og, g, ts, td, tw, V, E, dev, hbm_peak):
+    import torch
+    out = {}
+    # ---- sort + CSR build (both directions, weighted) --------------------
+    g2 = lib.device_graph()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        g2.build(ts, td, V, 0, weight=tw)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(5):
+        start.record()
+        g2.build(ts, td, V, 0, weight=tw)
+        stop.record()
+        torch.cuda.synchronize()
+        times.append(start.elapsed_time(stop))
+    g2.close()
+    build_ms = statistics.median(times)
+    P = 3  # 8-bit digit passes for 22-bit ids
+    wgt = 1
+    alg = 2 * ((16 + 4 * wgt) * E * P + 4 * E + 4 * E + 12 * V) + (16 + 8 * wgt) * E
+    out["csr_build"] = {"ms": round(build_ms, 3), "medges_per_s": round(E / build_ms / 1e3, 1),
+                        "algorithmic_gb": round(alg / 1e9, 3), "gbs": round(alg / build_ms / 1e6, 1),
+                        "frac": round(alg / build_ms / 1e6 / hbm_peak, 4),
+                        "note": "device sort+CSR both directions incl. one 8 KB host read per sort"}
+    # ---- PageRank pull / push to 1e-6 -----------------------------------
+    ranks = torch.empty(V, dtype=torch.float32, device=dev)
+    for mode, name, per_edge in ((0, "pr_pull", 8), (1, "pr_push", 12)):
+        for _ in range(3):
+            g.pagerank(ranks, mode=mode, max_iterations=PR_MAX, epsilon=PR_TOL)
+        torch.cuda.synchronize()
+        info = g.pagerank(ranks, mode=mode, max_iterations=PR_MAX, epsilon=PR_TOL)
+        errs, _ = g.pagerank_history()
+        hit = next((i for i, e in enumerate(errs) if e < PR_TOL), None)
+        # per-iteration time at a fixed count (no early exit)
+        start.record()
+        info20 = g.pagerank(ranks, mode=mode, max_iterations=20, epsilon=0.0)
+        stop.record()
+        torch.cuda.synchronize()
+        it_ms = start.elapsed_time(stop) / 20
+        alg = per_edge * E + 28 * V
+        out[name] = {"ms_per_iteration": round(it_ms, 4), "gteps": round(E / it_ms / 1e6, 2),
+                     "gbs": round(alg / it_ms / 1e6, 1), "frac": round(alg / it_ms / 1e6 / hbm_peak, 4),
+                     "iterations_to_1e-6_l1": (hit + 1) if hit is not None else None,
+                     "ms_to_1e-6_l1": round(it_ms * (hit + 1), 3) if hit is not None else None,
+                     "reference_stop_rule_iterations": info["iterations"],
+                     "device_ms_run": round(info["ms"], 3)}
+    return out
+
+
+def cpu_baseline(og, s, d, w, roots):
+    """The reference's own OpenMP BFS (oracle/_ref, WEIGHTED build) on this
+    host's cores, same .wbin graph, same roots."""
+    from oracle.oracle import Reference
+    if not Reference.available(True):
+        return {"value": None, "unit": "GTEPS", "kind": "reference", "note": "oracle/_ref not built"}
+    ref = Reference(True)
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, f"rmat{SCALE}.wbin")
+    og.write_edge_file(path, s, d, w)
+    cores = os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    t0 = time.perf_counter()
+    rg = ref.build_graph(path, weighted_file=True)
+    build_s = time.perf_counter() - t0
+    ga_outdeg = og.as_numpy(rg.contents.vertices.contents.out_degree, rg.contents.num_vertices, np.uint32)
+    edges, secs = 0, 0.0
+    for r in roots:
+        p, _, st = ref.bfs(rg, r, 2)
+        edges += int(ga_outdeg[p >= 0].astype(np.uint64).sum())
+        secs += st["time_total"]
+    ref.graphCSRFree(rg)
+    os.remove(path)
+    return {"value": round(edges / secs / 1e9, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
+            "sample": f"{len(roots)} of the {NROOTS} roots (DO-BFS, stats->time_total), same RMAT-{SCALE} graph",
+            "csr_build_s": round(build_s, 3)}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    import opengraph_b200 as og
+    from oracle.oracle import Reference
+    if not Reference.available(True):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference CPU build) not present"}))
+        return
+    s, d, w = og.generate_rmat(SCALE, EDGE_FACTOR, SEED, weighted=True)
+    V = 1 << SCALE
+    ref = Reference(True)
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, f"rmat{SCALE}.wbin")
+    og.write_edge_file(path, s, d, w)
+    cores = os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    rg = ref.build_graph(path, weighted_file=True)
+    outdeg = og.as_numpy(rg.contents.vertices.contents.out_degree, V, np.uint32)
+    rng = np.random.default_rng(1000)
+    roots = [int(x) for x in rng.choice(np.nonzero(outdeg > 0)[0], size=NROOTS, replace=False)]
+    per_step = args.cpu_roots
+
+    def step(k):
+        e, t = 0, 0.0
+        for r in roots[(k * per_step) % NROOTS:][:per_step]:
+            p, _, st = ref.bfs(rg, r, 2)
+            e += int(outdeg[p >= 0].astype(np.uint64).sum())
+            t += st["time_total"]
+        return e, t
+
+    for k in range(args.warmup):
+        step(k)
+    E_tot, T_tot = 0, 0.0
+    for k in range(args.steps):
+        e, t = step(k)
+        E_tot += e
+        T_tot += t
+    ref.graphCSRFree(rg)
+    os.remove(path)
+    val = E_tot / T_tot / 1e9
+    sample = f"{per_step} DO-BFS roots per step (of the {NROOTS}), RMAT-{SCALE}, reference stats->time_total"
+    print(json.dumps({
+        "metric": METRIC, "value": round(val, 4), "unit": "GTEPS", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(T_tot * 1e3 / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded RMAT generator)",
+        "config": {"workload": f"RMAT scale {SCALE}, DO-BFS from seeded random roots", "parallelism": "openmp"},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(val, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(val, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-roots", type=int, default=8)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-stages", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

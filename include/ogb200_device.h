@@ -51,6 +51,8 @@ typedef struct ogb_bfs_info
     uint64_t reached_out_edges;/* sum of out-degrees of reached vertices */
     uint64_t edges_examined;   /* edges read by the steps               */
     double ms;                 /* device time of the traversal          */
+    uint32_t launches;         /* kernels launched by the traversal     */
+    uint32_t pad;
 } ogb_bfs_info;
 
 /* One step of the BFS level trace (ogb_bfs_trace). */
@@ -75,6 +77,8 @@ typedef struct ogb_pr_info
     uint32_t converged;      /* 1 if an iteration had no active vertex */
     double error_total;      /* of the last iteration                 */
     double ms;               /* device time, init to normalization    */
+    uint32_t launches;       /* kernels launched (early-exit ones included) */
+    uint32_t pad;
 } ogb_pr_info;
 
 const char *ogb_last_error(void);
@@ -82,6 +86,9 @@ const char *ogb_last_error(void);
 int ogb_weighted_layout(void);
 /* Silence the reference-style progress tables printed by ogb200.h calls. */
 void ogb_set_quiet(int quiet);
+/* Record CUDA events around every BFS step (per-level device times in the
+ * level trace).  Off by default. */
+void ogb_set_level_timing(int on);
 
 int ogb_graph_create(ogb_graph **g);
 void ogb_graph_destroy(ogb_graph *g);

@@ -118,7 +118,7 @@ class CsrView(C.Structure):
 class BfsInfo(C.Structure):
     _fields_ = [("iteration", u32), ("processed_nodes", u32), ("td_steps", u32), ("bu_steps", u32),
                 ("reached", u32), ("levels", u32), ("reached_out_edges", C.c_uint64),
-                ("edges_examined", C.c_uint64), ("ms", C.c_double)]
+                ("edges_examined", C.c_uint64), ("ms", C.c_double), ("launches", u32), ("pad", u32)]
 
 
 class BfsLevel(C.Structure):
@@ -128,7 +128,7 @@ class BfsLevel(C.Structure):
 
 class PrInfo(C.Structure):
     _fields_ = [("iterations", u32), ("executed", u32), ("activeVertices", u32), ("converged", u32),
-                ("error_total", C.c_double), ("ms", C.c_double)]
+                ("error_total", C.c_double), ("ms", C.c_double), ("launches", u32), ("pad", u32)]
 
 
 def info_dict(s: C.Structure) -> dict:
@@ -188,6 +188,7 @@ _DEVICE_API = [
     ("ogb_last_error", C.c_char_p, []),
     ("ogb_weighted_layout", C.c_int, []),
     ("ogb_set_quiet", None, [C.c_int]),
+    ("ogb_set_level_timing", None, [C.c_int]),
     ("ogb_graph_create", C.c_int, [C.POINTER(vp)]),
     ("ogb_graph_destroy", None, [vp]),
     ("ogb_graph_build", C.c_int, [vp, vp, vp, vp, u32, u32, u32, vp]),

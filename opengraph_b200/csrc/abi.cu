@@ -358,15 +358,17 @@ static void alloc_labels(EdgeList* e, uint32_t V) {
 
 // readEdgeListsbin (edgeList.c:336-594): records of 8 bytes, or 12 when
 // weighted (the weight is read in the WEIGHTED layout and skipped in the
-// other); the WEIGHTED layout without file weights draws them from MT19937
-// seeded 27491095 in edge order.  symmetric appends the reversed copy.
+// other).  The WEIGHTED layout always reads 12-byte records
+// (edgeList.c:383-393) and, when `weighted` is 0, ignores the file's weight
+// and draws one from MT19937 seeded 27491095 in edge order.  symmetric
+// appends the reversed copy.
 extern "C" struct EdgeList* readEdgeListsbin(const char* fname, uint8_t inverse, uint32_t symmetric,
                                              uint32_t weighted) {
   int fd = open(fname, O_RDONLY);
   if (fd == -1) err(1, "open: %s", fname);
   struct stat fs;
   if (fstat(fd, &fs) == -1) err(1, "stat: %s", fname);
-  const size_t rec = weighted ? 12 : 8;
+  const size_t rec = (OGB200_WEIGHTED || weighted) ? 12 : 8;
   const uint32_t num_edges = (uint32_t)((uint64_t)fs.st_size / rec);
   const uint32_t total = symmetric ? num_edges * 2 : num_edges;
   EdgeList* e = newEdgeList(total);
@@ -1161,6 +1163,8 @@ extern "C" uint32_t generateRandomRootGraphCSR(mt19937state* mt, struct GraphCSR
 extern "C" const char* ogb_last_error(void) { return ogb::last_error(); }
 extern "C" int ogb_weighted_layout(void) { return OGB200_WEIGHTED; }
 extern "C" void ogb_set_quiet(int q) { g_quiet = q ? 1 : 0; }
+static bool g_level_timing = false;
+extern "C" void ogb_set_level_timing(int on) { g_level_timing = on != 0; }
 
 extern "C" int ogb_graph_create(ogb_graph** g) {
   if (!g) return fail(ERR_ARG, "null");
@@ -1218,7 +1222,7 @@ extern "C" int ogb_bfs(ogb_graph* g, uint32_t root, uint32_t mode, int32_t* d_pa
   if (!g || !d_parents || !d_distances) return fail(ERR_ARG, "null");
   if (mode > 2) return fail(ERR_ARG, "bfs mode %u", mode);
   static thread_local BfsResult r;
-  OGB_TRY(bfs_run(g->g, root, mode, d_parents, d_distances, &r, false, false, as_stream(stream)));
+  OGB_TRY(bfs_run(g->g, root, mode, d_parents, d_distances, &r, g_level_timing, false, as_stream(stream)));
   g->g.bfs_last_levels = r.nlevels;
   if (info) {
     info->iteration = r.iteration;
@@ -1230,6 +1234,8 @@ extern "C" int ogb_bfs(ogb_graph* g, uint32_t root, uint32_t mode, int32_t* d_pa
     info->reached_out_edges = r.reached_out_edges;
     info->edges_examined = r.edges_examined;
     info->ms = r.ms;
+    info->launches = r.launches;
+    info->pad = 0;
   }
   memcpy(g->g.bfs_trace, r.levels, sizeof(r.levels[0]) * std::min(r.nlevels, 512));
   return OK;
@@ -1270,6 +1276,8 @@ extern "C" int ogb_pagerank(ogb_graph* g, uint32_t mode, uint32_t max_iters, dou
     info->converged = r.converged;
     info->error_total = r.error_total;
     info->ms = r.ms;
+    info->launches = r.launches;
+    info->pad = 0;
   }
   return OK;
 }

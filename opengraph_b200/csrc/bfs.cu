@@ -317,6 +317,7 @@ int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_
 
   bfs_init_kernel<<<grid_v, 256, 0, s>>>(V, g.fwd.d_out_degree(), parents, distances, root, q_cur);
   OGB_CUDA(cudaGetLastError());
+  uint32_t launches = 1;
   uint32_t root_deg = 0;
   OGB_CUDA(cudaMemcpyAsync(&w->h_ctl->mf, g.fwd.d_out_degree() + root, 4, cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaStreamSynchronize(s));
@@ -352,12 +353,14 @@ int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_
       OGB_CUDA(cudaMemsetAsync(bm_cur, 0, (size_t)words * 4, s));
       bfs_queue_to_bitmap_kernel<<<std::min<uint32_t>(grid_v, ceil_div(qsize, 256)), 256, 0, s>>>(q_cur, qsize, bm_cur);
       OGB_CUDA(cudaGetLastError());
+      launches++;
       nf = bu_entry_nf_frontier ? qsize : 0;
       uint32_t frontier = qsize;
       do {
         nf_prev = nf;
         OGB_CUDA(cudaMemsetAsync(d_ctl, 0, sizeof(BfsCtl), s));
         if (time_levels) OGB_CUDA(cudaEventRecord(w->ev_a, s));
+        launches++;
         if (!ul_valid) {
           bfs_bu_dense_kernel<false><<<grid_v, 256, 0, s>>>(V, g.inv.d_rows(), g.inv.d_dst(), bm_cur, bm_next,
                                                             parents, distances, ul_next, d_ctl);
@@ -389,6 +392,7 @@ int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_
       bfs_bitmap_to_queue_kernel<<<std::min<uint32_t>(grid_v, ceil_div(words, 256)), 256, 0, s>>>(bm_cur, words,
                                                                                                     q_cur, &d_ctl->qnext);
       OGB_CUDA(cudaGetLastError());
+      launches++;
       OGB_TRY(read_ctl(w, s));
       qsize = w->h_ctl->qnext;
       mf = 1;
@@ -400,6 +404,7 @@ int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_
       bfs_td_kernel<<<grid_td, 256, 0, s>>>(g.fwd.d_rows(), g.fwd.d_dst(), q_cur, qsize, q_next, parents, distances,
                                              d_ctl);
       OGB_CUDA(cudaGetLastError());
+      launches++;
       if (time_levels) OGB_CUDA(cudaEventRecord(w->ev_b, s));
       OGB_TRY(read_ctl(w, s));
       float ms = 0.f;
@@ -421,6 +426,7 @@ int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_
   float total_ms = 0.f;
   OGB_CUDA(cudaEventElapsedTime(&total_ms, w->ev_start, w->ev_stop));
   r.ms = total_ms;
+  r.launches = launches;
 
   OGB_CUDA(cudaMemsetAsync(d_ctl, 0, sizeof(BfsCtl), s));
   bfs_reached_kernel<<<grid_v, 256, 0, s>>>(V, parents, g.fwd.d_out_degree(), d_ctl);

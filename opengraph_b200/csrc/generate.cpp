@@ -115,7 +115,8 @@ extern "C" int ogb_generate_uniform(uint32_t num_vertices, uint64_t num_edges, u
 extern "C" int ogb_generate_grid(uint32_t side, double p, uint64_t seed, uint32_t* src, uint32_t* dst, float* w,
                                  uint64_t* num_edges) {
   if (side < 2 || !num_edges || (uint64_t)side * side > 0xFFFFFFFFull) return OGB_ERR_ARG;
-  const uint64_t thresh = (uint64_t)(p * 18446744073709551616.0);
+  const bool always = p >= 1.0;
+  const uint64_t thresh = always ? ~0ull : (uint64_t)(p * 18446744073709551616.0);
   uint64_t k = 0;
   for (uint32_t r = 0; r < side; r++) {
     for (uint32_t c = 0; c < side; c++) {
@@ -132,7 +133,7 @@ extern "C" int ogb_generate_grid(uint32_t side, double p, uint64_t seed, uint32_
       if (r + 1 < side) emit(v, v + side);
       if (c > 0) emit(v, v - 1);
       if (c + 1 < side) emit(v, v + 1);
-      if (r + 1 < side && c + 1 < side && p > 0 && draw(seed, v, 7) < thresh) {
+      if (r + 1 < side && c + 1 < side && p > 0 && (always || draw(seed, v, 7) < thresh)) {
         emit(v, v + side + 1);
         emit(v + side + 1, v);
       }

@@ -88,6 +88,7 @@ struct BfsResult {
   uint64_t edges_examined = 0;
   uint64_t reached_out_edges = 0;  // sum of out-degrees of reached vertices
   uint32_t reached = 0;
+  uint32_t launches = 0;  // kernels launched by the traversal
   double ms = 0.0;
   int nlevels = 0;
   BfsLevel levels[512];
@@ -125,6 +126,7 @@ struct PrResult {
   uint32_t activeVertices = 0;
   double error_total = 0.0;
   double ms = 0.0;
+  uint32_t launches = 0;
   int converged = 0;
   double err_hist[1024];
   uint32_t active_hist[1024];

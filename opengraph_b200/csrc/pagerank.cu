@@ -366,6 +366,7 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
   OGB_CUDA(cudaEventElapsedTime(&ms, w->ev0, w->ev1));
   PrResult r;
   r.ms = ms;
+  r.launches = 2 + max_iters * (pull ? 1 : 2);
   if (w->h_ctl->stop) {
     r.converged = 1;
     r.iterations = w->h_ctl->stop_iter;

@@ -1,0 +1,192 @@
+"""GPU drop-in parity: the OpenGraph C API of libogb200 against the
+reference's own CPU build (oracle/_ref) on the same .bin/.wbin files, called
+exactly as the reference driver calls it (graphRun.c:323, :675, :1038)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def files(tmp_path_factory, og, graphs):
+    d = tmp_path_factory.mktemp("graphs")
+    out = {}
+    s, dd, w, V = graphs("rmat", scale=14, ef=16, seed=11, weighted=True)
+    out["rmat"] = str(d / "rmat14.bin")
+    og.write_edge_file(out["rmat"], s, dd)
+    out["rmat_w"] = str(d / "rmat14.wbin")
+    og.write_edge_file(out["rmat_w"], s, dd, w)
+    s, dd, w, V = graphs("star", n=3000, seed=4, weighted=True)
+    out["star_w"] = str(d / "star.wbin")
+    og.write_edge_file(out["star_w"], s, dd, w)
+    return out
+
+
+def _build(lib_or_ref, path, **kw):
+    a = lib_or_ref.og.default_arguments(fnameb=path, **kw) if hasattr(lib_or_ref, "og") else None
+    return a
+
+
+def our_graph(og, lib, path, **kw):
+    a = og.default_arguments(fnameb=path, **kw)
+    lib.initializeMersenneState(C.byref(a.mt19937var), 27491095)
+    g = lib.graphCSRPreProcessingStep(C.byref(a))
+    return g, a
+
+
+@pytest.mark.parametrize("sort", [0, 1, 2, 3])
+@pytest.mark.parametrize("dflag", [0, 1])
+@pytest.mark.parametrize("weighted", [False, True])
+def test_preprocessing_step_matches_reference(og, lib, libw, ref, refw, files, sort, dflag, weighted):
+    L, R = (libw, refw) if weighted else (lib, ref)
+    path = files["rmat_w"] if weighted else files["rmat"]
+    kw = dict(sort=sort, dflag=dflag, weighted=1 if weighted else 0)
+    g, _ = our_graph(og, L, path, **kw)
+    rg = R.build_graph(path, sort=sort, dflag=dflag, weighted_file=weighted)
+    ours, theirs = og.graph_arrays(g), og.graph_arrays(rg)
+    for k, v in theirs.items():
+        if isinstance(v, np.ndarray):
+            assert np.array_equal(ours[k], v), k
+        else:
+            assert ours[k] == v, k
+    L.graphCSRFree(g)
+    R.graphCSRFree(rg)
+
+
+def test_dedup_weighted_star_matches_reference(og, libw, refw, files):
+    g, _ = our_graph(og, libw, files["star_w"], sort=1, dflag=1, weighted=1)
+    rg = refw.build_graph(files["star_w"], sort=1, dflag=1, weighted_file=True)
+    ours, theirs = og.graph_arrays(g), og.graph_arrays(rg)
+    for k, v in theirs.items():
+        if isinstance(v, np.ndarray):
+            assert np.array_equal(ours[k], v), k
+    libw.graphCSRFree(g)
+    refw.graphCSRFree(rg)
+
+
+@pytest.mark.parametrize("pushpull", [0, 1, 2, 3, 4])
+def test_bfs_dropin_matches_reference(og, lib, ref, files, pushpull):
+    g, _ = our_graph(og, lib, files["rmat"])
+    rg = ref.build_graph(files["rmat"])
+    ga = og.graph_arrays(g)
+    roots = [int(np.argmax(ga["f_outdeg"])), 1, 77, 4000]
+    for root in roots:
+        a = og.default_arguments(source=root, pushpull=pushpull)
+        st = lib.breadthFirstSearchGraphCSR(C.byref(a), g)
+        rp, rd, rs = ref.bfs(rg, root, pushpull)
+        s = st.contents
+        V = s.num_vertices
+        dist = og.as_numpy(s.distances, V, np.uint32)
+        par = og.as_numpy(s.parents, V, np.int32)
+        assert np.array_equal(dist, rd), (root, pushpull)
+        assert s.processed_nodes == rs["processed_nodes"]
+        assert s.iteration == rs["iteration"]
+        assert a.source == root  # label array is the identity here
+        assert np.array_equal(par < 0, rp < 0)
+        assert np.array_equal(par[par < 0], rp[rp < 0])   # sentinels untouched
+        if pushpull == 0:
+            assert np.array_equal(par, rp)
+        lib.freeBFSStats(st)
+    lib.graphCSRFree(g)
+    ref.graphCSRFree(rg)
+
+
+def test_bfs_out_of_range_root_returns_initial_stats(og, lib, files):
+    g, _ = our_graph(og, lib, files["rmat"])
+    V = g.contents.num_vertices
+    a = og.default_arguments(source=V + 5, pushpull=2)
+    st = lib.breadthFirstSearchGraphCSR(C.byref(a), g)
+    s = st.contents
+    assert s.processed_nodes == 0 and s.iteration == 0
+    assert np.all(og.as_numpy(s.distances, V, np.uint32) == 0)
+    lib.freeBFSStats(st)
+    lib.graphCSRFree(g)
+
+
+@pytest.mark.parametrize("pushpull", [0, 1])
+def test_pagerank_dropin_matches_reference(og, lib, ref, files, pushpull):
+    g, _ = our_graph(og, lib, files["rmat"])
+    rg = ref.build_graph(files["rmat"])
+    a = og.default_arguments(pushpull=pushpull, iterations=20, epsilon=1e-4)
+    st = lib.pageRankGraphCSR(C.byref(a), g)
+    rr, rs = ref.pagerank(rg, pushpull, 20, 1e-4)
+    s = st.contents
+    pr = og.as_numpy(s.pageRanks, s.num_vertices, np.float32)
+    assert s.iterations == rs["iterations"]
+    assert float(np.abs(pr.astype(np.float64) - rr).sum()) <= 1e-6
+    assert abs(s.error_total - rs["error_total"]) <= 1e-9 + 1e-6 * rs["error_total"]
+    assert np.array_equal(og.as_numpy(s.realRanks, s.num_vertices, np.uint32), np.arange(s.num_vertices))
+    lib.freePageRankStats(st)
+    # unsupported variants return NULL like an unknown structure
+    a.pushpull = 5
+    assert not lib.pageRankGraphCSR(C.byref(a), g)
+    lib.graphCSRFree(g)
+    ref.graphCSRFree(rg)
+
+
+def test_sort_entry_points_match_reference(og, lib, ref, files):
+    for fn in ("radixSortEdgesBySource", "radixSortEdgesBySourceAndDestination", "countSortEdgesBySource",
+               "countSortEdgesByDestination", "countSortEdgesBySourceAndDestination"):
+        ours = lib.readEdgeListsbin(files["rmat"].encode(), 0, 0, 0)
+        theirs = ref.readEdgeListsbin(files["rmat"].encode(), 0, 0, 0)
+        o = getattr(lib, fn)(ours)
+        t = getattr(ref, fn)(theirs)
+        oa, ta = og.edge_list_arrays(o), og.edge_list_arrays(t)
+        assert np.array_equal(oa["src"], ta["src"]) and np.array_equal(oa["dst"], ta["dst"]), fn
+        lib.freeEdgeList(o)
+        ref.freeEdgeList(t)
+
+
+def test_step_functions_match_reference(og, lib, ref, files):
+    """topDownStepGraphCSR / bottomUpStepGraphCSR over host queues/bitmaps."""
+    g, _ = our_graph(og, lib, files["rmat"])
+    rg = ref.build_graph(files["rmat"])
+    ga = og.graph_arrays(g)
+    V = ga["num_vertices"]
+    root = int(np.argmax(ga["f_outdeg"]))
+    # top-down level 1 from the root, on both libraries
+    res = {}
+    for name, L, G in (("ours", lib, g), ("ref", ref, rg)):
+        st = L.newBFSStatsGraphCSR(G)
+        s = st.contents
+        s.parents[root] = root
+        q = og.ArrayQueue()
+        qbuf = (C.c_uint32 * V)()
+        qbuf[0] = root
+        q.head, q.tail, q.tail_next, q.size = 0, 1, 1, V
+        q.queue = C.cast(qbuf, C.POINTER(C.c_uint32))
+        locals_ = (C.POINTER(og.ArrayQueue) * 64)()
+        if name == "ref":
+            # the reference's step writes into per-thread queues of size V
+            keep = []
+            newq = ref.d.newArrayQueue
+            newq.restype = C.POINTER(og.ArrayQueue)
+            newq.argtypes = [C.c_uint32]
+            for i in range(64):
+                locals_[i] = newq(V)
+        mf = L.topDownStepGraphCSR(G, C.byref(q), locals_, st)
+        nq = sorted(qbuf[q.tail:q.tail_next])
+        dist = og.as_numpy(s.distances, V, np.uint32)
+        res[name] = (mf, nq, dist.copy())
+        # then a bottom-up level from that frontier
+        bm_words = (V + 31) // 32
+        cur = (C.c_uint32 * bm_words)()
+        nxt = (C.c_uint32 * bm_words)()
+        for v in nq:
+            cur[v >> 5] |= 1 << (v & 31)
+        b1, b2 = og.Bitmap(), og.Bitmap()
+        b1.size = b2.size = V
+        b1.real_size = b2.real_size = bm_words
+        b1.bitarray = C.cast(cur, C.POINTER(C.c_uint32))
+        b2.bitarray = C.cast(nxt, C.POINTER(C.c_uint32))
+        nf = L.bottomUpStepGraphCSR(G, C.byref(b1), C.byref(b2), st)
+        res[name] += (nf, np.frombuffer(nxt, np.uint32).copy(), og.as_numpy(s.distances, V, np.uint32),
+                      og.as_numpy(s.parents, V, np.int32))
+        L.freeBFSStats(st)
+    o, r = res["ours"], res["ref"]
+    assert o[0] == r[0] and o[1] == r[1] and np.array_equal(o[2], r[2])
+    assert o[3] == r[3] and np.array_equal(o[4], r[4]) and np.array_equal(o[5], r[5])
+    lib.graphCSRFree(g)
+    ref.graphCSRFree(rg)

@@ -1,0 +1,133 @@
+"""Pinning the oracle (CPU, no GPU): the C restatement in oracle/og_oracle.c
+must reproduce the reference's outputs bit for bit -- against the committed
+golden fixtures (made by tests/golden/make_golden.py from the reference's own
+build) and, when oracle/_ref is present, against the reference live."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+LAW_ENRON = "/root/reference/01_test_graphs/LAW/LAW-enron/graph.bin"
+
+
+def test_fixtures_present():
+    assert len(FIXTURES) >= 8
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p) for p in FIXTURES])
+def test_oracle_matches_golden(oracle, path):
+    z = dict(np.load(path))
+    weighted = path.endswith("_w1.npz")
+    s, d = z["src"], z["dst"]
+    w = z["w"] if weighted else None
+    for sort in range(4):
+        es, ed, ew = oracle.sort(s, d, w, 1 if sort in (1, 3) else 0)
+        assert np.array_equal(es, z[f"sort{sort}_src"]) and np.array_equal(ed, z[f"sort{sort}_dst"]), sort
+        if weighted:
+            assert np.array_equal(ew.view(np.uint32), z[f"sort{sort}_w"].view(np.uint32))
+    V = int(z["csr_s0_d0_num_vertices"])
+    for sort in (0, 1):
+        g = oracle.build(s, d, V, sort, w)
+        tag = f"csr_s{sort}_d0_"
+        for k in ("f_src", "f_dst", "f_outdeg", "f_indeg", "f_idx", "i_src", "i_dst", "i_outdeg", "i_indeg", "i_idx"):
+            assert np.array_equal(g[k], z[tag + k]), (sort, k)
+        if weighted:
+            assert np.array_equal(g["f_w"].view(np.uint32), z[tag + "f_w"].view(np.uint32))
+            assert np.array_equal(g["i_w"].view(np.uint32), z[tag + "i_w"].view(np.uint32))
+    # dedup path (sort 1 + removeDulpicatesSelfLoopEdges)
+    ss, sd, sw = oracle.sort(s, d, w, 1)
+    ds, dd, dw = oracle.dedup(ss, sd, sw, truncate_w=weighted)
+    g = oracle.build(ds, dd, V, 1, dw)
+    for k in ("f_src", "f_dst", "f_outdeg", "f_idx", "i_src", "i_dst", "i_outdeg", "i_idx"):
+        assert np.array_equal(g[k], z["csr_s1_d1_" + k]), ("dedup", k)
+    if weighted:
+        assert np.array_equal(g["f_w"].view(np.uint32), z["csr_s1_d1_f_w"].view(np.uint32))
+    # BFS and PageRank on the sort-0 graph
+    g = oracle.build(s, d, V, 0, None)
+    for mode in (0, 1, 2):
+        for i, r in enumerate(z["bfs_roots"]):
+            par, dist, st = oracle.bfs(g, int(r), mode)
+            assert np.array_equal(dist, z[f"bfs_m{mode}_r{i}_dist"]), (mode, i)
+            assert [st["processed_nodes"], st["iteration"]] == list(z[f"bfs_m{mode}_r{i}_stats"])
+            if mode == 0:
+                assert np.array_equal(par, z[f"bfs_m{mode}_r{i}_par"])
+    ranks, st = oracle.pagerank(g, 0, 20, 1e-4)
+    assert np.array_equal(ranks.view(np.uint32), z["pr_pull_ranks"].view(np.uint32))
+    assert st["iterations"] == int(z["pr_pull_stats"][0])
+    assert abs(st["error_total"] - float(z["pr_pull_error"][0])) <= 1e-12
+
+
+@pytest.mark.parametrize("scale,sort", [(10, 0), (12, 1), (12, 2), (13, 3)])
+def test_oracle_matches_reference_live(og, oracle, ref, tmp_path, scale, sort):
+    s, d, _ = og.generate_rmat(scale, 16, 7)
+    path = str(tmp_path / "g.bin")
+    og.write_edge_file(path, s, d)
+    rg = ref.build_graph(path, sort=sort)
+    ga = og.graph_arrays(rg)
+    g = oracle.build(s, d, ga["num_vertices"], sort)
+    for k, v in g.items():
+        if isinstance(v, np.ndarray):
+            assert np.array_equal(v, ga[k]), k
+    root = int(np.argmax(ga["f_outdeg"]))
+    for mode in (0, 1, 2):
+        rp, rd, rs = ref.bfs(rg, root, mode)
+        op, od, os_ = oracle.bfs(g, root, mode)
+        assert np.array_equal(rd, od)
+        assert rs["processed_nodes"] == os_["processed_nodes"] and rs["iteration"] == os_["iteration"]
+    rr, rs = ref.pagerank(rg, 0, 30, 1e-6)
+    orr, os_ = oracle.pagerank(g, 0, 30, 1e-6)
+    assert np.array_equal(rr.view(np.uint32), orr.view(np.uint32))
+    assert rs["iterations"] == os_["iterations"]
+    ref.graphCSRFree(rg)
+
+
+@pytest.mark.skipif(not os.path.exists(LAW_ENRON), reason="reference test graph not mounted")
+def test_oracle_matches_reference_on_law_enron(og, oracle, ref):
+    """The reference's own equivalence-test input (test_open-graph-match.c:59-86:
+    LAW-enron, dflag=1 so sort=1)."""
+    raw = np.fromfile(LAW_ENRON, dtype=np.uint32).reshape(-1, 2)
+    s, d = raw[:, 0].copy(), raw[:, 1].copy()
+    rg = ref.build_graph(LAW_ENRON, sort=1, dflag=1)
+    ga = og.graph_arrays(rg)
+    V = ga["num_vertices"]
+    ss, sd, _ = oracle.sort(s, d, None, 1)
+    ds, dd, _ = oracle.dedup(ss, sd)
+    g = oracle.build(ds, dd, V, 1)
+    for k, v in g.items():
+        if isinstance(v, np.ndarray):
+            assert np.array_equal(v, ga[k]), k
+    for root in (int(np.argmax(ga["f_outdeg"])), 0, 12345):
+        rp, rd, rs = ref.bfs(rg, root, 2)
+        op, od, os_ = oracle.bfs(g, root, 2)
+        assert np.array_equal(rd, od)
+    rr, rs = ref.pagerank(rg, 0, 100, 1e-6)
+    orr, os_ = oracle.pagerank(g, 0, 100, 1e-6)
+    assert np.array_equal(rr.view(np.uint32), orr.view(np.uint32)) and rs["iterations"] == os_["iterations"]
+    ref.graphCSRFree(rg)
+
+
+def test_oracle_fp64_close_to_fp32(og, oracle):
+    s, d, _ = og.generate_rmat(11, 16, 1)
+    V = int(max(s.max(), d.max())) + 1
+    g = oracle.build(s, d, V, 0)
+    r32, _ = oracle.pagerank(g, 0, 30, 0.0)
+    r64 = oracle.pagerank_f64(g, 30)
+    assert float(np.abs(r32 - r64).sum()) < 1e-5
+
+
+def test_oracle_random_roots_match_reference_picker(og, oracle, ref, tmp_path):
+    import ctypes as C
+    s, d, _ = og.generate_rmat(10, 16, 2)
+    path = str(tmp_path / "g.bin")
+    og.write_edge_file(path, s, d)
+    rg = ref.build_graph(path)
+    ga = og.graph_arrays(rg)
+    roots = oracle.random_roots(ga["num_vertices"], ga["avg_degree"], ga["f_outdeg"], 20)
+    mt = og.mt19937state()
+    ref.initializeMersenneState(C.byref(mt), 27491095)
+    for r in roots:
+        assert ref.d.generateRandomRootGraphCSR(C.byref(mt), rg) == r
+    ref.graphCSRFree(rg)
