@@ -116,6 +116,12 @@ int ogb_bfs_trace(ogb_graph *g, ogb_bfs_level *levels, uint32_t max_levels, uint
  * d_init (may be NULL) replaces the uniform unnormalized start 1-0.85. */
 int ogb_pagerank(ogb_graph *g, uint32_t mode, uint32_t max_iterations, double epsilon, float *d_ranks,
                  const float *d_init, ogb_pr_info *info, void *stream);
+/* Work split of the PageRank kernels by row length: rows of at most warp_thr
+ * edges are reduced by one thread in CSR order (the reference's summation
+ * order), longer rows by a warp, rows above cta_thr by a CTA of cta_threads
+ * threads (fixed-order butterfly sums).  Defaults 32 / 2048 / 256. */
+void ogb_pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr);
+void ogb_pagerank_get_bins(uint32_t *warp_thr, uint32_t *cta_thr, uint32_t *cta_threads);
 /* Per-iteration L1 error and active count of the last ogb_pagerank on g. */
 int ogb_pagerank_history(ogb_graph *g, double *errors, uint32_t *active, uint32_t max_entries, uint32_t *count);
 

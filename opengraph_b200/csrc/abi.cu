@@ -1282,6 +1282,12 @@ extern "C" int ogb_pagerank(ogb_graph* g, uint32_t mode, uint32_t max_iters, dou
   return OK;
 }
 
+extern "C" void ogb_pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr) { pagerank_set_bins(warp_thr, cta_thr); }
+
+extern "C" void ogb_pagerank_get_bins(uint32_t* warp_thr, uint32_t* cta_thr, uint32_t* cta_threads) {
+  pagerank_get_bins(warp_thr, cta_thr, cta_threads);
+}
+
 extern "C" int ogb_pagerank_history(ogb_graph* g, double* errors, uint32_t* active, uint32_t max_entries,
                                     uint32_t* count) {
   if (!g) return fail(ERR_ARG, "null");

@@ -141,4 +141,9 @@ enum PrMode : uint32_t { PR_PULL = 0, PR_PUSH = 1 };
 int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon, float* ranks,
                  const float* init, PrResult* res, cudaStream_t s);
 
+// Row-length thresholds of the PageRank work split (light rows per thread,
+// heavy rows per warp, very heavy rows per CTA of cta_threads threads).
+void pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr);
+void pagerank_get_bins(uint32_t* warp_thr, uint32_t* cta_thr, uint32_t* cta_threads);
+
 }  // namespace ogb

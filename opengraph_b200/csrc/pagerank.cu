@@ -16,12 +16,16 @@
 // Device design: the contrib of the next iteration is written by the update
 // of this one (double-buffered), so an iteration of pull is ONE kernel that
 // gathers, updates, writes the next contrib and reduces error/active.
-// Vertices are split once per graph into degree bins: a thread per vertex
-// (sequential fp32 sum in CSR order, the reference's exact order), a warp
-// per vertex, and a CTA per vertex (fixed-order tree sums; deterministic run
-// to run).  Iterations are launched back to back without host round trips:
-// each iteration's last CTA records error/active and, when active == 0, sets
-// a stop flag that later launches read first.
+// Work split by row length (in-degree for pull, out-degree for push):
+//   light rows (<= warp_thr edges): a thread per vertex, vertices in
+//     ascending order so a warp's 32 rows are adjacent in memory; pull sums
+//     sequentially in CSR order -- the reference's exact order;
+//   heavy rows (> warp_thr): a warp per vertex, lanes strided over the row,
+//     butterfly-folded; rows > cta_thr: a 256-thread CTA per vertex.
+// The heavy lists are built once per graph and direction.  Iterations are
+// launched back to back without host round trips: each iteration's last CTA
+// records error/active and, when active == 0, sets a stop flag that later
+// launches read first.
 #include "graph.cuh"
 
 #include <algorithm>
@@ -30,8 +34,22 @@
 namespace ogb {
 
 constexpr uint32_t kPrMaxIters = 1024;
-constexpr uint32_t kBinWarp = 32;    // in-degree above this: warp per vertex
-constexpr uint32_t kBinCta = 2048;   // in-degree above this: CTA per vertex
+constexpr int kPrThreads = 256;
+
+// Row-length thresholds of the work split (settable; the GPU-order mode of
+// the oracle takes the same values).
+static uint32_t g_warp_thr = 32;
+static uint32_t g_cta_thr = 2048;
+
+void pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr) {
+  g_warp_thr = warp_thr;
+  g_cta_thr = std::max(cta_thr, warp_thr);
+}
+void pagerank_get_bins(uint32_t* warp_thr, uint32_t* cta_thr, uint32_t* cta_threads) {
+  *warp_thr = g_warp_thr;
+  *cta_thr = g_cta_thr;
+  *cta_threads = kPrThreads;
+}
 
 struct PrCtl {
   double err[kPrMaxIters];
@@ -43,10 +61,11 @@ struct PrCtl {
 
 struct PrWork {
   uint32_t V = 0;
-  int binned_for_pull = -1;  // which direction the bins describe
+  int listed_pull = -1;                // direction the heavy lists describe
+  uint32_t listed_warp = 0, listed_cta = 0;
   DevBuf contrib0, contrib1, next, ctl;
-  DevBuf bins;               // vertex ids: [thread bin | warp bin | cta bin]
-  uint32_t n_thread = 0, n_warp = 0, n_cta = 0;
+  DevBuf heavy;                        // vertex ids: [warp list | cta list]
+  uint32_t n_warp = 0, n_cta = 0;
   PrCtl* h_ctl = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   ~PrWork() {
@@ -58,26 +77,31 @@ struct PrWork {
 
 void pr_work_free(PrWork* w) { delete w; }
 
-// ------------------------------------------------------------------ bins ----
+// ------------------------------------------------------------ heavy lists ---
 
-__global__ void pr_bin_count_kernel(uint32_t V, const uint2* __restrict__ rows, uint32_t* __restrict__ counts) {
-  uint32_t c[3] = {0, 0, 0};
+__global__ void pr_heavy_count_kernel(uint32_t V, const uint2* __restrict__ rows, uint32_t warp_thr,
+                                      uint32_t cta_thr, uint32_t* __restrict__ counts) {
+  uint32_t cw = 0, cc = 0;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     const uint32_t d = rows[v].y;
-    c[d > kBinCta ? 2 : (d > kBinWarp ? 1 : 0)]++;
+    cw += (d > warp_thr && d <= cta_thr);
+    cc += (d > cta_thr);
   }
-  for (int b = 0; b < 3; b++) warp_atomic_add_total(&counts[b], c[b]);
+  warp_atomic_add_total(&counts[0], cw);
+  warp_atomic_add_total(&counts[1], cc);
 }
 
-// Order inside a bin does not matter for the results (each vertex is
-// reduced by exactly one thread, warp or CTA).
-__global__ void pr_bin_fill_kernel(uint32_t V, const uint2* __restrict__ rows, uint32_t* __restrict__ cursor,
-                                   uint32_t* __restrict__ bins, uint32_t off_warp, uint32_t off_cta) {
+// Order inside a list does not change results: each heavy vertex is reduced
+// by exactly one warp or CTA in a fixed order.
+__global__ void pr_heavy_fill_kernel(uint32_t V, const uint2* __restrict__ rows, uint32_t warp_thr,
+                                     uint32_t cta_thr, uint32_t* __restrict__ cursor, uint32_t* __restrict__ list,
+                                     uint32_t off_cta) {
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     const uint32_t d = rows[v].y;
-    const int b = d > kBinCta ? 2 : (d > kBinWarp ? 1 : 0);
-    uint32_t base = b == 0 ? 0 : (b == 1 ? off_warp : off_cta);
-    bins[base + atomicAdd(&cursor[b], 1u)] = v;
+    if (d > cta_thr)
+      list[off_cta + atomicAdd(&cursor[1], 1u)] = v;
+    else if (d > warp_thr)
+      list[atomicAdd(&cursor[0], 1u)] = v;
   }
 }
 
@@ -86,8 +110,8 @@ __global__ void pr_bin_fill_kernel(uint32_t V, const uint2* __restrict__ rows, u
 struct PrParams {
   float base_pr, damp;
   double epsilon;
-  double inv_v;  // 1.0 / V is NOT used: the reference divides each error by V
   uint32_t V;
+  uint32_t warp_thr;
 };
 
 __device__ __forceinline__ void pr_update(uint32_t v, float s, float* __restrict__ pr,
@@ -104,10 +128,9 @@ __device__ __forceinline__ void pr_update(uint32_t v, float s, float* __restrict
   active += (e >= p.epsilon) ? 1u : 0u;
 }
 
-template <int THREADS>
 __device__ __forceinline__ void pr_block_finish(double err, uint32_t active, PrCtl* ctl, uint32_t it) {
-  __shared__ double s_err[THREADS / 32];
-  __shared__ uint32_t s_act[THREADS / 32];
+  __shared__ double s_err[kPrThreads / 32];
+  __shared__ uint32_t s_act[kPrThreads / 32];
   for (int o = 16; o; o >>= 1) {
     err += __shfl_down_sync(0xffffffffu, err, o);
     active += __shfl_down_sync(0xffffffffu, active, o);
@@ -121,7 +144,7 @@ __device__ __forceinline__ void pr_block_finish(double err, uint32_t active, PrC
   if (threadIdx.x == 0) {
     double e = 0;
     uint32_t a = 0;
-    for (int w = 0; w < THREADS / 32; w++) {
+    for (int w = 0; w < kPrThreads / 32; w++) {
       e += s_err[w];
       a += s_act[w];
     }
@@ -139,114 +162,120 @@ __device__ __forceinline__ void pr_block_finish(double err, uint32_t active, PrC
   }
 }
 
-// Pull iteration: all three bins in one grid.  Blocks [0, nb_thread) run the
-// thread bin, the next nb_warp blocks the warp bin, the rest the CTA bin.
-template <int THREADS>
-__global__ void __launch_bounds__(THREADS) pr_pull_kernel(
-    const uint32_t* __restrict__ bins, uint32_t n_thread, uint32_t n_warp, uint32_t n_cta, uint32_t nb_thread,
-    uint32_t nb_warp, const uint2* __restrict__ rows, const uint32_t* __restrict__ nbr,
-    const uint32_t* __restrict__ out_degree, const float* __restrict__ contrib, float* __restrict__ contrib_next,
-    float* __restrict__ pr, PrParams p, PrCtl* __restrict__ ctl, uint32_t it) {
+// Sum of c[nbr[j]] over a row by the calling warp (lanes strided, butterfly).
+__device__ __forceinline__ float warp_row_sum(const float* __restrict__ c, const uint32_t* __restrict__ nbr,
+                                              uint2 row) {
+  float s = 0.0f;
+  for (uint32_t j = row.x + lane_id(); j < row.x + row.y; j += 32) s = __fadd_rn(s, c[nbr[j] & 0x3FFFFFFFu]);
+#pragma unroll
+  for (int o = 16; o; o >>= 1) s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
+  return s;
+}
+
+// Pull iteration, one grid: blocks [0, nb_light) walk all vertices in order
+// and take the light rows, the next nb_warp blocks the warp list, the rest
+// the CTA list.
+__global__ void __launch_bounds__(kPrThreads) pr_pull_kernel(
+    uint32_t nb_light, uint32_t nb_warp, const uint32_t* __restrict__ heavy, uint32_t n_warp, uint32_t n_cta,
+    const uint2* __restrict__ rows, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ out_degree,
+    const float* __restrict__ contrib, float* __restrict__ contrib_next, float* __restrict__ pr, PrParams p,
+    PrCtl* __restrict__ ctl, uint32_t it) {
   if (ctl->stop) return;
   double err = 0.0;
   uint32_t active = 0;
   const uint32_t b = blockIdx.x;
-  if (b < nb_thread) {
-    for (uint32_t t = b * THREADS + threadIdx.x; t < n_thread; t += nb_thread * THREADS) {
-      const uint32_t v = bins[t];
+  if (b < nb_light) {
+    for (uint32_t v = b * kPrThreads + threadIdx.x; v < p.V; v += nb_light * kPrThreads) {
       const uint2 row = rows[v];
+      if (row.y > p.warp_thr) continue;
       float s = 0.0f;
       for (uint32_t j = row.x; j < row.x + row.y; j++) s = __fadd_rn(s, contrib[nbr[j] & 0x3FFFFFFFu]);
       pr_update(v, s, pr, out_degree, contrib_next, p, err, active);
     }
-  } else if (b < nb_thread + nb_warp) {
-    const uint32_t lane = lane_id();
-    const uint32_t w0 = (b - nb_thread) * (THREADS / 32) + (threadIdx.x >> 5);
-    const uint32_t wstride = nb_warp * (THREADS / 32);
+  } else if (b < nb_light + nb_warp) {
+    const uint32_t w0 = (b - nb_light) * (kPrThreads / 32) + (threadIdx.x >> 5);
+    const uint32_t wstride = nb_warp * (kPrThreads / 32);
     for (uint32_t t = w0; t < n_warp; t += wstride) {
-      const uint32_t v = bins[n_thread + t];
-      const uint2 row = rows[v];
-      float s = 0.0f;
-      for (uint32_t j = row.x + lane; j < row.x + row.y; j += 32) s = __fadd_rn(s, contrib[nbr[j] & 0x3FFFFFFFu]);
-      for (int o = 16; o; o >>= 1) s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
-      if (lane == 0) pr_update(v, s, pr, out_degree, contrib_next, p, err, active);
+      const uint32_t v = heavy[t];
+      const float s = warp_row_sum(contrib, nbr, rows[v]);
+      if (lane_id() == 0) pr_update(v, s, pr, out_degree, contrib_next, p, err, active);
     }
   } else {
-    __shared__ float s_part[THREADS / 32];
-    const uint32_t cb = b - nb_thread - nb_warp;
-    const uint32_t ncb = gridDim.x - nb_thread - nb_warp;
+    __shared__ float s_part[kPrThreads / 32];
+    const uint32_t cb = b - nb_light - nb_warp;
+    const uint32_t ncb = gridDim.x - nb_light - nb_warp;
     for (uint32_t t = cb; t < n_cta; t += ncb) {
-      const uint32_t v = bins[n_thread + n_warp + t];
+      const uint32_t v = heavy[n_warp + t];
       const uint2 row = rows[v];
       float s = 0.0f;
-      for (uint32_t j = row.x + threadIdx.x; j < row.x + row.y; j += THREADS)
+      for (uint32_t j = row.x + threadIdx.x; j < row.x + row.y; j += kPrThreads)
         s = __fadd_rn(s, contrib[nbr[j] & 0x3FFFFFFFu]);
+#pragma unroll
       for (int o = 16; o; o >>= 1) s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
       if (lane_id() == 0) s_part[threadIdx.x >> 5] = s;
       __syncthreads();
       if (threadIdx.x == 0) {
         float tot = 0.0f;
-        for (int w = 0; w < THREADS / 32; w++) tot = __fadd_rn(tot, s_part[w]);
+        for (int w = 0; w < kPrThreads / 32; w++) tot = __fadd_rn(tot, s_part[w]);
         pr_update(v, tot, pr, out_degree, contrib_next, p, err, active);
       }
       __syncthreads();
     }
   }
-  pr_block_finish<THREADS>(err, active, ctl, it);
+  pr_block_finish(err, active, ctl, it);
 }
 
-// Push scatter: contrib of each source added to its out-neighbours.
-template <int THREADS>
-__global__ void __launch_bounds__(THREADS) pr_push_scatter_kernel(
-    const uint32_t* __restrict__ bins, uint32_t n_thread, uint32_t n_warp, uint32_t n_cta, uint32_t nb_thread,
-    uint32_t nb_warp, const uint2* __restrict__ rows, const uint32_t* __restrict__ nbr,
+// Push scatter: contrib of each source added to its out-neighbours, split by
+// out-degree like the pull gather.
+__global__ void __launch_bounds__(kPrThreads) pr_push_scatter_kernel(
+    uint32_t nb_light, uint32_t nb_warp, const uint32_t* __restrict__ heavy, uint32_t n_warp, uint32_t n_cta,
+    uint32_t V, uint32_t warp_thr, const uint2* __restrict__ rows, const uint32_t* __restrict__ nbr,
     const float* __restrict__ contrib, float* __restrict__ next, const PrCtl* __restrict__ ctl) {
   if (ctl->stop) return;
   const uint32_t b = blockIdx.x;
-  if (b < nb_thread) {
-    for (uint32_t t = b * THREADS + threadIdx.x; t < n_thread; t += nb_thread * THREADS) {
-      const uint32_t v = bins[t];
+  if (b < nb_light) {
+    for (uint32_t v = b * kPrThreads + threadIdx.x; v < V; v += nb_light * kPrThreads) {
       const uint2 row = rows[v];
+      if (row.y > warp_thr) continue;
       const float c = contrib[v];
       for (uint32_t j = row.x; j < row.x + row.y; j++) atomicAdd(&next[nbr[j] & 0x3FFFFFFFu], c);
     }
-  } else if (b < nb_thread + nb_warp) {
-    const uint32_t lane = lane_id();
-    const uint32_t w0 = (b - nb_thread) * (THREADS / 32) + (threadIdx.x >> 5);
-    const uint32_t wstride = nb_warp * (THREADS / 32);
+  } else if (b < nb_light + nb_warp) {
+    const uint32_t w0 = (b - nb_light) * (kPrThreads / 32) + (threadIdx.x >> 5);
+    const uint32_t wstride = nb_warp * (kPrThreads / 32);
     for (uint32_t t = w0; t < n_warp; t += wstride) {
-      const uint32_t v = bins[n_thread + t];
+      const uint32_t v = heavy[t];
       const uint2 row = rows[v];
       const float c = contrib[v];
-      for (uint32_t j = row.x + lane; j < row.x + row.y; j += 32) atomicAdd(&next[nbr[j] & 0x3FFFFFFFu], c);
+      for (uint32_t j = row.x + lane_id(); j < row.x + row.y; j += 32) atomicAdd(&next[nbr[j] & 0x3FFFFFFFu], c);
     }
   } else {
-    const uint32_t cb = b - nb_thread - nb_warp;
-    const uint32_t ncb = gridDim.x - nb_thread - nb_warp;
+    const uint32_t cb = b - nb_light - nb_warp;
+    const uint32_t ncb = gridDim.x - nb_light - nb_warp;
     for (uint32_t t = cb; t < n_cta; t += ncb) {
-      const uint32_t v = bins[n_thread + n_warp + t];
+      const uint32_t v = heavy[n_warp + t];
       const uint2 row = rows[v];
       const float c = contrib[v];
-      for (uint32_t j = row.x + threadIdx.x; j < row.x + row.y; j += THREADS) atomicAdd(&next[nbr[j] & 0x3FFFFFFFu], c);
+      for (uint32_t j = row.x + threadIdx.x; j < row.x + row.y; j += kPrThreads)
+        atomicAdd(&next[nbr[j] & 0x3FFFFFFFu], c);
     }
   }
 }
 
-template <int THREADS>
-__global__ void __launch_bounds__(THREADS) pr_push_update_kernel(uint32_t V, const uint32_t* __restrict__ out_degree,
-                                                                 float* __restrict__ next,
-                                                                 float* __restrict__ contrib_next,
-                                                                 float* __restrict__ pr, PrParams p,
-                                                                 PrCtl* __restrict__ ctl, uint32_t it) {
+__global__ void __launch_bounds__(kPrThreads) pr_push_update_kernel(uint32_t V, const uint32_t* __restrict__ out_degree,
+                                                                    float* __restrict__ next,
+                                                                    float* __restrict__ contrib_next,
+                                                                    float* __restrict__ pr, PrParams p,
+                                                                    PrCtl* __restrict__ ctl, uint32_t it) {
   if (ctl->stop) return;
   double err = 0.0;
   uint32_t active = 0;
-  for (uint32_t v = blockIdx.x * THREADS + threadIdx.x; v < V; v += gridDim.x * THREADS) {
+  for (uint32_t v = blockIdx.x * kPrThreads + threadIdx.x; v < V; v += gridDim.x * kPrThreads) {
     const float s = next[v];
     next[v] = 0.0f;
     pr_update(v, s, pr, out_degree, contrib_next, p, err, active);
   }
-  pr_block_finish<THREADS>(err, active, ctl, it);
+  pr_block_finish(err, active, ctl, it);
 }
 
 __global__ void pr_init_kernel(uint32_t V, const uint32_t* __restrict__ out_degree, const float* __restrict__ init,
@@ -275,10 +304,10 @@ static int pr_work_get(DevGraph& g, bool pull, PrWork** out, cudaStream_t s) {
     OGB_TRY(w->contrib0.alloc((size_t)V * 4 + 16));
     OGB_TRY(w->contrib1.alloc((size_t)V * 4 + 16));
     OGB_TRY(w->next.alloc((size_t)V * 4 + 16));
-    OGB_TRY(w->bins.alloc((size_t)V * 4 + 16));
-    OGB_TRY(w->ctl.alloc(sizeof(PrCtl)));
+    OGB_TRY(w->heavy.alloc((size_t)V * 4 + 16));
+    OGB_TRY(w->ctl.alloc(sizeof(PrCtl) + 64));
     w->V = V;
-    w->binned_for_pull = -1;
+    w->listed_pull = -1;
   }
   if (!w->h_ctl) OGB_CUDA(cudaMallocHost(&w->h_ctl, sizeof(PrCtl)));
   if (!w->ev0) {
@@ -286,26 +315,24 @@ static int pr_work_get(DevGraph& g, bool pull, PrWork** out, cudaStream_t s) {
     OGB_CUDA(cudaEventCreate(&w->ev1));
   }
   const int want = pull ? 1 : 0;
-  if (w->binned_for_pull != want) {
+  if (w->listed_pull != want || w->listed_warp != g_warp_thr || w->listed_cta != g_cta_thr) {
     const uint2* rows = pull ? g.inv.d_rows() : g.fwd.d_rows();
-    uint32_t* d_cnt = reinterpret_cast<uint32_t*>(w->h_ctl);  // reuse pinned memory as scratch
-    DevBuf cnt;
-    OGB_TRY(cnt.alloc(32));
-    OGB_CUDA(cudaMemsetAsync(cnt.p, 0, 32, s));
+    uint32_t* cnt = w->ctl.as<uint32_t>() + sizeof(PrCtl) / 4;  // 16 scratch words after the control block
+    OGB_CUDA(cudaMemsetAsync(cnt, 0, 16, s));
     const int grid = sm_count() * 8;
-    pr_bin_count_kernel<<<grid, 256, 0, s>>>(V, rows, cnt.as<uint32_t>());
+    pr_heavy_count_kernel<<<grid, 256, 0, s>>>(V, rows, g_warp_thr, g_cta_thr, cnt);
     OGB_CUDA(cudaGetLastError());
-    OGB_CUDA(cudaMemcpyAsync(d_cnt, cnt.p, 12, cudaMemcpyDeviceToHost, s));
+    OGB_CUDA(cudaMemcpyAsync(w->h_ctl, cnt, 8, cudaMemcpyDeviceToHost, s));
     OGB_CUDA(cudaStreamSynchronize(s));
-    w->n_thread = d_cnt[0];
-    w->n_warp = d_cnt[1];
-    w->n_cta = d_cnt[2];
-    OGB_CUDA(cudaMemsetAsync(cnt.p, 0, 32, s));
-    pr_bin_fill_kernel<<<grid, 256, 0, s>>>(V, rows, cnt.as<uint32_t>(), w->bins.as<uint32_t>(), w->n_thread,
-                                            w->n_thread + w->n_warp);
+    w->n_warp = reinterpret_cast<uint32_t*>(w->h_ctl)[0];
+    w->n_cta = reinterpret_cast<uint32_t*>(w->h_ctl)[1];
+    OGB_CUDA(cudaMemsetAsync(cnt, 0, 16, s));
+    pr_heavy_fill_kernel<<<grid, 256, 0, s>>>(V, rows, g_warp_thr, g_cta_thr, cnt, w->heavy.as<uint32_t>(),
+                                              w->n_warp);
     OGB_CUDA(cudaGetLastError());
-    OGB_CUDA(cudaStreamSynchronize(s));
-    w->binned_for_pull = want;
+    w->listed_pull = want;
+    w->listed_warp = g_warp_thr;
+    w->listed_cta = g_cta_thr;
   }
   *out = w;
   return OK;
@@ -319,14 +346,14 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
   const bool pull = mode == PR_PULL;
   PrWork* w = nullptr;
   OGB_TRY(pr_work_get(g, pull, &w, s));
-  constexpr int T = 256;
+  constexpr int T = kPrThreads;
   const int sms = sm_count();
   PrParams p;
   p.damp = 0.85f;
   p.base_pr = 1.0f - p.damp;
   p.epsilon = epsilon;
-  p.inv_v = 0.0;
   p.V = V;
+  p.warp_thr = g_warp_thr;
   PrCtl* d_ctl = w->ctl.as<PrCtl>();
   OGB_CUDA(cudaMemsetAsync(d_ctl, 0, sizeof(PrCtl), s));
   float* c_cur = w->contrib0.as<float>();
@@ -335,24 +362,23 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
   pr_init_kernel<<<sms * 8, 256, 0, s>>>(V, g.fwd.d_out_degree(), init, p.base_pr, ranks, c_cur, pull ? nullptr : nxt);
   OGB_CUDA(cudaGetLastError());
 
-  // grid split between the bins (roughly by work)
-  const uint32_t nb_thread = std::max<uint32_t>(1, std::min<uint32_t>(sms * 8, ceil_div(w->n_thread, T)));
+  const uint32_t nb_light = std::max<uint32_t>(1, std::min<uint32_t>(sms * 8, ceil_div(V, T)));
   const uint32_t nb_warp = w->n_warp ? std::max<uint32_t>(1, std::min<uint32_t>(sms * 8, ceil_div(w->n_warp, T / 32))) : 0;
   const uint32_t nb_cta = w->n_cta ? std::min<uint32_t>(sms * 2, w->n_cta) : 0;
-  const uint32_t grid = nb_thread + nb_warp + nb_cta;
+  const uint32_t grid = nb_light + nb_warp + nb_cta;
   const uint2* rows = pull ? g.inv.d_rows() : g.fwd.d_rows();
   const uint32_t* nbr = pull ? g.inv.d_dst() : g.fwd.d_dst();
-  const uint32_t* bins = w->bins.as<uint32_t>();
+  const uint32_t* heavy = w->heavy.as<uint32_t>();
 
   OGB_CUDA(cudaEventRecord(w->ev0, s));
   for (uint32_t it = 0; it < max_iters; it++) {
     if (pull) {
-      pr_pull_kernel<T><<<grid, T, 0, s>>>(bins, w->n_thread, w->n_warp, w->n_cta, nb_thread, nb_warp, rows, nbr,
-                                           g.fwd.d_out_degree(), c_cur, c_nxt, ranks, p, d_ctl, it);
+      pr_pull_kernel<<<grid, T, 0, s>>>(nb_light, nb_warp, heavy, w->n_warp, w->n_cta, rows, nbr,
+                                         g.fwd.d_out_degree(), c_cur, c_nxt, ranks, p, d_ctl, it);
     } else {
-      pr_push_scatter_kernel<T><<<grid, T, 0, s>>>(bins, w->n_thread, w->n_warp, w->n_cta, nb_thread, nb_warp, rows,
-                                                   nbr, c_cur, nxt, d_ctl);
-      pr_push_update_kernel<T><<<sms * 8, T, 0, s>>>(V, g.fwd.d_out_degree(), nxt, c_nxt, ranks, p, d_ctl, it);
+      pr_push_scatter_kernel<<<grid, T, 0, s>>>(nb_light, nb_warp, heavy, w->n_warp, w->n_cta, V, g_warp_thr, rows,
+                                                 nbr, c_cur, nxt, d_ctl);
+      pr_push_update_kernel<<<sms * 8, T, 0, s>>>(V, g.fwd.d_out_degree(), nxt, c_nxt, ranks, p, d_ctl, it);
     }
     OGB_CUDA(cudaGetLastError());
     std::swap(c_cur, c_nxt);

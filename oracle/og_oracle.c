@@ -216,6 +216,45 @@ int orc_bfs(uint32_t V, uint32_t E, const uint32_t *f_outdeg, const uint32_t *f_
 
 /* -------------------------------------------------------------- PageRank -- */
 
+/* Reduction order of the GPU pull kernel (mode 2 of orc_pagerank): rows with
+ * in-degree <= warp_thr are summed sequentially; rows above it by 32 lanes
+ * (lane l sums edges l, l+32, ... in order) folded by the butterfly
+ * s_l + s_(l^o), o = 16..1; rows above cta_thr by cta_threads threads, each
+ * warp folded the same way, then the warp results summed in warp order. */
+static uint32_t g_warp_thr = 32, g_cta_thr = 2048, g_cta_threads = 256;
+
+void orc_set_gpu_order(uint32_t warp_thr, uint32_t cta_thr, uint32_t cta_threads)
+{
+    g_warp_thr = warp_thr;
+    g_cta_thr = cta_thr;
+    g_cta_threads = cta_threads;
+}
+
+static float tree_sum(const float *c, const uint32_t *nbr, uint32_t a, uint32_t d, uint32_t T)
+{
+    float part[1024];
+    for (uint32_t t = 0; t < T; t++)
+    {
+        float s = 0.0f;
+        for (uint32_t j = a + t; j < a + d; j += T) s += c[nbr[j] & 0x3FFFFFFFu];
+        part[t] = s;
+    }
+    for (uint32_t w = 0; w < T / 32; w++)
+    {
+        float *p = part + w * 32;
+        for (uint32_t o = 16; o; o >>= 1)
+        {
+            float q[32];
+            for (uint32_t l = 0; l < 32; l++) q[l] = p[l] + p[l ^ o];
+            memcpy(p, q, sizeof(q));
+        }
+    }
+    if (T == 32) return part[0];
+    float tot = 0.0f;
+    for (uint32_t w = 0; w < T / 32; w++) tot += part[w * 32];
+    return tot;
+}
+
 uint32_t orc_pagerank(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_idx, const uint32_t *f_dst,
                       const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, int mode,
                       uint32_t max_iters, double epsilon, const float *init, float *pr,
@@ -240,6 +279,23 @@ uint32_t orc_pagerank(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_id
                 float s = 0.0f;
                 for (uint32_t j = i_idx[v]; j < i_idx[v] + i_outdeg[v]; j++) s += contrib[i_dst[j] & 0x3FFFFFFFu];
                 next[v] = s;
+            }
+        }
+        else if (mode == 2)
+        {
+            for (uint32_t v = 0; v < V; v++)
+            {
+                const uint32_t d = i_outdeg[v];
+                if (d > g_cta_thr)
+                    next[v] = tree_sum(contrib, i_dst, i_idx[v], d, g_cta_threads);
+                else if (d > g_warp_thr)
+                    next[v] = tree_sum(contrib, i_dst, i_idx[v], d, 32);
+                else
+                {
+                    float s = 0.0f;
+                    for (uint32_t j = i_idx[v]; j < i_idx[v] + d; j++) s += contrib[i_dst[j] & 0x3FFFFFFFu];
+                    next[v] = s;
+                }
             }
         }
         else

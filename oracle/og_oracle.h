@@ -62,7 +62,8 @@ int orc_bfs(uint32_t V, uint32_t E, const uint32_t *f_outdeg, const uint32_t *f_
             uint32_t max_dirs);
 
 /* PageRank fp32 (pageRank.c:939-1186): mode 0 pull (sequential sums in CSR
- * order), 1 push (sequential scatter in vertex order).  init (may be NULL)
+ * order), 1 push (sequential scatter in vertex order), 2 pull in the GPU
+ * kernel's reduction order (orc_set_gpu_order).  init (may be NULL)
  * replaces the start 1-0.85f.  ranks receives the normalized ranks;
  * err_hist/active_hist (may be NULL) one entry per executed iteration.
  * Returns the number of executed iterations. */
@@ -70,6 +71,10 @@ uint32_t orc_pagerank(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_id
                       const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, int mode,
                       uint32_t max_iters, double epsilon, const float *init, float *ranks,
                       uint32_t *iterations_out, double *error_out, double *err_hist, uint32_t *active_hist);
+
+/* mode 2 of orc_pagerank: pull with the GPU kernel's reduction order for
+ * rows above the given in-degree thresholds (see og_oracle.c). */
+void orc_set_gpu_order(uint32_t warp_thr, uint32_t cta_thr, uint32_t cta_threads);
 
 /* The same pull iteration in double precision throughout (the FP64 oracle the
  * fp32 error is stated against).  Runs exactly `iters` iterations. */
