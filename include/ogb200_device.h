@@ -125,6 +125,29 @@ void ogb_pagerank_get_bins(uint32_t *warp_thr, uint32_t *cta_thr, uint32_t *cta_
 /* Per-iteration L1 error and active count of the last ogb_pagerank on g. */
 int ogb_pagerank_history(ogb_graph *g, double *errors, uint32_t *active, uint32_t max_entries, uint32_t *count);
 
+/* No counterpart in the reference.  PageRank pull that allocates no memory,
+ * for callers that cannot allocate device memory when they need the result:
+ * another allocator or pool owns the device memory, or their request path
+ * must not call cudaMalloc (it synchronizes the device and can fail when
+ * memory is fragmented).  All scratch is one fixed __device__ array inside
+ * the library, about 12.6 MB held on every GPU that loads the library until
+ * the process exits; so num_vertices is limited to OGB_NOALLOC_MAX_VERTICES
+ * and a larger graph is rejected with OGB_ERR_RANGE.
+ * Inputs (device arrays): the inverse CSR -- row starts d_in_edges_idx,
+ * in-degrees d_in_degree, in-neighbour ids d_in_neighbors -- and the forward
+ * out-degrees.  Outputs: d_ranks (V normalized ranks) and, if d_info is not
+ * NULL, a DEVICE ogb_pr_info (ms and launches are 0).  Same semantics, work
+ * split and summation order as ogb_pagerank pull at its default thresholds.
+ * The work is enqueued on `stream` (NULL = the default stream) and the call
+ * returns without waiting.  The first call on each device looks up the
+ * scratch address: make that first call before any stream capture.  Every
+ * call shares the one scratch array and overwrites what the last call left
+ * in it, so calls that overlap on the GPU race with each other. */
+#define OGB_NOALLOC_MAX_VERTICES (1u << 20)
+int ogb_pagerank_pull_noalloc(uint32_t num_vertices, const uint32_t *d_in_edges_idx, const uint32_t *d_in_degree,
+                              const uint32_t *d_in_neighbors, const uint32_t *d_out_degree, uint32_t max_iterations,
+                              double epsilon, float *d_ranks, ogb_pr_info *d_info, void *stream);
+
 /* ---- synthetic inputs (host, multi-threaded, deterministic) ------------- */
 
 /* RMAT (a, b, c; d = 1-a-b-c) with 2^scale vertices and edge_factor*2^scale
