@@ -121,7 +121,7 @@ int ogb_pagerank(ogb_graph *g, uint32_t mode, uint32_t max_iterations, double ep
  * order), longer rows by a warp, rows above cta_thr by a CTA of cta_threads
  * threads (fixed-order butterfly sums).  Defaults 32 / 2048 / 256. */
 void ogb_pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr);
-void ogb_pagerank_get_bins(uint32_t *warp_thr, uint32_t *cta_thr, uint32_t *cta_threads);
+void ogb_pagerank_get_bins(uint32_t *warp_thr, uint32_t *cta_thr, uint32_t *cta_threads, uint32_t *chunk_edges);
 /* Per-iteration L1 error and active count of the last ogb_pagerank on g. */
 int ogb_pagerank_history(ogb_graph *g, double *errors, uint32_t *active, uint32_t max_entries, uint32_t *count);
 

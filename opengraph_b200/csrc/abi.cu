@@ -1284,8 +1284,9 @@ extern "C" int ogb_pagerank(ogb_graph* g, uint32_t mode, uint32_t max_iters, dou
 
 extern "C" void ogb_pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr) { pagerank_set_bins(warp_thr, cta_thr); }
 
-extern "C" void ogb_pagerank_get_bins(uint32_t* warp_thr, uint32_t* cta_thr, uint32_t* cta_threads) {
-  pagerank_get_bins(warp_thr, cta_thr, cta_threads);
+extern "C" void ogb_pagerank_get_bins(uint32_t* warp_thr, uint32_t* cta_thr, uint32_t* cta_threads,
+                                      uint32_t* chunk_edges) {
+  pagerank_get_bins(warp_thr, cta_thr, cta_threads, chunk_edges);
 }
 
 extern "C" int ogb_pagerank_history(ogb_graph* g, double* errors, uint32_t* active, uint32_t max_entries,

@@ -63,7 +63,7 @@ struct BfsCtl {
   unsigned long long edges;  // edges examined
   unsigned long long reached_edges;
   uint32_t reached;
-  uint32_t pad;
+  uint32_t all_count;        // host-state step: entries written to all_out
 };
 
 struct BfsWork {
@@ -239,9 +239,12 @@ __global__ void __launch_bounds__(kExpT) bfs_td_expand_kernel(
     uint32_t* __restrict__ distances, uint32_t* __restrict__ next_list, uint32_t* __restrict__ all_out,
     BfsCtl* __restrict__ ctl) {
   __shared__ uint32_t s_off[kExpTile + 2], s_start[kExpTile + 2], s_v[kExpTile + 2], s_d[kExpTile + 2];
+  __shared__ BlockAppend<kExpTile> q_list, q_all;
+  ba_init(q_list);
+  ba_init(q_all);
   const uint32_t total = ctl->total_edges;
   const uint32_t ntiles = (total + kExpTile - 1) / kExpTile;
-  uint32_t mf = 0;
+  uint32_t mf = 0, found = 0;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const uint32_t e0 = t * kExpTile;
     const uint32_t e1 = min(e0 + kExpTile, total);
@@ -270,13 +273,17 @@ __global__ void __launch_bounds__(kExpT) bfs_td_expand_kernel(
       if (p < 0 && atomicCAS(&parents[u], p, (int32_t)s_v[lo]) == p) {
         distances[u] = s_d[lo];
         mf += (uint32_t)(-p);
-        const uint32_t slot = warp_atomic_inc(&ctl->qnext);
-        if (all_out) all_out[slot] = u;
-        if (out_degree[u]) next_list[warp_atomic_inc(&ctl->lnext)] = u;
+        found++;
+        if (all_out) ba_push(q_all, u);
+        if (out_degree[u]) ba_push(q_list, u);
       }
     }
+    // at most kExpTile discoveries per tile: flush every tile
+    ba_flush(q_list, next_list, &ctl->lnext);
+    if (all_out) ba_flush(q_all, all_out, &ctl->all_count);
   }
   warp_atomic_add_total(&ctl->mf, mf);
+  warp_atomic_add_total(&ctl->qnext, found);
 }
 
 // Keep the entries of a queue that have out-edges (host-state step API).
@@ -302,47 +309,51 @@ __global__ void __launch_bounds__(256) bfs_bu_dense_kernel(uint32_t V, const uin
                                                            uint32_t* __restrict__ distances,
                                                            uint32_t* __restrict__ ul_next,
                                                            BfsCtl* __restrict__ ctl) {
-  const uint32_t lane = lane_id();
-  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  constexpr uint32_t kRound = 1024;  // vertices per block round (4 bitmap words per warp)
+  __shared__ BlockAppend<2 * kRound> q_ul;
+  ba_init(q_ul);
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
   uint32_t nf = 0;
   unsigned long long edges = 0;
-  for (uint32_t base = gwarp * 32; base < V; base += nwarps * 32) {
-    const uint32_t v = base + lane;
-    bool found = false;
-    bool unvisited = false;
-    if (v < V && parents[v] < 0) {
-      const uint2 row = rows[v];
-      uint32_t j = row.x;
-      const uint32_t end = row.x + row.y;
-      for (; j < end; j++) {
-        const uint32_t u = nbr[j] & 0x3FFFFFFFu;
-        if ((bm_cur[u >> 5] >> (u & 31)) & 1u) {
-          parents[v] = (int32_t)u;
-          distances[v] = distances[u] + 1;
-          found = true;
-          j++;
-          break;
+  for (uint32_t rbase = blockIdx.x * kRound; rbase < V; rbase += gridDim.x * kRound) {
+#pragma unroll
+    for (uint32_t k = 0; k < kRound / 256; k++) {
+      const uint32_t base = rbase + k * 256 + warp * 32;
+      const uint32_t v = base + lane;
+      bool found = false;
+      bool unvisited = false;
+      if (v < V && parents[v] < 0) {
+        const uint2 row = rows[v];
+        uint32_t j = row.x;
+        const uint32_t end = row.x + row.y;
+        for (; j < end; j++) {
+          const uint32_t u = nbr[j] & 0x3FFFFFFFu;
+          if ((bm_cur[u >> 5] >> (u & 31)) & 1u) {
+            parents[v] = (int32_t)u;
+            distances[v] = distances[u] + 1;
+            found = true;
+            j++;
+            break;
+          }
         }
+        edges += j - row.x;
+        unvisited = !found;
       }
-      edges += j - row.x;
-      unvisited = !found;
+      const uint32_t word = __ballot_sync(0xffffffffu, found);
+      if (lane == 0 && base < V) {
+        if (OR_INTO)
+          bm_next[base >> 5] |= word;
+        else
+          bm_next[base >> 5] = word;
+      }
+      nf += found;
+      if (unvisited) ba_push(q_ul, v);
     }
-    const uint32_t word = __ballot_sync(0xffffffffu, found);
-    if (lane == 0) {
-      if (OR_INTO)
-        bm_next[base >> 5] |= word;
-      else
-        bm_next[base >> 5] = word;
-    }
-    nf += found;
-    if (unvisited) ul_next[warp_atomic_inc(&ctl->ul_size)] = v;
+    if (ba_size(q_ul) > kRound) ba_flush(q_ul, ul_next, &ctl->ul_size);
   }
-  nf = __reduce_add_sync(0xffffffffu, nf);
-  if (lane == 0) {
-    if (nf) atomicAdd(&ctl->nf, nf);
-    if (edges) atomicAdd(&ctl->edges, edges);
-  }
+  ba_flush(q_ul, ul_next, &ctl->ul_size);
+  warp_atomic_add_total(&ctl->nf, nf);
+  warp_atomic_add_total64(&ctl->edges, (uint32_t)edges);
 }
 
 // One bottom-up level over the unvisited list (bm_next must be cleared).
@@ -355,33 +366,43 @@ __global__ void __launch_bounds__(256) bfs_bu_list_kernel(const uint32_t* __rest
                                                           uint32_t* __restrict__ distances,
                                                           uint32_t* __restrict__ ul_next,
                                                           BfsCtl* __restrict__ ctl) {
+  constexpr uint32_t kRound = 1024;  // list entries per block round
+  __shared__ BlockAppend<2 * kRound> q_ul;
+  ba_init(q_ul);
   uint32_t nf = 0;
   unsigned long long edges = 0;
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
-    const uint32_t v = list[t];
-    if (parents[v] >= 0) continue;  // visited by a top-down step since the list was made
-    const uint2 row = rows[v];
-    uint32_t j = row.x;
-    const uint32_t end = row.x + row.y;
-    bool found = false;
-    for (; j < end; j++) {
-      const uint32_t u = nbr[j] & 0x3FFFFFFFu;
-      if ((bm_cur[u >> 5] >> (u & 31)) & 1u) {
-        parents[v] = (int32_t)u;
-        distances[v] = distances[u] + 1;
-        found = true;
-        j++;
-        break;
+  for (uint32_t rbase = blockIdx.x * kRound; rbase < count; rbase += gridDim.x * kRound) {
+#pragma unroll
+    for (uint32_t k = 0; k < kRound / 256; k++) {
+      const uint32_t t = rbase + k * 256 + threadIdx.x;
+      if (t >= count) continue;
+      const uint32_t v = list[t];
+      if (parents[v] >= 0) continue;  // visited by a top-down step since the list was made
+      const uint2 row = rows[v];
+      uint32_t j = row.x;
+      const uint32_t end = row.x + row.y;
+      bool found = false;
+      for (; j < end; j++) {
+        const uint32_t u = nbr[j] & 0x3FFFFFFFu;
+        if ((bm_cur[u >> 5] >> (u & 31)) & 1u) {
+          parents[v] = (int32_t)u;
+          distances[v] = distances[u] + 1;
+          found = true;
+          j++;
+          break;
+        }
+      }
+      edges += j - row.x;
+      if (found) {
+        atomicOr(&bm_next[v >> 5], 1u << (v & 31));
+        nf++;
+      } else {
+        ba_push(q_ul, v);
       }
     }
-    edges += j - row.x;
-    if (found) {
-      atomicOr(&bm_next[v >> 5], 1u << (v & 31));
-      nf++;
-    } else {
-      ul_next[warp_atomic_inc(&ctl->ul_size)] = v;
-    }
+    if (ba_size(q_ul) > kRound) ba_flush(q_ul, ul_next, &ctl->ul_size);
   }
+  ba_flush(q_ul, ul_next, &ctl->ul_size);
   warp_atomic_add_total(&ctl->nf, nf);
   warp_atomic_add_total64(&ctl->edges, (uint32_t)edges);
 }
@@ -401,21 +422,25 @@ __global__ void __launch_bounds__(256) bfs_bitmap_to_list_kernel(const uint32_t*
                                                                  const uint32_t* __restrict__ out_degree,
                                                                  uint32_t* __restrict__ list,
                                                                  BfsCtl* __restrict__ ctl) {
-  const uint32_t lane = lane_id();
-  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  constexpr uint32_t kRoundWords = 128;  // bitmap words per block round (<= 4096 bits)
+  __shared__ BlockAppend<2 * kRoundWords * 32> q;
+  ba_init(q);
   uint32_t cnt = 0;
-  for (uint32_t base = gwarp * 32; base < words; base += nwarps * 32) {
-    const uint32_t w = base + lane;
-    uint32_t word = (w < words) ? bm[w] : 0u;
-    cnt += __popc(word);
-    while (word) {
-      const int bit = __ffs(word) - 1;
-      const uint32_t v = w * 32 + (uint32_t)bit;
-      if (out_degree[v]) list[warp_atomic_inc(&ctl->lnext)] = v;
-      word &= word - 1;
+  for (uint32_t rbase = blockIdx.x * kRoundWords; rbase < words; rbase += gridDim.x * kRoundWords) {
+    const uint32_t w = rbase + threadIdx.x;
+    if (threadIdx.x < kRoundWords && w < words) {
+      uint32_t word = bm[w];
+      cnt += __popc(word);
+      while (word) {
+        const int bit = __ffs(word) - 1;
+        const uint32_t v = w * 32 + (uint32_t)bit;
+        if (out_degree[v]) ba_push(q, v);
+        word &= word - 1;
+      }
     }
+    if (ba_size(q) > kRoundWords * 32) ba_flush(q, list, &ctl->lnext);
   }
+  ba_flush(q, list, &ctl->lnext);
   warp_atomic_add_total(&ctl->qnext, cnt);
 }
 

@@ -130,6 +130,51 @@ __device__ __forceinline__ uint32_t warp_atomic_inc(uint32_t* ctr) {
   return base + __popc(active & lanemask_lt());
 }
 
+// Block-level append buffer: items pushed by any thread of a block are staged
+// in shared memory and written out with ONE global atomic per flush, instead
+// of one atomic per warp on a counter every block shares.
+template <int CAP>
+struct BlockAppend {
+  uint32_t n;     // staged items
+  uint32_t base;  // global offset of the flush in progress
+  uint32_t buf[CAP];
+};
+
+template <int CAP>
+__device__ __forceinline__ void ba_init(BlockAppend<CAP>& q) {
+  if (threadIdx.x == 0) q.n = 0;
+  __syncthreads();
+}
+
+// Any thread, any divergence; the caller keeps n + pushes <= CAP.
+template <int CAP>
+__device__ __forceinline__ void ba_push(BlockAppend<CAP>& q, uint32_t x) {
+  q.buf[warp_atomic_inc(&q.n)] = x;
+}
+
+// Staged count, uniform over the block (call from block-uniform code).
+template <int CAP>
+__device__ __forceinline__ uint32_t ba_size(BlockAppend<CAP>& q) {
+  __syncthreads();
+  const uint32_t n = q.n;
+  __syncthreads();
+  return n;
+}
+
+// Every thread of the block calls it: appends the staged items to out[] at
+// an offset reserved from *count, then empties the buffer.
+template <int CAP>
+__device__ __forceinline__ void ba_flush(BlockAppend<CAP>& q, uint32_t* out, uint32_t* count) {
+  __syncthreads();
+  const uint32_t n = q.n;
+  if (threadIdx.x == 0 && n) q.base = atomicAdd(count, n);
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) out[q.base + k] = q.buf[k];
+  __syncthreads();
+  if (threadIdx.x == 0) q.n = 0;
+  __syncthreads();
+}
+
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
 
 }  // namespace ogb

@@ -144,6 +144,6 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
 // Row-length thresholds of the PageRank work split (light rows per thread,
 // heavy rows per warp, very heavy rows per CTA of cta_threads threads).
 void pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr);
-void pagerank_get_bins(uint32_t* warp_thr, uint32_t* cta_thr, uint32_t* cta_threads);
+void pagerank_get_bins(uint32_t* warp_thr, uint32_t* cta_thr, uint32_t* cta_threads, uint32_t* chunk);
 
 }  // namespace ogb

@@ -219,15 +219,18 @@ int orc_bfs(uint32_t V, uint32_t E, const uint32_t *f_outdeg, const uint32_t *f_
 /* Reduction order of the GPU pull kernel (mode 2 of orc_pagerank): rows with
  * in-degree <= warp_thr are summed sequentially; rows above it by 32 lanes
  * (lane l sums edges l, l+32, ... in order) folded by the butterfly
- * s_l + s_(l^o), o = 16..1; rows above cta_thr by cta_threads threads, each
- * warp folded the same way, then the warp results summed in warp order. */
-static uint32_t g_warp_thr = 32, g_cta_thr = 2048, g_cta_threads = 256;
+ * s_l + s_(l^o), o = 16..1; rows above cta_thr are cut into chunks of `chunk`
+ * edges, each chunk summed by cta_threads threads (each warp folded the same
+ * way, then the warp results summed in warp order), and the chunk sums added
+ * in chunk order. */
+static uint32_t g_warp_thr = 32, g_cta_thr = 2048, g_cta_threads = 256, g_chunk = 8192;
 
-void orc_set_gpu_order(uint32_t warp_thr, uint32_t cta_thr, uint32_t cta_threads)
+void orc_set_gpu_order(uint32_t warp_thr, uint32_t cta_thr, uint32_t cta_threads, uint32_t chunk)
 {
     g_warp_thr = warp_thr;
     g_cta_thr = cta_thr;
     g_cta_threads = cta_threads;
+    g_chunk = chunk ? chunk : 0xFFFFFFFFu;
 }
 
 static float tree_sum(const float *c, const uint32_t *nbr, uint32_t a, uint32_t d, uint32_t T)
@@ -287,7 +290,15 @@ uint32_t orc_pagerank(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_id
             {
                 const uint32_t d = i_outdeg[v];
                 if (d > g_cta_thr)
-                    next[v] = tree_sum(contrib, i_dst, i_idx[v], d, g_cta_threads);
+                {
+                    float tot = 0.0f;
+                    for (uint32_t c = 0; c < d; c += g_chunk)
+                    {
+                        const uint32_t len = (d - c < g_chunk) ? d - c : g_chunk;
+                        tot += tree_sum(contrib, i_dst, i_idx[v] + c, len, g_cta_threads);
+                    }
+                    next[v] = tot;
+                }
                 else if (d > g_warp_thr)
                     next[v] = tree_sum(contrib, i_dst, i_idx[v], d, 32);
                 else

@@ -74,7 +74,7 @@ uint32_t orc_pagerank(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_id
 
 /* mode 2 of orc_pagerank: pull with the GPU kernel's reduction order for
  * rows above the given in-degree thresholds (see og_oracle.c). */
-void orc_set_gpu_order(uint32_t warp_thr, uint32_t cta_thr, uint32_t cta_threads);
+void orc_set_gpu_order(uint32_t warp_thr, uint32_t cta_thr, uint32_t cta_threads, uint32_t chunk);
 
 /* The same pull iteration in double precision throughout (the FP64 oracle the
  * fp32 error is stated against).  Runs exactly `iters` iterations. */

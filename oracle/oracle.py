@@ -62,11 +62,12 @@ class Oracle:
         d.orc_pagerank.restype = u32
         d.orc_pagerank_f64.argtypes = [u32, vp, vp, vp, vp, u32, vp, vp]
         d.orc_random_roots.argtypes = [u32, u32, u32, vp, u32, vp]
-        d.orc_set_gpu_order.argtypes = [u32, u32, u32]
+        d.orc_set_gpu_order.argtypes = [u32, u32, u32, u32]
 
-    def set_gpu_order(self, warp_thr: int = 32, cta_thr: int = 2048, cta_threads: int = 256) -> None:
-        """Reduction order that pagerank(mode=2) emulates (the GPU pull kernel's bins)."""
-        self.d.orc_set_gpu_order(warp_thr, cta_thr, cta_threads)
+    def set_gpu_order(self, warp_thr: int = 32, cta_thr: int = 2048, cta_threads: int = 256,
+                      chunk: int = 8192) -> None:
+        """Reduction order that pagerank(mode=2) emulates (the GPU pull kernel's work split)."""
+        self.d.orc_set_gpu_order(warp_thr, cta_thr, cta_threads, chunk)
 
     def sort(self, src, dst, w=None, mode: int = 0):
         E = len(src)

@@ -43,9 +43,9 @@ IDS = [f"{k}-{i}" for i, (k, _) in enumerate(CASES)]
 
 
 def bins(lib):
-    w, c, t = C.c_uint32(), C.c_uint32(), C.c_uint32()
-    lib.ogb_pagerank_get_bins(C.byref(w), C.byref(c), C.byref(t))
-    return w.value, c.value, t.value
+    w, c, t, k = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+    lib.ogb_pagerank_get_bins(C.byref(w), C.byref(c), C.byref(t), C.byref(k))
+    return w.value, c.value, t.value, k.value
 
 
 @pytest.fixture
