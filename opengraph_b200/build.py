@@ -24,7 +24,7 @@ LAYOUT_SOURCES = ["abi.cu"]  # compiled once per struct layout
 CXX_SOURCES = ["generate.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3,-fopenmp", "--expt-relaxed-constexpr",
               "-I", INCLUDE, "-I", CSRC] + ARCH
 
 LIBS = {"libogb200.so": 0, "libogb200_w.so": 1}
@@ -94,7 +94,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | N
         target = os.path.join(HERE, lib)
         if force or not _newer(target, objs):
             _run([nv, *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fPIC",
-                  "-Xlinker", "-Bsymbolic-functions", "-o", target, *objs, "-lpthread"], verbose)
+                  "-Xlinker", "-Bsymbolic-functions", "-o", target, *objs, "-lgomp", "-lpthread"], verbose)
         out.append(target)
     return out
 

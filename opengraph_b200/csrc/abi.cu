@@ -88,18 +88,19 @@ static void* host_alloc(size_t bytes) {
     if (_st != ::ogb::OK) die_status(#call, _st); \
   } while (0)
 
-// Host <-> device copies of malloc'd (pageable) arrays run through a pinned
-// bounce buffer in chunks, double-buffered, with the host-side memcpy split
-// over threads.
+// Host <-> device copies of malloc'd (pageable) arrays run through pinned
+// bounce buffers: kBufs chunks in flight on the DMA engine while OpenMP
+// threads move the previous chunk between the bounce buffer and the array.
 namespace {
 struct Bounce {
-  static constexpr size_t kChunk = 32u << 20;
-  void* h[2] = {nullptr, nullptr};
-  cudaEvent_t ev[2] = {nullptr, nullptr};
+  static constexpr size_t kChunk = 8u << 20;
+  static constexpr int kBufs = 4;
+  void* h[kBufs] = {};
+  cudaEvent_t ev[kBufs] = {};
   std::mutex mu;
   int init() {
     if (h[0]) return OK;
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < kBufs; i++) {
       OGB_CUDA(cudaMallocHost(&h[i], kChunk));
       OGB_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
     }
@@ -111,22 +112,23 @@ Bounce& bounce() {
   return b;
 }
 
+int host_threads() {
+  static const int n = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+  return n;
+}
+
 void par_memcpy(void* dst, const void* src, size_t n) {
-  const size_t kMin = 4u << 20;
-  unsigned nt = std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
-  if (n < kMin || nt == 1) {
+  const size_t kBlock = 1u << 20;
+  if (n < (2u << 20)) {
     memcpy(dst, src, n);
     return;
   }
-  std::vector<std::thread> th;
-  const size_t chunk = (n + nt - 1) / nt;
-  for (unsigned t = 0; t < nt; t++) {
-    const size_t lo = t * chunk;
-    if (lo >= n) break;
-    const size_t len = std::min(chunk, n - lo);
-    th.emplace_back([=] { memcpy((char*)dst + lo, (const char*)src + lo, len); });
+  const long nb = (long)((n + kBlock - 1) / kBlock);
+#pragma omp parallel for num_threads(host_threads()) schedule(static)
+  for (long b = 0; b < nb; b++) {
+    const size_t lo = (size_t)b * kBlock;
+    memcpy((char*)dst + lo, (const char*)src + lo, std::min(kBlock, n - lo));
   }
-  for (auto& x : th) x.join();
 }
 }  // namespace
 
@@ -139,12 +141,12 @@ static int h2d(void* d, const void* h, size_t n, cudaStream_t s) {
   int i = 0;
   while (off < n) {
     const size_t len = std::min(Bounce::kChunk, n - off);
-    OGB_CUDA(cudaEventSynchronize(b.ev[i]));
+    OGB_CUDA(cudaEventSynchronize(b.ev[i]));  // buffer i free again
     par_memcpy(b.h[i], (const char*)h + off, len);
     OGB_CUDA(cudaMemcpyAsync((char*)d + off, b.h[i], len, cudaMemcpyHostToDevice, s));
     OGB_CUDA(cudaEventRecord(b.ev[i], s));
     off += len;
-    i ^= 1;
+    i = (i + 1) % Bounce::kBufs;
   }
   OGB_CUDA(cudaStreamSynchronize(s));
   return OK;
@@ -155,28 +157,22 @@ static int d2h(void* h, const void* d, size_t n, cudaStream_t s) {
   Bounce& b = bounce();
   std::lock_guard<std::mutex> lk(b.mu);
   OGB_TRY(b.init());
-  // pipeline: copy chunk k+1 on the GPU while the host drains chunk k
-  size_t off = 0, pend_off = 0, pend_len = 0;
-  int i = 0, pend = -1;
-  while (off < n || pend >= 0) {
-    if (off < n) {
-      const size_t len = std::min(Bounce::kChunk, n - off);
-      OGB_CUDA(cudaMemcpyAsync(b.h[i], (const char*)d + off, len, cudaMemcpyDeviceToHost, s));
+  const size_t nchunks = (n + Bounce::kChunk - 1) / Bounce::kChunk;
+  size_t issued = 0;
+  // keep up to kBufs chunks queued on the copy engine, drain in order
+  for (size_t k = 0; k < nchunks; k++) {
+    while (issued < nchunks && issued < k + Bounce::kBufs) {
+      const size_t off = issued * Bounce::kChunk;
+      const int i = (int)(issued % Bounce::kBufs);
+      OGB_CUDA(cudaMemcpyAsync(b.h[i], (const char*)d + off, std::min(Bounce::kChunk, n - off),
+                               cudaMemcpyDeviceToHost, s));
       OGB_CUDA(cudaEventRecord(b.ev[i], s));
-      if (pend >= 0) {
-        OGB_CUDA(cudaEventSynchronize(b.ev[pend]));
-        par_memcpy((char*)h + pend_off, b.h[pend], pend_len);
-      }
-      pend = i;
-      pend_off = off;
-      pend_len = len;
-      off += len;
-      i ^= 1;
-    } else {
-      OGB_CUDA(cudaEventSynchronize(b.ev[pend]));
-      par_memcpy((char*)h + pend_off, b.h[pend], pend_len);
-      pend = -1;
+      issued++;
     }
+    const int i = (int)(k % Bounce::kBufs);
+    const size_t off = k * Bounce::kChunk;
+    OGB_CUDA(cudaEventSynchronize(b.ev[i]));
+    par_memcpy((char*)h + off, b.h[i], std::min(Bounce::kChunk, n - off));
   }
   return OK;
 }
@@ -185,6 +181,7 @@ static int d2h(void* h, const void* d, size_t n, cudaStream_t s) {
 
 struct ogb_graph {
   DevGraph g;
+  DevBuf d_parents, d_distances, d_ranks;  // result arrays of the drop-in calls
 };
 
 namespace {
@@ -900,8 +897,25 @@ extern "C" void graphCSRFree(struct GraphCSR* g) {
 
 // -------------------------------------------------------------------- BFS ---
 
-extern "C" struct BFSStats* newBFSStatsGraphCSR(struct GraphCSR* graph) {
-  const uint32_t V = graph->num_vertices;
+// Run fn(lo, hi) over [0, n) on the OpenMP host threads (as the reference's
+// own parallel loops).
+template <class F>
+static void host_par_for(size_t n, F&& fn) {
+  if (n < (1u << 16)) {
+    fn((size_t)0, n);
+    return;
+  }
+  const long nb = 256;
+  const size_t chunk = (n + nb - 1) / nb;
+#pragma omp parallel for num_threads(host_threads()) schedule(static)
+  for (long b = 0; b < nb; b++) {
+    const size_t lo = (size_t)b * chunk, hi = std::min(n, lo + chunk);
+    if (lo < hi) fn(lo, hi);
+  }
+}
+
+// BFSStats with its four arrays allocated but not initialized.
+static BFSStats* bfs_stats_alloc(uint32_t V) {
   BFSStats* st = (BFSStats*)host_alloc(sizeof(BFSStats));
   st->distances = (uint32_t*)host_alloc((size_t)V * 4);
   st->distances_DualOrder = (uint32_t*)host_alloc((size_t)V * 4);
@@ -911,12 +925,23 @@ extern "C" struct BFSStats* newBFSStatsGraphCSR(struct GraphCSR* graph) {
   st->iteration = 0;
   st->num_vertices = V;
   st->time_total = 0.0;
-  for (uint32_t v = 0; v < V; v++) {
-    st->distances[v] = 0;
-    const uint32_t d = graph->vertices->out_degree[v];
-    st->parents[v] = d ? -(int)d : -1;
-    st->parents_DualOrder[v] = st->parents[v];
-  }
+  return st;
+}
+
+// newBFSStatsGraphCSR (BFS.c:42-78): distances 0, parents (and the DualOrder
+// copy) -out_degree or -1; the reference's parallel loop, on host threads.
+extern "C" struct BFSStats* newBFSStatsGraphCSR(struct GraphCSR* graph) {
+  const uint32_t V = graph->num_vertices;
+  BFSStats* st = bfs_stats_alloc(V);
+  const uint32_t* od = graph->vertices->out_degree;
+  host_par_for(V, [&](size_t lo, size_t hi) {
+    for (size_t v = lo; v < hi; v++) {
+      st->distances[v] = 0;
+      const uint32_t d = od[v];
+      st->parents[v] = d ? -(int)d : -1;
+      st->parents_DualOrder[v] = st->parents[v];
+    }
+  });
   return st;
 }
 
@@ -933,16 +958,26 @@ static BfsResult g_last_bfs;  // level trace of the last drop-in BFS
 
 static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, uint32_t mode, const char* title,
                                    bool bitmap_nf) {
-  BFSStats* st = newBFSStatsGraphCSR(graph);
   const uint32_t V = graph->num_vertices;
   // The reference checks source > V (BFS.c:482); source == V would index
   // past the label array there, so it is rejected here too.
   if (a->source < 0 || (uint32_t)a->source >= V) {
+    BFSStats* st0 = newBFSStatsGraphCSR(graph);
     say(" -----------------------------------------------------\n");
     say("| %-51s | \n", "ERROR!! CHECK SOURCE RANGE");
     say(" -----------------------------------------------------\n");
-    return st;
+    return st0;
   }
+  // parents and distances are overwritten whole by the device result; only
+  // the DualOrder parent copy keeps its initial sentinels (BFS.c:64-73).  It
+  // is filled on host threads while the search runs on the GPU.
+  BFSStats* st = bfs_stats_alloc(V);
+  const uint32_t* od = graph->vertices->out_degree;
+  std::thread fill([st, od, V] {
+    host_par_for(V, [&](size_t lo, size_t hi) {
+      for (size_t v = lo; v < hi; v++) st->parents_DualOrder[v] = od[v] ? -(int)od[v] : -1;
+    });
+  });
   const uint32_t* labels = graph->sorted_edges_array ? graph->sorted_edges_array->label_array : nullptr;
   a->source = labels ? (int)labels[a->source] : a->source;
   say(" -----------------------------------------------------\n");
@@ -954,18 +989,22 @@ static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, 
   say(" -----------------------------------------------------\n");
   int status = OK;
   ogb_graph* dg = mirror_of(graph, &status);
-  if (!dg) die_status("device copy of GraphCSR", status);
+  if (!dg) {
+    fill.join();
+    die_status("device copy of GraphCSR", status);
+  }
   cudaStream_t s = lib_stream();
-  DevBuf d_par, d_dist;
-  OGB_MUST(d_par.alloc((size_t)V * 4 + 4));
-  OGB_MUST(d_dist.alloc((size_t)V * 4 + 4));
+  // device result arrays live with the device copy (no per-call cudaMalloc)
+  OGB_MUST(dg->d_parents.alloc((size_t)V * 4 + 4));
+  OGB_MUST(dg->d_distances.alloc((size_t)V * 4 + 4));
   BfsResult& r = g_last_bfs;
   const double t0 = now_s();
-  OGB_MUST(bfs_run(dg->g, (uint32_t)a->source, mode, d_par.as<int32_t>(), d_dist.as<uint32_t>(), &r, !quiet(),
-                   bitmap_nf, s));
+  OGB_MUST(bfs_run(dg->g, (uint32_t)a->source, mode, dg->d_parents.as<int32_t>(), dg->d_distances.as<uint32_t>(),
+                   &r, !quiet(), bitmap_nf, s));
   const double t_trav = now_s() - t0;
-  OGB_MUST(d2h(st->parents, d_par.p, (size_t)V * 4, s));
-  OGB_MUST(d2h(st->distances, d_dist.p, (size_t)V * 4, s));
+  OGB_MUST(d2h(st->parents, dg->d_parents.p, (size_t)V * 4, s));
+  OGB_MUST(d2h(st->distances, dg->d_distances.p, (size_t)V * 4, s));
+  fill.join();
   st->processed_nodes = r.processed_nodes;
   st->iteration = r.iteration;
   st->time_total = t_trav;

@@ -118,6 +118,24 @@ __device__ __forceinline__ void warp_atomic_add_total64(unsigned long long* ctr,
   if ((int)lane_id() == __ffs(active) - 1) atomicAdd(ctr, (unsigned long long)total);
 }
 
+// Block-aggregated counter add: every thread of the block calls it with its
+// own value (block-uniform call site); thread 0 adds the block total with one
+// atomic, and none when the total is 0.  s_tmp holds one entry per warp.
+template <class T>
+__device__ __forceinline__ void block_add_total(T* ctr, T val, T* s_tmp) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) val += __shfl_down_sync(0xffffffffu, val, o);
+  const uint32_t warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane_id() == 0) s_tmp[warp] = val;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    T t = 0;
+    for (uint32_t i = 0; i < nw; i++) t += s_tmp[i];
+    if (t) atomicAdd(ctr, t);
+  }
+}
+
 // Warp-aggregated increment by 1 (the common case): cheaper than the
 // general version.
 __device__ __forceinline__ uint32_t warp_atomic_inc(uint32_t* ctr) {
