@@ -23,16 +23,16 @@
 //    as in the reference; depths are exact).
 //
 // Device design:
-//  * the whole switch state lives in device memory (BfsDevState) and two
-//    one-thread control kernels apply the reference's rules: `decide` before
-//    a step (termination, direction, conversions) and `finish` after it
-//    (counters, bottom-up continuation).  A search is therefore ONE CUDA
-//    graph: a WHILE node whose body is [IF bitmap->list] decide [IF
-//    list->bitmap] [IF top-down] [IF bottom-up first] [IF bottom-up list]
-//    finish, the IF conditions set by the control kernels.  No host round
-//    trip per level; the loop is bounded (max_steps) so it cannot run away.
-//    A host-stepped driver launches the same kernels one by one (used when
-//    per-level CUDA-event times are wanted);
+//  * a whole search is ONE cooperative launch (bfsk_search): the CTAs run the
+//    level loop together and meet at grid barriers between phases.  Every
+//    CTA keeps its own copy of the switch state in shared memory and updates
+//    it from the same per-phase counters, so all copies agree without an
+//    extra barrier; no host round trip and no launch per level.  Every
+//    barrier wait is bounded (error word, then exit) and the loop is bounded
+//    by V + 8 steps;
+//  * the search is level-synchronous, so every frontier vertex has the same
+//    depth: a discovered vertex gets depth + 1 without reading its parent's
+//    distance (what the reference computes as distances[parent] + 1);
 //  * the frontier is kept twice: its logical size (every vertex discovered
 //    by the last step, which drives the loop) and an expansion list of the
 //    frontier vertices WITH out-edges -- a vertex without out-edges is never
@@ -41,14 +41,24 @@
 //  * top-down is load-balanced by edges: a chained scan over the list's
 //    out-degrees gives each vertex its edge offset and scatters, for every
 //    tile of kExpTile edges, the list index where the tile starts; the expand
-//    kernel then gives each CTA whole edge tiles (coalesced neighbour reads,
+//    phase then gives each CTA whole edge tiles (coalesced neighbour reads,
 //    independent of the degree skew).  The scan's look-back words carry the
-//    step's epoch, so they never need clearing;
+//    scan's epoch, so they never need clearing;
 //  * bottom-up: the first bottom-up level of a search walks all vertices (a
 //    warp's ballot is one whole word of the next bitmap), later levels walk
-//    the compacted list of still-unvisited vertices;
+//    the compacted list of still-unvisited vertices; each probe loads four
+//    in-neighbours and their frontier bits at once (the first hit in CSR
+//    order still wins);
+//  * a top-down step sets the bitmap bit of every vertex it discovers and a
+//    bottom-up step lists the vertices it discovers, so a change of
+//    direction needs no conversion pass (arrayQueueToBitmap /
+//    bitmapToArrayQueue, arrayQueue.c:289-337); three bitmaps rotate (read,
+//    write, clear), so every step clears the bitmap a later step writes while
+//    it runs;
+//  * a top-down step whose list has at most kExpTile entries runs as one
+//    phase: every CTA scans the short list itself;
 //  * queue appends are staged per CTA in shared memory (one global atomic
-//    per flush);
+//    per flush); counters are summed per CTA (one atomic per CTA);
 //  * bitmaps: bit v = word v>>5, bit v&31 (bitmap.h:7-9).
 #include "graph.cuh"
 
@@ -60,10 +70,12 @@ namespace ogb {
 constexpr int kScanT = 256;            // threads of the degree scan
 constexpr int kScanI = 8;              // list entries per thread
 constexpr int kScanTile = kScanT * kScanI;
-constexpr int kExpT = 256;             // threads of the expand kernel
+constexpr int kExpT = 256;             // threads of the expand phase
 constexpr uint32_t kExpTile = 1024;    // edges per expand tile
+constexpr int kSearchT = 256;          // threads per CTA of the persistent search
 constexpr int kMaxTrace = 512;
 constexpr uint32_t kAlpha = 15, kBeta = 18;
+constexpr uint32_t kBuRound = 1024;    // vertices per CTA round of a bottom-up step
 
 struct BfsCtl {
   uint32_t qnext;            // logical size of the next frontier
@@ -80,23 +92,28 @@ struct BfsCtl {
   uint32_t pad;
 };
 
-// Direction codes of BfsDevState::dir.
-constexpr uint32_t kDirTD = 0, kDirBU = 1, kDirNone = 2;
+// The reference's switch state plus this search's bookkeeping.  Each CTA of
+// bfsk_search holds one copy in shared memory.
+struct BfsCtrl {
+  uint32_t mode, bu_entry_frontier, n, max_steps;
+  uint32_t mu, mf, nf, nf_prev;
+  uint32_t qcount, lsize, frontier, in_bu;
+  uint32_t ul_valid, ul_size, par_l, par_ul;
+  uint32_t bm_r, bm_w, bm_c, depth;
+  uint32_t iteration, processed, td_steps, bu_steps;
+  uint32_t nlevels, epoch, overflow, pad;
+  unsigned long long edges_examined;
+};
 
 struct BfsDevState {
-  uint32_t mode, bu_entry_frontier, n, E;
-  uint32_t max_steps, root;
+  BfsCtrl c;
   int32_t* parents;
   uint32_t* distances;
-  uint32_t mu, mf, nf, nf_prev;          // the reference's switch state
-  uint32_t qcount, lsize, frontier, dir;  // logical frontier, expansion list, step
-  uint32_t in_bu, need_b2l, l2b_now, dense_now;
-  uint32_t ul_valid, ul_size, par_l, par_bm;
-  uint32_t par_ul, iteration, processed, td_steps;
-  uint32_t bu_steps, nlevels, done, err;
-  uint32_t epoch, pad;
-  unsigned long long edges_examined;
-  BfsCtl ctl;
+  uint32_t err;       // ERR_SPIN when a bounded wait gave up
+  uint32_t bar;       // grid barrier word
+  uint32_t pad[2];
+  BfsCtl ctl[3];      // per-phase counters, rotating
+  BfsCtl aux;         // reached counts and the host-state steps
   BfsLevel trace[kMaxTrace];
 };
 
@@ -108,39 +125,28 @@ struct BfsBufs {
   const uint32_t* nbr_i;
   const uint32_t* out_degree;
   uint32_t* list[2];
-  uint32_t* bm[2];
+  uint32_t* bm[3];
   uint32_t* ul[2];
   uint32_t* offs;
   uint32_t* fstart;
   uint32_t* fdist;
   uint32_t* tile_i0;
   unsigned long long* status;
-  uint32_t* all_out;  // host-state top-down step only
   uint32_t V, words;
-};
-
-struct BfsGraph {
-  cudaGraphExec_t exec = nullptr;
 };
 
 struct BfsWork {
   uint32_t V = 0, E = 0;
-  DevBuf q0, q1, bm0, bm1, ul0, ul1, state;
-  DevBuf offs, fstart, fdist, tile_i0, scan_status, all_out;
+  DevBuf q0, q1, bm0, bm1, bm2, ul0, ul1, state;
+  DevBuf offs, fstart, fdist, tile_i0, scan_status;
   BfsDevState* h_state = nullptr;   // pinned copy
-  cudaStream_t cap = nullptr;       // capture stream
-  BfsGraph graphs[3][2];            // [mode][bu_entry_frontier]
-  cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_a = nullptr, ev_b = nullptr;
+  uint32_t epoch = 0;               // last scan epoch used
+  int search_grid = 0;
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
   ~BfsWork() {
-    for (auto& gm : graphs)
-      for (auto& gg : gm)
-        if (gg.exec) cudaGraphExecDestroy(gg.exec);
     if (h_state) cudaFreeHost(h_state);
-    if (cap) cudaStreamDestroy(cap);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
-    if (ev_a) cudaEventDestroy(ev_a);
-    if (ev_b) cudaEventDestroy(ev_b);
   }
 };
 
@@ -152,16 +158,11 @@ static int bfs_work_get(DevGraph& g, BfsWork** out) {
   const uint32_t V = g.V, E = g.E;
   const size_t words = ((size_t)V + 31) / 32;
   if (w->V != V || w->E != E || !w->q0.p) {
-    for (auto& gm : w->graphs)
-      for (auto& gg : gm)
-        if (gg.exec) {
-          cudaGraphExecDestroy(gg.exec);
-          gg.exec = nullptr;
-        }
     OGB_TRY(w->q0.alloc((size_t)V * 4 + 16));
     OGB_TRY(w->q1.alloc((size_t)V * 4 + 16));
     OGB_TRY(w->bm0.alloc(words * 4 + 16));
     OGB_TRY(w->bm1.alloc(words * 4 + 16));
+    OGB_TRY(w->bm2.alloc(words * 4 + 16));
     OGB_TRY(w->ul0.alloc((size_t)V * 4 + 16));
     OGB_TRY(w->ul1.alloc((size_t)V * 4 + 16));
     OGB_TRY(w->offs.alloc((size_t)V * 4 + 16));
@@ -179,15 +180,12 @@ static int bfs_work_get(DevGraph& g, BfsWork** out) {
   if (!w->ev_start) {
     OGB_CUDA(cudaEventCreate(&w->ev_start));
     OGB_CUDA(cudaEventCreate(&w->ev_stop));
-    OGB_CUDA(cudaEventCreate(&w->ev_a));
-    OGB_CUDA(cudaEventCreate(&w->ev_b));
   }
-  if (!w->cap) OGB_CUDA(cudaStreamCreateWithFlags(&w->cap, cudaStreamNonBlocking));
   *out = w;
   return OK;
 }
 
-static BfsBufs make_bufs(DevGraph& g, BfsWork* w, uint32_t* all_out) {
+static BfsBufs make_bufs(DevGraph& g, BfsWork* w) {
   BfsBufs b;
   b.rows_f = g.fwd.d_rows();
   b.nbr_f = g.fwd.d_dst();
@@ -198,6 +196,7 @@ static BfsBufs make_bufs(DevGraph& g, BfsWork* w, uint32_t* all_out) {
   b.list[1] = w->q1.as<uint32_t>();
   b.bm[0] = w->bm0.as<uint32_t>();
   b.bm[1] = w->bm1.as<uint32_t>();
+  b.bm[2] = w->bm2.as<uint32_t>();
   b.ul[0] = w->ul0.as<uint32_t>();
   b.ul[1] = w->ul1.as<uint32_t>();
   b.offs = w->offs.as<uint32_t>();
@@ -205,227 +204,86 @@ static BfsBufs make_bufs(DevGraph& g, BfsWork* w, uint32_t* all_out) {
   b.fdist = w->fdist.as<uint32_t>();
   b.tile_i0 = w->tile_i0.as<uint32_t>();
   b.status = w->scan_status.as<unsigned long long>();
-  b.all_out = all_out;
   b.V = g.V;
   b.words = (g.V + 31) / 32;
   return b;
 }
 
-// ------------------------------------------------------------ init ---------
+// ------------------------------------------------------------ shared memory
 
-// parents[v] = -out_degree[v] (or -1), distances[v] = 0 (BFS.c:58-74); the
-// root gets itself as parent; the state starts as the reference's loop does
-// (mu = E, mf = out_degree(root), queue = {root}, iteration 1).
-__global__ void __launch_bounds__(256) bfsk_init(BfsBufs b, BfsDevState* __restrict__ st, uint32_t root,
-                                                 int32_t* __restrict__ parents, uint32_t* __restrict__ distances,
-                                                 uint32_t mode, uint32_t bu_entry_frontier, uint32_t E) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < b.V; v += gridDim.x * blockDim.x) {
-    const uint32_t d = b.out_degree[v];
-    parents[v] = (v == root) ? (int32_t)root : (d ? -(int32_t)d : -1);
-    distances[v] = 0;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    const uint32_t d = b.out_degree[root];
-    const uint32_t epoch = st->epoch;  // keeps growing across searches
-    char* raw = reinterpret_cast<char*>(st);
-    for (size_t i = 0; i < offsetof(BfsDevState, trace); i++) raw[i] = 0;
-    st->mode = mode;
-    st->bu_entry_frontier = bu_entry_frontier;
-    st->n = b.V;
-    st->E = E;
-    st->max_steps = b.V + 8;
-    st->root = root;
-    st->parents = parents;
-    st->distances = distances;
-    st->mu = E;
-    st->mf = d;
-    st->qcount = 1;
-    st->lsize = d ? 1u : 0u;
-    st->dir = kDirNone;
-    st->iteration = 1;
-    st->processed = 1;
-    st->epoch = epoch;
-    b.list[0][0] = root;
+struct ScanSmem {
+  uint32_t w[kScanT / 32];
+  uint32_t tile, prefix;
+};
+// Top-down: the list entries of one edge tile (or the whole list of a small
+// step) and the step's appends.
+struct TdSmem {
+  uint32_t off[kExpTile + 2], start[kExpTile + 2], v[kExpTile + 2], d[kExpTile + 2];
+  BlockAppend<kExpTile> q_list;
+  BlockAppend<kExpTile> q_all;
+  uint32_t w[kExpT / 32];
+};
+// Bottom-up: a round's appends and its deferred long in-edge rows.
+struct BuSmem {
+  BlockAppend<kBuRound> q_ul;
+  BlockAppend<kBuRound> q_list;
+  uint32_t nheavy;
+  uint32_t hv[kBuRound], hj[kBuRound], he[kBuRound];
+};
+union BfsSmem {
+  ScanSmem scan;
+  TdSmem td;
+  BuSmem bu;
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void grid_clear(uint32_t* a, uint32_t* b2, uint32_t words) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x) {
+    if (a) a[i] = 0;
+    if (b2) b2[i] = 0;
   }
 }
 
-// ------------------------------------------------------------ control ------
+// ------------------------------------------------------------ grid barrier -
 
-// Before a step: turns a finished bottom-up phase's bitmap count into the
-// queue (mf = 1), stops on an empty queue, and otherwise picks the step's
-// direction with the reference's rule.  Sets the IF conditions of the step
-// (graph mode) and the matching flags (host-stepped mode).
-__global__ void bfsk_decide(BfsDevState* __restrict__ st, int use_handles, cudaGraphConditionalHandle h_l2b,
-                            cudaGraphConditionalHandle h_td, cudaGraphConditionalHandle h_bud,
-                            cudaGraphConditionalHandle h_bul) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  uint32_t l2b = 0, td = 0, bud = 0, bul = 0;
-  if (!st->done) {
-    if (st->need_b2l) {
-      st->qcount = st->ctl.qnext;
-      st->lsize = st->ctl.lnext;
-      st->mf = 1;
-      st->need_b2l = 0;
-    }
-    if (!st->in_bu && st->qcount == 0) {
-      st->done = 1;
-      st->dir = kDirNone;
-    } else {
-      const uint32_t epoch = st->epoch + 1;
-      BfsCtl z = {};
-      st->ctl = z;
-      st->epoch = epoch;
-      if (st->in_bu) {
-        st->dir = kDirBU;
-        st->frontier = st->nf;
-        st->nf_prev = st->nf;
-      } else {
-        const bool bu = (st->mode == BFS_PULL) || (st->mode == BFS_DO && st->mf > st->mu / kAlpha);
-        st->frontier = st->qcount;
-        if (bu) {
-          st->in_bu = 1;
-          l2b = 1;
-          st->nf = st->bu_entry_frontier ? st->qcount : 0u;
-          st->nf_prev = st->nf;
-          st->dir = kDirBU;
-        } else {
-          st->mu -= st->mf;
-          st->dir = kDirTD;
-        }
+// Barrier of all CTAs of a cooperative launch.  One counter: CTA 0 adds
+// 2^31 - (grid - 1), every other CTA adds 1, so bit 31 flips exactly when the
+// last CTA arrives and the low bits return to 0 (the word starts at 0).
+// The wait is bounded; a CTA that gives up, or sees the error word set by
+// another, returns false and the caller leaves the search.
+__device__ __forceinline__ bool grid_sync(uint32_t* bar, uint32_t* err, uint32_t* s_ok) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t add = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1) : 1u;
+    __threadfence();
+    const uint32_t old = atomicAdd(bar, add);
+    uint32_t ok = 1, spins = 0;
+    while (((old ^ ld_volatile_u32(bar)) & 0x80000000u) == 0) {
+      if (ld_volatile_u32(err)) {
+        ok = 0;
+        break;
       }
-      if (st->dir == kDirTD)
-        td = 1;
-      else if (!st->ul_valid)
-        bud = 1;
-      else
-        bul = 1;
-    }
-  }
-  st->l2b_now = l2b;
-  st->dense_now = bud;
-  if (use_handles) {
-    cudaGraphSetConditional(h_l2b, l2b);
-    cudaGraphSetConditional(h_td, td);
-    cudaGraphSetConditional(h_bud, bud);
-    cudaGraphSetConditional(h_bul, bul);
-  }
-}
-
-// After a step: the step's counters into the switch state, the trace, the
-// parities; decides whether the bottom-up phase continues (else the next
-// iteration converts the bitmap to the queue) and whether the loop goes on.
-__global__ void bfsk_finish(BfsDevState* __restrict__ st, int use_handles, cudaGraphConditionalHandle h_while,
-                            cudaGraphConditionalHandle h_b2l) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  uint32_t again = 0, b2l = 0;
-  if (!st->done) {
-    uint32_t discovered;
-    unsigned long long edges;
-    if (st->dir == kDirTD) {
-      st->mf = st->ctl.mf;
-      st->qcount = st->ctl.qnext;
-      st->lsize = st->ctl.lnext;
-      st->par_l ^= 1u;
-      st->td_steps++;
-      discovered = st->qcount;
-      edges = st->ctl.total_edges;
-    } else {
-      st->nf = st->ctl.nf;
-      st->ul_size = st->ctl.ul_size;
-      st->ul_valid = 1;
-      st->par_ul ^= 1u;
-      st->par_bm ^= 1u;
-      st->bu_steps++;
-      discovered = st->nf;
-      edges = st->ctl.edges;
-      const bool cont = (st->mode == BFS_PULL) ? (st->nf > 0)
-                                               : ((st->nf > st->nf_prev) || (st->nf > st->n / kBeta));
-      if (!cont) {
-        st->in_bu = 0;
-        st->need_b2l = 1;
-        st->ctl.qnext = 0;
-        st->ctl.lnext = 0;
-        b2l = 1;
+      if (++spins > kSpinLimit) {
+        atomicExch(err, (uint32_t)ERR_SPIN);
+        ok = 0;
+        break;
       }
     }
-    st->processed += discovered;
-    st->edges_examined += edges;
-    if (st->nlevels < (uint32_t)kMaxTrace) {
-      BfsLevel& L = st->trace[st->nlevels];
-      L.direction = st->dir;
-      L.discovered = discovered;
-      L.frontier = st->frontier;
-      L.mf = st->mf;
-      L.mu = st->mu;
-      L.edges = edges;
-      L.ms = 0.0f;
-    }
-    st->nlevels++;
-    st->iteration++;
-    if (st->dir == kDirTD && st->qcount == 0) {
-      st->done = 1;
-    } else if (st->iteration > st->max_steps) {
-      st->err = ERR_SPIN;
-      st->done = 1;
-    } else {
-      again = 1;
-    }
+    __threadfence();
+    *s_ok = ok;
   }
-  if (use_handles) {
-    cudaGraphSetConditional(h_b2l, b2l);
-    cudaGraphSetConditional(h_while, again);
-  }
-}
-
-// ------------------------------------------------------------ conversions --
-
-__global__ void __launch_bounds__(256) bfsk_clear_bitmap(BfsBufs b, const BfsDevState* __restrict__ st,
-                                                         int next) {
-  uint32_t* bm = b.bm[st->par_bm ^ (uint32_t)next];
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.words; i += gridDim.x * blockDim.x) bm[i] = 0;
-}
-
-// arrayQueueToBitmap (arrayQueue.c:289-307) over the expansion list (the
-// bitmap was cleared by bfsk_clear_bitmap).
-__global__ void __launch_bounds__(256) bfsk_list_to_bitmap(BfsBufs b, const BfsDevState* __restrict__ st) {
-  const uint32_t* q = b.list[st->par_l];
-  uint32_t* bm = b.bm[st->par_bm];
-  const uint32_t n = st->lsize;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t v = q[i];
-    atomicOr(&bm[v >> 5], 1u << (v & 31));
-  }
-}
-
-// bitmapToArrayQueue (arrayQueue.c:310-337): the logical size counts every
-// set bit; the expansion list keeps the ones with out-edges.
-__global__ void __launch_bounds__(256) bfsk_bitmap_to_list(BfsBufs b, BfsDevState* __restrict__ st) {
-  constexpr uint32_t kRoundWords = 128;  // bitmap words per block round (<= 4096 bits)
-  __shared__ BlockAppend<2 * kRoundWords * 32> q;
-  ba_init(q);
-  const uint32_t* bm = b.bm[st->par_bm];
-  uint32_t* list = b.list[st->par_l];
-  uint32_t cnt = 0;
-  for (uint32_t rbase = blockIdx.x * kRoundWords; rbase < b.words; rbase += gridDim.x * kRoundWords) {
-    const uint32_t w = rbase + threadIdx.x;
-    if (threadIdx.x < kRoundWords && w < b.words) {
-      uint32_t word = bm[w];
-      cnt += __popc(word);
-      while (word) {
-        const int bit = __ffs(word) - 1;
-        const uint32_t v = w * 32 + (uint32_t)bit;
-        if (b.out_degree[v]) ba_push(q, v);
-        word &= word - 1;
-      }
-    }
-    if (ba_size(q) > kRoundWords * 32) ba_flush(q, list, &st->ctl.lnext);
-  }
-  ba_flush(q, list, &st->ctl.lnext);
-  warp_atomic_add_total(&st->ctl.qnext, cnt);
+  __syncthreads();
+  return *s_ok != 0;
 }
 
 // ------------------------------------------------------------ top-down -----
 
+// Exclusive block scan (kScanT == kExpT threads).
 __device__ __forceinline__ uint32_t scan_block_excl(uint32_t v, uint32_t* s_w, uint32_t* total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t x = v;
@@ -451,29 +309,25 @@ __device__ __forceinline__ uint32_t scan_block_excl(uint32_t v, uint32_t* s_w, u
 }
 
 // Look-back word: value (32 bits) | flag (bits 32-33: 1 aggregate, 2
-// inclusive) | epoch (bits 34-63).  A word from an older step never matches.
+// inclusive) | epoch (bits 34-63).  A word of an older scan never matches.
 __device__ __forceinline__ unsigned long long lb_word(uint32_t epoch, uint32_t flag, uint32_t value) {
   return ((unsigned long long)(epoch & 0x3FFFFFFFu) << 34) | ((unsigned long long)flag << 32) | value;
 }
 
-// Top-down, phase 1: exclusive scan of the out-degrees of the expansion list
+// Top-down, part 1: exclusive scan of the out-degrees of the expansion list
 // (single pass, decoupled look-back; CTAs claim tiles in order until the
 // list is done).  Writes offs[i] (first edge of entry i in the level's edge
-// range), fstart[i] (its first CSR edge), fdist[i] (its depth + 1), the total
-// into ctl, and for every edge tile the list index of the entry holding the
-// tile's first edge.
-__global__ void __launch_bounds__(kScanT) bfsk_td_scan(BfsBufs b, BfsDevState* __restrict__ st) {
-  __shared__ uint32_t s_tile, s_prefix;
-  __shared__ uint32_t s_w[kScanT / 32];
-  const uint32_t* list = b.list[st->par_l];
-  const uint32_t n = st->lsize;
-  const uint32_t epoch = st->epoch;
-  const uint32_t* distances = st->distances;
-  BfsCtl* ctl = &st->ctl;
+// range), fstart[i] (its first CSR edge), fdist[i] (its depth + 1, unless
+// the depth is known), the total into ctl, and for every edge tile the list
+// index of the entry holding the tile's first edge.
+template <bool kDepthKnown>
+__device__ void td_scan_phase(const BfsBufs& b, const uint32_t* list, uint32_t n, const uint32_t* distances,
+                              uint32_t epoch, BfsCtl* ctl, uint32_t* err, ScanSmem& sm) {
+  if ((uint64_t)blockIdx.x * kScanTile >= n) return;  // the lower CTAs claim every tile
   for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(&ctl->scan_tiles, 1u);
+    if (threadIdx.x == 0) sm.tile = atomicAdd(&ctl->scan_tiles, 1u);
     __syncthreads();
-    const uint32_t tile = s_tile;
+    const uint32_t tile = sm.tile;
     if ((uint64_t)tile * kScanTile >= n) break;
     const uint64_t base = (uint64_t)tile * kScanTile + (uint64_t)threadIdx.x * kScanI;
     uint32_t deg[kScanI], sum = 0;
@@ -483,15 +337,15 @@ __global__ void __launch_bounds__(kScanT) bfsk_td_scan(BfsBufs b, BfsDevState* _
       deg[k] = 0;
       if (i < n) {
         const uint32_t v = list[i];
-        const uint2 r = b.rows_f[v];
+        const uint2 r = __ldg(&b.rows_f[v]);
         deg[k] = r.y;
         b.fstart[i] = r.x;
-        b.fdist[i] = distances[v] + 1;
+        if (!kDepthKnown) b.fdist[i] = distances[v] + 1;
         sum += r.y;
       }
     }
     uint32_t tile_total = 0;
-    const uint32_t excl = scan_block_excl(sum, s_w, &tile_total);
+    const uint32_t excl = scan_block_excl(sum, sm.w, &tile_total);
     if (threadIdx.x == 0) {
       uint32_t prefix = 0;
       unsigned long long* sw = b.status + tile;
@@ -506,7 +360,7 @@ __global__ void __launch_bounds__(kScanT) bfsk_td_scan(BfsBufs b, BfsDevState* _
           const uint32_t ep = (uint32_t)(v >> 34), flag = (uint32_t)(v >> 32) & 3u;
           if (ep != (epoch & 0x3FFFFFFFu) || flag == 0) {
             if (++spins > kSpinLimit) {
-              atomicExch(&st->err, (uint32_t)ERR_SPIN);
+              atomicExch(err, (uint32_t)ERR_SPIN);
               break;
             }
             continue;
@@ -517,11 +371,11 @@ __global__ void __launch_bounds__(kScanT) bfsk_td_scan(BfsBufs b, BfsDevState* _
         }
         st_volatile_u64(sw, lb_word(epoch, 2, prefix + tile_total));
       }
-      s_prefix = prefix;
+      sm.prefix = prefix;
       if ((uint64_t)(tile + 1) * kScanTile >= n) ctl->total_edges = prefix + tile_total;
     }
     __syncthreads();
-    uint32_t o = s_prefix + excl;
+    uint32_t o = sm.prefix + excl;
 #pragma unroll
     for (int k = 0; k < kScanI; k++) {
       const uint64_t i = base + k;
@@ -536,24 +390,72 @@ __global__ void __launch_bounds__(kScanT) bfsk_td_scan(BfsBufs b, BfsDevState* _
     __syncthreads();
   }
 }
+// Expand the step's edges [e0, e1); staged entries [0, cnt) cover them
+// (sm.off holds each entry's first edge in the step's edge range).  Each
+// thread takes four edges at once: neighbour ids, then their parents, then
+// the claiming CASes, each group issued back to back.  A claimed vertex gets
+// its depth, its bit in bm_w (when given) and, with out-edges, a list slot.
+template <bool kDepthKnown>
+__device__ __forceinline__ void expand_edges(const BfsBufs& b, uint32_t e0, uint32_t e1, uint32_t cnt,
+                                             int32_t* parents, uint32_t* distances, uint32_t dnext, uint32_t* bm_w,
+                                             uint32_t* all_out, TdSmem& sm, uint32_t& mf, uint32_t& found) {
+  constexpr int K = kExpTile / kExpT;
+  uint32_t u[K], src[K], dd[K];
+  bool ok[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const uint32_t e = e0 + threadIdx.x + k * kExpT;
+    ok[k] = e < e1;
+    u[k] = 0;
+    src[k] = 0;
+    dd[k] = dnext;
+    if (ok[k]) {
+      uint32_t lo = 0, hi = cnt - 1;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (sm.off[mid] <= e)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+      u[k] = __ldg(&b.nbr_f[sm.start[lo] + (e - sm.off[lo])]) & 0x3FFFFFFFu;
+      src[k] = sm.v[lo];
+      if (!kDepthKnown) dd[k] = sm.d[lo];
+    }
+  }
+  int32_t p[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) p[k] = ok[k] ? parents[u[k]] : 0;
+  bool won[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) won[k] = ok[k] && p[k] < 0 && atomicCAS(&parents[u[k]], p[k], (int32_t)src[k]) == p[k];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    if (won[k]) {
+      distances[u[k]] = dd[k];
+      mf += (uint32_t)(-p[k]);
+      found++;
+      if (bm_w) atomicOr(&bm_w[u[k] >> 5], 1u << (u[k] & 31));
+      if (all_out) ba_push(sm.q_all, u[k]);
+      if (__ldg(&b.out_degree[u[k]])) ba_push(sm.q_list, u[k]);
+    }
+  }
+}
 
-// Top-down, phase 2: each CTA takes whole tiles of kExpTile edges of the
-// level; the list entries overlapping a tile are staged in shared memory and
-// each edge finds its entry by binary search there.  A vertex is claimed by
-// CAS on its parent; the winner appends it to the next frontier.
-__global__ void __launch_bounds__(kExpT) bfsk_td_expand(BfsBufs b, BfsDevState* __restrict__ st) {
-  __shared__ uint32_t s_off[kExpTile + 2], s_start[kExpTile + 2], s_v[kExpTile + 2], s_d[kExpTile + 2];
-  __shared__ BlockAppend<kExpTile> q_list, q_all;
-  ba_init(q_list);
-  ba_init(q_all);
-  const uint32_t* list = b.list[st->par_l];
-  uint32_t* next_list = b.list[st->par_l ^ 1u];
-  const uint32_t n = st->lsize;
-  int32_t* parents = st->parents;
-  uint32_t* distances = st->distances;
-  BfsCtl* ctl = &st->ctl;
-  const uint32_t total = ctl->total_edges;
+// Top-down, part 2 (lists longer than kExpTile): each CTA takes whole tiles
+// of kExpTile edges of the step; the list entries overlapping a tile are
+// staged in shared memory and each edge finds its entry by binary search
+// there.  A vertex is claimed by CAS on its parent; the winner appends it to
+// the next frontier.
+template <bool kDepthKnown>
+__device__ void td_expand_phase(const BfsBufs& b, const uint32_t* list, uint32_t* next_list, uint32_t n,
+                                uint32_t total, int32_t* parents, uint32_t* distances, uint32_t dnext,
+                                uint32_t* bm_w, uint32_t* all_out, BfsCtl* ctl, TdSmem& sm,
+                                unsigned long long* s_red) {
   const uint32_t ntiles = (total + kExpTile - 1) / kExpTile;
+  if (blockIdx.x >= ntiles) return;
+  ba_init(sm.q_list);
+  ba_init(sm.q_all);
   uint32_t mf = 0, found = 0;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const uint32_t e0 = t * kExpTile;
@@ -562,146 +464,512 @@ __global__ void __launch_bounds__(kExpT) bfsk_td_expand(BfsBufs b, BfsDevState* 
     const uint32_t i1 = (t + 1 < ntiles) ? b.tile_i0[t + 1] : n - 1;
     const uint32_t cnt = i1 - i0 + 1;
     __syncthreads();
-    for (uint32_t k = threadIdx.x; k < cnt; k += kExpT) {
-      s_off[k] = b.offs[i0 + k];
-      s_start[k] = b.fstart[i0 + k];
-      s_v[k] = list[i0 + k];
-      s_d[k] = b.fdist[i0 + k];
+    for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) {
+      sm.off[k] = b.offs[i0 + k];
+      sm.start[k] = b.fstart[i0 + k];
+      sm.v[k] = list[i0 + k];
+      if (!kDepthKnown) sm.d[k] = b.fdist[i0 + k];
     }
     __syncthreads();
-    for (uint32_t e = e0 + threadIdx.x; e < e1; e += kExpT) {
-      uint32_t lo = 0, hi = cnt - 1;
-      while (lo < hi) {
-        const uint32_t mid = (lo + hi + 1) >> 1;
-        if (s_off[mid] <= e)
-          lo = mid;
-        else
-          hi = mid - 1;
-      }
-      const uint32_t u = b.nbr_f[s_start[lo] + (e - s_off[lo])] & 0x3FFFFFFFu;
-      const int32_t p = parents[u];
-      if (p < 0 && atomicCAS(&parents[u], p, (int32_t)s_v[lo]) == p) {
-        distances[u] = s_d[lo];
-        mf += (uint32_t)(-p);
-        found++;
-        if (b.all_out) ba_push(q_all, u);
-        if (b.out_degree[u]) ba_push(q_list, u);
-      }
-    }
+    expand_edges<kDepthKnown>(b, e0, e1, cnt, parents, distances, dnext, bm_w, all_out, sm, mf, found);
     // at most kExpTile discoveries per tile: flush every tile
-    ba_flush(q_list, next_list, &ctl->lnext);
-    if (b.all_out) ba_flush(q_all, b.all_out, &ctl->all_count);
+    ba_flush(sm.q_list, next_list, &ctl->lnext);
+    if (all_out) ba_flush(sm.q_all, all_out, &ctl->all_count);
   }
-  warp_atomic_add_total(&ctl->mf, mf);
-  warp_atomic_add_total(&ctl->qnext, found);
+  block_add_total<uint32_t>(&ctl->mf, mf, reinterpret_cast<uint32_t*>(s_red));
+  block_add_total<uint32_t>(&ctl->qnext, found, reinterpret_cast<uint32_t*>(s_red));
+}
+
+// A top-down step over a list of at most kExpTile entries: every CTA loads
+// the whole list and scans its out-degrees itself (no cross-CTA scan, so the
+// step needs one grid barrier), then expands its share of the edge tiles.
+__device__ void td_small_phase(const BfsBufs& b, const uint32_t* list, uint32_t* next_list, uint32_t n,
+                               int32_t* parents, uint32_t* distances, uint32_t dnext, uint32_t* bm_w, BfsCtl* ctl,
+                               TdSmem& sm, unsigned long long* s_red) {
+  constexpr int K = kExpTile / kExpT;
+  uint32_t deg[K], sum = 0;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const uint32_t i = threadIdx.x * K + k;
+    deg[k] = 0;
+    if (i < n) {
+      const uint32_t v = list[i];
+      const uint2 r = __ldg(&b.rows_f[v]);
+      sm.v[i] = v;
+      sm.start[i] = r.x;
+      deg[k] = r.y;
+      sum += r.y;
+    }
+  }
+  uint32_t total = 0;
+  uint32_t o = scan_block_excl(sum, sm.w, &total);
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const uint32_t i = threadIdx.x * K + k;
+    if (i < n) {
+      sm.off[i] = o;
+      o += deg[k];
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->total_edges = total;
+  __syncthreads();
+  const uint32_t ntiles = (total + kExpTile - 1) / kExpTile;
+  if (blockIdx.x >= ntiles) return;
+  ba_init(sm.q_list);
+  uint32_t mf = 0, found = 0;
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint32_t e0 = t * kExpTile;
+    const uint32_t e1 = min(e0 + kExpTile, total);
+    expand_edges<true>(b, e0, e1, n, parents, distances, dnext, bm_w, nullptr, sm, mf, found);
+    ba_flush(sm.q_list, next_list, &ctl->lnext);
+  }
+  block_add_total<uint32_t>(&ctl->mf, mf, reinterpret_cast<uint32_t*>(s_red));
+  block_add_total<uint32_t>(&ctl->qnext, found, reinterpret_cast<uint32_t*>(s_red));
 }
 
 // ------------------------------------------------------------ bottom-up ----
 
+constexpr uint32_t kInvalid = 0xFFFFFFFFu;
+constexpr int kBuV = kBuRound / kSearchT;  // candidates per thread per round
+constexpr uint32_t kFirst = 4;             // in-edges probed per candidate before deferral
+
+// One bottom-up step of the search.  Candidates: every vertex (dense, the
+// first bottom-up step of a search) or the unvisited list.  Each thread
+// takes kBuV candidates at once: parents, then in-edge rows, then the first
+// kFirst in-neighbours of each and their frontier bits, all issued
+// together.  A candidate with more in-edges and no hit yet is deferred to
+// the round's long-row list, which groups of 8 lanes scan 8 in-edges per
+// load (the first hit in CSR order still wins).  Found vertices get their
+// bit in bm_next (a warp's ballot stores a whole word in the dense case) and,
+// with out-edges, a slot in list_next; unfound ones with in-edges go to
+// ul_next (a vertex without in-edges can never be found).  bm_clear is
+// zeroed on the way.
+template <bool kDense>
+__device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t* bm_next, uint32_t* bm_clear,
+                              const uint32_t* ul_cur, uint32_t ul_count, uint32_t* ul_next, uint32_t* list_next,
+                              int32_t* parents, uint32_t* distances, uint32_t dnext, BfsCtl* ctl, BuSmem& sm,
+                              unsigned long long* s_red) {
+  grid_clear(bm_clear, nullptr, b.words);
+  if (threadIdx.x == 0) {
+    sm.q_ul.n = 0;
+    sm.q_list.n = 0;
+    sm.nheavy = 0;
+  }
+  __syncthreads();
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  const uint32_t count = kDense ? b.V : ul_count;
+  uint32_t nf = 0, edges = 0;
+  for (uint32_t rbase = blockIdx.x * kBuRound; rbase < count; rbase += gridDim.x * kBuRound) {
+    uint32_t v[kBuV];
+#pragma unroll
+    for (int k = 0; k < kBuV; k++) {
+      const uint32_t idx = rbase + k * kSearchT + threadIdx.x;
+      v[k] = idx < count ? (kDense ? idx : ul_cur[idx]) : kInvalid;
+    }
+    int32_t pv[kBuV];
+#pragma unroll
+    for (int k = 0; k < kBuV; k++) pv[k] = v[k] != kInvalid ? parents[v[k]] : 0;
+    uint2 row[kBuV];
+#pragma unroll
+    for (int k = 0; k < kBuV; k++)
+      row[k] = (v[k] != kInvalid && pv[k] < 0) ? __ldg(&b.rows_i[v[k]]) : make_uint2(0u, 0u);
+    uint32_t u[kBuV][kFirst];
+#pragma unroll
+    for (int k = 0; k < kBuV; k++)
+#pragma unroll
+      for (uint32_t m = 0; m < kFirst; m++)
+        u[k][m] = m < row[k].y ? (__ldg(&b.nbr_i[row[k].x + m]) & 0x3FFFFFFFu) : kInvalid;
+    uint32_t hit[kBuV], par[kBuV];
+#pragma unroll
+    for (int k = 0; k < kBuV; k++) {
+      hit[k] = kFirst;
+      par[k] = 0;
+#pragma unroll
+      for (int m = (int)kFirst - 1; m >= 0; m--) {
+        const uint32_t x = u[k][m];
+        if (x != kInvalid && ((bm_cur[x >> 5] >> (x & 31)) & 1u)) {
+          hit[k] = (uint32_t)m;
+          par[k] = x;
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kBuV; k++) {
+      bool found = false;
+      if (row[k].y) {
+        if (hit[k] < kFirst) {
+          parents[v[k]] = (int32_t)par[k];
+          distances[v[k]] = dnext;
+          found = true;
+          nf++;
+          edges += hit[k] + 1;
+          if (!kDense) atomicOr(&bm_next[v[k] >> 5], 1u << (v[k] & 31));
+          if (__ldg(&b.out_degree[v[k]])) ba_push(sm.q_list, v[k]);
+        } else if (row[k].y > kFirst) {
+          edges += kFirst;
+          const uint32_t h = warp_atomic_inc(&sm.nheavy);
+          sm.hv[h] = v[k];
+          sm.hj[h] = row[k].x + kFirst;
+          sm.he[h] = row[k].x + row[k].y;
+        } else {
+          edges += row[k].y;
+          ba_push(sm.q_ul, v[k]);
+        }
+      }
+      if (kDense) {
+        const uint32_t word = __ballot_sync(0xffffffffu, found);
+        const uint32_t base = rbase + k * kSearchT + warp * 32;
+        if (lane == 0 && base < b.V) bm_next[base >> 5] = word;
+      }
+    }
+    __syncthreads();
+    // long rows: a group of 8 lanes per row, 8 in-edges per load
+    const uint32_t nh = sm.nheavy;
+    const uint32_t gl = threadIdx.x & 7;
+    const uint32_t gmask = 0xFFu << (lane & 24);
+    for (uint32_t h = threadIdx.x >> 3; h < nh; h += kSearchT / 8) {
+      const uint32_t hv = sm.hv[h], j0 = sm.hj[h], end = sm.he[h];
+      bool hit_row = false;
+      for (uint32_t j = j0; j < end; j += 8) {
+        const uint32_t jj = j + gl;
+        const uint32_t x = jj < end ? (__ldg(&b.nbr_i[jj]) & 0x3FFFFFFFu) : kInvalid;
+        const bool bit = x != kInvalid && ((bm_cur[x >> 5] >> (x & 31)) & 1u);
+        const uint32_t m = (__ballot_sync(gmask, bit) >> (lane & 24)) & 0xFFu;
+        if (m) {
+          const uint32_t first = (uint32_t)__ffs(m) - 1;
+          if (gl == first) {
+            parents[hv] = (int32_t)x;
+            distances[hv] = dnext;
+            atomicOr(&bm_next[hv >> 5], 1u << (hv & 31));
+            nf++;
+            edges += j + first + 1 - j0;
+            if (__ldg(&b.out_degree[hv])) ba_push(sm.q_list, hv);
+          }
+          hit_row = true;
+          break;
+        }
+      }
+      if (!hit_row && gl == 0) {
+        edges += end - j0;
+        ba_push(sm.q_ul, hv);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) sm.nheavy = 0;
+    ba_flush(sm.q_ul, ul_next, &ctl->ul_size);
+    ba_flush(sm.q_list, list_next, &ctl->lnext);
+  }
+  block_add_total<uint32_t>(&ctl->nf, nf, reinterpret_cast<uint32_t*>(s_red));
+  block_add_total<unsigned long long>(&ctl->edges, (unsigned long long)edges, s_red);
+}
+
+// ---- bottom-up of the host-state step (depth read from the parent) --------
+
+struct BuHostSmem {
+  BlockAppend<2 * kBuRound> q;
+};
+
 // Scan v's in-edges in CSR order for the first in-neighbour in the frontier.
-__device__ __forceinline__ bool bu_probe(const BfsBufs& b, const uint32_t* __restrict__ bm_cur, uint32_t v,
-                                         int32_t* __restrict__ parents, uint32_t* __restrict__ distances,
-                                         unsigned long long& edges) {
-  const uint2 row = b.rows_i[v];
-  uint32_t j = row.x;
-  const uint32_t end = row.x + row.y;
-  bool found = false;
-  for (; j < end; j++) {
-    const uint32_t u = b.nbr_i[j] & 0x3FFFFFFFu;
+__device__ __forceinline__ bool bu_probe_host(const BfsBufs& b, const uint32_t* bm_cur, uint32_t v, int32_t* parents,
+                                              uint32_t* distances, uint32_t& edges) {
+  const uint2 row = __ldg(&b.rows_i[v]);
+  for (uint32_t j = row.x; j < row.x + row.y; j++) {
+    const uint32_t u = __ldg(&b.nbr_i[j]) & 0x3FFFFFFFu;
     if ((bm_cur[u >> 5] >> (u & 31)) & 1u) {
       parents[v] = (int32_t)u;
       distances[v] = distances[u] + 1;
-      found = true;
-      j++;
-      break;
+      edges += j + 1 - row.x;
+      return true;
     }
   }
-  edges += j - row.x;
-  return found;
+  edges += row.y;
+  return false;
 }
 
-// First bottom-up level of a search: a warp covers 32 consecutive vertices,
-// so its ballot is a whole word of the next bitmap (no atomics, no
-// clearing).  Vertices left unvisited go to the unvisited list.
-template <bool OR_INTO>
-__global__ void __launch_bounds__(256) bfsk_bu_dense(BfsBufs b, BfsDevState* __restrict__ st) {
-  constexpr uint32_t kRound = 1024;  // vertices per block round (4 bitmap words per warp)
-  __shared__ BlockAppend<2 * kRound> q_ul;
-  ba_init(q_ul);
-  const uint32_t* bm_cur = b.bm[st->par_bm];
-  uint32_t* bm_next = b.bm[st->par_bm ^ 1u];
-  uint32_t* ul_next = b.ul[st->par_ul ^ 1u];
-  int32_t* parents = st->parents;
-  uint32_t* distances = st->distances;
-  const uint32_t V = b.V;
+// Every vertex; a warp's ballot is OR-ed into one word of bm_next.
+__device__ void bu_host_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t* bm_next, uint32_t* ul_next,
+                              int32_t* parents, uint32_t* distances, BfsCtl* ctl, BuHostSmem& sm,
+                              unsigned long long* s_red) {
+  ba_init(sm.q);
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-  uint32_t nf = 0;
-  unsigned long long edges = 0;
-  for (uint32_t rbase = blockIdx.x * kRound; rbase < V; rbase += gridDim.x * kRound) {
+  uint32_t nf = 0, edges = 0;
+  for (uint32_t rbase = blockIdx.x * kBuRound; rbase < b.V; rbase += gridDim.x * kBuRound) {
 #pragma unroll
-    for (uint32_t k = 0; k < kRound / 256; k++) {
-      const uint32_t base = rbase + k * 256 + warp * 32;
+    for (uint32_t k = 0; k < kBuRound / kSearchT; k++) {
+      const uint32_t base = rbase + k * kSearchT + warp * 32;
       const uint32_t v = base + lane;
       bool found = false, unvisited = false;
-      if (v < V && parents[v] < 0) {
-        found = bu_probe(b, bm_cur, v, parents, distances, edges);
+      if (v < b.V && parents[v] < 0) {
+        found = bu_probe_host(b, bm_cur, v, parents, distances, edges);
         unvisited = !found;
       }
       const uint32_t word = __ballot_sync(0xffffffffu, found);
-      if (lane == 0 && base < V) {
-        if (OR_INTO)
-          bm_next[base >> 5] |= word;
-        else
-          bm_next[base >> 5] = word;
-      }
+      if (lane == 0 && base < b.V) bm_next[base >> 5] |= word;
       nf += found;
-      if (unvisited) ba_push(q_ul, v);
+      if (unvisited) ba_push(sm.q, v);
     }
-    if (ba_size(q_ul) > kRound) ba_flush(q_ul, ul_next, &st->ctl.ul_size);
+    if (ba_size(sm.q) > kBuRound) ba_flush(sm.q, ul_next, &ctl->ul_size);
   }
-  ba_flush(q_ul, ul_next, &st->ctl.ul_size);
-  warp_atomic_add_total(&st->ctl.nf, nf);
-  warp_atomic_add_total64(&st->ctl.edges, (uint32_t)edges);
+  ba_flush(sm.q, ul_next, &ctl->ul_size);
+  block_add_total<uint32_t>(&ctl->nf, nf, reinterpret_cast<uint32_t*>(s_red));
+  block_add_total<unsigned long long>(&ctl->edges, (unsigned long long)edges, s_red);
 }
 
-// Later bottom-up levels over the unvisited list (bm_next cleared first).
-__global__ void __launch_bounds__(256) bfsk_bu_list(BfsBufs b, BfsDevState* __restrict__ st) {
-  constexpr uint32_t kRound = 1024;  // list entries per block round
-  __shared__ BlockAppend<2 * kRound> q_ul;
-  ba_init(q_ul);
-  const uint32_t* bm_cur = b.bm[st->par_bm];
-  uint32_t* bm_next = b.bm[st->par_bm ^ 1u];
-  const uint32_t* ul_cur = b.ul[st->par_ul];
-  uint32_t* ul_next = b.ul[st->par_ul ^ 1u];
-  const uint32_t count = st->ul_size;
+// ------------------------------------------------------------ control ------
+
+constexpr uint32_t kActDone = 0, kActTD = 1, kActBU = 2;
+
+// Counters of a finished phase, read past any cached copy.
+__device__ __forceinline__ void load_ctl(const BfsCtl* p, BfsCtl& out) {
+  const volatile BfsCtl* v = p;
+  out.qnext = v->qnext;
+  out.lnext = v->lnext;
+  out.mf = v->mf;
+  out.nf = v->nf;
+  out.ul_size = v->ul_size;
+  out.total_edges = v->total_edges;
+  out.edges = v->edges;
+}
+
+__device__ __forceinline__ void zero_ctl(BfsCtl* p) {
+  BfsCtl z = {};
+  *p = z;
+}
+
+// Before a step: stop on an empty queue, else pick the direction with the
+// reference's rule (BFS.c:520-560).
+__device__ uint32_t ctrl_decide(BfsCtrl& c) {
+  if (c.overflow) return kActDone;
+  if (!c.in_bu && c.qcount == 0) return kActDone;
+  if (c.in_bu) {
+    c.frontier = c.nf;
+    c.nf_prev = c.nf;
+    return kActBU;
+  }
+  const bool bu = (c.mode == BFS_PULL) || (c.mode == BFS_DO && c.mf > c.mu / kAlpha);
+  c.frontier = c.qcount;
+  if (bu) {
+    c.in_bu = 1;
+    c.nf = c.bu_entry_frontier ? c.qcount : 0u;
+    c.nf_prev = c.nf;
+    return kActBU;
+  }
+  c.mu -= c.mf;
+  c.epoch++;
+  return kActTD;
+}
+
+__device__ void ctrl_level(BfsCtrl& c, BfsDevState* st, bool leader, uint32_t dir, uint32_t disc,
+                           unsigned long long edges, unsigned long long t0) {
+  if (leader && c.nlevels < (uint32_t)kMaxTrace) {
+    BfsLevel L;
+    L.direction = dir;
+    L.discovered = disc;
+    L.frontier = c.frontier;
+    L.mf = c.mf;
+    L.mu = c.mu;
+    L.edges = edges;
+    L.ms = (float)((double)(global_ns() - t0) * 1e-6);
+    st->trace[c.nlevels] = L;
+  }
+  c.nlevels++;
+  c.iteration++;
+  c.depth++;
+  c.processed += disc;
+  c.edges_examined += edges;
+  if (c.iteration > c.max_steps) c.overflow = 1;
+}
+
+// After a top-down step: it wrote its discoveries into bm_w and cleared the
+// other two bitmaps, so bm_w becomes the frontier bitmap.
+__device__ void ctrl_finish_td(BfsCtrl& c, uint32_t total_edges, const BfsCtl& k, BfsDevState* st, bool leader,
+                               unsigned long long t0) {
+  c.mf = k.mf;
+  c.qcount = k.qnext;
+  c.lsize = k.lnext;
+  c.par_l ^= 1u;
+  const uint32_t r = c.bm_r;
+  c.bm_r = c.bm_w;
+  c.bm_w = r;
+  c.td_steps++;
+  ctrl_level(c, st, leader, 0, c.qcount, total_edges, t0);
+}
+
+// After a bottom-up step (read bm_r, wrote bm_w, cleared bm_c): rotate, and
+// decide whether the bottom-up phase continues (BFS.c:583-585).  The step
+// also listed its discoveries, so the queue is ready when the phase ends
+// (mf = 1 then, BFS.c:588).
+__device__ void ctrl_finish_bu(BfsCtrl& c, const BfsCtl& k, BfsDevState* st, bool leader, unsigned long long t0) {
+  c.nf = k.nf;
+  c.ul_size = k.ul_size;
+  c.ul_valid = 1;
+  c.par_ul ^= 1u;
+  c.qcount = k.nf;
+  c.lsize = k.lnext;
+  c.par_l ^= 1u;
+  const uint32_t r = c.bm_r;
+  c.bm_r = c.bm_w;
+  c.bm_w = c.bm_c;
+  c.bm_c = r;
+  c.bu_steps++;
+  ctrl_level(c, st, leader, 1, c.nf, k.edges, t0);
+  const bool cont = (c.mode == BFS_PULL) ? (c.nf > 0) : ((c.nf > c.nf_prev) || (c.nf > c.n / kBeta));
+  if (!cont) {
+    c.in_bu = 0;
+    c.mf = 1;
+  }
+}
+
+// ------------------------------------------------------------ kernels ------
+
+// parents[v] = -out_degree[v] (or -1), distances[v] = 0 (BFS.c:58-74); the
+// root gets itself as parent; bitmap 0 holds the root, the others are clear;
+// the state starts as the reference's loop does (mu = E, mf =
+// out_degree(root), queue = {root}).
+__global__ void __launch_bounds__(256) bfsk_init(BfsBufs b, BfsDevState* st, uint32_t root, int32_t* parents,
+                                                 uint32_t* distances, uint32_t mode, uint32_t bu_entry_frontier,
+                                                 uint32_t E, uint32_t epoch) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < b.V; v += stride) {
+    const uint32_t d = b.out_degree[v];
+    parents[v] = (v == root) ? (int32_t)root : (d ? -(int32_t)d : -1);
+    distances[v] = 0;
+  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.words; i += stride) {
+    b.bm[0][i] = (i == (root >> 5)) ? (1u << (root & 31)) : 0u;
+    b.bm[1][i] = 0;
+    b.bm[2][i] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const uint32_t d = b.out_degree[root];
+    BfsCtrl c = {};
+    c.mode = mode;
+    c.bu_entry_frontier = bu_entry_frontier;
+    c.n = b.V;
+    c.max_steps = b.V + 8;
+    c.mu = E;
+    c.mf = d;
+    c.qcount = 1;
+    c.lsize = d ? 1u : 0u;
+    c.bm_r = 0;
+    c.bm_w = 1;
+    c.bm_c = 2;
+    c.iteration = 1;
+    c.processed = 1;
+    c.epoch = epoch;
+    st->c = c;
+    st->parents = parents;
+    st->distances = distances;
+    st->err = 0;
+    st->bar = 0;
+    zero_ctl(&st->ctl[0]);
+    zero_ctl(&st->ctl[1]);
+    zero_ctl(&st->ctl[2]);
+    b.list[0][0] = root;
+  }
+}
+
+// The whole search: all CTAs co-resident (cooperative launch), one grid
+// barrier after every phase.  Phase p counts into ctl[p % 3]; CTA 0 clears
+// ctl[(p + 1) % 3] when phase p starts (its last reader finished two
+// barriers earlier).  A top-down step is one phase when its list has at most
+// kExpTile entries, else two (scan, expand); a bottom-up step is one phase.
+__global__ void __launch_bounds__(kSearchT, 5) bfsk_search(BfsBufs b, BfsDevState* st) {
+  __shared__ BfsSmem sm;
+  __shared__ BfsCtrl S;
+  __shared__ unsigned long long s_red[kSearchT / 32];
+  __shared__ uint32_t s_act, s_ok;
+  __shared__ unsigned long long s_t0;
+  const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+  if (threadIdx.x == 0) S = st->c;
+  __syncthreads();
   int32_t* parents = st->parents;
   uint32_t* distances = st->distances;
-  uint32_t nf = 0;
-  unsigned long long edges = 0;
-  for (uint32_t rbase = blockIdx.x * kRound; rbase < count; rbase += gridDim.x * kRound) {
-#pragma unroll
-    for (uint32_t k = 0; k < kRound / 256; k++) {
-      const uint32_t t = rbase + k * 256 + threadIdx.x;
-      if (t >= count) continue;
-      const uint32_t v = ul_cur[t];
-      if (parents[v] >= 0) continue;  // visited by a top-down step since the list was made
-      if (bu_probe(b, bm_cur, v, parents, distances, edges)) {
-        atomicOr(&bm_next[v >> 5], 1u << (v & 31));
-        nf++;
-      } else {
-        ba_push(q_ul, v);
-      }
+  BfsCtl* ctl = st->ctl;
+  uint32_t p = 0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_act = ctrl_decide(S);
+      s_t0 = global_ns();
     }
-    if (ba_size(q_ul) > kRound) ba_flush(q_ul, ul_next, &st->ctl.ul_size);
+    __syncthreads();
+    const uint32_t act = s_act;
+    if (act == kActDone) break;
+    const uint32_t dnext = S.depth + 1;
+    if (act == kActTD) {
+      const uint32_t* list = b.list[S.par_l];
+      uint32_t* next = b.list[S.par_l ^ 1u];
+      uint32_t* bm_w = b.bm[S.bm_w];
+      const uint32_t n = S.lsize;
+      grid_clear(b.bm[S.bm_r], b.bm[S.bm_c], b.words);  // a top-down step reads no bitmap
+      if (leader) zero_ctl(&ctl[(p + 1) % 3]);
+      uint32_t total;
+      if (n <= kExpTile) {
+        td_small_phase(b, list, next, n, parents, distances, dnext, bm_w, &ctl[p % 3], sm.td, s_red);
+        if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
+        total = ld_volatile_u32(&ctl[p % 3].total_edges);
+      } else {
+        td_scan_phase<true>(b, list, n, distances, S.epoch, &ctl[p % 3], &st->err, sm.scan);
+        if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
+        total = ld_volatile_u32(&ctl[p % 3].total_edges);
+        p++;
+        if (leader) zero_ctl(&ctl[(p + 1) % 3]);
+        td_expand_phase<true>(b, list, next, n, total, parents, distances, dnext, bm_w, nullptr, &ctl[p % 3], sm.td,
+                              s_red);
+        if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
+      }
+      if (threadIdx.x == 0) {
+        BfsCtl k;
+        load_ctl(&ctl[p % 3], k);
+        ctrl_finish_td(S, total, k, st, blockIdx.x == 0, s_t0);
+      }
+      p++;
+    } else {
+      if (leader) zero_ctl(&ctl[(p + 1) % 3]);
+      if (!S.ul_valid)
+        bu_step_phase<true>(b, b.bm[S.bm_r], b.bm[S.bm_w], b.bm[S.bm_c], nullptr, 0, b.ul[S.par_ul ^ 1u],
+                            b.list[S.par_l ^ 1u], parents, distances, dnext, &ctl[p % 3], sm.bu, s_red);
+      else
+        bu_step_phase<false>(b, b.bm[S.bm_r], b.bm[S.bm_w], b.bm[S.bm_c], b.ul[S.par_ul], S.ul_size,
+                             b.ul[S.par_ul ^ 1u], b.list[S.par_l ^ 1u], parents, distances, dnext, &ctl[p % 3],
+                             sm.bu, s_red);
+      if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
+      if (threadIdx.x == 0) {
+        BfsCtl k;
+        load_ctl(&ctl[p % 3], k);
+        ctrl_finish_bu(S, k, st, blockIdx.x == 0, s_t0);
+      }
+      p++;
+    }
   }
-  ba_flush(q_ul, ul_next, &st->ctl.ul_size);
-  warp_atomic_add_total(&st->ctl.nf, nf);
-  warp_atomic_add_total64(&st->ctl.edges, (uint32_t)edges);
+  if (leader) st->c = S;
 }
 
-// ------------------------------------------------------------ misc ---------
+// ---- kernels of the host-state steps (depth read from the parent) --------
 
-// Keep the entries of a queue that have out-edges (host-state step API).
+__global__ void __launch_bounds__(kScanT) bfsk_td_scan_host(BfsBufs b, BfsDevState* st, uint32_t n,
+                                                           const uint32_t* distances, uint32_t epoch) {
+  __shared__ ScanSmem sm;
+  td_scan_phase<false>(b, b.list[0], n, distances, epoch, &st->aux, &st->err, sm);
+}
+
+__global__ void __launch_bounds__(kExpT) bfsk_td_expand_host(BfsBufs b, BfsDevState* st, uint32_t n,
+                                                             int32_t* parents, uint32_t* distances,
+                                                             uint32_t* all_out) {
+  __shared__ TdSmem sm;
+  __shared__ unsigned long long s_red[kExpT / 32];
+  td_expand_phase<false>(b, b.list[0], b.list[1], n, st->aux.total_edges, parents, distances, 0, nullptr, all_out,
+                         &st->aux, sm, s_red);
+}
+
+__global__ void __launch_bounds__(kSearchT) bfsk_bu_host(BfsBufs b, BfsDevState* st, int32_t* parents,
+                                                        uint32_t* distances) {
+  __shared__ BuHostSmem sm;
+  __shared__ unsigned long long s_red[kSearchT / 32];
+  bu_host_phase(b, b.bm[0], b.bm[1], b.ul[1], parents, distances, &st->aux, sm, s_red);
+}
+
+// Keep the entries of a queue that have out-edges.
 __global__ void bfsk_filter_list(const uint32_t* __restrict__ in, uint32_t n, const uint32_t* __restrict__ out_degree,
                                  uint32_t* __restrict__ out, uint32_t* __restrict__ count) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -711,8 +979,9 @@ __global__ void bfsk_filter_list(const uint32_t* __restrict__ in, uint32_t n, co
 }
 
 // Number of reached vertices and the sum of their out-degrees (Graph500
-// traversed edges).
-__global__ void __launch_bounds__(256) bfsk_reached(BfsBufs b, BfsDevState* __restrict__ st) {
+// traversed edges), into st->aux.
+__global__ void __launch_bounds__(256) bfsk_reached(BfsBufs b, BfsDevState* st) {
+  __shared__ unsigned long long s_red[8];
   const int32_t* parents = st->parents;
   unsigned long long e = 0;
   uint32_t r = 0;
@@ -722,219 +991,58 @@ __global__ void __launch_bounds__(256) bfsk_reached(BfsBufs b, BfsDevState* __re
       e += b.out_degree[v];
     }
   }
-  for (int o = 16; o; o >>= 1) {
-    e += __shfl_down_sync(0xffffffffu, e, o);
-    r += __shfl_down_sync(0xffffffffu, r, o);
-  }
-  if (lane_id() == 0) {
-    if (e) atomicAdd(&st->ctl.reached_edges, e);
-    if (r) atomicAdd(&st->ctl.reached, r);
-  }
-}
-
-__global__ void bfsk_zero_reached(BfsDevState* __restrict__ st) {
-  st->ctl.reached = 0;
-  st->ctl.reached_edges = 0;
+  block_add_total<unsigned long long>(&st->aux.reached_edges, e, s_red);
+  block_add_total<uint32_t>(&st->aux.reached, r, reinterpret_cast<uint32_t*>(s_red));
 }
 
 // ------------------------------------------------------------ drivers ------
 
-struct Grids {
-  int v, small;
-};
-static Grids grids(const BfsBufs& b) {
-  const int sms = sm_count();
-  return {sms * 8, sms * 4};
-}
-
-// Launch the kernels of one step on `s` (host-stepped driver and graph
-// capture share this).  `which`: 0 top-down, 1 bottom-up first, 2 bottom-up
-// list, 3 list->bitmap, 4 bitmap->list.
-static void launch_part(int which, const BfsBufs& b, BfsDevState* st, cudaStream_t s) {
-  const Grids gr = grids(b);
-  switch (which) {
-    case 0:
-      bfsk_td_scan<<<gr.v, kScanT, 0, s>>>(b, st);
-      bfsk_td_expand<<<gr.v, kExpT, 0, s>>>(b, st);
-      break;
-    case 1:
-      bfsk_bu_dense<false><<<gr.v, 256, 0, s>>>(b, st);
-      break;
-    case 2:
-      bfsk_clear_bitmap<<<gr.small, 256, 0, s>>>(b, st, 1);
-      bfsk_bu_list<<<gr.v, 256, 0, s>>>(b, st);
-      break;
-    case 3:
-      bfsk_clear_bitmap<<<gr.small, 256, 0, s>>>(b, st, 0);
-      bfsk_list_to_bitmap<<<gr.small, 256, 0, s>>>(b, st);
-      break;
-    case 4:
-      bfsk_bitmap_to_list<<<gr.small, 256, 0, s>>>(b, st);
-      break;
-  }
-}
-
-static int add_if(cudaGraph_t g, cudaGraphNode_t* node, cudaGraphNode_t dep, cudaGraphConditionalHandle h,
-                  cudaGraph_t* body) {
-  cudaGraphNodeParams p = {};
-  p.type = cudaGraphNodeTypeConditional;
-  p.conditional.handle = h;
-  p.conditional.type = cudaGraphCondTypeIf;
-  p.conditional.size = 1;
-  OGB_CUDA(cudaGraphAddNode(node, g, dep ? &dep : nullptr, dep ? 1 : 0, &p));
-  *body = p.conditional.phGraph_out[0];
-  return OK;
-}
-
-static int capture_into(cudaGraph_t body, cudaStream_t cap, int which, const BfsBufs& b, BfsDevState* st) {
-  OGB_CUDA(cudaStreamBeginCaptureToGraph(cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-  launch_part(which, b, st, cap);
-  cudaGraph_t out = nullptr;
-  OGB_CUDA(cudaStreamEndCapture(cap, &out));
-  return OK;
-}
-
-template <class... A>
-static int add_kernel(cudaGraph_t g, cudaGraphNode_t* node, cudaGraphNode_t dep, void (*fn)(A...), void** args) {
-  cudaKernelNodeParams p = {};
-  p.func = reinterpret_cast<void*>(fn);
-  p.gridDim = dim3(1);
-  p.blockDim = dim3(32);
-  p.sharedMemBytes = 0;
-  p.kernelParams = args;
-  p.extra = nullptr;
-  OGB_CUDA(cudaGraphAddKernelNode(node, g, dep ? &dep : nullptr, dep ? 1 : 0, &p));
-  return OK;
-}
-
-// The search loop as one executable graph (per graph buffers, mode and
-// bottom-up entry rule).
-static int build_search_graph(BfsWork* w, const BfsBufs& b, cudaGraphExec_t* exec) {
-  BfsDevState* st = w->state.as<BfsDevState>();
-  cudaGraph_t g = nullptr;
-  OGB_CUDA(cudaGraphCreate(&g, 0));
-  cudaGraphConditionalHandle h_while, h_b2l, h_l2b, h_td, h_bud, h_bul;
-  OGB_CUDA(cudaGraphConditionalHandleCreate(&h_while, g, 1, cudaGraphCondAssignDefault));
-  OGB_CUDA(cudaGraphConditionalHandleCreate(&h_b2l, g, 0, cudaGraphCondAssignDefault));
-  OGB_CUDA(cudaGraphConditionalHandleCreate(&h_l2b, g, 0, cudaGraphCondAssignDefault));
-  OGB_CUDA(cudaGraphConditionalHandleCreate(&h_td, g, 0, cudaGraphCondAssignDefault));
-  OGB_CUDA(cudaGraphConditionalHandleCreate(&h_bud, g, 0, cudaGraphCondAssignDefault));
-  OGB_CUDA(cudaGraphConditionalHandleCreate(&h_bul, g, 0, cudaGraphCondAssignDefault));
-  cudaGraphNodeParams wp = {};
-  wp.type = cudaGraphNodeTypeConditional;
-  wp.conditional.handle = h_while;
-  wp.conditional.type = cudaGraphCondTypeWhile;
-  wp.conditional.size = 1;
-  cudaGraphNode_t wnode;
-  OGB_CUDA(cudaGraphAddNode(&wnode, g, nullptr, 0, &wp));
-  cudaGraph_t body = wp.conditional.phGraph_out[0];
-
-  int use = 1;
-  cudaGraphNode_t n_b2l, n_dec, n_l2b, n_td, n_bud, n_bul, n_fin;
-  cudaGraph_t bb;
-  OGB_TRY(add_if(body, &n_b2l, nullptr, h_b2l, &bb));
-  OGB_TRY(capture_into(bb, w->cap, 4, b, st));
-  void* dec_args[] = {&st, &use, &h_l2b, &h_td, &h_bud, &h_bul};
-  OGB_TRY(add_kernel(body, &n_dec, n_b2l, bfsk_decide, dec_args));
-  OGB_TRY(add_if(body, &n_l2b, n_dec, h_l2b, &bb));
-  OGB_TRY(capture_into(bb, w->cap, 3, b, st));
-  OGB_TRY(add_if(body, &n_td, n_l2b, h_td, &bb));
-  OGB_TRY(capture_into(bb, w->cap, 0, b, st));
-  OGB_TRY(add_if(body, &n_bud, n_td, h_bud, &bb));
-  OGB_TRY(capture_into(bb, w->cap, 1, b, st));
-  OGB_TRY(add_if(body, &n_bul, n_bud, h_bul, &bb));
-  OGB_TRY(capture_into(bb, w->cap, 2, b, st));
-  void* fin_args[] = {&st, &use, &h_while, &h_b2l};
-  OGB_TRY(add_kernel(body, &n_fin, n_bul, bfsk_finish, fin_args));
-  cudaError_t e = cudaGraphInstantiate(exec, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) return fail(ERR_CUDA, "bfs graph instantiate: %s", cudaGetErrorString(e));
-  return OK;
-}
-
-static int read_state(BfsWork* w, cudaStream_t s) {
-  OGB_CUDA(cudaMemcpyAsync(w->h_state, w->state.p, offsetof(BfsDevState, trace), cudaMemcpyDeviceToHost, s));
-  OGB_CUDA(cudaStreamSynchronize(s));
-  return OK;
-}
-
 int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_t* distances, BfsResult* res,
             bool time_levels, bool bu_entry_nf_frontier, cudaStream_t s) {
+  (void)time_levels;  // the search always records per-level device times
   const uint32_t V = g.V;
   if (root >= V) return fail(ERR_ARG, "bfs: root %u out of range (V=%u)", root, V);
   if (mode > BFS_DO) return fail(ERR_ARG, "bfs: mode %u", mode);
   BfsWork* w = nullptr;
   OGB_TRY(bfs_work_get(g, &w));
-  const BfsBufs b = make_bufs(g, w, nullptr);
+  BfsBufs b = make_bufs(g, w);
   BfsDevState* st = w->state.as<BfsDevState>();
-  const Grids gr = grids(b);
-  std::vector<float> level_ms;
-
-  bfsk_init<<<gr.v, 256, 0, s>>>(b, st, root, parents, distances, mode, bu_entry_nf_frontier ? 1u : 0u, g.E);
+  if (!w->search_grid) {
+    int nb = 0;
+    OGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, bfsk_search, kSearchT, 0));
+    if (nb < 1) return fail(ERR_CUDA, "bfs: search kernel does not fit on an SM");
+    w->search_grid = nb * sm_count();
+  }
+  bfsk_init<<<sm_count() * 8, 256, 0, s>>>(b, st, root, parents, distances, mode, bu_entry_nf_frontier ? 1u : 0u,
+                                            g.E, w->epoch);
   OGB_CUDA(cudaGetLastError());
   OGB_CUDA(cudaEventRecord(w->ev_start, s));
-  uint32_t launches = 1;
-  if (!time_levels) {
-    BfsGraph& gg = w->graphs[mode][bu_entry_nf_frontier ? 1 : 0];
-    if (!gg.exec) OGB_TRY(build_search_graph(w, b, &gg.exec));
-    OGB_CUDA(cudaGraphLaunch(gg.exec, s));
-  } else {
-    // host-stepped: the same kernels, one step at a time, timed with events
-    BfsDevState* h = w->h_state;
-    OGB_TRY(read_state(w, s));
-    while (!h->done) {
-      if (h->need_b2l) {
-        launch_part(4, b, st, s);
-        launches++;
-      }
-      bfsk_decide<<<1, 32, 0, s>>>(st, 0, 0, 0, 0, 0);
-      OGB_TRY(read_state(w, s));
-      launches++;
-      if (h->done) break;
-      if (h->l2b_now) {
-        launch_part(3, b, st, s);
-        launches += 2;
-      }
-      OGB_CUDA(cudaEventRecord(w->ev_a, s));
-      const int part = h->dir == kDirTD ? 0 : (h->dense_now ? 1 : 2);
-      launch_part(part, b, st, s);
-      launches += (part == 1) ? 1 : 2;
-      OGB_CUDA(cudaEventRecord(w->ev_b, s));
-      bfsk_finish<<<1, 32, 0, s>>>(st, 0, 0, 0);
-      launches++;
-      OGB_CUDA(cudaGetLastError());
-      OGB_TRY(read_state(w, s));
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, w->ev_a, w->ev_b);
-      level_ms.push_back(ms);
-    }
-  }
-  OGB_CUDA(cudaGetLastError());
+  void* args[] = {(void*)&b, (void*)&st};
+  OGB_CUDA(cudaLaunchCooperativeKernel((void*)bfsk_search, dim3(w->search_grid), dim3(kSearchT), args, 0, s));
   OGB_CUDA(cudaEventRecord(w->ev_stop, s));
-  bfsk_zero_reached<<<1, 1, 0, s>>>(st);
-  bfsk_reached<<<gr.v, 256, 0, s>>>(b, st);
+  OGB_CUDA(cudaMemsetAsync(&st->aux, 0, sizeof(BfsCtl), s));
+  bfsk_reached<<<sm_count() * 8, 256, 0, s>>>(b, st);
   OGB_CUDA(cudaGetLastError());
   OGB_CUDA(cudaMemcpyAsync(w->h_state, w->state.p, sizeof(BfsDevState), cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaStreamSynchronize(s));
   float total_ms = 0.f;
   OGB_CUDA(cudaEventElapsedTime(&total_ms, w->ev_start, w->ev_stop));
   const BfsDevState* h = w->h_state;
-  if (h->err) return fail((int)h->err, "bfs: a bounded device loop gave up");
+  w->epoch = h->c.epoch;
+  if (h->err) return fail((int)h->err, "bfs: a bounded device wait gave up");
+  if (h->c.overflow) return fail(ERR_SPIN, "bfs: more than V + 8 steps");
   BfsResult r;
-  r.iteration = h->iteration;
-  r.processed_nodes = h->processed;
-  r.td_steps = h->td_steps;
-  r.bu_steps = h->bu_steps;
-  r.edges_examined = h->edges_examined;
-  r.reached = h->ctl.reached;
-  r.reached_out_edges = h->ctl.reached_edges;
+  r.iteration = h->c.iteration;
+  r.processed_nodes = h->c.processed;
+  r.td_steps = h->c.td_steps;
+  r.bu_steps = h->c.bu_steps;
+  r.edges_examined = h->c.edges_examined;
+  r.reached = h->aux.reached;
+  r.reached_out_edges = h->aux.reached_edges;
   r.ms = total_ms;
-  r.launches = time_levels ? launches : 1 + 3 * (h->td_steps + h->bu_steps);
-  r.nlevels = (int)std::min<uint32_t>(h->nlevels, kMaxTrace);
-  for (int i = 0; i < r.nlevels; i++) {
-    r.levels[i] = h->trace[i];
-    if (i < (int)level_ms.size()) r.levels[i].ms = level_ms[i];
-  }
+  r.launches = 2;  // init + search
+  r.nlevels = (int)std::min<uint32_t>(h->c.nlevels, kMaxTrace);
+  for (int i = 0; i < r.nlevels; i++) r.levels[i] = h->trace[i];
   if (res) *res = r;
   return OK;
 }
@@ -956,38 +1064,34 @@ int bfs_td_step_host(DevGraph& g, const uint32_t* q, uint32_t qsize, int32_t* pa
   OGB_TRY(d_dist.alloc((size_t)V * 4 + 4));
   OGB_TRY(d_all.alloc((size_t)V * 4 + 4));
   OGB_TRY(d_cnt.alloc(16));
+  BfsDevState* st = w->state.as<BfsDevState>();
+  const BfsBufs b = make_bufs(g, w);
   OGB_CUDA(cudaMemcpyAsync(d_par.p, parents, (size_t)V * 4, cudaMemcpyHostToDevice, s));
   OGB_CUDA(cudaMemcpyAsync(d_dist.p, distances, (size_t)V * 4, cudaMemcpyHostToDevice, s));
   OGB_CUDA(cudaMemcpyAsync(w->ul0.p, q, (size_t)qsize * 4, cudaMemcpyHostToDevice, s));
   OGB_CUDA(cudaMemsetAsync(d_cnt.p, 0, 16, s));
+  OGB_CUDA(cudaMemsetAsync(&st->aux, 0, sizeof(BfsCtl), s));
+  OGB_CUDA(cudaMemsetAsync(&st->err, 0, 4, s));
   if (qsize) {
     bfsk_filter_list<<<std::min<uint32_t>(sm_count() * 8, ceil_div(qsize, 256)), 256, 0, s>>>(
-        w->ul0.as<uint32_t>(), qsize, g.fwd.d_out_degree(), w->q0.as<uint32_t>(), d_cnt.as<uint32_t>());
+        w->ul0.as<uint32_t>(), qsize, g.fwd.d_out_degree(), b.list[0], d_cnt.as<uint32_t>());
     OGB_CUDA(cudaGetLastError());
   }
   uint32_t n = 0;
   OGB_CUDA(cudaMemcpyAsync(&n, d_cnt.p, 4, cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaStreamSynchronize(s));
-  // a state for one step: list 0 holds the window, epoch one past the last
-  BfsDevState* h = w->h_state;
-  OGB_CUDA(cudaMemcpyAsync(h, w->state.p, offsetof(BfsDevState, trace), cudaMemcpyDeviceToHost, s));
+  if (n) {
+    const uint32_t epoch = ++w->epoch;
+    bfsk_td_scan_host<<<sm_count() * 8, kScanT, 0, s>>>(b, st, n, d_dist.as<uint32_t>(), epoch);
+    bfsk_td_expand_host<<<sm_count() * 8, kExpT, 0, s>>>(b, st, n, d_par.as<int32_t>(), d_dist.as<uint32_t>(),
+                                                         d_all.as<uint32_t>());
+    OGB_CUDA(cudaGetLastError());
+  }
+  OGB_CUDA(cudaMemcpyAsync(w->h_state, w->state.p, offsetof(BfsDevState, trace), cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaStreamSynchronize(s));
-  const uint32_t epoch = h->epoch + 1;
-  memset(h, 0, offsetof(BfsDevState, trace));
-  h->n = V;
-  h->E = g.E;
-  h->parents = d_par.as<int32_t>();
-  h->distances = d_dist.as<uint32_t>();
-  h->lsize = n;
-  h->epoch = epoch;
-  h->dir = kDirTD;
-  OGB_CUDA(cudaMemcpyAsync(w->state.p, h, offsetof(BfsDevState, trace), cudaMemcpyHostToDevice, s));
-  const BfsBufs b = make_bufs(g, w, d_all.as<uint32_t>());
-  if (n) launch_part(0, b, w->state.as<BfsDevState>(), s);
-  OGB_CUDA(cudaGetLastError());
-  OGB_TRY(read_state(w, s));
-  *next_size = h->ctl.qnext;
-  *mf = h->ctl.mf;
+  if (w->h_state->err) return fail((int)w->h_state->err, "bfs step: a bounded device wait gave up");
+  *next_size = w->h_state->aux.qnext;
+  *mf = w->h_state->aux.mf;
   OGB_CUDA(cudaMemcpyAsync(next_q, d_all.p, (size_t)(*next_size) * 4, cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaMemcpyAsync(parents, d_par.p, (size_t)V * 4, cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaMemcpyAsync(distances, d_dist.p, (size_t)V * 4, cudaMemcpyDeviceToHost, s));
@@ -1006,26 +1110,18 @@ int bfs_bu_step_host(DevGraph& g, const uint32_t* bm_cur, uint32_t* bm_next, int
   DevBuf d_par, d_dist;
   OGB_TRY(d_par.alloc((size_t)V * 4 + 4));
   OGB_TRY(d_dist.alloc((size_t)V * 4 + 4));
+  BfsDevState* st = w->state.as<BfsDevState>();
+  const BfsBufs b = make_bufs(g, w);
   OGB_CUDA(cudaMemcpyAsync(d_par.p, parents, (size_t)V * 4, cudaMemcpyHostToDevice, s));
   OGB_CUDA(cudaMemcpyAsync(d_dist.p, distances, (size_t)V * 4, cudaMemcpyHostToDevice, s));
   OGB_CUDA(cudaMemcpyAsync(w->bm0.p, bm_cur, words * 4, cudaMemcpyHostToDevice, s));
   OGB_CUDA(cudaMemcpyAsync(w->bm1.p, bm_next, words * 4, cudaMemcpyHostToDevice, s));
-  BfsDevState* h = w->h_state;
-  OGB_CUDA(cudaMemcpyAsync(h, w->state.p, offsetof(BfsDevState, trace), cudaMemcpyDeviceToHost, s));
-  OGB_CUDA(cudaStreamSynchronize(s));
-  const uint32_t epoch = h->epoch;
-  memset(h, 0, offsetof(BfsDevState, trace));
-  h->n = V;
-  h->parents = d_par.as<int32_t>();
-  h->distances = d_dist.as<uint32_t>();
-  h->epoch = epoch;
-  h->dir = kDirBU;
-  OGB_CUDA(cudaMemcpyAsync(w->state.p, h, offsetof(BfsDevState, trace), cudaMemcpyHostToDevice, s));
-  const BfsBufs b = make_bufs(g, w, nullptr);
-  bfsk_bu_dense<true><<<sm_count() * 8, 256, 0, s>>>(b, w->state.as<BfsDevState>());
+  OGB_CUDA(cudaMemsetAsync(&st->aux, 0, sizeof(BfsCtl), s));
+  bfsk_bu_host<<<sm_count() * 8, kSearchT, 0, s>>>(b, st, d_par.as<int32_t>(), d_dist.as<uint32_t>());
   OGB_CUDA(cudaGetLastError());
-  OGB_TRY(read_state(w, s));
-  *nf = h->ctl.nf;
+  OGB_CUDA(cudaMemcpyAsync(w->h_state, w->state.p, offsetof(BfsDevState, trace), cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  *nf = w->h_state->aux.nf;
   OGB_CUDA(cudaMemcpyAsync(bm_next, w->bm1.p, words * 4, cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaMemcpyAsync(parents, d_par.p, (size_t)V * 4, cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaMemcpyAsync(distances, d_dist.p, (size_t)V * 4, cudaMemcpyDeviceToHost, s));
