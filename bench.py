@@ -126,6 +126,21 @@ def bfs_bytes(trace, V: int) -> tuple[float, dict]:
     return total, per_dir
 
 
+def profiled_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` (dram__bytes_read.sum +
+    dram__bytes_write.sum) from its committed ncu summary, a line
+    `dram_bytes_per_launch: N` in profiles/<kernel>_*.md; None if absent."""
+    import glob
+    for f in sorted(glob.glob(os.path.join(ROOT, "profiles", f"{kernel}_*.md"))):
+        for line in open(f):
+            if line.strip().startswith("dram_bytes_per_launch:"):
+                try:
+                    return int(line.split(":", 1)[1].strip().split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -161,7 +176,6 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
     par = torch.empty(V, dtype=torch.int32, device=dev)
     dis = torch.empty(V, dtype=torch.int32, device=dev)
-    lib.ogb_set_level_timing(1)
 
     def sweep():
         tot_ms, tot_edges, launches = 0.0, 0, 0
@@ -204,7 +218,7 @@ def run_ours(args):
         max_ms, all_edges = my_ms, float(edges_total)
     gteps = all_edges / (max_ms / 1e3) / 1e9
 
-    # ---- roofline of the dominant BFS kernel (bottom-up steps) -----------
+    # ---- roofline of the dominant kernel: bfsk_search, one launch = one search
     bu_bytes = bu_ms = td_bytes = td_ms = 0.0
     for tr in traces:
         _, per = bfs_bytes(tr, V)
@@ -214,7 +228,8 @@ def run_ours(args):
         td_ms += sum(L["ms"] for L in tr if L["direction"] == 0)
     all_bytes = sum(bfs_bytes(tr, V)[0] for tr in traces)
     sweep_ms = step_ms[-1]
-    bu_gbs = bu_bytes / (bu_ms / 1e3) / 1e9 if bu_ms else 0.0
+    search_gbs = all_bytes / (sweep_ms / 1e3) / 1e9 if sweep_ms else 0.0
+    traffic = profiled_traffic("bfsk_search")
 
     # ---- e2e: the reference-facing C-ABI call with host buffers ----------
     e2e = e2e_dropin(lib, og, s, d, w, roots, rank, dev)
@@ -252,12 +267,15 @@ def run_ours(args):
                    "global_batch": NROOTS * ws, "seq_len": None, "parallelism": f"replicas{ws}",
                    "l2": "flushed (256 MB write) before every search",
                    "step": f"{NROOTS} DO-BFS searches"},
-        "roofline": {"bound": "hbm", "kernel": "bfs_bu (bottom-up steps)", "achieved": round(bu_gbs, 1),
-                     "peak": hbm_peak, "unit": "GB/s", "frac": round(bu_gbs / hbm_peak, 4),
-                     "peak_kind": peak_kind, "traffic": None,
-                     "bfs_all_kernels_gbs": round(all_bytes / (sweep_ms / 1e3) / 1e9, 1),
-                     "bu_share_of_search_time": round(bu_ms / sweep_ms, 3) if sweep_ms else None,
-                     "td_gbs": round(td_bytes / (td_ms / 1e3) / 1e9, 1) if td_ms else None},
+        "roofline": {"bound": "hbm", "kernel": "bfsk_search (one DO-BFS search per launch)",
+                     "achieved": round(search_gbs, 1), "peak": hbm_peak, "unit": "GB/s",
+                     "frac": round(search_gbs / hbm_peak, 4), "peak_kind": peak_kind,
+                     "traffic": traffic,
+                     "algorithmic_bytes_per_launch": int(all_bytes / len(traces)) if traces else None,
+                     "ms_per_launch": round(sweep_ms / len(traces), 4) if traces else None,
+                     "bu_levels_gbs": round(bu_bytes / (bu_ms / 1e3) / 1e9, 1) if bu_ms else None,
+                     "td_levels_gbs": round(td_bytes / (td_ms / 1e3) / 1e9, 1) if td_ms else None,
+                     "bu_share_of_search_time": round(bu_ms / sweep_ms, 3) if sweep_ms else None},
         "e2e": e2e,
         "gpu_launches": int(launches_total),
         "clocks": clk,
@@ -434,6 +452,58 @@ def run_reference(args):
     }), flush=True)
 
 
+def run_case(args):
+    """One hot-path kernel family on its own, for profiler captures: `bfs`
+    runs --n DO-BFS searches, `pr-pull` / `pr-push` one PageRank run of --n
+    iterations, `build` --n sort + CSR builds, all on the seeded RMAT graph
+    of --scale.  Prints one JSON line with the device times."""
+    import torch
+    import opengraph_b200 as og
+    dev = torch.device("cuda", 0)
+    lib = og.load(True)
+    lib.quiet(True)
+    s, d, w = og.generate_rmat(args.scale, EDGE_FACTOR, SEED, weighted=True)
+    V, E = 1 << args.scale, len(s)
+    ts = torch.from_numpy(s.view(np.int32)).to(dev)
+    td = torch.from_numpy(d.view(np.int32)).to(dev)
+    tw = torch.from_numpy(w).to(dev)
+    g = lib.device_graph()
+    out = {"case": args.case, "scale": args.scale, "V": V, "E": E, "n": args.n}
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.case == "build":
+        times = []
+        for _ in range(args.n):
+            start.record()
+            g.build(ts, td, V, 0, weight=tw)
+            stop.record()
+            torch.cuda.synchronize()
+            times.append(round(start.elapsed_time(stop), 4))
+        out["ms"] = times
+    else:
+        g.build(ts, td, V, 0, weight=tw)
+        torch.cuda.synchronize()
+        if args.case == "bfs":
+            outdeg = g.view(False).out_degree.cpu().numpy().view(np.uint32)
+            rng = np.random.default_rng(1000)
+            roots = [int(x) for x in rng.choice(np.nonzero(outdeg > 0)[0], size=args.n, replace=False)]
+            par = torch.empty(V, dtype=torch.int32, device=dev)
+            dis = torch.empty(V, dtype=torch.int32, device=dev)
+            res = []
+            for r in roots:
+                info = g.bfs(r, par, dis, mode=2)
+                nbytes, _ = bfs_bytes(g.bfs_trace(), V)
+                res.append({"root": r, "ms": round(info["ms"], 4), "algorithmic_bytes": int(nbytes),
+                            "reached_out_edges": int(info["reached_out_edges"])})
+            out["searches"] = res
+        else:
+            ranks = torch.empty(V, dtype=torch.float32, device=dev)
+            mode = 0 if args.case == "pr-pull" else 1
+            info = g.pagerank(ranks, mode=mode, max_iterations=args.n, epsilon=0.0)
+            out["ms_per_iteration"] = round(info["ms"] / max(args.n, 1), 4)
+    g.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -443,9 +513,15 @@ def main():
     ap.add_argument("--cpu-roots", type=int, default=8)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-stages", action="store_true")
+    ap.add_argument("--case", default="full", choices=["full", "bfs", "pr-pull", "pr-push", "build"],
+                    help="full = the benchmark line; the others run one kernel family for profiling")
+    ap.add_argument("--scale", type=int, default=SCALE, help="RMAT scale of a --case run")
+    ap.add_argument("--n", type=int, default=3, help="searches / iterations / builds of a --case run")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    if args.impl == "reference":
+    if args.case != "full":
+        run_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

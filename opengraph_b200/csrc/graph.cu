@@ -148,6 +148,7 @@ int graph_build(DevGraph& g, const uint32_t* in_src, const uint32_t* in_dst, con
   g.E = E;
   g.weighted = weighted;
   g.sort_type = sort_type;
+  g.build_id++;
   OGB_TRY(reserve_csr(g.fwd, V, E, weighted));
   OGB_TRY(reserve_csr(g.inv, V, E, weighted));
   OGB_TRY(g.err.alloc(16));

@@ -47,6 +47,7 @@ struct DevGraph {
   SortWorkspace sort_ws;
   DevBuf input_src, input_dst, input_w;  // staging of host uploads
   DevBuf err;                            // u32 error word of the build kernels
+  uint32_t build_id = 0;  // bumped whenever the edges change (caches key on it)
   BfsWork* bfs = nullptr;
   PrWork* pr = nullptr;
   // traces of the last BFS / PageRank run through the device API
@@ -145,5 +146,7 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
 // heavy rows per warp, very heavy rows per CTA of cta_threads threads).
 void pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr);
 void pagerank_get_bins(uint32_t* warp_thr, uint32_t* cta_thr, uint32_t* cta_threads, uint32_t* chunk);
+void pagerank_set_hot_limit(uint32_t max_vertices);
+uint32_t pagerank_get_hot_limit();
 
 }  // namespace ogb

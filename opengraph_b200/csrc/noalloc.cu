@@ -13,11 +13,11 @@
 // (kScratchBytes below, about 12.6 MB) until the process exits.
 //
 // The computation is the library's pull PageRank (pageRank.c:939-1062
-// semantics) with the same work split and summation order as
-// pagerank_run's pull kernel at its default thresholds (rows <= 32 edges
-// summed by one thread in CSR order, rows <= 2048 by a warp, longer rows by a
-// 256-thread CTA), reading the row start and length arrays directly instead
-// of the packed rows of a DevGraph.
+// semantics) with the row split of pagerank_run's pull kernel at its default
+// thresholds (rows <= 32 edges summed by one thread in CSR order, rows <= 2048
+// by a warp, both in the same order as that kernel; longer rows by one
+// 256-thread CTA, where that kernel cuts them into chunks), reading the row
+// start and length arrays directly instead of the packed rows of a DevGraph.
 //
 // Calls share the one array and each call overwrites what the previous one
 // left there; two calls whose work overlaps on the GPU (different streams, or

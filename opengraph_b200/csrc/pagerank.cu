@@ -29,8 +29,19 @@
 //     iteration, and every sum has one fixed order (deterministic).
 // Every strided loop issues four independent gathers before it adds them, in
 // the same order as the plain loop, so the order is unchanged.
-// Chunk CTAs come first in the grid, then warp rows, then light rows, so the
-// long-latency work starts first.  Iterations are launched back to back
+// Pull gathers one contrib value per edge, at random, so it is bound by
+// memory latency more than by HBM bandwidth.  Pull therefore runs on a
+// re-laid copy of the inverse neighbour array (built once per graph): source
+// ids renumbered by descending out-degree, so the contribs of the sources of
+// most edges share few cache lines (contrib is kept in that numbering; a
+// pull CTA can also stage the leading renumbered sources in shared memory,
+// off by default), and the rows of in-degree <= warp_thr stored first and
+// contiguous, so a warp loads the edges of 128 light rows with coalesced
+// loads and gathers them 256 at a time (light rows were the latency tail of
+// the iteration: a lane walked its row one dependent gather per step).  The
+// rows, their order and every summation order are unchanged, so the results
+// are bit-identical.  Pull runs one 1024-thread CTA per SM; it takes chunks
+// first (four 256-thread groups per CTA), then warp rows, then light rows.  Iterations are launched back to back
 // without host round trips: each iteration's last CTA records error/active
 // and, when active == 0, sets a stop flag that later launches read first.
 #include "graph.cuh"
@@ -41,13 +52,26 @@
 namespace ogb {
 
 constexpr uint32_t kPrMaxIters = 1024;
-constexpr int kPrThreads = 256;
+constexpr int kPrThreads = 256;      // push kernels
+constexpr int kPullThreads = 1024;   // pull: one CTA per SM
+constexpr int kPullGroup = 256;      // threads per chunk group (the oracle's cta_threads)
+constexpr int kPullGroups = kPullThreads / kPullGroup;
+constexpr uint32_t kStage = 256;     // staged light edges per warp and window
+constexpr int kLightR = 4;           // light rows per lane (128 per warp unit)
 constexpr uint32_t kPrChunk = 8192;  // edges per chunk of a very heavy row
 
 // Row-length thresholds of the work split (settable; the GPU-order mode of
 // the oracle takes the same values).
 static uint32_t g_warp_thr = 32;
 static uint32_t g_cta_thr = 2048;
+
+// Upper bound on the renumbered sources whose contrib a pull CTA stages in
+// shared memory.  Default 0: on RMAT-22 staging the leading 4k..57k sources
+// measured 0.38..0.44 ms per iteration against 0.38 ms without (the shared
+// memory it takes is L1 the gathers lose).
+static uint32_t g_hot_limit = 0;
+void pagerank_set_hot_limit(uint32_t max_vertices) { g_hot_limit = max_vertices; }
+uint32_t pagerank_get_hot_limit() { return g_hot_limit; }
 
 void pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr) {
   g_warp_thr = warp_thr;
@@ -56,7 +80,7 @@ void pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr) {
 void pagerank_get_bins(uint32_t* warp_thr, uint32_t* cta_thr, uint32_t* cta_threads, uint32_t* chunk) {
   *warp_thr = g_warp_thr;
   *cta_thr = g_cta_thr;
-  *cta_threads = kPrThreads;
+  *cta_threads = kPullGroup;
   *chunk = kPrChunk;
 }
 
@@ -75,7 +99,12 @@ struct PrChunkItem {
 struct PrWork {
   uint32_t V = 0;
   int listed_pull = -1;                // direction the lists describe
-  uint32_t listed_warp = 0, listed_cta = 0;
+  uint32_t listed_warp = 0, listed_cta = 0, listed_build = 0;
+  // pull: source ids renumbered by descending out-degree
+  uint32_t rl_build = 0, rl_warp = 0;
+  bool rl_ready = false;
+  DevBuf perm, nbr_rl, rows_rl, off_light, rl_keys, rl_ids, rl_tmp;
+  uint32_t hot_max = 0;                // leading renumbered vertices that fit in shared memory
   DevBuf contrib0, contrib1, next, ctl;
   DevBuf heavy;                        // vertex ids of the warp rows (n_warp), then the chunked rows
   DevBuf chunks;                       // PrChunkItem per chunk
@@ -133,23 +162,25 @@ struct PrParams {
   uint32_t warp_thr;
 };
 
+// contrib_next is indexed by renumbered id when perm is given.
 __device__ __forceinline__ void pr_update(uint32_t v, float s, float* __restrict__ pr,
                                           const uint32_t* __restrict__ out_degree,
                                           float* __restrict__ contrib_next, const PrParams& p, double& err,
-                                          uint32_t& active) {
+                                          uint32_t& active, const uint32_t* __restrict__ perm = nullptr) {
   const float nv = __fadd_rn(p.base_pr, __fmul_rn(p.damp, s));
   const float prev = pr[v];
   pr[v] = nv;
   const uint32_t d = out_degree[v];
-  contrib_next[v] = d ? __fdiv_rn(nv, (float)d) : 0.0f;
+  contrib_next[perm ? perm[v] : v] = d ? __fdiv_rn(nv, (float)d) : 0.0f;
   const double e = fabs((double)__fsub_rn(nv, prev));
   err += e / (double)p.V;
   active += (e >= p.epsilon) ? 1u : 0u;
 }
 
+template <int NT = kPrThreads>
 __device__ __forceinline__ void pr_block_finish(double err, uint32_t active, PrCtl* ctl, uint32_t it) {
-  __shared__ double s_err[kPrThreads / 32];
-  __shared__ uint32_t s_act[kPrThreads / 32];
+  __shared__ double s_err[NT / 32];
+  __shared__ uint32_t s_act[NT / 32];
   for (int o = 16; o; o >>= 1) {
     err += __shfl_down_sync(0xffffffffu, err, o);
     active += __shfl_down_sync(0xffffffffu, active, o);
@@ -163,7 +194,7 @@ __device__ __forceinline__ void pr_block_finish(double err, uint32_t active, PrC
   if (threadIdx.x == 0) {
     double e = 0;
     uint32_t a = 0;
-    for (int w = 0; w < kPrThreads / 32; w++) {
+    for (int w = 0; w < NT / 32; w++) {
       e += s_err[w];
       a += s_act[w];
     }
@@ -181,23 +212,34 @@ __device__ __forceinline__ void pr_block_finish(double err, uint32_t active, PrC
   }
 }
 
-// s += c[nbr[j]] for j = j0, j0+STRIDE, ... < j1, in that order, with four
-// gathers in flight.
+// contrib of renumbered source u: shared memory for the leading `hot` ids.
+__device__ __forceinline__ float ld_c(const float* s_hot, uint32_t hot, const float* __restrict__ c, uint32_t u) {
+  float x;
+  if (u < hot)
+    x = s_hot[u];
+  else
+    x = __ldg(&c[u]);
+  return x;
+}
+
+// s += c[nbr[j]] for j = j0, j0+STRIDE, ... < j1, in that order; each step
+// issues four predicated neighbour loads, then their four gathers (no
+// serial tail loop: a row of 33..128 edges is one step).
 template <uint32_t STRIDE>
-__device__ __forceinline__ float strided_sum(const float* __restrict__ c, const uint32_t* __restrict__ nbr,
-                                             uint32_t j0, uint32_t j1) {
+__device__ __forceinline__ float strided_sum(const float* s_hot, uint32_t hot, const float* __restrict__ c,
+                                             const uint32_t* __restrict__ nbr, uint32_t j0, uint32_t j1) {
   float s = 0.0f;
-  uint32_t j = j0;
-  for (; j + 3 * STRIDE < j1; j += 4 * STRIDE) {
-    const uint32_t a = nbr[j] & 0x3FFFFFFFu, b = nbr[j + STRIDE] & 0x3FFFFFFFu;
-    const uint32_t d = nbr[j + 2 * STRIDE] & 0x3FFFFFFFu, e = nbr[j + 3 * STRIDE] & 0x3FFFFFFFu;
-    const float ca = c[a], cb = c[b], cd = c[d], ce = c[e];
-    s = __fadd_rn(s, ca);
-    s = __fadd_rn(s, cb);
-    s = __fadd_rn(s, cd);
-    s = __fadd_rn(s, ce);
+  for (uint32_t j = j0; j < j1; j += 4 * STRIDE) {
+    uint32_t x[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) x[k] = (j + k * STRIDE < j1) ? __ldg(&nbr[j + k * STRIDE]) : 0u;
+    float cx[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) cx[k] = (j + k * STRIDE < j1) ? ld_c(s_hot, hot, c, x[k]) : 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (j + k * STRIDE < j1) s = __fadd_rn(s, cx[k]);
   }
-  for (; j < j1; j += STRIDE) s = __fadd_rn(s, c[nbr[j] & 0x3FFFFFFFu]);
   return s;
 }
 
@@ -208,155 +250,346 @@ __device__ __forceinline__ float warp_fold(float s) {
 }
 
 // Two strided sums at once (rows A and B of one warp), each in the order of
-// strided_sum<32>: eight gathers in flight per lane instead of four.
-__device__ __forceinline__ void strided_sum2(const float* __restrict__ c, const uint32_t* __restrict__ nbr,
-                                             uint32_t a0, uint32_t a1, uint32_t b0, uint32_t b1, float& sa,
-                                             float& sb) {
+// strided_sum<32>: eight gathers in flight per lane.
+__device__ __forceinline__ void strided_sum2(const float* s_hot, uint32_t hot, const float* __restrict__ c,
+                                             const uint32_t* __restrict__ nbr, uint32_t a0, uint32_t a1,
+                                             uint32_t b0, uint32_t b1, float& sa, float& sb) {
   constexpr uint32_t S = 32;
   sa = 0.0f;
   sb = 0.0f;
-  uint32_t ja = a0, jb = b0;
-  while (ja + 3 * S < a1 && jb + 3 * S < b1) {
-    const uint32_t x0 = nbr[ja] & 0x3FFFFFFFu, x1 = nbr[ja + S] & 0x3FFFFFFFu;
-    const uint32_t x2 = nbr[ja + 2 * S] & 0x3FFFFFFFu, x3 = nbr[ja + 3 * S] & 0x3FFFFFFFu;
-    const uint32_t y0 = nbr[jb] & 0x3FFFFFFFu, y1 = nbr[jb + S] & 0x3FFFFFFFu;
-    const uint32_t y2 = nbr[jb + 2 * S] & 0x3FFFFFFFu, y3 = nbr[jb + 3 * S] & 0x3FFFFFFFu;
-    const float cx0 = c[x0], cx1 = c[x1], cx2 = c[x2], cx3 = c[x3];
-    const float cy0 = c[y0], cy1 = c[y1], cy2 = c[y2], cy3 = c[y3];
-    sa = __fadd_rn(sa, cx0);
-    sa = __fadd_rn(sa, cx1);
-    sa = __fadd_rn(sa, cx2);
-    sa = __fadd_rn(sa, cx3);
-    sb = __fadd_rn(sb, cy0);
-    sb = __fadd_rn(sb, cy1);
-    sb = __fadd_rn(sb, cy2);
-    sb = __fadd_rn(sb, cy3);
-    ja += 4 * S;
-    jb += 4 * S;
+  for (uint32_t ja = a0, jb = b0; ja < a1 || jb < b1; ja += 4 * S, jb += 4 * S) {
+    uint32_t x[4], y[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      x[k] = (ja + k * S < a1) ? __ldg(&nbr[ja + k * S]) : 0u;
+      y[k] = (jb + k * S < b1) ? __ldg(&nbr[jb + k * S]) : 0u;
+    }
+    float cx[4], cy[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      cx[k] = (ja + k * S < a1) ? ld_c(s_hot, hot, c, x[k]) : 0.0f;
+      cy[k] = (jb + k * S < b1) ? ld_c(s_hot, hot, c, y[k]) : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      if (ja + k * S < a1) sa = __fadd_rn(sa, cx[k]);
+      if (jb + k * S < b1) sb = __fadd_rn(sb, cy[k]);
+    }
   }
-  // tails, each in its own order (identical to continuing strided_sum<32>)
-  for (; ja + 3 * S < a1; ja += 4 * S) {
-    const uint32_t x0 = nbr[ja] & 0x3FFFFFFFu, x1 = nbr[ja + S] & 0x3FFFFFFFu;
-    const uint32_t x2 = nbr[ja + 2 * S] & 0x3FFFFFFFu, x3 = nbr[ja + 3 * S] & 0x3FFFFFFFu;
-    const float cx0 = c[x0], cx1 = c[x1], cx2 = c[x2], cx3 = c[x3];
-    sa = __fadd_rn(sa, cx0);
-    sa = __fadd_rn(sa, cx1);
-    sa = __fadd_rn(sa, cx2);
-    sa = __fadd_rn(sa, cx3);
-  }
-  for (; jb + 3 * S < b1; jb += 4 * S) {
-    const uint32_t y0 = nbr[jb] & 0x3FFFFFFFu, y1 = nbr[jb + S] & 0x3FFFFFFFu;
-    const uint32_t y2 = nbr[jb + 2 * S] & 0x3FFFFFFFu, y3 = nbr[jb + 3 * S] & 0x3FFFFFFFu;
-    const float cy0 = c[y0], cy1 = c[y1], cy2 = c[y2], cy3 = c[y3];
-    sb = __fadd_rn(sb, cy0);
-    sb = __fadd_rn(sb, cy1);
-    sb = __fadd_rn(sb, cy2);
-    sb = __fadd_rn(sb, cy3);
-  }
-  for (; ja < a1; ja += S) sa = __fadd_rn(sa, c[nbr[ja] & 0x3FFFFFFFu]);
-  for (; jb < b1; jb += S) sb = __fadd_rn(sb, c[nbr[jb] & 0x3FFFFFFFu]);
 }
 
-// Pull iteration, one grid: blocks [0, nb_chunk) reduce chunks of very heavy
-// rows, the next nb_warp blocks the warp rows, the rest walk all vertices in
-// order and take the light rows.
-__global__ void __launch_bounds__(kPrThreads) pr_pull_kernel(
-    uint32_t nb_chunk, uint32_t nb_warp, const uint32_t* __restrict__ heavy, uint32_t n_warp,
-    const PrChunkItem* __restrict__ chunks, uint32_t n_chunks, const uint32_t* __restrict__ vfirst,
-    const uint32_t* __restrict__ vcount, uint32_t* __restrict__ done, float* __restrict__ partials,
-    const uint2* __restrict__ rows, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ out_degree,
-    const float* __restrict__ contrib, float* __restrict__ contrib_next, float* __restrict__ pr, PrParams p,
-    PrCtl* __restrict__ ctl, uint32_t it) {
-  __shared__ float s_part[kPrThreads / 32];
-  __shared__ uint32_t s_last;
+// Update inputs of vertex v, loaded before its sum is ready.
+struct PrVtx {
+  float prev;
+  uint32_t deg, pm;
+};
+__device__ __forceinline__ PrVtx pr_vtx(uint32_t v, const float* __restrict__ pr, const uint32_t* __restrict__ out_degree,
+                                        const uint32_t* __restrict__ perm) {
+  PrVtx x;
+  x.prev = pr[v];
+  x.deg = __ldg(&out_degree[v]);
+  x.pm = __ldg(&perm[v]);
+  return x;
+}
+// pr_update with preloaded inputs (contrib_next at the renumbered id).
+__device__ __forceinline__ void pr_update_pre(uint32_t v, float s, const PrVtx& x, float* __restrict__ pr,
+                                              float* __restrict__ contrib_next, const PrParams& p, double& err,
+                                              uint32_t& active) {
+  const float nv = __fadd_rn(p.base_pr, __fmul_rn(p.damp, s));
+  pr[v] = nv;
+  contrib_next[x.pm] = x.deg ? __fdiv_rn(nv, (float)x.deg) : 0.0f;
+  const double e = fabs((double)__fsub_rn(nv, x.prev));
+  err += e / (double)p.V;
+  active += (e >= p.epsilon) ? 1u : 0u;
+}
+
+
+// Pull iteration, one CTA per SM (1024 threads).  Shared memory holds the
+// contrib of renumbered sources [0, hot) and one stage of kStage floats per
+// warp.  Work, each kind strided over the grid:
+//  (1) chunks of very heavy rows, one 256-thread group per chunk (four
+//      chunks in flight per CTA), lanes strided, warps folded, the group's
+//      warps summed in order, the chunk sums in chunk order by the group that
+//      finishes a row's last chunk;
+//  (2) warp rows, a warp per two rows, lanes strided, butterfly-folded;
+//  (3) light rows, a warp per 128 consecutive vertices: their edges are
+//      contiguous in the light segment of nbr (off_light), so the warp loads
+//      them coalesced and gathers kStage contribs at a time into its stage,
+//      then each lane adds its four rows' values in CSR order.
+// rows (renumbered layout), pr and out_degree are in original vertex order;
+// contrib / contrib_next are indexed by renumbered id.
+__global__ void __launch_bounds__(kPullThreads, 1) pr_pull_kernel(
+    uint32_t hot, const uint32_t* __restrict__ heavy, uint32_t n_warp, const PrChunkItem* __restrict__ chunks,
+    uint32_t n_chunks, const uint32_t* __restrict__ vfirst, const uint32_t* __restrict__ vcount,
+    uint32_t* __restrict__ done, float* __restrict__ partials, const uint2* __restrict__ rows,
+    const uint32_t* __restrict__ off_light, const uint32_t* __restrict__ nbr,
+    const uint32_t* __restrict__ out_degree, const uint32_t* __restrict__ perm, const float* __restrict__ contrib,
+    float* __restrict__ contrib_next, float* __restrict__ pr, PrParams p, PrCtl* __restrict__ ctl, uint32_t it) {
+  extern __shared__ float4 s_dyn4[];
+  float* s_stage = reinterpret_cast<float*>(s_dyn4);  // kPullThreads / 32 stages
+  const float* s_hot = s_stage + (kPullThreads / 32) * kStage;
+  __shared__ float s_part[kPullGroups][kPullGroup / 32];
+  __shared__ uint32_t s_last[kPullGroups];
   if (ctl->stop) return;
+  {
+    float4* h4 = s_dyn4 + (kPullThreads / 32) * kStage / 4;
+    for (uint32_t i = threadIdx.x; i < hot / 4; i += kPullThreads) h4[i] = __ldg(reinterpret_cast<const float4*>(contrib) + i);
+  }
+  __syncthreads();
   double err = 0.0;
   uint32_t active = 0;
-  const uint32_t b = blockIdx.x;
-  if (b < nb_chunk) {
-    for (uint32_t g = b; g < n_chunks; g += nb_chunk) {
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+
+  // (1) chunks of very heavy rows, one group per chunk
+  {
+    const uint32_t grp = threadIdx.x / kPullGroup, gt = threadIdx.x % kPullGroup;
+    for (uint32_t g = blockIdx.x * kPullGroups + grp; g < n_chunks; g += gridDim.x * kPullGroups) {
       const PrChunkItem ci = chunks[g];
-      float s = strided_sum<kPrThreads>(contrib, nbr, ci.j0 + threadIdx.x, ci.j1);
-      s = warp_fold(s);
-      if (lane_id() == 0) s_part[threadIdx.x >> 5] = s;
-      __syncthreads();
-      if (threadIdx.x == 0) {
+      float sum = strided_sum<kPullGroup>(s_hot, hot, contrib, nbr, ci.j0 + gt, ci.j1);
+      sum = warp_fold(sum);
+      if (lane == 0) s_part[grp][gt >> 5] = sum;
+      asm volatile("bar.sync %0, %1;" ::"r"(grp + 1), "r"(kPullGroup) : "memory");
+      if (gt == 0) {
         float tot = 0.0f;
-        for (int w = 0; w < kPrThreads / 32; w++) tot = __fadd_rn(tot, s_part[w]);
+        for (int w = 0; w < kPullGroup / 32; w++) tot = __fadd_rn(tot, s_part[grp][w]);
         partials[g] = tot;
         __threadfence();
         const uint32_t cnt = vcount[ci.k];
-        s_last = (atomicAdd(&done[ci.k], 1u) == cnt - 1) ? 1u : 0u;
-        if (s_last) {
+        s_last[grp] = (atomicAdd(&done[ci.k], 1u) == cnt - 1) ? 1u : 0u;
+        if (s_last[grp]) {
           __threadfence();
           const uint32_t f = vfirst[ci.k];
-          float sum = 0.0f;
-          for (uint32_t c = 0; c < cnt; c++) sum = __fadd_rn(sum, __ldcg(&partials[f + c]));
+          float rs = 0.0f;
+          for (uint32_t c = 0; c < cnt; c++) rs = __fadd_rn(rs, __ldcg(&partials[f + c]));
           done[ci.k] = 0;
-          pr_update(ci.v, sum, pr, out_degree, contrib_next, p, err, active);
+          pr_update(ci.v, rs, pr, out_degree, contrib_next, p, err, active, perm);
         }
       }
-      __syncthreads();
-    }
-  } else if (b < nb_chunk + nb_warp) {
-    // a warp reduces two rows at a time (t and t + wstride)
-    const uint32_t lane = lane_id();
-    const uint32_t w0 = (b - nb_chunk) * (kPrThreads / 32) + (threadIdx.x >> 5);
-    const uint32_t wstride = nb_warp * (kPrThreads / 32);
-    for (uint32_t t = w0; t < n_warp; t += 2 * wstride) {
-      const uint32_t va = heavy[t];
-      const bool has_b = t + wstride < n_warp;
-      const uint32_t vb = has_b ? heavy[t + wstride] : va;
-      const uint2 ra = rows[va];
-      const uint2 rb = has_b ? rows[vb] : make_uint2(0, 0);
-      float sa, sb;
-      strided_sum2(contrib, nbr, ra.x + lane, ra.x + ra.y, rb.x + lane, rb.x + rb.y, sa, sb);
-      sa = warp_fold(sa);
-      sb = warp_fold(sb);
-      if (lane == 0) {
-        pr_update(va, sa, pr, out_degree, contrib_next, p, err, active);
-        if (has_b) pr_update(vb, sb, pr, out_degree, contrib_next, p, err, active);
-      }
-    }
-  } else {
-    // light rows: a warp takes 128 consecutive vertices, each lane four rows
-    // (lane, lane+32, lane+64, lane+96) reduced side by side, every row
-    // sequentially in CSR order from 0.0f
-    constexpr int R = 4;
-    const uint32_t lane = lane_id();
-    const uint32_t lw = (b - nb_chunk - nb_warp) * (kPrThreads / 32) + (threadIdx.x >> 5);
-    const uint32_t nlw = (gridDim.x - nb_chunk - nb_warp) * (kPrThreads / 32);
-    for (uint32_t base = lw * (32 * R); base < p.V; base += nlw * (32 * R)) {
-      uint32_t a[R], d[R], dmax = 0;
-      float s[R];
-#pragma unroll
-      for (int k = 0; k < R; k++) {
-        const uint32_t v = base + k * 32 + lane;
-        const uint2 r = (v < p.V) ? rows[v] : make_uint2(0, 0);
-        a[k] = r.x;
-        d[k] = (v < p.V && r.y <= p.warp_thr) ? r.y : 0u;
-        s[k] = 0.0f;
-        dmax = max(dmax, d[k]);
-      }
-      for (uint32_t i = 0; i < dmax; i++) {
-        uint32_t u[R];
-#pragma unroll
-        for (int k = 0; k < R; k++) u[k] = (i < d[k]) ? (nbr[a[k] + i] & 0x3FFFFFFFu) : 0u;
-        float c[R];
-#pragma unroll
-        for (int k = 0; k < R; k++) c[k] = (i < d[k]) ? contrib[u[k]] : 0.0f;
-#pragma unroll
-        for (int k = 0; k < R; k++)
-          if (i < d[k]) s[k] = __fadd_rn(s[k], c[k]);
-      }
-#pragma unroll
-      for (int k = 0; k < R; k++) {
-        const uint32_t v = base + k * 32 + lane;
-        if (v < p.V && rows[v].y <= p.warp_thr) pr_update(v, s[k], pr, out_degree, contrib_next, p, err, active);
-      }
+      asm volatile("bar.sync %0, %1;" ::"r"(grp + 1), "r"(kPullGroup) : "memory");
     }
   }
-  pr_block_finish(err, active, ctl, it);
+
+  // (2) warp rows: a warp reduces two rows at a time (t and t + nw)
+  const uint32_t gw = blockIdx.x * (kPullThreads / 32) + warp;
+  const uint32_t nw = gridDim.x * (kPullThreads / 32);
+  for (uint32_t t = gw; t < n_warp; t += 2 * nw) {
+    const uint32_t va = heavy[t];
+    const bool has_b = t + nw < n_warp;
+    const uint32_t vb = has_b ? heavy[t + nw] : va;
+    const uint2 ra = rows[va];
+    const uint2 rb = has_b ? rows[vb] : make_uint2(0, 0);
+    PrVtx xa, xb;
+    if (lane == 0) {
+      xa = pr_vtx(va, pr, out_degree, perm);
+      xb = pr_vtx(vb, pr, out_degree, perm);
+    }
+    float sa, sb;
+    strided_sum2(s_hot, hot, contrib, nbr, ra.x + lane, ra.x + ra.y, rb.x + lane, rb.x + rb.y, sa, sb);
+    sa = warp_fold(sa);
+    sb = warp_fold(sb);
+    if (lane == 0) {
+      pr_update_pre(va, sa, xa, pr, contrib_next, p, err, active);
+      if (has_b) pr_update_pre(vb, sb, xb, pr, contrib_next, p, err, active);
+    }
+  }
+
+  // (3) light rows, staged
+  float* stage = s_stage + warp * kStage;
+  for (uint32_t base = gw * (32 * kLightR); base < p.V; base += nw * (32 * kLightR)) {
+    const uint32_t vend = min(base + 32 * kLightR, p.V);
+    uint32_t st[kLightR], en[kLightR];
+    bool light[kLightR];
+    PrVtx x[kLightR];
+    float s[kLightR];
+#pragma unroll
+    for (int k = 0; k < kLightR; k++) {
+      const uint32_t v = base + k * 32 + lane;
+      st[k] = en[k] = 0;
+      light[k] = false;
+      s[k] = 0.0f;
+      if (v < p.V) {
+        light[k] = rows[v].y <= p.warp_thr;
+        st[k] = off_light[v];
+        en[k] = off_light[v + 1];
+        if (light[k]) x[k] = pr_vtx(v, pr, out_degree, perm);
+      }
+    }
+    const uint32_t seg0 = off_light[base], seg1 = off_light[vend];
+    for (uint32_t w0 = seg0; w0 < seg1; w0 += kStage) {
+      const uint32_t w1 = min(w0 + kStage, seg1);
+      uint32_t u[kStage / 32];
+#pragma unroll
+      for (uint32_t m = 0; m < kStage / 32; m++) {
+        const uint32_t j = w0 + m * 32 + lane;
+        u[m] = j < w1 ? __ldg(&nbr[j]) : 0u;
+      }
+      float c[kStage / 32];
+#pragma unroll
+      for (uint32_t m = 0; m < kStage / 32; m++) {
+        const uint32_t j = w0 + m * 32 + lane;
+        c[m] = j < w1 ? ld_c(s_hot, hot, contrib, u[m]) : 0.0f;
+      }
+#pragma unroll
+      for (uint32_t m = 0; m < kStage / 32; m++) stage[m * 32 + lane] = c[m];
+      __syncwarp();
+      uint32_t lo[kLightR], n[kLightR], nmax = 0;
+#pragma unroll
+      for (int k = 0; k < kLightR; k++) {
+        lo[k] = max(st[k], w0);
+        const uint32_t hi = min(en[k], w1);
+        n[k] = hi > lo[k] ? hi - lo[k] : 0u;
+        nmax = max(nmax, n[k]);
+      }
+      for (uint32_t i = 0; i < nmax; i++) {
+#pragma unroll
+        for (int k = 0; k < kLightR; k++)
+          if (i < n[k]) s[k] = __fadd_rn(s[k], stage[lo[k] - w0 + i]);
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int k = 0; k < kLightR; k++)
+      if (light[k]) pr_update_pre(base + k * 32 + lane, s[k], x[k], pr, contrib_next, p, err, active);
+  }
+  pr_block_finish<kPullThreads>(err, active, ctl, it);
+}
+
+// ---------------------------------------------------------------- renumbering
+
+// key = ~out_degree (ascending sort = descending degree), payload = id.
+__global__ void pr_rl_keys_kernel(uint32_t V, const uint32_t* __restrict__ out_degree, uint32_t* __restrict__ keys,
+                                  uint32_t* __restrict__ ids) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    keys[v] = ~out_degree[v];
+    ids[v] = v;
+  }
+}
+
+// perm[old id] = new id, from the sorted ids (new id -> old id).
+__global__ void pr_rl_perm_kernel(uint32_t V, const uint32_t* __restrict__ order, uint32_t* __restrict__ perm) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) perm[order[i]] = i;
+}
+
+// Row lengths split by class: light rows (in-degree <= warp_thr) and the rest.
+__global__ void pr_rl_split_kernel(uint32_t V, const uint2* __restrict__ rows, uint32_t warp_thr,
+                                   uint32_t* __restrict__ dl, uint32_t* __restrict__ dh) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const uint32_t d = rows[v].y;
+    dl[v] = d <= warp_thr ? d : 0u;
+    dh[v] = d <= warp_thr ? 0u : d;
+  }
+}
+
+// New row offsets: light rows first (vertex order), heavy rows after them.
+__global__ void pr_rl_rows_kernel(uint32_t V, const uint2* __restrict__ rows, uint32_t warp_thr,
+                                  const uint32_t* __restrict__ off_l, const uint32_t* __restrict__ off_h,
+                                  uint2* __restrict__ rows_rl) {
+  const uint32_t total_l = off_l[V];
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const uint32_t d = rows[v].y;
+    rows_rl[v] = make_uint2(d <= warp_thr ? off_l[v] : total_l + off_h[v], d);
+  }
+}
+
+// Copy every row into the new layout with renumbered source ids (a warp
+// per row).
+__global__ void pr_rl_copy_kernel(uint32_t V, const uint2* __restrict__ rows, const uint32_t* __restrict__ nbr,
+                                  const uint2* __restrict__ rows_rl, const uint32_t* __restrict__ perm,
+                                  uint32_t* __restrict__ out) {
+  const uint32_t lane = lane_id();
+  const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
+  for (uint32_t v = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); v < V; v += nwarps) {
+    const uint2 r = rows[v];
+    const uint32_t o = rows_rl[v].x;
+    for (uint32_t i = lane; i < r.y; i += 32) out[o + i] = perm[nbr[r.x + i] & 0x3FFFFFFFu];
+  }
+}
+
+// ---------------------------------------------------------------- scan ------
+
+constexpr uint32_t kScanTileN = 4096;  // 256 threads x 16
+
+__device__ __forceinline__ uint32_t block_excl_256(uint32_t v, uint32_t* s_w, uint32_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_w[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t t = lane < 8 ? s_w[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    if (lane < 8) s_w[lane] = t;
+  }
+  __syncthreads();
+  *total = s_w[7];
+  const uint32_t r = (warp ? s_w[warp - 1] : 0) + x - v;
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(256) scan_tile_sum_kernel(const uint32_t* __restrict__ in, uint32_t n,
+                                                            uint32_t* __restrict__ sums) {
+  __shared__ uint32_t s_w[8];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTileN + threadIdx.x * 16;
+  uint32_t t = 0;
+  for (int k = 0; k < 16; k++)
+    if (base + k < n) t += in[base + k];
+  uint32_t total;
+  block_excl_256(t, s_w, &total);
+  if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+// One CTA: exclusive scan of the tile sums in place; total into sums[ntiles].
+__global__ void __launch_bounds__(256) scan_sums_kernel(uint32_t* __restrict__ sums, uint32_t ntiles) {
+  __shared__ uint32_t s_w[8];
+  uint32_t carry = 0;
+  for (uint32_t b = 0; b < ntiles; b += 256) {
+    const uint32_t i = b + threadIdx.x;
+    const uint32_t v = i < ntiles ? sums[i] : 0u;
+    uint32_t total;
+    const uint32_t e = block_excl_256(v, s_w, &total);
+    if (i < ntiles) sums[i] = carry + e;
+    carry += total;
+  }
+  if (threadIdx.x == 0) sums[ntiles] = carry;
+}
+
+__global__ void __launch_bounds__(256) scan_tile_kernel(const uint32_t* __restrict__ in, uint32_t n,
+                                                        const uint32_t* __restrict__ sums, uint32_t* __restrict__ out) {
+  __shared__ uint32_t s_w[8];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTileN + threadIdx.x * 16;
+  uint32_t v[16], t = 0;
+  for (int k = 0; k < 16; k++) {
+    v[k] = base + k < n ? in[base + k] : 0u;
+    t += v[k];
+  }
+  uint32_t total;
+  uint32_t o = sums[blockIdx.x] + block_excl_256(t, s_w, &total);
+  for (int k = 0; k < 16; k++)
+    if (base + k < n) {
+      out[base + k] = o;
+      o += v[k];
+    }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = sums[gridDim.x];
+}
+
+// out[0..n] = exclusive scan of in[0..n) followed by the total (out holds
+// n + 1 entries); tmp holds n / kScanTileN + 2 words.
+static int scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t s) {
+  const uint32_t ntiles = std::max<uint32_t>(1, ceil_div(n, kScanTileN));
+  scan_tile_sum_kernel<<<ntiles, 256, 0, s>>>(in, n, tmp);
+  scan_sums_kernel<<<1, 256, 0, s>>>(tmp, ntiles);
+  scan_tile_kernel<<<ntiles, 256, 0, s>>>(in, n, tmp, out);
+  OGB_CUDA(cudaGetLastError());
+  return OK;
 }
 
 // Push scatter: contrib of each source added to its out-neighbours, split by
@@ -413,12 +646,12 @@ __global__ void __launch_bounds__(kPrThreads) pr_push_update_kernel(uint32_t V, 
 
 __global__ void pr_init_kernel(uint32_t V, const uint32_t* __restrict__ out_degree, const float* __restrict__ init,
                                float base_pr, float* __restrict__ pr, float* __restrict__ contrib,
-                               float* __restrict__ next) {
+                               float* __restrict__ next, const uint32_t* __restrict__ perm) {
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     const float x = init ? init[v] : base_pr;
     pr[v] = x;
     const uint32_t d = out_degree[v];
-    contrib[v] = d ? __fdiv_rn(x, (float)d) : 0.0f;
+    contrib[perm ? perm[v] : v] = d ? __fdiv_rn(x, (float)d) : 0.0f;
     if (next) next[v] = 0.0f;
   }
 }
@@ -431,9 +664,11 @@ __global__ void pr_normalize_kernel(uint32_t V, float* __restrict__ pr) {
 
 // Heavy lists and the chunk table of one direction (built once per graph,
 // direction and thresholds; the only host round trips of PageRank).
+// Pull lists refer to the renumbered layout (rows_rl), push lists to the
+// forward CSR.
 static int pr_build_lists(DevGraph& g, PrWork* w, bool pull, cudaStream_t s) {
   const uint32_t V = g.V;
-  const uint2* rows = pull ? g.inv.d_rows() : g.fwd.d_rows();
+  const uint2* rows = pull ? w->rows_rl.as<uint2>() : g.fwd.d_rows();
   uint32_t* cnt = w->ctl.as<uint32_t>() + sizeof(PrCtl) / 4;  // scratch words after the control block
   OGB_CUDA(cudaMemsetAsync(cnt, 0, 16, s));
   const int grid = sm_count() * 8;
@@ -477,6 +712,59 @@ static int pr_build_lists(DevGraph& g, PrWork* w, bool pull, cudaStream_t s) {
   return OK;
 }
 
+// Renumbering of the pull sources (once per graph and warp_thr): ids sorted
+// by descending out-degree (stable: ties by id), perm = old -> new; a new
+// layout of the inverse neighbour array with renumbered ids, light rows
+// (in-degree <= warp_thr) first in vertex order, then the other rows in
+// vertex order; rows_rl = {new offset, in-degree}, off_light = offsets of the
+// light rows (V + 1 entries, heavy rows empty); and the number of leading
+// renumbered ids whose contrib fits in a pull CTA's shared memory.
+static int pr_build_relabel(DevGraph& g, PrWork* w, cudaStream_t s) {
+  const uint32_t V = g.V, E = g.E;
+  OGB_TRY(w->perm.alloc((size_t)V * 4 + 16));
+  OGB_TRY(w->nbr_rl.alloc((size_t)E * 4 + 16));
+  OGB_TRY(w->rows_rl.alloc((size_t)V * 8 + 16));
+  OGB_TRY(w->off_light.alloc((size_t)V * 4 + 16));
+  OGB_TRY(w->rl_keys.alloc((size_t)V * 4 + 16));
+  OGB_TRY(w->rl_ids.alloc((size_t)V * 4 + 16));
+  OGB_TRY(w->rl_tmp.alloc((size_t)V * 8 + 64 + ((size_t)V / kScanTileN + 4) * 4));
+  const int grid = sm_count() * 8;
+  uint32_t* keys = w->rl_keys.as<uint32_t>();
+  uint32_t* ids = w->rl_ids.as<uint32_t>();
+  uint32_t* skeys = w->rl_tmp.as<uint32_t>();
+  uint32_t* order = skeys + ((V + 7) & ~3u);
+  uint32_t* scan_tmp = order + ((V + 7) & ~3u);
+  pr_rl_keys_kernel<<<grid, 256, 0, s>>>(V, g.fwd.d_out_degree(), keys, ids);
+  OGB_CUDA(cudaGetLastError());
+  KV in{keys, ids, nullptr};
+  KV out{skeys, order, nullptr};
+  OGB_TRY(sort_pairs(in, out, V, g.sort_ws, s));
+  pr_rl_perm_kernel<<<grid, 256, 0, s>>>(V, order, w->perm.as<uint32_t>());
+  // layout: keys/ids become the split lengths, skeys/order their offsets
+  pr_rl_split_kernel<<<grid, 256, 0, s>>>(V, g.inv.d_rows(), g_warp_thr, keys, ids);
+  OGB_CUDA(cudaGetLastError());
+  OGB_TRY(scan_exclusive(keys, w->off_light.as<uint32_t>(), V, scan_tmp, s));
+  OGB_TRY(scan_exclusive(ids, skeys, V, scan_tmp, s));
+  pr_rl_rows_kernel<<<grid, 256, 0, s>>>(V, g.inv.d_rows(), g_warp_thr, w->off_light.as<uint32_t>(), skeys,
+                                         w->rows_rl.as<uint2>());
+  pr_rl_copy_kernel<<<grid, 256, 0, s>>>(V, g.inv.d_rows(), g.inv.d_dst(), w->rows_rl.as<uint2>(),
+                                         w->perm.as<uint32_t>(), w->nbr_rl.as<uint32_t>());
+  OGB_CUDA(cudaGetLastError());
+  int dev = 0, optin = 0;
+  OGB_CUDA(cudaGetDevice(&dev));
+  OGB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  OGB_CUDA(cudaFuncGetAttributes(&fa, pr_pull_kernel));
+  const size_t stage_bytes = (size_t)(kPullThreads / 32) * kStage * 4;
+  const size_t room = (size_t)optin - fa.sharedSizeBytes - stage_bytes - 1024;  // and a margin
+  const uint32_t vcap = (V + 3) & ~3u;  // contrib buffers hold V + 4 floats
+  w->hot_max = (uint32_t)std::min<size_t>(vcap, (room / 16) * 4);
+  OGB_CUDA(cudaFuncSetAttribute(pr_pull_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(stage_bytes + (size_t)w->hot_max * 4)));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  return OK;
+}
+
 static int pr_work_get(DevGraph& g, bool pull, PrWork** out, cudaStream_t s) {
   if (!g.pr) g.pr = new PrWork();
   PrWork* w = g.pr;
@@ -496,11 +784,20 @@ static int pr_work_get(DevGraph& g, bool pull, PrWork** out, cudaStream_t s) {
     OGB_CUDA(cudaEventCreate(&w->ev1));
   }
   const int want = pull ? 1 : 0;
-  if (w->listed_pull != want || w->listed_warp != g_warp_thr || w->listed_cta != g_cta_thr) {
+  if (pull && (!w->rl_ready || w->rl_build != g.build_id || w->rl_warp != g_warp_thr)) {
+    OGB_TRY(pr_build_relabel(g, w, s));
+    w->rl_ready = true;
+    w->rl_build = g.build_id;
+    w->rl_warp = g_warp_thr;
+    w->listed_pull = -1;
+  }
+  if (w->listed_pull != want || w->listed_warp != g_warp_thr || w->listed_cta != g_cta_thr ||
+      w->listed_build != g.build_id) {
     OGB_TRY(pr_build_lists(g, w, pull, s));
     w->listed_pull = want;
     w->listed_warp = g_warp_thr;
     w->listed_cta = g_cta_thr;
+    w->listed_build = g.build_id;
   }
   *out = w;
   return OK;
@@ -527,7 +824,10 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
   float* c_cur = w->contrib0.as<float>();
   float* c_nxt = w->contrib1.as<float>();
   float* nxt = w->next.as<float>();
-  pr_init_kernel<<<sms * 8, 256, 0, s>>>(V, g.fwd.d_out_degree(), init, p.base_pr, ranks, c_cur, pull ? nullptr : nxt);
+  const uint32_t* perm = pull ? w->perm.as<uint32_t>() : nullptr;
+  const uint32_t hot = std::min(w->hot_max, g_hot_limit & ~3u);
+  pr_init_kernel<<<sms * 8, 256, 0, s>>>(V, g.fwd.d_out_degree(), init, p.base_pr, ranks, c_cur, pull ? nullptr : nxt,
+                                         perm);
   OGB_CUDA(cudaGetLastError());
 
   const uint32_t nb_chunk = w->n_chunks ? std::min<uint32_t>(sms * 4, w->n_chunks) : 0;
@@ -542,10 +842,10 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
   OGB_CUDA(cudaEventRecord(w->ev0, s));
   for (uint32_t it = 0; it < max_iters; it++) {
     if (pull) {
-      pr_pull_kernel<<<grid, T, 0, s>>>(nb_chunk, nb_warp, heavy, w->n_warp, chunks, w->n_chunks,
-                                         w->vfirst.as<uint32_t>(), w->vcount.as<uint32_t>(), w->done.as<uint32_t>(),
-                                         w->partials.as<float>(), rows, nbr, g.fwd.d_out_degree(), c_cur, c_nxt,
-                                         ranks, p, d_ctl, it);
+      pr_pull_kernel<<<sms, kPullThreads, (kPullThreads / 32) * kStage * 4 + hot * 4, s>>>(
+          hot, heavy, w->n_warp, chunks, w->n_chunks, w->vfirst.as<uint32_t>(), w->vcount.as<uint32_t>(),
+          w->done.as<uint32_t>(), w->partials.as<float>(), w->rows_rl.as<uint2>(), w->off_light.as<uint32_t>(),
+          w->nbr_rl.as<uint32_t>(), g.fwd.d_out_degree(), perm, c_cur, c_nxt, ranks, p, d_ctl, it);
     } else {
       pr_push_scatter_kernel<<<grid, T, 0, s>>>(nb_chunk, nb_warp, heavy, w->n_warp, chunks, w->n_chunks, V,
                                                  g_warp_thr, rows, nbr, c_cur, nxt, d_ctl);
