@@ -122,12 +122,6 @@ int ogb_pagerank(ogb_graph *g, uint32_t mode, uint32_t max_iterations, double ep
  * threads (fixed-order butterfly sums).  Defaults 32 / 2048 / 256. */
 void ogb_pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr);
 void ogb_pagerank_get_bins(uint32_t *warp_thr, uint32_t *cta_thr, uint32_t *cta_threads, uint32_t *chunk_edges);
-/* Pull PageRank stages the contrib of the leading sources (renumbered by
- * descending out-degree) in each CTA's shared memory; this caps how many
- * (0 = none, default = as many as fit).  Results do not depend on it.  No
- * reference counterpart (a tuning knob of this library). */
-void ogb_pagerank_set_hot_limit(uint32_t max_vertices);
-uint32_t ogb_pagerank_get_hot_limit(void);
 /* Per-iteration L1 error and active count of the last ogb_pagerank on g. */
 int ogb_pagerank_history(ogb_graph *g, double *errors, uint32_t *active, uint32_t max_entries, uint32_t *count);
 

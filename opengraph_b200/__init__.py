@@ -200,8 +200,6 @@ _DEVICE_API = [
     ("ogb_pagerank", C.c_int, [vp, u32, u32, C.c_double, vp, vp, C.POINTER(PrInfo), vp]),
     ("ogb_pagerank_history", C.c_int, [vp, C.POINTER(C.c_double), u32p, u32, C.POINTER(u32)]),
     ("ogb_pagerank_set_bins", None, [u32, u32]),
-    ("ogb_pagerank_set_hot_limit", None, [u32]),
-    ("ogb_pagerank_get_hot_limit", u32, []),
     ("ogb_pagerank_pull_noalloc", C.c_int, [u32, vp, vp, vp, vp, u32, C.c_double, vp, vp, vp]),
     ("ogb_pagerank_get_bins", None, [u32p, u32p, u32p, u32p]),
     ("ogb_generate_rmat", C.c_int, [u32, u32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_int, vp, vp,

@@ -1323,8 +1323,6 @@ extern "C" int ogb_pagerank(ogb_graph* g, uint32_t mode, uint32_t max_iters, dou
 }
 
 extern "C" void ogb_pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr) { pagerank_set_bins(warp_thr, cta_thr); }
-extern "C" void ogb_pagerank_set_hot_limit(uint32_t max_vertices) { pagerank_set_hot_limit(max_vertices); }
-extern "C" uint32_t ogb_pagerank_get_hot_limit(void) { return pagerank_get_hot_limit(); }
 
 extern "C" void ogb_pagerank_get_bins(uint32_t* warp_thr, uint32_t* cta_thr, uint32_t* cta_threads,
                                       uint32_t* chunk_edges) {

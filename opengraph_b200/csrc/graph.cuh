@@ -146,7 +146,5 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
 // heavy rows per warp, very heavy rows per CTA of cta_threads threads).
 void pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr);
 void pagerank_get_bins(uint32_t* warp_thr, uint32_t* cta_thr, uint32_t* cta_threads, uint32_t* chunk);
-void pagerank_set_hot_limit(uint32_t max_vertices);
-uint32_t pagerank_get_hot_limit();
 
 }  // namespace ogb

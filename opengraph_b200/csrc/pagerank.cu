@@ -56,22 +56,19 @@ constexpr int kPrThreads = 256;      // push kernels
 constexpr int kPullThreads = 1024;   // pull: one CTA per SM
 constexpr int kPullGroup = 256;      // threads per chunk group (the oracle's cta_threads)
 constexpr int kPullGroups = kPullThreads / kPullGroup;
-constexpr uint32_t kStage = 256;     // staged light edges per warp and window
+constexpr uint32_t kStage = 256;     // staged edges per warp and window
 constexpr int kLightR = 4;           // light rows per lane (128 per warp unit)
+constexpr uint32_t kUnit = 4096;     // medium-row edges per warp unit
+constexpr uint32_t kTab = 64;        // medium rows per table batch
+constexpr uint32_t kWarpSmemWords = kStage + 3 * kTab + 1;  // stage + table of one warp
+constexpr size_t kPullDynSmem = (size_t)(kPullThreads / 32) * kWarpSmemWords * 4;
+constexpr uint32_t kHotLimit = 0;    // renumbered sources whose contrib a pull CTA stages in shared memory
 constexpr uint32_t kPrChunk = 8192;  // edges per chunk of a very heavy row
 
 // Row-length thresholds of the work split (settable; the GPU-order mode of
 // the oracle takes the same values).
 static uint32_t g_warp_thr = 32;
 static uint32_t g_cta_thr = 2048;
-
-// Upper bound on the renumbered sources whose contrib a pull CTA stages in
-// shared memory.  Default 0: on RMAT-22 staging the leading 4k..57k sources
-// measured 0.38..0.44 ms per iteration against 0.38 ms without (the shared
-// memory it takes is L1 the gathers lose).
-static uint32_t g_hot_limit = 0;
-void pagerank_set_hot_limit(uint32_t max_vertices) { g_hot_limit = max_vertices; }
-uint32_t pagerank_get_hot_limit() { return g_hot_limit; }
 
 void pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr) {
   g_warp_thr = warp_thr;
@@ -88,6 +85,8 @@ struct PrCtl {
   double err[kPrMaxIters];
   uint32_t active[kPrMaxIters];
   uint32_t blocks_done[kPrMaxIters];
+  uint32_t claim_med[kPrMaxIters];    // pull: medium units handed out
+  uint32_t claim_light[kPrMaxIters];  // pull: light units handed out
   uint32_t stop;       // 1 once an iteration ended with no active vertex
   uint32_t stop_iter;  // index of that iteration
 };
@@ -101,10 +100,11 @@ struct PrWork {
   int listed_pull = -1;                // direction the lists describe
   uint32_t listed_warp = 0, listed_cta = 0, listed_build = 0;
   // pull: source ids renumbered by descending out-degree
-  uint32_t rl_build = 0, rl_warp = 0;
+  uint32_t rl_build = 0, rl_warp = 0, rl_cta = 0;
   bool rl_ready = false;
-  DevBuf perm, nbr_rl, rows_rl, off_light, rl_keys, rl_ids, rl_tmp;
-  uint32_t hot_max = 0;                // leading renumbered vertices that fit in shared memory
+  DevBuf perm, nbr_rl, rows_rl, off_light, med_v, med_off, unit_first, rl_tmp;
+  uint32_t n_med = 0, n_units = 0, med_base = 0;
+  uint32_t hot = 0;  // staged renumbered sources
   DevBuf contrib0, contrib1, next, ctl;
   DevBuf heavy;                        // vertex ids of the warp rows (n_warp), then the chunked rows
   DevBuf chunks;                       // PrChunkItem per chunk
@@ -212,22 +212,11 @@ __device__ __forceinline__ void pr_block_finish(double err, uint32_t active, PrC
   }
 }
 
-// contrib of renumbered source u: shared memory for the leading `hot` ids.
-__device__ __forceinline__ float ld_c(const float* s_hot, uint32_t hot, const float* __restrict__ c, uint32_t u) {
-  float x;
-  if (u < hot)
-    x = s_hot[u];
-  else
-    x = __ldg(&c[u]);
-  return x;
-}
-
 // s += c[nbr[j]] for j = j0, j0+STRIDE, ... < j1, in that order; each step
-// issues four predicated neighbour loads, then their four gathers (no
-// serial tail loop: a row of 33..128 edges is one step).
+// issues four predicated neighbour loads, then their four gathers.
 template <uint32_t STRIDE>
-__device__ __forceinline__ float strided_sum(const float* s_hot, uint32_t hot, const float* __restrict__ c,
-                                             const uint32_t* __restrict__ nbr, uint32_t j0, uint32_t j1) {
+__device__ __forceinline__ float strided_sum(const float* __restrict__ c, const uint32_t* __restrict__ nbr,
+                                             uint32_t j0, uint32_t j1) {
   float s = 0.0f;
   for (uint32_t j = j0; j < j1; j += 4 * STRIDE) {
     uint32_t x[4];
@@ -235,7 +224,7 @@ __device__ __forceinline__ float strided_sum(const float* s_hot, uint32_t hot, c
     for (int k = 0; k < 4; k++) x[k] = (j + k * STRIDE < j1) ? __ldg(&nbr[j + k * STRIDE]) : 0u;
     float cx[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++) cx[k] = (j + k * STRIDE < j1) ? ld_c(s_hot, hot, c, x[k]) : 0.0f;
+    for (int k = 0; k < 4; k++) cx[k] = (j + k * STRIDE < j1) ? __ldg(&c[x[k]]) : 0.0f;
 #pragma unroll
     for (int k = 0; k < 4; k++)
       if (j + k * STRIDE < j1) s = __fadd_rn(s, cx[k]);
@@ -249,34 +238,7 @@ __device__ __forceinline__ float warp_fold(float s) {
   return s;
 }
 
-// Two strided sums at once (rows A and B of one warp), each in the order of
-// strided_sum<32>: eight gathers in flight per lane.
-__device__ __forceinline__ void strided_sum2(const float* s_hot, uint32_t hot, const float* __restrict__ c,
-                                             const uint32_t* __restrict__ nbr, uint32_t a0, uint32_t a1,
-                                             uint32_t b0, uint32_t b1, float& sa, float& sb) {
-  constexpr uint32_t S = 32;
-  sa = 0.0f;
-  sb = 0.0f;
-  for (uint32_t ja = a0, jb = b0; ja < a1 || jb < b1; ja += 4 * S, jb += 4 * S) {
-    uint32_t x[4], y[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      x[k] = (ja + k * S < a1) ? __ldg(&nbr[ja + k * S]) : 0u;
-      y[k] = (jb + k * S < b1) ? __ldg(&nbr[jb + k * S]) : 0u;
-    }
-    float cx[4], cy[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      cx[k] = (ja + k * S < a1) ? ld_c(s_hot, hot, c, x[k]) : 0.0f;
-      cy[k] = (jb + k * S < b1) ? ld_c(s_hot, hot, c, y[k]) : 0.0f;
-    }
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      if (ja + k * S < a1) sa = __fadd_rn(sa, cx[k]);
-      if (jb + k * S < b1) sb = __fadd_rn(sb, cy[k]);
-    }
-  }
-}
+__device__ __forceinline__ uint32_t ceil_div_dev(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
 
 // Update inputs of vertex v, loaded before its sum is ready.
 struct PrVtx {
@@ -303,38 +265,79 @@ __device__ __forceinline__ void pr_update_pre(uint32_t v, float s, const PrVtx& 
   active += (e >= p.epsilon) ? 1u : 0u;
 }
 
+__device__ __forceinline__ void cp_async4(float* dst_smem, const float* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
 
-// Pull iteration, one CTA per SM (1024 threads).  Shared memory holds the
-// contrib of renumbered sources [0, hot) and one stage of kStage floats per
-// warp.  Work, each kind strided over the grid:
-//  (1) chunks of very heavy rows, one 256-thread group per chunk (four
-//      chunks in flight per CTA), lanes strided, warps folded, the group's
-//      warps summed in order, the chunk sums in chunk order by the group that
-//      finishes a row's last chunk;
-//  (2) warp rows, a warp per two rows, lanes strided, butterfly-folded;
+// A warp walks an edge range [e0, e1) in windows of kStage edges: the
+// contribs of a window are copied straight into the warp's stage by
+// asynchronous 4-byte copies (kStage / 32 per lane in flight, no registers
+// held for them), and the neighbour ids of the next window load meanwhile.
+struct StagePipe {
+  uint32_t u[kStage / 32];
+  __device__ __forceinline__ void load(const uint32_t* __restrict__ nbr, uint32_t w0, uint32_t e1, uint32_t lane) {
+#pragma unroll
+    for (uint32_t m = 0; m < kStage / 32; m++) {
+      const uint32_t j = w0 + m * 32 + lane;
+      u[m] = j < e1 ? __ldg(&nbr[j]) : 0u;
+    }
+  }
+  // Gather window [w0, min(w0 + kStage, e1)) into stage; the next window's
+  // ids are loaded into u meanwhile.  The caller syncs the warp afterwards.
+  __device__ __forceinline__ void gather(float* stage, const uint32_t* __restrict__ nbr, const float* __restrict__ c,
+                                         const float* s_hot, uint32_t hot, uint32_t w0, uint32_t e1, uint32_t lane) {
+#pragma unroll
+    for (uint32_t m = 0; m < kStage / 32; m++) {
+      const uint32_t j = w0 + m * 32 + lane;
+      if (j < e1) {
+        if (u[m] < hot)
+          stage[m * 32 + lane] = s_hot[u[m]];
+        else
+          cp_async4(&stage[m * 32 + lane], c + u[m]);
+      }
+    }
+    load(nbr, w0 + kStage, e1, lane);
+    cp_async_wait_all();
+  }
+};
+
+// Pull iteration, one CTA per SM (1024 threads).  The inverse neighbour
+// array is in the re-laid form: light rows (in-degree <= warp_thr) first,
+// then medium rows (<= cta_thr), then the rest, each class contiguous in
+// vertex order, with renumbered source ids.  Work, each kind strided over
+// the grid:
+//  (1) chunks of very heavy rows, one 256-thread group per chunk (four in
+//      flight per CTA): lanes strided, warps folded, the group's warps summed
+//      in order, the chunk sums in chunk order by the group that finishes a
+//      row's last chunk;
+//  (2) medium rows, a warp per unit of kUnit edges (the rows starting in
+//      it): the unit's edges are gathered kStage at a time into the warp's
+//      stage with coalesced loads; lane l adds the elements l, l+32, ... of
+//      each row in order, and the row is butterfly-folded when it ends;
 //  (3) light rows, a warp per 128 consecutive vertices: their edges are
-//      contiguous in the light segment of nbr (off_light), so the warp loads
-//      them coalesced and gathers kStage contribs at a time into its stage,
-//      then each lane adds its four rows' values in CSR order.
-// rows (renumbered layout), pr and out_degree are in original vertex order;
-// contrib / contrib_next are indexed by renumbered id.
+//      contiguous, gathered into the stage the same way, and each lane adds
+//      its four rows' values in CSR order.
+// rows_rl, pr and out_degree are in original vertex order; contrib and
+// contrib_next are indexed by renumbered id (perm).
 __global__ void __launch_bounds__(kPullThreads, 1) pr_pull_kernel(
-    uint32_t hot, const uint32_t* __restrict__ heavy, uint32_t n_warp, const PrChunkItem* __restrict__ chunks,
-    uint32_t n_chunks, const uint32_t* __restrict__ vfirst, const uint32_t* __restrict__ vcount,
-    uint32_t* __restrict__ done, float* __restrict__ partials, const uint2* __restrict__ rows,
-    const uint32_t* __restrict__ off_light, const uint32_t* __restrict__ nbr,
-    const uint32_t* __restrict__ out_degree, const uint32_t* __restrict__ perm, const float* __restrict__ contrib,
-    float* __restrict__ contrib_next, float* __restrict__ pr, PrParams p, PrCtl* __restrict__ ctl, uint32_t it) {
-  extern __shared__ float4 s_dyn4[];
-  float* s_stage = reinterpret_cast<float*>(s_dyn4);  // kPullThreads / 32 stages
-  const float* s_hot = s_stage + (kPullThreads / 32) * kStage;
+    uint32_t hot, const PrChunkItem* __restrict__ chunks, uint32_t n_chunks, const uint32_t* __restrict__ vfirst,
+    const uint32_t* __restrict__ vcount, uint32_t* __restrict__ done, float* __restrict__ partials,
+    const uint2* __restrict__ rows, const uint32_t* __restrict__ off_light, const uint32_t* __restrict__ unit_first,
+    uint32_t n_units, const uint32_t* __restrict__ med_off, const uint32_t* __restrict__ med_v, uint32_t med_base,
+    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ out_degree, const uint32_t* __restrict__ perm,
+    const float* __restrict__ contrib, float* __restrict__ contrib_next, float* __restrict__ pr, PrParams p,
+    PrCtl* __restrict__ ctl, uint32_t it) {
+  extern __shared__ uint32_t s_dyn[];  // per warp: stage and medium-row table; then the hot contribs
   __shared__ float s_part[kPullGroups][kPullGroup / 32];
   __shared__ uint32_t s_last[kPullGroups];
   if (ctl->stop) return;
-  {
-    float4* h4 = s_dyn4 + (kPullThreads / 32) * kStage / 4;
-    for (uint32_t i = threadIdx.x; i < hot / 4; i += kPullThreads) h4[i] = __ldg(reinterpret_cast<const float4*>(contrib) + i);
-  }
+  float* s_hot = reinterpret_cast<float*>(s_dyn + (kPullThreads / 32) * kWarpSmemWords);
+  for (uint32_t i = threadIdx.x; i < hot / 4; i += kPullThreads)
+    reinterpret_cast<float4*>(s_hot)[i] = __ldg(reinterpret_cast<const float4*>(contrib) + i);
   __syncthreads();
   double err = 0.0;
   uint32_t active = 0;
@@ -345,7 +348,7 @@ __global__ void __launch_bounds__(kPullThreads, 1) pr_pull_kernel(
     const uint32_t grp = threadIdx.x / kPullGroup, gt = threadIdx.x % kPullGroup;
     for (uint32_t g = blockIdx.x * kPullGroups + grp; g < n_chunks; g += gridDim.x * kPullGroups) {
       const PrChunkItem ci = chunks[g];
-      float sum = strided_sum<kPullGroup>(s_hot, hot, contrib, nbr, ci.j0 + gt, ci.j1);
+      float sum = strided_sum<kPullGroup>(contrib, nbr, ci.j0 + gt, ci.j1);
       sum = warp_fold(sum);
       if (lane == 0) s_part[grp][gt >> 5] = sum;
       asm volatile("bar.sync %0, %1;" ::"r"(grp + 1), "r"(kPullGroup) : "memory");
@@ -369,33 +372,62 @@ __global__ void __launch_bounds__(kPullThreads, 1) pr_pull_kernel(
     }
   }
 
-  // (2) warp rows: a warp reduces two rows at a time (t and t + nw)
-  const uint32_t gw = blockIdx.x * (kPullThreads / 32) + warp;
-  const uint32_t nw = gridDim.x * (kPullThreads / 32);
-  for (uint32_t t = gw; t < n_warp; t += 2 * nw) {
-    const uint32_t va = heavy[t];
-    const bool has_b = t + nw < n_warp;
-    const uint32_t vb = has_b ? heavy[t + nw] : va;
-    const uint2 ra = rows[va];
-    const uint2 rb = has_b ? rows[vb] : make_uint2(0, 0);
-    PrVtx xa, xb;
-    if (lane == 0) {
-      xa = pr_vtx(va, pr, out_degree, perm);
-      xb = pr_vtx(vb, pr, out_degree, perm);
+  uint32_t* mine = s_dyn + warp * kWarpSmemWords;
+  float* stage = reinterpret_cast<float*>(mine);
+
+  // (2) medium rows, a warp per unit, rows taken in batches of kTab
+  uint32_t* toff = mine + kStage;
+  uint32_t* tv = toff + kTab + 1;
+  float* tsum = reinterpret_cast<float*>(tv + kTab);
+  uint32_t* claim = &ctl->claim_med[it];
+  uint32_t t = __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(claim, 1u) : 0u, 0);
+  while (t < n_units) {
+    const uint32_t t_next = lane == 0 ? atomicAdd(claim, 1u) : 0u;  // next claim, in flight meanwhile
+    const uint32_t i0 = unit_first[t], i1 = unit_first[t + 1];
+    for (uint32_t ib = i0; ib < i1; ib += kTab) {
+      const uint32_t nr = min(ib + kTab, i1) - ib;
+      for (uint32_t k = lane; k <= nr; k += 32) toff[k] = med_base + med_off[ib + k];
+      for (uint32_t k = lane; k < nr; k += 32) tv[k] = med_v[ib + k];
+      __syncwarp();
+      const uint32_t e0 = toff[0], e1 = toff[nr];
+      uint32_t r = 0;
+      float s = 0.0f;
+      StagePipe pipe;
+      pipe.load(nbr, e0, e1, lane);
+      for (uint32_t w0 = e0; w0 < e1; w0 += kStage) {
+        const uint32_t w1 = min(w0 + kStage, e1);
+        pipe.gather(stage, nbr, contrib, s_hot, hot, w0, e1, lane);
+        __syncwarp();
+        while (r < nr) {
+          const uint32_t rs = toff[r], re = toff[r + 1];
+          const uint32_t lo = max(rs, w0), hi = min(re, w1);
+          // lane l takes the row's elements rs + l + 32 m
+          for (uint32_t j = lo + ((rs + lane - lo) & 31u); j < hi; j += 32) s = __fadd_rn(s, stage[j - w0]);
+          if (re > w1) break;  // the row goes on in the next window
+          s = warp_fold(s);
+          if (lane == 0) tsum[r] = s;
+          s = 0.0f;
+          r++;
+        }
+        __syncwarp();
+      }
+      for (uint32_t k = lane; k < nr; k += 32) {
+        const uint32_t v = tv[k];
+        const PrVtx x = pr_vtx(v, pr, out_degree, perm);
+        pr_update_pre(v, tsum[k], x, pr, contrib_next, p, err, active);
+      }
+      __syncwarp();
     }
-    float sa, sb;
-    strided_sum2(s_hot, hot, contrib, nbr, ra.x + lane, ra.x + ra.y, rb.x + lane, rb.x + rb.y, sa, sb);
-    sa = warp_fold(sa);
-    sb = warp_fold(sb);
-    if (lane == 0) {
-      pr_update_pre(va, sa, xa, pr, contrib_next, p, err, active);
-      if (has_b) pr_update_pre(vb, sb, xb, pr, contrib_next, p, err, active);
-    }
+    t = __shfl_sync(0xffffffffu, t_next, 0);
   }
 
-  // (3) light rows, staged
-  float* stage = s_stage + warp * kStage;
-  for (uint32_t base = gw * (32 * kLightR); base < p.V; base += nw * (32 * kLightR)) {
+  // (3) light rows, a warp per 128 consecutive vertices
+  const uint32_t n_light = ceil_div_dev(p.V, 32 * kLightR);
+  claim = &ctl->claim_light[it];
+  t = __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(claim, 1u) : 0u, 0);
+  while (t < n_light) {
+    const uint32_t t_next = lane == 0 ? atomicAdd(claim, 1u) : 0u;
+    const uint32_t base = t * (32 * kLightR);
     const uint32_t vend = min(base + 32 * kLightR, p.V);
     uint32_t st[kLightR], en[kLightR];
     bool light[kLightR];
@@ -415,22 +447,11 @@ __global__ void __launch_bounds__(kPullThreads, 1) pr_pull_kernel(
       }
     }
     const uint32_t seg0 = off_light[base], seg1 = off_light[vend];
+    StagePipe pipe;
+    pipe.load(nbr, seg0, seg1, lane);
     for (uint32_t w0 = seg0; w0 < seg1; w0 += kStage) {
       const uint32_t w1 = min(w0 + kStage, seg1);
-      uint32_t u[kStage / 32];
-#pragma unroll
-      for (uint32_t m = 0; m < kStage / 32; m++) {
-        const uint32_t j = w0 + m * 32 + lane;
-        u[m] = j < w1 ? __ldg(&nbr[j]) : 0u;
-      }
-      float c[kStage / 32];
-#pragma unroll
-      for (uint32_t m = 0; m < kStage / 32; m++) {
-        const uint32_t j = w0 + m * 32 + lane;
-        c[m] = j < w1 ? ld_c(s_hot, hot, contrib, u[m]) : 0.0f;
-      }
-#pragma unroll
-      for (uint32_t m = 0; m < kStage / 32; m++) stage[m * 32 + lane] = c[m];
+      pipe.gather(stage, nbr, contrib, s_hot, hot, w0, seg1, lane);
       __syncwarp();
       uint32_t lo[kLightR], n[kLightR], nmax = 0;
 #pragma unroll
@@ -450,6 +471,7 @@ __global__ void __launch_bounds__(kPullThreads, 1) pr_pull_kernel(
 #pragma unroll
     for (int k = 0; k < kLightR; k++)
       if (light[k]) pr_update_pre(base + k * 32 + lane, s[k], x[k], pr, contrib_next, p, err, active);
+    t = __shfl_sync(0xffffffffu, t_next, 0);
   }
   pr_block_finish<kPullThreads>(err, active, ctl, it);
 }
@@ -470,24 +492,60 @@ __global__ void pr_rl_perm_kernel(uint32_t V, const uint32_t* __restrict__ order
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) perm[order[i]] = i;
 }
 
-// Row lengths split by class: light rows (in-degree <= warp_thr) and the rest.
-__global__ void pr_rl_split_kernel(uint32_t V, const uint2* __restrict__ rows, uint32_t warp_thr,
-                                   uint32_t* __restrict__ dl, uint32_t* __restrict__ dh) {
+// Row lengths by class (light <= warp_thr < medium <= cta_thr < chunked),
+// and the medium flag.
+__global__ void pr_rl_split_kernel(uint32_t V, const uint2* __restrict__ rows, uint32_t warp_thr, uint32_t cta_thr,
+                                   uint32_t* __restrict__ dl, uint32_t* __restrict__ dm, uint32_t* __restrict__ dc,
+                                   uint32_t* __restrict__ fm) {
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     const uint32_t d = rows[v].y;
-    dl[v] = d <= warp_thr ? d : 0u;
-    dh[v] = d <= warp_thr ? 0u : d;
+    const uint32_t cls = d <= warp_thr ? 0u : (d <= cta_thr ? 1u : 2u);
+    dl[v] = cls == 0 ? d : 0u;
+    dm[v] = cls == 1 ? d : 0u;
+    dc[v] = cls == 2 ? d : 0u;
+    fm[v] = cls == 1 ? 1u : 0u;
   }
 }
 
-// New row offsets: light rows first (vertex order), heavy rows after them.
-__global__ void pr_rl_rows_kernel(uint32_t V, const uint2* __restrict__ rows, uint32_t warp_thr,
-                                  const uint32_t* __restrict__ off_l, const uint32_t* __restrict__ off_h,
-                                  uint2* __restrict__ rows_rl) {
-  const uint32_t total_l = off_l[V];
+// New row offsets (light | medium | chunked), and the medium row list:
+// med_v[i] = vertex, med_off[i] = its offset inside the medium class.
+__global__ void pr_rl_rows_kernel(uint32_t V, const uint2* __restrict__ rows, uint32_t warp_thr, uint32_t cta_thr,
+                                  const uint32_t* __restrict__ off_l, const uint32_t* __restrict__ off_m,
+                                  const uint32_t* __restrict__ off_c, const uint32_t* __restrict__ idx_m,
+                                  uint2* __restrict__ rows_rl, uint32_t* __restrict__ med_v,
+                                  uint32_t* __restrict__ med_off) {
+  const uint32_t L = off_l[V], M = off_m[V];
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     const uint32_t d = rows[v].y;
-    rows_rl[v] = make_uint2(d <= warp_thr ? off_l[v] : total_l + off_h[v], d);
+    uint32_t o;
+    if (d <= warp_thr) {
+      o = off_l[v];
+    } else if (d <= cta_thr) {
+      o = L + off_m[v];
+      med_v[idx_m[v]] = v;
+      med_off[idx_m[v]] = off_m[v];
+    } else {
+      o = L + M + off_c[v];
+    }
+    rows_rl[v] = make_uint2(o, d);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) med_off[idx_m[V]] = M;
+}
+
+// unit_first[t] = first medium row starting at or after t * kUnit.
+__global__ void pr_rl_units_kernel(uint32_t n_units, const uint32_t* __restrict__ med_off, uint32_t n_med,
+                                   uint32_t* __restrict__ unit_first) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t <= n_units; t += gridDim.x * blockDim.x) {
+    const uint64_t key = (uint64_t)t * kUnit;
+    uint32_t lo = 0, hi = n_med;  // answer in [0, n_med]
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if ((uint64_t)med_off[mid] < key)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    unit_first[t] = lo;
   }
 }
 
@@ -712,41 +770,56 @@ static int pr_build_lists(DevGraph& g, PrWork* w, bool pull, cudaStream_t s) {
   return OK;
 }
 
-// Renumbering of the pull sources (once per graph and warp_thr): ids sorted
-// by descending out-degree (stable: ties by id), perm = old -> new; a new
-// layout of the inverse neighbour array with renumbered ids, light rows
-// (in-degree <= warp_thr) first in vertex order, then the other rows in
-// vertex order; rows_rl = {new offset, in-degree}, off_light = offsets of the
-// light rows (V + 1 entries, heavy rows empty); and the number of leading
-// renumbered ids whose contrib fits in a pull CTA's shared memory.
+// Re-laid pull graph (once per graph, warp_thr and cta_thr): ids sorted by
+// descending out-degree (stable: ties by id), perm = old -> new; the inverse
+// neighbour array copied with renumbered ids into light | medium | chunked
+// classes, each contiguous in vertex order; rows_rl = {new offset,
+// in-degree}; off_light = offsets of the light rows (V + 1 entries, other
+// rows empty); the medium row list (med_v, med_off) and its units.
 static int pr_build_relabel(DevGraph& g, PrWork* w, cudaStream_t s) {
   const uint32_t V = g.V, E = g.E;
+  const size_t Vp = ((size_t)V + 8) & ~(size_t)3;  // words per V + 1 array, padded
   OGB_TRY(w->perm.alloc((size_t)V * 4 + 16));
   OGB_TRY(w->nbr_rl.alloc((size_t)E * 4 + 16));
   OGB_TRY(w->rows_rl.alloc((size_t)V * 8 + 16));
-  OGB_TRY(w->off_light.alloc((size_t)V * 4 + 16));
-  OGB_TRY(w->rl_keys.alloc((size_t)V * 4 + 16));
-  OGB_TRY(w->rl_ids.alloc((size_t)V * 4 + 16));
-  OGB_TRY(w->rl_tmp.alloc((size_t)V * 8 + 64 + ((size_t)V / kScanTileN + 4) * 4));
+  OGB_TRY(w->off_light.alloc(Vp * 4));
+  OGB_TRY(w->rl_tmp.alloc((Vp * 8 + ((size_t)V / kScanTileN + 4)) * 4));
   const int grid = sm_count() * 8;
-  uint32_t* keys = w->rl_keys.as<uint32_t>();
-  uint32_t* ids = w->rl_ids.as<uint32_t>();
-  uint32_t* skeys = w->rl_tmp.as<uint32_t>();
-  uint32_t* order = skeys + ((V + 7) & ~3u);
-  uint32_t* scan_tmp = order + ((V + 7) & ~3u);
-  pr_rl_keys_kernel<<<grid, 256, 0, s>>>(V, g.fwd.d_out_degree(), keys, ids);
+  uint32_t* t0 = w->rl_tmp.as<uint32_t>();
+  uint32_t* a[8];
+  for (int i = 0; i < 8; i++) a[i] = t0 + i * Vp;
+  uint32_t* scan_tmp = t0 + 8 * Vp;
+  // sort ids by ~out_degree: a0 keys, a1 ids -> a2 sorted keys, a3 order
+  pr_rl_keys_kernel<<<grid, 256, 0, s>>>(V, g.fwd.d_out_degree(), a[0], a[1]);
   OGB_CUDA(cudaGetLastError());
-  KV in{keys, ids, nullptr};
-  KV out{skeys, order, nullptr};
+  KV in{a[0], a[1], nullptr};
+  KV out{a[2], a[3], nullptr};
   OGB_TRY(sort_pairs(in, out, V, g.sort_ws, s));
-  pr_rl_perm_kernel<<<grid, 256, 0, s>>>(V, order, w->perm.as<uint32_t>());
-  // layout: keys/ids become the split lengths, skeys/order their offsets
-  pr_rl_split_kernel<<<grid, 256, 0, s>>>(V, g.inv.d_rows(), g_warp_thr, keys, ids);
+  pr_rl_perm_kernel<<<grid, 256, 0, s>>>(V, a[3], w->perm.as<uint32_t>());
+  // classes: a0 light, a1 medium, a2 chunked lengths, a3 medium flags; scans
+  // into off_light, a4, a5, a6
+  pr_rl_split_kernel<<<grid, 256, 0, s>>>(V, g.inv.d_rows(), g_warp_thr, g_cta_thr, a[0], a[1], a[2], a[3]);
   OGB_CUDA(cudaGetLastError());
-  OGB_TRY(scan_exclusive(keys, w->off_light.as<uint32_t>(), V, scan_tmp, s));
-  OGB_TRY(scan_exclusive(ids, skeys, V, scan_tmp, s));
-  pr_rl_rows_kernel<<<grid, 256, 0, s>>>(V, g.inv.d_rows(), g_warp_thr, w->off_light.as<uint32_t>(), skeys,
-                                         w->rows_rl.as<uint2>());
+  OGB_TRY(scan_exclusive(a[0], w->off_light.as<uint32_t>(), V, scan_tmp, s));
+  OGB_TRY(scan_exclusive(a[1], a[4], V, scan_tmp, s));
+  OGB_TRY(scan_exclusive(a[2], a[5], V, scan_tmp, s));
+  OGB_TRY(scan_exclusive(a[3], a[6], V, scan_tmp, s));
+  uint32_t tot[3];
+  OGB_CUDA(cudaMemcpyAsync(&tot[0], w->off_light.as<uint32_t>() + V, 4, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaMemcpyAsync(&tot[1], a[4] + V, 4, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaMemcpyAsync(&tot[2], a[6] + V, 4, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  w->med_base = tot[0];
+  w->n_med = tot[2];
+  w->n_units = ceil_div(tot[1], kUnit);
+  OGB_TRY(w->med_v.alloc((size_t)w->n_med * 4 + 16));
+  OGB_TRY(w->med_off.alloc((size_t)w->n_med * 4 + 16));
+  OGB_TRY(w->unit_first.alloc((size_t)w->n_units * 4 + 16));
+  pr_rl_rows_kernel<<<grid, 256, 0, s>>>(V, g.inv.d_rows(), g_warp_thr, g_cta_thr, w->off_light.as<uint32_t>(), a[4],
+                                         a[5], a[6], w->rows_rl.as<uint2>(), w->med_v.as<uint32_t>(),
+                                         w->med_off.as<uint32_t>());
+  pr_rl_units_kernel<<<grid, 256, 0, s>>>(w->n_units, w->med_off.as<uint32_t>(), w->n_med,
+                                          w->unit_first.as<uint32_t>());
   pr_rl_copy_kernel<<<grid, 256, 0, s>>>(V, g.inv.d_rows(), g.inv.d_dst(), w->rows_rl.as<uint2>(),
                                          w->perm.as<uint32_t>(), w->nbr_rl.as<uint32_t>());
   OGB_CUDA(cudaGetLastError());
@@ -755,12 +828,17 @@ static int pr_build_relabel(DevGraph& g, PrWork* w, cudaStream_t s) {
   OGB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   cudaFuncAttributes fa;
   OGB_CUDA(cudaFuncGetAttributes(&fa, pr_pull_kernel));
-  const size_t stage_bytes = (size_t)(kPullThreads / 32) * kStage * 4;
-  const size_t room = (size_t)optin - fa.sharedSizeBytes - stage_bytes - 1024;  // and a margin
+  const size_t room = (size_t)optin - fa.sharedSizeBytes - kPullDynSmem - 1024;  // and a margin
   const uint32_t vcap = (V + 3) & ~3u;  // contrib buffers hold V + 4 floats
-  w->hot_max = (uint32_t)std::min<size_t>(vcap, (room / 16) * 4);
-  OGB_CUDA(cudaFuncSetAttribute(pr_pull_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(stage_bytes + (size_t)w->hot_max * 4)));
+  w->hot = std::min<uint32_t>(kHotLimit & ~3u, (uint32_t)std::min<size_t>(vcap, (room / 16) * 4));
+  const size_t smem = kPullDynSmem + (size_t)w->hot * 4;
+  OGB_CUDA(cudaFuncSetAttribute(pr_pull_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // the rest of the SM's unified L1 / shared memory stays L1: the gathers of
+  // the highest-degree sources hit there
+  int smem_per_sm = 0;
+  OGB_CUDA(cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  const int pct = (int)std::min<size_t>(100, ((smem + fa.sharedSizeBytes + 2048) * 100 + smem_per_sm - 1) / smem_per_sm);
+  OGB_CUDA(cudaFuncSetAttribute(pr_pull_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
   OGB_CUDA(cudaStreamSynchronize(s));
   return OK;
 }
@@ -784,11 +862,12 @@ static int pr_work_get(DevGraph& g, bool pull, PrWork** out, cudaStream_t s) {
     OGB_CUDA(cudaEventCreate(&w->ev1));
   }
   const int want = pull ? 1 : 0;
-  if (pull && (!w->rl_ready || w->rl_build != g.build_id || w->rl_warp != g_warp_thr)) {
+  if (pull && (!w->rl_ready || w->rl_build != g.build_id || w->rl_warp != g_warp_thr || w->rl_cta != g_cta_thr)) {
     OGB_TRY(pr_build_relabel(g, w, s));
     w->rl_ready = true;
     w->rl_build = g.build_id;
     w->rl_warp = g_warp_thr;
+    w->rl_cta = g_cta_thr;
     w->listed_pull = -1;
   }
   if (w->listed_pull != want || w->listed_warp != g_warp_thr || w->listed_cta != g_cta_thr ||
@@ -825,7 +904,6 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
   float* c_nxt = w->contrib1.as<float>();
   float* nxt = w->next.as<float>();
   const uint32_t* perm = pull ? w->perm.as<uint32_t>() : nullptr;
-  const uint32_t hot = std::min(w->hot_max, g_hot_limit & ~3u);
   pr_init_kernel<<<sms * 8, 256, 0, s>>>(V, g.fwd.d_out_degree(), init, p.base_pr, ranks, c_cur, pull ? nullptr : nxt,
                                          perm);
   OGB_CUDA(cudaGetLastError());
@@ -842,10 +920,11 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
   OGB_CUDA(cudaEventRecord(w->ev0, s));
   for (uint32_t it = 0; it < max_iters; it++) {
     if (pull) {
-      pr_pull_kernel<<<sms, kPullThreads, (kPullThreads / 32) * kStage * 4 + hot * 4, s>>>(
-          hot, heavy, w->n_warp, chunks, w->n_chunks, w->vfirst.as<uint32_t>(), w->vcount.as<uint32_t>(),
-          w->done.as<uint32_t>(), w->partials.as<float>(), w->rows_rl.as<uint2>(), w->off_light.as<uint32_t>(),
-          w->nbr_rl.as<uint32_t>(), g.fwd.d_out_degree(), perm, c_cur, c_nxt, ranks, p, d_ctl, it);
+      pr_pull_kernel<<<sms, kPullThreads, kPullDynSmem + (size_t)w->hot * 4, s>>>(
+          w->hot, chunks, w->n_chunks, w->vfirst.as<uint32_t>(), w->vcount.as<uint32_t>(), w->done.as<uint32_t>(),
+          w->partials.as<float>(), w->rows_rl.as<uint2>(), w->off_light.as<uint32_t>(), w->unit_first.as<uint32_t>(),
+          w->n_units, w->med_off.as<uint32_t>(), w->med_v.as<uint32_t>(), w->med_base, w->nbr_rl.as<uint32_t>(),
+          g.fwd.d_out_degree(), perm, c_cur, c_nxt, ranks, p, d_ctl, it);
     } else {
       pr_push_scatter_kernel<<<grid, T, 0, s>>>(nb_chunk, nb_warp, heavy, w->n_warp, chunks, w->n_chunks, V,
                                                  g_warp_thr, rows, nbr, c_cur, nxt, d_ctl);
