@@ -233,6 +233,7 @@ static int d2h(void* h, const void* d, size_t n, cudaStream_t s) {
 struct ogb_graph {
   DevGraph g;
   DevBuf d_parents, d_distances, d_ranks;  // result arrays of the drop-in calls
+  DevBuf d_pack, d_pack_tmp;               // packed BFS result and its scratch
 };
 
 namespace {
@@ -1009,6 +1010,112 @@ extern "C" void freeBFSStats(struct BFSStats* st) {
 
 static BfsResult g_last_bfs;  // level trace of the last drop-in BFS
 
+// Pinned staging of packed BFS results (one per process, grows).
+namespace {
+struct PackStage {
+  static constexpr int kEv = 17;
+  std::mutex mu;
+  uint32_t* h = nullptr;
+  size_t bytes = 0;
+  cudaEvent_t ev[kEv] = {};
+  int reserve(size_t n) {
+    if (!ev[0])
+      for (auto& e : ev) OGB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    if (n <= bytes) return OK;
+    if (h) cudaFreeHost(h);
+    h = nullptr;
+    bytes = 0;
+    OGB_CUDA(cudaMallocHost(&h, n));
+    bytes = n;
+    return OK;
+  }
+};
+PackStage& pack_stage() {
+  static PackStage p;
+  return p;
+}
+}  // namespace
+
+// Expand packed tiles [t0, t1) into the reference's arrays: reached vertices
+// take their parent and depth, the others the -out_degree (or -1) sentinel
+// and depth 0; the DualOrder parent copy gets the sentinel everywhere
+// (BFS.c:58-74).  One pass, one team of host threads.
+static void expand_tiles(const BfsPackLayout& L, uint32_t V, const uint32_t* hp, const uint32_t* od, int* parents,
+                         uint32_t* dist, int* dual, size_t t0, size_t t1) {
+  if (t1 <= t0) return;
+  const uint32_t* off = hp + L.off_words;
+  const uint32_t* bm = hp + L.bitmap_words;
+  const uint8_t* d8 = reinterpret_cast<const uint8_t*>(hp + L.d8_words);
+  const int32_t* par = reinterpret_cast<const int32_t*>(hp + L.par_words);
+  const long nt = (long)(t1 - t0);
+#pragma omp parallel for num_threads(host_threads()) schedule(dynamic, 1)
+  for (long k = 0; k < nt; k++) {
+    {
+      const size_t t = t0 + (size_t)k;
+      uint32_t p = off[t];
+      const size_t v0 = t * kPackTile, v1 = std::min<size_t>(V, v0 + kPackTile);
+      for (size_t v = v0; v < v1; v++) {
+        const uint32_t d = od[v];
+        const int sentinel = d ? -(int)d : -1;
+        dual[v] = sentinel;
+        if ((bm[v >> 5] >> (v & 31)) & 1u) {
+          parents[v] = par[p++];
+          dist[v] = d8[v];
+        } else {
+          parents[v] = sentinel;
+          dist[v] = 0;
+        }
+      }
+    }
+  }
+}
+
+// The result of a search into host arrays: packed on the device (about
+// 12 MB instead of 32 MB at V = 4M; the host link is the bottleneck of a
+// call), copied in pieces, expanded by host threads as the pieces land.
+static int bfs_result_to_host(ogb_graph* dg, uint32_t V, uint32_t levels, const uint32_t* od, int* parents,
+                              uint32_t* dist, int* dual, cudaStream_t s) {
+  if (levels >= 255) {  // depths do not fit a byte: plain copies
+    OGB_TRY(d2h(parents, dg->d_parents.p, (size_t)V * 4, s));
+    OGB_TRY(d2h(dist, dg->d_distances.p, (size_t)V * 4, s));
+    host_par_for(V, [&](size_t lo, size_t hi) {
+      for (size_t v = lo; v < hi; v++) dual[v] = od[v] ? -(int)od[v] : -1;
+    });
+    return OK;
+  }
+  const BfsPackLayout L = bfs_pack_layout(V);
+  OGB_TRY(dg->d_pack.alloc(L.max_words * 4));
+  OGB_TRY(dg->d_pack_tmp.alloc(bfs_pack_tmp_words(V) * 4));
+  OGB_TRY(bfs_pack(V, dg->d_parents.as<int32_t>(), dg->d_distances.as<uint32_t>(), dg->d_pack.as<uint32_t>(),
+                   dg->d_pack_tmp.as<uint32_t>(), s));
+  PackStage& ps = pack_stage();
+  std::lock_guard<std::mutex> lk(ps.mu);
+  OGB_TRY(ps.reserve(L.max_words * 4));
+  const uint32_t* dp = dg->d_pack.as<uint32_t>();
+  OGB_CUDA(cudaMemcpyAsync(ps.h, dp, L.par_words * 4, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  const uint32_t R = ps.h[L.off_words + L.tiles];
+  const size_t chunk = std::max<size_t>(size_t(1) << 19, ((size_t)R + PackStage::kEv - 2) / (PackStage::kEv - 1));
+  const size_t nchunks = ((size_t)R + chunk - 1) / chunk;
+  for (size_t c = 0; c < nchunks; c++) {
+    const size_t a = L.par_words + c * chunk, n = std::min(chunk, (size_t)R - c * chunk);
+    OGB_CUDA(cudaMemcpyAsync(ps.h + a, dp + a, n * 4, cudaMemcpyDeviceToHost, s));
+    OGB_CUDA(cudaEventRecord(ps.ev[c], s));
+  }
+  const uint32_t* off = ps.h + L.off_words;
+  size_t done = 0;
+  for (size_t c = 0; c < nchunks; c++) {
+    OGB_CUDA(cudaEventSynchronize(ps.ev[c]));
+    const size_t recv = std::min((size_t)R, (c + 1) * chunk);
+    size_t hi = done;
+    while (hi < L.tiles && off[hi + 1] <= recv) hi++;
+    expand_tiles(L, V, ps.h, od, parents, dist, dual, done, hi);
+    done = hi;
+  }
+  expand_tiles(L, V, ps.h, od, parents, dist, dual, done, L.tiles);
+  return OK;
+}
+
 static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, uint32_t mode, const char* title,
                                    bool bitmap_nf) {
   const uint32_t V = graph->num_vertices;
@@ -1021,16 +1128,10 @@ static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, 
     say(" -----------------------------------------------------\n");
     return st0;
   }
-  // parents and distances are overwritten whole by the device result; only
-  // the DualOrder parent copy keeps its initial sentinels (BFS.c:64-73).  It
-  // is filled on host threads while the search runs on the GPU.
+  // parents, distances and the DualOrder parent copy (its initial sentinels,
+  // BFS.c:64-73) are written whole from the device result.
   BFSStats* st = bfs_stats_alloc(V);
   const uint32_t* od = graph->vertices->out_degree;
-  std::thread fill([st, od, V] {
-    host_par_for(V, [&](size_t lo, size_t hi) {
-      for (size_t v = lo; v < hi; v++) st->parents_DualOrder[v] = od[v] ? -(int)od[v] : -1;
-    });
-  });
   const uint32_t* labels = graph->sorted_edges_array ? graph->sorted_edges_array->label_array : nullptr;
   a->source = labels ? (int)labels[a->source] : a->source;
   say(" -----------------------------------------------------\n");
@@ -1042,10 +1143,7 @@ static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, 
   say(" -----------------------------------------------------\n");
   int status = OK;
   ogb_graph* dg = mirror_of(graph, &status);
-  if (!dg) {
-    fill.join();
-    die_status("device copy of GraphCSR", status);
-  }
+  if (!dg) die_status("device copy of GraphCSR", status);
   cudaStream_t s = lib_stream();
   // device result arrays live with the device copy (no per-call cudaMalloc)
   OGB_MUST(dg->d_parents.alloc((size_t)V * 4 + 4));
@@ -1055,9 +1153,7 @@ static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, 
   OGB_MUST(bfs_run(dg->g, (uint32_t)a->source, mode, dg->d_parents.as<int32_t>(), dg->d_distances.as<uint32_t>(),
                    &r, !quiet(), bitmap_nf, s));
   const double t_trav = now_s() - t0;
-  OGB_MUST(d2h(st->parents, dg->d_parents.p, (size_t)V * 4, s));
-  OGB_MUST(d2h(st->distances, dg->d_distances.p, (size_t)V * 4, s));
-  fill.join();
+  OGB_MUST(bfs_result_to_host(dg, V, (uint32_t)r.nlevels, od, st->parents, st->distances, st->parents_DualOrder, s));
   st->processed_nodes = r.processed_nodes;
   st->iteration = r.iteration;
   st->time_total = t_trav;

@@ -1010,6 +1010,105 @@ __global__ void __launch_bounds__(256) bfsk_reached(BfsBufs b, BfsDevState* st) 
   block_add_total<uint32_t>(&st->aux.reached, r, reinterpret_cast<uint32_t*>(s_red));
 }
 
+// ------------------------------------------------------------ packing ------
+
+// Reached bits (a warp per 1024 vertices: the ballot of step k is word k),
+// one-byte depths, and the reached count of every kPackTile-vertex tile.
+__global__ void __launch_bounds__(256) bfsk_pack_bits(uint32_t V, const int32_t* __restrict__ parents,
+                                                      const uint32_t* __restrict__ distances,
+                                                      uint32_t* __restrict__ bitmap, uint8_t* __restrict__ d8,
+                                                      uint32_t* __restrict__ tile_cnt) {
+  const uint32_t lane = lane_id();
+  const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
+  for (uint32_t wb = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); (uint64_t)wb * 1024 < V; wb += nwarps) {
+    const uint32_t base = wb * 1024;
+    uint32_t mine = 0;
+#pragma unroll 4
+    for (uint32_t k = 0; k < 32; k++) {
+      const uint32_t v = base + k * 32 + lane;
+      bool r = false;
+      if (v < V) {
+        r = parents[v] >= 0;
+        d8[v] = (uint8_t)distances[v];
+      }
+      const uint32_t word = __ballot_sync(0xffffffffu, r);
+      if (lane == k) mine = word;
+    }
+    if (base + lane * 32 < V) bitmap[wb * 32 + lane] = mine;
+    const uint32_t cnt = __reduce_add_sync(0xffffffffu, (uint32_t)__popc(mine));
+    if (lane == 0 && cnt) atomicAdd(&tile_cnt[base / kPackTile], cnt);
+  }
+}
+
+// Parents of the reached vertices, vertex order: a CTA per tile, a thread per
+// bitmap word (32 vertices), offsets by a block scan of the word counts.
+__global__ void __launch_bounds__(kPackTile / 32) bfsk_pack_parents(uint32_t V, const int32_t* __restrict__ parents,
+                                                                   const uint32_t* __restrict__ bitmap,
+                                                                   const uint32_t* __restrict__ tile_off,
+                                                                   int32_t* __restrict__ out) {
+  __shared__ uint32_t s_w[kPackTile / 32 / 32];
+  const uint32_t t = blockIdx.x;
+  const uint32_t w = t * (kPackTile / 32) + threadIdx.x;
+  const uint32_t word = ((uint64_t)w * 32 < V) ? bitmap[w] : 0u;
+  // block exclusive scan of popc(word)
+  const uint32_t c = __popc(word), lane = lane_id(), warp = threadIdx.x >> 5;
+  uint32_t x = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_w[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t y = lane < kPackTile / 32 / 32 ? s_w[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t z = __shfl_up_sync(0xffffffffu, y, o);
+      if (lane >= o) y += z;
+    }
+    if (lane < kPackTile / 32 / 32) s_w[lane] = y;
+  }
+  __syncthreads();
+  uint32_t o = tile_off[t] + (warp ? s_w[warp - 1] : 0u) + x - c;
+  uint32_t bits = word;
+  while (bits) {
+    const uint32_t i = (uint32_t)__ffs(bits) - 1;
+    out[o++] = parents[w * 32 + i];
+    bits &= bits - 1;
+  }
+}
+
+BfsPackLayout bfs_pack_layout(uint32_t V) {
+  BfsPackLayout L;
+  L.tiles = (V + kPackTile - 1) / kPackTile;
+  auto up4 = [](size_t x) { return (x + 3) & ~(size_t)3; };
+  L.off_words = 0;
+  L.bitmap_words = up4(L.tiles + 1);
+  L.d8_words = L.bitmap_words + up4(((size_t)V + 31) / 32);
+  L.par_words = L.d8_words + up4(((size_t)V + 3) / 4);
+  L.max_words = L.par_words + (size_t)V + 4;
+  return L;
+}
+
+int bfs_pack(uint32_t V, const int32_t* parents, const uint32_t* distances, uint32_t* out, uint32_t* tmp,
+             cudaStream_t s) {
+  const BfsPackLayout L = bfs_pack_layout(V);
+  uint32_t* tile_cnt = tmp;
+  uint32_t* scan_tmp = tmp + L.tiles + 4;
+  OGB_CUDA(cudaMemsetAsync(tile_cnt, 0, (L.tiles + 1) * 4, s));
+  bfsk_pack_bits<<<sm_count() * 8, 256, 0, s>>>(V, parents, distances, out + L.bitmap_words,
+                                                 reinterpret_cast<uint8_t*>(out + L.d8_words), tile_cnt);
+  OGB_CUDA(cudaGetLastError());
+  OGB_TRY(scan_exclusive_u32(tile_cnt, out + L.off_words, L.tiles, scan_tmp, s));
+  bfsk_pack_parents<<<L.tiles, kPackTile / 32, 0, s>>>(V, parents, out + L.bitmap_words, out + L.off_words,
+                                                      reinterpret_cast<int32_t*>(out + L.par_words));
+  OGB_CUDA(cudaGetLastError());
+  return OK;
+}
+
+size_t bfs_pack_tmp_words(uint32_t V) { return bfs_pack_layout(V).tiles + 8 + scan_tmp_words(bfs_pack_layout(V).tiles); }
+
 // ------------------------------------------------------------ drivers ------
 
 int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_t* distances, BfsResult* res,

@@ -75,6 +75,11 @@ int csr_map(DevCSR& c, DevCSR& other, uint32_t V, uint32_t E, uint32_t* d_err, c
 int csr_pack_rows(DevCSR& c, uint32_t V, cudaStream_t s);
 
 int sort_check(SortWorkspace& ws, cudaStream_t stream);
+
+// out[0..n] = exclusive scan of in[0..n) followed by the total (out holds
+// n + 1 entries); tmp holds scan_tmp_words(n) words.  scan.cu.
+int scan_exclusive_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t s);
+size_t scan_tmp_words(uint32_t n);
 int graph_check(DevGraph& g, cudaStream_t s);
 
 // ---- BFS -------------------------------------------------------------------
@@ -107,6 +112,20 @@ struct BfsSwitchState {
 // frontier size as the bitmap DO-BFS.
 int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_t* distances,
             BfsResult* res, bool time_levels, bool bu_entry_nf_frontier, cudaStream_t s);
+
+// Packed search result for a host copy: tile offsets (exclusive scan of the
+// reached count of every kPackTile-vertex tile, tiles + 1 words), the
+// reached bitmap, one byte of depth per vertex (valid when the search has
+// fewer than 255 levels) and the parents of the reached vertices in vertex
+// order; sections start at the word offsets below.  bfs.cu.
+constexpr uint32_t kPackTile = 8192;
+struct BfsPackLayout {
+  size_t tiles, off_words, bitmap_words, d8_words, par_words, max_words;
+};
+BfsPackLayout bfs_pack_layout(uint32_t V);
+size_t bfs_pack_tmp_words(uint32_t V);
+int bfs_pack(uint32_t V, const int32_t* parents, const uint32_t* distances, uint32_t* out, uint32_t* tmp,
+             cudaStream_t s);
 
 }  // namespace ogb
 

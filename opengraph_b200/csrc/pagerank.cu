@@ -563,92 +563,6 @@ __global__ void pr_rl_copy_kernel(uint32_t V, const uint2* __restrict__ rows, co
   }
 }
 
-// ---------------------------------------------------------------- scan ------
-
-constexpr uint32_t kScanTileN = 4096;  // 256 threads x 16
-
-__device__ __forceinline__ uint32_t block_excl_256(uint32_t v, uint32_t* s_w, uint32_t* total) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) s_w[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t t = lane < 8 ? s_w[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 8; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
-      if (lane >= o) t += y;
-    }
-    if (lane < 8) s_w[lane] = t;
-  }
-  __syncthreads();
-  *total = s_w[7];
-  const uint32_t r = (warp ? s_w[warp - 1] : 0) + x - v;
-  __syncthreads();
-  return r;
-}
-
-__global__ void __launch_bounds__(256) scan_tile_sum_kernel(const uint32_t* __restrict__ in, uint32_t n,
-                                                            uint32_t* __restrict__ sums) {
-  __shared__ uint32_t s_w[8];
-  const uint64_t base = (uint64_t)blockIdx.x * kScanTileN + threadIdx.x * 16;
-  uint32_t t = 0;
-  for (int k = 0; k < 16; k++)
-    if (base + k < n) t += in[base + k];
-  uint32_t total;
-  block_excl_256(t, s_w, &total);
-  if (threadIdx.x == 0) sums[blockIdx.x] = total;
-}
-
-// One CTA: exclusive scan of the tile sums in place; total into sums[ntiles].
-__global__ void __launch_bounds__(256) scan_sums_kernel(uint32_t* __restrict__ sums, uint32_t ntiles) {
-  __shared__ uint32_t s_w[8];
-  uint32_t carry = 0;
-  for (uint32_t b = 0; b < ntiles; b += 256) {
-    const uint32_t i = b + threadIdx.x;
-    const uint32_t v = i < ntiles ? sums[i] : 0u;
-    uint32_t total;
-    const uint32_t e = block_excl_256(v, s_w, &total);
-    if (i < ntiles) sums[i] = carry + e;
-    carry += total;
-  }
-  if (threadIdx.x == 0) sums[ntiles] = carry;
-}
-
-__global__ void __launch_bounds__(256) scan_tile_kernel(const uint32_t* __restrict__ in, uint32_t n,
-                                                        const uint32_t* __restrict__ sums, uint32_t* __restrict__ out) {
-  __shared__ uint32_t s_w[8];
-  const uint64_t base = (uint64_t)blockIdx.x * kScanTileN + threadIdx.x * 16;
-  uint32_t v[16], t = 0;
-  for (int k = 0; k < 16; k++) {
-    v[k] = base + k < n ? in[base + k] : 0u;
-    t += v[k];
-  }
-  uint32_t total;
-  uint32_t o = sums[blockIdx.x] + block_excl_256(t, s_w, &total);
-  for (int k = 0; k < 16; k++)
-    if (base + k < n) {
-      out[base + k] = o;
-      o += v[k];
-    }
-  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = sums[gridDim.x];
-}
-
-// out[0..n] = exclusive scan of in[0..n) followed by the total (out holds
-// n + 1 entries); tmp holds n / kScanTileN + 2 words.
-static int scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t s) {
-  const uint32_t ntiles = std::max<uint32_t>(1, ceil_div(n, kScanTileN));
-  scan_tile_sum_kernel<<<ntiles, 256, 0, s>>>(in, n, tmp);
-  scan_sums_kernel<<<1, 256, 0, s>>>(tmp, ntiles);
-  scan_tile_kernel<<<ntiles, 256, 0, s>>>(in, n, tmp, out);
-  OGB_CUDA(cudaGetLastError());
-  return OK;
-}
 
 // Push scatter: contrib of each source added to its out-neighbours, split by
 // out-degree like the pull gather (chunks scatter their edge range).
@@ -783,7 +697,7 @@ static int pr_build_relabel(DevGraph& g, PrWork* w, cudaStream_t s) {
   OGB_TRY(w->nbr_rl.alloc((size_t)E * 4 + 16));
   OGB_TRY(w->rows_rl.alloc((size_t)V * 8 + 16));
   OGB_TRY(w->off_light.alloc(Vp * 4));
-  OGB_TRY(w->rl_tmp.alloc((Vp * 8 + ((size_t)V / kScanTileN + 4)) * 4));
+  OGB_TRY(w->rl_tmp.alloc((Vp * 8 + scan_tmp_words(V)) * 4));
   const int grid = sm_count() * 8;
   uint32_t* t0 = w->rl_tmp.as<uint32_t>();
   uint32_t* a[8];
@@ -800,10 +714,10 @@ static int pr_build_relabel(DevGraph& g, PrWork* w, cudaStream_t s) {
   // into off_light, a4, a5, a6
   pr_rl_split_kernel<<<grid, 256, 0, s>>>(V, g.inv.d_rows(), g_warp_thr, g_cta_thr, a[0], a[1], a[2], a[3]);
   OGB_CUDA(cudaGetLastError());
-  OGB_TRY(scan_exclusive(a[0], w->off_light.as<uint32_t>(), V, scan_tmp, s));
-  OGB_TRY(scan_exclusive(a[1], a[4], V, scan_tmp, s));
-  OGB_TRY(scan_exclusive(a[2], a[5], V, scan_tmp, s));
-  OGB_TRY(scan_exclusive(a[3], a[6], V, scan_tmp, s));
+  OGB_TRY(scan_exclusive_u32(a[0], w->off_light.as<uint32_t>(), V, scan_tmp, s));
+  OGB_TRY(scan_exclusive_u32(a[1], a[4], V, scan_tmp, s));
+  OGB_TRY(scan_exclusive_u32(a[2], a[5], V, scan_tmp, s));
+  OGB_TRY(scan_exclusive_u32(a[3], a[6], V, scan_tmp, s));
   uint32_t tot[3];
   OGB_CUDA(cudaMemcpyAsync(&tot[0], w->off_light.as<uint32_t>() + V, 4, cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaMemcpyAsync(&tot[1], a[4] + V, 4, cudaMemcpyDeviceToHost, s));
