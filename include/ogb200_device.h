@@ -112,6 +112,25 @@ int ogb_bfs(ogb_graph *g, uint32_t root, uint32_t mode, int32_t *d_parents, uint
 /* Level trace of the last ogb_bfs on g (up to max_levels entries). */
 int ogb_bfs_trace(ogb_graph *g, ogb_bfs_level *levels, uint32_t max_levels, uint32_t *count);
 
+/* Multi-source BFS (no reference counterpart: a batch of the reference's
+ * single-root searches, BFS.c:476-626).  Up to 64 roots (host array), one
+ * bit-lane each; d_depths (device, V * 64 uint16) receives, for vertex v and
+ * lane i, d_depths[v * 64 + i] = v's depth in the search from roots[i], or
+ * 0xFFFF when unreached.  Every lane's depths equal the single-root BFS
+ * distances of that root. */
+typedef struct ogb_msbfs_info
+{
+    uint32_t levels;           /* levels until every frontier emptied     */
+    uint32_t push_levels;
+    uint32_t pull_levels;
+    uint32_t launches;
+    uint64_t reached_pairs;    /* (vertex, lane) pairs reached, roots too */
+    uint64_t edges_examined;
+    double ms;                 /* device time of the batch                */
+} ogb_msbfs_info;
+int ogb_msbfs(ogb_graph *g, const uint32_t *roots, uint32_t nroots, uint16_t *d_depths, ogb_msbfs_info *info,
+              void *stream);
+
 /* PageRank; mode 0 pull, 1 push.  d_ranks receives V normalized ranks;
  * d_init (may be NULL) replaces the uniform unnormalized start 1-0.85. */
 int ogb_pagerank(ogb_graph *g, uint32_t mode, uint32_t max_iterations, double epsilon, float *d_ranks,

@@ -121,6 +121,11 @@ class BfsInfo(C.Structure):
                 ("edges_examined", C.c_uint64), ("ms", C.c_double), ("launches", u32), ("pad", u32)]
 
 
+class MsBfsInfo(C.Structure):
+    _fields_ = [("levels", u32), ("push_levels", u32), ("pull_levels", u32), ("launches", u32),
+                ("reached_pairs", C.c_uint64), ("edges_examined", C.c_uint64), ("ms", C.c_double)]
+
+
 class BfsLevel(C.Structure):
     _fields_ = [("direction", u32), ("discovered", u32), ("frontier", u32), ("mf", u32), ("mu", u32),
                 ("pad", u32), ("edges", C.c_uint64), ("ms", C.c_float), ("pad2", C.c_float)]
@@ -197,6 +202,7 @@ _DEVICE_API = [
     ("ogb_sort_edges", C.c_int, [vp, vp, vp, u32, u32, vp, vp, vp, vp]),
     ("ogb_bfs", C.c_int, [vp, u32, u32, vp, vp, C.POINTER(BfsInfo), vp]),
     ("ogb_bfs_trace", C.c_int, [vp, C.POINTER(BfsLevel), u32, C.POINTER(u32)]),
+    ("ogb_msbfs", C.c_int, [vp, u32p, u32, vp, C.POINTER(MsBfsInfo), vp]),
     ("ogb_pagerank", C.c_int, [vp, u32, u32, C.c_double, vp, vp, C.POINTER(PrInfo), vp]),
     ("ogb_pagerank_history", C.c_int, [vp, C.POINTER(C.c_double), u32p, u32, C.POINTER(u32)]),
     ("ogb_pagerank_set_bins", None, [u32, u32]),
@@ -388,6 +394,15 @@ class DeviceGraph:
         info = BfsInfo()
         self.lib.check(self.lib.ogb_bfs(self.handle, int(root), int(mode), _ptr(parents), _ptr(distances),
                                         C.byref(info), stream), "ogb_bfs")
+        return info_dict(info)
+
+    def msbfs(self, roots, depths, stream=None) -> dict:
+        """Up to 64 searches at once; depths is a device uint16/int16 tensor
+        of V * 64 entries (row v = v's depth in each lane, 0xFFFF unreached)."""
+        arr = (u32 * len(roots))(*[int(r) for r in roots])
+        info = MsBfsInfo()
+        self.lib.check(self.lib.ogb_msbfs(self.handle, arr, len(roots), _ptr(depths), C.byref(info), stream),
+                       "ogb_msbfs")
         return info_dict(info)
 
     def bfs_trace(self, max_levels: int = 512) -> list[dict]:

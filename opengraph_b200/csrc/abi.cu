@@ -1432,6 +1432,23 @@ extern "C" int ogb_bfs(ogb_graph* g, uint32_t root, uint32_t mode, int32_t* d_pa
   return OK;
 }
 
+extern "C" int ogb_msbfs(ogb_graph* g, const uint32_t* roots, uint32_t nroots, uint16_t* d_depths,
+                         ogb_msbfs_info* info, void* stream) {
+  if (!g || !roots || !d_depths) return fail(ERR_ARG, "ogb_msbfs: null argument");
+  MsResult r;
+  OGB_TRY(msbfs_run(g->g, roots, nroots, d_depths, &r, as_stream(stream)));
+  if (info) {
+    info->levels = r.levels;
+    info->push_levels = r.push_levels;
+    info->pull_levels = r.pull_levels;
+    info->launches = r.launches;
+    info->reached_pairs = r.reached;
+    info->edges_examined = r.edges_examined;
+    info->ms = r.ms;
+  }
+  return OK;
+}
+
 extern "C" int ogb_bfs_trace(ogb_graph* g, ogb_bfs_level* levels, uint32_t max_levels, uint32_t* count) {
   if (!g) return fail(ERR_ARG, "null");
   const uint32_t n = std::min<uint32_t>(max_levels, (uint32_t)g->g.bfs_last_levels);

@@ -63,6 +63,7 @@ int sm_count() {
 DevGraph::~DevGraph() {
   bfs_work_free(bfs);
   pr_work_free(pr);
+  ms_work_free(ms);
 }
 
 // ------------------------------------------------------------- CSR kernels --

@@ -26,8 +26,10 @@ struct DevCSR {
 
 struct BfsWork;  // bfs.cu
 struct PrWork;   // pagerank.cu
+struct MsWork;   // batch.cu
 void bfs_work_free(BfsWork* w);
 void pr_work_free(PrWork* w);
+void ms_work_free(MsWork* w);
 
 struct BfsLevel {
   uint32_t direction;  // 0 top-down, 1 bottom-up
@@ -50,6 +52,7 @@ struct DevGraph {
   uint32_t build_id = 0;  // bumped whenever the edges change (caches key on it)
   BfsWork* bfs = nullptr;
   PrWork* pr = nullptr;
+  MsWork* ms = nullptr;
   // traces of the last BFS / PageRank run through the device API
   int bfs_last_levels = 0;
   BfsLevel bfs_trace[512];
@@ -112,6 +115,17 @@ struct BfsSwitchState {
 // frontier size as the bitmap DO-BFS.
 int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_t* distances,
             BfsResult* res, bool time_levels, bool bu_entry_nf_frontier, cudaStream_t s);
+
+// ---- multi-source BFS (batch.cu) -------------------------------------------
+struct MsResult {
+  uint32_t levels = 0, push_levels = 0, pull_levels = 0, launches = 0;
+  unsigned long long reached = 0;         // (vertex, lane) pairs reached, roots included
+  unsigned long long edges_examined = 0;  // edges read by the levels
+  double ms = 0.0;                        // device time
+};
+// Up to 64 BFS searches at once, one lane per root; depth[v * 64 + lane] =
+// depth of v in that lane's search, 0xFFFF when unreached (V * 64 u16).
+int msbfs_run(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint16_t* depth, MsResult* res, cudaStream_t s);
 
 // Packed search result for a host copy: tile offsets (exclusive scan of the
 // reached count of every kPackTile-vertex tile, tiles + 1 words), the
