@@ -131,6 +131,25 @@ typedef struct ogb_msbfs_info
 int ogb_msbfs(ogb_graph *g, const uint32_t *roots, uint32_t nroots, uint16_t *d_depths, ogb_msbfs_info *info,
               void *stream);
 
+/* Batched personalized PageRank (no reference counterpart: the reference's
+ * pull PageRank, pageRank.c:984-1044, with the teleport term replaced by
+ * (1 - 0.85) on the seed vertex only).  Up to 32 seeds (host array), one
+ * vector each, started from the seed's one-hot vector; d_ranks (device, may
+ * be NULL) receives V * 32 floats, d_ranks[v * 32 + k] = v's (unnormalized)
+ * rank in seed k's vector.  Stops after an iteration in which every vector
+ * changed by < epsilon (L1), or after max_iterations. */
+typedef struct ogb_ppr_info
+{
+    uint32_t executed;         /* iterations run                          */
+    uint32_t converged;        /* 1 when the epsilon rule stopped the run */
+    uint32_t launches;
+    uint32_t pad;
+    double ms;                 /* device time                             */
+    double err_last[32];       /* last L1 change of each seed's vector    */
+} ogb_ppr_info;
+int ogb_ppr(ogb_graph *g, const uint32_t *seeds, uint32_t nseeds, uint32_t max_iterations, double epsilon,
+            float *d_ranks, ogb_ppr_info *info, void *stream);
+
 /* PageRank; mode 0 pull, 1 push.  d_ranks receives V normalized ranks;
  * d_init (may be NULL) replaces the uniform unnormalized start 1-0.85. */
 int ogb_pagerank(ogb_graph *g, uint32_t mode, uint32_t max_iterations, double epsilon, float *d_ranks,

@@ -126,6 +126,11 @@ class MsBfsInfo(C.Structure):
                 ("reached_pairs", C.c_uint64), ("edges_examined", C.c_uint64), ("ms", C.c_double)]
 
 
+class PprBatchInfo(C.Structure):
+    _fields_ = [("executed", u32), ("converged", u32), ("launches", u32), ("pad", u32), ("ms", C.c_double),
+                ("err_last", C.c_double * 32)]
+
+
 class BfsLevel(C.Structure):
     _fields_ = [("direction", u32), ("discovered", u32), ("frontier", u32), ("mf", u32), ("mu", u32),
                 ("pad", u32), ("edges", C.c_uint64), ("ms", C.c_float), ("pad2", C.c_float)]
@@ -203,6 +208,7 @@ _DEVICE_API = [
     ("ogb_bfs", C.c_int, [vp, u32, u32, vp, vp, C.POINTER(BfsInfo), vp]),
     ("ogb_bfs_trace", C.c_int, [vp, C.POINTER(BfsLevel), u32, C.POINTER(u32)]),
     ("ogb_msbfs", C.c_int, [vp, u32p, u32, vp, C.POINTER(MsBfsInfo), vp]),
+    ("ogb_ppr", C.c_int, [vp, u32p, u32, u32, C.c_double, vp, C.POINTER(PprBatchInfo), vp]),
     ("ogb_pagerank", C.c_int, [vp, u32, u32, C.c_double, vp, vp, C.POINTER(PrInfo), vp]),
     ("ogb_pagerank_history", C.c_int, [vp, C.POINTER(C.c_double), u32p, u32, C.POINTER(u32)]),
     ("ogb_pagerank_set_bins", None, [u32, u32]),
@@ -404,6 +410,17 @@ class DeviceGraph:
         self.lib.check(self.lib.ogb_msbfs(self.handle, arr, len(roots), _ptr(depths), C.byref(info), stream),
                        "ogb_msbfs")
         return info_dict(info)
+
+    def ppr(self, seeds, ranks=None, max_iterations: int = 20, epsilon: float = 0.0, stream=None) -> dict:
+        """Personalized PageRank for up to 32 one-hot seeds; ranks (device
+        float32, V * 32) receives row v = v's rank in each seed's vector."""
+        arr = (u32 * len(seeds))(*[int(x) for x in seeds])
+        info = PprBatchInfo()
+        self.lib.check(self.lib.ogb_ppr(self.handle, arr, len(seeds), int(max_iterations), float(epsilon),
+                                        _ptr(ranks), C.byref(info), stream), "ogb_ppr")
+        d = info_dict(info)
+        d["err_last"] = list(info.err_last)[:len(seeds)]
+        return d
 
     def bfs_trace(self, max_levels: int = 512) -> list[dict]:
         arr = (BfsLevel * max_levels)()

@@ -1449,6 +1449,22 @@ extern "C" int ogb_msbfs(ogb_graph* g, const uint32_t* roots, uint32_t nroots, u
   return OK;
 }
 
+extern "C" int ogb_ppr(ogb_graph* g, const uint32_t* seeds, uint32_t nseeds, uint32_t max_iterations,
+                       double epsilon, float* d_ranks, ogb_ppr_info* info, void* stream) {
+  if (!g || !seeds) return fail(ERR_ARG, "ogb_ppr: null argument");
+  PprResult r;
+  OGB_TRY(ppr_run(g->g, seeds, nseeds, max_iterations, epsilon, d_ranks, &r, as_stream(stream)));
+  if (info) {
+    info->executed = r.executed;
+    info->converged = r.converged;
+    info->launches = r.launches;
+    info->pad = 0;
+    info->ms = r.ms;
+    for (int k = 0; k < 32; k++) info->err_last[k] = r.err_last[k];
+  }
+  return OK;
+}
+
 extern "C" int ogb_bfs_trace(ogb_graph* g, ogb_bfs_level* levels, uint32_t max_levels, uint32_t* count) {
   if (!g) return fail(ERR_ARG, "null");
   const uint32_t n = std::min<uint32_t>(max_levels, (uint32_t)g->g.bfs_last_levels);

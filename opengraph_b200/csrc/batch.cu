@@ -403,4 +403,328 @@ int msbfs_run(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint16_t* dep
   return OK;
 }
 
+
+// ===========================================================================
+// Batched personalized PageRank (no reference counterpart: the reference's
+// pull PageRank, pageRank.c:984-1044, with the teleport term base_pr
+// replaced by (1 - d) on the seed vertex only, one vector per seed).  Up to
+// 32 seeds at once; ranks are row-major by vertex, 32 floats (128 bytes) per
+// vertex, so every in-edge gathers one full cache line: the 32 contribs of
+// its source.  Per iteration, for every vertex v and seed k:
+//   s_k = sum of c_k[u] over the in-edges (u, v)
+//   r'_k[v] = (v == seed_k ? 1 - d : 0) + d * s_k,  c'_k[v] = r'_k[v] / out_degree(v)
+//   err_k += |r'_k[v] - r_k[v]|   (fp64)
+// starting from r_k = e_seed_k; the run stops when every seed's err_k is
+// below epsilon, or after max_iterations.  A warp takes a vertex (or a chunk
+// of a long row): its four 8-lane groups walk the row's edges in turn, each
+// lane owning 4 seeds (one float4 of the row), four edges per group in
+// flight; the groups' sums are folded at the end.  Rows longer than
+// kPprChunk edges are cut into chunks (handed out one per claim, before the
+// other vertices, 64 per claim) whose sums the warp finishing the last one
+// adds in chunk order.  Dangling vertices' rank is not redistributed,
+// as in the reference.
+// ===========================================================================
+
+constexpr uint32_t kPprSeeds = 32;
+constexpr uint32_t kPprChunk = 512;
+constexpr uint32_t kPprMaxIters = 1024;
+
+struct PprCtl {
+  double err[kPprMaxIters][kPprSeeds];
+  uint32_t stop, stop_iter;
+  uint32_t claim_chunk[kPprMaxIters];  // chunks handed out, one per claim
+  uint32_t claim_row[kPprMaxIters];    // other vertices handed out, 64 per claim
+};
+
+struct PprChunk {
+  uint32_t v, j0, j1, k;  // vertex, edge range, index of the vertex among the chunked ones
+};
+
+struct PprWork {
+  uint32_t V = 0, build = 0;
+  bool ready = false;
+  DevBuf R, C0, C1, ctl, chunks, vfirst, vcount, done, partials, light;
+  uint32_t n_chunks = 0, n_cut = 0, n_light = 0;
+  PprCtl* h_ctl = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  ~PprWork() {
+    if (h_ctl) cudaFreeHost(h_ctl);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+  }
+};
+
+void ppr_work_free(PprWork* w) { delete w; }
+
+__global__ void pprk_seed(const uint32_t* __restrict__ seeds, uint32_t nseeds, const uint32_t* __restrict__ out_degree,
+                          float* __restrict__ R, float* __restrict__ C) {
+  const uint32_t k = threadIdx.x;
+  if (k < nseeds) {
+    const uint32_t v = seeds[k];
+    R[(size_t)v * kPprSeeds + k] = 1.0f;
+    const uint32_t d = out_degree[v];
+    C[(size_t)v * kPprSeeds + k] = d ? __fdiv_rn(1.0f, (float)d) : 0.0f;
+  }
+}
+
+// Sum of the 32-float contrib rows of in-edges [j0, j1) (each lane: 4 seeds):
+// group g of 8 lanes takes edges g, g+4, g+8, g+12, then the next 16, four
+// rows in flight per group; the four groups are folded at the end.
+__device__ __forceinline__ float4 ppr_row_sum(const uint32_t* __restrict__ nbr, const float4* __restrict__ C4,
+                                              uint32_t j0, uint32_t j1, uint32_t grp, uint32_t sub) {
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (uint32_t j = j0 + grp; j < j1; j += 16) {
+    uint32_t u[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) u[q] = (j + 4 * q < j1) ? (__ldg(&nbr[j + 4 * q]) & 0x3FFFFFFFu) : 0xFFFFFFFFu;
+    float4 c[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      c[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (u[q] != 0xFFFFFFFFu) c[q] = __ldg(&C4[(size_t)u[q] * 8 + sub]);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      acc.x += c[q].x;
+      acc.y += c[q].y;
+      acc.z += c[q].z;
+      acc.w += c[q].w;
+    }
+  }
+  // fold the four groups (lanes sub, sub + 8, sub + 16, sub + 24)
+#pragma unroll
+  for (int o = 8; o < 32; o <<= 1) {
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+    acc.z += __shfl_xor_sync(0xffffffffu, acc.z, o);
+    acc.w += __shfl_xor_sync(0xffffffffu, acc.w, o);
+  }
+  return acc;
+}
+
+struct PprParams {
+  float damp, base;
+  double eps;
+  uint32_t nseeds;
+  const uint32_t* seeds;
+};
+
+// Update of vertex v from its sums (lanes 0..7 hold seeds 4l..4l+3).
+__device__ __forceinline__ void ppr_update(uint32_t v, float4 s, uint32_t sub, const PprParams& p,
+                                           const uint32_t* __restrict__ out_degree, float* __restrict__ R,
+                                           float* __restrict__ Cn, double* err4) {
+  const uint32_t d = out_degree[v];
+  float4* R4 = reinterpret_cast<float4*>(R) + (size_t)v * 8 + sub;
+  float4* C4 = reinterpret_cast<float4*>(Cn) + (size_t)v * 8 + sub;
+  const float4 old = *R4;
+  float sv[4] = {s.x, s.y, s.z, s.w}, ov[4] = {old.x, old.y, old.z, old.w}, nv[4], cv[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const uint32_t k = sub * 4 + i;
+    const float tele = (k < p.nseeds && p.seeds[k] == v) ? p.base : 0.0f;
+    nv[i] = __fadd_rn(tele, __fmul_rn(p.damp, sv[i]));
+    cv[i] = d ? __fdiv_rn(nv[i], (float)d) : 0.0f;
+    err4[i] += fabs((double)nv[i] - (double)ov[i]);
+  }
+  *R4 = make_float4(nv[0], nv[1], nv[2], nv[3]);
+  *C4 = make_float4(cv[0], cv[1], cv[2], cv[3]);
+}
+
+__global__ void __launch_bounds__(256) pprk_iter(const PprChunk* __restrict__ chunks, uint32_t n_chunks,
+                                                 const uint32_t* __restrict__ vfirst,
+                                                 const uint32_t* __restrict__ vcount, uint32_t* __restrict__ done,
+                                                 float4* __restrict__ partials, const uint32_t* __restrict__ light,
+                                                 uint32_t n_light, const uint2* __restrict__ rows,
+                                                 const uint32_t* __restrict__ nbr,
+                                                 const uint32_t* __restrict__ out_degree, const float* __restrict__ C,
+                                                 float* __restrict__ Cn, float* __restrict__ R, PprParams p,
+                                                 PprCtl* __restrict__ ctl, uint32_t it) {
+  __shared__ double s_err[8][kPprSeeds];
+  if (ctl->stop) return;
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  const uint32_t grp = lane >> 3, sub = lane & 7;
+  const float4* C4 = reinterpret_cast<const float4*>(C);
+  double err4[4] = {0, 0, 0, 0};
+  // chunks of long rows, one per claim
+  for (;;) {
+    uint32_t t = 0;
+    if (lane == 0) t = atomicAdd(&ctl->claim_chunk[it], 1u);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= n_chunks) break;
+    const PprChunk ci = chunks[t];
+    const float4 s = ppr_row_sum(nbr, C4, ci.j0, ci.j1, grp, sub);
+    uint32_t last = 0;
+    if (lane < 8) partials[(size_t)t * 8 + sub] = s;
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) last = (atomicAdd(&done[ci.k], 1u) == vcount[ci.k] - 1) ? 1u : 0u;
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (last) {
+      __threadfence();
+      const uint32_t f = vfirst[ci.k], cnt = vcount[ci.k];
+      float4 tot = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (uint32_t c = 0; c < cnt; c++) {
+        const float4 q = __ldcg(&partials[(size_t)(f + c) * 8 + sub]);
+        tot.x += q.x;
+        tot.y += q.y;
+        tot.z += q.z;
+        tot.w += q.w;
+      }
+      if (lane < 8) ppr_update(ci.v, tot, sub, p, out_degree, R, Cn, err4);
+      if (lane == 0) done[ci.k] = 0;
+    }
+  }
+  // the other vertices, 64 per claim
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&ctl->claim_row[it], 64u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n_light) break;
+    const uint32_t end = min(base + 64, n_light);
+    for (uint32_t t = base; t < end; t++) {
+      const uint32_t v = light[t];
+      const uint2 r = rows[v];
+      const float4 s = ppr_row_sum(nbr, C4, r.x, r.x + r.y, grp, sub);
+      if (lane < 8) ppr_update(v, s, sub, p, out_degree, R, Cn, err4);
+    }
+  }
+  // per-seed error: lanes 0..7 hold seeds 4l..4l+3
+  if (lane < 8)
+    for (int i = 0; i < 4; i++) s_err[warp][lane * 4 + i] = err4[i];
+  __syncthreads();
+  if (threadIdx.x < kPprSeeds) {
+    double e = 0.0;
+    for (int w = 0; w < 8; w++) e += s_err[w][threadIdx.x];
+    if (e != 0.0) atomicAdd(&ctl->err[it][threadIdx.x], e);
+  }
+}
+
+// the run stops after an iteration in which every seed changed by < eps (L1)
+__global__ void pprk_check(PprCtl* __restrict__ ctl, uint32_t it, uint32_t nseeds, double eps) {
+  if (threadIdx.x != 0 || ctl->stop) return;
+  bool all = true;
+  for (uint32_t k = 0; k < nseeds; k++) all = all && (ctl->err[it][k] < eps);
+  if (all) {
+    ctl->stop = 1;
+    ctl->stop_iter = it;
+  }
+}
+
+static int ppr_work_get(DevGraph& g, PprWork** out, cudaStream_t s) {
+  if (!g.ppr) g.ppr = new PprWork();
+  PprWork* w = g.ppr;
+  const uint32_t V = g.V;
+  if (w->V != V || !w->R.p) {
+    OGB_TRY(w->R.alloc((size_t)V * kPprSeeds * 4 + 64));
+    OGB_TRY(w->C0.alloc((size_t)V * kPprSeeds * 4 + 64));
+    OGB_TRY(w->C1.alloc((size_t)V * kPprSeeds * 4 + 64));
+    OGB_TRY(w->ctl.alloc(sizeof(PprCtl) + 64));
+    w->V = V;
+    w->ready = false;
+  }
+  if (!w->h_ctl) OGB_CUDA(cudaMallocHost(&w->h_ctl, sizeof(PprCtl)));
+  if (!w->ev0) {
+    OGB_CUDA(cudaEventCreate(&w->ev0));
+    OGB_CUDA(cudaEventCreate(&w->ev1));
+  }
+  if (!w->ready || w->build != g.build_id) {
+    // rows from the inverse CSR: rows over kPprChunk in-edges become chunks
+    const uint2* rows = g.inv.d_rows();
+    std::vector<uint2> h_rows(V);
+    OGB_CUDA(cudaMemcpyAsync(h_rows.data(), rows, (size_t)V * 8, cudaMemcpyDeviceToHost, s));
+    OGB_CUDA(cudaStreamSynchronize(s));
+    std::vector<uint32_t> light;
+    std::vector<PprChunk> chunks;
+    std::vector<uint32_t> first, count;
+    light.reserve(V);
+    for (uint32_t v = 0; v < V; v++) {
+      const uint2 r = h_rows[v];
+      if (r.y > kPprChunk) {
+        const uint32_t k = (uint32_t)first.size();
+        first.push_back((uint32_t)chunks.size());
+        for (uint32_t c = 0; c < r.y; c += kPprChunk) chunks.push_back({v, r.x + c, r.x + std::min(r.y, c + kPprChunk), k});
+        count.push_back((uint32_t)chunks.size() - first.back());
+      } else {
+        light.push_back(v);
+      }
+    }
+    w->n_light = (uint32_t)light.size();
+    w->n_chunks = (uint32_t)chunks.size();
+    w->n_cut = (uint32_t)first.size();
+    OGB_TRY(w->light.alloc((size_t)w->n_light * 4 + 16));
+    OGB_TRY(w->chunks.alloc((size_t)w->n_chunks * sizeof(PprChunk) + 16));
+    OGB_TRY(w->partials.alloc((size_t)w->n_chunks * kPprSeeds * 4 + 16));
+    OGB_TRY(w->vfirst.alloc((size_t)w->n_cut * 4 + 16));
+    OGB_TRY(w->vcount.alloc((size_t)w->n_cut * 4 + 16));
+    OGB_TRY(w->done.alloc((size_t)w->n_cut * 4 + 16));
+    if (w->n_light) OGB_CUDA(cudaMemcpyAsync(w->light.p, light.data(), light.size() * 4, cudaMemcpyHostToDevice, s));
+    if (w->n_chunks)
+      OGB_CUDA(cudaMemcpyAsync(w->chunks.p, chunks.data(), chunks.size() * sizeof(PprChunk), cudaMemcpyHostToDevice, s));
+    if (w->n_cut) {
+      OGB_CUDA(cudaMemcpyAsync(w->vfirst.p, first.data(), first.size() * 4, cudaMemcpyHostToDevice, s));
+      OGB_CUDA(cudaMemcpyAsync(w->vcount.p, count.data(), count.size() * 4, cudaMemcpyHostToDevice, s));
+    }
+    OGB_CUDA(cudaMemsetAsync(w->done.p, 0, (size_t)w->n_cut * 4 + 16, s));
+    OGB_CUDA(cudaStreamSynchronize(s));
+    w->ready = true;
+    w->build = g.build_id;
+  }
+  *out = w;
+  return OK;
+}
+
+int ppr_run(DevGraph& g, const uint32_t* seeds, uint32_t nseeds, uint32_t max_iters, double epsilon, float* ranks,
+            PprResult* res, cudaStream_t s) {
+  const uint32_t V = g.V;
+  if (nseeds == 0 || nseeds > kPprSeeds) return fail(ERR_ARG, "ppr: %u seeds (1..%u)", nseeds, kPprSeeds);
+  if (max_iters > kPprMaxIters) return fail(ERR_ARG, "ppr: at most %u iterations", kPprMaxIters);
+  for (uint32_t i = 0; i < nseeds; i++)
+    if (seeds[i] >= V) return fail(ERR_ARG, "ppr: seed %u out of range (V=%u)", seeds[i], V);
+  PprWork* w = nullptr;
+  OGB_TRY(ppr_work_get(g, &w, s));
+  DevBuf d_seeds;
+  OGB_TRY(d_seeds.alloc(kPprSeeds * 4));
+  OGB_CUDA(cudaMemcpyAsync(d_seeds.p, seeds, nseeds * 4, cudaMemcpyHostToDevice, s));
+  PprCtl* ctl = w->ctl.as<PprCtl>();
+  float* C = w->C0.as<float>();
+  float* Cn = w->C1.as<float>();
+  float* R = w->R.as<float>();
+  PprParams p;
+  p.damp = 0.85f;
+  p.base = 1.0f - p.damp;
+  p.eps = epsilon;
+  p.nseeds = nseeds;
+  p.seeds = d_seeds.as<uint32_t>();
+  const int sms = sm_count();
+  OGB_CUDA(cudaEventRecord(w->ev0, s));
+  OGB_CUDA(cudaMemsetAsync(ctl, 0, sizeof(PprCtl), s));
+  OGB_CUDA(cudaMemsetAsync(R, 0, (size_t)V * kPprSeeds * 4, s));
+  OGB_CUDA(cudaMemsetAsync(C, 0, (size_t)V * kPprSeeds * 4, s));
+  pprk_seed<<<1, 32, 0, s>>>(p.seeds, nseeds, g.fwd.d_out_degree(), R, C);
+  OGB_CUDA(cudaGetLastError());
+  for (uint32_t it = 0; it < max_iters; it++) {
+    pprk_iter<<<sms * 8, 256, 0, s>>>(w->chunks.as<PprChunk>(), w->n_chunks, w->vfirst.as<uint32_t>(),
+                                      w->vcount.as<uint32_t>(), w->done.as<uint32_t>(), w->partials.as<float4>(),
+                                      w->light.as<uint32_t>(), w->n_light, g.inv.d_rows(), g.inv.d_dst(),
+                                      g.fwd.d_out_degree(), C, Cn, R, p, ctl, it);
+    pprk_check<<<1, 32, 0, s>>>(ctl, it, nseeds, epsilon);
+    OGB_CUDA(cudaGetLastError());
+    std::swap(C, Cn);
+  }
+  OGB_CUDA(cudaEventRecord(w->ev1, s));
+  if (ranks) OGB_CUDA(cudaMemcpyAsync(ranks, R, (size_t)V * kPprSeeds * 4, cudaMemcpyDeviceToDevice, s));
+  OGB_CUDA(cudaMemcpyAsync(w->h_ctl, ctl, sizeof(PprCtl), cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  OGB_CUDA(cudaEventElapsedTime(&ms, w->ev0, w->ev1));
+  PprResult r;
+  r.ms = ms;
+  r.executed = w->h_ctl->stop ? w->h_ctl->stop_iter + 1 : max_iters;
+  r.converged = w->h_ctl->stop;
+  r.launches = 2 + 2 * max_iters;
+  for (uint32_t k = 0; k < nseeds; k++) r.err_last[k] = r.executed ? w->h_ctl->err[r.executed - 1][k] : 0.0;
+  if (res) *res = r;
+  return OK;
+}
+
 }  // namespace ogb

@@ -64,6 +64,7 @@ DevGraph::~DevGraph() {
   bfs_work_free(bfs);
   pr_work_free(pr);
   ms_work_free(ms);
+  ppr_work_free(ppr);
 }
 
 // ------------------------------------------------------------- CSR kernels --

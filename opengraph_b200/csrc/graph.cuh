@@ -27,9 +27,11 @@ struct DevCSR {
 struct BfsWork;  // bfs.cu
 struct PrWork;   // pagerank.cu
 struct MsWork;   // batch.cu
+struct PprWork;  // batch.cu
 void bfs_work_free(BfsWork* w);
 void pr_work_free(PrWork* w);
 void ms_work_free(MsWork* w);
+void ppr_work_free(PprWork* w);
 
 struct BfsLevel {
   uint32_t direction;  // 0 top-down, 1 bottom-up
@@ -53,6 +55,7 @@ struct DevGraph {
   BfsWork* bfs = nullptr;
   PrWork* pr = nullptr;
   MsWork* ms = nullptr;
+  PprWork* ppr = nullptr;
   // traces of the last BFS / PageRank run through the device API
   int bfs_last_levels = 0;
   BfsLevel bfs_trace[512];
@@ -126,6 +129,17 @@ struct MsResult {
 // Up to 64 BFS searches at once, one lane per root; depth[v * 64 + lane] =
 // depth of v in that lane's search, 0xFFFF when unreached (V * 64 u16).
 int msbfs_run(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint16_t* depth, MsResult* res, cudaStream_t s);
+
+// ---- batched personalized PageRank (batch.cu) -------------------------------
+struct PprResult {
+  uint32_t executed = 0, converged = 0, launches = 0;
+  double ms = 0.0;
+  double err_last[32] = {};  // L1 change of each seed's vector in the last iteration
+};
+// Up to 32 one-hot seeds; ranks (may be null) receives V * 32 floats, row v
+// = v's rank in each seed's vector (unnormalized, as the reference's pull).
+int ppr_run(DevGraph& g, const uint32_t* seeds, uint32_t nseeds, uint32_t max_iters, double epsilon, float* ranks,
+            PprResult* res, cudaStream_t s);
 
 // Packed search result for a host copy: tile offsets (exclusive scan of the
 // reached count of every kPackTile-vertex tile, tiles + 1 words), the

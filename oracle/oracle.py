@@ -137,6 +137,36 @@ class Oracle:
                                 _p(init), _p(ranks))
         return ranks
 
+    @staticmethod
+    def ppr_f64(g: dict, seeds, iters: int, damp: float = 0.85):
+        """Personalized PageRank in FP64, one vector per seed, as a restatement
+        of the reference's pull iteration (pageRank.c:984-1044) with the
+        teleport term base_pr replaced by (1 - damp) on the seed vertex only,
+        started from the seed's one-hot vector; dangling rank is not
+        redistributed (as in the reference).  Returns (ranks [V, S], the L1
+        change of each vector per iteration [iters, S]).  Numpy, small graphs."""
+        V = g["num_vertices"]
+        outdeg = g["f_outdeg"].astype(np.float64)
+        idx, deg, nbr = g["i_idx"].astype(np.int64), g["i_outdeg"].astype(np.int64), g["i_dst"].astype(np.int64)
+        # destination of every inverse edge, in CSR order
+        dst = np.repeat(np.arange(V), deg)
+        src = np.concatenate([nbr[idx[v]: idx[v] + deg[v]] for v in range(V)]) if len(dst) else np.zeros(0, np.int64)
+        S = len(seeds)
+        r = np.zeros((V, S))
+        r[np.asarray(seeds), np.arange(S)] = 1.0
+        tele = np.zeros((V, S))
+        tele[np.asarray(seeds), np.arange(S)] = 1.0 - damp
+        inv = np.where(outdeg > 0, 1.0 / np.maximum(outdeg, 1), 0.0)
+        hist = np.zeros((iters, S))
+        for it in range(iters):
+            c = r * inv[:, None]
+            s = np.zeros((V, S))
+            np.add.at(s, dst, c[src])
+            nr = tele + damp * s
+            hist[it] = np.abs(nr - r).sum(axis=0)
+            r = nr
+        return r, hist
+
     def random_roots(self, V: int, avg_degree: int, out_degree, n: int, seed: int = 27491095):
         roots = np.empty(n, np.uint32)
         self.d.orc_random_roots(seed, V, avg_degree, _p(out_degree), n, _p(roots))

@@ -78,3 +78,58 @@ def test_msbfs_rejects_bad_roots(torch_cuda, lib, graphs):
     with pytest.raises(Exception):
         dg.msbfs([], depth_t)
     dg.close()
+
+
+PPR_CASES = [
+    ("rmat", dict(scale=12, ef=16, seed=1)),
+    ("uniform", dict(n=20_000, m=100_000, seed=3)),
+    ("grid", dict(side=60, p=0.01, seed=2)),
+    ("star", dict(n=5_000, seed=4)),
+]
+PPR_L1_TOL = 1e-5  # per seed vector (mass <= 1): fp32 sums vs the FP64 restatement
+
+
+@pytest.mark.parametrize("kind,kw", PPR_CASES, ids=[f"{k}-{i}" for i, (k, _) in enumerate(PPR_CASES)])
+def test_ppr_vs_fp64(torch_cuda, lib, oracle, graphs, kind, kw):
+    torch = torch_cuda
+    s, d, _, V = graphs(kind, **kw)
+    g = oracle.build(s, d, V, 0)
+    dg = lib.device_graph()
+    dg.build(dev(torch, s), dev(torch, d), V, 0)
+    ranks_t = torch.empty(V * 32, dtype=torch.float32, device="cuda")
+    rng = np.random.default_rng(7)
+    for n in (32, 5):
+        seeds = [int(x) for x in rng.choice(V, size=n, replace=False)]
+        if n == 32:
+            seeds[1] = seeds[0]                                  # duplicate seed: identical vectors
+            seeds[2] = int(np.argmax(g["i_outdeg"]))             # the in-hub
+        info = dg.ppr(seeds, ranks_t, max_iterations=20, epsilon=0.0)
+        got = host(ranks_t, np.float32).reshape(V, 32)[:, :n].astype(np.float64)
+        want, hist = oracle.ppr_f64(g, seeds, 20)
+        l1 = np.abs(got - want).sum(axis=0)
+        assert np.all(l1 <= PPR_L1_TOL), (n, l1.max())
+        assert np.allclose(info["err_last"], hist[-1], rtol=1e-4, atol=1e-7)
+        assert info["executed"] == 20 and not info["converged"]
+        if n == 32:
+            assert np.array_equal(got[:, 0], got[:, 1])
+    dg.close()
+
+
+def test_ppr_stops_on_epsilon(torch_cuda, lib, oracle, graphs):
+    torch = torch_cuda
+    s, d, _, V = graphs("rmat", scale=11, ef=8, seed=2)
+    g = oracle.build(s, d, V, 0)
+    dg = lib.device_graph()
+    dg.build(dev(torch, s), dev(torch, d), V, 0)
+    seeds = list(range(0, 64, 2))
+    info = dg.ppr(seeds, None, max_iterations=200, epsilon=1e-6)
+    assert info["converged"] and info["executed"] < 200
+    _, hist = oracle.ppr_f64(g, seeds, info["executed"])
+    # the run stopped at the first iteration whose every vector changed by < 1e-6
+    assert hist[-1].max() < 1.5e-6
+    assert hist[-2].max() >= 0.5e-6
+    with pytest.raises(Exception):
+        dg.ppr(list(range(33)), None)
+    with pytest.raises(Exception):
+        dg.ppr([V], None)
+    dg.close()
