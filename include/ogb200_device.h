@@ -150,6 +150,62 @@ typedef struct ogb_ppr_info
 int ogb_ppr(ogb_graph *g, const uint32_t *seeds, uint32_t nseeds, uint32_t max_iterations, double epsilon,
             float *d_ranks, ogb_ppr_info *info, void *stream);
 
+/* Many graphs in one (no reference counterpart: each graph's results equal
+ * the reference path run on that graph alone).  The graphs are packed into
+ * one disjoint union on the device; BFS of all of them is one launch and
+ * PageRank of all of them one CUDA graph, each graph with its own stop rule
+ * and normalization.  Edge lists use local ids, back to back: graph i's
+ * edges are src/dst[edge_offsets[i] .. edge_offsets[i+1]) (host arrays),
+ * ids < num_vertices[i].  Vertex arrays of the batch (parents, distances,
+ * ranks) hold the graphs' vertices back to back (ogb_batch_offsets). */
+typedef struct ogb_batch ogb_batch;
+ogb_batch *ogb_batch_create(uint32_t num_graphs, const uint32_t *num_vertices, const uint64_t *edge_offsets,
+                            const uint32_t *src, const uint32_t *dst, uint32_t sort_type);
+void ogb_batch_free(ogb_batch *b);
+/* vertex_offsets: num_graphs + 1 entries (host) */
+int ogb_batch_offsets(ogb_batch *b, uint32_t *vertex_offsets);
+typedef struct ogb_batch_bfs_info
+{
+    uint32_t levels;           /* steps of the joint search              */
+    uint32_t td_steps;
+    uint32_t bu_steps;
+    uint32_t reached;          /* vertices reached, all graphs           */
+    double ms;                 /* device time of the search              */
+} ogb_batch_bfs_info;
+/* DO-BFS of every graph from roots[i] (local id, host array); d_parents
+ * (local ids, sentinel -out_degree / -1 for unreached) and d_distances. */
+int ogb_batch_bfs(ogb_batch *b, const uint32_t *roots, int32_t *d_parents, uint32_t *d_distances,
+                  ogb_batch_bfs_info *info, void *stream);
+typedef struct ogb_batch_pr_graph
+{
+    uint32_t iterations;       /* PageRankStats.iterations of the graph   */
+    uint32_t executed;
+    uint32_t activeVertices;
+    uint32_t converged;
+    double error_total;
+} ogb_batch_pr_graph;
+typedef struct ogb_batch_pr_info
+{
+    double ms;                 /* device time of the graph launch         */
+    uint32_t captured;         /* 1 when this call (re)built the graph    */
+    uint32_t pad;
+} ogb_batch_pr_info;
+/* Pull PageRank of every graph; d_ranks receives the normalized ranks of all
+ * vertices; per_graph (host, num_graphs entries, may be NULL). */
+int ogb_batch_pagerank(ogb_batch *b, uint32_t max_iterations, double epsilon, float *d_ranks,
+                       ogb_batch_pr_graph *per_graph, ogb_batch_pr_info *info, void *stream);
+typedef struct ogb_tune_info
+{
+    uint32_t ncandidates;
+    uint32_t best;             /* index of the chosen candidate           */
+    uint32_t warp_thr[16];
+    uint32_t cta_thr[16];
+    double ms[16];             /* pull ms per iteration of each candidate */
+} ogb_tune_info;
+/* Times the pull PageRank bin thresholds on this batch and keeps the
+ * fastest (ogb_pagerank_set_bins). */
+int ogb_batch_autotune(ogb_batch *b, ogb_tune_info *info);
+
 /* PageRank; mode 0 pull, 1 push.  d_ranks receives V normalized ranks;
  * d_init (may be NULL) replaces the uniform unnormalized start 1-0.85. */
 int ogb_pagerank(ogb_graph *g, uint32_t mode, uint32_t max_iterations, double epsilon, float *d_ranks,

@@ -131,6 +131,24 @@ class PprBatchInfo(C.Structure):
                 ("err_last", C.c_double * 32)]
 
 
+class BatchBfsInfo(C.Structure):
+    _fields_ = [("levels", u32), ("td_steps", u32), ("bu_steps", u32), ("reached", u32), ("ms", C.c_double)]
+
+
+class BatchPrGraph(C.Structure):
+    _fields_ = [("iterations", u32), ("executed", u32), ("activeVertices", u32), ("converged", u32),
+                ("error_total", C.c_double)]
+
+
+class BatchPrInfo(C.Structure):
+    _fields_ = [("ms", C.c_double), ("captured", u32), ("pad", u32)]
+
+
+class TuneInfo(C.Structure):
+    _fields_ = [("ncandidates", u32), ("best", u32), ("warp_thr", u32 * 16), ("cta_thr", u32 * 16),
+                ("ms", C.c_double * 16)]
+
+
 class BfsLevel(C.Structure):
     _fields_ = [("direction", u32), ("discovered", u32), ("frontier", u32), ("mf", u32), ("mu", u32),
                 ("pad", u32), ("edges", C.c_uint64), ("ms", C.c_float), ("pad2", C.c_float)]
@@ -209,6 +227,12 @@ _DEVICE_API = [
     ("ogb_bfs_trace", C.c_int, [vp, C.POINTER(BfsLevel), u32, C.POINTER(u32)]),
     ("ogb_msbfs", C.c_int, [vp, u32p, u32, vp, C.POINTER(MsBfsInfo), vp]),
     ("ogb_ppr", C.c_int, [vp, u32p, u32, u32, C.c_double, vp, C.POINTER(PprBatchInfo), vp]),
+    ("ogb_batch_create", vp, [u32, u32p, C.POINTER(C.c_uint64), u32p, u32p, u32]),
+    ("ogb_batch_free", None, [vp]),
+    ("ogb_batch_offsets", C.c_int, [vp, u32p]),
+    ("ogb_batch_bfs", C.c_int, [vp, u32p, vp, vp, C.POINTER(BatchBfsInfo), vp]),
+    ("ogb_batch_pagerank", C.c_int, [vp, u32, C.c_double, vp, vp, C.POINTER(BatchPrInfo), vp]),
+    ("ogb_batch_autotune", C.c_int, [vp, C.POINTER(TuneInfo)]),
     ("ogb_pagerank", C.c_int, [vp, u32, u32, C.c_double, vp, vp, C.POINTER(PrInfo), vp]),
     ("ogb_pagerank_history", C.c_int, [vp, C.POINTER(C.c_double), u32p, u32, C.POINTER(u32)]),
     ("ogb_pagerank_set_bins", None, [u32, u32]),
@@ -352,6 +376,54 @@ class CsrArrays:
     out_degree: object
     in_degree: object
     edges_idx: object
+
+
+class GraphBatch:
+    """Many graphs packed into one device union (ogb_batch_*): edge lists in
+    local ids, back to back; every vertex array of the batch holds the
+    graphs' vertices back to back (offsets)."""
+
+    def __init__(self, lib, num_vertices, edge_offsets, src, dst, sort_type: int = 0):
+        self.lib = lib
+        nv = np.ascontiguousarray(np.asarray(num_vertices, dtype=np.uint32))
+        eo = np.ascontiguousarray(np.asarray(edge_offsets, dtype=np.uint64))
+        s = np.ascontiguousarray(np.asarray(src, dtype=np.uint32))
+        d = np.ascontiguousarray(np.asarray(dst, dtype=np.uint32))
+        self.n = len(nv)
+        h = lib.ogb_batch_create(self.n, nv.ctypes.data_as(u32p), eo.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                 s.ctypes.data_as(u32p), d.ctypes.data_as(u32p), int(sort_type))
+        if not h:
+            msg = lib.ogb_last_error()
+            raise OgbError("ogb_batch_create: " + (msg.decode() if msg else ""))
+        self.handle = h
+        off = np.zeros(self.n + 1, np.uint32)
+        lib.check(lib.ogb_batch_offsets(h, off.ctypes.data_as(u32p)), "ogb_batch_offsets")
+        self.offsets = off
+
+    def bfs(self, roots, parents, distances, stream=None) -> dict:
+        r = np.ascontiguousarray(np.asarray(roots, dtype=np.uint32))
+        info = BatchBfsInfo()
+        self.lib.check(self.lib.ogb_batch_bfs(self.handle, r.ctypes.data_as(u32p), _ptr(parents), _ptr(distances),
+                                              C.byref(info), stream), "ogb_batch_bfs")
+        return info_dict(info)
+
+    def pagerank(self, ranks, max_iterations: int = 100, epsilon: float = 1e-4, stream=None):
+        per = (BatchPrGraph * self.n)()
+        info = BatchPrInfo()
+        self.lib.check(self.lib.ogb_batch_pagerank(self.handle, int(max_iterations), float(epsilon), _ptr(ranks),
+                                                   per, C.byref(info), stream), "ogb_batch_pagerank")
+        return info_dict(info), [info_dict(per[i]) for i in range(self.n)]
+
+    def autotune(self) -> dict:
+        t = TuneInfo()
+        self.lib.check(self.lib.ogb_batch_autotune(self.handle, C.byref(t)), "ogb_batch_autotune")
+        n = t.ncandidates
+        return {"best": t.best, "candidates": [(t.warp_thr[i], t.cta_thr[i], t.ms[i]) for i in range(n)]}
+
+    def close(self):
+        if self.handle:
+            self.lib.ogb_batch_free(self.handle)
+            self.handle = None
 
 
 class DeviceGraph:

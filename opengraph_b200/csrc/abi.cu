@@ -1465,6 +1465,94 @@ extern "C" int ogb_ppr(ogb_graph* g, const uint32_t* seeds, uint32_t nseeds, uin
   return OK;
 }
 
+struct ogb_batch {
+  GraphBatch* b = nullptr;
+};
+
+extern "C" ogb_batch* ogb_batch_create(uint32_t num_graphs, const uint32_t* num_vertices,
+                                       const uint64_t* edge_offsets, const uint32_t* src, const uint32_t* dst,
+                                       uint32_t sort_type) {
+  if (!num_vertices || !edge_offsets || (!src && edge_offsets[num_graphs]) || (!dst && edge_offsets[num_graphs])) {
+    fail(ERR_ARG, "ogb_batch_create: null argument");
+    return nullptr;
+  }
+  GraphBatch* b = batch_new();
+  if (batch_create(*b, num_graphs, num_vertices, edge_offsets, src, dst, sort_type, lib_stream()) != OK) {
+    batch_free(b);
+    return nullptr;
+  }
+  ogb_batch* h = new ogb_batch();
+  h->b = b;
+  return h;
+}
+
+extern "C" void ogb_batch_free(ogb_batch* b) {
+  if (!b) return;
+  batch_free(b->b);
+  delete b;
+}
+
+extern "C" int ogb_batch_offsets(ogb_batch* b, uint32_t* vertex_offsets) {
+  if (!b || !vertex_offsets) return fail(ERR_ARG, "ogb_batch_offsets: null argument");
+  memcpy(vertex_offsets, batch_voff(b->b), (size_t)(batch_ngraphs(b->b) + 1) * 4);
+  return OK;
+}
+
+extern "C" int ogb_batch_bfs(ogb_batch* b, const uint32_t* roots, int32_t* d_parents, uint32_t* d_distances,
+                             ogb_batch_bfs_info* info, void* stream) {
+  if (!b || !roots || !d_parents || !d_distances) return fail(ERR_ARG, "ogb_batch_bfs: null argument");
+  BfsResult r;
+  OGB_TRY(batch_bfs(*b->b, roots, d_parents, d_distances, &r, as_stream(stream)));
+  if (info) {
+    info->levels = (uint32_t)r.nlevels;
+    info->td_steps = r.td_steps;
+    info->bu_steps = r.bu_steps;
+    info->reached = r.reached;
+    info->ms = r.ms;
+  }
+  return OK;
+}
+
+extern "C" int ogb_batch_pagerank(ogb_batch* b, uint32_t max_iterations, double epsilon, float* d_ranks,
+                                  ogb_batch_pr_graph* per_graph, ogb_batch_pr_info* info, void* stream) {
+  if (!b || !d_ranks) return fail(ERR_ARG, "ogb_batch_pagerank: null argument");
+  const uint32_t n = batch_ngraphs(b->b);
+  std::vector<BatchPrGraph> pg(n);
+  double ms = 0.0;
+  uint32_t cap = 0;
+  OGB_TRY(batch_pagerank(*b->b, max_iterations, epsilon, d_ranks, pg.data(), &ms, &cap, as_stream(stream)));
+  if (per_graph)
+    for (uint32_t i = 0; i < n; i++) {
+      per_graph[i].iterations = pg[i].iterations;
+      per_graph[i].executed = pg[i].executed;
+      per_graph[i].activeVertices = pg[i].activeVertices;
+      per_graph[i].converged = pg[i].converged;
+      per_graph[i].error_total = pg[i].error_total;
+    }
+  if (info) {
+    info->ms = ms;
+    info->captured = cap;
+    info->pad = 0;
+  }
+  return OK;
+}
+
+extern "C" int ogb_batch_autotune(ogb_batch* b, ogb_tune_info* info) {
+  if (!b) return fail(ERR_ARG, "ogb_batch_autotune: null argument");
+  TuneResult t;
+  OGB_TRY(batch_autotune(*b->b, 5, &t, lib_stream()));
+  if (info) {
+    info->ncandidates = t.n;
+    info->best = t.best;
+    for (int i = 0; i < 16; i++) {
+      info->warp_thr[i] = t.warp_thr[i];
+      info->cta_thr[i] = t.cta_thr[i];
+      info->ms[i] = t.ms[i];
+    }
+  }
+  return OK;
+}
+
 extern "C" int ogb_bfs_trace(ogb_graph* g, ogb_bfs_level* levels, uint32_t max_levels, uint32_t* count) {
   if (!g) return fail(ERR_ARG, "null");
   const uint32_t n = std::min<uint32_t>(max_levels, (uint32_t)g->g.bfs_last_levels);

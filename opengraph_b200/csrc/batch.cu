@@ -727,4 +727,245 @@ int ppr_run(DevGraph& g, const uint32_t* seeds, uint32_t nseeds, uint32_t max_it
   return OK;
 }
 
+
+// ===========================================================================
+// Many graphs in one launch (no reference counterpart: each graph's results
+// equal the reference path run on that graph alone).  The graphs are packed
+// into one disjoint union (vertex ids shifted by each graph's offset, one
+// sort builds every graph's CSR side by side), so the single-graph kernels
+// and their load balancing serve the whole batch:
+//  * BFS: one search from every graph's root at once -- one cooperative
+//    launch for the whole batch; each vertex gets its depth from its own
+//    graph's root (no edges cross graphs); parents are returned in local ids;
+//  * PageRank pull: every graph keeps its own stop rule and normalization
+//    (a per-graph reduction after each iteration freezes a graph whose
+//    vertices all changed by < epsilon); the whole run is one CUDA graph.
+// ===========================================================================
+
+struct GraphBatch {
+  DevGraph g;
+  uint32_t ngraphs = 0;
+  std::vector<uint32_t> voff;  // host copy of the vertex offsets
+  DevBuf d_voff, d_eoff, gid, frozen, stop_iter, executed, active_last, err_last, delta;
+  cudaGraphExec_t pr_exec = nullptr;
+  uint32_t pr_iters = 0, pr_warp = 0, pr_cta = 0, pr_build = 0;
+  double pr_eps = -1.0;
+  float* pr_ranks = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  ~GraphBatch() {
+    if (pr_exec) cudaGraphExecDestroy(pr_exec);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+  }
+};
+
+GraphBatch* batch_new() { return new GraphBatch(); }
+void batch_free(GraphBatch* b) { delete b; }
+uint32_t batch_ngraphs(const GraphBatch* b) { return b->ngraphs; }
+const uint32_t* batch_voff(const GraphBatch* b) { return b->voff.data(); }
+DevGraph& batch_graph(GraphBatch* b) { return b->g; }
+
+// local ids -> union ids (edge e of graph g: + voff[g]); an id outside its
+// graph sets *err
+__global__ void bk_shift(uint64_t E, const uint64_t* __restrict__ eoff, const uint32_t* __restrict__ voff,
+                         uint32_t ng, uint32_t* __restrict__ src, uint32_t* __restrict__ dst, uint32_t* err) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = ng - 1;  // last g with eoff[g] <= e
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (eoff[mid] <= e)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const uint32_t n = voff[lo + 1] - voff[lo];
+    if (src[e] >= n || dst[e] >= n) *err = 1;
+    src[e] += voff[lo];
+    dst[e] += voff[lo];
+  }
+}
+
+__global__ void bk_gid(uint32_t V, const uint32_t* __restrict__ voff, uint32_t ng, uint32_t* __restrict__ gid) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = ng - 1;  // last g with voff[g] <= v
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (voff[mid] <= v)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    gid[v] = lo;
+  }
+}
+
+__global__ void bk_localize(uint32_t V, const uint32_t* __restrict__ gid, const uint32_t* __restrict__ voff,
+                            int32_t* __restrict__ parents) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const int32_t p = parents[v];
+    if (p >= 0) parents[v] = p - (int32_t)voff[gid[v]];
+  }
+}
+
+int batch_create(GraphBatch& b, uint32_t ngraphs, const uint32_t* nv, const uint64_t* eoff, const uint32_t* src,
+                 const uint32_t* dst, uint32_t sort_type, cudaStream_t s) {
+  if (ngraphs == 0) return fail(ERR_ARG, "batch: no graphs");
+  if (sort_type > 3) return fail(ERR_ARG, "batch: sort type %u", sort_type);
+  b.voff.assign(ngraphs + 1, 0);
+  uint64_t V = 0;
+  for (uint32_t i = 0; i < ngraphs; i++) {
+    if (eoff[i + 1] < eoff[i]) return fail(ERR_ARG, "batch: edge offsets decrease at graph %u", i);
+    V += nv[i];
+    if (V > (1u << 30)) return fail(ERR_RANGE, "batch: more than 2^30 vertices in all");
+    b.voff[i + 1] = (uint32_t)V;
+  }
+  const uint64_t E = eoff[ngraphs] - eoff[0];
+  if (eoff[0] != 0) return fail(ERR_ARG, "batch: edge offsets must start at 0");
+  if (E > 0xFFFFFFFFull) return fail(ERR_RANGE, "batch: more than 2^32 - 1 edges in all");
+  b.ngraphs = ngraphs;
+  OGB_TRY(b.d_voff.alloc((size_t)(ngraphs + 1) * 4));
+  OGB_TRY(b.d_eoff.alloc((size_t)(ngraphs + 1) * 8));
+  OGB_CUDA(cudaMemcpyAsync(b.d_voff.p, b.voff.data(), (size_t)(ngraphs + 1) * 4, cudaMemcpyHostToDevice, s));
+  OGB_CUDA(cudaMemcpyAsync(b.d_eoff.p, eoff, (size_t)(ngraphs + 1) * 8, cudaMemcpyHostToDevice, s));
+  DevBuf us, ud, derr;
+  OGB_TRY(us.alloc(E * 4 + 16));
+  OGB_TRY(ud.alloc(E * 4 + 16));
+  OGB_TRY(derr.alloc(16));
+  OGB_CUDA(cudaMemsetAsync(derr.p, 0, 4, s));
+  if (E) {
+    OGB_CUDA(cudaMemcpyAsync(us.p, src, E * 4, cudaMemcpyHostToDevice, s));
+    OGB_CUDA(cudaMemcpyAsync(ud.p, dst, E * 4, cudaMemcpyHostToDevice, s));
+    bk_shift<<<sm_count() * 8, 256, 0, s>>>(E, b.d_eoff.as<uint64_t>(), b.d_voff.as<uint32_t>(), ngraphs,
+                                           us.as<uint32_t>(), ud.as<uint32_t>(), derr.as<uint32_t>());
+    OGB_CUDA(cudaGetLastError());
+  }
+  uint32_t herr = 0;
+  OGB_CUDA(cudaMemcpyAsync(&herr, derr.p, 4, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  if (herr) return fail(ERR_RANGE, "batch: an edge id is not below its graph's vertex count");
+  OGB_TRY(graph_build(b.g, us.as<uint32_t>(), ud.as<uint32_t>(), nullptr, (uint32_t)E, (uint32_t)V, sort_type, s));
+  OGB_TRY(graph_check(b.g, s));
+  OGB_TRY(b.gid.alloc(V * 4 + 16));
+  bk_gid<<<sm_count() * 8, 256, 0, s>>>((uint32_t)V, b.d_voff.as<uint32_t>(), ngraphs, b.gid.as<uint32_t>());
+  OGB_CUDA(cudaGetLastError());
+  OGB_TRY(b.frozen.alloc((size_t)ngraphs * 4 + 16));
+  OGB_TRY(b.stop_iter.alloc((size_t)ngraphs * 4 + 16));
+  OGB_TRY(b.executed.alloc((size_t)ngraphs * 4 + 16));
+  OGB_TRY(b.active_last.alloc((size_t)ngraphs * 4 + 16));
+  OGB_TRY(b.err_last.alloc((size_t)ngraphs * 8 + 16));
+  OGB_TRY(b.delta.alloc(V * 4 + 16));
+  if (!b.ev0) {
+    OGB_CUDA(cudaEventCreate(&b.ev0));
+    OGB_CUDA(cudaEventCreate(&b.ev1));
+  }
+  OGB_CUDA(cudaStreamSynchronize(s));
+  return OK;
+}
+
+int batch_bfs(GraphBatch& b, const uint32_t* roots, int32_t* parents, uint32_t* distances, BfsResult* res,
+              cudaStream_t s) {
+  std::vector<uint32_t> r(b.ngraphs);
+  for (uint32_t i = 0; i < b.ngraphs; i++) {
+    if (roots[i] >= b.voff[i + 1] - b.voff[i]) return fail(ERR_ARG, "batch bfs: root %u of graph %u out of range", roots[i], i);
+    r[i] = roots[i] + b.voff[i];
+  }
+  OGB_TRY(bfs_run_roots(b.g, r.data(), b.ngraphs, BFS_DO, parents, distances, res, false, false, s));
+  bk_localize<<<sm_count() * 8, 256, 0, s>>>(b.g.V, b.gid.as<uint32_t>(), b.d_voff.as<uint32_t>(), parents);
+  OGB_CUDA(cudaGetLastError());
+  OGB_CUDA(cudaStreamSynchronize(s));
+  return OK;
+}
+
+int batch_pagerank(GraphBatch& b, uint32_t max_iters, double epsilon, float* ranks, BatchPrGraph* per_graph,
+                   double* ms_out, uint32_t* captured, cudaStream_t s) {
+  uint32_t wt = 0, ct = 0, cth = 0, ch = 0;
+  pagerank_get_bins(&wt, &ct, &cth, &ch);
+  if (b.pr_exec && (b.pr_iters != max_iters || b.pr_eps != epsilon || b.pr_ranks != ranks || b.pr_warp != wt ||
+                    b.pr_cta != ct || b.pr_build != b.g.build_id)) {
+    cudaGraphExecDestroy(b.pr_exec);
+    b.pr_exec = nullptr;
+  }
+  PrBatchDev d;
+  d.voff = b.d_voff.as<uint32_t>();
+  d.gid = b.gid.as<uint32_t>();
+  d.frozen = b.frozen.as<uint32_t>();
+  d.stop_iter = b.stop_iter.as<uint32_t>();
+  d.executed = b.executed.as<uint32_t>();
+  d.active_last = b.active_last.as<uint32_t>();
+  d.err_last = b.err_last.as<double>();
+  d.delta = b.delta.as<float>();
+  bool rebuilt = false;
+  // capture happens outside the timed region
+  if (!b.pr_exec) {
+    OGB_TRY(pagerank_batch_run(b.g, d, b.ngraphs, max_iters, epsilon, ranks, &b.pr_exec, &rebuilt, s));
+    OGB_CUDA(cudaStreamSynchronize(s));
+    b.pr_iters = max_iters;
+    b.pr_eps = epsilon;
+    b.pr_ranks = ranks;
+    b.pr_warp = wt;
+    b.pr_cta = ct;
+    b.pr_build = b.g.build_id;
+  }
+  OGB_CUDA(cudaEventRecord(b.ev0, s));
+  OGB_TRY(pagerank_batch_run(b.g, d, b.ngraphs, max_iters, epsilon, ranks, &b.pr_exec, nullptr, s));
+  OGB_CUDA(cudaEventRecord(b.ev1, s));
+  std::vector<uint32_t> stop(b.ngraphs), exe(b.ngraphs), act(b.ngraphs);
+  std::vector<double> err(b.ngraphs);
+  OGB_CUDA(cudaMemcpyAsync(stop.data(), d.stop_iter, (size_t)b.ngraphs * 4, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaMemcpyAsync(exe.data(), d.executed, (size_t)b.ngraphs * 4, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaMemcpyAsync(act.data(), d.active_last, (size_t)b.ngraphs * 4, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaMemcpyAsync(err.data(), d.err_last, (size_t)b.ngraphs * 8, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  OGB_CUDA(cudaEventElapsedTime(&ms, b.ev0, b.ev1));
+  if (ms_out) *ms_out = ms;
+  if (captured) *captured = rebuilt ? 1u : 0u;
+  if (per_graph)
+    for (uint32_t i = 0; i < b.ngraphs; i++) {
+      const bool conv = stop[i] != 0xFFFFFFFFu;
+      per_graph[i].converged = conv ? 1u : 0u;
+      per_graph[i].iterations = conv ? stop[i] : max_iters;
+      per_graph[i].executed = exe[i];
+      per_graph[i].activeVertices = act[i];
+      per_graph[i].error_total = err[i];
+    }
+  return OK;
+}
+
+// Bin thresholds for this batch: each candidate (warp_thr, cta_thr) runs a
+// few pull iterations over the union (its per-graph layout is rebuilt for
+// it, outside the timing); the fastest is kept as the library's setting.
+int batch_autotune(GraphBatch& b, uint32_t iters, TuneResult* out, cudaStream_t s) {
+  static const uint32_t cand[][2] = {{16, 1024}, {32, 2048}, {64, 2048}, {64, 4096}, {128, 4096}, {32, 8192}};
+  const uint32_t n = sizeof(cand) / sizeof(cand[0]);
+  float* ranks = nullptr;
+  DevBuf rb;
+  OGB_TRY(rb.alloc((size_t)b.g.V * 4 + 16));
+  ranks = rb.as<float>();
+  double best = 1e30;
+  uint32_t bi = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    pagerank_set_bins(cand[i][0], cand[i][1]);
+    PrResult r;
+    OGB_TRY(pagerank_run(b.g, PR_PULL, 1, 0.0, ranks, nullptr, &r, s));  // builds the layout
+    OGB_TRY(pagerank_run(b.g, PR_PULL, iters, 0.0, ranks, nullptr, &r, s));
+    const double ms = r.ms / iters;
+    if (out) {
+      out->warp_thr[i] = cand[i][0];
+      out->cta_thr[i] = cand[i][1];
+      out->ms[i] = ms;
+    }
+    if (ms < best) {
+      best = ms;
+      bi = i;
+    }
+  }
+  pagerank_set_bins(cand[bi][0], cand[bi][1]);
+  if (out) {
+    out->n = n;
+    out->best = bi;
+  }
+  return OK;
+}
+
 }  // namespace ogb

@@ -884,6 +884,28 @@ __global__ void __launch_bounds__(256) bfsk_init(BfsBufs b, BfsDevState* st, uin
   }
 }
 
+// More roots after bfsk_init's first one (a search over a disjoint union of
+// graphs, one root each): each gets itself as parent and its frontier bit,
+// joins the queue (and the expansion list when it has out-edges); mf sums
+// their out-degrees.  Duplicates are skipped.  One thread, after bfsk_init.
+__global__ void bfsk_set_roots(BfsBufs b, BfsDevState* st, const uint32_t* __restrict__ roots, uint32_t n) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int32_t* parents = st->parents;
+  BfsCtrl c = st->c;
+  for (uint32_t i = 1; i < n; i++) {
+    const uint32_t r = roots[i];
+    if (parents[r] == (int32_t)r) continue;
+    parents[r] = (int32_t)r;
+    b.bm[0][r >> 5] |= 1u << (r & 31);
+    const uint32_t d = b.out_degree[r];
+    c.qcount++;
+    c.processed++;
+    c.mf += d;
+    if (d) b.list[0][c.lsize++] = r;
+  }
+  st->c = c;
+}
+
 // The whole search: all CTAs co-resident (cooperative launch), one grid
 // barrier after every phase.  Phase p counts into ctl[p % 3]; CTA 0 clears
 // ctl[(p + 1) % 3] when phase p starts (its last reader finished two
@@ -1113,9 +1135,17 @@ size_t bfs_pack_tmp_words(uint32_t V) { return bfs_pack_layout(V).tiles + 8 + sc
 
 int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_t* distances, BfsResult* res,
             bool time_levels, bool bu_entry_nf_frontier, cudaStream_t s) {
+  return bfs_run_roots(g, &root, 1, mode, parents, distances, res, time_levels, bu_entry_nf_frontier, s);
+}
+
+int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t mode, int32_t* parents,
+                  uint32_t* distances, BfsResult* res, bool time_levels, bool bu_entry_nf_frontier, cudaStream_t s) {
   (void)time_levels;  // the search always records per-level device times
   const uint32_t V = g.V;
-  if (root >= V) return fail(ERR_ARG, "bfs: root %u out of range (V=%u)", root, V);
+  if (nroots == 0) return fail(ERR_ARG, "bfs: no root");
+  for (uint32_t i = 0; i < nroots; i++)
+    if (roots[i] >= V) return fail(ERR_ARG, "bfs: root %u out of range (V=%u)", roots[i], V);
+  const uint32_t root = roots[0];
   if (mode > BFS_DO) return fail(ERR_ARG, "bfs: mode %u", mode);
   BfsWork* w = nullptr;
   OGB_TRY(bfs_work_get(g, &w));
@@ -1129,6 +1159,12 @@ int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_
   }
   bfsk_init<<<sm_count() * 8, 256, 0, s>>>(b, st, root, parents, distances, mode, bu_entry_nf_frontier ? 1u : 0u,
                                             g.E, w->epoch);
+  DevBuf d_roots;
+  if (nroots > 1) {
+    OGB_TRY(d_roots.alloc((size_t)nroots * 4));
+    OGB_CUDA(cudaMemcpyAsync(d_roots.p, roots, (size_t)nroots * 4, cudaMemcpyHostToDevice, s));
+    bfsk_set_roots<<<1, 32, 0, s>>>(b, st, d_roots.as<uint32_t>(), nroots);
+  }
   OGB_CUDA(cudaGetLastError());
   OGB_CUDA(cudaEventRecord(w->ev_start, s));
   void* args[] = {(void*)&b, (void*)&st};

@@ -118,6 +118,11 @@ struct BfsSwitchState {
 // frontier size as the bitmap DO-BFS.
 int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_t* distances,
             BfsResult* res, bool time_levels, bool bu_entry_nf_frontier, cudaStream_t s);
+// The same from several roots at once (host array): on a disjoint union of
+// graphs with one root each, every vertex gets its depth from its own
+// graph's root.  The switch state covers the whole union.
+int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t mode, int32_t* parents,
+                  uint32_t* distances, BfsResult* res, bool time_levels, bool bu_entry_nf_frontier, cudaStream_t s);
 
 // ---- multi-source BFS (batch.cu) -------------------------------------------
 struct MsResult {
@@ -129,6 +134,48 @@ struct MsResult {
 // Up to 64 BFS searches at once, one lane per root; depth[v * 64 + lane] =
 // depth of v in that lane's search, 0xFFFF when unreached (V * 64 u16).
 int msbfs_run(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint16_t* depth, MsResult* res, cudaStream_t s);
+
+// ---- PageRank over many graphs at once (a disjoint union) -------------------
+struct PrBatchDev {
+  const uint32_t* voff;   // ngraphs + 1 vertex offsets
+  const uint32_t* gid;    // graph of every vertex
+  uint32_t* frozen;       // per graph: stopped
+  uint32_t* stop_iter;    // per graph: iteration at which it stopped (~0u: did not)
+  uint32_t* executed;     // per graph: iterations run
+  uint32_t* active_last;  // per graph: active vertices of its last iteration
+  double* err_last;       // per graph: error_total of its last iteration
+  float* delta;           // per vertex: change in the last iteration
+};
+int pagerank_batch_run(DevGraph& g, const PrBatchDev& b, uint32_t ngraphs, uint32_t max_iters, double epsilon,
+                       float* ranks, cudaGraphExec_t* exec, bool* rebuilt, cudaStream_t s);
+
+// ---- many graphs in one disjoint union (batch.cu) ---------------------------
+struct GraphBatch;
+struct BatchPrGraph {
+  uint32_t iterations, executed, activeVertices, converged;
+  double error_total;
+};
+struct TuneResult {
+  uint32_t n = 0, best = 0;
+  uint32_t warp_thr[16] = {}, cta_thr[16] = {};
+  double ms[16] = {};
+};
+GraphBatch* batch_new();
+void batch_free(GraphBatch* b);
+uint32_t batch_ngraphs(const GraphBatch* b);
+const uint32_t* batch_voff(const GraphBatch* b);
+DevGraph& batch_graph(GraphBatch* b);
+// Graphs given by local-id edge lists back to back (edges of graph i at
+// [eoff[i], eoff[i+1]) of src/dst, host arrays); nv[i] vertices each.
+int batch_create(GraphBatch& b, uint32_t ngraphs, const uint32_t* nv, const uint64_t* eoff, const uint32_t* src,
+                 const uint32_t* dst, uint32_t sort_type, cudaStream_t s);
+// DO-BFS of every graph from its root (local ids, host array): parents
+// (local ids) and distances of all vertices, graph after graph.
+int batch_bfs(GraphBatch& b, const uint32_t* roots, int32_t* parents, uint32_t* distances, BfsResult* res,
+              cudaStream_t s);
+int batch_pagerank(GraphBatch& b, uint32_t max_iters, double epsilon, float* ranks, BatchPrGraph* per_graph,
+                   double* ms, uint32_t* captured, cudaStream_t s);
+int batch_autotune(GraphBatch& b, uint32_t iters, TuneResult* out, cudaStream_t s);
 
 // ---- batched personalized PageRank (batch.cu) -------------------------------
 struct PprResult {

@@ -160,6 +160,12 @@ struct PrParams {
   double epsilon;
   uint32_t V;
   uint32_t warp_thr;
+  // many graphs in one (a disjoint union): graph of each vertex, graphs that
+  // stopped (their vertices keep their rank), and each vertex's change for
+  // the per-graph error / stop rule; null for a single graph
+  const uint32_t* gid;
+  const uint32_t* frozen;
+  float* delta;
 };
 
 // contrib_next is indexed by renumbered id when perm is given.
@@ -167,11 +173,13 @@ __device__ __forceinline__ void pr_update(uint32_t v, float s, float* __restrict
                                           const uint32_t* __restrict__ out_degree,
                                           float* __restrict__ contrib_next, const PrParams& p, double& err,
                                           uint32_t& active, const uint32_t* __restrict__ perm = nullptr) {
-  const float nv = __fadd_rn(p.base_pr, __fmul_rn(p.damp, s));
   const float prev = pr[v];
+  float nv = __fadd_rn(p.base_pr, __fmul_rn(p.damp, s));
+  if (p.frozen && p.frozen[p.gid[v]]) nv = prev;
   pr[v] = nv;
   const uint32_t d = out_degree[v];
   contrib_next[perm ? perm[v] : v] = d ? __fdiv_rn(nv, (float)d) : 0.0f;
+  if (p.delta) p.delta[v] = __fsub_rn(nv, prev);
   const double e = fabs((double)__fsub_rn(nv, prev));
   err += e / (double)p.V;
   active += (e >= p.epsilon) ? 1u : 0u;
@@ -257,9 +265,11 @@ __device__ __forceinline__ PrVtx pr_vtx(uint32_t v, const float* __restrict__ pr
 __device__ __forceinline__ void pr_update_pre(uint32_t v, float s, const PrVtx& x, float* __restrict__ pr,
                                               float* __restrict__ contrib_next, const PrParams& p, double& err,
                                               uint32_t& active) {
-  const float nv = __fadd_rn(p.base_pr, __fmul_rn(p.damp, s));
+  float nv = __fadd_rn(p.base_pr, __fmul_rn(p.damp, s));
+  if (p.frozen && p.frozen[p.gid[v]]) nv = x.prev;
   pr[v] = nv;
   contrib_next[x.pm] = x.deg ? __fdiv_rn(nv, (float)x.deg) : 0.0f;
+  if (p.delta) p.delta[v] = __fsub_rn(nv, x.prev);
   const double e = fabs((double)__fsub_rn(nv, x.prev));
   err += e / (double)p.V;
   active += (e >= p.epsilon) ? 1u : 0u;
@@ -812,6 +822,9 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
   p.epsilon = epsilon;
   p.V = V;
   p.warp_thr = g_warp_thr;
+  p.gid = nullptr;
+  p.frozen = nullptr;
+  p.delta = nullptr;
   PrCtl* d_ctl = w->ctl.as<PrCtl>();
   OGB_CUDA(cudaMemsetAsync(d_ctl, 0, sizeof(PrCtl), s));
   float* c_cur = w->contrib0.as<float>();
@@ -874,6 +887,121 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
     r.activeVertices = w->h_ctl->active[r.executed - 1];
   }
   if (res) *res = r;
+  return OK;
+}
+
+// ------------------------------------------------------------ many graphs ---
+
+// Per-graph error and stop rule of one iteration over a disjoint union: a
+// CTA per graph sums |change| / V_g (fp64) and counts the vertices that
+// changed by >= epsilon; a graph with none stops (its vertices keep their
+// rank from then on), as the reference's loop breaks (pageRank.c:1024-1033).
+__global__ void __launch_bounds__(256) prk_batch_reduce(PrBatchDev b, double eps, uint32_t it) {
+  __shared__ double s_e[8];
+  __shared__ uint32_t s_a[8];
+  const uint32_t gph = blockIdx.x;
+  if (b.frozen[gph]) return;
+  const uint32_t lo = b.voff[gph], hi = b.voff[gph + 1];
+  const double n = (double)(hi - lo);
+  double e = 0.0;
+  uint32_t a = 0;
+  for (uint32_t v = lo + threadIdx.x; v < hi; v += blockDim.x) {
+    const double d = fabs((double)b.delta[v]);
+    e += d / n;
+    a += (d >= eps) ? 1u : 0u;
+  }
+  for (int o = 16; o; o >>= 1) {
+    e += __shfl_down_sync(0xffffffffu, e, o);
+    a += __shfl_down_sync(0xffffffffu, a, o);
+  }
+  if (lane_id() == 0) {
+    s_e[threadIdx.x >> 5] = e;
+    s_a[threadIdx.x >> 5] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double te = 0.0;
+    uint32_t ta = 0;
+    for (int w = 0; w < 8; w++) {
+      te += s_e[w];
+      ta += s_a[w];
+    }
+    b.err_last[gph] = te;
+    b.active_last[gph] = ta;
+    b.executed[gph] = it + 1;
+    if (ta == 0) {
+      b.frozen[gph] = 1;
+      b.stop_iter[gph] = it;
+    }
+  }
+}
+
+// pr /= V of the vertex's own graph (pageRank.c:1049-1052)
+__global__ void prk_batch_normalize(uint32_t V, PrBatchDev b, float* __restrict__ pr) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const uint32_t gph = b.gid[v];
+    pr[v] = __fdiv_rn(pr[v], (float)(b.voff[gph + 1] - b.voff[gph]));
+  }
+}
+
+// PageRank pull over a disjoint union of graphs, every graph with its own
+// stop rule and normalization; the results equal single-graph runs (same
+// rows, same summation orders).  The whole run -- init, the iterations,
+// the per-graph reductions and the normalization -- is captured once into a
+// CUDA graph (cached in *exec for the same arguments) and launched as one.
+int pagerank_batch_run(DevGraph& g, const PrBatchDev& b, uint32_t ngraphs, uint32_t max_iters, double epsilon,
+                       float* ranks, cudaGraphExec_t* exec, bool* rebuilt, cudaStream_t s) {
+  if (max_iters > kPrMaxIters) return fail(ERR_ARG, "pagerank: at most %u iterations", kPrMaxIters);
+  const uint32_t V = g.V;
+  if (V == 0) return fail(ERR_ARG, "pagerank: empty graph");
+  PrWork* w = nullptr;
+  OGB_TRY(pr_work_get(g, true, &w, s));
+  if (rebuilt) *rebuilt = false;
+  if (!*exec) {
+    const int sms = sm_count();
+    PrParams p;
+    p.damp = 0.85f;
+    p.base_pr = 1.0f - p.damp;
+    p.epsilon = epsilon;
+    p.V = V;
+    p.warp_thr = g_warp_thr;
+    p.gid = b.gid;
+    p.frozen = b.frozen;
+    p.delta = b.delta;
+    PrCtl* d_ctl = w->ctl.as<PrCtl>();
+    float* c_cur = w->contrib0.as<float>();
+    float* c_nxt = w->contrib1.as<float>();
+    const uint32_t* perm = w->perm.as<uint32_t>();
+    cudaStream_t cs = nullptr;
+    OGB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      cudaMemsetAsync(d_ctl, 0, sizeof(PrCtl), cs);
+      cudaMemsetAsync(b.frozen, 0, (size_t)ngraphs * 4, cs);
+      cudaMemsetAsync(b.stop_iter, 0xFF, (size_t)ngraphs * 4, cs);
+      cudaMemsetAsync(b.executed, 0, (size_t)ngraphs * 4, cs);
+      pr_init_kernel<<<sms * 8, 256, 0, cs>>>(V, g.fwd.d_out_degree(), nullptr, p.base_pr, ranks, c_cur, nullptr, perm);
+      for (uint32_t it = 0; it < max_iters; it++) {
+        pr_pull_kernel<<<sms, kPullThreads, kPullDynSmem + (size_t)w->hot * 4, cs>>>(
+            w->hot, w->chunks.as<PrChunkItem>(), w->n_chunks, w->vfirst.as<uint32_t>(), w->vcount.as<uint32_t>(),
+            w->done.as<uint32_t>(), w->partials.as<float>(), w->rows_rl.as<uint2>(), w->off_light.as<uint32_t>(),
+            w->unit_first.as<uint32_t>(), w->n_units, w->med_off.as<uint32_t>(), w->med_v.as<uint32_t>(),
+            w->med_base, w->nbr_rl.as<uint32_t>(), g.fwd.d_out_degree(), perm, c_cur, c_nxt, ranks, p, d_ctl, it);
+        prk_batch_reduce<<<ngraphs, 256, 0, cs>>>(b, epsilon, it);
+        std::swap(c_cur, c_nxt);
+      }
+      prk_batch_normalize<<<sms * 8, 256, 0, cs>>>(V, b, ranks);
+      e = cudaStreamEndCapture(cs, &graph);
+    }
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) return fail(ERR_CUDA, "pagerank batch capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(ERR_CUDA, "pagerank batch instantiate: %s", cudaGetErrorString(e));
+    if (rebuilt) *rebuilt = true;
+  }
+  OGB_CUDA(cudaGraphLaunch(*exec, s));
   return OK;
 }
 

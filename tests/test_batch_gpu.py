@@ -133,3 +133,97 @@ def test_ppr_stops_on_epsilon(torch_cuda, lib, oracle, graphs):
     with pytest.raises(Exception):
         dg.ppr([V], None)
     dg.close()
+
+
+def small_batch(og, n, seed):
+    """n seeded RMAT graphs of uneven size (scales 6..11, edge factors 4..16)
+    plus a 3-vertex graph without edges; local ids, back to back."""
+    rng = np.random.default_rng(seed)
+    nv, srcs, dsts = [], [], []
+    for i in range(n):
+        sc, ef = int(rng.integers(6, 12)), int(rng.integers(4, 17))
+        s, d, _ = og.generate_rmat(sc, ef, 1000 + i)
+        nv.append(1 << sc)
+        srcs.append(s.astype(np.uint32))
+        dsts.append(d.astype(np.uint32))
+    nv.append(3)
+    srcs.append(np.zeros(0, np.uint32))
+    dsts.append(np.zeros(0, np.uint32))
+    eoff = np.zeros(len(nv) + 1, np.uint64)
+    eoff[1:] = np.cumsum([len(x) for x in srcs])
+    return nv, eoff, srcs, dsts
+
+
+def test_batch_equals_single_graphs(torch_cuda, lib):
+    import opengraph_b200 as og
+    torch = torch_cuda
+    nv, eoff, srcs, dsts = small_batch(og, 24, 0)
+    b = og.GraphBatch(lib, nv, eoff, np.concatenate(srcs), np.concatenate(dsts))
+    off = b.offsets
+    Vt = int(off[-1])
+    assert list(np.diff(off)) == nv
+    par_t = torch.empty(Vt, dtype=torch.int32, device="cuda")
+    dist_t = torch.empty(Vt, dtype=torch.int32, device="cuda")
+    rng = np.random.default_rng(3)
+    roots = [int(rng.integers(0, x)) for x in nv]
+    binfo = b.bfs(roots, par_t, dist_t)
+    bpar, bdist = host(par_t, np.int32), host(dist_t)
+    ranks_t = torch.empty(Vt, dtype=torch.float32, device="cuda")
+    pinfo, per = b.pagerank(ranks_t, max_iterations=100, epsilon=1e-4)
+    branks = host(ranks_t, np.float32)
+    reached = 0
+    for i, V in enumerate(nv):
+        lo, hi = int(off[i]), int(off[i + 1])
+        dg = lib.device_graph()
+        dg.build(dev(torch, srcs[i]), dev(torch, dsts[i]), V, 0)
+        p1 = torch.empty(V, dtype=torch.int32, device="cuda")
+        d1 = torch.empty(V, dtype=torch.int32, device="cuda")
+        dg.bfs(roots[i], p1, d1, mode=2)
+        sp, sd = host(p1, np.int32), host(d1)
+        assert np.array_equal(bdist[lo:hi], sd), i
+        assert np.array_equal(bpar[lo:hi] >= 0, sp >= 0), i
+        assert bpar[lo + roots[i]] == roots[i]
+        assert np.array_equal(bpar[lo:hi][sp < 0], sp[sp < 0])   # sentinels of unreached vertices
+        reached += int((sp >= 0).sum())
+        r1 = torch.empty(V, dtype=torch.float32, device="cuda")
+        info = dg.pagerank(r1, mode=0, max_iterations=100, epsilon=1e-4)
+        assert per[i]["iterations"] == info["iterations"], i
+        assert np.array_equal(branks[lo:hi].view(np.uint32), host(r1, np.float32).view(np.uint32)), i
+        assert abs(per[i]["error_total"] - info["error_total"]) <= 1e-12 + 1e-9 * abs(info["error_total"]), i
+        dg.close()
+    assert binfo["reached"] == reached
+    # the same call again replays the captured graph
+    pinfo2, per2 = b.pagerank(ranks_t, max_iterations=100, epsilon=1e-4)
+    assert not pinfo2["captured"] and per2 == per
+    assert np.array_equal(host(ranks_t, np.float32).view(np.uint32), branks.view(np.uint32))
+    b.close()
+
+
+def test_batch_autotune_and_bad_input(torch_cuda, lib):
+    import opengraph_b200 as og
+    torch = torch_cuda
+    nv, eoff, srcs, dsts = small_batch(og, 8, 1)
+    b = og.GraphBatch(lib, nv, eoff, np.concatenate(srcs), np.concatenate(dsts))
+    saved = lib_bins(lib)
+    try:
+        t = b.autotune()
+        assert 0 <= t["best"] < len(t["candidates"])
+        best = t["candidates"][t["best"]]
+        assert lib_bins(lib)[:2] == best[:2]
+        assert best[2] == min(c[2] for c in t["candidates"])
+    finally:
+        lib.ogb_pagerank_set_bins(saved[0], saved[1])
+    b.close()
+    with pytest.raises(Exception):   # an id outside its graph
+        og.GraphBatch(lib, [4, 4], [0, 1, 2], np.array([0, 5], np.uint32), np.array([1, 1], np.uint32))
+    with pytest.raises(Exception):   # a root outside its graph
+        b2 = og.GraphBatch(lib, [4], [0, 1], np.array([0], np.uint32), np.array([1], np.uint32))
+        p = torch.empty(4, dtype=torch.int32, device="cuda")
+        b2.bfs([4], p, p)
+
+
+def lib_bins(lib):
+    import ctypes as C
+    w, c, t, k = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+    lib.ogb_pagerank_get_bins(C.byref(w), C.byref(c), C.byref(t), C.byref(k))
+    return w.value, c.value
