@@ -238,6 +238,9 @@ def run_ours(args):
     if rank == 0 and not args.skip_stages:
         extra = stages(lib, og, g, ts, td, tw, V, E, dev, hbm_peak)
 
+    if rank == 0 and not args.skip_stages:
+        extra["batching"] = batching(lib, og, g, roots, V, E, dev, sum(step_ms) / len(step_ms), extra)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.skip_cpu:
         cpu = cpu_baseline(og, s, d, w, roots[:args.cpu_roots])
@@ -378,6 +381,82 @@ def stages(lib, og, g, ts, td, tw, V, E, dev, hbm_peak):
                      "reference_stop_rule_iterations": info["iterations"],
                      "device_ms_run": round(info["ms"], 3),
                      "prepare_ms_once_per_graph": round(prepare_ms, 3)}
+    return out
+
+
+def batching(lib, og, g, roots, V, E, dev, sweep_ms, extra):
+    """The batched paths on the same GPU: 64-root multi-source BFS against the
+    64 single searches of the step, 32-seed personalized PageRank against 32
+    single pull iterations, and 256 uneven small RMAT graphs (scales 10-17,
+    edge factors 8-32) in one batch against the same graphs one by one."""
+    import torch
+    out = {}
+    depth = torch.empty(V * 64, dtype=torch.int16, device=dev)
+    for _ in range(2):
+        g.msbfs(roots, depth)
+    ms = min(g.msbfs(roots, depth)["ms"] for _ in range(3))
+    out["msbfs_64_roots"] = {"ms": round(ms, 3), "sequential_64_searches_ms": round(sweep_ms, 3),
+                             "speedup": round(sweep_ms / ms, 2)}
+    del depth
+    rng = np.random.default_rng(5)
+    seeds = [int(x) for x in rng.choice(V, size=32, replace=False)]
+    ranks = torch.empty(V * 32, dtype=torch.float32, device=dev)
+    g.ppr(seeds, ranks, max_iterations=3)
+    info = g.ppr(seeds, ranks, max_iterations=20)
+    it_ms = info["ms"] / 20
+    single = extra.get("pr_pull", {}).get("ms_per_iteration")
+    out["ppr_32_seeds"] = {"ms_per_iteration": round(it_ms, 3),
+                           "seed_edge_updates_per_s": round(32 * E / it_ms / 1e6, 1),
+                           "vs_32_single_iterations": round(32 * single / it_ms, 2) if single else None}
+    del ranks
+    lib_b = og.load(False)
+    rng = np.random.default_rng(42)
+    nv, srcs, dsts = [], [], []
+    for i in range(256):
+        sc, ef = int(rng.integers(10, 18)), int(rng.integers(8, 33))
+        s_, d_, _ = og.generate_rmat(sc, ef, 5000 + i)
+        nv.append(1 << sc)
+        srcs.append(s_)
+        dsts.append(d_)
+    eoff = np.zeros(257, np.uint64)
+    eoff[1:] = np.cumsum([len(x) for x in srcs])
+    broots = [int(np.argmax(np.bincount(x, minlength=n))) for x, n in zip(srcs, nv)]
+    b = og.GraphBatch(lib_b, nv, eoff, np.concatenate(srcs), np.concatenate(dsts))
+    Vt = int(b.offsets[-1])
+    par = torch.empty(Vt, dtype=torch.int32, device=dev)
+    dis = torch.empty(Vt, dtype=torch.int32, device=dev)
+    rk = torch.empty(Vt, dtype=torch.float32, device=dev)
+    tune = b.autotune()
+    b.bfs(broots, par, dis)
+    bfs_ms = min(b.bfs(broots, par, dis)["ms"] for _ in range(3))
+    b.pagerank(rk, max_iterations=100, epsilon=1e-4)
+    pr_ms = min(b.pagerank(rk, max_iterations=100, epsilon=1e-4)[0]["ms"] for _ in range(2))
+    gs = []
+    for i in range(256):
+        gi = lib_b.device_graph()
+        gi.build(torch.from_numpy(srcs[i].view(np.int32)).to(dev), torch.from_numpy(dsts[i].view(np.int32)).to(dev),
+                 nv[i], 0)
+        gs.append(gi)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i, gi in enumerate(gs):
+        gi.bfs(broots[i], par[:nv[i]], dis[:nv[i]], mode=2)
+    torch.cuda.synchronize()
+    seq_bfs = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    for i, gi in enumerate(gs):
+        gi.pagerank(rk[:nv[i]], mode=0, max_iterations=100, epsilon=1e-4)
+    torch.cuda.synchronize()
+    seq_pr = (time.perf_counter() - t0) * 1e3
+    for gi in gs:
+        gi.close()
+    b.close()
+    best = tune["candidates"][tune["best"]]
+    out["graphs_256"] = {"vertices": Vt, "edges": int(eoff[-1]), "bfs_ms": round(bfs_ms, 3),
+                         "bfs_sequential_ms": round(seq_bfs, 2), "pagerank_ms": round(pr_ms, 2),
+                         "pagerank_sequential_ms": round(seq_pr, 2),
+                         "autotuned_bins": {"warp_thr": best[0], "cta_thr": best[1]},
+                         "note": "sequential = the same graphs one by one through the single-graph API, wall clock"}
     return out
 
 
