@@ -105,12 +105,49 @@ ogb_graph *ogb_graph_of(const void *graphCSR);
 int ogb_sort_edges(const uint32_t *d_src, const uint32_t *d_dst, const float *d_w, uint32_t num_edges,
                    uint32_t sort_type, uint32_t *d_out_src, uint32_t *d_out_dst, float *d_out_w, void *stream);
 
-/* BFS from root; mode 0 pull, 1 push, 2 direction-optimized.  d_parents
- * (int32) and d_distances (u32) hold V entries each. */
+/* BFS from root; mode 0 pull, 1 push, 2 direction-optimized, 3
+ * direction-optimized with the learned switch (ogb_bfs_set_policy; depths
+ * are the same, the step directions and counts are the policy's), 4 pull
+ * with every bottom-up step over all vertices (a cost probe: the learned
+ * switch's training data).  d_parents (int32) and d_distances (u32) hold V
+ * entries each. */
 int ogb_bfs(ogb_graph *g, uint32_t root, uint32_t mode, int32_t *d_parents, uint32_t *d_distances,
             ogb_bfs_info *info, void *stream);
 /* Level trace of the last ogb_bfs on g (up to max_levels entries). */
 int ogb_bfs_trace(ogb_graph *g, ogb_bfs_level *levels, uint32_t max_levels, uint32_t *count);
+
+/* Learned parts (no reference counterpart).  Networks have one shape: in
+ * (<= 8) -> hidden (<= 64, ReLU) -> hidden (ReLU) -> 1; fp32 parameters
+ * (host arrays of ogb_mlp_nparams floats) packed as W1[h][in], b1[h],
+ * W2[h][h], b2[h], w3[h], b3; inference rounds them to bf16 and accumulates
+ * in fp32.  loss 0 = squared error, 1 = binary cross-entropy on the logit.
+ * ogb_mlp_grad: the batch-mean loss and its gradient (host) for d_X (batch
+ * x in) and d_T (batch).  ogb_mlp_train: Adam on shuffled mini-batches,
+ * params in/out; loss_hist (may be NULL) gets the mean loss per epoch. */
+uint32_t ogb_mlp_nparams(uint32_t in, uint32_t hidden);
+int ogb_mlp_grad(uint32_t in, uint32_t hidden, uint32_t loss, const float *d_X, const float *d_T, uint32_t batch,
+                 const float *params, float *grad, float *loss_out, void *stream);
+int ogb_mlp_train(uint32_t in, uint32_t hidden, uint32_t loss, const float *d_X, const float *d_T, uint32_t n,
+                  uint32_t epochs, uint32_t batch, float lr, uint32_t seed, float *params, float *loss_hist,
+                  void *stream);
+int ogb_mlp_infer(uint32_t in, uint32_t hidden, const float *params, const float *d_X, uint32_t n, float *d_Y,
+                  void *stream);
+/* The learned direction switch used by ogb_bfs mode 3: an 8 -> 64 -> 64 -> 1
+ * network whose output > 0 picks a bottom-up step; NULL removes it.  Its
+ * inputs, before every step, are scale-free (L(x) = log2(1 + x)):
+ * L(frontier) - L(V), L(frontier out-edges) - L(unexplored out-edges),
+ * L(frontier out-edges) - L(frontier), 1 when a bottom-up step would walk
+ * the unvisited list (else all vertices), visited fraction,
+ * L(frontier) - L(previous frontier), L(unvisited) - L(V),
+ * L(unexplored out-edges) - L(E). */
+int ogb_bfs_set_policy(const float *params);
+/* Those inputs for every step of the last ogb_bfs on g (count x 8 floats). */
+int ogb_bfs_features(ogb_graph *g, float *features, uint32_t max_levels, uint32_t *count);
+/* PageRank warm start: a 2 -> hidden -> hidden -> 1 network of
+ * log2(1 + in_degree), log2(1 + out_degree) predicts log2 of each vertex's
+ * unnormalized rank; d_init (V floats) = 2^prediction, for ogb_pagerank's
+ * d_init. */
+int ogb_pagerank_warm_start(ogb_graph *g, uint32_t hidden, const float *params, float *d_init, void *stream);
 
 /* Multi-source BFS (no reference counterpart: a batch of the reference's
  * single-root searches, BFS.c:476-626).  Up to 64 roots (host array), one

@@ -226,6 +226,13 @@ _DEVICE_API = [
     ("ogb_bfs", C.c_int, [vp, u32, u32, vp, vp, C.POINTER(BfsInfo), vp]),
     ("ogb_bfs_trace", C.c_int, [vp, C.POINTER(BfsLevel), u32, C.POINTER(u32)]),
     ("ogb_msbfs", C.c_int, [vp, u32p, u32, vp, C.POINTER(MsBfsInfo), vp]),
+    ("ogb_bfs_features", C.c_int, [vp, vp, u32, C.POINTER(u32)]),
+    ("ogb_bfs_set_policy", C.c_int, [vp]),
+    ("ogb_mlp_nparams", u32, [u32, u32]),
+    ("ogb_mlp_grad", C.c_int, [u32, u32, u32, vp, vp, u32, vp, vp, C.POINTER(C.c_float), vp]),
+    ("ogb_mlp_train", C.c_int, [u32, u32, u32, vp, vp, u32, u32, u32, C.c_float, u32, vp, vp, vp]),
+    ("ogb_mlp_infer", C.c_int, [u32, u32, vp, vp, u32, vp, vp]),
+    ("ogb_pagerank_warm_start", C.c_int, [vp, u32, vp, vp, vp]),
     ("ogb_ppr", C.c_int, [vp, u32p, u32, u32, C.c_double, vp, C.POINTER(PprBatchInfo), vp]),
     ("ogb_batch_create", vp, [u32, u32p, C.POINTER(C.c_uint64), u32p, u32p, u32]),
     ("ogb_batch_free", None, [vp]),
@@ -295,6 +302,45 @@ def load(weighted: bool = False) -> Library:
     if w not in _LIBS:
         _LIBS[w] = Library(w)
     return _LIBS[w]
+
+
+def mlp_nparams(lib, n_in: int, hidden: int) -> int:
+    return int(lib.ogb_mlp_nparams(n_in, hidden))
+
+
+def mlp_init(lib, n_in: int, hidden: int, seed: int = 0) -> np.ndarray:
+    """He-initialized fp32 parameters in the library's packing."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(mlp_nparams(lib, n_in, hidden), np.float32)
+    o = 0
+    for fan_in, n_out in ((n_in, hidden), (hidden, hidden), (hidden, 1)):
+        w = rng.normal(0.0, np.sqrt(2.0 / fan_in), size=(n_out, fan_in)).astype(np.float32)
+        p[o: o + w.size] = w.ravel()
+        o += w.size + n_out  # biases start at 0
+    return p
+
+
+def mlp_grad(lib, n_in, hidden, loss, X, T, params, stream=None):
+    """Batch-mean loss and gradient (device tensors X [B, in], T [B])."""
+    g = np.zeros_like(params)
+    l = C.c_float()
+    lib.check(lib.ogb_mlp_grad(n_in, hidden, loss, _ptr(X), _ptr(T), int(T.numel()), params.ctypes.data, g.ctypes.data,
+                               C.byref(l), stream), "ogb_mlp_grad")
+    return l.value, g
+
+
+def mlp_train(lib, n_in, hidden, loss, X, T, params, epochs=10, batch=4096, lr=1e-3, seed=0, stream=None):
+    p = np.ascontiguousarray(params.astype(np.float32).copy())
+    hist = np.zeros(max(epochs, 1), np.float32)
+    lib.check(lib.ogb_mlp_train(n_in, hidden, loss, _ptr(X), _ptr(T), int(T.numel()), epochs, batch, float(lr), seed,
+                                p.ctypes.data, hist.ctypes.data, stream), "ogb_mlp_train")
+    return p, hist[:epochs]
+
+
+def mlp_infer(lib, n_in, hidden, params, X, Y, stream=None):
+    p = np.ascontiguousarray(np.asarray(params, np.float32))
+    lib.check(lib.ogb_mlp_infer(n_in, hidden, p.ctypes.data, _ptr(X), int(Y.numel()), _ptr(Y), stream),
+              "ogb_mlp_infer")
 
 
 def default_arguments(**overrides) -> Arguments:
@@ -493,6 +539,19 @@ class DeviceGraph:
         d = info_dict(info)
         d["err_last"] = list(info.err_last)[:len(seeds)]
         return d
+
+    def bfs_features(self, max_levels: int = 512) -> np.ndarray:
+        """The learned switch's inputs before every step of the last bfs."""
+        out = np.zeros((max_levels, 8), np.float32)
+        n = u32()
+        self.lib.check(self.lib.ogb_bfs_features(self.handle, out.ctypes.data, max_levels, C.byref(n)),
+                       "ogb_bfs_features")
+        return out[:n.value].copy()
+
+    def pagerank_warm_start(self, params, init, hidden: int = 32, stream=None) -> None:
+        p = np.ascontiguousarray(np.asarray(params, np.float32))
+        self.lib.check(self.lib.ogb_pagerank_warm_start(self.handle, hidden, p.ctypes.data, _ptr(init), stream),
+                       "ogb_pagerank_warm_start")
 
     def bfs_trace(self, max_levels: int = 512) -> list[dict]:
         arr = (BfsLevel * max_levels)()

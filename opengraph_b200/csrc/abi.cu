@@ -1411,7 +1411,7 @@ extern "C" int ogb_sort_edges(const uint32_t* d_src, const uint32_t* d_dst, cons
 extern "C" int ogb_bfs(ogb_graph* g, uint32_t root, uint32_t mode, int32_t* d_parents, uint32_t* d_distances,
                        ogb_bfs_info* info, void* stream) {
   if (!g || !d_parents || !d_distances) return fail(ERR_ARG, "null");
-  if (mode > 2) return fail(ERR_ARG, "bfs mode %u", mode);
+  if (mode > 4) return fail(ERR_ARG, "bfs mode %u", mode);
   static thread_local BfsResult r;
   OGB_TRY(bfs_run(g->g, root, mode, d_parents, d_distances, &r, g_level_timing, false, as_stream(stream)));
   g->g.bfs_last_levels = r.nlevels;
@@ -1429,7 +1429,46 @@ extern "C" int ogb_bfs(ogb_graph* g, uint32_t root, uint32_t mode, int32_t* d_pa
     info->pad = 0;
   }
   memcpy(g->g.bfs_trace, r.levels, sizeof(r.levels[0]) * std::min(r.nlevels, 512));
+  memcpy(g->g.bfs_feat, r.feat, sizeof(r.feat[0]) * std::min(r.nlevels, 512));
   return OK;
+}
+
+extern "C" int ogb_bfs_features(ogb_graph* g, float* features, uint32_t max_levels, uint32_t* count) {
+  if (!g || !features || !count) return fail(ERR_ARG, "ogb_bfs_features: null argument");
+  const uint32_t n = std::min<uint32_t>(max_levels, (uint32_t)g->g.bfs_last_levels);
+  memcpy(features, g->g.bfs_feat, (size_t)n * 8 * sizeof(float));
+  *count = n;
+  return OK;
+}
+
+extern "C" int ogb_bfs_set_policy(const float* params) { return bfs_set_policy(params); }
+
+extern "C" uint32_t ogb_mlp_nparams(uint32_t in, uint32_t hidden) { return (uint32_t)mlp_nparams_host((int)in, (int)hidden); }
+
+extern "C" int ogb_mlp_grad(uint32_t in, uint32_t hidden, uint32_t loss, const float* d_X, const float* d_T,
+                            uint32_t batch, const float* params, float* grad, float* loss_out, void* stream) {
+  if (!d_X || !d_T || !params || !grad) return fail(ERR_ARG, "ogb_mlp_grad: null argument");
+  return mlp_grad((int)in, (int)hidden, (int)loss, d_X, d_T, (int)batch, params, grad, loss_out, as_stream(stream));
+}
+
+extern "C" int ogb_mlp_train(uint32_t in, uint32_t hidden, uint32_t loss, const float* d_X, const float* d_T,
+                             uint32_t n, uint32_t epochs, uint32_t batch, float lr, uint32_t seed, float* params,
+                             float* loss_hist, void* stream) {
+  if (!d_X || !d_T || !params) return fail(ERR_ARG, "ogb_mlp_train: null argument");
+  return mlp_train((int)in, (int)hidden, (int)loss, d_X, d_T, (int)n, (int)epochs, (int)batch, lr, seed, params,
+                   loss_hist, as_stream(stream));
+}
+
+extern "C" int ogb_mlp_infer(uint32_t in, uint32_t hidden, const float* params, const float* d_X, uint32_t n,
+                             float* d_Y, void* stream) {
+  if (!params || (n && (!d_X || !d_Y))) return fail(ERR_ARG, "ogb_mlp_infer: null argument");
+  return mlp_infer((int)in, (int)hidden, params, d_X, (int)n, d_Y, as_stream(stream));
+}
+
+extern "C" int ogb_pagerank_warm_start(ogb_graph* g, uint32_t hidden, const float* params, float* d_init,
+                                       void* stream) {
+  if (!g || !params || !d_init) return fail(ERR_ARG, "ogb_pagerank_warm_start: null argument");
+  return pr_warm_start(g->g, (int)hidden, params, d_init, as_stream(stream));
 }
 
 extern "C" int ogb_msbfs(ogb_graph* g, const uint32_t* roots, uint32_t nroots, uint16_t* d_depths,

@@ -60,6 +60,8 @@
 //  * queue appends are staged per CTA in shared memory (one global atomic
 //    per flush); counters are summed per CTA (one atomic per CTA);
 //  * bitmaps: bit v = word v>>5, bit v&31 (bitmap.h:7-9).
+#include <cuda_bf16.h>
+
 #include "graph.cuh"
 
 #include <algorithm>
@@ -90,6 +92,7 @@ struct BfsCtl {
   unsigned long long reached_edges;
   uint32_t reached;
   uint32_t pad;
+  unsigned long long fedges;  // out-edges of the vertices the step discovered
 };
 
 // The reference's switch state plus this search's bookkeeping.  Each CTA of
@@ -101,9 +104,14 @@ struct BfsCtrl {
   uint32_t ul_valid, ul_size, par_l, par_ul;
   uint32_t bm_r, bm_w, bm_c, depth;
   uint32_t iteration, processed, td_steps, bu_steps;
-  uint32_t nlevels, epoch, overflow, pad;
+  uint32_t nlevels, epoch, overflow, qcount_prev;
   unsigned long long edges_examined;
+  unsigned long long fedges;         // out-edges of the current frontier
+  unsigned long long edges_visited;  // out-edges of every visited vertex
 };
+
+// Inputs of the learned direction switch, from the state before a step.
+constexpr int kFeat = 8;
 
 struct BfsDevState {
   BfsCtrl c;
@@ -115,6 +123,7 @@ struct BfsDevState {
   BfsCtl ctl[3];      // per-phase counters, rotating
   BfsCtl aux;         // reached counts and the host-state steps
   BfsLevel trace[kMaxTrace];
+  float feat[kMaxTrace][kFeat];  // switch inputs before every step
 };
 
 // Device buffers of one graph (fixed; passed by value to every kernel).
@@ -132,8 +141,11 @@ struct BfsBufs {
   uint32_t* fdist;
   uint32_t* tile_i0;
   unsigned long long* status;
-  uint32_t V, words;
+  uint32_t V, words, E, pad;
+  const __nv_bfloat16* policy;  // learned switch weights (8 -> 64 -> 64 -> 1), or null
 };
+
+const __nv_bfloat16* bfs_policy_weights();
 
 struct BfsWork {
   uint32_t V = 0, E = 0;
@@ -206,7 +218,43 @@ static BfsBufs make_bufs(DevGraph& g, BfsWork* w) {
   b.status = w->scan_status.as<unsigned long long>();
   b.V = g.V;
   b.words = (g.V + 31) / 32;
+  b.E = g.E;
+  b.pad = 0;
+  b.policy = bfs_policy_weights();
   return b;
+}
+
+// ------------------------------------------------------------ learned switch
+
+// bf16 weights of the installed direction policy (null: none), per process.
+static DevBuf g_policy;
+static bool g_policy_set = false;
+const __nv_bfloat16* bfs_policy_weights() { return g_policy_set ? g_policy.as<__nv_bfloat16>() : nullptr; }
+
+__global__ void bfsk_policy_to_bf16(const float* __restrict__ p, int n, __nv_bfloat16* __restrict__ q) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) q[i] = __float2bfloat16_rn(p[i]);
+}
+
+int bfs_set_policy(const float* params_host) {
+  if (!params_host) {
+    g_policy_set = false;
+    return OK;
+  }
+  // the library's packing (W1, b1, W2[i][j], b2, w3, b3) with W2 transposed
+  constexpr int in = 8, h = 64, np = h * in + h + h * h + h + h + 1;
+  std::vector<float> p(params_host, params_host + np);
+  const int w2 = h * in + h;
+  for (int i = 0; i < h; i++)
+    for (int j = 0; j < h; j++) p[w2 + j * h + i] = params_host[w2 + i * h + j];
+  DevBuf tmp;
+  OGB_TRY(tmp.alloc(np * 4));
+  OGB_TRY(g_policy.alloc(np * 2 + 16));
+  OGB_CUDA(cudaMemcpy(tmp.p, p.data(), np * 4, cudaMemcpyHostToDevice));
+  bfsk_policy_to_bf16<<<(np + 255) / 256, 256>>>(tmp.as<float>(), np, g_policy.as<__nv_bfloat16>());
+  OGB_CUDA(cudaGetLastError());
+  OGB_CUDA(cudaDeviceSynchronize());
+  g_policy_set = true;
+  return OK;
 }
 
 // ------------------------------------------------------------ shared memory
@@ -413,7 +461,8 @@ __device__ void td_scan_phase(const BfsBufs& b, const uint32_t* list, uint32_t n
 template <bool kDepthKnown>
 __device__ __forceinline__ void expand_edges(const BfsBufs& b, uint32_t e0, uint32_t e1, uint32_t cnt,
                                              int32_t* parents, uint32_t* distances, uint32_t dnext, uint32_t* bm_w,
-                                             uint32_t* all_out, TdSmem& sm, uint32_t& mf, uint32_t& found) {
+                                             uint32_t* all_out, TdSmem& sm, uint32_t& mf, uint32_t& found,
+                                             unsigned long long& fed) {
   constexpr int K = kExpTile / kExpT;
   uint32_t u[K], src[K], dd[K];
   bool ok[K];
@@ -452,7 +501,9 @@ __device__ __forceinline__ void expand_edges(const BfsBufs& b, uint32_t e0, uint
       found++;
       if (bm_w) atomicOr(&bm_w[u[k] >> 5], 1u << (u[k] & 31));
       if (all_out) ba_push(sm.q_all, u[k]);
-      if (__ldg(&b.out_degree[u[k]])) ba_push(sm.q_list, u[k]);
+      const uint32_t od = __ldg(&b.out_degree[u[k]]);
+      fed += od;
+      if (od) ba_push(sm.q_list, u[k]);
     }
   }
 }
@@ -472,6 +523,7 @@ __device__ void td_expand_phase(const BfsBufs& b, const uint32_t* list, uint32_t
   ba_init(sm.q_list);
   ba_init(sm.q_all);
   uint32_t mf = 0, found = 0;
+  unsigned long long fed = 0;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const uint32_t e0 = t * kExpTile;
     const uint32_t e1 = min(e0 + kExpTile, total);
@@ -486,13 +538,14 @@ __device__ void td_expand_phase(const BfsBufs& b, const uint32_t* list, uint32_t
       if (!kDepthKnown) sm.d[k] = b.fdist[i0 + k];
     }
     __syncthreads();
-    expand_edges<kDepthKnown>(b, e0, e1, cnt, parents, distances, dnext, bm_w, all_out, sm, mf, found);
+    expand_edges<kDepthKnown>(b, e0, e1, cnt, parents, distances, dnext, bm_w, all_out, sm, mf, found, fed);
     // at most kExpTile discoveries per tile: flush every tile
     ba_flush(sm.q_list, next_list, &ctl->lnext);
     if (all_out) ba_flush(sm.q_all, all_out, &ctl->all_count);
   }
   block_add_total<uint32_t>(&ctl->mf, mf, reinterpret_cast<uint32_t*>(s_red));
   block_add_total<uint32_t>(&ctl->qnext, found, reinterpret_cast<uint32_t*>(s_red));
+  block_add_total<unsigned long long>(&ctl->fedges, fed, s_red);
 }
 
 // A top-down step over a list of at most kExpTile entries: every CTA loads
@@ -532,14 +585,16 @@ __device__ void td_small_phase(const BfsBufs& b, const uint32_t* list, uint32_t*
   if (blockIdx.x >= ntiles) return;
   ba_init(sm.q_list);
   uint32_t mf = 0, found = 0;
+  unsigned long long fed = 0;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const uint32_t e0 = t * kExpTile;
     const uint32_t e1 = min(e0 + kExpTile, total);
-    expand_edges<true>(b, e0, e1, n, parents, distances, dnext, bm_w, nullptr, sm, mf, found);
+    expand_edges<true>(b, e0, e1, n, parents, distances, dnext, bm_w, nullptr, sm, mf, found, fed);
     ba_flush(sm.q_list, next_list, &ctl->lnext);
   }
   block_add_total<uint32_t>(&ctl->mf, mf, reinterpret_cast<uint32_t*>(s_red));
   block_add_total<uint32_t>(&ctl->qnext, found, reinterpret_cast<uint32_t*>(s_red));
+  block_add_total<unsigned long long>(&ctl->fedges, fed, s_red);
 }
 
 // ------------------------------------------------------------ bottom-up ----
@@ -574,6 +629,7 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
   const uint32_t count = kDense ? b.V : ul_count;
   uint32_t nf = 0, edges = 0;
+  unsigned long long fed = 0;
   for (uint32_t rbase = blockIdx.x * kBuRound; rbase < count; rbase += gridDim.x * kBuRound) {
     uint32_t v[kBuV];
 #pragma unroll
@@ -619,7 +675,9 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
           nf++;
           edges += hit[k] + 1;
           if (!kDense) atomicOr(&bm_next[v[k] >> 5], 1u << (v[k] & 31));
-          if (__ldg(&b.out_degree[v[k]])) ba_push(sm.q_list, v[k]);
+          const uint32_t od = __ldg(&b.out_degree[v[k]]);
+          fed += od;
+          if (od) ba_push(sm.q_list, v[k]);
         } else if (row[k].y > kFirst) {
           edges += kFirst;
           const uint32_t h = warp_atomic_inc(&sm.nheavy);
@@ -658,7 +716,9 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
             atomicOr(&bm_next[hv >> 5], 1u << (hv & 31));
             nf++;
             edges += j + first + 1 - j0;
-            if (__ldg(&b.out_degree[hv])) ba_push(sm.q_list, hv);
+            const uint32_t od = __ldg(&b.out_degree[hv]);
+            fed += od;
+            if (od) ba_push(sm.q_list, hv);
           }
           hit_row = true;
           break;
@@ -676,6 +736,7 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
   }
   block_add_total<uint32_t>(&ctl->nf, nf, reinterpret_cast<uint32_t*>(s_red));
   block_add_total<unsigned long long>(&ctl->edges, (unsigned long long)edges, s_red);
+  block_add_total<unsigned long long>(&ctl->fedges, fed, s_red);
 }
 
 // ---- bottom-up of the host-state step (depth read from the parent) --------
@@ -744,6 +805,7 @@ __device__ __forceinline__ void load_ctl(const BfsCtl* p, BfsCtl& out) {
   out.ul_size = v->ul_size;
   out.total_edges = v->total_edges;
   out.edges = v->edges;
+  out.fedges = v->fedges;
 }
 
 __device__ __forceinline__ void zero_ctl(BfsCtl* p) {
@@ -753,15 +815,32 @@ __device__ __forceinline__ void zero_ctl(BfsCtl* p) {
 
 // Before a step: stop on an empty queue, else pick the direction with the
 // reference's rule (BFS.c:520-560).
-__device__ uint32_t ctrl_decide(BfsCtrl& c) {
+__device__ uint32_t ctrl_decide(BfsCtrl& c, bool policy_bu) {
   if (c.overflow) return kActDone;
+  if (c.mode == BFS_LEARNED) {
+    // the learned switch: every step's direction from the policy (any order
+    // of directions is valid: both kinds of step keep the frontier as a list
+    // and as a bitmap); the loop ends on an empty frontier
+    if (c.qcount == 0) return kActDone;
+    c.frontier = c.qcount;
+    if (policy_bu) {
+      c.in_bu = 1;
+      c.nf = c.qcount;
+      c.nf_prev = c.nf;
+      return kActBU;
+    }
+    c.in_bu = 0;
+    c.mu -= min(c.mf, c.mu);
+    c.epoch++;
+    return kActTD;
+  }
   if (!c.in_bu && c.qcount == 0) return kActDone;
   if (c.in_bu) {
     c.frontier = c.nf;
     c.nf_prev = c.nf;
     return kActBU;
   }
-  const bool bu = (c.mode == BFS_PULL) || (c.mode == BFS_DO && c.mf > c.mu / kAlpha);
+  const bool bu = (c.mode == BFS_PULL) || (c.mode == BFS_PULL_DENSE) || (c.mode == BFS_DO && c.mf > c.mu / kAlpha);
   c.frontier = c.qcount;
   if (bu) {
     c.in_bu = 1;
@@ -792,16 +871,65 @@ __device__ void ctrl_level(BfsCtrl& c, BfsDevState* st, bool leader, uint32_t di
   c.depth++;
   c.processed += disc;
   c.edges_examined += edges;
+  c.qcount_prev = c.frontier;
   if (c.iteration > c.max_steps) c.overflow = 1;
 }
 
-// After a top-down step: it wrote its discoveries into bm_w and cleared the
-// other two bitmaps, so bm_w becomes the frontier bitmap.
+// The learned switch's inputs: scale-free ratios of the state before a step
+// (log2(1 + x) of the counts, differenced), so that a policy trained on one
+// graph size applies to others.
+__device__ __forceinline__ void bfs_features(const BfsCtrl& c, uint32_t E, float* f) {
+  const unsigned long long left = (unsigned long long)E > c.edges_visited ? (unsigned long long)E - c.edges_visited : 0ull;
+  const float lq = log2f(1.0f + (float)c.qcount), ln = log2f(1.0f + (float)c.n), le = log2f(1.0f + (float)E);
+  const float lfe = log2f(1.0f + (float)c.fedges), lleft = log2f(1.0f + (float)left);
+  f[0] = lq - ln;                                                    // frontier fraction
+  f[1] = lfe - lleft;                                                // frontier edges vs unexplored edges
+  f[2] = lfe - lq;                                                   // mean out-degree of the frontier
+  f[3] = c.ul_valid ? 1.0f : 0.0f;                                   // a bottom-up step would walk the unvisited list
+  f[4] = (float)c.processed / (float)max(c.n, 1u);                   // visited fraction
+  f[5] = lq - log2f(1.0f + (float)c.qcount_prev);                    // frontier growth
+  f[6] = log2f(1.0f + (float)(c.n - min(c.processed, c.n))) - ln;    // unvisited fraction
+  f[7] = lleft - le;                                                 // unexplored edge fraction
+}
+
+// Policy network layout on the device (bf16): W1[64][8], b1[64], W2T[64][64]
+// (transposed: W2T[j][i] = W2[i][j]), b2[64], w3[64], b3.
+constexpr int kPolIn = kFeat, kPolH = 64;
+constexpr int kPolW1 = 0, kPolB1 = kPolH * kPolIn, kPolW2T = kPolB1 + kPolH, kPolB2 = kPolW2T + kPolH * kPolH,
+              kPolW3 = kPolB2 + kPolH, kPolB3 = kPolW3 + kPolH, kPolN = kPolB3 + 1;
+
+// Policy output of a warp (bf16 weights in shared memory, fp32 sums): lane
+// l owns hidden units l and l + 32; every lane returns the output.
+__device__ __forceinline__ float policy_logit(const __nv_bfloat16* P, const float* f, uint32_t lane) {
+  float ha = __bfloat162float(P[kPolB1 + lane]), hb = __bfloat162float(P[kPolB1 + lane + 32]);
+#pragma unroll
+  for (int j = 0; j < kPolIn; j++) {
+    ha = fmaf(__bfloat162float(P[kPolW1 + lane * kPolIn + j]), f[j], ha);
+    hb = fmaf(__bfloat162float(P[kPolW1 + (lane + 32) * kPolIn + j]), f[j], hb);
+  }
+  ha = fmaxf(ha, 0.f);
+  hb = fmaxf(hb, 0.f);
+  float sa = __bfloat162float(P[kPolB2 + lane]), sb = __bfloat162float(P[kPolB2 + lane + 32]);
+#pragma unroll 8
+  for (int j = 0; j < kPolH; j++) {
+    const float hj = __shfl_sync(0xffffffffu, j < 32 ? ha : hb, j & 31);
+    sa = fmaf(__bfloat162float(P[kPolW2T + j * kPolH + lane]), hj, sa);
+    sb = fmaf(__bfloat162float(P[kPolW2T + j * kPolH + lane + 32]), hj, sb);
+  }
+  float y = __bfloat162float(P[kPolW3 + lane]) * fmaxf(sa, 0.f) +
+            __bfloat162float(P[kPolW3 + lane + 32]) * fmaxf(sb, 0.f);
+#pragma unroll
+  for (int o = 16; o; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+  return y + __bfloat162float(P[kPolB3]);
+}
+
 __device__ void ctrl_finish_td(BfsCtrl& c, uint32_t total_edges, const BfsCtl& k, BfsDevState* st, bool leader,
                                unsigned long long t0) {
   c.mf = k.mf;
   c.qcount = k.qnext;
   c.lsize = k.lnext;
+  c.fedges = k.fedges;
+  c.edges_visited += k.fedges;
   c.par_l ^= 1u;
   const uint32_t r = c.bm_r;
   c.bm_r = c.bm_w;
@@ -817,10 +945,12 @@ __device__ void ctrl_finish_td(BfsCtrl& c, uint32_t total_edges, const BfsCtl& k
 __device__ void ctrl_finish_bu(BfsCtrl& c, const BfsCtl& k, BfsDevState* st, bool leader, unsigned long long t0) {
   c.nf = k.nf;
   c.ul_size = k.ul_size;
-  c.ul_valid = 1;
+  c.ul_valid = c.mode == BFS_PULL_DENSE ? 0u : 1u;  // that mode walks every vertex in every step
   c.par_ul ^= 1u;
   c.qcount = k.nf;
   c.lsize = k.lnext;
+  c.fedges = k.fedges;
+  c.edges_visited += k.fedges;
   c.par_l ^= 1u;
   const uint32_t r = c.bm_r;
   c.bm_r = c.bm_w;
@@ -828,7 +958,9 @@ __device__ void ctrl_finish_bu(BfsCtrl& c, const BfsCtl& k, BfsDevState* st, boo
   c.bm_c = r;
   c.bu_steps++;
   ctrl_level(c, st, leader, 1, c.nf, k.edges, t0);
-  const bool cont = (c.mode == BFS_PULL) ? (c.nf > 0) : ((c.nf > c.nf_prev) || (c.nf > c.n / kBeta));
+  if (c.mode == BFS_LEARNED) return;  // the policy picks every step
+  const bool cont = (c.mode == BFS_PULL || c.mode == BFS_PULL_DENSE) ? (c.nf > 0)
+                                                                    : ((c.nf > c.nf_prev) || (c.nf > c.n / kBeta));
   if (!cont) {
     c.in_bu = 0;
     c.mf = 1;
@@ -872,6 +1004,8 @@ __global__ void __launch_bounds__(256) bfsk_init(BfsBufs b, BfsDevState* st, uin
     c.iteration = 1;
     c.processed = 1;
     c.epoch = epoch;
+    c.fedges = d;
+    c.edges_visited = d;
     st->c = c;
     st->parents = parents;
     st->distances = distances;
@@ -901,6 +1035,8 @@ __global__ void bfsk_set_roots(BfsBufs b, BfsDevState* st, const uint32_t* __res
     c.qcount++;
     c.processed++;
     c.mf += d;
+    c.fedges += d;
+    c.edges_visited += d;
     if (d) b.list[0][c.lsize++] = r;
   }
   st->c = c;
@@ -917,17 +1053,28 @@ __global__ void __launch_bounds__(kSearchT, 5) bfsk_search(BfsBufs b, BfsDevStat
   __shared__ unsigned long long s_red[kSearchT / 32];
   __shared__ uint32_t s_act, s_ok;
   __shared__ unsigned long long s_t0;
+  __shared__ __nv_bfloat16 s_pol[kPolN];
   const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
   if (threadIdx.x == 0) S = st->c;
+  if (b.policy)
+    for (int i = threadIdx.x; i < kPolN; i += blockDim.x) s_pol[i] = b.policy[i];
   __syncthreads();
   int32_t* parents = st->parents;
   uint32_t* distances = st->distances;
   BfsCtl* ctl = st->ctl;
   uint32_t p = 0;
   for (;;) {
-    if (threadIdx.x == 0) {
-      s_act = ctrl_decide(S);
-      s_t0 = global_ns();
+    if (threadIdx.x < 32) {
+      float f[kFeat];
+      bfs_features(S, b.E, f);
+      bool bu = false;
+      if (S.mode == BFS_LEARNED) bu = policy_logit(s_pol, f, threadIdx.x) > 0.0f;
+      if (leader && S.nlevels < (uint32_t)kMaxTrace && !S.overflow)
+        for (int i = 0; i < kFeat; i++) st->feat[S.nlevels][i] = f[i];
+      if (threadIdx.x == 0) {
+        s_act = ctrl_decide(S, bu);
+        s_t0 = global_ns();
+      }
     }
     __syncthreads();
     const uint32_t act = s_act;
@@ -1146,7 +1293,8 @@ int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t 
   for (uint32_t i = 0; i < nroots; i++)
     if (roots[i] >= V) return fail(ERR_ARG, "bfs: root %u out of range (V=%u)", roots[i], V);
   const uint32_t root = roots[0];
-  if (mode > BFS_DO) return fail(ERR_ARG, "bfs: mode %u", mode);
+  if (mode > BFS_PULL_DENSE) return fail(ERR_ARG, "bfs: mode %u", mode);
+  if (mode == BFS_LEARNED && !bfs_policy_weights()) return fail(ERR_ARG, "bfs: no learned switch installed");
   BfsWork* w = nullptr;
   OGB_TRY(bfs_work_get(g, &w));
   BfsBufs b = make_bufs(g, w);
@@ -1192,7 +1340,10 @@ int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t 
   r.ms = total_ms;
   r.launches = 1;  // kernels in the timed region: the search (init runs before it)
   r.nlevels = (int)std::min<uint32_t>(h->c.nlevels, kMaxTrace);
-  for (int i = 0; i < r.nlevels; i++) r.levels[i] = h->trace[i];
+  for (int i = 0; i < r.nlevels; i++) {
+    r.levels[i] = h->trace[i];
+    for (int k = 0; k < kFeat; k++) r.feat[i][k] = h->feat[i][k];
+  }
   if (res) *res = r;
   return OK;
 }

@@ -59,6 +59,7 @@ struct DevGraph {
   // traces of the last BFS / PageRank run through the device API
   int bfs_last_levels = 0;
   BfsLevel bfs_trace[512];
+  float bfs_feat[512][8];  // learned-switch inputs of the last BFS's steps
   uint32_t pr_last_executed = 0;
   double pr_err_hist[1024];
   uint32_t pr_active_hist[1024];
@@ -89,7 +90,9 @@ size_t scan_tmp_words(uint32_t n);
 int graph_check(DevGraph& g, cudaStream_t s);
 
 // ---- BFS -------------------------------------------------------------------
-enum BfsMode : uint32_t { BFS_PULL = 0, BFS_PUSH = 1, BFS_DO = 2 };
+// BFS_PULL_DENSE: pull-only with every bottom-up step over all vertices (no
+// unvisited list) -- a cost probe for the learned switch's training data.
+enum BfsMode : uint32_t { BFS_PULL = 0, BFS_PUSH = 1, BFS_DO = 2, BFS_LEARNED = 3, BFS_PULL_DENSE = 4 };
 
 
 
@@ -104,7 +107,12 @@ struct BfsResult {
   double ms = 0.0;
   int nlevels = 0;
   BfsLevel levels[512];
+  float feat[512][8];  // the learned switch's inputs before every step
 };
+
+// Learned direction switch (mode BFS_LEARNED): fp32 parameters of the
+// 8 -> 64 -> 64 -> 1 policy network (host; stored as bf16), or null to remove.
+int bfs_set_policy(const float* params_host);
 
 // Direction switch policy: plain rule (alpha/beta) unless a policy callback
 // is installed (learned switch).  Returns 1 for bottom-up.
@@ -176,6 +184,15 @@ int batch_bfs(GraphBatch& b, const uint32_t* roots, int32_t* parents, uint32_t* 
 int batch_pagerank(GraphBatch& b, uint32_t max_iters, double epsilon, float* ranks, BatchPrGraph* per_graph,
                    double* ms, uint32_t* captured, cudaStream_t s);
 int batch_autotune(GraphBatch& b, uint32_t iters, TuneResult* out, cudaStream_t s);
+
+// ---- the learned parts' networks (mlp.cu) -----------------------------------
+int mlp_nparams_host(int in, int h);
+int mlp_grad(int in, int h, int loss, const float* X, const float* T, int B, const float* params_host,
+             float* grad_host, float* loss_host, cudaStream_t s);
+int mlp_train(int in, int h, int loss, const float* X, const float* T, int N, int epochs, int batch, float lr,
+              uint32_t seed, float* params_host, float* loss_hist, cudaStream_t s);
+int mlp_infer(int in, int h, const float* params_host, const float* X, int N, float* Y, cudaStream_t s);
+int pr_warm_start(DevGraph& g, int h, const float* params_host, float* init, cudaStream_t s);
 
 // ---- batched personalized PageRank (batch.cu) -------------------------------
 struct PprResult {

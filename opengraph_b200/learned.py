@@ -1,0 +1,225 @@
+"""The learned parts beside the plain path: a direction-switch policy for BFS
+and a warm-start vector for PageRank, trained on the GPU by the library's
+own MLP kernels (ogb_mlp_train) on traces of the plain GPU runs, and used by
+hand-written inference kernels (bf16 weights, fp32 accumulation).
+
+  python -m opengraph_b200.learned train [dir] # writes opengraph_b200/weights/*.f32 (or dir)
+  python -m opengraph_b200.learned evaluate   # learned vs plain on held-out graphs
+
+Direction switch (8 -> 64 -> 64 -> 1, output > 0 = bottom-up step).  Every
+BFS level has the same frontier whatever the directions chosen before it
+(the search is level-synchronous), so a push-only and a pull-only search
+from one root give, level by level, the device time of a top-down and of a
+bottom-up step on the same frontier.  Training samples: the scale-free
+switch inputs the kernel records before each level (ogb_bfs_features), with
+target log2(top-down ms / bottom-up ms) (clipped to +-8): a squared-error
+fit of the time ratio, so the levels where the choice costs most weigh
+most.  The plain alpha/beta rule stays the default (mode 2); mode 3 uses
+the policy; depths are identical by construction.
+
+PageRank warm start (2 -> 32 -> 32 -> 1): inputs log2(1 + in-degree),
+log2(1 + out-degree); target log2 of the vertex's unnormalized rank after
+the plain pull run (100 iterations).  The start vector 2^prediction replaces
+the uniform 1 - 0.85 (pageRank.c:68); the iteration and its stop rule are
+unchanged, so the run converges to the same ranks (within the tolerance).
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+WEIGHTS = os.path.join(HERE, "weights")
+SWITCH = ("switch_mlp.f32", 8, 64)
+PR_START = ("pr_start_mlp.f32", 2, 32)
+
+
+def weights_path(spec) -> str:
+    return os.path.join(WEIGHTS, spec[0])
+
+
+def load_weights(lib, spec) -> np.ndarray | None:
+    """The committed fp32 parameters of a network, or None when absent."""
+    import opengraph_b200 as og
+    p = weights_path(spec)
+    if not os.path.exists(p):
+        return None
+    w = np.fromfile(p, dtype=np.float32)
+    if len(w) != og.mlp_nparams(lib, spec[1], spec[2]):
+        raise ValueError(f"{p}: {len(w)} parameters, expected {og.mlp_nparams(lib, spec[1], spec[2])}")
+    return w
+
+
+def _device_graph(lib, s, d, V):
+    import torch
+    g = lib.device_graph()
+    g.build(torch.from_numpy(s.view(np.int32)).cuda(), torch.from_numpy(d.view(np.int32)).cuda(), V, 0)
+    return g
+
+
+def _roots(g, n, seed):
+    outdeg = g.view(False).out_degree.cpu().numpy().view(np.uint32)
+    rng = np.random.default_rng(seed)
+    cand = np.nonzero(outdeg > 0)[0]
+    return [int(x) for x in rng.choice(cand, size=min(n, len(cand)), replace=False)]
+
+
+def switch_samples(lib, g, V, roots):
+    """(features, log2(td ms / bu ms)) per level: positive when the bottom-up
+    step on that level's frontier was faster than the top-down step.  Two
+    samples per level: a bottom-up step over all vertices (feature 3 = 0,
+    measured by the dense pull probe, mode 4) and one over the unvisited
+    list (feature 3 = 1, the pull-only search's steps after its first)."""
+    import torch
+    par = torch.empty(V, dtype=torch.int32, device="cuda")
+    dist = torch.empty(V, dtype=torch.int32, device="cuda")
+    X, Y = [], []
+
+    def ratio(a, b):
+        return np.clip(np.log2(np.maximum(np.asarray(a), 1e-4) / np.maximum(np.asarray(b), 1e-4)), -8, 8)
+
+    for r in roots:
+        g.bfs(r, par, dist, mode=1)            # push only
+        td = [L["ms"] for L in g.bfs_trace()]
+        feat = g.bfs_features()
+        g.bfs(r, par, dist, mode=4)            # pull, every step over all vertices
+        dense = [L["ms"] for L in g.bfs_trace()]
+        g.bfs(r, par, dist, mode=0)            # pull, unvisited list after the first step
+        lst = [L["ms"] for L in g.bfs_trace()]
+        n = min(len(td), len(dense), len(feat))
+        f0 = feat[:n].copy()
+        f0[:, 3] = 0.0
+        X.append(f0)
+        Y.append(ratio(td[:n], dense[:n]).astype(np.float32))
+        m = min(len(td), len(lst), len(feat))
+        if m > 1:
+            f1 = feat[1:m].copy()
+            f1[:, 3] = 1.0
+            X.append(f1)
+            Y.append(ratio(td[1:m], lst[1:m]).astype(np.float32))
+    return np.concatenate(X), np.concatenate(Y)
+
+
+def pr_samples(lib, g, V, n_samples, seed):
+    """(features, target) for a random subset of vertices."""
+    import torch
+    ranks = torch.empty(V, dtype=torch.float32, device="cuda")
+    g.pagerank(ranks, mode=0, max_iterations=100, epsilon=0.0)
+    r = ranks.cpu().numpy().astype(np.float64) * V       # unnormalized
+    indeg = g.view(True).out_degree.cpu().numpy().view(np.uint32).astype(np.float64)
+    outdeg = g.view(False).out_degree.cpu().numpy().view(np.uint32).astype(np.float64)
+    rng = np.random.default_rng(seed)
+    idx = rng.choice(V, size=min(n_samples, V), replace=False)
+    X = np.stack([np.log2(1 + indeg[idx]), np.log2(1 + outdeg[idx])], axis=1).astype(np.float32)
+    Y = np.log2(np.maximum(r[idx], 1e-30)).astype(np.float32)
+    return X, Y
+
+
+def train(scales=(18, 19, 20, 21, 22), seeds=(0, 1, 2, 3), roots_per_graph=8, out=WEIGHTS, log=print):
+    import torch
+
+    import opengraph_b200 as og
+    lib = og.load(False)
+    lib.quiet(True)
+    Xs, Ys, Xp, Yp = [], [], [], []
+    for sc in scales:
+        for sd in seeds:
+            s, d, _ = og.generate_rmat(sc, 16, 100 + sd)
+            V = 1 << sc
+            g = _device_graph(lib, s, d, V)
+            x, y = switch_samples(lib, g, V, _roots(g, roots_per_graph, sd))
+            Xs.append(x)
+            Ys.append(y)
+            x, y = pr_samples(lib, g, V, 200_000, sd)
+            Xp.append(x)
+            Yp.append(y)
+            g.close()
+            log(f"traces: RMAT-{sc} seed {sd}")
+    os.makedirs(out, exist_ok=True)
+    res = {}
+    for name, (X, Y), spec, loss, epochs, batch, lr in (
+            ("switch", (np.concatenate(Xs), np.concatenate(Ys)), SWITCH, 0, 600, 128, 1e-3),
+            ("pr_start", (np.concatenate(Xp), np.concatenate(Yp)), PR_START, 0, 30, 4096, 2e-3)):
+        tx = torch.from_numpy(np.ascontiguousarray(X)).cuda()
+        ty = torch.from_numpy(np.ascontiguousarray(Y)).cuda()
+        p0 = og.mlp_init(lib, spec[1], spec[2], seed=7)
+        p, hist = og.mlp_train(lib, spec[1], spec[2], loss, tx, ty, p0, epochs=epochs, batch=batch, lr=lr, seed=11)
+        p.astype(np.float32).tofile(os.path.join(out, spec[0]))
+        res[name] = {"samples": int(len(Y)), "loss_first": float(hist[0]), "loss_last": float(hist[-1])}
+        if name == "switch":
+            res[name]["bottom_up_faster_fraction"] = float((Y > 0).mean())
+        log(f"{name}: {res[name]}")
+    return res
+
+
+def evaluate(log=print):
+    """Learned vs plain on held-out graphs: RMAT-24 (seeds never used in
+    training) and a 4096 x 4096 grid with random shortcuts (p = 1e-4)."""
+    import torch
+
+    import opengraph_b200 as og
+    lib = og.load(False)
+    lib.quiet(True)
+    sw = load_weights(lib, SWITCH)
+    pw = load_weights(lib, PR_START)
+    if sw is None or pw is None:
+        raise SystemExit("no trained weights: run `python -m opengraph_b200.learned train` first")
+    lib.check(lib.ogb_bfs_set_policy(sw.ctypes.data), "ogb_bfs_set_policy")
+    out = {}
+    graphs = [("rmat24_seed900", lambda: og.generate_rmat(24, 16, 900)[:2], 1 << 24),
+              ("grid4096_p1e-4", lambda: og.generate_grid(4096, 1e-4, 901)[:2], 4096 * 4096)]
+    for name, gen, V in graphs:
+        s, d = gen()
+        g = _device_graph(lib, s, d, V)
+        par = torch.empty(V, dtype=torch.int32, device="cuda")
+        dist = torch.empty(V, dtype=torch.int32, device="cuda")
+        roots = _roots(g, 8, 77)
+        res = {}
+        for mode, tag in ((2, "plain"), (3, "learned")):
+            ms = edges = 0.0
+            depths = []
+            for r in roots:
+                g.bfs(r, par, dist, mode=mode)
+                info = g.bfs(r, par, dist, mode=mode)
+                ms += info["ms"]
+                edges += info["reached_out_edges"]
+                depths.append(dist.cpu().numpy().copy())
+            res[tag] = {"gteps": edges / ms / 1e6, "ms_per_search": ms / len(roots), "depths": depths}
+        same = all(np.array_equal(a, b) for a, b in zip(res["plain"]["depths"], res["learned"]["depths"]))
+        bfs = {t: {k: round(v, 4) for k, v in res[t].items() if k != "depths"} for t in res}
+        bfs["depths_identical"] = bool(same)
+        # PageRank: iterations until the L1 change of normalized ranks < 1e-6
+        ranks = torch.empty(V, dtype=torch.float32, device="cuda")
+        init = torch.empty(V, dtype=torch.float32, device="cuda")
+        pr = {}
+        for tag in ("plain", "learned"):
+            if tag == "learned":
+                g.pagerank_warm_start(pw, init, hidden=PR_START[2])
+                start = init
+            else:
+                start = None
+            info = g.pagerank(ranks, mode=0, max_iterations=200, epsilon=0.0, init=start)
+            errs, _ = g.pagerank_history()
+            hit = next((i for i, e in enumerate(errs) if e < 1e-6), None)
+            it_ms = info["ms"] / 200
+            pr[tag] = {"iterations_to_1e-6": (hit + 1) if hit is not None else None,
+                       "ms_to_1e-6": round(it_ms * (hit + 1), 3) if hit is not None else None,
+                       "ranks": ranks.cpu().numpy().astype(np.float64)}
+        l1 = float(np.abs(pr["plain"].pop("ranks") - pr["learned"].pop("ranks")).sum())
+        pr["final_l1_between"] = l1
+        out[name] = {"bfs": bfs, "pagerank": pr}
+        log(f"{name}: {json.dumps(out[name])}")
+        g.close()
+    lib.ogb_bfs_set_policy(None)
+    return out
+
+
+if __name__ == "__main__":
+    cmd = sys.argv[1] if len(sys.argv) > 1 else "evaluate"
+    if cmd == "train":
+        print(json.dumps(train(out=sys.argv[2] if len(sys.argv) > 2 else WEIGHTS)))
+    else:
+        print(json.dumps(evaluate()))

@@ -1,0 +1,166 @@
+"""GPU checks of the learned parts: the MLP kernels' gradients against an
+FP64 CPU computation, training, bf16 inference, the learned BFS switch (same
+depths as the plain path whatever the policy) and the PageRank warm start
+(same ranks within the tolerance, fewer iterations to reach it)."""
+import numpy as np
+import pytest
+
+from test_build_gpu import dev, host
+
+pytestmark = pytest.mark.gpu
+
+
+def np_mlp(p, X, n_in, h):
+    """FP64 forward of the library's packing; returns (y, cache)."""
+    p = p.astype(np.float64)
+    o = 0
+    W1 = p[o:o + h * n_in].reshape(h, n_in); o += h * n_in
+    b1 = p[o:o + h]; o += h
+    W2 = p[o:o + h * h].reshape(h, h); o += h * h
+    b2 = p[o:o + h]; o += h
+    w3 = p[o:o + h]; o += h
+    b3 = p[o]
+    z1 = X @ W1.T + b1
+    a1 = np.maximum(z1, 0)
+    z2 = a1 @ W2.T + b2
+    a2 = np.maximum(z2, 0)
+    y = a2 @ w3 + b3
+    return y, (W1, W2, w3, z1, a1, z2, a2)
+
+
+def np_grad(p, X, T, n_in, h, loss):
+    X = X.astype(np.float64)
+    T = T.astype(np.float64)
+    y, (W1, W2, w3, z1, a1, z2, a2) = np_mlp(p, X, n_in, h)
+    B = len(T)
+    if loss == 0:
+        L = np.mean((y - T) ** 2)
+        dy = 2 * (y - T) / B
+    else:
+        L = np.mean(np.maximum(y, 0) - y * T + np.log1p(np.exp(-np.abs(y))))
+        dy = (1 / (1 + np.exp(-y)) - T) / B
+    dw3 = a2.T @ dy
+    db3 = dy.sum()
+    d2 = np.outer(dy, w3) * (z2 > 0)
+    dW2 = d2.T @ a1
+    db2 = d2.sum(0)
+    d1 = (d2 @ W2) * (z1 > 0)
+    dW1 = d1.T @ X
+    db1 = d1.sum(0)
+    return L, np.concatenate([dW1.ravel(), db1, dW2.ravel(), db2, dw3, [db3]])
+
+
+@pytest.mark.parametrize("n_in,h,loss", [(8, 64, 1), (2, 32, 0), (3, 16, 0), (8, 64, 0)])
+def test_mlp_gradient_matches_fp64(torch_cuda, lib, n_in, h, loss):
+    import opengraph_b200 as og
+    torch = torch_cuda
+    rng = np.random.default_rng(n_in * 100 + h)
+    B = 257
+    X = rng.normal(size=(B, n_in)).astype(np.float32)
+    T = (rng.random(B) < 0.4).astype(np.float32) if loss == 1 else rng.normal(size=B).astype(np.float32)
+    p = og.mlp_init(lib, n_in, h, seed=3)
+    p[h * n_in: h * n_in + h] = rng.normal(0, 0.1, h)          # nonzero biases
+    Lg, g = og.mlp_grad(lib, n_in, h, loss, torch.from_numpy(X).cuda(), torch.from_numpy(T).cuda(), p)
+    Lr, gr = np_grad(p, X, T, n_in, h, loss)
+    assert abs(Lg - Lr) <= 1e-5 * max(1.0, abs(Lr))
+    rel = np.abs(g - gr).max() / (np.abs(gr).max() + 1e-12)
+    assert rel < 1e-4, rel
+
+
+def test_mlp_training_reduces_loss_and_bf16_inference(torch_cuda, lib):
+    import opengraph_b200 as og
+    torch = torch_cuda
+    rng = np.random.default_rng(0)
+    N = 20_000
+    X = rng.uniform(-2, 2, size=(N, 2)).astype(np.float32)
+    T = (np.sin(X[:, 0]) + 0.5 * X[:, 1] ** 2).astype(np.float32)
+    tx, ty = torch.from_numpy(X).cuda(), torch.from_numpy(T).cuda()
+    p0 = og.mlp_init(lib, 2, 32, seed=1)
+    L0, _ = og.mlp_grad(lib, 2, 32, 0, tx[:4096], ty[:4096], p0)
+    p, hist = og.mlp_train(lib, 2, 32, 0, tx, ty, p0, epochs=40, batch=512, lr=3e-3, seed=2)
+    L1, _ = og.mlp_grad(lib, 2, 32, 0, tx[:4096], ty[:4096], p)
+    assert L1 < 0.05 * L0, (L0, L1)
+    assert hist[-1] < hist[0]
+    # inference: bf16 weights, fp32 sums, against the FP64 forward with the
+    # same bf16-rounded weights
+    yt = torch.empty(N, dtype=torch.float32, device="cuda")
+    og.mlp_infer(lib, 2, 32, p, tx, yt)
+    pb = torch.from_numpy(p).to(torch.bfloat16).float().numpy()
+    yr, _ = np_mlp(pb, X.astype(np.float64), 2, 32)
+    assert np.abs(host(yt, np.float32) - yr).max() < 1e-3 * (np.abs(yr).max() + 1)
+
+
+def constant_policy(lib, bu: bool):
+    import opengraph_b200 as og
+    p = np.zeros(og.mlp_nparams(lib, 8, 64), np.float32)
+    p[-1] = 1.0 if bu else -1.0
+    return p
+
+
+@pytest.mark.parametrize("kind,kw", [("rmat", dict(scale=14, ef=16, seed=1)), ("grid", dict(side=80, p=0.01, seed=2)),
+                                     ("uniform", dict(n=40_000, m=200_000, seed=3))])
+def test_learned_switch_keeps_depths(torch_cuda, lib, oracle, graphs, kind, kw):
+    from opengraph_b200.learned import SWITCH, load_weights
+    torch = torch_cuda
+    s, d, _, V = graphs(kind, **kw)
+    g = oracle.build(s, d, V, 0)
+    dg = lib.device_graph()
+    dg.build(dev(torch, s), dev(torch, d), V, 0)
+    par = torch.empty(V, dtype=torch.int32, device="cuda")
+    dist = torch.empty(V, dtype=torch.int32, device="cuda")
+    policies = [constant_policy(lib, True), constant_policy(lib, False)]
+    trained = load_weights(lib, SWITCH)
+    if trained is not None:
+        policies.append(trained)
+    cand = np.nonzero(g["f_outdeg"] > 0)[0]
+    roots = [int(x) for x in np.random.default_rng(0).choice(cand, size=3, replace=False)]
+    try:
+        for pol in policies:
+            lib.check(lib.ogb_bfs_set_policy(pol.ctypes.data), "set policy")
+            for r in roots:
+                info = dg.bfs(r, par, dist, mode=3)
+                _, edist, est = oracle.bfs(g, r, 2)
+                assert np.array_equal(host(dist), edist)
+                assert info["reached"] == est["reached"]
+                p = host(par, np.int32)
+                assert p[r] == r
+                dirs = [L["direction"] for L in dg.bfs_trace()]
+                if pol is policies[0]:
+                    assert all(x == 1 for x in dirs)
+                if pol is policies[1]:
+                    assert all(x == 0 for x in dirs)
+                feats = dg.bfs_features()
+                assert feats.shape == (len(dirs), 8) and np.all(np.isfinite(feats))
+    finally:
+        lib.ogb_bfs_set_policy(None)
+    with pytest.raises(Exception):      # mode 3 without a policy
+        dg.bfs(roots[0], par, dist, mode=3)
+    dg.close()
+
+
+def test_pr_warm_start(torch_cuda, lib):
+    import opengraph_b200 as og
+    from opengraph_b200.learned import PR_START, load_weights
+    torch = torch_cuda
+    pw = load_weights(lib, PR_START)
+    if pw is None:
+        pytest.skip("no trained warm-start weights")
+    s, d, _ = og.generate_rmat(16, 16, 900)          # a seed never used in training
+    V = 1 << 16
+    dg = lib.device_graph()
+    dg.build(dev(torch, s), dev(torch, d), V, 0)
+    ranks = torch.empty(V, dtype=torch.float32, device="cuda")
+    init = torch.empty(V, dtype=torch.float32, device="cuda")
+    dg.pagerank(ranks, mode=0, max_iterations=200, epsilon=0.0)
+    plain_errs, _ = dg.pagerank_history()
+    plain = host(ranks, np.float32).astype(np.float64)
+    dg.pagerank_warm_start(pw, init, hidden=PR_START[2])
+    assert np.all(np.isfinite(host(init, np.float32)))
+    dg.pagerank(ranks, mode=0, max_iterations=200, epsilon=0.0, init=init)
+    warm_errs, _ = dg.pagerank_history()
+    warm = host(ranks, np.float32).astype(np.float64)
+    it_plain = next(i for i, e in enumerate(plain_errs) if e < 1e-6)
+    it_warm = next(i for i, e in enumerate(warm_errs) if e < 1e-6)
+    assert it_warm < it_plain, (it_warm, it_plain)
+    assert np.abs(plain - warm).sum() < 1e-6
+    dg.close()
