@@ -5,7 +5,8 @@
  * Every function returns 0 on success or a nonzero status (see
  * OGB_ERR_*), with a message in ogb_last_error().  Pointers named d_* are
  * device pointers of the current CUDA device; `stream` is a cudaStream_t
- * (NULL = the library stream).  Nothing here exits the process.
+ * (NULL = the legacy default stream, so a call is ordered after the caller's
+ * default-stream copies into its inputs).  Nothing here exits the process.
  */
 #ifndef OGB200_DEVICE_H
 #define OGB200_DEVICE_H
@@ -86,8 +87,8 @@ const char *ogb_last_error(void);
 int ogb_weighted_layout(void);
 /* Silence the reference-style progress tables printed by ogb200.h calls. */
 void ogb_set_quiet(int quiet);
-/* Record CUDA events around every BFS step (per-level device times in the
- * level trace).  Off by default. */
+/* Accepted for compatibility and ignored: the persistent search always
+ * records per-level device times (globaltimer) in its level trace. */
 void ogb_set_level_timing(int on);
 
 int ogb_graph_create(ogb_graph **g);
@@ -132,14 +133,16 @@ int ogb_mlp_train(uint32_t in, uint32_t hidden, uint32_t loss, const float *d_X,
                   void *stream);
 int ogb_mlp_infer(uint32_t in, uint32_t hidden, const float *params, const float *d_X, uint32_t n, float *d_Y,
                   void *stream);
-/* The learned direction switch used by ogb_bfs mode 3: an 8 -> 64 -> 64 -> 1
- * network whose output > 0 picks a bottom-up step; NULL removes it.  Its
- * inputs, before every step, are scale-free (L(x) = log2(1 + x)):
- * L(frontier) - L(V), L(frontier out-edges) - L(unexplored out-edges),
- * L(frontier out-edges) - L(frontier), 1 when a bottom-up step would walk
- * the unvisited list (else all vertices), visited fraction,
- * L(frontier) - L(previous frontier), L(unvisited) - L(V),
- * L(unexplored out-edges) - L(E). */
+/* The learned direction switch used by ogb_bfs mode 3.  params holds the
+ * 8 -> 64 -> 64 -> 1 network in the ogb_mlp packing (4801 floats) followed by
+ * a linear prior: 8 coefficients, a bias and a bound B (4811 floats in all).
+ * A step runs bottom-up when  prior . x + bias + clamp(network(x), -B, B) > 0,
+ * so the network is a bounded correction of the prior; NULL removes it.  The
+ * inputs x, before every step (L(x) = log2(1 + x)): L(frontier vertices),
+ * L(frontier out-edges), L(unexplored out-edges), L(bottom-up candidates:
+ * the unvisited list when one exists, else V), L(V), L(frontier) -
+ * L(previous frontier), visited fraction, 1 when a bottom-up step would
+ * walk the unvisited list (else 0). */
 int ogb_bfs_set_policy(const float *params);
 /* Those inputs for every step of the last ogb_bfs on g (count x 8 floats). */
 int ogb_bfs_features(ogb_graph *g, float *features, uint32_t max_levels, uint32_t *count);

@@ -325,7 +325,7 @@ def mlp_grad(lib, n_in, hidden, loss, X, T, params, stream=None):
     g = np.zeros_like(params)
     l = C.c_float()
     lib.check(lib.ogb_mlp_grad(n_in, hidden, loss, _ptr(X), _ptr(T), int(T.numel()), params.ctypes.data, g.ctypes.data,
-                               C.byref(l), stream), "ogb_mlp_grad")
+                               C.byref(l), _stream(stream)), "ogb_mlp_grad")
     return l.value, g
 
 
@@ -333,13 +333,13 @@ def mlp_train(lib, n_in, hidden, loss, X, T, params, epochs=10, batch=4096, lr=1
     p = np.ascontiguousarray(params.astype(np.float32).copy())
     hist = np.zeros(max(epochs, 1), np.float32)
     lib.check(lib.ogb_mlp_train(n_in, hidden, loss, _ptr(X), _ptr(T), int(T.numel()), epochs, batch, float(lr), seed,
-                                p.ctypes.data, hist.ctypes.data, stream), "ogb_mlp_train")
+                                p.ctypes.data, hist.ctypes.data, _stream(stream)), "ogb_mlp_train")
     return p, hist[:epochs]
 
 
 def mlp_infer(lib, n_in, hidden, params, X, Y, stream=None):
     p = np.ascontiguousarray(np.asarray(params, np.float32))
-    lib.check(lib.ogb_mlp_infer(n_in, hidden, p.ctypes.data, _ptr(X), int(Y.numel()), _ptr(Y), stream),
+    lib.check(lib.ogb_mlp_infer(n_in, hidden, p.ctypes.data, _ptr(X), int(Y.numel()), _ptr(Y), _stream(stream)),
               "ogb_mlp_infer")
 
 
@@ -404,6 +404,20 @@ def _ptr(t) -> int | None:
     return int(t.data_ptr())
 
 
+_CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the legacy default stream
+
+
+def _stream(stream) -> int:
+    """The stream a call runs on: the caller's, else torch's current stream
+    (so the call is ordered after the torch work that filled its inputs; the
+    legacy default stream is passed as cudaStreamLegacy)."""
+    if stream is not None:
+        return int(stream)
+    import torch
+    h = int(torch.cuda.current_stream().cuda_stream)
+    return h if h else _CUDA_STREAM_LEGACY
+
+
 class _CudaArray:
     """Zero-copy __cuda_array_interface__ view of library-owned device memory."""
 
@@ -450,14 +464,14 @@ class GraphBatch:
         r = np.ascontiguousarray(np.asarray(roots, dtype=np.uint32))
         info = BatchBfsInfo()
         self.lib.check(self.lib.ogb_batch_bfs(self.handle, r.ctypes.data_as(u32p), _ptr(parents), _ptr(distances),
-                                              C.byref(info), stream), "ogb_batch_bfs")
+                                              C.byref(info), _stream(stream)), "ogb_batch_bfs")
         return info_dict(info)
 
     def pagerank(self, ranks, max_iterations: int = 100, epsilon: float = 1e-4, stream=None):
         per = (BatchPrGraph * self.n)()
         info = BatchPrInfo()
         self.lib.check(self.lib.ogb_batch_pagerank(self.handle, int(max_iterations), float(epsilon), _ptr(ranks),
-                                                   per, C.byref(info), stream), "ogb_batch_pagerank")
+                                                   per, C.byref(info), _stream(stream)), "ogb_batch_pagerank")
         return info_dict(info), [info_dict(per[i]) for i in range(self.n)]
 
     def autotune(self) -> dict:
@@ -498,7 +512,7 @@ class DeviceGraph:
     def build(self, src, dst, num_vertices: int, sort_type: int = 0, weight=None, stream=None) -> None:
         """Sort + CSR build from device tensors (uint32 viewed as int32 is fine)."""
         self.lib.check(self.lib.ogb_graph_build(self.handle, _ptr(src), _ptr(dst), _ptr(weight), int(src.numel()),
-                                                int(num_vertices), int(sort_type), stream), "ogb_graph_build")
+                                                int(num_vertices), int(sort_type), _stream(stream)), "ogb_graph_build")
 
     def view(self, inverse: bool = False) -> CsrArrays:
         """Zero-copy torch views of one direction's device arrays."""
@@ -517,7 +531,7 @@ class DeviceGraph:
     def bfs(self, root: int, parents, distances, mode: int = 2, stream=None) -> dict:
         info = BfsInfo()
         self.lib.check(self.lib.ogb_bfs(self.handle, int(root), int(mode), _ptr(parents), _ptr(distances),
-                                        C.byref(info), stream), "ogb_bfs")
+                                        C.byref(info), _stream(stream)), "ogb_bfs")
         return info_dict(info)
 
     def msbfs(self, roots, depths, stream=None) -> dict:
@@ -525,7 +539,7 @@ class DeviceGraph:
         of V * 64 entries (row v = v's depth in each lane, 0xFFFF unreached)."""
         arr = (u32 * len(roots))(*[int(r) for r in roots])
         info = MsBfsInfo()
-        self.lib.check(self.lib.ogb_msbfs(self.handle, arr, len(roots), _ptr(depths), C.byref(info), stream),
+        self.lib.check(self.lib.ogb_msbfs(self.handle, arr, len(roots), _ptr(depths), C.byref(info), _stream(stream)),
                        "ogb_msbfs")
         return info_dict(info)
 
@@ -535,12 +549,12 @@ class DeviceGraph:
         arr = (u32 * len(seeds))(*[int(x) for x in seeds])
         info = PprBatchInfo()
         self.lib.check(self.lib.ogb_ppr(self.handle, arr, len(seeds), int(max_iterations), float(epsilon),
-                                        _ptr(ranks), C.byref(info), stream), "ogb_ppr")
+                                        _ptr(ranks), C.byref(info), _stream(stream)), "ogb_ppr")
         d = info_dict(info)
         d["err_last"] = list(info.err_last)[:len(seeds)]
         return d
 
-    def bfs_features(self, max_levels: int = 512) -> np.ndarray:
+    def bfs_features(self, max_levels: int = 16384) -> np.ndarray:
         """The learned switch's inputs before every step of the last bfs."""
         out = np.zeros((max_levels, 8), np.float32)
         n = u32()
@@ -550,10 +564,10 @@ class DeviceGraph:
 
     def pagerank_warm_start(self, params, init, hidden: int = 32, stream=None) -> None:
         p = np.ascontiguousarray(np.asarray(params, np.float32))
-        self.lib.check(self.lib.ogb_pagerank_warm_start(self.handle, hidden, p.ctypes.data, _ptr(init), stream),
+        self.lib.check(self.lib.ogb_pagerank_warm_start(self.handle, hidden, p.ctypes.data, _ptr(init), _stream(stream)),
                        "ogb_pagerank_warm_start")
 
-    def bfs_trace(self, max_levels: int = 512) -> list[dict]:
+    def bfs_trace(self, max_levels: int = 16384) -> list[dict]:
         arr = (BfsLevel * max_levels)()
         n = u32()
         self.lib.check(self.lib.ogb_bfs_trace(self.handle, arr, max_levels, C.byref(n)), "ogb_bfs_trace")
@@ -563,7 +577,7 @@ class DeviceGraph:
                  stream=None) -> dict:
         info = PrInfo()
         self.lib.check(self.lib.ogb_pagerank(self.handle, int(mode), int(max_iterations), float(epsilon),
-                                             _ptr(ranks), _ptr(init), C.byref(info), stream), "ogb_pagerank")
+                                             _ptr(ranks), _ptr(init), C.byref(info), _stream(stream)), "ogb_pagerank")
         return info_dict(info)
 
     def pagerank_history(self, max_entries: int = 1024) -> tuple[np.ndarray, np.ndarray]:

@@ -1159,7 +1159,7 @@ static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, 
   st->time_total = t_trav;
   if (!quiet()) {
     say("| %s %-12u | %-15u | %-15f | \n", mode == BFS_PULL ? "BU" : "TD", 0u, 1u, 0.0);
-    for (int i = 0; i < r.nlevels; i++) {
+    for (size_t i = 0; i < r.levels.size(); i++) {
       const BfsLevel& L = r.levels[i];
       say("| %s %-12u | %-15u | %-15f | \n", L.direction ? "BU" : "TD", (uint32_t)(i + 1), L.discovered,
           L.ms / 1000.0);
@@ -1354,8 +1354,7 @@ extern "C" uint32_t generateRandomRootGraphCSR(mt19937state* mt, struct GraphCSR
 extern "C" const char* ogb_last_error(void) { return ogb::last_error(); }
 extern "C" int ogb_weighted_layout(void) { return OGB200_WEIGHTED; }
 extern "C" void ogb_set_quiet(int q) { g_quiet = q ? 1 : 0; }
-static bool g_level_timing = false;
-extern "C" void ogb_set_level_timing(int on) { g_level_timing = on != 0; }
+extern "C" void ogb_set_level_timing(int on) { (void)on; }
 
 extern "C" int ogb_graph_create(ogb_graph** g) {
   if (!g) return fail(ERR_ARG, "null");
@@ -1365,7 +1364,9 @@ extern "C" int ogb_graph_create(ogb_graph** g) {
 
 extern "C" void ogb_graph_destroy(ogb_graph* g) { delete g; }
 
-static cudaStream_t as_stream(void* s) { return s ? (cudaStream_t)s : lib_stream(); }
+// A null stream argument is the legacy default stream (as in the CUDA
+// libraries), so the call waits for the caller's default-stream work.
+static cudaStream_t as_stream(void* s) { return s ? (cudaStream_t)s : cudaStreamLegacy; }
 
 extern "C" int ogb_graph_build(ogb_graph* g, const uint32_t* d_src, const uint32_t* d_dst, const float* d_w,
                                uint32_t E, uint32_t V, uint32_t sort_type, void* stream) {
@@ -1413,8 +1414,7 @@ extern "C" int ogb_bfs(ogb_graph* g, uint32_t root, uint32_t mode, int32_t* d_pa
   if (!g || !d_parents || !d_distances) return fail(ERR_ARG, "null");
   if (mode > 4) return fail(ERR_ARG, "bfs mode %u", mode);
   static thread_local BfsResult r;
-  OGB_TRY(bfs_run(g->g, root, mode, d_parents, d_distances, &r, g_level_timing, false, as_stream(stream)));
-  g->g.bfs_last_levels = r.nlevels;
+  OGB_TRY(bfs_run(g->g, root, mode, d_parents, d_distances, &r, true, false, as_stream(stream)));
   if (info) {
     info->iteration = r.iteration;
     info->processed_nodes = r.processed_nodes;
@@ -1428,15 +1428,15 @@ extern "C" int ogb_bfs(ogb_graph* g, uint32_t root, uint32_t mode, int32_t* d_pa
     info->launches = r.launches;
     info->pad = 0;
   }
-  memcpy(g->g.bfs_trace, r.levels, sizeof(r.levels[0]) * std::min(r.nlevels, 512));
-  memcpy(g->g.bfs_feat, r.feat, sizeof(r.feat[0]) * std::min(r.nlevels, 512));
+  g->g.bfs_trace.swap(r.levels);
+  g->g.bfs_feat.swap(r.feat);
   return OK;
 }
 
 extern "C" int ogb_bfs_features(ogb_graph* g, float* features, uint32_t max_levels, uint32_t* count) {
   if (!g || !features || !count) return fail(ERR_ARG, "ogb_bfs_features: null argument");
-  const uint32_t n = std::min<uint32_t>(max_levels, (uint32_t)g->g.bfs_last_levels);
-  memcpy(features, g->g.bfs_feat, (size_t)n * 8 * sizeof(float));
+  const uint32_t n = std::min<uint32_t>(max_levels, (uint32_t)g->g.bfs_trace.size());
+  memcpy(features, g->g.bfs_feat.data(), (size_t)n * 8 * sizeof(float));
   *count = n;
   return OK;
 }
@@ -1594,7 +1594,7 @@ extern "C" int ogb_batch_autotune(ogb_batch* b, ogb_tune_info* info) {
 
 extern "C" int ogb_bfs_trace(ogb_graph* g, ogb_bfs_level* levels, uint32_t max_levels, uint32_t* count) {
   if (!g) return fail(ERR_ARG, "null");
-  const uint32_t n = std::min<uint32_t>(max_levels, (uint32_t)g->g.bfs_last_levels);
+  const uint32_t n = std::min<uint32_t>(max_levels, (uint32_t)g->g.bfs_trace.size());
   for (uint32_t i = 0; i < n; i++) {
     const BfsLevel& L = g->g.bfs_trace[i];
     levels[i].direction = L.direction;

@@ -65,6 +65,7 @@
 #include "graph.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 namespace ogb {
@@ -75,7 +76,7 @@ constexpr int kScanTile = kScanT * kScanI;
 constexpr int kExpT = 256;             // threads of the expand phase
 constexpr uint32_t kExpTile = 1024;    // edges per expand tile
 constexpr int kSearchT = 256;          // threads per CTA of the persistent search
-constexpr int kMaxTrace = 512;
+constexpr int kMaxTrace = 16384;    // steps whose trace and switch inputs are kept
 constexpr uint32_t kAlpha = 15, kBeta = 18;
 constexpr uint32_t kBuRound = 1024;    // vertices per CTA round of a bottom-up step
 
@@ -142,10 +143,12 @@ struct BfsBufs {
   uint32_t* tile_i0;
   unsigned long long* status;
   uint32_t V, words, E, pad;
-  const __nv_bfloat16* policy;  // learned switch weights (8 -> 64 -> 64 -> 1), or null
+  const __nv_bfloat16* policy;  // learned switch network (8 -> 64 -> 64 -> 1, bf16), or null
+  const float* policy_tail;     // its linear prior (8 coefficients, bias) and correction bound
 };
 
 const __nv_bfloat16* bfs_policy_weights();
+const float* bfs_policy_tail();
 
 struct BfsWork {
   uint32_t V = 0, E = 0;
@@ -221,15 +224,24 @@ static BfsBufs make_bufs(DevGraph& g, BfsWork* w) {
   b.E = g.E;
   b.pad = 0;
   b.policy = bfs_policy_weights();
+  b.policy_tail = bfs_policy_tail();
   return b;
 }
 
 // ------------------------------------------------------------ learned switch
 
-// bf16 weights of the installed direction policy (null: none), per process.
+// The installed direction policy (none: null), per process: the network in
+// bf16 (W2 transposed), then, 16-byte aligned, the fp32 tail (prior
+// coefficients, prior bias, correction bound).
+constexpr int kPolMlpN = 64 * 8 + 64 + 64 * 64 + 64 + 64 + 1;  // the library's MLP packing
+constexpr int kPolTail = 8 + 1 + 1;
+constexpr size_t kPolTailOff = ((size_t)kPolMlpN * 2 + 15) / 16 * 16;
 static DevBuf g_policy;
 static bool g_policy_set = false;
 const __nv_bfloat16* bfs_policy_weights() { return g_policy_set ? g_policy.as<__nv_bfloat16>() : nullptr; }
+const float* bfs_policy_tail() {
+  return g_policy_set ? reinterpret_cast<const float*>(g_policy.as<char>() + kPolTailOff) : nullptr;
+}
 
 __global__ void bfsk_policy_to_bf16(const float* __restrict__ p, int n, __nv_bfloat16* __restrict__ q) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) q[i] = __float2bfloat16_rn(p[i]);
@@ -241,15 +253,21 @@ int bfs_set_policy(const float* params_host) {
     return OK;
   }
   // the library's packing (W1, b1, W2[i][j], b2, w3, b3) with W2 transposed
-  constexpr int in = 8, h = 64, np = h * in + h + h * h + h + h + 1;
+  constexpr int in = 8, h = 64, np = kPolMlpN;
+  const float* tail = params_host + np;
+  for (int i = 0; i < kPolTail; i++)
+    if (!std::isfinite(tail[i])) return fail(ERR_ARG, "bfs_set_policy: prior entry %d is not finite", i);
+  if (tail[kPolTail - 1] < 0.f) return fail(ERR_ARG, "bfs_set_policy: negative correction bound");
   std::vector<float> p(params_host, params_host + np);
   const int w2 = h * in + h;
   for (int i = 0; i < h; i++)
     for (int j = 0; j < h; j++) p[w2 + j * h + i] = params_host[w2 + i * h + j];
   DevBuf tmp;
   OGB_TRY(tmp.alloc(np * 4));
-  OGB_TRY(g_policy.alloc(np * 2 + 16));
+  g_policy_set = false;
+  OGB_TRY(g_policy.alloc(kPolTailOff + kPolTail * 4));
   OGB_CUDA(cudaMemcpy(tmp.p, p.data(), np * 4, cudaMemcpyHostToDevice));
+  OGB_CUDA(cudaMemcpy(g_policy.as<char>() + kPolTailOff, tail, kPolTail * 4, cudaMemcpyHostToDevice));
   bfsk_policy_to_bf16<<<(np + 255) / 256, 256>>>(tmp.as<float>(), np, g_policy.as<__nv_bfloat16>());
   OGB_CUDA(cudaGetLastError());
   OGB_CUDA(cudaDeviceSynchronize());
@@ -875,21 +893,21 @@ __device__ void ctrl_level(BfsCtrl& c, BfsDevState* st, bool leader, uint32_t di
   if (c.iteration > c.max_steps) c.overflow = 1;
 }
 
-// The learned switch's inputs: scale-free ratios of the state before a step
-// (log2(1 + x) of the counts, differenced), so that a policy trained on one
-// graph size applies to others.
+// The learned switch's inputs, from the reference's switch state before a
+// step (nf, nf_prev, mf, mu, n: BFS.c:510-516) plus the bottom-up step's
+// candidate count; counts enter as L(x) = log2(1 + x).
 __device__ __forceinline__ void bfs_features(const BfsCtrl& c, uint32_t E, float* f) {
   const unsigned long long left = (unsigned long long)E > c.edges_visited ? (unsigned long long)E - c.edges_visited : 0ull;
-  const float lq = log2f(1.0f + (float)c.qcount), ln = log2f(1.0f + (float)c.n), le = log2f(1.0f + (float)E);
-  const float lfe = log2f(1.0f + (float)c.fedges), lleft = log2f(1.0f + (float)left);
-  f[0] = lq - ln;                                                    // frontier fraction
-  f[1] = lfe - lleft;                                                // frontier edges vs unexplored edges
-  f[2] = lfe - lq;                                                   // mean out-degree of the frontier
-  f[3] = c.ul_valid ? 1.0f : 0.0f;                                   // a bottom-up step would walk the unvisited list
-  f[4] = (float)c.processed / (float)max(c.n, 1u);                   // visited fraction
+  const uint32_t cand = c.ul_valid ? c.ul_size : c.n;
+  const float lq = log2f(1.0f + (float)c.qcount);
+  f[0] = lq;                                                         // frontier vertices
+  f[1] = log2f(1.0f + (float)c.fedges);                              // frontier out-edges
+  f[2] = log2f(1.0f + (float)left);                                  // unexplored out-edges
+  f[3] = log2f(1.0f + (float)cand);                                  // bottom-up candidates (list or all)
+  f[4] = log2f(1.0f + (float)c.n);                                   // vertices
   f[5] = lq - log2f(1.0f + (float)c.qcount_prev);                    // frontier growth
-  f[6] = log2f(1.0f + (float)(c.n - min(c.processed, c.n))) - ln;    // unvisited fraction
-  f[7] = lleft - le;                                                 // unexplored edge fraction
+  f[6] = (float)c.processed / (float)max(c.n, 1u);                   // visited fraction
+  f[7] = c.ul_valid ? 1.0f : 0.0f;                                   // a bottom-up step would walk the unvisited list
 }
 
 // Policy network layout on the device (bf16): W1[64][8], b1[64], W2T[64][64]
@@ -897,6 +915,7 @@ __device__ __forceinline__ void bfs_features(const BfsCtrl& c, uint32_t E, float
 constexpr int kPolIn = kFeat, kPolH = 64;
 constexpr int kPolW1 = 0, kPolB1 = kPolH * kPolIn, kPolW2T = kPolB1 + kPolH, kPolB2 = kPolW2T + kPolH * kPolH,
               kPolW3 = kPolB2 + kPolH, kPolB3 = kPolW3 + kPolH, kPolN = kPolB3 + 1;
+static_assert(kPolN == kPolMlpN, "policy packing");
 
 // Policy output of a warp (bf16 weights in shared memory, fp32 sums): lane
 // l owns hidden units l and l + 32; every lane returns the output.
@@ -1054,10 +1073,13 @@ __global__ void __launch_bounds__(kSearchT, 5) bfsk_search(BfsBufs b, BfsDevStat
   __shared__ uint32_t s_act, s_ok;
   __shared__ unsigned long long s_t0;
   __shared__ __nv_bfloat16 s_pol[kPolN];
+  __shared__ float s_tail[kPolTail];
   const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
   if (threadIdx.x == 0) S = st->c;
-  if (b.policy)
+  if (b.policy) {
     for (int i = threadIdx.x; i < kPolN; i += blockDim.x) s_pol[i] = b.policy[i];
+    if (threadIdx.x < kPolTail) s_tail[threadIdx.x] = b.policy_tail[threadIdx.x];
+  }
   __syncthreads();
   int32_t* parents = st->parents;
   uint32_t* distances = st->distances;
@@ -1068,7 +1090,17 @@ __global__ void __launch_bounds__(kSearchT, 5) bfsk_search(BfsBufs b, BfsDevStat
       float f[kFeat];
       bfs_features(S, b.E, f);
       bool bu = false;
-      if (S.mode == BFS_LEARNED) bu = policy_logit(s_pol, f, threadIdx.x) > 0.0f;
+      if (S.mode == BFS_LEARNED) {
+        // z = prior . f + bias + clamp(network(f), -bound, bound).  The
+        // network moves z by at most bound, so it is evaluated only when
+        // that can change the sign (warp-uniform: every lane has the same z).
+        const float bound = s_tail[kFeat + 1];
+        float z = s_tail[kFeat];
+#pragma unroll
+        for (int i = 0; i < kFeat; i++) z = fmaf(s_tail[i], f[i], z);
+        if (fabsf(z) <= bound) z += fminf(fmaxf(policy_logit(s_pol, f, threadIdx.x), -bound), bound);
+        bu = z > 0.0f;
+      }
       if (leader && S.nlevels < (uint32_t)kMaxTrace && !S.overflow)
         for (int i = 0; i < kFeat; i++) st->feat[S.nlevels][i] = f[i];
       if (threadIdx.x == 0) {
@@ -1281,13 +1313,12 @@ size_t bfs_pack_tmp_words(uint32_t V) { return bfs_pack_layout(V).tiles + 8 + sc
 // ------------------------------------------------------------ drivers ------
 
 int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_t* distances, BfsResult* res,
-            bool time_levels, bool bu_entry_nf_frontier, cudaStream_t s) {
-  return bfs_run_roots(g, &root, 1, mode, parents, distances, res, time_levels, bu_entry_nf_frontier, s);
+            bool want_trace, bool bu_entry_nf_frontier, cudaStream_t s) {
+  return bfs_run_roots(g, &root, 1, mode, parents, distances, res, want_trace, bu_entry_nf_frontier, s);
 }
 
 int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t mode, int32_t* parents,
-                  uint32_t* distances, BfsResult* res, bool time_levels, bool bu_entry_nf_frontier, cudaStream_t s) {
-  (void)time_levels;  // the search always records per-level device times
+                  uint32_t* distances, BfsResult* res, bool want_trace, bool bu_entry_nf_frontier, cudaStream_t s) {
   const uint32_t V = g.V;
   if (nroots == 0) return fail(ERR_ARG, "bfs: no root");
   for (uint32_t i = 0; i < nroots; i++)
@@ -1321,7 +1352,7 @@ int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t 
   OGB_CUDA(cudaMemsetAsync(&st->aux, 0, sizeof(BfsCtl), s));
   bfsk_reached<<<sm_count() * 8, 256, 0, s>>>(b, st);
   OGB_CUDA(cudaGetLastError());
-  OGB_CUDA(cudaMemcpyAsync(w->h_state, w->state.p, sizeof(BfsDevState), cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaMemcpyAsync(w->h_state, w->state.p, offsetof(BfsDevState, trace), cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaStreamSynchronize(s));
   float total_ms = 0.f;
   OGB_CUDA(cudaEventElapsedTime(&total_ms, w->ev_start, w->ev_stop));
@@ -1339,12 +1370,16 @@ int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t 
   r.reached_out_edges = h->aux.reached_edges;
   r.ms = total_ms;
   r.launches = 1;  // kernels in the timed region: the search (init runs before it)
-  r.nlevels = (int)std::min<uint32_t>(h->c.nlevels, kMaxTrace);
-  for (int i = 0; i < r.nlevels; i++) {
-    r.levels[i] = h->trace[i];
-    for (int k = 0; k < kFeat; k++) r.feat[i][k] = h->feat[i][k];
+  r.nlevels = (int)h->c.nlevels;
+  const uint32_t ntrace = std::min<uint32_t>(h->c.nlevels, kMaxTrace);
+  if (want_trace && ntrace) {
+    r.levels.resize(ntrace);
+    r.feat.resize((size_t)ntrace * kFeat);
+    OGB_CUDA(cudaMemcpyAsync(r.levels.data(), st->trace, sizeof(BfsLevel) * ntrace, cudaMemcpyDeviceToHost, s));
+    OGB_CUDA(cudaMemcpyAsync(r.feat.data(), st->feat, sizeof(float) * kFeat * ntrace, cudaMemcpyDeviceToHost, s));
+    OGB_CUDA(cudaStreamSynchronize(s));
   }
-  if (res) *res = r;
+  if (res) *res = std::move(r);
   return OK;
 }
 

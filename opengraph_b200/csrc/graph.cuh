@@ -4,6 +4,8 @@
 #include "common.cuh"
 #include "sort.cuh"
 
+#include <vector>
+
 namespace ogb {
 
 // One direction of a CSR on the device.  Field meaning follows the
@@ -57,9 +59,8 @@ struct DevGraph {
   MsWork* ms = nullptr;
   PprWork* ppr = nullptr;
   // traces of the last BFS / PageRank run through the device API
-  int bfs_last_levels = 0;
-  BfsLevel bfs_trace[512];
-  float bfs_feat[512][8];  // learned-switch inputs of the last BFS's steps
+  std::vector<BfsLevel> bfs_trace;  // the last BFS's steps (up to the trace capacity)
+  std::vector<float> bfs_feat;      // learned-switch inputs before each of those steps, 8 per step
   uint32_t pr_last_executed = 0;
   double pr_err_hist[1024];
   uint32_t pr_active_hist[1024];
@@ -105,9 +106,9 @@ struct BfsResult {
   uint32_t reached = 0;
   uint32_t launches = 0;  // kernels launched by the traversal
   double ms = 0.0;
-  int nlevels = 0;
-  BfsLevel levels[512];
-  float feat[512][8];  // the learned switch's inputs before every step
+  int nlevels = 0;                // steps taken
+  std::vector<BfsLevel> levels;   // per-step trace (when asked for; at most the trace capacity)
+  std::vector<float> feat;        // the learned switch's 8 inputs before each traced step
 };
 
 // Learned direction switch (mode BFS_LEARNED): fp32 parameters of the
@@ -123,14 +124,15 @@ struct BfsSwitchState {
 // Run one BFS from `root` on the device graph; parents/distances are device
 // arrays of V entries.  bu_entry_nf selects the nf value at the start of a
 // bottom-up phase: 0 as the array-queue DO-BFS (BFS.c:550-551), or the
-// frontier size as the bitmap DO-BFS.
+// frontier size as the bitmap DO-BFS.  want_trace: also copy the per-step
+// trace and switch inputs back into res.
 int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_t* distances,
-            BfsResult* res, bool time_levels, bool bu_entry_nf_frontier, cudaStream_t s);
+            BfsResult* res, bool want_trace, bool bu_entry_nf_frontier, cudaStream_t s);
 // The same from several roots at once (host array): on a disjoint union of
 // graphs with one root each, every vertex gets its depth from its own
 // graph's root.  The switch state covers the whole union.
 int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t mode, int32_t* parents,
-                  uint32_t* distances, BfsResult* res, bool time_levels, bool bu_entry_nf_frontier, cudaStream_t s);
+                  uint32_t* distances, BfsResult* res, bool want_trace, bool bu_entry_nf_frontier, cudaStream_t s);
 
 // ---- multi-source BFS (batch.cu) -------------------------------------------
 struct MsResult {

@@ -3,19 +3,31 @@ and a warm-start vector for PageRank, trained on the GPU by the library's
 own MLP kernels (ogb_mlp_train) on traces of the plain GPU runs, and used by
 hand-written inference kernels (bf16 weights, fp32 accumulation).
 
-  python -m opengraph_b200.learned train [dir] # writes opengraph_b200/weights/*.f32 (or dir)
-  python -m opengraph_b200.learned evaluate   # learned vs plain on held-out graphs
+  python -m opengraph_b200.learned train [dir]        # writes opengraph_b200/weights/*.f32 (or dir)
+  python -m opengraph_b200.learned collect s.npz      # only the training traces
+  python -m opengraph_b200.learned fit s.npz [dir]    # only the fit, from saved traces
+  python -m opengraph_b200.learned evaluate           # learned vs plain on held-out graphs
 
-Direction switch (8 -> 64 -> 64 -> 1, output > 0 = bottom-up step).  Every
-BFS level has the same frontier whatever the directions chosen before it
-(the search is level-synchronous), so a push-only and a pull-only search
-from one root give, level by level, the device time of a top-down and of a
-bottom-up step on the same frontier.  Training samples: the scale-free
-switch inputs the kernel records before each level (ogb_bfs_features), with
-target log2(top-down ms / bottom-up ms) (clipped to +-8): a squared-error
-fit of the time ratio, so the levels where the choice costs most weigh
-most.  The plain alpha/beta rule stays the default (mode 2); mode 3 uses
-the policy; depths are identical by construction.
+Direction switch (8 -> 64 -> 64 -> 1 network plus a linear prior; a step
+runs bottom-up when prior(x) + clamp(network(x), -B, B) > 0).  Every BFS
+level has the same frontier whatever the directions chosen before it (the
+search is level-synchronous), so a push-only and a pull-only search from one
+root give, level by level, the device time of a top-down and of a bottom-up
+step on the same frontier.  Training samples: the switch inputs the kernel
+records before each level (ogb_bfs_features), with target
+y = log2(top-down ms / bottom-up ms) (clipped to +-8).  The prior is a
+least-squares fit of y on L(frontier out-edges) (the reference rule's mf,
+BFS.c:520-560), L(bottom-up candidates) (V, or the unvisited list) and the
+list flag: a power-law model of the two steps' costs, top-down work growing
+with the frontier's edges and bottom-up work with its candidates.  The
+network is fitted (squared error) to the remaining residual, clipped to +-B,
+so far from the training states it can move the decision by at most B and
+the prior decides.  (A prior on more counts fits the training graphs
+slightly better but extrapolates worse: with L(unexplored out-edges) and
+L(V) in it, the tail of a 4096 x 4096 grid search looks like an RMAT tail,
+where bottom-up wins, while a bottom-up step there walks 16M vertices.)
+The plain alpha/beta rule stays the default (mode 2); mode 3 uses the
+policy; depths are identical by construction.
 
 PageRank warm start (2 -> 32 -> 32 -> 1): inputs log2(1 + in-degree),
 log2(1 + out-degree); target log2 of the vertex's unnormalized rank after
@@ -33,8 +45,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "weights")
-SWITCH = ("switch_mlp.f32", 8, 64)
-PR_START = ("pr_start_mlp.f32", 2, 32)
+# (file, inputs, hidden units, extra floats after the network)
+SWITCH = ("switch_mlp.f32", 8, 64, 10)   # + prior coefficients[8], prior bias, correction bound
+PR_START = ("pr_start_mlp.f32", 2, 32, 0)
+SWITCH_BOUND = 2.0                        # B: the network moves log2(td / bu) by at most 2
+PRIOR_INPUTS = (1, 3, 7)                  # L(frontier out-edges), L(bottom-up candidates), list flag
 
 
 def weights_path(spec) -> str:
@@ -48,8 +63,9 @@ def load_weights(lib, spec) -> np.ndarray | None:
     if not os.path.exists(p):
         return None
     w = np.fromfile(p, dtype=np.float32)
-    if len(w) != og.mlp_nparams(lib, spec[1], spec[2]):
-        raise ValueError(f"{p}: {len(w)} parameters, expected {og.mlp_nparams(lib, spec[1], spec[2])}")
+    want = og.mlp_nparams(lib, spec[1], spec[2]) + spec[3]
+    if len(w) != want:
+        raise ValueError(f"{p}: {len(w)} parameters, expected {want}")
     return w
 
 
@@ -70,9 +86,10 @@ def _roots(g, n, seed):
 def switch_samples(lib, g, V, roots):
     """(features, log2(td ms / bu ms)) per level: positive when the bottom-up
     step on that level's frontier was faster than the top-down step.  Two
-    samples per level: a bottom-up step over all vertices (feature 3 = 0,
-    measured by the dense pull probe, mode 4) and one over the unvisited
-    list (feature 3 = 1, the pull-only search's steps after its first)."""
+    samples per level: a bottom-up step over all vertices (inputs of the
+    push-only search, candidates = V; timed by the dense pull probe, mode 4)
+    and one over the unvisited list (inputs of the pull-only search, whose
+    steps after its first walk the list)."""
     import torch
     par = torch.empty(V, dtype=torch.int32, device="cuda")
     dist = torch.empty(V, dtype=torch.int32, device="cuda")
@@ -84,21 +101,18 @@ def switch_samples(lib, g, V, roots):
     for r in roots:
         g.bfs(r, par, dist, mode=1)            # push only
         td = [L["ms"] for L in g.bfs_trace()]
-        feat = g.bfs_features()
+        feat_push = g.bfs_features()
         g.bfs(r, par, dist, mode=4)            # pull, every step over all vertices
         dense = [L["ms"] for L in g.bfs_trace()]
         g.bfs(r, par, dist, mode=0)            # pull, unvisited list after the first step
         lst = [L["ms"] for L in g.bfs_trace()]
-        n = min(len(td), len(dense), len(feat))
-        f0 = feat[:n].copy()
-        f0[:, 3] = 0.0
-        X.append(f0)
+        feat_pull = g.bfs_features()
+        n = min(len(td), len(dense), len(feat_push))
+        X.append(feat_push[:n])
         Y.append(ratio(td[:n], dense[:n]).astype(np.float32))
-        m = min(len(td), len(lst), len(feat))
+        m = min(len(td), len(lst), len(feat_pull))
         if m > 1:
-            f1 = feat[1:m].copy()
-            f1[:, 3] = 1.0
-            X.append(f1)
+            X.append(feat_pull[1:m])
             Y.append(ratio(td[1:m], lst[1:m]).astype(np.float32))
     return np.concatenate(X), np.concatenate(Y)
 
@@ -118,9 +132,10 @@ def pr_samples(lib, g, V, n_samples, seed):
     return X, Y
 
 
-def train(scales=(18, 19, 20, 21, 22), seeds=(0, 1, 2, 3), roots_per_graph=8, out=WEIGHTS, log=print):
-    import torch
-
+def collect(scales=(18, 19, 20, 21, 22), seeds=tuple(range(32)), roots_per_graph=4, pr_per_graph=25_000, log=print):
+    """Training samples from plain GPU runs on RMAT graphs (edge factor 16,
+    generator seeds 100 + seed): switch (X, y) from every root's levels and
+    warm-start (X, y) from a vertex subset of every graph."""
     import opengraph_b200 as og
     lib = og.load(False)
     lib.quiet(True)
@@ -133,26 +148,67 @@ def train(scales=(18, 19, 20, 21, 22), seeds=(0, 1, 2, 3), roots_per_graph=8, ou
             x, y = switch_samples(lib, g, V, _roots(g, roots_per_graph, sd))
             Xs.append(x)
             Ys.append(y)
-            x, y = pr_samples(lib, g, V, 200_000, sd)
+            x, y = pr_samples(lib, g, V, pr_per_graph, sd)
             Xp.append(x)
             Yp.append(y)
             g.close()
-            log(f"traces: RMAT-{sc} seed {sd}")
+        log(f"traces: RMAT-{sc}, {len(seeds)} seeds")
+    return {"switch_X": np.concatenate(Xs), "switch_y": np.concatenate(Ys),
+            "pr_X": np.concatenate(Xp), "pr_y": np.concatenate(Yp)}
+
+
+def fit_prior(X, y):
+    """Least squares y ~ sum_i a_i * X[:, i] (i in PRIOR_INPUTS) + b; returns
+    the 10-float tail (coefficients[8], bias, bound)."""
+    cols = list(PRIOR_INPUTS)
+    A = np.concatenate([X[:, cols].astype(np.float64), np.ones((len(X), 1))], axis=1)
+    coef, *_ = np.linalg.lstsq(A, y.astype(np.float64), rcond=None)
+    tail = np.zeros(10, np.float32)
+    tail[cols] = coef[:-1]
+    tail[8] = coef[-1]
+    tail[9] = SWITCH_BOUND
+    return tail
+
+
+def prior_of(tail, X):
+    return X.astype(np.float64) @ tail[:8].astype(np.float64) + float(tail[8])
+
+
+def fit(samples, out=WEIGHTS, log=print):
+    """Train the networks whose samples are given (switch_X/switch_y,
+    pr_X/pr_y) on the GPU (ogb_mlp_train) and write their files."""
+    import torch
+
+    import opengraph_b200 as og
+    lib = og.load(False)
     os.makedirs(out, exist_ok=True)
     res = {}
-    for name, (X, Y), spec, loss, epochs, batch, lr in (
-            ("switch", (np.concatenate(Xs), np.concatenate(Ys)), SWITCH, 0, 600, 128, 1e-3),
-            ("pr_start", (np.concatenate(Xp), np.concatenate(Yp)), PR_START, 0, 30, 4096, 2e-3)):
+    jobs = []
+    if "switch_X" in samples:
+        Xs, ys = samples["switch_X"], samples["switch_y"]
+        tail = fit_prior(Xs, ys)
+        resid = np.clip(ys - prior_of(tail, Xs), -SWITCH_BOUND, SWITCH_BOUND).astype(np.float32)
+        jobs.append(("switch", (Xs, resid), SWITCH, 0, 600, 128, 1e-3))
+    if "pr_X" in samples:
+        jobs.append(("pr_start", (samples["pr_X"], samples["pr_y"]), PR_START, 0, 30, 4096, 2e-3))
+    for name, (X, Y), spec, loss, epochs, batch, lr in jobs:
         tx = torch.from_numpy(np.ascontiguousarray(X)).cuda()
         ty = torch.from_numpy(np.ascontiguousarray(Y)).cuda()
         p0 = og.mlp_init(lib, spec[1], spec[2], seed=7)
         p, hist = og.mlp_train(lib, spec[1], spec[2], loss, tx, ty, p0, epochs=epochs, batch=batch, lr=lr, seed=11)
-        p.astype(np.float32).tofile(os.path.join(out, spec[0]))
+        blob = np.concatenate([p.astype(np.float32), tail]) if name == "switch" else p.astype(np.float32)
+        blob.tofile(os.path.join(out, spec[0]))
         res[name] = {"samples": int(len(Y)), "loss_first": float(hist[0]), "loss_last": float(hist[-1])}
         if name == "switch":
-            res[name]["bottom_up_faster_fraction"] = float((Y > 0).mean())
+            res[name]["bottom_up_faster_fraction"] = float((ys > 0).mean())
+            res[name]["prior"] = {"coefficients": [float(x) for x in tail[:8]], "bias": float(tail[8]),
+                                  "residual_rms": float(np.sqrt(np.mean(resid.astype(np.float64) ** 2)))}
         log(f"{name}: {res[name]}")
     return res
+
+
+def train(out=WEIGHTS, log=print, **kw):
+    return fit(collect(log=log, **kw), out=out, log=log)
 
 
 def evaluate(log=print):
@@ -221,5 +277,10 @@ if __name__ == "__main__":
     cmd = sys.argv[1] if len(sys.argv) > 1 else "evaluate"
     if cmd == "train":
         print(json.dumps(train(out=sys.argv[2] if len(sys.argv) > 2 else WEIGHTS)))
+    elif cmd == "collect":        # collect samples.npz: the traces alone
+        np.savez_compressed(sys.argv[2], **collect())
+    elif cmd == "fit":            # fit samples.npz [dir]: the networks from saved traces
+        z = np.load(sys.argv[2])
+        print(json.dumps(fit({k: z[k] for k in z.files}, out=sys.argv[3] if len(sys.argv) > 3 else WEIGHTS)))
     else:
         print(json.dumps(evaluate()))

@@ -7,6 +7,8 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import opengraph_b200 as og
+
 pytestmark = pytest.mark.gpu
 
 
@@ -47,7 +49,7 @@ def test_sort_matches_oracle(torch_cuda, lib, oracle, graphs, kind, kw, sort_typ
     ow = torch.empty_like(tw) if w is not None else None
     lib.check(lib.ogb_sort_edges(ts.data_ptr(), td.data_ptr(), tw.data_ptr() if tw is not None else None, E,
                                  sort_type, os_.data_ptr(), od.data_ptr(), ow.data_ptr() if ow is not None else None,
-                                 None), "sort")
+                                 og._stream(None)), "sort")
     torch.cuda.synchronize()
     assert np.array_equal(host(os_), es)
     assert np.array_equal(host(od), ed)
@@ -93,7 +95,7 @@ def test_sort_edge_sizes(torch_cuda, lib, oracle):
                 ts, td = dev(torch, s), dev(torch, d)
                 os_, od = torch.empty_like(ts), torch.empty_like(td)
                 lib.check(lib.ogb_sort_edges(ts.data_ptr(), td.data_ptr(), None, E, sort_type, os_.data_ptr(),
-                                             od.data_ptr(), None, None), "sort")
+                                             od.data_ptr(), None, og._stream(None)), "sort")
                 assert np.array_equal(host(os_), es) and np.array_equal(host(od), ed), (E, hi, sort_type)
     # E = 0 is a no-op
     lib.check(lib.ogb_sort_edges(None, None, None, 0, 0, None, None, None, None), "sort0")

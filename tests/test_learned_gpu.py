@@ -90,11 +90,18 @@ def test_mlp_training_reduces_loss_and_bf16_inference(torch_cuda, lib):
     assert np.abs(host(yt, np.float32) - yr).max() < 1e-3 * (np.abs(yr).max() + 1)
 
 
-def constant_policy(lib, bu: bool):
+def switch_policy(lib, b3: float, bias: float, bound: float):
+    """A switch whose network outputs b3 everywhere, prior = bias alone."""
     import opengraph_b200 as og
-    p = np.zeros(og.mlp_nparams(lib, 8, 64), np.float32)
-    p[-1] = 1.0 if bu else -1.0
+    p = np.zeros(og.mlp_nparams(lib, 8, 64) + 10, np.float32)
+    p[-11] = b3
+    p[-2] = bias
+    p[-1] = bound
     return p
+
+
+def constant_policy(lib, bu: bool):
+    return switch_policy(lib, 0.0, 1.0 if bu else -1.0, 0.0)
 
 
 @pytest.mark.parametrize("kind,kw", [("rmat", dict(scale=14, ef=16, seed=1)), ("grid", dict(side=80, p=0.01, seed=2)),
@@ -135,6 +142,28 @@ def test_learned_switch_keeps_depths(torch_cuda, lib, oracle, graphs, kind, kw):
         lib.ogb_bfs_set_policy(None)
     with pytest.raises(Exception):      # mode 3 without a policy
         dg.bfs(roots[0], par, dist, mode=3)
+    dg.close()
+
+
+def test_switch_correction_is_bounded(torch_cuda, lib, graphs):
+    """The network's output is clamped to +-bound before it joins the prior:
+    a huge output cannot outvote the prior beyond the bound."""
+    torch = torch_cuda
+    s, d, _, V = graphs("rmat", scale=12, ef=16, seed=1)
+    dg = lib.device_graph()
+    dg.build(dev(torch, s), dev(torch, d), V, 0)
+    par = torch.empty(V, dtype=torch.int32, device="cuda")
+    dist = torch.empty(V, dtype=torch.int32, device="cuda")
+    root = int(np.argmax(host(dg.view(False).out_degree, np.int32)))
+    try:
+        for b3, bias, bound, want in ((100.0, -1.0, 0.5, 0), (100.0, -1.0, 2.0, 1), (-100.0, 1.0, 0.5, 1),
+                                      (-100.0, 1.0, 3.0, 0)):
+            pol = switch_policy(lib, b3, bias, bound)   # held: the call reads it
+            lib.check(lib.ogb_bfs_set_policy(pol.ctypes.data), "set policy")
+            dg.bfs(root, par, dist, mode=3)
+            assert all(L["direction"] == want for L in dg.bfs_trace()), (b3, bias, bound)
+    finally:
+        lib.ogb_bfs_set_policy(None)
     dg.close()
 
 
