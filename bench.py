@@ -240,6 +240,7 @@ def run_ours(args):
 
     if rank == 0 and not args.skip_stages:
         extra["batching"] = batching(lib, og, g, roots, V, E, dev, sum(step_ms) / len(step_ms), extra)
+        extra["learned"] = learned_vs_plain(lib, og, g, roots, V, dev, flush, par, dis)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.skip_cpu:
@@ -457,6 +458,64 @@ def batching(lib, og, g, roots, V, E, dev, sweep_ms, extra):
                          "pagerank_sequential_ms": round(seq_pr, 2),
                          "autotuned_bins": {"warp_thr": best[0], "cta_thr": best[1]},
                          "note": "sequential = the same graphs one by one through the single-graph API, wall clock"}
+    return out
+
+
+def learned_vs_plain(lib, og, g, roots, V, dev, flush, par, dis):
+    """The learned parts against the plain ones on the bench graph: the same
+    roots searched with the plain alpha/beta switch (mode 2) and the learned
+    switch (mode 3), L2 flushed before each search, depths compared; and
+    PageRank pull to the 1e-6 tolerance from the uniform start and from the
+    warm-start network (its kernel timed in).  Held-out graphs (RMAT-24, a
+    4096 x 4096 grid): python -m opengraph_b200.learned evaluate."""
+    import torch
+
+    from opengraph_b200 import learned
+    sw = learned.load_weights(lib, learned.SWITCH)
+    pw = learned.load_weights(lib, learned.PR_START)
+    if sw is None or pw is None:
+        return {"unavailable": "no trained weights in opengraph_b200/weights"}
+    lib.check(lib.ogb_bfs_set_policy(sw.ctypes.data), "ogb_bfs_set_policy")
+    out = {}
+    try:
+        res = {}
+        same = True
+        for mode, tag in ((2, "plain"), (3, "learned")):
+            ms = edges = 0.0
+            for i, r in enumerate(roots):
+                flush.zero_()
+                torch.cuda.synchronize()
+                info = g.bfs(r, par, dis, mode=mode)
+                ms += info["ms"]
+                edges += info["reached_out_edges"]
+                if i < 4:
+                    dcopy = dis.cpu().numpy().copy()
+                    if tag == "plain":
+                        res.setdefault("depths", []).append(dcopy)
+                    else:
+                        same = same and np.array_equal(dcopy, res["depths"][i])
+            res[tag] = {"gteps": round(edges / ms / 1e6, 2), "ms_per_search": round(ms / len(roots), 4)}
+        out["bfs"] = {"plain": res["plain"], "learned": res["learned"], "depths_identical_first_4_roots": same}
+        ranks = torch.empty(V, dtype=torch.float32, device=dev)
+        init = torch.empty(V, dtype=torch.float32, device=dev)
+        pr = {}
+        for tag in ("plain", "learned"):
+            for rep in range(2):   # the second run is reported
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ev0.record()
+                if tag == "learned":
+                    g.pagerank_warm_start(pw, init, hidden=learned.PR_START[2])
+                info = g.pagerank(ranks, mode=0, max_iterations=200, epsilon=1e-6,
+                                  init=init if tag == "learned" else None)
+                ev1.record()
+                torch.cuda.synchronize()
+            pr[tag] = {"iterations": info["iterations"], "ms_to_1e-6": round(ev0.elapsed_time(ev1), 3),
+                       "ranks": ranks.cpu().numpy().astype(np.float64)}
+        l1 = float(np.abs(pr["plain"].pop("ranks") - pr["learned"].pop("ranks")).sum())
+        pr["final_l1_between"] = l1
+        out["pagerank_to_1e-6"] = pr
+    finally:
+        lib.ogb_bfs_set_policy(None)
     return out
 
 

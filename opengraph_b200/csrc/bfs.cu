@@ -156,7 +156,7 @@ struct BfsWork {
   DevBuf offs, fstart, fdist, tile_i0, scan_status;
   BfsDevState* h_state = nullptr;   // pinned copy
   uint32_t epoch = 0;               // last scan epoch used
-  int search_grid = 0;
+  int search_grid = 0;          // CTAs of the search launch (co-resident)
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
   ~BfsWork() {
     if (h_state) cudaFreeHost(h_state);
@@ -374,6 +374,46 @@ __device__ __forceinline__ uint32_t scan_block_excl(uint32_t v, uint32_t* s_w, u
   return (warp ? s_w[warp - 1] : 0) + x - v;
 }
 
+// Per-CTA sums of two 64-bit values in one reduction (one pair of
+// barriers); the totals are valid in thread 0.  A step's 32-bit counts travel
+// packed two to a value (low | high << 32): each half sums to less than 2^32
+// in a CTA (at most V vertices or E edges), so no carry crosses halves.
+// s_red holds 2 * (warps per CTA) entries.
+__device__ __forceinline__ void block_sum2(unsigned long long& a, unsigned long long& b, unsigned long long* s_red) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  const uint32_t warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane_id() == 0) {
+    s_red[warp] = a;
+    s_red[nw + warp] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a = b = 0;
+    for (uint32_t i = 0; i < nw; i++) {
+      a += s_red[i];
+      b += s_red[nw + i];
+    }
+  }
+}
+
+// A top-down step's counters: mf and the discoveries, packed, and the
+// discoveries' out-edges.
+__device__ __forceinline__ void td_publish(BfsCtl* ctl, uint32_t mf, uint32_t found, unsigned long long fed,
+                                           unsigned long long* s_red) {
+  unsigned long long a = (unsigned long long)mf | ((unsigned long long)found << 32), b = fed;
+  block_sum2(a, b, s_red);
+  if (threadIdx.x == 0) {
+    if ((uint32_t)a) atomicAdd(&ctl->mf, (uint32_t)a);
+    if (a >> 32) atomicAdd(&ctl->qnext, (uint32_t)(a >> 32));
+    if (b) atomicAdd(&ctl->fedges, b);
+  }
+}
+
 // Look-back word: value (32 bits) | flag (bits 32-33: 1 aggregate, 2
 // inclusive) | epoch (bits 34-63).  A word of an older scan never matches.
 __device__ __forceinline__ unsigned long long lb_word(uint32_t epoch, uint32_t flag, uint32_t value) {
@@ -561,9 +601,7 @@ __device__ void td_expand_phase(const BfsBufs& b, const uint32_t* list, uint32_t
     ba_flush(sm.q_list, next_list, &ctl->lnext);
     if (all_out) ba_flush(sm.q_all, all_out, &ctl->all_count);
   }
-  block_add_total<uint32_t>(&ctl->mf, mf, reinterpret_cast<uint32_t*>(s_red));
-  block_add_total<uint32_t>(&ctl->qnext, found, reinterpret_cast<uint32_t*>(s_red));
-  block_add_total<unsigned long long>(&ctl->fedges, fed, s_red);
+  td_publish(ctl, mf, found, fed, s_red);
 }
 
 // A top-down step over a list of at most kExpTile entries: every CTA loads
@@ -610,9 +648,7 @@ __device__ void td_small_phase(const BfsBufs& b, const uint32_t* list, uint32_t*
     expand_edges<true>(b, e0, e1, n, parents, distances, dnext, bm_w, nullptr, sm, mf, found, fed);
     ba_flush(sm.q_list, next_list, &ctl->lnext);
   }
-  block_add_total<uint32_t>(&ctl->mf, mf, reinterpret_cast<uint32_t*>(s_red));
-  block_add_total<uint32_t>(&ctl->qnext, found, reinterpret_cast<uint32_t*>(s_red));
-  block_add_total<unsigned long long>(&ctl->fedges, fed, s_red);
+  td_publish(ctl, mf, found, fed, s_red);
 }
 
 // ------------------------------------------------------------ bottom-up ----
@@ -752,9 +788,16 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
     ba_flush(sm.q_ul, ul_next, &ctl->ul_size);
     ba_flush(sm.q_list, list_next, &ctl->lnext);
   }
-  block_add_total<uint32_t>(&ctl->nf, nf, reinterpret_cast<uint32_t*>(s_red));
-  block_add_total<unsigned long long>(&ctl->edges, (unsigned long long)edges, s_red);
-  block_add_total<unsigned long long>(&ctl->fedges, fed, s_red);
+  {
+    // nf and the edges examined, packed, and the discoveries' out-edges
+    unsigned long long a = (unsigned long long)nf | ((unsigned long long)edges << 32), c = fed;
+    block_sum2(a, c, s_red);
+    if (threadIdx.x == 0) {
+      if ((uint32_t)a) atomicAdd(&ctl->nf, (uint32_t)a);
+      if (a >> 32) atomicAdd(&ctl->edges, a >> 32);
+      if (c) atomicAdd(&ctl->fedges, c);
+    }
+  }
 }
 
 // ---- bottom-up of the host-state step (depth read from the parent) --------
@@ -916,6 +959,9 @@ constexpr int kPolIn = kFeat, kPolH = 64;
 constexpr int kPolW1 = 0, kPolB1 = kPolH * kPolIn, kPolW2T = kPolB1 + kPolH, kPolB2 = kPolW2T + kPolH * kPolH,
               kPolW3 = kPolB2 + kPolH, kPolB3 = kPolW3 + kPolH, kPolN = kPolB3 + 1;
 static_assert(kPolN == kPolMlpN, "policy packing");
+constexpr size_t kPolSmem = ((size_t)kPolN * 2 + 15) / 16 * 16;  // bytes staged (the tail starts there)
+static_assert(kPolSmem == kPolTailOff, "the staged network ends where the tail begins");
+static_assert(sizeof(BfsSmem) >= kPolSmem, "the phase scratch holds the policy network");
 
 // Policy output of a warp (bf16 weights in shared memory, fp32 sums): lane
 // l owns hidden units l and l + 32; every lane returns the output.
@@ -1067,48 +1113,67 @@ __global__ void bfsk_set_roots(BfsBufs b, BfsDevState* st, const uint32_t* __res
 // barriers earlier).  A top-down step is one phase when its list has at most
 // kExpTile entries, else two (scan, expand); a bottom-up step is one phase.
 __global__ void __launch_bounds__(kSearchT, 5) bfsk_search(BfsBufs b, BfsDevState* st) {
-  __shared__ BfsSmem sm;
+  __shared__ __align__(16) BfsSmem sm;
   __shared__ BfsCtrl S;
-  __shared__ unsigned long long s_red[kSearchT / 32];
+  __shared__ unsigned long long s_red[2 * kSearchT / 32];
   __shared__ uint32_t s_act, s_ok;
   __shared__ unsigned long long s_t0;
-  __shared__ __nv_bfloat16 s_pol[kPolN];
   __shared__ float s_tail[kPolTail];
+  __shared__ float s_z;
+  __shared__ uint32_t s_need;
   const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
   if (threadIdx.x == 0) S = st->c;
-  if (b.policy) {
-    for (int i = threadIdx.x; i < kPolN; i += blockDim.x) s_pol[i] = b.policy[i];
-    if (threadIdx.x < kPolTail) s_tail[threadIdx.x] = b.policy_tail[threadIdx.x];
-  }
+  if (b.policy && threadIdx.x < kPolTail) s_tail[threadIdx.x] = b.policy_tail[threadIdx.x];
   __syncthreads();
   int32_t* parents = st->parents;
   uint32_t* distances = st->distances;
   BfsCtl* ctl = st->ctl;
   uint32_t p = 0;
   for (;;) {
+    const bool learned = S.mode == BFS_LEARNED;
     if (threadIdx.x < 32) {
       float f[kFeat];
       bfs_features(S, b.E, f);
-      bool bu = false;
-      if (S.mode == BFS_LEARNED) {
-        // z = prior . f + bias + clamp(network(f), -bound, bound).  The
-        // network moves z by at most bound, so it is evaluated only when
-        // that can change the sign (warp-uniform: every lane has the same z).
-        const float bound = s_tail[kFeat + 1];
+      if (leader && S.nlevels < (uint32_t)kMaxTrace && !S.overflow)
+        for (int i = 0; i < kFeat; i++) st->feat[S.nlevels][i] = f[i];
+      if (learned) {
+        // z = prior . f + bias; the network adds at most +-bound, so it is
+        // needed only when that can change the sign
         float z = s_tail[kFeat];
 #pragma unroll
         for (int i = 0; i < kFeat; i++) z = fmaf(s_tail[i], f[i], z);
-        if (fabsf(z) <= bound) z += fminf(fmaxf(policy_logit(s_pol, f, threadIdx.x), -bound), bound);
-        bu = z > 0.0f;
-      }
-      if (leader && S.nlevels < (uint32_t)kMaxTrace && !S.overflow)
-        for (int i = 0; i < kFeat; i++) st->feat[S.nlevels][i] = f[i];
-      if (threadIdx.x == 0) {
-        s_act = ctrl_decide(S, bu);
+        if (threadIdx.x == 0) {
+          s_z = z;
+          s_need = fabsf(z) <= s_tail[kFeat + 1] ? 1u : 0u;
+        }
+      } else if (threadIdx.x == 0) {
+        s_act = ctrl_decide(S, false);
         s_t0 = global_ns();
       }
     }
     __syncthreads();
+    if (learned) {
+      if (s_need) {
+        // stage the network in the phase scratch (no phase is running
+        // between steps), then warp 0 evaluates it
+        const uint4* src = reinterpret_cast<const uint4*>(b.policy);
+        uint4* dst = reinterpret_cast<uint4*>(&sm);
+        for (uint32_t i = threadIdx.x; i < kPolSmem / 16; i += blockDim.x) dst[i] = __ldg(&src[i]);
+        __syncthreads();
+        if (threadIdx.x < 32) {
+          float f[kFeat];
+          bfs_features(S, b.E, f);
+          const float bound = s_tail[kFeat + 1];
+          const float y = policy_logit(reinterpret_cast<const __nv_bfloat16*>(&sm), f, threadIdx.x);
+          if (threadIdx.x == 0) s_z += fminf(fmaxf(y, -bound), bound);
+        }
+      }
+      if (threadIdx.x == 0) {
+        s_act = ctrl_decide(S, s_z > 0.0f);
+        s_t0 = global_ns();
+      }
+      __syncthreads();
+    }
     const uint32_t act = s_act;
     if (act == kActDone) break;
     const uint32_t dnext = S.depth + 1;
@@ -1173,7 +1238,7 @@ __global__ void __launch_bounds__(kExpT) bfsk_td_expand_host(BfsBufs b, BfsDevSt
                                                              int32_t* parents, uint32_t* distances,
                                                              uint32_t* all_out) {
   __shared__ TdSmem sm;
-  __shared__ unsigned long long s_red[kExpT / 32];
+  __shared__ unsigned long long s_red[2 * kExpT / 32];
   td_expand_phase<false>(b, b.list[0], b.list[1], n, st->aux.total_edges, parents, distances, 0, nullptr, all_out,
                          &st->aux, sm, s_red);
 }
@@ -1181,7 +1246,7 @@ __global__ void __launch_bounds__(kExpT) bfsk_td_expand_host(BfsBufs b, BfsDevSt
 __global__ void __launch_bounds__(kSearchT) bfsk_bu_host(BfsBufs b, BfsDevState* st, int32_t* parents,
                                                         uint32_t* distances) {
   __shared__ BuHostSmem sm;
-  __shared__ unsigned long long s_red[kSearchT / 32];
+  __shared__ unsigned long long s_red[2 * kSearchT / 32];
   bu_host_phase(b, b.bm[0], b.bm[1], b.ul[1], parents, distances, &st->aux, sm, s_red);
 }
 
@@ -1335,6 +1400,10 @@ int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t 
     OGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, bfsk_search, kSearchT, 0));
     if (nb < 1) return fail(ERR_CUDA, "bfs: search kernel does not fit on an SM");
     w->search_grid = nb * sm_count();
+  }
+  if (mode != BFS_LEARNED) {  // the network is read only by the learned switch
+    b.policy = nullptr;
+    b.policy_tail = nullptr;
   }
   bfsk_init<<<sm_count() * 8, 256, 0, s>>>(b, st, root, parents, distances, mode, bu_entry_nf_frontier ? 1u : 0u,
                                             g.E, w->epoch);
