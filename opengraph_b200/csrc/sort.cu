@@ -62,28 +62,20 @@ __device__ __forceinline__ uint32_t block_exclusive_scan_256(uint32_t v, uint32_
   return warp_excl + x - v;
 }
 
-// Shared-memory histogram increment.  When every active lane of the warp
-// has the same digit (a constant high digit, or a hub vertex) one atomic of
-// the warp's size replaces 32 conflicting ones.
-__device__ __forceinline__ void hist_add(uint32_t* h, uint32_t dig) {
-  const uint32_t am = __activemask();
-  if (__reduce_and_sync(am, dig) == __reduce_or_sync(am, dig)) {
-    if ((int)lane_id() == __ffs(am) - 1) atomicAdd(&h[dig], (uint32_t)__popc(am));
-  } else {
-    atomicAdd(&h[dig], 1u);
-  }
-}
-
 // Histograms of `ndig` 8-bit digits of keys[0, n) into hist[ndig][256] and
-// the OR of all keys into *or_out.
-__global__ void __launch_bounds__(256) digit_hist_kernel(const uint32_t* __restrict__ keys, uint64_t n,
-                                                         int ndig, uint32_t* __restrict__ hist,
-                                                         uint32_t* __restrict__ or_out) {
-  __shared__ uint32_t sh[4][256];
+// the OR of all keys into *or_out.  Each warp counts into its own copy of
+// the histograms in shared memory (conflicts only inside a warp's atomic),
+// and the copies are summed once at the end.
+constexpr int kHistThreads = 256, kHistWarps = kHistThreads / 32;
+__global__ void __launch_bounds__(kHistThreads) digit_hist_kernel(const uint32_t* __restrict__ keys, uint64_t n,
+                                                                  int ndig, uint32_t* __restrict__ hist,
+                                                                  uint32_t* __restrict__ or_out) {
+  __shared__ uint32_t sh[kHistWarps][4][256];
   __shared__ uint32_t s_or;
-  for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) (&sh[0][0])[i] = 0;
+  for (int i = threadIdx.x; i < kHistWarps * 4 * 256; i += blockDim.x) (&sh[0][0][0])[i] = 0;
   if (threadIdx.x == 0) s_or = 0;
   __syncthreads();
+  uint32_t(*h)[256] = sh[threadIdx.x >> 5];
   uint32_t acc_or = 0;
   const uint64_t nvec = n / 4;
   const uint4* kv = reinterpret_cast<const uint4*>(keys);
@@ -92,27 +84,29 @@ __global__ void __launch_bounds__(256) digit_hist_kernel(const uint32_t* __restr
   if (aligned) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nvec;
          i += (uint64_t)gridDim.x * blockDim.x) {
-      uint4 q = __ldg(kv + i);
-      uint32_t a[4] = {q.x, q.y, q.z, q.w};
+      const uint4 q = __ldg(kv + i);
+      const uint32_t a[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         acc_or |= a[j];
-        for (int d = 0; d < ndig; d++) hist_add(sh[d], (a[j] >> (8 * d)) & 0xFF);
+        for (int d = 0; d < ndig; d++) atomicAdd(&h[d][(a[j] >> (8 * d)) & 0xFF], 1u);
       }
     }
     start_scalar = nvec * 4;
   }
   for (uint64_t i = start_scalar + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t k = keys[i];
+    const uint32_t k = keys[i];
     acc_or |= k;
-    for (int d = 0; d < ndig; d++) hist_add(sh[d], (k >> (8 * d)) & 0xFF);
+    for (int d = 0; d < ndig; d++) atomicAdd(&h[d][(k >> (8 * d)) & 0xFF], 1u);
   }
   acc_or = __reduce_or_sync(0xffffffffu, acc_or);
   if ((threadIdx.x & 31) == 0) atomicOr(&s_or, acc_or);
   __syncthreads();
   for (int i = threadIdx.x; i < ndig * 256; i += blockDim.x) {
-    uint32_t c = (&sh[0][0])[i];
+    uint32_t c = 0;
+#pragma unroll
+    for (int w = 0; w < kHistWarps; w++) c += (&sh[w][0][0])[i];
     if (c) atomicAdd(&hist[i], c);
   }
   if (threadIdx.x == 0) atomicOr(or_out, s_or);
@@ -128,7 +122,7 @@ __global__ void __launch_bounds__(256) digit_scan_kernel(const uint32_t* __restr
 }
 
 template <bool HAS_P1>
-__global__ void __launch_bounds__(kSortThreads, 2)
+__global__ void __launch_bounds__(kSortThreads, 3)
 onesweep_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ p0in,
                 const uint32_t* __restrict__ p1in, uint32_t* __restrict__ kout,
                 uint32_t* __restrict__ p0out, uint32_t* __restrict__ p1out, uint32_t n,
@@ -217,7 +211,7 @@ onesweep_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ p
     }
     st_volatile_u64(my_status, kFlagInc | (unsigned long long)(excl + cnt));
   }
-  s_global_start[tid] = digit_base[tid] + excl;
+  s_global_start[tid] = digit_base[tid] + excl - s_local_start[tid];
   __syncthreads();
 
   // Stage the tile in digit order.
@@ -238,8 +232,7 @@ onesweep_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ p
 #pragma unroll 4
   for (uint32_t j = tid; j < valid; j += kSortThreads) {
     const uint32_t k = s_k[j];
-    const uint32_t d = (k >> shift) & 0xFFu;
-    const uint32_t o = s_global_start[d] + (j - s_local_start[d]);
+    const uint32_t o = s_global_start[(k >> shift) & 0xFFu] + j;
     kout[o] = k;
     p0out[o] = s_p0[j];
     if (HAS_P1) p1out[o] = s_p1[j];
