@@ -76,15 +76,35 @@ __global__ void __launch_bounds__(256) csr_boundary_kernel(const uint32_t* __res
                                                            uint32_t V, uint32_t* __restrict__ edges_idx,
                                                            uint32_t* __restrict__ run_end,
                                                            uint32_t* __restrict__ err) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E;
-       i += (uint64_t)gridDim.x * blockDim.x) {
+  // four consecutive keys per thread (one 16-byte load; keys come from
+  // cudaMalloc, so 16-byte aligned) plus the two neighbours of the group
+  const uint32_t nq = E / 4;
+  const uint4* kq = reinterpret_cast<const uint4*>(key);
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+    const uint4 v = __ldg(kq + q);
+    const uint32_t i0 = q * 4;
+    const uint32_t k[6] = {i0 ? __ldg(key + i0 - 1) : 0xFFFFFFFFu, v.x, v.y, v.z, v.w,
+                           i0 + 4 < E ? __ldg(key + i0 + 4) : 0xFFFFFFFFu};
+#pragma unroll
+    for (int j = 1; j <= 4; j++) {
+      const uint32_t s = k[j];
+      if (s >= V) {
+        atomicExch(err, (uint32_t)ERR_RANGE);
+        continue;
+      }
+      if (k[j - 1] != s) edges_idx[s] = i0 + j - 1;
+      if (k[j + 1] != s) run_end[s] = i0 + j;
+    }
+  }
+  // the last E % 4 keys
+  for (uint32_t i = nq * 4 + blockIdx.x * blockDim.x + threadIdx.x; i < E; i += gridDim.x * blockDim.x) {
     const uint32_t s = key[i];
     if (s >= V) {
       atomicExch(err, (uint32_t)ERR_RANGE);
       continue;
     }
-    if (i == 0 || key[i - 1] != s) edges_idx[s] = (uint32_t)i;
-    if (i + 1 == E || key[i + 1] != s) run_end[s] = (uint32_t)(i + 1);
+    if (i == 0 || key[i - 1] != s) edges_idx[s] = i;
+    if (i + 1 == E || key[i + 1] != s) run_end[s] = i + 1;
   }
 }
 
@@ -161,13 +181,18 @@ int graph_build(DevGraph& g, const uint32_t* in_src, const uint32_t* in_dst, con
   KV in{const_cast<uint32_t*>(in_src), const_cast<uint32_t*>(in_dst),
         reinterpret_cast<uint32_t*>(const_cast<float*>(in_w))};
   KV fwd{g.fwd.d_src(), g.fwd.d_dst(), weighted ? reinterpret_cast<uint32_t*>(g.fwd.d_w()) : nullptr};
-  if (E) OGB_TRY(lex ? sort_pairs_lex(in, fwd, E, g.sort_ws, s) : sort_pairs(in, fwd, E, g.sort_ws, s));
+  // ids are below V (a larger one fails the build in csr_map), so the sort
+  // needs only the bits of V - 1
+  uint32_t bits = 1;
+  while (bits < 32 && (V - 1) >> bits) bits++;
+  if (E) OGB_TRY(lex ? sort_pairs_lex(in, fwd, E, g.sort_ws, s, bits) : sort_pairs(in, fwd, E, g.sort_ws, s, bits));
   OGB_TRY(csr_map(g.fwd, g.inv, V, E, g.err.as<uint32_t>(), s));
 
   // inverse: the sorted forward list with src/dst swapped, sorted again
   KV inv_in{g.fwd.d_dst(), g.fwd.d_src(), fwd.v1};
   KV inv{g.inv.d_src(), g.inv.d_dst(), weighted ? reinterpret_cast<uint32_t*>(g.inv.d_w()) : nullptr};
-  if (E) OGB_TRY(lex ? sort_pairs_lex(inv_in, inv, E, g.sort_ws, s) : sort_pairs(inv_in, inv, E, g.sort_ws, s));
+  if (E)
+    OGB_TRY(lex ? sort_pairs_lex(inv_in, inv, E, g.sort_ws, s, bits) : sort_pairs(inv_in, inv, E, g.sort_ws, s, bits));
   OGB_TRY(csr_map(g.inv, g.fwd, V, E, g.err.as<uint32_t>(), s));
   return OK;
 }

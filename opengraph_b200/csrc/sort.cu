@@ -62,13 +62,39 @@ __device__ __forceinline__ uint32_t block_exclusive_scan_256(uint32_t v, uint32_
   return warp_excl + x - v;
 }
 
-// Histograms of `ndig` 8-bit digits of keys[0, n) into hist[ndig][256] and
-// the OR of all keys into *or_out.  Each warp counts into its own copy of
+// Histograms of `ndig` digits of keys[0, n) into hist[ndig][256] (digit d
+// = (key >> 8-aligned or narrower lay.shift[d]) & lay.mask[d]) and the OR of
+// all keys into *or_out.  Each warp counts into its own copy of
 // the histograms in shared memory (conflicts only inside a warp's atomic),
 // and the copies are summed once at the end.
+// The digits of one key: ndig groups of at most 8 bits from bit 0 up.
+struct DigitLayout {
+  int ndig;
+  uint32_t shift[4], mask[4];
+};
+
+// Digits for keys below 2^bits: ceil(bits / 8) groups of nearly equal
+// width (the lower ones one bit wider), so each pass's digit runs are as
+// long as the key width allows (22 bits: 8 + 7 + 7 instead of 8 + 8 + 6).
+static DigitLayout digit_layout(uint32_t bits) {
+  bits = bits < 1 ? 1 : (bits > 32 ? 32 : bits);
+  DigitLayout l;
+  l.ndig = (int)((bits + 7) / 8);
+  const uint32_t w = bits / l.ndig, extra = bits % l.ndig;
+  uint32_t sh = 0;
+  for (int d = 0; d < 4; d++) {
+    const uint32_t wd = d < l.ndig ? w + ((uint32_t)d < extra ? 1u : 0u) : 0u;
+    l.shift[d] = sh;
+    l.mask[d] = wd ? (wd >= 32 ? 0xFFFFFFFFu : (1u << wd) - 1u) : 0u;
+    sh += wd;
+  }
+  return l;
+}
+
 constexpr int kHistThreads = 256, kHistWarps = kHistThreads / 32;
 __global__ void __launch_bounds__(kHistThreads) digit_hist_kernel(const uint32_t* __restrict__ keys, uint64_t n,
-                                                                  int ndig, uint32_t* __restrict__ hist,
+                                                                  int ndig, DigitLayout lay,
+                                                                  uint32_t* __restrict__ hist,
                                                                   uint32_t* __restrict__ or_out) {
   __shared__ uint32_t sh[kHistWarps][4][256];
   __shared__ uint32_t s_or;
@@ -89,7 +115,9 @@ __global__ void __launch_bounds__(kHistThreads) digit_hist_kernel(const uint32_t
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         acc_or |= a[j];
-        for (int d = 0; d < ndig; d++) atomicAdd(&h[d][(a[j] >> (8 * d)) & 0xFF], 1u);
+#pragma unroll
+        for (int d = 0; d < 4; d++)
+          if (d < ndig) atomicAdd(&h[d][(a[j] >> lay.shift[d]) & lay.mask[d]], 1u);
       }
     }
     start_scalar = nvec * 4;
@@ -98,7 +126,9 @@ __global__ void __launch_bounds__(kHistThreads) digit_hist_kernel(const uint32_t
        i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t k = keys[i];
     acc_or |= k;
-    for (int d = 0; d < ndig; d++) atomicAdd(&h[d][(k >> (8 * d)) & 0xFF], 1u);
+#pragma unroll
+    for (int d = 0; d < 4; d++)
+      if (d < ndig) atomicAdd(&h[d][(k >> lay.shift[d]) & lay.mask[d]], 1u);
   }
   acc_or = __reduce_or_sync(0xffffffffu, acc_or);
   if ((threadIdx.x & 31) == 0) atomicOr(&s_or, acc_or);
@@ -126,7 +156,7 @@ __global__ void __launch_bounds__(kSortThreads, 3)
 onesweep_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ p0in,
                 const uint32_t* __restrict__ p1in, uint32_t* __restrict__ kout,
                 uint32_t* __restrict__ p0out, uint32_t* __restrict__ p1out, uint32_t n,
-                uint32_t shift, const uint32_t* __restrict__ digit_base,
+                uint32_t shift, uint32_t mask, const uint32_t* __restrict__ digit_base,
                 unsigned long long* __restrict__ status, uint32_t* __restrict__ tile_ctr,
                 uint32_t* __restrict__ err) {
   __shared__ uint32_t s_tile;
@@ -167,7 +197,7 @@ onesweep_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ p
 #pragma unroll
   for (int i = 0; i < kSortItems; i++) {
     const uint64_t idx = warp_base + (uint64_t)i * 32 + lane;
-    const uint32_t d = (idx < n) ? ((key[i] >> shift) & 0xFFu) : 256u;
+    const uint32_t d = (idx < n) ? ((key[i] >> shift) & mask) : 256u;
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     uint32_t before = (d < 256) ? wh[d] : 0u;
     __syncwarp();
@@ -185,14 +215,16 @@ onesweep_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ p
     s_whist[w][tid] = cnt;
     cnt += c;
   }
+  // digits above the mask never occur in this pass: no status, no look-back
+  const bool live = (uint32_t)tid <= mask;
   unsigned long long* my_status = status + (uint64_t)tile * 256 + tid;
-  st_volatile_u64(my_status, (tile == 0 ? kFlagInc : kFlagAgg) | cnt);
+  if (live) st_volatile_u64(my_status, (tile == 0 ? kFlagInc : kFlagAgg) | cnt);
   const uint32_t local_start = block_exclusive_scan_256(cnt, s_warp);
   s_local_start[tid] = local_start;
 
   // Decoupled look-back over earlier tiles for this digit.
   uint32_t excl = 0;
-  if (tile > 0) {
+  if (tile > 0 && live) {
     int64_t pred = (int64_t)tile - 1;
     uint32_t spins = 0;
     while (pred >= 0) {
@@ -219,7 +251,7 @@ onesweep_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ p
   for (int i = 0; i < kSortItems; i++) {
     const uint64_t idx = warp_base + (uint64_t)i * 32 + lane;
     if (idx < n) {
-      const uint32_t d = (key[i] >> shift) & 0xFFu;
+      const uint32_t d = (key[i] >> shift) & mask;
       const uint32_t p = s_local_start[d] + s_whist[warp][d] + pos[i];
       s_k[p] = key[i];
       s_p0[p] = p0[i];
@@ -232,7 +264,7 @@ onesweep_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ p
 #pragma unroll 4
   for (uint32_t j = tid; j < valid; j += kSortThreads) {
     const uint32_t k = s_k[j];
-    const uint32_t o = s_global_start[(k >> shift) & 0xFFu] + j;
+    const uint32_t o = s_global_start[(k >> shift) & mask] + j;
     kout[o] = k;
     p0out[o] = s_p0[j];
     if (HAS_P1) p1out[o] = s_p1[j];
@@ -253,7 +285,7 @@ PinnedCounts& pinned_counts() {
 
 struct PassPlan {
   int role;  // 0: key = primary (k), payloads (v0, v1); 1: key = secondary (v0), payloads (k, v1)
-  uint32_t shift;
+  uint32_t shift, mask;
   int hist_index;  // which 256-bucket histogram holds the digit counts
 };
 
@@ -270,7 +302,7 @@ int SortWorkspace::reserve(uint64_t n, bool weighted, int max_passes) {
   return OK;
 }
 
-static int sort_impl(const KV& in, const KV& out, uint64_t n, bool lex, SortWorkspace& ws,
+static int sort_impl(const KV& in, const KV& out, uint64_t n, bool lex, uint32_t key_bits, SortWorkspace& ws,
                      cudaStream_t stream) {
   if (n == 0) return OK;
   if (n > 0xFFFFFFFFull) return fail(ERR_ARG, "sort: %llu edges exceed the u32 edge count", (unsigned long long)n);
@@ -287,8 +319,10 @@ static int sort_impl(const KV& in, const KV& out, uint64_t n, bool lex, SortWork
 
   const int grid = sm_count() * 4;
   // hist[0..3]: primary key digits; hist[4..7]: secondary key digits (lex).
-  digit_hist_kernel<<<grid, 256, 0, stream>>>(in.k, n, 4, d_hist, d_ctr + kCtrOr0);
-  if (lex) digit_hist_kernel<<<grid, 256, 0, stream>>>(in.v0, n, 4, d_hist + 4 * 256, d_ctr + kCtrOr0 + 1);
+  const DigitLayout lay = digit_layout(key_bits);
+  digit_hist_kernel<<<grid, 256, 0, stream>>>(in.k, n, lay.ndig, lay, d_hist, d_ctr + kCtrOr0);
+  if (lex)
+    digit_hist_kernel<<<grid, 256, 0, stream>>>(in.v0, n, lay.ndig, lay, d_hist + 4 * 256, d_ctr + kCtrOr0 + 1);
   OGB_CUDA(cudaGetLastError());
   digit_scan_kernel<<<lex ? 8 : 4, 256, 0, stream>>>(d_hist, d_base);
   OGB_CUDA(cudaGetLastError());
@@ -301,12 +335,12 @@ static int sort_impl(const KV& in, const KV& out, uint64_t n, bool lex, SortWork
   // LSD order: secondary digits first (lex), then primary digits.
   std::vector<PassPlan> plan;
   auto add_passes = [&](int role, int hbase) {
-    for (int d = 0; d < 4; d++) {
+    for (int d = 0; d < lay.ndig; d++) {
       const uint32_t* h = pc.h + (hbase + d) * 256;
       bool trivial = false;
       for (int b = 0; b < 256; b++)
         if (h[b] == n) trivial = true;
-      if (!trivial) plan.push_back({role, (uint32_t)(8 * d), hbase + d});
+      if (!trivial) plan.push_back({role, lay.shift[d], lay.mask[d], hbase + d});
     }
   };
   if (lex) add_passes(1, 4);
@@ -341,11 +375,11 @@ static int sort_impl(const KV& in, const KV& out, uint64_t n, bool lex, SortWork
     unsigned long long* st = ws.status.as<unsigned long long>() + (uint64_t)i * tiles * 256;
     if (has_p1)
       onesweep_kernel<true><<<(unsigned)tiles, kSortThreads, dyn_smem, stream>>>(
-          kin, p0in, cur.v1, kout, p0out, dst.v1, (uint32_t)n, pp.shift, d_base + pp.hist_index * 256, st,
+          kin, p0in, cur.v1, kout, p0out, dst.v1, (uint32_t)n, pp.shift, pp.mask, d_base + pp.hist_index * 256, st,
           d_ctr + i, d_ctr + kCtrErr);
     else
       onesweep_kernel<false><<<(unsigned)tiles, kSortThreads, dyn_smem, stream>>>(
-          kin, p0in, nullptr, kout, p0out, nullptr, (uint32_t)n, pp.shift, d_base + pp.hist_index * 256, st,
+          kin, p0in, nullptr, kout, p0out, nullptr, (uint32_t)n, pp.shift, pp.mask, d_base + pp.hist_index * 256, st,
           d_ctr + i, d_ctr + kCtrErr);
     OGB_CUDA(cudaGetLastError());
     cur = dst;
@@ -353,12 +387,13 @@ static int sort_impl(const KV& in, const KV& out, uint64_t n, bool lex, SortWork
   return OK;
 }
 
-int sort_pairs(const KV& in, const KV& out, uint64_t n, SortWorkspace& ws, cudaStream_t stream) {
-  return sort_impl(in, out, n, false, ws, stream);
+int sort_pairs(const KV& in, const KV& out, uint64_t n, SortWorkspace& ws, cudaStream_t stream, uint32_t key_bits) {
+  return sort_impl(in, out, n, false, key_bits, ws, stream);
 }
 
-int sort_pairs_lex(const KV& in, const KV& out, uint64_t n, SortWorkspace& ws, cudaStream_t stream) {
-  return sort_impl(in, out, n, true, ws, stream);
+int sort_pairs_lex(const KV& in, const KV& out, uint64_t n, SortWorkspace& ws, cudaStream_t stream,
+                   uint32_t key_bits) {
+  return sort_impl(in, out, n, true, key_bits, ws, stream);
 }
 
 // Reads the error word of the last sorts on `stream` (synchronizes).

@@ -20,18 +20,18 @@ struct SortWorkspace {
   int reserve(uint64_t n, bool weighted, int max_passes);
 };
 
-// Stable sort of `in` by key into `out`, moving the payloads along.  The
-// digits are the 8-bit groups of the key starting at bit 0; digit groups in
-// which every key has the same value are skipped.  `in` is not modified
-// unless it aliases `out`.  Runs on `stream`; one small device->host read
-// (the digit histograms) happens inside.
-//
-// Two-phase variant for (src, dst) ordering: sort_pairs_2key sorts by the
-// secondary key first and then stably by the primary key.
-int sort_pairs(const KV& in, const KV& out, uint64_t n, SortWorkspace& ws, cudaStream_t stream);
+// Stable sort of `in` by key into `out`, moving the payloads along.  Every
+// key must be below 2^key_bits (32: any key); the digits are ceil(key_bits /
+// 8) groups of nearly equal width from bit 0 up, and digit groups in which
+// every key has the same value are skipped.  `in` is not modified unless it
+// aliases `out`.  Runs on `stream`; one small device->host read (the digit
+// histograms) happens inside.
+int sort_pairs(const KV& in, const KV& out, uint64_t n, SortWorkspace& ws, cudaStream_t stream,
+               uint32_t key_bits = 32);
 
 // Lexicographic (primary, secondary) stable sort: `in.k` is the primary key
-// and `in.v0` the secondary key; payload v1 follows.
-int sort_pairs_lex(const KV& in, const KV& out, uint64_t n, SortWorkspace& ws, cudaStream_t stream);
+// and `in.v0` the secondary key (both below 2^key_bits); payload v1 follows.
+int sort_pairs_lex(const KV& in, const KV& out, uint64_t n, SortWorkspace& ws, cudaStream_t stream,
+                   uint32_t key_bits = 32);
 
 }  // namespace ogb
