@@ -684,20 +684,28 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
   const uint32_t count = kDense ? b.V : ul_count;
   uint32_t nf = 0, edges = 0;
   unsigned long long fed = 0;
-  for (uint32_t rbase = blockIdx.x * kBuRound; rbase < count; rbase += gridDim.x * kBuRound) {
+  // each CTA takes one contiguous, equal range of candidates (a multiple of
+  // 32, so a dense step's ballot words never straddle two CTAs)
+  const uint32_t per = ((count + gridDim.x - 1) / gridDim.x + 31u) & ~31u;
+  const uint32_t lo = min(count, blockIdx.x * per), hi = min(count, lo + per);
+  for (uint32_t rbase = lo; rbase < hi; rbase += kBuRound) {
     uint32_t v[kBuV];
 #pragma unroll
     for (int k = 0; k < kBuV; k++) {
       const uint32_t idx = rbase + k * kSearchT + threadIdx.x;
-      v[k] = idx < count ? (kDense ? idx : ul_cur[idx]) : kInvalid;
+      v[k] = idx < hi ? (kDense ? idx : ul_cur[idx]) : kInvalid;
     }
+    // parent and in-row together (a visited candidate's row is not used)
     int32_t pv[kBuV];
-#pragma unroll
-    for (int k = 0; k < kBuV; k++) pv[k] = v[k] != kInvalid ? parents[v[k]] : 0;
     uint2 row[kBuV];
 #pragma unroll
+    for (int k = 0; k < kBuV; k++) {
+      pv[k] = v[k] != kInvalid ? parents[v[k]] : 0;
+      row[k] = v[k] != kInvalid ? __ldg(&b.rows_i[v[k]]) : make_uint2(0u, 0u);
+    }
+#pragma unroll
     for (int k = 0; k < kBuV; k++)
-      row[k] = (v[k] != kInvalid && pv[k] < 0) ? __ldg(&b.rows_i[v[k]]) : make_uint2(0u, 0u);
+      if (pv[k] >= 0) row[k] = make_uint2(0u, 0u);
     uint32_t u[kBuV][kFirst];
 #pragma unroll
     for (int k = 0; k < kBuV; k++)
@@ -746,7 +754,7 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
       if (kDense) {
         const uint32_t word = __ballot_sync(0xffffffffu, found);
         const uint32_t base = rbase + k * kSearchT + warp * 32;
-        if (lane == 0 && base < b.V) bm_next[base >> 5] = word;
+        if (lane == 0 && base < hi) bm_next[base >> 5] = word;
       }
     }
     __syncthreads();
@@ -785,8 +793,7 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
     }
     __syncthreads();
     if (threadIdx.x == 0) sm.nheavy = 0;
-    ba_flush(sm.q_ul, ul_next, &ctl->ul_size);
-    ba_flush(sm.q_list, list_next, &ctl->lnext);
+    ba_flush2(sm.q_ul, ul_next, &ctl->ul_size, sm.q_list, list_next, &ctl->lnext);
   }
   {
     // nf and the edges examined, packed, and the discoveries' out-edges
