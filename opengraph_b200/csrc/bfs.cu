@@ -282,20 +282,56 @@ struct ScanSmem {
   uint32_t tile, prefix;
 };
 // Top-down: the list entries of one edge tile (or the whole list of a small
-// step) and the step's appends.
+// step) and the step's appends.  The search keeps only what it uses (the
+// rest of the SM's shared memory is L1, which its gathers need); the
+// host-state step adds the entries' depths and a list of every discovery.
 struct TdSmem {
-  uint32_t off[kExpTile + 2], start[kExpTile + 2], v[kExpTile + 2], d[kExpTile + 2];
+  static constexpr bool kHost = false;
+  uint32_t off[kExpTile + 2], start[kExpTile + 2], v[kExpTile + 2];
   BlockAppend<kExpTile> q_list;
-  BlockAppend<kExpTile> q_all;
   uint32_t w[kExpT / 32];
 };
-// Bottom-up: a round's appends and its deferred long in-edge rows.
+struct TdSmemHost : TdSmem {
+  static constexpr bool kHost = true;
+  uint32_t d[kExpTile + 2];
+  BlockAppend<kExpTile> q_all;
+};
+// Bottom-up: a round's appends and its deferred long in-edge rows.  A round
+// appends each of its at most kBuRound candidates to at most one list, so
+// the new frontier list fills one buffer from the front and the unvisited
+// list from the back.
 struct BuSmem {
-  BlockAppend<kBuRound> q_ul;
-  BlockAppend<kBuRound> q_list;
+  uint32_t nlist, nul, base_list, base_ul;
+  uint32_t buf[kBuRound];
   uint32_t nheavy;
   uint32_t hv[kBuRound], hj[kBuRound], he[kBuRound];
 };
+__device__ __forceinline__ void bu_push_list(BuSmem& sm, uint32_t v) { sm.buf[warp_atomic_inc(&sm.nlist)] = v; }
+__device__ __forceinline__ void bu_push_ul(BuSmem& sm, uint32_t v) {
+  sm.buf[kBuRound - 1u - warp_atomic_inc(&sm.nul)] = v;
+}
+// Both lists out (offsets reserved together), then the buffer is empty.
+__device__ __forceinline__ void bu_flush(BuSmem& sm, uint32_t* list_out, uint32_t* list_count, uint32_t* ul_out,
+                                         uint32_t* ul_count) {
+  __syncthreads();
+  const uint32_t nl = sm.nlist, nu = sm.nul;
+  if (threadIdx.x == 0) {
+    uint32_t bl = 0, bu = 0;
+    if (nl) bl = atomicAdd(list_count, nl);
+    if (nu) bu = atomicAdd(ul_count, nu);
+    sm.base_list = bl;
+    sm.base_ul = bu;
+  }
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < nl; k += blockDim.x) list_out[sm.base_list + k] = sm.buf[k];
+  for (uint32_t k = threadIdx.x; k < nu; k += blockDim.x) ul_out[sm.base_ul + k] = sm.buf[kBuRound - 1u - k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    sm.nlist = 0;
+    sm.nul = 0;
+  }
+  __syncthreads();
+}
 union BfsSmem {
   ScanSmem scan;
   TdSmem td;
@@ -516,11 +552,12 @@ __device__ void td_scan_phase(const BfsBufs& b, const uint32_t* list, uint32_t n
 // thread takes four edges at once: neighbour ids, then their parents, then
 // the claiming CASes, each group issued back to back.  A claimed vertex gets
 // its depth, its bit in bm_w (when given) and, with out-edges, a list slot.
-template <bool kDepthKnown>
+template <bool kDepthKnown, class TS>
 __device__ __forceinline__ void expand_edges(const BfsBufs& b, uint32_t e0, uint32_t e1, uint32_t cnt,
                                              int32_t* parents, uint32_t* distances, uint32_t dnext, uint32_t* bm_w,
-                                             uint32_t* all_out, TdSmem& sm, uint32_t& mf, uint32_t& found,
+                                             uint32_t* all_out, TS& sm, uint32_t& mf, uint32_t& found,
                                              unsigned long long& fed) {
+  static_assert(kDepthKnown || TS::kHost, "entry depths live in the host-step shared memory");
   constexpr int K = kExpTile / kExpT;
   uint32_t u[K], src[K], dd[K];
   bool ok[K];
@@ -542,7 +579,7 @@ __device__ __forceinline__ void expand_edges(const BfsBufs& b, uint32_t e0, uint
       }
       u[k] = __ldg(&b.nbr_f[sm.start[lo] + (e - sm.off[lo])]) & 0x3FFFFFFFu;
       src[k] = sm.v[lo];
-      if (!kDepthKnown) dd[k] = sm.d[lo];
+      if constexpr (!kDepthKnown) dd[k] = sm.d[lo];
     }
   }
   int32_t p[K];
@@ -558,7 +595,9 @@ __device__ __forceinline__ void expand_edges(const BfsBufs& b, uint32_t e0, uint
       mf += (uint32_t)(-p[k]);
       found++;
       if (bm_w) atomicOr(&bm_w[u[k] >> 5], 1u << (u[k] & 31));
-      if (all_out) ba_push(sm.q_all, u[k]);
+      if constexpr (TS::kHost) {
+        if (all_out) ba_push(sm.q_all, u[k]);
+      }
       const uint32_t od = __ldg(&b.out_degree[u[k]]);
       fed += od;
       if (od) ba_push(sm.q_list, u[k]);
@@ -571,15 +610,15 @@ __device__ __forceinline__ void expand_edges(const BfsBufs& b, uint32_t e0, uint
 // staged in shared memory and each edge finds its entry by binary search
 // there.  A vertex is claimed by CAS on its parent; the winner appends it to
 // the next frontier.
-template <bool kDepthKnown>
+template <bool kDepthKnown, class TS>
 __device__ void td_expand_phase(const BfsBufs& b, const uint32_t* list, uint32_t* next_list, uint32_t n,
                                 uint32_t total, int32_t* parents, uint32_t* distances, uint32_t dnext,
-                                uint32_t* bm_w, uint32_t* all_out, BfsCtl* ctl, TdSmem& sm,
+                                uint32_t* bm_w, uint32_t* all_out, BfsCtl* ctl, TS& sm,
                                 unsigned long long* s_red) {
   const uint32_t ntiles = (total + kExpTile - 1) / kExpTile;
   if (blockIdx.x >= ntiles) return;
   ba_init(sm.q_list);
-  ba_init(sm.q_all);
+  if constexpr (TS::kHost) ba_init(sm.q_all);
   uint32_t mf = 0, found = 0;
   unsigned long long fed = 0;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -593,13 +632,15 @@ __device__ void td_expand_phase(const BfsBufs& b, const uint32_t* list, uint32_t
       sm.off[k] = b.offs[i0 + k];
       sm.start[k] = b.fstart[i0 + k];
       sm.v[k] = list[i0 + k];
-      if (!kDepthKnown) sm.d[k] = b.fdist[i0 + k];
+      if constexpr (!kDepthKnown) sm.d[k] = b.fdist[i0 + k];
     }
     __syncthreads();
     expand_edges<kDepthKnown>(b, e0, e1, cnt, parents, distances, dnext, bm_w, all_out, sm, mf, found, fed);
     // at most kExpTile discoveries per tile: flush every tile
     ba_flush(sm.q_list, next_list, &ctl->lnext);
-    if (all_out) ba_flush(sm.q_all, all_out, &ctl->all_count);
+    if constexpr (TS::kHost) {
+      if (all_out) ba_flush(sm.q_all, all_out, &ctl->all_count);
+    }
   }
   td_publish(ctl, mf, found, fed, s_red);
 }
@@ -675,8 +716,8 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
                               unsigned long long* s_red) {
   grid_clear(bm_clear, nullptr, b.words);
   if (threadIdx.x == 0) {
-    sm.q_ul.n = 0;
-    sm.q_list.n = 0;
+    sm.nlist = 0;
+    sm.nul = 0;
     sm.nheavy = 0;
   }
   __syncthreads();
@@ -739,7 +780,7 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
           if (!kDense) atomicOr(&bm_next[v[k] >> 5], 1u << (v[k] & 31));
           const uint32_t od = __ldg(&b.out_degree[v[k]]);
           fed += od;
-          if (od) ba_push(sm.q_list, v[k]);
+          if (od) bu_push_list(sm, v[k]);
         } else if (row[k].y > kFirst) {
           edges += kFirst;
           const uint32_t h = warp_atomic_inc(&sm.nheavy);
@@ -748,7 +789,7 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
           sm.he[h] = row[k].x + row[k].y;
         } else {
           edges += row[k].y;
-          ba_push(sm.q_ul, v[k]);
+          bu_push_ul(sm, v[k]);
         }
       }
       if (kDense) {
@@ -780,7 +821,7 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
             edges += j + first + 1 - j0;
             const uint32_t od = __ldg(&b.out_degree[hv]);
             fed += od;
-            if (od) ba_push(sm.q_list, hv);
+            if (od) bu_push_list(sm, hv);
           }
           hit_row = true;
           break;
@@ -788,12 +829,12 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
       }
       if (!hit_row && gl == 0) {
         edges += end - j0;
-        ba_push(sm.q_ul, hv);
+        bu_push_ul(sm, hv);
       }
     }
     __syncthreads();
     if (threadIdx.x == 0) sm.nheavy = 0;
-    ba_flush2(sm.q_ul, ul_next, &ctl->ul_size, sm.q_list, list_next, &ctl->lnext);
+    bu_flush(sm, list_next, &ctl->lnext, ul_next, &ctl->ul_size);
   }
   {
     // nf and the edges examined, packed, and the discoveries' out-edges
@@ -1202,7 +1243,7 @@ __global__ void __launch_bounds__(kSearchT, 5) bfsk_search(BfsBufs b, BfsDevStat
         total = ld_volatile_u32(&ctl[p % 3].total_edges);
         p++;
         if (leader) zero_ctl(&ctl[(p + 1) % 3]);
-        td_expand_phase<true>(b, list, next, n, total, parents, distances, dnext, bm_w, nullptr, &ctl[p % 3], sm.td,
+        td_expand_phase<true, TdSmem>(b, list, next, n, total, parents, distances, dnext, bm_w, nullptr, &ctl[p % 3], sm.td,
                               s_red);
         if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
       }
@@ -1244,9 +1285,9 @@ __global__ void __launch_bounds__(kScanT) bfsk_td_scan_host(BfsBufs b, BfsDevSta
 __global__ void __launch_bounds__(kExpT) bfsk_td_expand_host(BfsBufs b, BfsDevState* st, uint32_t n,
                                                              int32_t* parents, uint32_t* distances,
                                                              uint32_t* all_out) {
-  __shared__ TdSmem sm;
+  __shared__ TdSmemHost sm;
   __shared__ unsigned long long s_red[2 * kExpT / 32];
-  td_expand_phase<false>(b, b.list[0], b.list[1], n, st->aux.total_edges, parents, distances, 0, nullptr, all_out,
+  td_expand_phase<false, TdSmemHost>(b, b.list[0], b.list[1], n, st->aux.total_edges, parents, distances, 0, nullptr, all_out,
                          &st->aux, sm, s_red);
 }
 

@@ -193,31 +193,6 @@ __device__ __forceinline__ void ba_flush(BlockAppend<CAP>& q, uint32_t* out, uin
   __syncthreads();
 }
 
-// Two ba_flush calls in one: both offsets are reserved at once (the two
-// atomics overlap), then both buffers are copied out.
-template <int CAP1, int CAP2>
-__device__ __forceinline__ void ba_flush2(BlockAppend<CAP1>& q1, uint32_t* out1, uint32_t* count1,
-                                          BlockAppend<CAP2>& q2, uint32_t* out2, uint32_t* count2) {
-  __syncthreads();
-  const uint32_t n1 = q1.n, n2 = q2.n;
-  if (threadIdx.x == 0) {
-    uint32_t b1 = 0, b2 = 0;
-    if (n1) b1 = atomicAdd(count1, n1);
-    if (n2) b2 = atomicAdd(count2, n2);
-    q1.base = b1;
-    q2.base = b2;
-  }
-  __syncthreads();
-  for (uint32_t k = threadIdx.x; k < n1; k += blockDim.x) out1[q1.base + k] = q1.buf[k];
-  for (uint32_t k = threadIdx.x; k < n2; k += blockDim.x) out2[q2.base + k] = q2.buf[k];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    q1.n = 0;
-    q2.n = 0;
-  }
-  __syncthreads();
-}
-
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
 
 }  // namespace ogb
