@@ -68,12 +68,19 @@ class ClockSampler:
         self.lines: list[str] = []
 
     def start(self):
+        """Starts sampling every 25 ms and returns once the sampler is running
+        (its first line has arrived), so the timed region that follows is
+        covered from its start."""
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "25"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 10:
+                time.sleep(0.005)
+            self.lines.clear()
         except Exception:
             self.proc = None
 
@@ -84,6 +91,11 @@ class ClockSampler:
     def stop(self) -> dict:
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        # a region shorter than the interval still gets the sample that
+        # follows it
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 1:
+            time.sleep(0.005)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
