@@ -106,6 +106,7 @@ struct BfsCtrl {
   uint32_t bm_r, bm_w, bm_c, depth;
   uint32_t iteration, processed, td_steps, bu_steps;
   uint32_t nlevels, epoch, overflow, qcount_prev;
+  uint32_t ul_cand0, pad_c;          // 1: the unvisited list is the graph's cached in-edge list
   unsigned long long edges_examined;
   unsigned long long fedges;         // out-edges of the current frontier
   unsigned long long edges_visited;  // out-edges of every visited vertex
@@ -137,6 +138,7 @@ struct BfsBufs {
   uint32_t* list[2];
   uint32_t* bm[3];
   uint32_t* ul[2];
+  const uint32_t* cand0;  // vertices with in-edges, in vertex order (the first unvisited list)
   uint32_t* offs;
   uint32_t* fstart;
   uint32_t* fdist;
@@ -154,6 +156,9 @@ struct BfsWork {
   uint32_t V = 0, E = 0;
   DevBuf q0, q1, bm0, bm1, bm2, ul0, ul1, state;
   DevBuf offs, fstart, fdist, tile_i0, scan_status;
+  DevBuf cand0;                     // vertices with in-edges (built once per graph)
+  uint32_t n_cand0 = 0, cand0_build = 0;
+  bool cand0_ready = false;
   BfsDevState* h_state = nullptr;   // pinned copy
   uint32_t epoch = 0;               // last scan epoch used
   int search_grid = 0;          // CTAs of the search launch (co-resident)
@@ -214,6 +219,7 @@ static BfsBufs make_bufs(DevGraph& g, BfsWork* w) {
   b.bm[2] = w->bm2.as<uint32_t>();
   b.ul[0] = w->ul0.as<uint32_t>();
   b.ul[1] = w->ul1.as<uint32_t>();
+  b.cand0 = w->cand0.as<uint32_t>();
   b.offs = w->offs.as<uint32_t>();
   b.fstart = w->fstart.as<uint32_t>();
   b.fdist = w->fdist.as<uint32_t>();
@@ -1065,6 +1071,7 @@ __device__ void ctrl_finish_bu(BfsCtrl& c, const BfsCtl& k, BfsDevState* st, boo
   c.nf = k.nf;
   c.ul_size = k.ul_size;
   c.ul_valid = c.mode == BFS_PULL_DENSE ? 0u : 1u;  // that mode walks every vertex in every step
+  c.ul_cand0 = 0;
   c.par_ul ^= 1u;
   c.qcount = k.nf;
   c.lsize = k.lnext;
@@ -1094,7 +1101,7 @@ __device__ void ctrl_finish_bu(BfsCtrl& c, const BfsCtl& k, BfsDevState* st, boo
 // out_degree(root), queue = {root}).
 __global__ void __launch_bounds__(256) bfsk_init(BfsBufs b, BfsDevState* st, uint32_t root, int32_t* parents,
                                                  uint32_t* distances, uint32_t mode, uint32_t bu_entry_frontier,
-                                                 uint32_t E, uint32_t epoch) {
+                                                 uint32_t E, uint32_t epoch, uint32_t n_cand0) {
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < b.V; v += stride) {
     const uint32_t d = b.out_degree[v];
@@ -1125,6 +1132,14 @@ __global__ void __launch_bounds__(256) bfsk_init(BfsBufs b, BfsDevState* st, uin
     c.epoch = epoch;
     c.fedges = d;
     c.edges_visited = d;
+    // the first bottom-up step walks the cached list of vertices with
+    // in-edges (a vertex without any can never be found bottom-up); the
+    // dense-probe mode walks every vertex in every step
+    if (n_cand0 && mode != BFS_PULL_DENSE) {
+      c.ul_valid = 1;
+      c.ul_size = n_cand0;
+      c.ul_cand0 = 1;
+    }
     st->c = c;
     st->parents = parents;
     st->distances = distances;
@@ -1265,7 +1280,7 @@ __global__ void __launch_bounds__(kSearchT, 5) bfsk_search(BfsBufs b, BfsDevStat
         bu_step_phase<true>(b, b.bm[S.bm_r], b.bm[S.bm_w], b.bm[S.bm_c], nullptr, 0, b.ul[S.par_ul ^ 1u],
                             b.list[S.par_l ^ 1u], parents, distances, dnext, &ctl[p % 3], sm.bu, s_red);
       else
-        bu_step_phase<false>(b, b.bm[S.bm_r], b.bm[S.bm_w], b.bm[S.bm_c], b.ul[S.par_ul], S.ul_size,
+        bu_step_phase<false>(b, b.bm[S.bm_r], b.bm[S.bm_w], b.bm[S.bm_c], S.ul_cand0 ? b.cand0 : b.ul[S.par_ul], S.ul_size,
                              b.ul[S.par_ul ^ 1u], b.list[S.par_l ^ 1u], parents, distances, dnext, &ctl[p % 3],
                              sm.bu, s_red);
       if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
@@ -1431,6 +1446,42 @@ size_t bfs_pack_tmp_words(uint32_t V) { return bfs_pack_layout(V).tiles + 8 + sc
 
 // ------------------------------------------------------------ drivers ------
 
+__global__ void bfsk_cand_flags(const uint2* __restrict__ rows_i, uint32_t V, uint32_t* __restrict__ flags) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
+    flags[v] = rows_i[v].y ? 1u : 0u;
+}
+
+__global__ void bfsk_cand_scatter(const uint2* __restrict__ rows_i, uint32_t V, const uint32_t* __restrict__ pos,
+                                  uint32_t* __restrict__ cand) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
+    if (rows_i[v].y) cand[pos[v]] = v;
+}
+
+// The graph's vertices with in-edges, in vertex order, once per build: the
+// first bottom-up step's candidates (about half the vertices of an RMAT
+// graph have no in-edge).
+static int bfs_cand0(DevGraph& g, BfsWork* w, cudaStream_t s) {
+  if (w->cand0_ready && w->cand0_build == g.build_id) return OK;
+  const uint32_t V = g.V;
+  OGB_TRY(w->cand0.alloc((size_t)V * 4 + 16));
+  uint32_t* flags = w->fstart.as<uint32_t>();  // free outside a search
+  uint32_t* pos = w->offs.as<uint32_t>();      // V + 1 words
+  DevBuf tmp;
+  OGB_TRY(tmp.alloc(scan_tmp_words(V) * 4));
+  const int grid = sm_count() * 8;
+  bfsk_cand_flags<<<grid, 256, 0, s>>>(g.inv.d_rows(), V, flags);
+  OGB_TRY(scan_exclusive_u32(flags, pos, V, tmp.as<uint32_t>(), s));
+  bfsk_cand_scatter<<<grid, 256, 0, s>>>(g.inv.d_rows(), V, pos, w->cand0.as<uint32_t>());
+  OGB_CUDA(cudaGetLastError());
+  uint32_t n = 0;
+  OGB_CUDA(cudaMemcpyAsync(&n, pos + V, 4, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  w->n_cand0 = n;
+  w->cand0_build = g.build_id;
+  w->cand0_ready = true;
+  return OK;
+}
+
 int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_t* distances, BfsResult* res,
             bool want_trace, bool bu_entry_nf_frontier, cudaStream_t s) {
   return bfs_run_roots(g, &root, 1, mode, parents, distances, res, want_trace, bu_entry_nf_frontier, s);
@@ -1459,8 +1510,10 @@ int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t 
     b.policy = nullptr;
     b.policy_tail = nullptr;
   }
+  OGB_TRY(bfs_cand0(g, w, s));
+  b.cand0 = w->cand0.as<uint32_t>();
   bfsk_init<<<sm_count() * 8, 256, 0, s>>>(b, st, root, parents, distances, mode, bu_entry_nf_frontier ? 1u : 0u,
-                                            g.E, w->epoch);
+                                            g.E, w->epoch, w->n_cand0);
   DevBuf d_roots;
   if (nroots > 1) {
     OGB_TRY(d_roots.alloc((size_t)nroots * 4));
