@@ -1205,37 +1205,39 @@ __global__ void __launch_bounds__(kSearchT, 5) bfsk_search(BfsBufs b, BfsDevStat
       bfs_features(S, b.E, f);
       if (leader && S.nlevels < (uint32_t)kMaxTrace && !S.overflow)
         for (int i = 0; i < kFeat; i++) st->feat[S.nlevels][i] = f[i];
+      bool bu = false, need = false;
       if (learned) {
         // z = prior . f + bias; the network adds at most +-bound, so it is
         // needed only when that can change the sign
         float z = s_tail[kFeat];
 #pragma unroll
         for (int i = 0; i < kFeat; i++) z = fmaf(s_tail[i], f[i], z);
-        if (threadIdx.x == 0) {
-          s_z = z;
-          s_need = fabsf(z) <= s_tail[kFeat + 1] ? 1u : 0u;
+        need = fabsf(z) <= s_tail[kFeat + 1];
+        bu = z > 0.0f;
+        if (threadIdx.x == 0) s_z = z;
+      }
+      if (threadIdx.x == 0) {
+        s_need = need ? 1u : 0u;
+        if (!need) {  // decided here: no second barrier
+          s_act = ctrl_decide(S, bu);
+          s_t0 = global_ns();
         }
-      } else if (threadIdx.x == 0) {
-        s_act = ctrl_decide(S, false);
-        s_t0 = global_ns();
       }
     }
     __syncthreads();
-    if (learned) {
-      if (s_need) {
-        // stage the network in the phase scratch (no phase is running
-        // between steps), then warp 0 evaluates it
-        const uint4* src = reinterpret_cast<const uint4*>(b.policy);
-        uint4* dst = reinterpret_cast<uint4*>(&sm);
-        for (uint32_t i = threadIdx.x; i < kPolSmem / 16; i += blockDim.x) dst[i] = __ldg(&src[i]);
-        __syncthreads();
-        if (threadIdx.x < 32) {
-          float f[kFeat];
-          bfs_features(S, b.E, f);
-          const float bound = s_tail[kFeat + 1];
-          const float y = policy_logit(reinterpret_cast<const __nv_bfloat16*>(&sm), f, threadIdx.x);
-          if (threadIdx.x == 0) s_z += fminf(fmaxf(y, -bound), bound);
-        }
+    if (s_need) {
+      // learned switch near its boundary: stage the network in the phase
+      // scratch (no phase is running between steps), warp 0 evaluates it
+      const uint4* src = reinterpret_cast<const uint4*>(b.policy);
+      uint4* dst = reinterpret_cast<uint4*>(&sm);
+      for (uint32_t i = threadIdx.x; i < kPolSmem / 16; i += blockDim.x) dst[i] = __ldg(&src[i]);
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        float f[kFeat];
+        bfs_features(S, b.E, f);
+        const float bound = s_tail[kFeat + 1];
+        const float y = policy_logit(reinterpret_cast<const __nv_bfloat16*>(&sm), f, threadIdx.x);
+        if (threadIdx.x == 0) s_z += fminf(fmaxf(y, -bound), bound);
       }
       if (threadIdx.x == 0) {
         s_act = ctrl_decide(S, s_z > 0.0f);

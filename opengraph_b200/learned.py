@@ -211,9 +211,10 @@ def train(out=WEIGHTS, log=print, **kw):
     return fit(collect(log=log, **kw), out=out, log=log)
 
 
-def evaluate(log=print):
-    """Learned vs plain on held-out graphs: RMAT-24 (seeds never used in
-    training) and a 4096 x 4096 grid with random shortcuts (p = 1e-4)."""
+def evaluate(log=print, grid_roots=8):
+    """Learned vs plain on held-out graphs: RMAT-24 (a seed never used in
+    training; 32 random roots) and a 4096 x 4096 grid with random shortcuts
+    (p = 1e-4; 8 roots, about 0.15 s per search)."""
     import torch
 
     import opengraph_b200 as og
@@ -225,27 +226,30 @@ def evaluate(log=print):
         raise SystemExit("no trained weights: run `python -m opengraph_b200.learned train` first")
     lib.check(lib.ogb_bfs_set_policy(sw.ctypes.data), "ogb_bfs_set_policy")
     out = {}
-    graphs = [("rmat24_seed900", lambda: og.generate_rmat(24, 16, 900)[:2], 1 << 24),
-              ("grid4096_p1e-4", lambda: og.generate_grid(4096, 1e-4, 901)[:2], 4096 * 4096)]
-    for name, gen, V in graphs:
+    graphs = [("rmat24_seed900", lambda: og.generate_rmat(24, 16, 900)[:2], 1 << 24, 32),
+              ("grid4096_p1e-4", lambda: og.generate_grid(4096, 1e-4, 901)[:2], 4096 * 4096, grid_roots)]
+    for name, gen, V, nroots in graphs:
         s, d = gen()
         g = _device_graph(lib, s, d, V)
         par = torch.empty(V, dtype=torch.int32, device="cuda")
         dist = torch.empty(V, dtype=torch.int32, device="cuda")
-        roots = _roots(g, 8, 77)
-        res = {}
-        for mode, tag in ((2, "plain"), (3, "learned")):
-            ms = edges = 0.0
-            depths = []
-            for r in roots:
+        roots = _roots(g, nroots, 77)
+        tot = {"plain": [0.0, 0.0], "learned": [0.0, 0.0]}
+        same = True
+        plain_depths = torch.empty_like(dist)
+        for r in roots:   # both switches per root, depths compared on the device
+            for mode, tag in ((2, "plain"), (3, "learned")):
                 g.bfs(r, par, dist, mode=mode)
                 info = g.bfs(r, par, dist, mode=mode)
-                ms += info["ms"]
-                edges += info["reached_out_edges"]
-                depths.append(dist.cpu().numpy().copy())
-            res[tag] = {"gteps": edges / ms / 1e6, "ms_per_search": ms / len(roots), "depths": depths}
-        same = all(np.array_equal(a, b) for a, b in zip(res["plain"]["depths"], res["learned"]["depths"]))
-        bfs = {t: {k: round(v, 4) for k, v in res[t].items() if k != "depths"} for t in res}
+                tot[tag][0] += info["ms"]
+                tot[tag][1] += info["reached_out_edges"]
+                if tag == "plain":
+                    plain_depths.copy_(dist)
+                else:
+                    same = same and bool(torch.equal(dist, plain_depths))
+        bfs = {t: {"gteps": round(e / ms / 1e6, 4), "ms_per_search": round(ms / len(roots), 4)}
+               for t, (ms, e) in tot.items()}
+        bfs["roots"] = len(roots)
         bfs["depths_identical"] = bool(same)
         # PageRank: iterations until the L1 change of normalized ranks < 1e-6
         ranks = torch.empty(V, dtype=torch.float32, device="cuda")
