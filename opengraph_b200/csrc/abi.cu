@@ -19,6 +19,7 @@
 #include <sys/mman.h>
 #include <sys/stat.h>
 #include <sys/time.h>
+#include <omp.h>
 #include <unistd.h>
 
 #include <algorithm>
@@ -1041,7 +1042,7 @@ PackStage& pack_stage() {
 // and depth 0; the DualOrder parent copy gets the sentinel everywhere
 // (BFS.c:58-74).  One pass, one team of host threads.
 static void expand_tiles(const BfsPackLayout& L, uint32_t V, const uint32_t* hp, const uint32_t* od, int* parents,
-                         uint32_t* dist, int* dual, size_t t0, size_t t1) {
+                         uint32_t* dist, size_t t0, size_t t1) {
   if (t1 <= t0) return;
   const uint32_t* off = hp + L.off_words;
   const uint32_t* bm = hp + L.bitmap_words;
@@ -1050,20 +1051,34 @@ static void expand_tiles(const BfsPackLayout& L, uint32_t V, const uint32_t* hp,
   const long nt = (long)(t1 - t0);
 #pragma omp parallel for num_threads(host_threads()) schedule(dynamic, 1)
   for (long k = 0; k < nt; k++) {
-    {
-      const size_t t = t0 + (size_t)k;
-      uint32_t p = off[t];
-      const size_t v0 = t * kPackTile, v1 = std::min<size_t>(V, v0 + kPackTile);
-      for (size_t v = v0; v < v1; v++) {
-        const uint32_t d = od[v];
-        const int sentinel = d ? -(int)d : -1;
-        dual[v] = sentinel;
-        if ((bm[v >> 5] >> (v & 31)) & 1u) {
-          parents[v] = par[p++];
-          dist[v] = d8[v];
-        } else {
-          parents[v] = sentinel;
+    const size_t t = t0 + (size_t)k;
+    const int32_t* pp = par + off[t];
+    const size_t v0 = t * kPackTile, v1 = std::min<size_t>(V, v0 + kPackTile);
+    // one bitmap word (32 vertices) at a time; whole-word cases without a
+    // per-vertex branch
+    for (size_t w0 = v0; w0 < v1; w0 += 32) {
+      const uint32_t word = bm[w0 >> 5];
+      const size_t we = std::min(v1, w0 + 32);
+      if (word == 0) {
+        for (size_t v = w0; v < we; v++) {
+          const uint32_t d = od[v];
+          parents[v] = d ? -(int)d : -1;
           dist[v] = 0;
+        }
+      } else if (word == 0xFFFFFFFFu && we == w0 + 32) {
+        for (size_t v = w0; v < we; v++) {
+          parents[v] = pp[v - w0];
+          dist[v] = d8[v];
+        }
+        pp += 32;
+      } else {
+        for (size_t v = w0; v < we; v++) {
+          const uint32_t d = od[v];
+          const uint32_t bit = (word >> (v - w0)) & 1u;
+          const int reached_parent = *pp;  // read ahead; used only when bit
+          parents[v] = bit ? reached_parent : (d ? -(int)d : -1);
+          dist[v] = bit ? (uint32_t)d8[v] : 0u;
+          pp += bit;
         }
       }
     }
@@ -1074,13 +1089,10 @@ static void expand_tiles(const BfsPackLayout& L, uint32_t V, const uint32_t* hp,
 // 12 MB instead of 32 MB at V = 4M; the host link is the bottleneck of a
 // call), copied in pieces, expanded by host threads as the pieces land.
 static int bfs_result_to_host(ogb_graph* dg, uint32_t V, uint32_t levels, const uint32_t* od, int* parents,
-                              uint32_t* dist, int* dual, cudaStream_t s) {
+                              uint32_t* dist, cudaStream_t s) {
   if (levels >= 255) {  // depths do not fit a byte: plain copies
     OGB_TRY(d2h(parents, dg->d_parents.p, (size_t)V * 4, s));
     OGB_TRY(d2h(dist, dg->d_distances.p, (size_t)V * 4, s));
-    host_par_for(V, [&](size_t lo, size_t hi) {
-      for (size_t v = lo; v < hi; v++) dual[v] = od[v] ? -(int)od[v] : -1;
-    });
     return OK;
   }
   const BfsPackLayout L = bfs_pack_layout(V);
@@ -1109,10 +1121,10 @@ static int bfs_result_to_host(ogb_graph* dg, uint32_t V, uint32_t levels, const 
     const size_t recv = std::min((size_t)R, (c + 1) * chunk);
     size_t hi = done;
     while (hi < L.tiles && off[hi + 1] <= recv) hi++;
-    expand_tiles(L, V, ps.h, od, parents, dist, dual, done, hi);
+    expand_tiles(L, V, ps.h, od, parents, dist, done, hi);
     done = hi;
   }
-  expand_tiles(L, V, ps.h, od, parents, dist, dual, done, L.tiles);
+  expand_tiles(L, V, ps.h, od, parents, dist, done, L.tiles);
   return OK;
 }
 
@@ -1150,10 +1162,26 @@ static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, 
   OGB_MUST(dg->d_distances.alloc((size_t)V * 4 + 4));
   BfsResult& r = g_last_bfs;
   const double t0 = now_s();
-  OGB_MUST(bfs_run(dg->g, (uint32_t)a->source, mode, dg->d_parents.as<int32_t>(), dg->d_distances.as<uint32_t>(),
-                   &r, !quiet(), bitmap_nf, s));
+  // The DualOrder parent copy keeps its initial sentinels (BFS.c:64-73): the
+  // other host threads write them while thread 0 runs the device search.
+  int run_status = OK;
+  int* dual = st->parents_DualOrder;
+#pragma omp parallel num_threads(host_threads())
+  {
+    const int tid = omp_get_thread_num(), nth = omp_get_num_threads();
+    if (tid == 0) {
+      run_status = bfs_run(dg->g, (uint32_t)a->source, mode, dg->d_parents.as<int32_t>(),
+                           dg->d_distances.as<uint32_t>(), &r, !quiet(), bitmap_nf, s);
+    }
+    if (tid > 0 || nth == 1) {
+      const size_t parts = nth > 1 ? (size_t)(nth - 1) : 1, me = nth > 1 ? (size_t)(tid - 1) : 0;
+      const size_t lo = (size_t)V * me / parts, hi = (size_t)V * (me + 1) / parts;
+      for (size_t v = lo; v < hi; v++) dual[v] = od[v] ? -(int)od[v] : -1;
+    }
+  }
+  OGB_MUST(run_status);
   const double t_trav = now_s() - t0;
-  OGB_MUST(bfs_result_to_host(dg, V, (uint32_t)r.nlevels, od, st->parents, st->distances, st->parents_DualOrder, s));
+  OGB_MUST(bfs_result_to_host(dg, V, (uint32_t)r.nlevels, od, st->parents, st->distances, s));
   st->processed_nodes = r.processed_nodes;
   st->iteration = r.iteration;
   st->time_total = t_trav;
