@@ -811,21 +811,27 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
       }
     }
     __syncthreads();
-    // long rows: a group of 8 lanes per row, 8 in-edges per load
+    // long rows: a group of 8 lanes per row, 16 in-edges per step (two per
+    // lane, both loads in flight); the first hit in CSR order wins
     const uint32_t nh = sm.nheavy;
     const uint32_t gl = threadIdx.x & 7;
     const uint32_t gmask = 0xFFu << (lane & 24);
     for (uint32_t h = threadIdx.x >> 3; h < nh; h += kSearchT / 8) {
       const uint32_t hv = sm.hv[h], j0 = sm.hj[h], end = sm.he[h];
       bool hit_row = false;
-      for (uint32_t j = j0; j < end; j += 8) {
-        const uint32_t jj = j + gl;
-        const uint32_t x = jj < end ? (__ldg(&b.nbr_i[jj]) & 0x3FFFFFFFu) : kInvalid;
-        const bool bit = x != kInvalid && ((bm_cur[x >> 5] >> (x & 31)) & 1u);
-        const uint32_t m = (__ballot_sync(gmask, bit) >> (lane & 24)) & 0xFFu;
+      for (uint32_t j = j0; j < end; j += 16) {
+        const uint32_t ja = j + gl, jb = j + 8 + gl;
+        const uint32_t xa = ja < end ? (__ldg(&b.nbr_i[ja]) & 0x3FFFFFFFu) : kInvalid;
+        const uint32_t xb = jb < end ? (__ldg(&b.nbr_i[jb]) & 0x3FFFFFFFu) : kInvalid;
+        const bool bita = xa != kInvalid && ((bm_cur[xa >> 5] >> (xa & 31)) & 1u);
+        const bool bitb = xb != kInvalid && ((bm_cur[xb >> 5] >> (xb & 31)) & 1u);
+        const uint32_t ma = (__ballot_sync(gmask, bita) >> (lane & 24)) & 0xFFu;
+        const uint32_t mb = (__ballot_sync(gmask, bitb) >> (lane & 24)) & 0xFFu;
+        const uint32_t m = ma | (mb << 8);
         if (m) {
           const uint32_t first = (uint32_t)__ffs(m) - 1;
-          if (gl == first) {
+          const uint32_t x = first < 8 ? xa : xb;
+          if (gl == (first & 7u)) {
             parents[hv] = (int32_t)x;
             distances[hv] = dnext;
             atomicOr(&bm_next[hv >> 5], 1u << (hv & 31));
