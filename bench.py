@@ -55,8 +55,29 @@ def dist_env():
     return ws, rank, local
 
 
+def rank_roots(outdeg, rank: int, n: int = NROOTS) -> list[int]:
+    """A rank's replica units: n distinct seeded roots with out-degree > 0
+    (seed 1000 + rank, so ranks search different roots)."""
+    rng = np.random.default_rng(1000 + rank)
+    cand = np.nonzero(np.asarray(outdeg) > 0)[0]
+    return [int(x) for x in rng.choice(cand, size=min(n, len(cand)), replace=False)]
+
+
+def job_totals(my_ms: float, my_edges: float, ws: int, dist=None, device=None) -> tuple[float, float]:
+    """Whole-job aggregate of the replicas: the slowest rank's timed
+    milliseconds (max over ranks) and the edges all ranks traversed (sum)."""
+    if ws == 1:
+        return float(my_ms), float(my_edges)
+    import torch
+    t = torch.tensor([float(my_ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e = torch.tensor([float(my_edges)], dtype=torch.float64, device=device)
+    dist.all_reduce(e, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(e.item())
+
+
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the background."""
+    """nvidia-smi clocks/throttle reasons sampled every 25 ms in the background."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -181,9 +202,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     f = g.view(False)
     outdeg = f.out_degree.cpu().numpy().view(np.uint32)
-    rng = np.random.default_rng(1000 + rank)
-    cand = np.nonzero(outdeg > 0)[0]
-    roots = [int(x) for x in rng.choice(cand, size=NROOTS, replace=False)]
+    roots = rank_roots(outdeg, rank)
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
     par = torch.empty(V, dtype=torch.int32, device=dev)
@@ -219,15 +238,7 @@ def run_ours(args):
     if ws > 1:
         dist.barrier()
     clk = clocks.stop()
-    my_ms = sum(step_ms)
-    if ws > 1:
-        t = torch.tensor([my_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e = torch.tensor([edges_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(e, op=dist.ReduceOp.SUM)
-        max_ms, all_edges = float(t.item()), float(e.item())
-    else:
-        max_ms, all_edges = my_ms, float(edges_total)
+    max_ms, all_edges = job_totals(sum(step_ms), edges_total, ws, dist, dev)
     gteps = all_edges / (max_ms / 1e3) / 1e9
 
     # ---- roofline of the dominant kernel: bfsk_search, one launch = one search
