@@ -624,6 +624,86 @@ def run_reference(args):
     }), flush=True)
 
 
+def run_scale(args):
+    """The plain pipeline at the scaling sizes (unweighted uint32 ids): RMAT
+    scale 26 (67 M vertices, 1.07 B edges) and Erdos-Renyi with 2^24
+    vertices and 2^28 uniform edges.  Per graph: sort + CSR build of both
+    directions, PageRank pull iterations and DO-BFS from 8 seeded roots (L2
+    flushed before each search), each with its algorithmic GB/s and fraction
+    of the measured HBM peak.  One JSON line."""
+    import torch
+
+    import opengraph_b200 as og
+    dev = torch.device("cuda", 0)
+    lib = og.load(False)
+    lib.quiet(True)
+    hbm_peak, peak_kind = peaks()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"case": "scale", "peak_gbs": hbm_peak, "peak_kind": peak_kind, "graphs": {}}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for name, gen, V in (("rmat26_ef16", lambda: og.generate_rmat(26, 16, 0)[:2], 1 << 26),
+                         ("er24_m2^28", lambda: og.generate_uniform(1 << 24, 1 << 28, 0)[:2], 1 << 24)):
+        t0 = time.perf_counter()
+        s, d = gen()
+        gen_s = time.perf_counter() - t0
+        E = len(s)
+        ts = torch.from_numpy(s.view(np.int32)).to(dev)
+        td = torch.from_numpy(d.view(np.int32)).to(dev)
+        del s, d
+        g = lib.device_graph()
+        g.build(ts, td, V, 0)
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(2):
+            start.record()
+            g.build(ts, td, V, 0)
+            stop.record()
+            torch.cuda.synchronize()
+            times.append(start.elapsed_time(stop))
+        build_ms = min(times)
+        P = -(-max(1, (V - 1).bit_length()) // 8)
+        alg = 2 * (16 * E * P + 4 * E + 4 * E + 12 * V) + 16 * E
+        res = {"V": V, "E": E, "host_generate_s": round(gen_s, 1),
+               "csr_build": {"ms": round(build_ms, 2), "passes": P, "gbs": round(alg / build_ms / 1e6, 1),
+                             "frac": round(alg / build_ms / 1e6 / hbm_peak, 4)}}
+        del ts, td
+        torch.cuda.empty_cache()
+        ranks = torch.empty(V, dtype=torch.float32, device=dev)
+        g.pagerank(ranks, mode=0, max_iterations=1, epsilon=0.0)   # builds the renumbered layout
+        g.pagerank(ranks, mode=0, max_iterations=3, epsilon=0.0)
+        start.record()
+        g.pagerank(ranks, mode=0, max_iterations=10, epsilon=0.0)
+        stop.record()
+        torch.cuda.synchronize()
+        it_ms = start.elapsed_time(stop) / 10
+        alg = 8 * E + 28 * V
+        res["pr_pull"] = {"ms_per_iteration": round(it_ms, 3), "gteps": round(E / it_ms / 1e6, 1),
+                          "gbs": round(alg / it_ms / 1e6, 1), "frac": round(alg / it_ms / 1e6 / hbm_peak, 4)}
+        del ranks
+        outdeg = g.view(False).out_degree.cpu().numpy().view(np.uint32)
+        roots = rank_roots(outdeg, 0, 8)
+        par = torch.empty(V, dtype=torch.int32, device=dev)
+        dis = torch.empty(V, dtype=torch.int32, device=dev)
+        g.bfs(roots[0], par, dis, mode=2)
+        ms = edges = nbytes = 0.0
+        for r in roots:
+            flush.zero_()
+            torch.cuda.synchronize()
+            info = g.bfs(r, par, dis, mode=2)
+            ms += info["ms"]
+            edges += info["reached_out_edges"]
+            nbytes += bfs_bytes(g.bfs_trace(), V)[0]
+        res["dobfs"] = {"roots": len(roots), "ms_per_search": round(ms / len(roots), 3),
+                        "gteps": round(edges / ms / 1e6, 1), "gbs": round(nbytes / ms / 1e6, 1),
+                        "frac": round(nbytes / ms / 1e6 / hbm_peak, 4)}
+        del par, dis
+        g.close()
+        torch.cuda.empty_cache()
+        out["graphs"][name] = res
+        print(json.dumps({name: res}), file=sys.stderr, flush=True)
+    print(json.dumps(out), flush=True)
+
+
 def run_case(args):
     """One hot-path kernel family on its own, for profiler captures: `bfs`
     runs --n DO-BFS searches, `pr-pull` / `pr-push` one PageRank run of --n
@@ -685,13 +765,16 @@ def main():
     ap.add_argument("--cpu-roots", type=int, default=8)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-stages", action="store_true")
-    ap.add_argument("--case", default="full", choices=["full", "bfs", "pr-pull", "pr-push", "build"],
-                    help="full = the benchmark line; the others run one kernel family for profiling")
+    ap.add_argument("--case", default="full", choices=["full", "bfs", "pr-pull", "pr-push", "build", "scale"],
+                    help="full = the benchmark line; scale = the plain pipeline on RMAT-26 and ER-24; "
+                         "the others run one kernel family for profiling")
     ap.add_argument("--scale", type=int, default=SCALE, help="RMAT scale of a --case run")
     ap.add_argument("--n", type=int, default=3, help="searches / iterations / builds of a --case run")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    if args.case != "full":
+    if args.case == "scale":
+        run_scale(args)
+    elif args.case != "full":
         run_case(args)
     elif args.impl == "reference":
         run_reference(args)
