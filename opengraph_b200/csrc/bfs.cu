@@ -708,7 +708,7 @@ __device__ void td_small_phase(const BfsBufs& b, const uint32_t* list, uint32_t*
 
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
 constexpr int kBuV = kBuRound / kSearchT;  // candidates per thread per round
-constexpr uint32_t kFirst = 4;             // in-edges probed per candidate before deferral
+constexpr uint32_t kFirst = 6;             // in-edges probed per candidate before deferral
 
 // One bottom-up step of the search.  Candidates: every vertex (dense, the
 // first bottom-up step of a search) or the unvisited list.  Each thread
@@ -1187,7 +1187,7 @@ __global__ void bfsk_set_roots(BfsBufs b, BfsDevState* st, const uint32_t* __res
 // ctl[(p + 1) % 3] when phase p starts (its last reader finished two
 // barriers earlier).  A top-down step is one phase when its list has at most
 // kExpTile entries, else two (scan, expand); a bottom-up step is one phase.
-__global__ void __launch_bounds__(kSearchT, 5) bfsk_search(BfsBufs b, BfsDevState* st) {
+__global__ void __launch_bounds__(kSearchT, 4) bfsk_search(BfsBufs b, BfsDevState* st) {
   __shared__ __align__(16) BfsSmem sm;
   __shared__ BfsCtrl S;
   __shared__ unsigned long long s_red[2 * kSearchT / 32];
