@@ -159,7 +159,7 @@ struct BfsWork {
   DevBuf cand0;                     // vertices with in-edges (built once per graph)
   uint32_t n_cand0 = 0, cand0_build = 0;
   bool cand0_ready = false;
-  BfsDevState* h_state = nullptr;   // pinned copy
+  BfsDevState* h_state = nullptr;   // pinned copy of the header only (up to the trace)
   uint32_t epoch = 0;               // last scan epoch used
   int search_grid = 0;          // CTAs of the search launch (co-resident)
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
@@ -196,7 +196,9 @@ static int bfs_work_get(DevGraph& g, BfsWork** out) {
     w->V = V;
     w->E = E;
   }
-  if (!w->h_state) OGB_CUDA(cudaMallocHost(&w->h_state, sizeof(BfsDevState)));
+  // the header (control state, error word, counters) is all the host reads
+  // back through it; the trace arrays after it are copied on request
+  if (!w->h_state) OGB_CUDA(cudaMallocHost(&w->h_state, offsetof(BfsDevState, trace)));
   if (!w->ev_start) {
     OGB_CUDA(cudaEventCreate(&w->ev_start));
     OGB_CUDA(cudaEventCreate(&w->ev_stop));
@@ -1472,13 +1474,13 @@ static int bfs_cand0(DevGraph& g, BfsWork* w, cudaStream_t s) {
   if (w->cand0_ready && w->cand0_build == g.build_id) return OK;
   const uint32_t V = g.V;
   OGB_TRY(w->cand0.alloc((size_t)V * 4 + 16));
-  uint32_t* flags = w->fstart.as<uint32_t>();  // free outside a search
+  // scratch from the search's own V-sized buffers (free outside a search)
+  uint32_t* flags = w->fstart.as<uint32_t>();
   uint32_t* pos = w->offs.as<uint32_t>();      // V + 1 words
-  DevBuf tmp;
-  OGB_TRY(tmp.alloc(scan_tmp_words(V) * 4));
+  uint32_t* tmp = w->fdist.as<uint32_t>();     // scan_tmp_words(V) <= V + 4 words
   const int grid = sm_count() * 8;
   bfsk_cand_flags<<<grid, 256, 0, s>>>(g.inv.d_rows(), V, flags);
-  OGB_TRY(scan_exclusive_u32(flags, pos, V, tmp.as<uint32_t>(), s));
+  OGB_TRY(scan_exclusive_u32(flags, pos, V, tmp, s));
   bfsk_cand_scatter<<<grid, 256, 0, s>>>(g.inv.d_rows(), V, pos, w->cand0.as<uint32_t>());
   OGB_CUDA(cudaGetLastError());
   uint32_t n = 0;
