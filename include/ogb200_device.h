@@ -24,6 +24,7 @@ extern "C" {
 #define OGB_ERR_RANGE 4
 #define OGB_ERR_NOMEM 5
 #define OGB_ERR_UNSUPPORTED 6
+#define OGB_ERR_STATE 7 /* a device-side consistency check failed */
 
 typedef struct ogb_graph ogb_graph; /* device-resident CSR, both directions */
 

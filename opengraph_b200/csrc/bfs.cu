@@ -298,6 +298,7 @@ struct TdSmem {
   uint32_t off[kExpTile + 2], start[kExpTile + 2], v[kExpTile + 2];
   BlockAppend<kExpTile> q_list;
   uint32_t w[kExpT / 32];
+  uint32_t lo, hi;  // mid-size step: the list entries holding a tile's first and last edge
 };
 struct TdSmemHost : TdSmem {
   static constexpr bool kHost = true;
@@ -701,6 +702,74 @@ __device__ void td_small_phase(const BfsBufs& b, const uint32_t* list, uint32_t*
     const uint32_t e0 = t * kExpTile;
     const uint32_t e1 = min(e0 + kExpTile, total);
     expand_edges<true>(b, e0, e1, n, parents, distances, dnext, bm_w, nullptr, sm, mf, found, fed);
+    ba_flush(sm.q_list, next_list, &ctl->lnext);
+  }
+  td_publish(ctl, mf, found, fed, s_red);
+}
+
+// A top-down step over a list of kExpTile < n <= kMidList entries, in one
+// phase as well: every CTA that has an edge tile (tile count from the
+// frontier's out-edge total, known from the previous step) reads the whole
+// list's out-degrees (kMidList / kExpT per thread, kept in registers) and
+// scans them; then, per tile, the entries overlapping the tile are staged
+// (a contiguous index range: the entry holding the tile's first edge and
+// the one holding its last) and expanded as in a two-phase step.  A scan
+// total that disagrees with the expected one sets ERR_STATE.
+constexpr uint32_t kMidList = 4096;
+__device__ void td_mid_phase(const BfsBufs& b, const uint32_t* list, uint32_t* next_list, uint32_t n,
+                             unsigned long long expect_total, int32_t* parents, uint32_t* distances, uint32_t dnext,
+                             uint32_t* bm_w, BfsCtl* ctl, uint32_t* err, TdSmem& sm, unsigned long long* s_red) {
+  constexpr int K = kMidList / kExpT;
+  const uint32_t ntiles = (uint32_t)((expect_total + kExpTile - 1) / kExpTile);
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->total_edges = (uint32_t)expect_total;
+  if (blockIdx.x >= ntiles) return;
+  uint32_t deg[K], sum = 0;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const uint32_t i = threadIdx.x * K + k;
+    deg[k] = i < n ? __ldg(&b.rows_f[list[i]]).y : 0u;
+    sum += deg[k];
+  }
+  uint32_t total = 0;
+  const uint32_t excl = scan_block_excl(sum, sm.w, &total);
+  if (total != expect_total) {
+    if (threadIdx.x == 0) atomicExch(err, (uint32_t)ERR_STATE);
+    return;
+  }
+  ba_init(sm.q_list);
+  uint32_t mf = 0, found = 0;
+  unsigned long long fed = 0;
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint32_t e0 = t * kExpTile;
+    const uint32_t e1 = min(e0 + kExpTile, total);
+    uint32_t o = excl;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const uint32_t i = threadIdx.x * K + k;
+      if (deg[k]) {
+        if (o <= e0 && e0 < o + deg[k]) sm.lo = i;
+        if (o <= e1 - 1 && e1 - 1 < o + deg[k]) sm.hi = i;
+      }
+      o += deg[k];
+    }
+    __syncthreads();
+    const uint32_t lo = sm.lo, cnt = sm.hi - lo + 1;
+    o = excl;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const uint32_t i = threadIdx.x * K + k;
+      if (deg[k] && i >= lo && i < lo + cnt) {
+        const uint32_t v = list[i];
+        sm.v[i - lo] = v;
+        sm.start[i - lo] = __ldg(&b.rows_f[v]).x;
+        sm.off[i - lo] = o;
+      }
+      o += deg[k];
+    }
+    __syncthreads();
+    expand_edges<true>(b, e0, e1, cnt, parents, distances, dnext, bm_w, nullptr, sm, mf, found, fed);
+    // at most kExpTile discoveries per tile: flush every tile (its barriers
+    // also end this tile's use of the staged entries)
     ba_flush(sm.q_list, next_list, &ctl->lnext);
   }
   td_publish(ctl, mf, found, fed, s_red);
@@ -1268,6 +1337,11 @@ __global__ void __launch_bounds__(kSearchT, 4) bfsk_search(BfsBufs b, BfsDevStat
         td_small_phase(b, list, next, n, parents, distances, dnext, bm_w, &ctl[p % 3], sm.td, s_red);
         if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
         total = ld_volatile_u32(&ctl[p % 3].total_edges);
+      } else if (n <= kMidList) {
+        td_mid_phase(b, list, next, n, S.fedges, parents, distances, dnext, bm_w, &ctl[p % 3], &st->err, sm.td,
+                     s_red);
+        if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
+        total = ld_volatile_u32(&ctl[p % 3].total_edges);
       } else {
         td_scan_phase<true>(b, list, n, distances, S.epoch, &ctl[p % 3], &st->err, sm.scan);
         if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
@@ -1544,7 +1618,9 @@ int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t 
   OGB_CUDA(cudaEventElapsedTime(&total_ms, w->ev_start, w->ev_stop));
   const BfsDevState* h = w->h_state;
   w->epoch = h->c.epoch;
-  if (h->err) return fail((int)h->err, "bfs: a bounded device wait gave up");
+  if (h->err)
+    return fail((int)h->err, h->err == ERR_STATE ? "bfs: a device-side consistency check failed"
+                                                 : "bfs: a bounded device wait gave up");
   if (h->c.overflow) return fail(ERR_SPIN, "bfs: more than V + 8 steps");
   BfsResult r;
   r.iteration = h->c.iteration;

@@ -18,6 +18,7 @@ enum Status : int {
   ERR_RANGE = 4,         // vertex id out of the supported range
   ERR_NOMEM = 5,         // allocation failed
   ERR_UNSUPPORTED = 6,   // variant not provided by this library
+  ERR_STATE = 7,         // a device-side consistency check failed (counters disagree)
 };
 
 // Last error message of the calling thread (set by fail()).
