@@ -29,7 +29,8 @@
 //    it from the same per-phase counters, so all copies agree without an
 //    extra barrier; no host round trip and no launch per level.  Every
 //    barrier wait is bounded (error word, then exit) and the loop is bounded
-//    by V + 8 steps;
+//    by V + 8 steps.  The learned switch (mode BFS_LEARNED) decides each step
+//    from a linear prior and, near its boundary, a small network;
 //  * the search is level-synchronous, so every frontier vertex has the same
 //    depth: a discovered vertex gets depth + 1 without reading its parent's
 //    distance (what the reference computes as distances[parent] + 1);
@@ -44,11 +45,15 @@
 //    phase then gives each CTA whole edge tiles (coalesced neighbour reads,
 //    independent of the degree skew).  The scan's look-back words carry the
 //    scan's epoch, so they never need clearing;
-//  * bottom-up: the first bottom-up level of a search walks all vertices (a
-//    warp's ballot is one whole word of the next bitmap), later levels walk
-//    the compacted list of still-unvisited vertices; each probe loads four
-//    in-neighbours and their frontier bits at once (the first hit in CSR
-//    order still wins);
+//  * bottom-up: the first bottom-up level of a search walks a cached list of
+//    the graph's vertices with in-edges (built once per graph: a vertex
+//    without one can never be found bottom-up), later levels walk the
+//    compacted list of still-unvisited vertices; each CTA takes one equal,
+//    contiguous range of candidates; a candidate's first kFirst in-neighbours
+//    and their frontier bits are loaded at once, longer rows go to a per-round
+//    list scanned by groups of 8 lanes (the first hit in CSR order still
+//    wins); the dense-probe mode walks every vertex (a warp's ballot is one
+//    whole word of the next bitmap);
 //  * a top-down step sets the bitmap bit of every vertex it discovers and a
 //    bottom-up step lists the vertices it discovers, so a change of
 //    direction needs no conversion pass (arrayQueueToBitmap /
@@ -56,7 +61,8 @@
 //    write, clear), so every step clears the bitmap a later step writes while
 //    it runs;
 //  * a top-down step whose list has at most kExpTile entries runs as one
-//    phase: every CTA scans the short list itself;
+//    phase: every CTA scans the short list itself; up to kMidList entries it
+//    is one phase too, the CTAs that own an edge tile scanning the list;
 //  * queue appends are staged per CTA in shared memory (one global atomic
 //    per flush); counters are summed per CTA (one atomic per CTA);
 //  * bitmaps: bit v = word v>>5, bit v&31 (bitmap.h:7-9).
