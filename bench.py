@@ -63,6 +63,11 @@ def rank_roots(outdeg, rank: int, n: int = NROOTS) -> list[int]:
     return [int(x) for x in rng.choice(cand, size=min(n, len(cand)), replace=False)]
 
 
+def sort_passes(V: int) -> int:
+    """Radix passes of the CSR build's byte model: ceil(ceil(log2 V) / 8)."""
+    return -(-max(1, (V - 1).bit_length()) // 8)
+
+
 def job_totals(my_ms: float, my_edges: float, ws: int, dist=None, device=None) -> tuple[float, float]:
     """Whole-job aggregate of the replicas: the slowest rank's timed
     milliseconds (max over ranks) and the edges all ranks traversed (sum)."""
@@ -365,7 +370,7 @@ def stages(lib, og, g, ts, td, tw, V, E, dev, hbm_peak):
         times.append(start.elapsed_time(stop))
     g2.close()
     build_ms = statistics.median(times)
-    P = 3  # 8-bit digit passes for 22-bit ids
+    P = sort_passes(V)
     wgt = 1
     alg = 2 * ((16 + 4 * wgt) * E * P + 4 * E + 4 * E + 12 * V) + (16 + 8 * wgt) * E
     out["csr_build"] = {"ms": round(build_ms, 3), "medges_per_s": round(E / build_ms / 1e3, 1),
@@ -661,7 +666,7 @@ def run_scale(args):
             torch.cuda.synchronize()
             times.append(start.elapsed_time(stop))
         build_ms = min(times)
-        P = -(-max(1, (V - 1).bit_length()) // 8)
+        P = sort_passes(V)
         alg = 2 * (16 * E * P + 4 * E + 4 * E + 12 * V) + 16 * E
         res = {"V": V, "E": E, "host_generate_s": round(gen_s, 1),
                "csr_build": {"ms": round(build_ms, 2), "passes": P, "gbs": round(alg / build_ms / 1e6, 1),
