@@ -17,8 +17,9 @@ step on the same frontier.  Training samples: the switch inputs the kernel
 records before each level (ogb_bfs_features), with target
 y = log2(top-down ms / bottom-up ms) (clipped to +-8).  The prior is a
 least-squares fit of y on L(frontier out-edges) (the reference rule's mf,
-BFS.c:520-560), L(bottom-up candidates) (V, or the unvisited list) and the
-list flag: a power-law model of the two steps' costs, top-down work growing
+BFS.c:520-560), L(bottom-up candidates) (the list a bottom-up step would
+walk: the graph's vertices with in-edges before the first bottom-up step,
+the unvisited list after it, all V in the dense probe) and the list flag: a power-law model of the two steps' costs, top-down work growing
 with the frontier's edges and bottom-up work with its candidates.  The
 network is fitted (squared error) to the remaining residual, clipped to +-B,
 so far from the training states it can move the decision by at most B and
