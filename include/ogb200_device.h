@@ -141,9 +141,10 @@ int ogb_mlp_infer(uint32_t in, uint32_t hidden, const float *params, const float
  * so the network is a bounded correction of the prior; NULL removes it.  The
  * inputs x, before every step (L(x) = log2(1 + x)): L(frontier vertices),
  * L(frontier out-edges), L(unexplored out-edges), L(bottom-up candidates:
- * the unvisited list when one exists, else V), L(V), L(frontier) -
- * L(previous frontier), visited fraction, 1 when a bottom-up step would
- * walk the unvisited list (else 0). */
+ * the list a bottom-up step would walk -- the graph's vertices with in-edges
+ * before the first bottom-up step, the unvisited list after it; V in mode 4),
+ * L(V), L(frontier) - L(previous frontier), visited fraction, 1 when a
+ * bottom-up step would walk a list (else 0). */
 int ogb_bfs_set_policy(const float *params);
 /* Those inputs for every step of the last ogb_bfs on g (count x 8 floats). */
 int ogb_bfs_features(ogb_graph *g, float *features, uint32_t max_levels, uint32_t *count);
