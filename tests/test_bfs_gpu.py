@@ -119,3 +119,40 @@ def test_bfs_scale22_properties(torch_cuda, lib, graphs):
     dg.bfs(root, par_t, dist_t, mode=0)
     assert torch.equal(dist, dist_t)
     dg.close()
+
+
+def fanout_graph(children: int, per_child: int, seed: int):
+    """Root 0 -> `children` vertices -> `per_child` grandchildren each (some
+    shared, so claims race), plus edges back to the root: the second
+    top-down level expands a list of exactly `children` entries."""
+    rng = np.random.default_rng(seed)
+    kids = np.arange(1, children + 1, dtype=np.uint32)
+    V = 1 + children + children * per_child // 2
+    gkids = rng.integers(children + 1, V, size=(children, per_child)).astype(np.uint32)
+    s = np.concatenate([np.zeros(children, np.uint32), np.repeat(kids, per_child), gkids[:, 0]])
+    d = np.concatenate([kids, gkids.reshape(-1), np.zeros(children, np.uint32)])
+    return s, d, int(V)
+
+
+@pytest.mark.parametrize("children", [1000, 1024, 1025, 3000, 4096, 4097, 6000])
+def test_bfs_top_down_list_sizes(torch_cuda, lib, oracle, children):
+    """Top-down steps over lists of at most 1024 entries (one phase, every
+    CTA scans the list), 1025..4096 (one phase, tile owners scan it) and
+    more (two phases, chained scan): depths, counts and parents as the
+    oracle, in push-only and direction-optimized modes."""
+    torch = torch_cuda
+    s, d, V = fanout_graph(children, 5, children)
+    g = oracle.build(s, d, V, 0)
+    dg = lib.device_graph()
+    dg.build(dev(torch, s), dev(torch, d), V, 0)
+    par_t = torch.empty(V, dtype=torch.int32, device="cuda")
+    dist_t = torch.empty(V, dtype=torch.int32, device="cuda")
+    for mode in (1, 2):
+        info = dg.bfs(0, par_t, dist_t, mode=mode)
+        par, dist = host(par_t, np.int32), host(dist_t)
+        _, edist, est = oracle.bfs(g, 0, mode)
+        assert np.array_equal(dist, edist), mode
+        assert info["iteration"] == est["iteration"] and info["reached"] == est["reached"]
+        assert [t["direction"] for t in dg.bfs_trace()] == list(est["dirs"][:info["levels"]])
+        check_parents(g, 0, par, dist)
+    dg.close()
