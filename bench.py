@@ -579,21 +579,24 @@ def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    import opengraph_b200 as og
-    from oracle.oracle import Reference
+    # This arm runs the reference alone: the input is made by the oracle's
+    # restatement of the generator and written with numpy, so no product
+    # library is loaded into this process.
+    from oracle.oracle import Oracle, Reference, write_edge_file
     if not Reference.available(True):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference CPU build) not present"}))
         return
-    s, d, w = og.generate_rmat(SCALE, EDGE_FACTOR, SEED, weighted=True)
+    s, d, w = Oracle().generate_rmat(SCALE, EDGE_FACTOR, SEED, weighted=True)
     V = 1 << SCALE
     ref = Reference(True)
     tmp = tempfile.mkdtemp()
     path = os.path.join(tmp, f"rmat{SCALE}.wbin")
-    og.write_edge_file(path, s, d, w)
+    write_edge_file(path, s, d, w)
+    del s, d, w
     cores = os.cpu_count()
     os.environ["OMP_NUM_THREADS"] = str(cores)
     rg = ref.build_graph(path, weighted_file=True)
-    outdeg = og.as_numpy(rg.contents.vertices.contents.out_degree, V, np.uint32)
+    outdeg = np.ctypeslib.as_array(rg.contents.vertices.contents.out_degree, shape=(V,)).astype(np.uint32)
     rng = np.random.default_rng(1000)
     roots = [int(x) for x in rng.choice(np.nonzero(outdeg > 0)[0], size=NROOTS, replace=False)]
     per_step = args.cpu_roots

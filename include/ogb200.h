@@ -227,9 +227,9 @@ void graphCSRPrint(struct GraphCSR *graphCSR);
 
 /* ---- BFS (GPU) ---------------------------------------------------------- */
 
-/* 00_graph_bench/include/algorithms/openmp/BFS.h:32 ; BFS.c:42-78 */
+/* 00_graph_bench/include/algorithms/openmp/BFS.h:31 ; BFS.c:42-78 */
 struct BFSStats *newBFSStatsGraphCSR(struct GraphCSR *graph);
-/* BFS.h:37 ; BFS.c:163-180 */
+/* BFS.h:36 ; BFS.c:163-180 */
 void freeBFSStats(struct BFSStats *stats);
 /* BFS.h:42 ; BFS.c:238-268.  pushpull 0 pull, 1 push, 2 direction-optimized,
  * 3/4 bitmap-frontier variants (same depths, GPU), default DO. */
@@ -240,9 +240,9 @@ struct BFSStats *breadthFirstSearchPullGraphCSR(struct Arguments *arguments, str
 struct BFSStats *breadthFirstSearchPushGraphCSR(struct Arguments *arguments, struct GraphCSR *graph);
 /* BFS.h:46 ; BFS.c:476-626 (alpha = 15, beta = 18) */
 struct BFSStats *breadthFirstSearchDirectionOptimizedGraphCSR(struct Arguments *arguments, struct GraphCSR *graph);
-/* BFS.h:52 ; BFS.c:785-... (GPU: the top-down path) */
+/* BFS.h:55 ; BFS.c:785-... (GPU: the top-down path) */
 struct BFSStats *breadthFirstSearchPushBitmapGraphCSR(struct Arguments *arguments, struct GraphCSR *graph);
-/* BFS.h:53 ; BFS.c (GPU: the direction-optimized path) */
+/* BFS.h:56 ; BFS.c (GPU: the direction-optimized path) */
 struct BFSStats *breadthFirstSearchPushDirectionOptimizedBitmapGraphCSR(struct Arguments *arguments, struct GraphCSR *graph);
 /* BFS.h:48 ; BFS.c:639-687.  One top-down level over host queues: the
  * current window [head, tail) of the shared queue is expanded on the GPU and

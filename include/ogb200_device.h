@@ -88,9 +88,6 @@ const char *ogb_last_error(void);
 int ogb_weighted_layout(void);
 /* Silence the reference-style progress tables printed by ogb200.h calls. */
 void ogb_set_quiet(int quiet);
-/* Accepted for compatibility and ignored: the persistent search always
- * records per-level device times (globaltimer) in its level trace. */
-void ogb_set_level_timing(int on);
 
 int ogb_graph_create(ogb_graph **g);
 void ogb_graph_destroy(ogb_graph *g);
@@ -272,8 +269,12 @@ int ogb_pagerank_history(ogb_graph *g, double *errors, uint32_t *active, uint32_
  * Inputs (device arrays): the inverse CSR -- row starts d_in_edges_idx,
  * in-degrees d_in_degree, in-neighbour ids d_in_neighbors -- and the forward
  * out-degrees.  Outputs: d_ranks (V normalized ranks) and, if d_info is not
- * NULL, a DEVICE ogb_pr_info (ms and launches are 0).  Same semantics, work
- * split and summation order as ogb_pagerank pull at its default thresholds.
+ * NULL, a DEVICE ogb_pr_info (ms and launches are 0).  Same semantics as
+ * ogb_pagerank pull; rows of at most 2048 in-edges are summed in the same
+ * order as its default thresholds give, longer rows by one 256-thread CTA
+ * (ogb_pagerank cuts them into chunks), so the ranks can differ in the last
+ * bits: they agree with ogb_pagerank and with the reference's sequential
+ * order within 1e-6 L1 at the same iteration count.
  * The work is enqueued on `stream` (NULL = the default stream) and the call
  * returns without waiting.  The first call on each device looks up the
  * scratch address: make that first call before any stream capture.  Every
@@ -295,7 +296,7 @@ int ogb_generate_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, doubl
 int ogb_generate_uniform(uint32_t num_vertices, uint64_t num_edges, uint64_t seed, uint32_t *src, uint32_t *dst,
                          float *w);
 /* side x side 4-neighbour grid (both directions) plus, per vertex with
- * probability p, one shortcut to a random vertex.  Returns the edge count in
+ * probability p, a diagonal shortcut to (r+1, c+1) and back.  Returns the edge count in
  * *num_edges; call with src == NULL to get the capacity needed. */
 int ogb_generate_grid(uint32_t side, double p, uint64_t seed, uint32_t *src, uint32_t *dst, float *w,
                       uint64_t *num_edges);

@@ -1382,7 +1382,6 @@ extern "C" uint32_t generateRandomRootGraphCSR(mt19937state* mt, struct GraphCSR
 extern "C" const char* ogb_last_error(void) { return ogb::last_error(); }
 extern "C" int ogb_weighted_layout(void) { return OGB200_WEIGHTED; }
 extern "C" void ogb_set_quiet(int q) { g_quiet = q ? 1 : 0; }
-extern "C" void ogb_set_level_timing(int on) { (void)on; }
 
 extern "C" int ogb_graph_create(ogb_graph** g) {
   if (!g) return fail(ERR_ARG, "null");

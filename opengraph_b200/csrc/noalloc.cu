@@ -25,6 +25,7 @@
 #include <stdio.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "../../include/ogb200_device.h"
 #include "common.cuh"
@@ -65,6 +66,7 @@ struct DevInfo {
 };
 constexpr int kMaxDevices = 64;
 static DevInfo g_dev[kMaxDevices];  // filled by the first call on each device
+static std::mutex g_dev_mu;         // guards g_dev: two host threads may make a first call at once
 
 struct NaParams {
   float base_pr, damp;
@@ -226,6 +228,7 @@ __global__ void na_finish_kernel(uint32_t V, float* __restrict__ pr, const NaCtl
 // scratch array (the host-side name is only a stand-in for the symbol).
 int noalloc_setup(int dev, DevInfo** out) {
   if (dev < 0 || dev >= kMaxDevices) return ogb::fail(ogb::ERR_ARG, "noalloc: device %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_dev_mu);
   DevInfo& di = g_dev[dev];
   if (!di.scratch) {
     void* p = nullptr;

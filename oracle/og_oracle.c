@@ -415,3 +415,79 @@ void orc_random_roots(uint32_t seed, uint32_t V, uint32_t avg_degree, const uint
         }
     }
 }
+
+/* ------------------------------------------------------------- inputs -- */
+
+/* The benchmark's synthetic RMAT input, restated here so that the timed
+ * reference arm can make its .wbin file without loading the product library.
+ * Every draw is SplitMix64's finalizer (Steele, Lea, Flood 2014) of (seed,
+ * edge index, level); quadrant a/b/c/d per level from a 53-bit uniform; ids
+ * relabelled by a seeded Fisher-Yates permutation; weights uniform in
+ * [1, 256).  Must equal the product's generator bit for bit (tested). */
+static uint64_t orc_mix64(uint64_t z)
+{
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static uint64_t orc_draw(uint64_t seed, uint64_t index, uint64_t k)
+{
+    return orc_mix64(orc_mix64(seed ^ (k * 0xD1B54A32D192ED03ull)) ^ index);
+}
+
+int orc_generate_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, double a, double b, double c,
+                      int permute, uint32_t *src, uint32_t *dst, float *w)
+{
+    if (scale == 0 || scale > 30) return -1;
+    const uint64_t V = 1ull << scale, E = V * edge_factor;
+    if (E > 0xFFFFFFFFull) return -1;
+    uint32_t *perm = NULL;
+    if (permute)
+    {
+        perm = malloc(V * 4);
+        for (uint64_t i = 0; i < V; i++) perm[i] = (uint32_t)i;
+        uint64_t state = orc_mix64(seed ^ 0xA5A5A5A5ull);
+        for (uint64_t i = V; i > 1; i--)
+        {
+            state = orc_mix64(state);
+            const uint32_t j = (uint32_t)(((unsigned __int128)state * i) >> 64);
+            const uint32_t t = perm[i - 1];
+            perm[i - 1] = perm[j];
+            perm[j] = t;
+        }
+    }
+    /* per-level keys do not depend on the edge: hoist them */
+    uint64_t key[32];
+    for (uint32_t l = 0; l < scale; l++) key[l] = orc_mix64(seed ^ ((uint64_t)l * 0xD1B54A32D192ED03ull));
+    const double ab = a + b, abc = a + b + c;
+    /* edges are independent draws: the only parallel loop of the oracle */
+#pragma omp parallel for schedule(static)
+    for (uint64_t i = 0; i < E; i++)
+    {
+        uint32_t u = 0, v = 0;
+        for (uint32_t l = 0; l < scale; l++)
+        {
+            const double r = (double)(orc_mix64(key[l] ^ i) >> 11) * (1.0 / 9007199254740992.0);
+            const uint32_t bu = r >= ab;
+            const uint32_t bv = (r >= a && r < ab) || r >= abc;
+            u = (u << 1) | bu;
+            v = (v << 1) | bv;
+        }
+        if (perm)
+        {
+            u = perm[u];
+            v = perm[v];
+        }
+        src[i] = u;
+        dst[i] = v;
+        if (w)
+        {
+            const double x = (double)(orc_draw(seed ^ 0x5713ull, i, 0xFFFF) >> 40) * (1.0 / 16777216.0);
+            w[i] = (float)(1.0 + 255.0 * x);
+        }
+    }
+    free(perm);
+    return 0;
+}

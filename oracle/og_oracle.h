@@ -86,4 +86,10 @@ void orc_pagerank_f64(uint32_t V, const uint32_t *f_outdeg, const uint32_t *i_ou
 void orc_random_roots(uint32_t seed, uint32_t V, uint32_t avg_degree, const uint32_t *out_degree, uint32_t n,
                       uint32_t *roots);
 
+/* The benchmark's seeded RMAT edge list (the product's ogb_generate_rmat,
+ * restated so the timed reference arm needs no product library).  Returns -1
+ * on bad sizes. */
+int orc_generate_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, double a, double b, double c,
+                      int permute, uint32_t *src, uint32_t *dst, float *w);
+
 #endif

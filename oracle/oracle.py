@@ -24,7 +24,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
-REFERENCE_SRC = "/root/reference/00_graph_bench"
+# the reference tree (read only where it is mounted; override with OGB_REFERENCE_ROOT)
+REFERENCE_ROOT = os.environ.get("OGB_REFERENCE_ROOT", "/root/reference")
+REFERENCE_SRC = os.path.join(REFERENCE_ROOT, "00_graph_bench")
 
 u32 = C.c_uint32
 vp = C.c_void_p
@@ -35,7 +37,7 @@ def build(ref: bool = True) -> None:
     targets = ["oracle"]
     if ref and os.path.isdir(REFERENCE_SRC):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE, "-j8", *targets], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "-j8", f"REF={REFERENCE_SRC}", *targets], check=True)
 
 
 def _p(a):
@@ -63,6 +65,20 @@ class Oracle:
         d.orc_pagerank_f64.argtypes = [u32, vp, vp, vp, vp, u32, vp, vp]
         d.orc_random_roots.argtypes = [u32, u32, u32, vp, u32, vp]
         d.orc_set_gpu_order.argtypes = [u32, u32, u32, u32]
+        d.orc_generate_rmat.argtypes = [u32, u32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_int, vp, vp,
+                                        vp]
+        d.orc_generate_rmat.restype = C.c_int
+
+    def generate_rmat(self, scale: int, edge_factor: int, seed: int, a=0.57, b=0.19, c=0.19, permute=True,
+                      weighted=False):
+        """The benchmark's seeded RMAT edge list, made without the product
+        library (equal to opengraph_b200.generate_rmat bit for bit)."""
+        E = (1 << scale) * edge_factor
+        src, dst = np.empty(E, np.uint32), np.empty(E, np.uint32)
+        w = np.empty(E, np.float32) if weighted else None
+        if self.d.orc_generate_rmat(scale, edge_factor, seed, a, b, c, 1 if permute else 0, _p(src), _p(dst), _p(w)):
+            raise ValueError("oracle generate_rmat: bad sizes")
+        return src, dst, w
 
     def set_gpu_order(self, warp_thr: int = 32, cta_thr: int = 2048, cta_threads: int = 256,
                       chunk: int = 8192) -> None:
@@ -171,6 +187,17 @@ class Oracle:
         roots = np.empty(n, np.uint32)
         self.d.orc_random_roots(seed, V, avg_degree, _p(out_degree), n, _p(roots))
         return roots
+
+
+def write_edge_file(path: str, src, dst, w=None) -> None:
+    """The reference's binary edge file (edgeList.c:336-594): little-endian
+    {u32 src, u32 dst} records (.bin), or {u32 src, u32 dst, f32 w} (.wbin)."""
+    rec = np.empty((len(src), 3 if w is not None else 2), np.uint32)
+    rec[:, 0] = src
+    rec[:, 1] = dst
+    if w is not None:
+        rec[:, 2] = np.asarray(w, np.float32).view(np.uint32)
+    rec.astype("<u4", copy=False).tofile(path)
 
 
 @contextlib.contextmanager

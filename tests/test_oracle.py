@@ -9,8 +9,9 @@ import numpy as np
 import pytest
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
-LAW_ENRON = "/root/reference/01_test_graphs/LAW/LAW-enron/graph.bin"
+FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "*_w[01].npz")))
+REFERENCE_ROOT = os.environ.get("OGB_REFERENCE_ROOT", "/root/reference")
+LAW_ENRON = os.path.join(REFERENCE_ROOT, "01_test_graphs/LAW/LAW-enron/graph.bin")
 
 
 def test_fixtures_present():
@@ -131,3 +132,61 @@ def test_oracle_random_roots_match_reference_picker(og, oracle, ref, tmp_path):
     for r in roots:
         assert ref.d.generateRandomRootGraphCSR(C.byref(mt), rg) == r
     ref.graphCSRFree(rg)
+
+
+def test_oracle_matches_law_enron_fixture(oracle):
+    """The reference's equivalence-test input (committed as
+    tests/golden/law_enron.npz by make_law_enron.py from the reference's own
+    build): sort 1 + dedup + CSR digests, BFS distances / counts / pull
+    parents from the reference's MT19937 roots, PageRank pull ranks
+    bit-exact and push ranks within 1e-6 L1."""
+    import hashlib
+
+    def digest(a):
+        return np.frombuffer(hashlib.sha256(np.ascontiguousarray(a).tobytes()).digest(), np.uint8)
+
+    z = dict(np.load(os.path.join(GOLDEN, "law_enron.npz")))
+    V = int(z["shape"][0])
+    ss, sd, _ = oracle.sort(z["src"], z["dst"], None, 1)
+    ds, dd, _ = oracle.dedup(ss, sd)
+    g = oracle.build(ds, dd, V, 1)
+    assert len(ds) == int(z["shape"][1])
+    for k in ("f_src", "f_dst", "f_outdeg", "f_indeg", "f_idx", "i_src", "i_dst", "i_outdeg", "i_indeg", "i_idx"):
+        assert np.array_equal(digest(g[k]), z["csr_" + k]), k
+    for i, r in enumerate(z["roots"]):
+        for mode in (0, 1, 2):
+            p, dist, st = oracle.bfs(g, int(r), mode)
+            assert np.array_equal(digest(dist), z[f"bfs_m{mode}_r{i}_dist"]), (i, mode)
+            assert [st["processed_nodes"], st["iteration"]] == list(z[f"bfs_m{mode}_r{i}_stats"]), (i, mode)
+            if mode == 0:
+                assert np.array_equal(digest(p), z[f"bfs_m{mode}_r{i}_par"]), i
+    # pull sums each row sequentially: bit-exact; the reference's push adds
+    # with OpenMP atomics in thread order, so it is held to 1e-6 L1
+    r, st = oracle.pagerank(g, 0, 100, 1e-4)
+    assert st["iterations"] == int(z["pr_pull_stats"][0])
+    assert np.array_equal(r.view(np.uint32), z["pr_pull_ranks"].view(np.uint32))
+    r, st = oracle.pagerank(g, 1, 100, 1e-4)
+    assert st["iterations"] == int(z["pr_push_stats"][0])
+    assert float(np.abs(r.astype(np.float64) - z["pr_push_ranks"]).sum()) <= 1e-6
+
+
+def test_oracle_generator_equals_product_generator(og, oracle):
+    """bench.py's reference arm makes its input with the oracle's generator
+    (no product library in that process): it must equal the product's
+    ogb_generate_rmat bit for bit (both are host code)."""
+    for scale, ef, seed, weighted in ((12, 16, 3, True), (10, 8, 0, False), (15, 16, 0, True)):
+        a = oracle.generate_rmat(scale, ef, seed, weighted=weighted)
+        b = og.generate_rmat(scale, ef, seed, weighted=weighted)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        if weighted:
+            assert np.array_equal(a[2].view(np.uint32), b[2].view(np.uint32))
+
+
+def test_oracle_edge_file_writer_equals_product(og, tmp_path):
+    from oracle.oracle import write_edge_file
+    s, d, w = og.generate_rmat(10, 8, 1, weighted=True)
+    for weighted in (False, True):
+        p1, p2 = str(tmp_path / "a"), str(tmp_path / "b")
+        write_edge_file(p1, s, d, w if weighted else None)
+        og.write_edge_file(p2, s, d, w if weighted else None)
+        assert open(p1, "rb").read() == open(p2, "rb").read()
