@@ -334,11 +334,18 @@ def e2e_dropin(lib, og, s, d, w, roots, rank, dev):
         a.source = r
         lib.freeBFSStats(lib.breadthFirstSearchGraphCSR(C.byref(a), gh))
     torch.cuda.synchronize()
+    names = ("call", "stats_alloc", "device_search", "dual_sentinels", "search_and_sentinels",
+             "result_copy")
+    ph = (C.c_double * len(names))()
+    acc = np.zeros(len(names))
     t0 = time.perf_counter()
     for r in roots:
         a.source = r
         lib.freeBFSStats(lib.breadthFirstSearchGraphCSR(C.byref(a), gh))
+        lib.ogb_dropin_bfs_phases(ph, len(names))
+        acc += np.frombuffer(ph, np.float64)
     t1 = time.perf_counter()
+    phases_ms = {k: round(float(v) / len(roots) * 1e3, 4) for k, v in zip(names, acc)}
     # traversed edges of these roots (the same searches, run on the device copy)
     g = og.DeviceGraph(lib, handle=lib.ogb_graph_of(C.cast(gh, C.c_void_p)), owned=False)
     pt = torch.empty(V, dtype=torch.int32, device=dev)
@@ -349,6 +356,8 @@ def e2e_dropin(lib, og, s, d, w, roots, rank, dev):
     n = len(roots)
     return {"value": round(edges / (t1 - t0) / 1e9, 3), "unit": "GTEPS", "h2d_bytes_per_step": 0,
             "d2h_bytes_per_step": int(n * 8 * V), "calls_per_step": n,
+            "ms_per_call": round((t1 - t0) / n * 1e3, 4), "phases_ms_per_call": phases_ms,
+            "host_bytes_written_per_call": int(12 * V),
             "api": "breadthFirstSearchGraphCSR(pushpull=2) on a graphCSRPreProcessingStep GraphCSR"}
 
 

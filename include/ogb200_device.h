@@ -89,6 +89,16 @@ int ogb_weighted_layout(void);
 /* Silence the reference-style progress tables printed by ogb200.h calls. */
 void ogb_set_quiet(int quiet);
 
+/* No counterpart in the reference.  Wall-clock phases, in seconds, of the
+ * last breadthFirstSearchGraphCSR-family call: [0] the whole call, [1] stats
+ * allocation and the device copy lookup, [2] the device search as the
+ * calling thread sees it (launch to result header), [3] writing the DualOrder
+ * parent copy's sentinels (host threads, during the search), [4] both of
+ * those together, [5] the device-to-host copy of the result into the
+ * reference's arrays (depths as bytes, widened on the host; parents whole).  Writes min(n, OGB_DROPIN_BFS_PHASES) values. */
+#define OGB_DROPIN_BFS_PHASES 6
+int ogb_dropin_bfs_phases(double *seconds, uint32_t n);
+
 int ogb_graph_create(ogb_graph **g);
 void ogb_graph_destroy(ogb_graph *g);
 /* Sort (SORT_TYPE semantics) and build both CSR directions from device edge

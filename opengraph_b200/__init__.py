@@ -216,6 +216,7 @@ _DEVICE_API = [
     ("ogb_last_error", C.c_char_p, []),
     ("ogb_weighted_layout", C.c_int, []),
     ("ogb_set_quiet", None, [C.c_int]),
+    ("ogb_dropin_bfs_phases", C.c_int, [C.POINTER(C.c_double), u32]),
     ("ogb_graph_create", C.c_int, [C.POINTER(vp)]),
     ("ogb_graph_destroy", None, [vp]),
     ("ogb_graph_build", C.c_int, [vp, vp, vp, vp, u32, u32, u32, vp]),

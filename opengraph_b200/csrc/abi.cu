@@ -19,6 +19,7 @@
 #include <sys/mman.h>
 #include <sys/stat.h>
 #include <sys/time.h>
+#include <emmintrin.h>
 #include <omp.h>
 #include <unistd.h>
 
@@ -234,7 +235,7 @@ static int d2h(void* h, const void* d, size_t n, cudaStream_t s) {
 struct ogb_graph {
   DevGraph g;
   DevBuf d_parents, d_distances, d_ranks;  // result arrays of the drop-in calls
-  DevBuf d_pack, d_pack_tmp;               // packed BFS result and its scratch
+  DevBuf d_depth8;                         // BFS depths as bytes, for the host copy
 };
 
 namespace {
@@ -1011,12 +1012,27 @@ extern "C" void freeBFSStats(struct BFSStats* st) {
 
 static BfsResult g_last_bfs;  // level trace of the last drop-in BFS
 
-// Pinned staging of packed BFS results (one per process, grows).
+// Wall-clock phases of the last drop-in BFS call, in seconds (see
+// ogb_dropin_bfs_phases in ogb200_device.h).
+static double g_bfs_phase[OGB_DROPIN_BFS_PHASES];
+
+// 32 consecutive int32 values to 128-byte-aligned memory with non-temporal
+// 16-byte stores: the result arrays are written whole and not read again by
+// this call, so bypassing the cache saves the read-for-ownership of every
+// line (half of the memory traffic of an ordinary store).
+static inline void stream32(void* dst, const int32_t* src) {
+  __m128i* d = reinterpret_cast<__m128i*>(dst);
+  const __m128i* q = reinterpret_cast<const __m128i*>(src);
+#pragma unroll
+  for (int i = 0; i < 8; i++) _mm_stream_si128(d + i, _mm_loadu_si128(q + i));
+}
+
+// Pinned staging of BFS results (one per process, grows).
 namespace {
-struct PackStage {
-  static constexpr int kEv = 17;
+struct ResultStage {
+  static constexpr int kEv = 17;  // one for the depths, the rest for parent chunks
   std::mutex mu;
-  uint32_t* h = nullptr;
+  unsigned char* h = nullptr;
   size_t bytes = 0;
   cudaEvent_t ev[kEv] = {};
   int reserve(size_t n) {
@@ -1031,100 +1047,60 @@ struct PackStage {
     return OK;
   }
 };
-PackStage& pack_stage() {
-  static PackStage p;
+ResultStage& result_stage() {
+  static ResultStage p;
   return p;
 }
 }  // namespace
 
-// Expand packed tiles [t0, t1) into the reference's arrays: reached vertices
-// take their parent and depth, the others the -out_degree (or -1) sentinel
-// and depth 0; the DualOrder parent copy gets the sentinel everywhere
-// (BFS.c:58-74).  One pass, one team of host threads.
-static void expand_tiles(const BfsPackLayout& L, uint32_t V, const uint32_t* hp, const uint32_t* od, int* parents,
-                         uint32_t* dist, size_t t0, size_t t1) {
-  if (t1 <= t0) return;
-  const uint32_t* off = hp + L.off_words;
-  const uint32_t* bm = hp + L.bitmap_words;
-  const uint8_t* d8 = reinterpret_cast<const uint8_t*>(hp + L.d8_words);
-  const int32_t* par = reinterpret_cast<const int32_t*>(hp + L.par_words);
-  const long nt = (long)(t1 - t0);
-#pragma omp parallel for num_threads(host_threads()) schedule(dynamic, 1)
-  for (long k = 0; k < nt; k++) {
-    const size_t t = t0 + (size_t)k;
-    const int32_t* pp = par + off[t];
-    const size_t v0 = t * kPackTile, v1 = std::min<size_t>(V, v0 + kPackTile);
-    // one bitmap word (32 vertices) at a time; whole-word cases without a
-    // per-vertex branch
-    for (size_t w0 = v0; w0 < v1; w0 += 32) {
-      const uint32_t word = bm[w0 >> 5];
-      const size_t we = std::min(v1, w0 + 32);
-      if (word == 0) {
-        for (size_t v = w0; v < we; v++) {
-          const uint32_t d = od[v];
-          parents[v] = d ? -(int)d : -1;
-          dist[v] = 0;
-        }
-      } else if (word == 0xFFFFFFFFu && we == w0 + 32) {
-        for (size_t v = w0; v < we; v++) {
-          parents[v] = pp[v - w0];
-          dist[v] = d8[v];
-        }
-        pp += 32;
-      } else {
-        for (size_t v = w0; v < we; v++) {
-          const uint32_t d = od[v];
-          const uint32_t bit = (word >> (v - w0)) & 1u;
-          const int reached_parent = *pp;  // read ahead; used only when bit
-          parents[v] = bit ? reached_parent : (d ? -(int)d : -1);
-          dist[v] = bit ? (uint32_t)d8[v] : 0u;
-          pp += bit;
-        }
-      }
-    }
-  }
-}
-
-// The result of a search into host arrays: packed on the device (about
-// 12 MB instead of 32 MB at V = 4M; the host link is the bottleneck of a
-// call), copied in pieces, expanded by host threads as the pieces land.
-static int bfs_result_to_host(ogb_graph* dg, uint32_t V, uint32_t levels, const uint32_t* od, int* parents,
-                              uint32_t* dist, cudaStream_t s) {
+// The result of a search into the reference's host arrays.  The device
+// arrays already hold the reference's values (parents: the tree, with the
+// -out_degree / -1 sentinels of unreached vertices; depth 0 for those), so
+// the host only copies.  Depths travel as one byte per vertex when the search
+// has fewer than 255 levels (V bytes instead of 4V on the host link) and are
+// widened by the host threads while the parents, copied whole in chunks, are
+// still on the link; each chunk is copied out by all threads as it lands.
+static int bfs_result_to_host(ogb_graph* dg, uint32_t V, uint32_t levels, int* parents, uint32_t* dist,
+                              cudaStream_t s) {
   if (levels >= 255) {  // depths do not fit a byte: plain copies
     OGB_TRY(d2h(parents, dg->d_parents.p, (size_t)V * 4, s));
     OGB_TRY(d2h(dist, dg->d_distances.p, (size_t)V * 4, s));
     return OK;
   }
-  const BfsPackLayout L = bfs_pack_layout(V);
-  OGB_TRY(dg->d_pack.alloc(L.max_words * 4));
-  OGB_TRY(dg->d_pack_tmp.alloc(bfs_pack_tmp_words(V) * 4));
-  OGB_TRY(bfs_pack(V, dg->d_parents.as<int32_t>(), dg->d_distances.as<uint32_t>(), dg->d_pack.as<uint32_t>(),
-                   dg->d_pack_tmp.as<uint32_t>(), s));
-  PackStage& ps = pack_stage();
-  std::lock_guard<std::mutex> lk(ps.mu);
-  OGB_TRY(ps.reserve(L.max_words * 4));
-  const uint32_t* dp = dg->d_pack.as<uint32_t>();
-  OGB_CUDA(cudaMemcpyAsync(ps.h, dp, L.par_words * 4, cudaMemcpyDeviceToHost, s));
-  OGB_CUDA(cudaStreamSynchronize(s));
-  const uint32_t R = ps.h[L.off_words + L.tiles];
-  const size_t chunk = std::max<size_t>(size_t(1) << 19, ((size_t)R + PackStage::kEv - 2) / (PackStage::kEv - 1));
-  const size_t nchunks = ((size_t)R + chunk - 1) / chunk;
-  for (size_t c = 0; c < nchunks; c++) {
-    const size_t a = L.par_words + c * chunk, n = std::min(chunk, (size_t)R - c * chunk);
-    OGB_CUDA(cudaMemcpyAsync(ps.h + a, dp + a, n * 4, cudaMemcpyDeviceToHost, s));
-    OGB_CUDA(cudaEventRecord(ps.ev[c], s));
+  const size_t d8_bytes = ((size_t)V + 3) / 4 * 4;
+  OGB_TRY(dg->d_depth8.alloc(d8_bytes));
+  OGB_TRY(bfs_depth_bytes(V, dg->d_distances.as<uint32_t>(), dg->d_depth8.as<uint8_t>(), s));
+  ResultStage& rs = result_stage();
+  std::lock_guard<std::mutex> lk(rs.mu);
+  OGB_TRY(rs.reserve(d8_bytes + (size_t)V * 4));
+  const unsigned char* h8 = rs.h;
+  int32_t* hp = reinterpret_cast<int32_t*>(rs.h + d8_bytes);
+  const int32_t* dp = dg->d_parents.as<int32_t>();
+  OGB_CUDA(cudaMemcpyAsync(rs.h, dg->d_depth8.p, d8_bytes, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaEventRecord(rs.ev[0], s));
+  const size_t nch = ResultStage::kEv - 1;
+  const size_t chunk = std::max<size_t>(1, ((size_t)V + nch - 1) / nch);  // vertices per chunk
+  size_t nchunks = 0;
+  for (size_t lo = 0; lo < V && nchunks < nch; lo += chunk, nchunks++) {
+    const size_t n = std::min(chunk, (size_t)V - lo);
+    OGB_CUDA(cudaMemcpyAsync(hp + lo, dp + lo, n * 4, cudaMemcpyDeviceToHost, s));
+    OGB_CUDA(cudaEventRecord(rs.ev[1 + nchunks], s));
   }
-  const uint32_t* off = ps.h + L.off_words;
-  size_t done = 0;
-  for (size_t c = 0; c < nchunks; c++) {
-    OGB_CUDA(cudaEventSynchronize(ps.ev[c]));
-    const size_t recv = std::min((size_t)R, (c + 1) * chunk);
-    size_t hi = done;
-    while (hi < L.tiles && off[hi + 1] <= recv) hi++;
-    expand_tiles(L, V, ps.h, od, parents, dist, done, hi);
-    done = hi;
+  int failed = 0;
+#pragma omp parallel num_threads(host_threads()) reduction(| : failed)
+  {
+    const size_t tid = (size_t)omp_get_thread_num(), nth = (size_t)omp_get_num_threads();
+    if (cudaEventSynchronize(rs.ev[0]) != cudaSuccess) failed = 1;
+    const size_t lo = (size_t)V * tid / nth, hi = (size_t)V * (tid + 1) / nth;
+    for (size_t v = lo; v < hi; v++) dist[v] = h8[v];
+    for (size_t c = 0; c < nchunks; c++) {
+      if (cudaEventSynchronize(rs.ev[1 + c]) != cudaSuccess) failed = 1;
+      const size_t clo = c * chunk, cn = std::min(chunk, (size_t)V - clo);
+      const size_t a = clo + cn * tid / nth, b = clo + cn * (tid + 1) / nth;
+      if (b > a) memcpy(parents + a, hp + a, (b - a) * 4);
+    }
   }
-  expand_tiles(L, V, ps.h, od, parents, dist, done, L.tiles);
+  if (failed) return fail(ERR_CUDA, "bfs result copy: %s", cudaGetErrorString(cudaGetLastError()));
   return OK;
 }
 
@@ -1142,6 +1118,7 @@ static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, 
   }
   // parents, distances and the DualOrder parent copy (its initial sentinels,
   // BFS.c:64-73) are written whole from the device result.
+  const double t_call = now_s();
   BFSStats* st = bfs_stats_alloc(V);
   const uint32_t* od = graph->vertices->out_degree;
   const uint32_t* labels = graph->sorted_edges_array ? graph->sorted_edges_array->label_array : nullptr;
@@ -1162,26 +1139,45 @@ static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, 
   OGB_MUST(dg->d_distances.alloc((size_t)V * 4 + 4));
   BfsResult& r = g_last_bfs;
   const double t0 = now_s();
+  g_bfs_phase[1] = t0 - t_call;
   // The DualOrder parent copy keeps its initial sentinels (BFS.c:64-73): the
-  // other host threads write them while thread 0 runs the device search.
+  // other host threads write them (streamed, 32 vertices at a time, ranges
+  // split on 32-vertex boundaries) while thread 0 runs the device search.
   int run_status = OK;
   int* dual = st->parents_DualOrder;
+  double t_search = 0.0, t_dual = 0.0;
 #pragma omp parallel num_threads(host_threads())
   {
     const int tid = omp_get_thread_num(), nth = omp_get_num_threads();
     if (tid == 0) {
       run_status = bfs_run(dg->g, (uint32_t)a->source, mode, dg->d_parents.as<int32_t>(),
                            dg->d_distances.as<uint32_t>(), &r, !quiet(), bitmap_nf, s);
+      t_search = now_s() - t0;
     }
     if (tid > 0 || nth == 1) {
       const size_t parts = nth > 1 ? (size_t)(nth - 1) : 1, me = nth > 1 ? (size_t)(tid - 1) : 0;
-      const size_t lo = (size_t)V * me / parts, hi = (size_t)V * (me + 1) / parts;
-      for (size_t v = lo; v < hi; v++) dual[v] = od[v] ? -(int)od[v] : -1;
+      const size_t words = ((size_t)V + 31) / 32;
+      const size_t lo = std::min<size_t>(V, words * me / parts * 32), hi = std::min<size_t>(V, words * (me + 1) / parts * 32);
+      alignas(16) int32_t buf[32];
+      size_t v = lo;
+      for (; v + 32 <= hi; v += 32) {
+        for (int i = 0; i < 32; i++) buf[i] = od[v + i] ? -(int)od[v + i] : -1;
+        stream32(dual + v, buf);
+      }
+      for (; v < hi; v++) dual[v] = od[v] ? -(int)od[v] : -1;
+      _mm_sfence();
+      if (tid == 1 || nth == 1) t_dual = now_s() - t0;
     }
   }
   OGB_MUST(run_status);
   const double t_trav = now_s() - t0;
-  OGB_MUST(bfs_result_to_host(dg, V, (uint32_t)r.nlevels, od, st->parents, st->distances, s));
+  g_bfs_phase[2] = t_search;
+  g_bfs_phase[3] = t_dual;
+  g_bfs_phase[4] = t_trav;
+  const double t1 = now_s();
+  OGB_MUST(bfs_result_to_host(dg, V, (uint32_t)r.nlevels, st->parents, st->distances, s));
+  g_bfs_phase[5] = now_s() - t1;
+  g_bfs_phase[0] = now_s() - t_call;
   st->processed_nodes = r.processed_nodes;
   st->iteration = r.iteration;
   st->time_total = t_trav;
@@ -1378,6 +1374,12 @@ extern "C" uint32_t generateRandomRootGraphCSR(mt19937state* mt, struct GraphCSR
 }
 
 // ------------------------------------------------------------- device API ---
+
+extern "C" int ogb_dropin_bfs_phases(double* seconds, uint32_t n) {
+  if (!seconds) return ogb::fail(ogb::ERR_ARG, "null output");
+  for (uint32_t i = 0; i < n && i < OGB_DROPIN_BFS_PHASES; i++) seconds[i] = g_bfs_phase[i];
+  return ogb::OK;
+}
 
 extern "C" const char* ogb_last_error(void) { return ogb::last_error(); }
 extern "C" int ogb_weighted_layout(void) { return OGB200_WEIGHTED; }

@@ -98,7 +98,7 @@ struct BfsCtl {
   unsigned long long edges;  // bottom-up: edges examined
   unsigned long long reached_edges;
   uint32_t reached;
-  uint32_t pad;
+  uint32_t maxdeg;            // largest out-degree on the next expansion list
   unsigned long long fedges;  // out-edges of the vertices the step discovered
 };
 
@@ -112,7 +112,8 @@ struct BfsCtrl {
   uint32_t bm_r, bm_w, bm_c, depth;
   uint32_t iteration, processed, td_steps, bu_steps;
   uint32_t nlevels, epoch, overflow, qcount_prev;
-  uint32_t ul_cand0, pad_c;          // 1: the unvisited list is the graph's cached in-edge list
+  uint32_t ul_cand0;                 // 1: the unvisited list is the graph's cached in-edge list
+  uint32_t lmax;                     // largest out-degree on the expansion list
   unsigned long long edges_examined;
   unsigned long long fedges;         // out-edges of the current frontier
   unsigned long long edges_visited;  // out-edges of every visited vertex
@@ -347,10 +348,15 @@ __device__ __forceinline__ void bu_flush(BuSmem& sm, uint32_t* list_out, uint32_
   }
   __syncthreads();
 }
+// A flat top-down step's appends: each of a CTA's threads expands one list
+// entry of at most kFlatMaxDeg out-edges per pass.
+constexpr uint32_t kFlatMaxDeg = 16;
+constexpr uint32_t kFlatCap = 256 * kFlatMaxDeg;
 union BfsSmem {
   ScanSmem scan;
   TdSmem td;
   BuSmem bu;
+  BlockAppend<kFlatCap> flat;
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -431,43 +437,50 @@ __device__ __forceinline__ uint32_t scan_block_excl(uint32_t v, uint32_t* s_w, u
   return (warp ? s_w[warp - 1] : 0) + x - v;
 }
 
-// Per-CTA sums of two 64-bit values in one reduction (one pair of
-// barriers); the totals are valid in thread 0.  A step's 32-bit counts travel
-// packed two to a value (low | high << 32): each half sums to less than 2^32
-// in a CTA (at most V vertices or E edges), so no carry crosses halves.
-// s_red holds 2 * (warps per CTA) entries.
-__device__ __forceinline__ void block_sum2(unsigned long long& a, unsigned long long& b, unsigned long long* s_red) {
+// Per-CTA sums of two 64-bit values and the maximum of a 32-bit one in one
+// reduction (one pair of barriers); the results are valid in thread 0.  A
+// step's 32-bit counts travel packed two to a value (low | high << 32): each
+// half sums to less than 2^32 in a CTA (at most V vertices or E edges), so
+// no carry crosses halves.  s_red holds kRedSlots * (warps per CTA) entries.
+constexpr int kRedSlots = 3;
+__device__ __forceinline__ void block_sum2_max(unsigned long long& a, unsigned long long& b, uint32_t& m,
+                                               unsigned long long* s_red) {
 #pragma unroll
   for (int o = 16; o; o >>= 1) {
     a += __shfl_down_sync(0xffffffffu, a, o);
     b += __shfl_down_sync(0xffffffffu, b, o);
   }
+  m = __reduce_max_sync(0xffffffffu, m);
   const uint32_t warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   __syncthreads();
   if (lane_id() == 0) {
     s_red[warp] = a;
     s_red[nw + warp] = b;
+    s_red[2 * nw + warp] = m;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     a = b = 0;
+    m = 0;
     for (uint32_t i = 0; i < nw; i++) {
       a += s_red[i];
       b += s_red[nw + i];
+      m = max(m, (uint32_t)s_red[2 * nw + i]);
     }
   }
 }
 
-// A top-down step's counters: mf and the discoveries, packed, and the
-// discoveries' out-edges.
+// A top-down step's counters: mf and the discoveries, packed, the
+// discoveries' out-edges, and the largest out-degree it put on the list.
 __device__ __forceinline__ void td_publish(BfsCtl* ctl, uint32_t mf, uint32_t found, unsigned long long fed,
-                                           unsigned long long* s_red) {
+                                           uint32_t mx, unsigned long long* s_red) {
   unsigned long long a = (unsigned long long)mf | ((unsigned long long)found << 32), b = fed;
-  block_sum2(a, b, s_red);
+  block_sum2_max(a, b, mx, s_red);
   if (threadIdx.x == 0) {
     if ((uint32_t)a) atomicAdd(&ctl->mf, (uint32_t)a);
     if (a >> 32) atomicAdd(&ctl->qnext, (uint32_t)(a >> 32));
     if (b) atomicAdd(&ctl->fedges, b);
+    if (mx) atomicMax(&ctl->maxdeg, mx);
   }
 }
 
@@ -577,7 +590,7 @@ template <bool kDepthKnown, class TS>
 __device__ __forceinline__ void expand_edges(const BfsBufs& b, uint32_t e0, uint32_t e1, uint32_t cnt,
                                              int32_t* parents, uint32_t* distances, uint32_t dnext, uint32_t* bm_w,
                                              uint32_t* all_out, TS& sm, uint32_t& mf, uint32_t& found,
-                                             unsigned long long& fed) {
+                                             unsigned long long& fed, uint32_t& mx) {
   static_assert(kDepthKnown || TS::kHost, "entry depths live in the host-step shared memory");
   constexpr int K = kExpTile / kExpT;
   uint32_t u[K], src[K], dd[K];
@@ -603,9 +616,15 @@ __device__ __forceinline__ void expand_edges(const BfsBufs& b, uint32_t e0, uint
       if constexpr (!kDepthKnown) dd[k] = sm.d[lo];
     }
   }
+  // parents and out-degrees together (the out-degree of a vertex this step
+  // does not claim is not used, but loading it here takes it off the chain)
   int32_t p[K];
+  uint32_t od[K];
 #pragma unroll
-  for (int k = 0; k < K; k++) p[k] = ok[k] ? parents[u[k]] : 0;
+  for (int k = 0; k < K; k++) {
+    p[k] = ok[k] ? parents[u[k]] : 0;
+    od[k] = ok[k] ? __ldg(&b.out_degree[u[k]]) : 0u;
+  }
   bool won[K];
 #pragma unroll
   for (int k = 0; k < K; k++) won[k] = ok[k] && p[k] < 0 && atomicCAS(&parents[u[k]], p[k], (int32_t)src[k]) == p[k];
@@ -619,9 +638,11 @@ __device__ __forceinline__ void expand_edges(const BfsBufs& b, uint32_t e0, uint
       if constexpr (TS::kHost) {
         if (all_out) ba_push(sm.q_all, u[k]);
       }
-      const uint32_t od = __ldg(&b.out_degree[u[k]]);
-      fed += od;
-      if (od) ba_push(sm.q_list, u[k]);
+      fed += od[k];
+      if (od[k]) {
+        ba_push(sm.q_list, u[k]);
+        mx = max(mx, od[k]);
+      }
     }
   }
 }
@@ -640,7 +661,7 @@ __device__ void td_expand_phase(const BfsBufs& b, const uint32_t* list, uint32_t
   if (blockIdx.x >= ntiles) return;
   ba_init(sm.q_list);
   if constexpr (TS::kHost) ba_init(sm.q_all);
-  uint32_t mf = 0, found = 0;
+  uint32_t mf = 0, found = 0, mx = 0;
   unsigned long long fed = 0;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const uint32_t e0 = t * kExpTile;
@@ -656,14 +677,14 @@ __device__ void td_expand_phase(const BfsBufs& b, const uint32_t* list, uint32_t
       if constexpr (!kDepthKnown) sm.d[k] = b.fdist[i0 + k];
     }
     __syncthreads();
-    expand_edges<kDepthKnown>(b, e0, e1, cnt, parents, distances, dnext, bm_w, all_out, sm, mf, found, fed);
+    expand_edges<kDepthKnown>(b, e0, e1, cnt, parents, distances, dnext, bm_w, all_out, sm, mf, found, fed, mx);
     // at most kExpTile discoveries per tile: flush every tile
     ba_flush(sm.q_list, next_list, &ctl->lnext);
     if constexpr (TS::kHost) {
       if (all_out) ba_flush(sm.q_all, all_out, &ctl->all_count);
     }
   }
-  td_publish(ctl, mf, found, fed, s_red);
+  td_publish(ctl, mf, found, fed, mx, s_red);
 }
 
 // A top-down step over a list of at most kExpTile entries: every CTA loads
@@ -702,15 +723,15 @@ __device__ void td_small_phase(const BfsBufs& b, const uint32_t* list, uint32_t*
   const uint32_t ntiles = (total + kExpTile - 1) / kExpTile;
   if (blockIdx.x >= ntiles) return;
   ba_init(sm.q_list);
-  uint32_t mf = 0, found = 0;
+  uint32_t mf = 0, found = 0, mx = 0;
   unsigned long long fed = 0;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const uint32_t e0 = t * kExpTile;
     const uint32_t e1 = min(e0 + kExpTile, total);
-    expand_edges<true>(b, e0, e1, n, parents, distances, dnext, bm_w, nullptr, sm, mf, found, fed);
+    expand_edges<true>(b, e0, e1, n, parents, distances, dnext, bm_w, nullptr, sm, mf, found, fed, mx);
     ba_flush(sm.q_list, next_list, &ctl->lnext);
   }
-  td_publish(ctl, mf, found, fed, s_red);
+  td_publish(ctl, mf, found, fed, mx, s_red);
 }
 
 // A top-down step over a list of kExpTile < n <= kMidList entries, in one
@@ -743,7 +764,7 @@ __device__ void td_mid_phase(const BfsBufs& b, const uint32_t* list, uint32_t* n
     return;
   }
   ba_init(sm.q_list);
-  uint32_t mf = 0, found = 0;
+  uint32_t mf = 0, found = 0, mx = 0;
   unsigned long long fed = 0;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const uint32_t e0 = t * kExpTile;
@@ -773,12 +794,78 @@ __device__ void td_mid_phase(const BfsBufs& b, const uint32_t* list, uint32_t* n
       o += deg[k];
     }
     __syncthreads();
-    expand_edges<true>(b, e0, e1, cnt, parents, distances, dnext, bm_w, nullptr, sm, mf, found, fed);
+    expand_edges<true>(b, e0, e1, cnt, parents, distances, dnext, bm_w, nullptr, sm, mf, found, fed, mx);
     // at most kExpTile discoveries per tile: flush every tile (its barriers
     // also end this tile's use of the staged entries)
     ba_flush(sm.q_list, next_list, &ctl->lnext);
   }
-  td_publish(ctl, mf, found, fed, s_red);
+  td_publish(ctl, mf, found, fed, mx, s_red);
+}
+
+// A top-down step over a list longer than kMidList whose entries all have at
+// most kFlatMaxDeg out-edges (the largest out-degree on the list is counted
+// by the step that made it): one phase, no scan.  Every thread takes one
+// list entry per pass and expands its out-edges four at a time (neighbour
+// ids, then parents and out-degrees, then the claiming CASes).  This is the
+// usual shape of the top-down steps after a bottom-up phase: thousands of
+// low-degree vertices and few edges, where a two-phase step pays a whole
+// scan phase and its grid barrier for a handful of edge tiles.
+__device__ void td_flat_phase(const BfsBufs& b, const uint32_t* list, uint32_t* next_list, uint32_t n,
+                              unsigned long long total, int32_t* parents, uint32_t* distances, uint32_t dnext,
+                              uint32_t* bm_w, BfsCtl* ctl, uint32_t* err, BlockAppend<kFlatCap>& q,
+                              unsigned long long* s_red) {
+  constexpr int K = 4;
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->total_edges = (uint32_t)total;
+  if ((uint64_t)blockIdx.x * blockDim.x >= n) return;  // CTA-uniform: no entry for this CTA
+  ba_init(q);
+  uint32_t mf = 0, found = 0, mx = 0;
+  unsigned long long fed = 0;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const uint32_t i = base + threadIdx.x;
+    uint32_t src = 0;
+    uint2 r = make_uint2(0u, 0u);
+    if (i < n) {
+      src = list[i];
+      r = __ldg(&b.rows_f[src]);
+      if (r.y > kFlatMaxDeg) {  // the list's maximum said otherwise: refuse rather than overflow
+        atomicExch(err, (uint32_t)ERR_STATE);
+        r.y = 0;
+      }
+    }
+    for (uint32_t j0 = 0; j0 < r.y; j0 += K) {
+      uint32_t u[K], od[K];
+      int32_t pp[K];
+      bool ok[K];
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        ok[k] = j0 + k < r.y;
+        u[k] = ok[k] ? (__ldg(&b.nbr_f[r.x + j0 + k]) & 0x3FFFFFFFu) : 0u;
+      }
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        pp[k] = ok[k] ? parents[u[k]] : 0;
+        od[k] = ok[k] ? __ldg(&b.out_degree[u[k]]) : 0u;
+      }
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        if (ok[k] && pp[k] < 0 && atomicCAS(&parents[u[k]], pp[k], (int32_t)src) == pp[k]) {
+          distances[u[k]] = dnext;
+          mf += (uint32_t)(-pp[k]);
+          found++;
+          atomicOr(&bm_w[u[k] >> 5], 1u << (u[k] & 31));
+          fed += od[k];
+          if (od[k]) {
+            ba_push(q, u[k]);
+            mx = max(mx, od[k]);
+          }
+        }
+      }
+    }
+    // at most blockDim.x * kFlatMaxDeg claims per pass: flush every pass
+    ba_flush(q, next_list, &ctl->lnext);
+  }
+  td_publish(ctl, mf, found, fed, mx, s_red);
 }
 
 // ------------------------------------------------------------ bottom-up ----
@@ -812,7 +899,7 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
   __syncthreads();
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
   const uint32_t count = kDense ? b.V : ul_count;
-  uint32_t nf = 0, edges = 0;
+  uint32_t nf = 0, edges = 0, mx = 0;
   unsigned long long fed = 0;
   // each CTA takes one contiguous, equal range of candidates (a multiple of
   // 32, so a dense step's ballot words never straddle two CTAs)
@@ -869,7 +956,10 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
           if (!kDense) atomicOr(&bm_next[v[k] >> 5], 1u << (v[k] & 31));
           const uint32_t od = __ldg(&b.out_degree[v[k]]);
           fed += od;
-          if (od) bu_push_list(sm, v[k]);
+          if (od) {
+            bu_push_list(sm, v[k]);
+            mx = max(mx, od);
+          }
         } else if (row[k].y > kFirst) {
           edges += kFirst;
           const uint32_t h = warp_atomic_inc(&sm.nheavy);
@@ -916,7 +1006,10 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
             edges += j + first + 1 - j0;
             const uint32_t od = __ldg(&b.out_degree[hv]);
             fed += od;
-            if (od) bu_push_list(sm, hv);
+            if (od) {
+              bu_push_list(sm, hv);
+              mx = max(mx, od);
+            }
           }
           hit_row = true;
           break;
@@ -934,11 +1027,12 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
   {
     // nf and the edges examined, packed, and the discoveries' out-edges
     unsigned long long a = (unsigned long long)nf | ((unsigned long long)edges << 32), c = fed;
-    block_sum2(a, c, s_red);
+    block_sum2_max(a, c, mx, s_red);
     if (threadIdx.x == 0) {
       if ((uint32_t)a) atomicAdd(&ctl->nf, (uint32_t)a);
       if (a >> 32) atomicAdd(&ctl->edges, a >> 32);
       if (c) atomicAdd(&ctl->fedges, c);
+      if (mx) atomicMax(&ctl->maxdeg, mx);
     }
   }
 }
@@ -1010,6 +1104,7 @@ __device__ __forceinline__ void load_ctl(const BfsCtl* p, BfsCtl& out) {
   out.total_edges = v->total_edges;
   out.edges = v->edges;
   out.fedges = v->fedges;
+  out.maxdeg = v->maxdeg;
 }
 
 __device__ __forceinline__ void zero_ctl(BfsCtl* p) {
@@ -1136,6 +1231,7 @@ __device__ void ctrl_finish_td(BfsCtrl& c, uint32_t total_edges, const BfsCtl& k
   c.mf = k.mf;
   c.qcount = k.qnext;
   c.lsize = k.lnext;
+  c.lmax = k.maxdeg;
   c.fedges = k.fedges;
   c.edges_visited += k.fedges;
   c.par_l ^= 1u;
@@ -1158,6 +1254,7 @@ __device__ void ctrl_finish_bu(BfsCtrl& c, const BfsCtl& k, BfsDevState* st, boo
   c.par_ul ^= 1u;
   c.qcount = k.nf;
   c.lsize = k.lnext;
+  c.lmax = k.maxdeg;
   c.fedges = k.fedges;
   c.edges_visited += k.fedges;
   c.par_l ^= 1u;
@@ -1215,6 +1312,7 @@ __global__ void __launch_bounds__(256) bfsk_init(BfsBufs b, BfsDevState* st, uin
     c.epoch = epoch;
     c.fedges = d;
     c.edges_visited = d;
+    c.lmax = d;
     // the first bottom-up step walks the cached list of vertices with
     // in-edges (a vertex without any can never be found bottom-up); the
     // dense-probe mode walks every vertex in every step
@@ -1249,6 +1347,7 @@ __global__ void bfsk_set_roots(BfsBufs b, BfsDevState* st, const uint32_t* __res
     parents[r] = (int32_t)r;
     b.bm[0][r >> 5] |= 1u << (r & 31);
     const uint32_t d = b.out_degree[r];
+    c.lmax = max(c.lmax, d);
     c.qcount++;
     c.processed++;
     c.mf += d;
@@ -1267,7 +1366,7 @@ __global__ void bfsk_set_roots(BfsBufs b, BfsDevState* st, const uint32_t* __res
 __global__ void __launch_bounds__(kSearchT, 4) bfsk_search(BfsBufs b, BfsDevState* st) {
   __shared__ __align__(16) BfsSmem sm;
   __shared__ BfsCtrl S;
-  __shared__ unsigned long long s_red[2 * kSearchT / 32];
+  __shared__ unsigned long long s_red[kRedSlots * kSearchT / 32];
   __shared__ uint32_t s_act, s_ok;
   __shared__ unsigned long long s_t0;
   __shared__ float s_tail[kPolTail];
@@ -1348,6 +1447,11 @@ __global__ void __launch_bounds__(kSearchT, 4) bfsk_search(BfsBufs b, BfsDevStat
                      s_red);
         if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
         total = ld_volatile_u32(&ctl[p % 3].total_edges);
+      } else if (S.lmax <= kFlatMaxDeg) {
+        td_flat_phase(b, list, next, n, S.fedges, parents, distances, dnext, bm_w, &ctl[p % 3], &st->err, sm.flat,
+                      s_red);
+        if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
+        total = ld_volatile_u32(&ctl[p % 3].total_edges);
       } else {
         td_scan_phase<true>(b, list, n, distances, S.epoch, &ctl[p % 3], &st->err, sm.scan);
         if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
@@ -1370,9 +1474,9 @@ __global__ void __launch_bounds__(kSearchT, 4) bfsk_search(BfsBufs b, BfsDevStat
         bu_step_phase<true>(b, b.bm[S.bm_r], b.bm[S.bm_w], b.bm[S.bm_c], nullptr, 0, b.ul[S.par_ul ^ 1u],
                             b.list[S.par_l ^ 1u], parents, distances, dnext, &ctl[p % 3], sm.bu, s_red);
       else
-        bu_step_phase<false>(b, b.bm[S.bm_r], b.bm[S.bm_w], b.bm[S.bm_c], S.ul_cand0 ? b.cand0 : b.ul[S.par_ul], S.ul_size,
-                             b.ul[S.par_ul ^ 1u], b.list[S.par_l ^ 1u], parents, distances, dnext, &ctl[p % 3],
-                             sm.bu, s_red);
+        bu_step_phase<false>(b, b.bm[S.bm_r], b.bm[S.bm_w], b.bm[S.bm_c], S.ul_cand0 ? b.cand0 : b.ul[S.par_ul],
+                             S.ul_size, b.ul[S.par_ul ^ 1u], b.list[S.par_l ^ 1u], parents, distances, dnext,
+                             &ctl[p % 3], sm.bu, s_red);
       if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
       if (threadIdx.x == 0) {
         BfsCtl k;
@@ -1397,7 +1501,7 @@ __global__ void __launch_bounds__(kExpT) bfsk_td_expand_host(BfsBufs b, BfsDevSt
                                                              int32_t* parents, uint32_t* distances,
                                                              uint32_t* all_out) {
   __shared__ TdSmemHost sm;
-  __shared__ unsigned long long s_red[2 * kExpT / 32];
+  __shared__ unsigned long long s_red[kRedSlots * kExpT / 32];
   td_expand_phase<false, TdSmemHost>(b, b.list[0], b.list[1], n, st->aux.total_edges, parents, distances, 0, nullptr, all_out,
                          &st->aux, sm, s_red);
 }
@@ -1435,104 +1539,31 @@ __global__ void __launch_bounds__(256) bfsk_reached(BfsBufs b, BfsDevState* st) 
   block_add_total<uint32_t>(&st->aux.reached, r, reinterpret_cast<uint32_t*>(s_red));
 }
 
-// ------------------------------------------------------------ packing ------
+// ------------------------------------------------------------ host copy ----
 
-// Reached bits (a warp per 1024 vertices: the ballot of step k is word k),
-// one-byte depths, and the reached count of every kPackTile-vertex tile.
-__global__ void __launch_bounds__(256) bfsk_pack_bits(uint32_t V, const int32_t* __restrict__ parents,
-                                                      const uint32_t* __restrict__ distances,
-                                                      uint32_t* __restrict__ bitmap, uint8_t* __restrict__ d8,
-                                                      uint32_t* __restrict__ tile_cnt) {
-  const uint32_t lane = lane_id();
-  const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
-  for (uint32_t wb = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); (uint64_t)wb * 1024 < V; wb += nwarps) {
-    const uint32_t base = wb * 1024;
-    uint32_t mine = 0;
-#pragma unroll 4
-    for (uint32_t k = 0; k < 32; k++) {
-      const uint32_t v = base + k * 32 + lane;
-      bool r = false;
-      if (v < V) {
-        r = parents[v] >= 0;
-        d8[v] = (uint8_t)distances[v];
-      }
-      const uint32_t word = __ballot_sync(0xffffffffu, r);
-      if (lane == k) mine = word;
-    }
-    if (base + lane * 32 < V) bitmap[wb * 32 + lane] = mine;
-    const uint32_t cnt = __reduce_add_sync(0xffffffffu, (uint32_t)__popc(mine));
-    if (lane == 0 && cnt) atomicAdd(&tile_cnt[base / kPackTile], cnt);
+// One byte of depth per vertex (a search of fewer than 255 levels): the host
+// copy moves V bytes of depths instead of 4V and widens them.
+__global__ void __launch_bounds__(256) bfsk_depth_bytes(uint32_t V, const uint32_t* __restrict__ distances,
+                                                        uchar4* __restrict__ out) {
+  const uint32_t n4 = (V + 3) / 4;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x) {
+    const uint32_t v = 4 * i;
+    uchar4 q;
+    q.x = (unsigned char)distances[v];
+    q.y = v + 1 < V ? (unsigned char)distances[v + 1] : 0;
+    q.z = v + 2 < V ? (unsigned char)distances[v + 2] : 0;
+    q.w = v + 3 < V ? (unsigned char)distances[v + 3] : 0;
+    out[i] = q;
   }
 }
 
-// Parents of the reached vertices, vertex order: a CTA per tile, a thread per
-// bitmap word (32 vertices), offsets by a block scan of the word counts.
-__global__ void __launch_bounds__(kPackTile / 32) bfsk_pack_parents(uint32_t V, const int32_t* __restrict__ parents,
-                                                                   const uint32_t* __restrict__ bitmap,
-                                                                   const uint32_t* __restrict__ tile_off,
-                                                                   int32_t* __restrict__ out) {
-  __shared__ uint32_t s_w[kPackTile / 32 / 32];
-  const uint32_t t = blockIdx.x;
-  const uint32_t w = t * (kPackTile / 32) + threadIdx.x;
-  const uint32_t word = ((uint64_t)w * 32 < V) ? bitmap[w] : 0u;
-  // block exclusive scan of popc(word)
-  const uint32_t c = __popc(word), lane = lane_id(), warp = threadIdx.x >> 5;
-  uint32_t x = c;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) s_w[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t y = lane < kPackTile / 32 / 32 ? s_w[lane] : 0u;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t z = __shfl_up_sync(0xffffffffu, y, o);
-      if (lane >= o) y += z;
-    }
-    if (lane < kPackTile / 32 / 32) s_w[lane] = y;
-  }
-  __syncthreads();
-  uint32_t o = tile_off[t] + (warp ? s_w[warp - 1] : 0u) + x - c;
-  uint32_t bits = word;
-  while (bits) {
-    const uint32_t i = (uint32_t)__ffs(bits) - 1;
-    out[o++] = parents[w * 32 + i];
-    bits &= bits - 1;
-  }
-}
-
-BfsPackLayout bfs_pack_layout(uint32_t V) {
-  BfsPackLayout L;
-  L.tiles = (V + kPackTile - 1) / kPackTile;
-  auto up4 = [](size_t x) { return (x + 3) & ~(size_t)3; };
-  L.off_words = 0;
-  L.bitmap_words = up4(L.tiles + 1);
-  L.d8_words = L.bitmap_words + up4(((size_t)V + 31) / 32);
-  L.par_words = L.d8_words + up4(((size_t)V + 3) / 4);
-  L.max_words = L.par_words + (size_t)V + 4;
-  return L;
-}
-
-int bfs_pack(uint32_t V, const int32_t* parents, const uint32_t* distances, uint32_t* out, uint32_t* tmp,
-             cudaStream_t s) {
-  const BfsPackLayout L = bfs_pack_layout(V);
-  uint32_t* tile_cnt = tmp;
-  uint32_t* scan_tmp = tmp + L.tiles + 4;
-  OGB_CUDA(cudaMemsetAsync(tile_cnt, 0, (L.tiles + 1) * 4, s));
-  bfsk_pack_bits<<<sm_count() * 8, 256, 0, s>>>(V, parents, distances, out + L.bitmap_words,
-                                                 reinterpret_cast<uint8_t*>(out + L.d8_words), tile_cnt);
-  OGB_CUDA(cudaGetLastError());
-  OGB_TRY(scan_exclusive_u32(tile_cnt, out + L.off_words, L.tiles, scan_tmp, s));
-  bfsk_pack_parents<<<L.tiles, kPackTile / 32, 0, s>>>(V, parents, out + L.bitmap_words, out + L.off_words,
-                                                      reinterpret_cast<int32_t*>(out + L.par_words));
+int bfs_depth_bytes(uint32_t V, const uint32_t* distances, uint8_t* out, cudaStream_t s) {
+  const uint32_t n4 = (V + 3) / 4;
+  const int grid = (int)std::min<uint32_t>(sm_count() * 8, std::max<uint32_t>(1, (n4 + 255) / 256));
+  bfsk_depth_bytes<<<grid, 256, 0, s>>>(V, distances, reinterpret_cast<uchar4*>(out));
   OGB_CUDA(cudaGetLastError());
   return OK;
 }
-
-size_t bfs_pack_tmp_words(uint32_t V) { return bfs_pack_layout(V).tiles + 8 + scan_tmp_words(bfs_pack_layout(V).tiles); }
 
 // ------------------------------------------------------------ drivers ------
 

@@ -207,19 +207,9 @@ struct PprResult {
 int ppr_run(DevGraph& g, const uint32_t* seeds, uint32_t nseeds, uint32_t max_iters, double epsilon, float* ranks,
             PprResult* res, cudaStream_t s);
 
-// Packed search result for a host copy: tile offsets (exclusive scan of the
-// reached count of every kPackTile-vertex tile, tiles + 1 words), the
-// reached bitmap, one byte of depth per vertex (valid when the search has
-// fewer than 255 levels) and the parents of the reached vertices in vertex
-// order; sections start at the word offsets below.  bfs.cu.
-constexpr uint32_t kPackTile = 8192;
-struct BfsPackLayout {
-  size_t tiles, off_words, bitmap_words, d8_words, par_words, max_words;
-};
-BfsPackLayout bfs_pack_layout(uint32_t V);
-size_t bfs_pack_tmp_words(uint32_t V);
-int bfs_pack(uint32_t V, const int32_t* parents, const uint32_t* distances, uint32_t* out, uint32_t* tmp,
-             cudaStream_t s);
+// Depths as bytes (out: V bytes, rounded up to a multiple of 4), for the host
+// copy of a search of fewer than 255 levels.  bfs.cu.
+int bfs_depth_bytes(uint32_t V, const uint32_t* distances, uint8_t* out, cudaStream_t s);
 
 }  // namespace ogb
 
