@@ -63,6 +63,17 @@ def rank_roots(outdeg, rank: int, n: int = NROOTS) -> list[int]:
     return [int(x) for x in rng.choice(cand, size=min(n, len(cand)), replace=False)]
 
 
+def workload_config(ws: int) -> dict:
+    """The benchmarked workload (the same for both arms)."""
+    V, E = 1 << SCALE, (1 << SCALE) * EDGE_FACTOR
+    return {"workload": f"RMAT scale {SCALE} (V={V}, E={E}), a/b/c/d=.57/.19/.19/.05, permuted ids, float32 weights; "
+                        f"DO-BFS from {NROOTS} seeded random roots with out-degree>0 per rank, each search timed "
+                        "individually",
+            "global_batch": NROOTS * ws, "seq_len": None, "parallelism": f"replicas{ws}",
+            "l2": "flushed (256 MB write) before every search",
+            "step": f"{NROOTS} DO-BFS searches"}
+
+
 def sort_passes(V: int) -> int:
     """Radix passes of the CSR build's byte model: ceil(ceil(log2 V) / 8)."""
     return -(-max(1, (V - 1).bit_length()) // 8)
@@ -293,12 +304,7 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic (seeded RMAT generator)",
-        "config": {"workload": f"RMAT scale {SCALE} (V={V}, E={E}), a/b/c/d=.57/.19/.19/.05, permuted ids, "
-                               f"float32 weights; DO-BFS from {NROOTS} seeded random roots with out-degree>0 "
-                               "per rank, each search timed individually",
-                   "global_batch": NROOTS * ws, "seq_len": None, "parallelism": f"replicas{ws}",
-                   "l2": "flushed (256 MB write) before every search",
-                   "step": f"{NROOTS} DO-BFS searches"},
+        "config": workload_config(ws),
         "roofline": {"bound": "hbm", "kernel": "bfsk_search (one DO-BFS search per launch)",
                      "achieved": round(search_gbs, 1), "peak": hbm_peak, "unit": "GB/s",
                      "frac": round(search_gbs / hbm_peak, 4), "peak_kind": peak_kind,
@@ -588,20 +594,22 @@ def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    # This arm runs the reference alone: the input is made by the oracle's
-    # restatement of the generator and written with numpy, so no product
-    # library is loaded into this process.
-    from oracle.oracle import Oracle, Reference, write_edge_file
+    # This arm runs the reference alone: the input file is written by a
+    # separate process (oracle/gen_rmat, the oracle's restatement of the
+    # generator), so this process loads nothing but the reference's build.
+    from oracle.oracle import HERE as ORACLE_DIR
+    from oracle.oracle import Reference
     if not Reference.available(True):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference CPU build) not present"}))
         return
-    s, d, w = Oracle().generate_rmat(SCALE, EDGE_FACTOR, SEED, weighted=True)
+    gen = os.path.join(ORACLE_DIR, "gen_rmat")
+    if not os.path.exists(gen):
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR, "gen_rmat"], check=True)
     V = 1 << SCALE
     ref = Reference(True)
     tmp = tempfile.mkdtemp()
     path = os.path.join(tmp, f"rmat{SCALE}.wbin")
-    write_edge_file(path, s, d, w)
-    del s, d, w
+    subprocess.run([gen, str(SCALE), str(EDGE_FACTOR), str(SEED), "1", path], check=True)
     cores = os.cpu_count()
     os.environ["OMP_NUM_THREADS"] = str(cores)
     rg = ref.build_graph(path, weighted_file=True)
@@ -633,7 +641,7 @@ def run_reference(args):
         "metric": METRIC, "value": round(val, 4), "unit": "GTEPS", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(T_tot * 1e3 / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded RMAT generator)",
-        "config": {"workload": f"RMAT scale {SCALE}, DO-BFS from seeded random roots", "parallelism": "openmp"},
+        "config": dict(workload_config(ws), parallelism="openmp (reference CPU build, all host cores)"),
         "impl": "reference",
         "cpu_baseline": {"value": round(val, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
                          "sample": sample},

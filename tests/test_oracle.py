@@ -190,3 +190,20 @@ def test_oracle_edge_file_writer_equals_product(og, tmp_path):
         write_edge_file(p1, s, d, w if weighted else None)
         og.write_edge_file(p2, s, d, w if weighted else None)
         assert open(p1, "rb").read() == open(p2, "rb").read()
+
+
+def test_gen_rmat_file_equals_product_file(og, tmp_path):
+    """oracle/gen_rmat (what bench.py's reference arm runs to make its input)
+    writes the same .wbin / .bin bytes as the product's generator + writer."""
+    import subprocess
+
+    from oracle.oracle import HERE
+    gen = os.path.join(HERE, "gen_rmat")
+    if not os.path.exists(gen):
+        subprocess.run(["make", "-s", "-C", HERE, "gen_rmat"], check=True)
+    for weighted in (True, False):
+        p1, p2 = str(tmp_path / "a"), str(tmp_path / "b")
+        subprocess.run([gen, "11", "16", "5", "1" if weighted else "0", p1], check=True)
+        s, d, w = og.generate_rmat(11, 16, 5, weighted=weighted)
+        og.write_edge_file(p2, s, d, w)
+        assert open(p1, "rb").read() == open(p2, "rb").read()
