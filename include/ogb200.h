@@ -146,6 +146,17 @@ struct PageRankStats
     double error_total;
 };
 
+/* 00_graph_bench/include/algorithms/openmp/SPMV.h:19-27 */
+struct SPMVStats
+{
+    uint32_t iterations;
+    struct Arguments *arguments;
+    uint32_t num_vertices;
+    float *vector_output;
+    float *vector_input;
+    double time_total;
+};
+
 /* 00_graph_bench/include/structures/bitmap.h:19-26 */
 struct Bitmap
 {
@@ -262,14 +273,38 @@ uint32_t bottomUpStepGraphCSR(struct GraphCSR *graph, struct Bitmap *bitmapCurr,
 struct PageRankStats *newPageRankStatsGraphCSR(struct GraphCSR *graph);
 /* pageRank.h:37 ; pageRank.c:167-177 */
 void freePageRankStats(struct PageRankStats *stats);
-/* pageRank.h:69 ; pageRank.c:871-936.  pushpull 0 pull, 1 push; other
- * values are the reference's fixed-point/quantized/data-driven variants,
- * which this library does not provide (message + NULL). */
+/* pageRank.h:69 ; pageRank.c:871-936.  pushpull 0 pull, 1 push, 6
+ * data-driven pull, 7 data-driven push, 8 data-driven pull-push; 2-5 and
+ * 9-13 are the reference's fixed-point / quantized variants, which this
+ * library does not provide (message + NULL); larger values pull. */
 struct PageRankStats *pageRankGraphCSR(struct Arguments *arguments, struct GraphCSR *graph);
 /* pageRank.h:70 ; pageRank.c:939-1062 */
 struct PageRankStats *pageRankPullGraphCSR(struct Arguments *arguments, struct GraphCSR *graph);
 /* pageRank.h:71 ; pageRank.c:1064-1186 */
 struct PageRankStats *pageRankPushGraphCSR(struct Arguments *arguments, struct GraphCSR *graph);
+/* pageRank.h:84 ; pageRank.c:2405-2564 */
+struct PageRankStats *pageRankDataDrivenPullGraphCSR(struct Arguments *arguments, struct GraphCSR *graph);
+/* pageRank.h:85 ; pageRank.c:2566-2721 */
+struct PageRankStats *pageRankDataDrivenPushGraphCSR(struct Arguments *arguments, struct GraphCSR *graph);
+/* pageRank.h:86 ; pageRank.c:2723-2919 */
+struct PageRankStats *pageRankDataDrivenPullPushGraphCSR(struct Arguments *arguments, struct GraphCSR *graph);
+/* 00_graph_bench/include/preprocess/reorder.h:68 ; reorder.c:165-221.  The
+ * labels are sorted in place (ascending fixed-point rank) and returned. */
+uint32_t *radixSortEdgesByPageRank(float *pageRanks, uint32_t *labels, uint32_t num_vertices);
+
+/* ---- SPMV (GPU) --------------------------------------------------------- */
+
+/* 00_graph_bench/include/algorithms/openmp/SPMV.h:30 ; SPMV.c:45-66 */
+struct SPMVStats *newSPMVStatsGraphCSR(struct GraphCSR *graph);
+/* SPMV.h:35 ; SPMV.c:139-154 */
+void freeSPMVStats(struct SPMVStats *stats);
+/* SPMV.h:51 ; SPMV.c:588-614.  pushpull 0 pull, 1 push; 2 and 3 are the
+ * reference's fixed-point variants (message + NULL); other values pull. */
+struct SPMVStats *SPMVGraphCSR(struct Arguments *arguments, struct GraphCSR *graph);
+/* SPMV.h:52 ; SPMV.c:616-713 */
+struct SPMVStats *SPMVPullGraphCSR(struct Arguments *arguments, struct GraphCSR *graph);
+/* SPMV.h:53 ; SPMV.c:715-810 */
+struct SPMVStats *SPMVPushGraphCSR(struct Arguments *arguments, struct GraphCSR *graph);
 
 /* ---- roots and RNG ------------------------------------------------------ */
 

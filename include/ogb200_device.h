@@ -255,10 +255,29 @@ typedef struct ogb_tune_info
  * fastest (ogb_pagerank_set_bins). */
 int ogb_batch_autotune(ogb_batch *b, ogb_tune_info *info);
 
-/* PageRank; mode 0 pull, 1 push.  d_ranks receives V normalized ranks;
- * d_init (may be NULL) replaces the uniform unnormalized start 1-0.85. */
+/* PageRank; mode = the reference's PULL_PUSH value: 0 pull, 1 push, 6
+ * data-driven pull, 7 data-driven push, 8 data-driven pull-push
+ * (pageRank.c:939-1186, 2405-2919).  d_ranks receives V normalized ranks;
+ * d_init (may be NULL; modes 0 and 1 only) replaces the uniform unnormalized
+ * start 1-0.85. */
 int ogb_pagerank(ogb_graph *g, uint32_t mode, uint32_t max_iterations, double epsilon, float *d_ranks,
                  const float *d_init, ogb_pr_info *info, void *stream);
+
+typedef struct ogb_spmv_info
+{
+    uint32_t iterations;
+    uint32_t weighted; /* 1: the graph's edge weights were used, 0: 0.0001 each */
+    double ms;         /* device time of the iterations */
+} ogb_spmv_info;
+/* SPMV (SPMV.c:588-811); mode 0 pull, 1 push.  d_x receives the input
+ * vector (1 / out_degree, 0.001 without out-edges), d_y the output summed
+ * over `iterations` passes (never reset between them, as the reference).
+ * Device arrays of V floats. */
+int ogb_spmv(ogb_graph *g, uint32_t mode, uint32_t iterations, float *d_x, float *d_y, ogb_spmv_info *info,
+             void *stream);
+/* radixSortEdgesByPageRank (reorder.c:165-221) on device arrays: d_labels
+ * stably sorted in place, ascending by (uint32_t)(rank * 2^20 + 0.5f). */
+int ogb_sort_by_rank(const float *d_ranks, uint32_t *d_labels, uint32_t n, void *stream);
 /* Work split of the PageRank kernels by row length: rows of at most warp_thr
  * edges are reduced by one thread in CSR order (the reference's summation
  * order), longer rows by a warp, rows above cta_thr by a CTA of cta_threads

@@ -97,6 +97,12 @@ class PageRankStats(C.Structure):
                 ("error_total", C.c_double)]
 
 
+class SPMVStats(C.Structure):
+    """algorithms/openmp/SPMV.h:19-27"""
+    _fields_ = [("iterations", u32), ("arguments", vp), ("num_vertices", u32), ("vector_output", f32p),
+                ("vector_input", f32p), ("time_total", C.c_double)]
+
+
 class Bitmap(C.Structure):
     """structures/bitmap.h:19-26"""
     _fields_ = [("real_size", u32), ("size", u32), ("numSetBits", u32), ("bitarray", u32p)]
@@ -154,6 +160,10 @@ class BfsLevel(C.Structure):
                 ("pad", u32), ("edges", C.c_uint64), ("ms", C.c_float), ("pad2", C.c_float)]
 
 
+class SpmvInfo(C.Structure):
+    _fields_ = [("iterations", u32), ("weighted", u32), ("ms", C.c_double)]
+
+
 class PrInfo(C.Structure):
     _fields_ = [("iterations", u32), ("executed", u32), ("activeVertices", u32), ("converged", u32),
                 ("error_total", C.c_double), ("ms", C.c_double), ("launches", u32), ("pad", u32)]
@@ -205,6 +215,15 @@ def _api(EL, G):
         ("pageRankGraphCSR", C.POINTER(PageRankStats), [Ap, Gp]),
         ("pageRankPullGraphCSR", C.POINTER(PageRankStats), [Ap, Gp]),
         ("pageRankPushGraphCSR", C.POINTER(PageRankStats), [Ap, Gp]),
+        ("pageRankDataDrivenPullGraphCSR", C.POINTER(PageRankStats), [Ap, Gp]),
+        ("pageRankDataDrivenPushGraphCSR", C.POINTER(PageRankStats), [Ap, Gp]),
+        ("pageRankDataDrivenPullPushGraphCSR", C.POINTER(PageRankStats), [Ap, Gp]),
+        ("radixSortEdgesByPageRank", u32p, [f32p, u32p, u32]),
+        ("newSPMVStatsGraphCSR", C.POINTER(SPMVStats), [Gp]),
+        ("freeSPMVStats", None, [C.POINTER(SPMVStats)]),
+        ("SPMVGraphCSR", C.POINTER(SPMVStats), [Ap, Gp]),
+        ("SPMVPullGraphCSR", C.POINTER(SPMVStats), [Ap, Gp]),
+        ("SPMVPushGraphCSR", C.POINTER(SPMVStats), [Ap, Gp]),
         ("initializeMersenneState", None, [C.POINTER(mt19937state), C.c_ulong]),
         ("generateRandInt", C.c_ulong, [C.POINTER(mt19937state)]),
         ("generateRandFloat", C.c_float, [C.POINTER(mt19937state)]),
@@ -242,6 +261,8 @@ _DEVICE_API = [
     ("ogb_batch_autotune", C.c_int, [vp, C.POINTER(TuneInfo)]),
     ("ogb_pagerank", C.c_int, [vp, u32, u32, C.c_double, vp, vp, C.POINTER(PrInfo), vp]),
     ("ogb_pagerank_history", C.c_int, [vp, C.POINTER(C.c_double), u32p, u32, C.POINTER(u32)]),
+    ("ogb_spmv", C.c_int, [vp, u32, u32, vp, vp, C.POINTER(SpmvInfo), vp]),
+    ("ogb_sort_by_rank", C.c_int, [vp, vp, u32, vp]),
     ("ogb_pagerank_set_bins", None, [u32, u32]),
     ("ogb_pagerank_pull_noalloc", C.c_int, [u32, vp, vp, vp, vp, u32, C.c_double, vp, vp, vp]),
     ("ogb_pagerank_get_bins", None, [u32p, u32p, u32p, u32p]),
@@ -580,6 +601,14 @@ class DeviceGraph:
                                              _ptr(ranks), _ptr(init), C.byref(info), _stream(stream)), "ogb_pagerank")
         return info_dict(info)
 
+    def spmv(self, x, y, mode: int = 0, iterations: int = 20, stream=None) -> dict:
+        """SPMV (mode 0 pull, 1 push): x receives the input vector, y the
+        output accumulated over `iterations` passes (device float32, V)."""
+        info = SpmvInfo()
+        self.lib.check(self.lib.ogb_spmv(self.handle, int(mode), int(iterations), _ptr(x), _ptr(y), C.byref(info),
+                                         _stream(stream)), "ogb_spmv")
+        return info_dict(info)
+
     def pagerank_history(self, max_entries: int = 1024) -> tuple[np.ndarray, np.ndarray]:
         err = (C.c_double * max_entries)()
         act = (u32 * max_entries)()
@@ -589,6 +618,13 @@ class DeviceGraph:
 
 
 # -------------------------------------------------------------- generators --
+
+def sort_by_rank(lib, ranks, labels, stream=None) -> None:
+    """radixSortEdgesByPageRank on device tensors: labels (int32/uint32, n)
+    sorted in place by the fixed-point key of ranks (float32, n)."""
+    lib.check(lib.ogb_sort_by_rank(_ptr(ranks), _ptr(labels), int(labels.numel()), _stream(stream)),
+              "ogb_sort_by_rank")
+
 
 def generate_rmat(scale: int, edge_factor: int, seed: int, a=0.57, b=0.19, c=0.19, permute=True,
                   weighted=False, lib: Library | None = None):

@@ -271,7 +271,17 @@ int upload_graph(const GraphCSR* h, ogb_graph* dg, cudaStream_t s) {
     OGB_TRY(h2d(c.in_degree.p, hv->in_degree, (size_t)V * 4, s));
     OGB_TRY(h2d(c.edges_idx.p, hv->edges_idx, (size_t)V * 4, s));
     OGB_TRY(csr_pack_rows(c, V, s));
+#if OGB200_WEIGHTED
+    // the WEIGHTED layout carries edge weights (SPMV reads them)
+    if (he->edges_array_weight) {
+      OGB_TRY(c.w.alloc((size_t)E * 4 + 4));
+      OGB_TRY(h2d(c.w.p, he->edges_array_weight, (size_t)E * 4, s));
+    }
+#endif
   }
+#if OGB200_WEIGHTED
+  g.weighted = h->sorted_edges_array->edges_array_weight && h->inverse_sorted_edges_array->edges_array_weight;
+#endif
   OGB_CUDA(cudaStreamSynchronize(s));
   return OK;
 }
@@ -1313,7 +1323,10 @@ static struct PageRankStats* pr_dropin(struct Arguments* a, struct GraphCSR* gra
   OGB_MUST(d_pr.alloc((size_t)V * 4 + 4));
   static PrResult r;
   const double t0 = now_s();
-  OGB_MUST(pagerank_run(dg->g, mode, a->iterations, a->epsilon, d_pr.as<float>(), nullptr, &r, s));
+  if (mode == PR_PULL || mode == PR_PUSH)
+    OGB_MUST(pagerank_run(dg->g, mode, a->iterations, a->epsilon, d_pr.as<float>(), nullptr, &r, s));
+  else
+    OGB_MUST(pagerank_dd_run(dg->g, mode, a->iterations, a->epsilon, d_pr.as<float>(), &r, s));
   OGB_MUST(d2h(st->pageRanks, d_pr.p, (size_t)V * 4, s));
   st->time_total = now_s() - t0;
   st->iterations = r.iterations;
@@ -1340,22 +1353,141 @@ extern "C" struct PageRankStats* pageRankPullGraphCSR(struct Arguments* a, struc
 extern "C" struct PageRankStats* pageRankPushGraphCSR(struct Arguments* a, struct GraphCSR* g) {
   return pr_dropin(a, g, PR_PUSH, "Starting Page Rank Push (tolerance/epsilon)");
 }
+extern "C" struct PageRankStats* pageRankDataDrivenPullGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  return pr_dropin(a, g, PR_DD_PULL, "Starting Page Rank Pull DD (tolerance/epsilon)");
+}
+extern "C" struct PageRankStats* pageRankDataDrivenPushGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  return pr_dropin(a, g, PR_DD_PUSH, "Starting Page Rank Push DD (tolerance/epsilon)");
+}
+extern "C" struct PageRankStats* pageRankDataDrivenPullPushGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  return pr_dropin(a, g, PR_DD_PULLPUSH, "Starting Page Rank Pull-Push DD (tolerance/epsilon)");
+}
 
-// pageRankGraphCSR (pageRank.c:871-936): pull and push are provided; the
-// fixed-point, quantized and data-driven variants are not part of this
-// library.
+// pageRankGraphCSR (pageRank.c:871-936): pull, push and the data-driven
+// variants (6 pull, 7 push, 8 pull-push) are provided; the fixed-point and
+// quantized variants are not part of this library.
 extern "C" struct PageRankStats* pageRankGraphCSR(struct Arguments* a, struct GraphCSR* g) {
   switch (a->pushpull) {
     case 0:
       return pageRankPullGraphCSR(a, g);
     case 1:
       return pageRankPushGraphCSR(a, g);
+    case 6:
+      return pageRankDataDrivenPullGraphCSR(a, g);
+    case 7:
+      return pageRankDataDrivenPushGraphCSR(a, g);
+    case 8:
+      return pageRankDataDrivenPullPushGraphCSR(a, g);
     default:
       if (a->pushpull > 13) return pageRankPullGraphCSR(a, g);
       say(" -----------------------------------------------------\n");
-      say("| %-51s | \n", "PR variant not provided by ogb200 (use 0 or 1)");
+      say("| %-51s | \n", "PR variant not provided by ogb200 (use 0, 1, 6, 7 or 8)");
       say(" -----------------------------------------------------\n");
       return nullptr;
+  }
+}
+
+// radixSortEdgesByPageRank (reorder.c:165-221): labels stably sorted by the
+// fixed-point rank key, in place; the same array is returned.
+extern "C" uint32_t* radixSortEdgesByPageRank(float* pageRanks, uint32_t* labels, uint32_t num_vertices) {
+  if (!num_vertices) return labels;
+  cudaStream_t s = lib_stream();
+  DevBuf d_r, d_l;
+  OGB_MUST(d_r.alloc((size_t)num_vertices * 4));
+  OGB_MUST(d_l.alloc((size_t)num_vertices * 4));
+  OGB_MUST(h2d(d_r.p, pageRanks, (size_t)num_vertices * 4, s));
+  OGB_MUST(h2d(d_l.p, labels, (size_t)num_vertices * 4, s));
+  OGB_MUST(rank_sort(d_r.as<float>(), d_l.as<uint32_t>(), num_vertices, s));
+  OGB_MUST(d2h(labels, d_l.p, (size_t)num_vertices * 4, s));
+  return labels;
+}
+
+// ------------------------------------------------------------------- SPMV ---
+
+// newSPMVStatsGraphCSR (SPMV.c:45-66): both vectors zeroed.
+extern "C" struct SPMVStats* newSPMVStatsGraphCSR(struct GraphCSR* graph) {
+  const uint32_t V = graph->num_vertices;
+  SPMVStats* st = (SPMVStats*)host_alloc(sizeof(SPMVStats));
+  st->iterations = 0;
+  st->arguments = nullptr;
+  st->num_vertices = V;
+  st->time_total = 0.0;
+  st->vector_output = (float*)host_alloc((size_t)V * 4);
+  st->vector_input = (float*)host_alloc((size_t)V * 4);
+  host_par_for(V, [&](size_t lo, size_t hi) {
+    for (size_t v = lo; v < hi; v++) {
+      st->vector_output[v] = 0.0f;
+      st->vector_input[v] = 0.0f;
+    }
+  });
+  return st;
+}
+
+// freeSPMVStats (SPMV.c:139-154).
+extern "C" void freeSPMVStats(struct SPMVStats* st) {
+  if (!st) return;
+  free(st->vector_output);
+  free(st->vector_input);
+  free(st);
+}
+
+static struct SPMVStats* spmv_dropin(struct Arguments* a, struct GraphCSR* graph, uint32_t mode,
+                                     const char* title) {
+  SPMVStats* st = newSPMVStatsGraphCSR(graph);
+  say(" -----------------------------------------------------\n");
+  say("| %-51s | \n", title);
+  say(" -----------------------------------------------------\n");
+  say("| %-21s | %-27s | \n", "Iteration", "Time (S)");
+  say(" -----------------------------------------------------\n");
+  int status = OK;
+  ogb_graph* dg = mirror_of(graph, &status);
+  if (!dg) die_status("device copy of GraphCSR", status);
+  cudaStream_t s = lib_stream();
+  const uint32_t V = graph->num_vertices;
+  DevBuf d_x, d_y;
+  OGB_MUST(d_x.alloc((size_t)V * 4 + 4));
+  OGB_MUST(d_y.alloc((size_t)V * 4 + 4));
+  double ms = 0.0;
+  OGB_MUST(spmv_run(dg->g, mode, a->iterations, d_x.as<float>(), d_y.as<float>(), &ms, s));
+  OGB_MUST(d2h(st->vector_input, d_x.p, (size_t)V * 4, s));
+  OGB_MUST(d2h(st->vector_output, d_y.p, (size_t)V * 4, s));
+  st->iterations = a->iterations;
+  st->time_total = ms / 1000.0;
+  if (!quiet()) {
+    double sum = 0.0;
+    for (uint32_t v = 0; v < V; v++) sum += ((int)(st->vector_output[v] * 100 + .5) / 100.0);
+    say(" -----------------------------------------------------\n");
+    say("| %-15s | %-15s | %-15s | \n", "Iterations", "Sum", "Time (S)");
+    say(" -----------------------------------------------------\n");
+    say("| %-15u | %-15lf | %-15f | \n", st->iterations, sum, st->time_total);
+    say(" -----------------------------------------------------\n");
+  }
+  return st;
+}
+
+extern "C" struct SPMVStats* SPMVPullGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  return spmv_dropin(a, g, 0, "Starting SPMV-PULL");
+}
+extern "C" struct SPMVStats* SPMVPushGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  return spmv_dropin(a, g, 1, "Starting SPMV-PUSH");
+}
+
+// SPMVGraphCSR (SPMV.c:588-614): 0 pull, 1 push, other values pull; the
+// fixed-point variants (2, 3) are not part of this library (message + NULL).
+extern "C" struct SPMVStats* SPMVGraphCSR(struct Arguments* a, struct GraphCSR* g) {
+  switch (a->pushpull) {
+    case 0:
+      return SPMVPullGraphCSR(a, g);
+    case 1:
+      return SPMVPushGraphCSR(a, g);
+    case 2:
+    case 3:
+      say(" -----------------------------------------------------\n");
+      say("| %-51s | \n", "SPMV variant not provided by ogb200 (use 0 or 1)");
+      say(" -----------------------------------------------------\n");
+      return nullptr;
+    default:
+      return SPMVPullGraphCSR(a, g);
   }
 }
 
@@ -1643,9 +1775,14 @@ extern "C" int ogb_bfs_trace(ogb_graph* g, ogb_bfs_level* levels, uint32_t max_l
 extern "C" int ogb_pagerank(ogb_graph* g, uint32_t mode, uint32_t max_iters, double eps, float* d_ranks,
                             const float* d_init, ogb_pr_info* info, void* stream) {
   if (!g || !d_ranks) return fail(ERR_ARG, "null");
-  if (mode > 1) return fail(ERR_ARG, "pagerank mode %u", mode);
+  const bool dd = mode == PR_DD_PULL || mode == PR_DD_PUSH || mode == PR_DD_PULLPUSH;
+  if (mode > 1 && !dd) return fail(ERR_ARG, "pagerank mode %u", mode);
+  if (dd && d_init) return fail(ERR_ARG, "pagerank mode %u takes no start vector", mode);
   static thread_local PrResult r;
-  OGB_TRY(pagerank_run(g->g, mode, max_iters, eps, d_ranks, d_init, &r, as_stream(stream)));
+  if (dd)
+    OGB_TRY(pagerank_dd_run(g->g, mode, max_iters, eps, d_ranks, &r, as_stream(stream)));
+  else
+    OGB_TRY(pagerank_run(g->g, mode, max_iters, eps, d_ranks, d_init, &r, as_stream(stream)));
   g->g.pr_last_executed = r.executed;
   memcpy(g->g.pr_err_hist, r.err_hist, sizeof(double) * std::min<uint32_t>(r.executed, 1024));
   memcpy(g->g.pr_active_hist, r.active_hist, sizeof(uint32_t) * std::min<uint32_t>(r.executed, 1024));
@@ -1660,6 +1797,24 @@ extern "C" int ogb_pagerank(ogb_graph* g, uint32_t mode, uint32_t max_iters, dou
     info->pad = 0;
   }
   return OK;
+}
+
+extern "C" int ogb_spmv(ogb_graph* g, uint32_t mode, uint32_t iterations, float* d_x, float* d_y, ogb_spmv_info* info,
+                        void* stream) {
+  if (!g || !d_x || !d_y) return fail(ERR_ARG, "null");
+  double ms = 0.0;
+  OGB_TRY(spmv_run(g->g, mode, iterations, d_x, d_y, &ms, as_stream(stream)));
+  if (info) {
+    info->iterations = iterations;
+    info->weighted = g->g.weighted ? 1u : 0u;
+    info->ms = ms;
+  }
+  return OK;
+}
+
+extern "C" int ogb_sort_by_rank(const float* d_ranks, uint32_t* d_labels, uint32_t n, void* stream) {
+  if (n && (!d_ranks || !d_labels)) return fail(ERR_ARG, "null");
+  return rank_sort(d_ranks, d_labels, n, as_stream(stream));
 }
 
 extern "C" void ogb_pagerank_set_bins(uint32_t warp_thr, uint32_t cta_thr) { pagerank_set_bins(warp_thr, cta_thr); }

@@ -1,0 +1,771 @@
+// dd.cu -- data-driven PageRank, SPMV and the sort of vertices by rank.
+//
+// References (00_graph_bench/src/...):
+//  * pageRankDataDrivenPullGraphCSR      algorithms/openmp/pageRank.c:2405-2564  (pushpull 6)
+//  * pageRankDataDrivenPushGraphCSR      algorithms/openmp/pageRank.c:2566-2721  (pushpull 7)
+//  * pageRankDataDrivenPullPushGraphCSR  algorithms/openmp/pageRank.c:2723-2919  (pushpull 8)
+//  * SPMVPullGraphCSR / SPMVPushGraphCSR algorithms/openmp/SPMV.c:616-810
+//  * radixSortEdgesByPageRank            preprocess/reorder.c:165-221
+//
+// Semantics kept:
+//  * data-driven pull: every iteration first takes contrib[u] = pr[u] /
+//    out_degree[u] for all vertices (0 without out-edges), then each vertex on
+//    the current worklist sums its in-neighbours' contribs, computes
+//    0.15 + 0.85 s, adds |new - old| / V to the error, and only when that
+//    change is >= epsilon stores the new rank, counts itself active and puts
+//    its out-neighbours on the next worklist.  Stop when no vertex was
+//    active; ranks are divided by V at the end.  Deterministic: with the
+//    summation order below the result is reproducible bit for bit;
+//  * data-driven push: residuals start at (1 - d) d sum(1 / out_degree) over
+//    in-neighbours; an active vertex takes its residual r, adds it to its
+//    rank (error |new/V - old/V|) and pushes d r / out_degree to each
+//    out-neighbour; an out-neighbour whose residual crosses epsilon (before
+//    <= epsilon, after >= epsilon) counts as active and joins the next
+//    worklist.  The reference runs this with unsynchronised reads of the
+//    residuals (its result depends on thread timing); here the residual is
+//    taken with an atomic exchange and every push is an atomic add whose
+//    returned value decides the crossing, so no push is lost.  A self loop's
+//    push is dropped, as in a sequential run of the reference (which zeroes
+//    the vertex's residual after its own pushes).  Pull-push (8) sums
+//    in-neighbours' current ranks / out-degree instead and, like the
+//    reference, adds the delta a second time on a crossing;
+//  * SPMV: x[v] = 1 / out_degree[v] (0.001 without out-edges); every
+//    iteration adds w * x[src] to y[dst] for every edge, y never reset
+//    (w = the edge weight in the WEIGHTED layout, else 0.0001); pull sums
+//    the in-row, push uses float atomics;
+//  * rank sort: stable ascending sort of the labels by the key
+//    (uint32_t)(rank * 2^20 + 0.5f) (FloatToFixed32SORT, fixedPoint.h:33).
+//
+// Summation order of a row (pull sums): rows of at most kWarpThr edges are
+// summed by one thread in CSR order (the reference's order); rows of at most
+// kCtaThr edges by a warp (lane l adds elements l, l + 32, ... in order, then
+// a butterfly fold); longer rows in chunks of kChunk edges, each chunk by
+// kCtaThreads threads (strided the same way, warps folded, the warp sums
+// added in warp order), the chunk sums added in chunk order.  The same split
+// as the PageRank pull kernel at its default thresholds; the oracle
+// reproduces it.  SPMV adds a row's sum to y (light rows add each term to y
+// directly, as the reference does).
+#include "graph.cuh"
+#include "sort.cuh"
+
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+namespace ogb {
+
+namespace {
+
+constexpr int kT = 256;
+constexpr uint32_t kWarpThr = 32, kCtaThr = 2048, kChunk = 8192;
+constexpr uint32_t kCtaThreads = kT;
+constexpr uint32_t kMarkThr = 32;       // out-rows longer than this are pushed by a CTA
+constexpr uint32_t kDdMaxIters = 1024;
+
+struct DdCtl {
+  double err[kDdMaxIters];
+  uint32_t active[kDdMaxIters];
+  uint32_t done_a[kDdMaxIters];   // blocks of the iteration's first kernel that finished
+  uint32_t done_b[kDdMaxIters];   // blocks of its second kernel that finished
+  uint32_t nbig[kDdMaxIters];     // deferred long out-rows of the iteration
+  uint32_t stop, stop_iter;
+  uint32_t n_med, n_heavy, cur_med, cur_heavy;
+};
+
+struct DdWork {
+  uint32_t V = 0;
+  DevBuf ctl, contrib, flags0, flags1, resid, med, heavy, big_v, big_d, xin;
+  DdCtl* h_ctl = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  ~DdWork() {
+    if (h_ctl) cudaFreeHost(h_ctl);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+  }
+};
+
+// One work area per device graph, kept in a small table keyed by the graph
+// (the graph's destructor releases it through dd_work_free).
+struct DdSlot {
+  const DevGraph* g;
+  DdWork* w;
+};
+std::mutex g_dd_mu;
+std::vector<DdSlot> g_dd;
+
+__global__ void dd_count_kernel(uint32_t V, const uint2* __restrict__ rows, DdCtl* __restrict__ ctl) {
+  uint32_t cm = 0, ch = 0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const uint32_t d = rows[v].y;
+    cm += (d > kWarpThr && d <= kCtaThr);
+    ch += (d > kCtaThr);
+  }
+  warp_atomic_add_total(&ctl->n_med, cm);
+  warp_atomic_add_total(&ctl->n_heavy, ch);
+}
+
+__global__ void dd_fill_kernel(uint32_t V, const uint2* __restrict__ rows, uint32_t* __restrict__ med,
+                               uint32_t* __restrict__ heavy, DdCtl* __restrict__ ctl) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const uint32_t d = rows[v].y;
+    if (d > kCtaThr)
+      heavy[atomicAdd(&ctl->cur_heavy, 1u)] = v;
+    else if (d > kWarpThr)
+      med[atomicAdd(&ctl->cur_med, 1u)] = v;
+  }
+}
+
+// ---- row sums in the GPU summation order -------------------------------------
+
+// Sum of term(j) over the row [a, a + d) by one warp (d <= kCtaThr): lane l
+// adds elements l, l + 32, ... in order, then a butterfly fold; every lane
+// returns the sum.
+template <class Term>
+__device__ __forceinline__ float warp_row_sum(uint32_t a, uint32_t d, const Term& term) {
+  float s = 0.0f;
+  for (uint32_t j = a + lane_id(); j < a + d; j += 32) s = __fadd_rn(s, term(j));
+#pragma unroll
+  for (int o = 16; o; o >>= 1) s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
+  return s;
+}
+
+// Sum over a long row by the whole CTA (kCtaThreads threads): chunks of
+// kChunk edges, each chunk strided over the threads, warps folded, warp sums
+// added in warp order; chunk sums added in chunk order.  The total is valid
+// in thread 0.  Called by every thread of the CTA.
+template <class Term>
+__device__ float cta_row_sum(uint32_t a, uint32_t d, const Term& term, float* s_part) {
+  float tot = 0.0f;
+  for (uint32_t c = 0; c < d; c += kChunk) {
+    const uint32_t len = min(kChunk, d - c);
+    float s = 0.0f;
+    for (uint32_t j = a + c + threadIdx.x; j < a + c + len; j += kCtaThreads) s = __fadd_rn(s, term(j));
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
+    if (lane_id() == 0) s_part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float ch = 0.0f;
+      for (uint32_t w = 0; w < kCtaThreads / 32; w++) ch = __fadd_rn(ch, s_part[w]);
+      tot = __fadd_rn(tot, ch);
+    }
+    __syncthreads();
+  }
+  return tot;
+}
+
+// One pass over the rows of the inverse CSR in three classes: blocks
+// [0, nb_light) take the rows of at most kWarpThr edges (a thread each, in
+// CSR order), the next nb_med blocks the medium list (a warp each), the rest
+// the heavy list (a CTA each).  For each row with P.want(v): s = the row sum
+// of P.term(j) in the order above, light rows starting from P.start(v),
+// others P.start(v) + sum; then P.finish(v, s) (by lane 0 / thread 0 for the
+// warp and CTA rows).
+template <class P>
+__device__ void rows_pass(const uint2* __restrict__ rows, const uint32_t* __restrict__ med,
+                          const uint32_t* __restrict__ heavy, uint32_t n_med, uint32_t n_heavy, uint32_t V,
+                          uint32_t nb_light, uint32_t nb_med, P& pol) {
+  __shared__ float s_part[kT / 32];
+  const uint32_t b = blockIdx.x;
+  if (b < nb_light) {
+    for (uint32_t v = b * kT + threadIdx.x; v < V; v += nb_light * kT) {
+      const uint2 r = rows[v];
+      if (r.y > kWarpThr || !pol.want(v)) continue;
+      float s = pol.start(v);
+      for (uint32_t j = r.x; j < r.x + r.y; j++) s = __fadd_rn(s, pol.term(j));
+      pol.finish(v, s);
+    }
+  } else if (b < nb_light + nb_med) {
+    const uint32_t w0 = (b - nb_light) * (kT / 32) + (threadIdx.x >> 5);
+    for (uint32_t t = w0; t < n_med; t += nb_med * (kT / 32)) {
+      const uint32_t v = med[t];
+      if (!pol.want(v)) continue;  // warp-uniform
+      const uint2 r = rows[v];
+      const float s = warp_row_sum(r.x, r.y, [&](uint32_t j) { return pol.term(j); });
+      if (lane_id() == 0) pol.finish(v, __fadd_rn(pol.start(v), s));
+    }
+  } else {
+    const uint32_t cb = b - nb_light - nb_med, ncb = gridDim.x - nb_light - nb_med;
+    for (uint32_t t = cb; t < n_heavy; t += ncb) {
+      const uint32_t v = heavy[t];
+      if (!pol.want(v)) continue;  // CTA-uniform
+      const uint2 r = rows[v];
+      const float s = cta_row_sum(r.x, r.y, [&](uint32_t j) { return pol.term(j); }, s_part);
+      if (threadIdx.x == 0) pol.finish(v, __fadd_rn(pol.start(v), s));
+    }
+  }
+}
+
+// Per-block error / active totals into ctl; the last block of the kernel
+// (counter `done`) returns true in thread 0.
+__device__ bool block_totals(double err, uint32_t act, double* g_err, uint32_t* g_act, uint32_t* done) {
+  __shared__ double s_e[kT / 32];
+  __shared__ uint32_t s_a[kT / 32];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    err += __shfl_down_sync(0xffffffffu, err, o);
+    act += __shfl_down_sync(0xffffffffu, act, o);
+  }
+  if (lane_id() == 0) {
+    s_e[threadIdx.x >> 5] = err;
+    s_a[threadIdx.x >> 5] = act;
+  }
+  __syncthreads();
+  bool last = false;
+  if (threadIdx.x == 0) {
+    double e = 0.0;
+    uint32_t a = 0;
+    for (uint32_t w = 0; w < blockDim.x / 32; w++) {
+      e += s_e[w];
+      a += s_a[w];
+    }
+    if (e != 0.0) atomicAdd(g_err, e);
+    if (a) atomicAdd(g_act, a);
+    __threadfence();
+    last = atomicAdd(done, 1u) == gridDim.x - 1;
+    if (last) __threadfence();
+  }
+  return last;
+}
+
+struct DdParams {
+  uint32_t V;
+  float damp, base_pr;
+  double epsilon;
+};
+
+// ---- data-driven pull (6) -----------------------------------------------------
+
+__global__ void dd_contrib_kernel(uint32_t V, const uint32_t* __restrict__ out_degree, const float* __restrict__ pr,
+                                  float* __restrict__ contrib, uint8_t* __restrict__ next,
+                                  const DdCtl* __restrict__ ctl) {
+  if (ctl->stop) return;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const uint32_t d = out_degree[v];
+    contrib[v] = d ? __fdiv_rn(pr[v], (float)d) : 0.0f;
+    next[v] = 0;
+  }
+}
+
+struct PullPolicy {
+  const uint8_t* cur;
+  uint8_t* next;
+  const float* contrib;
+  const uint32_t* nbr;
+  float* pr;
+  const uint2* rows_f;
+  const uint32_t* nbr_f;
+  uint32_t* big;
+  uint32_t* nbig;
+  DdParams p;
+  double err = 0.0;
+  uint32_t act = 0;
+  __device__ bool want(uint32_t v) const { return cur[v] != 0; }
+  __device__ float start(uint32_t) const { return 0.0f; }
+  __device__ float term(uint32_t j) const { return contrib[nbr[j] & 0x3FFFFFFFu]; }
+  __device__ void finish(uint32_t v, float s) {
+    const float nv = __fadd_rn(p.base_pr, __fmul_rn(p.damp, s));
+    const float old = pr[v];
+    const double e = fabs((double)__fsub_rn(nv, old));
+    err += e / (double)p.V;
+    if (e >= p.epsilon) {
+      pr[v] = nv;
+      act++;
+      const uint2 r = rows_f[v];
+      if (r.y <= kMarkThr) {
+        for (uint32_t j = r.x; j < r.x + r.y; j++) next[nbr_f[j] & 0x3FFFFFFFu] = 1;
+      } else {
+        big[atomicAdd(nbig, 1u)] = v;
+      }
+    }
+  }
+};
+
+__global__ void __launch_bounds__(kT) dd_pull_kernel(const uint2* __restrict__ rows, const uint32_t* __restrict__ med,
+                                                     const uint32_t* __restrict__ heavy, uint32_t nb_light,
+                                                     uint32_t nb_med, PullPolicy pol, DdCtl* __restrict__ ctl,
+                                                     uint32_t it) {
+  if (ctl->stop) return;
+  rows_pass(rows, med, heavy, ctl->n_med, ctl->n_heavy, pol.p.V, nb_light, nb_med, pol);
+  if (block_totals(pol.err, pol.act, &ctl->err[it], &ctl->active[it], &ctl->done_a[it])) {
+    if (ld_volatile_u32(&ctl->active[it]) == 0) {
+      ctl->stop_iter = it;
+      ctl->stop = 1;
+    }
+  }
+}
+
+// Worklist marks of the out-rows deferred by dd_pull_kernel: a CTA per row.
+__global__ void __launch_bounds__(kT) dd_mark_kernel(const uint2* __restrict__ rows_f,
+                                                     const uint32_t* __restrict__ nbr_f,
+                                                     const uint32_t* __restrict__ big, const DdCtl* __restrict__ ctl,
+                                                     uint32_t it, uint8_t* __restrict__ next) {
+  const uint32_t n = ctl->nbig[it];
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint2 r = rows_f[big[i]];
+    for (uint32_t j = r.x + threadIdx.x; j < r.x + r.y; j += blockDim.x) next[nbr_f[j] & 0x3FFFFFFFu] = 1;
+  }
+}
+
+// ---- data-driven push (7) and pull-push (8) --------------------------------
+
+// Initial residuals: (1 - d) d * sum over in-neighbours u of 1 / out_degree[u].
+struct ResidPolicy {
+  const uint32_t* nbr;
+  const uint32_t* out_degree;
+  float* resid;
+  float coef;
+  __device__ bool want(uint32_t) const { return true; }
+  __device__ float start(uint32_t) const { return 0.0f; }
+  __device__ float term(uint32_t j) const {
+    const uint32_t d = out_degree[nbr[j] & 0x3FFFFFFFu];
+    return d ? __fdiv_rn(1.0f, (float)d) : 0.0f;
+  }
+  __device__ void finish(uint32_t v, float s) { resid[v] = __fmul_rn(coef, s); }
+};
+
+__global__ void __launch_bounds__(kT) dd_resid_kernel(const uint2* __restrict__ rows, const uint32_t* __restrict__ med,
+                                                      const uint32_t* __restrict__ heavy, uint32_t nb_light,
+                                                      uint32_t nb_med, ResidPolicy pol, const DdCtl* __restrict__ ctl,
+                                                      uint32_t V) {
+  rows_pass(rows, med, heavy, ctl->n_med, ctl->n_heavy, V, nb_light, nb_med, pol);
+}
+
+// The pushes of one vertex's out-row [a, a + d) from `lane0` of `nl` lanes
+// (nl = 1: a thread; nl = blockDim.x: a CTA).  Returns the crossings counted.
+__device__ __forceinline__ uint32_t push_row(uint32_t v, uint32_t a, uint32_t d, float delta, uint32_t lane,
+                                             uint32_t nl, const uint32_t* __restrict__ nbr_f, float* resid,
+                                             uint8_t* next, double eps, bool twice) {
+  uint32_t act = 0;
+  for (uint32_t j = a + lane; j < a + d; j += nl) {
+    const uint32_t u = nbr_f[j] & 0x3FFFFFFFu;
+    if (u == v) continue;  // a self loop's push is dropped (see the header)
+    const float prev = atomicAdd(&resid[u], delta);
+    if ((double)fabsf(__fadd_rn(prev, delta)) >= eps && (double)prev <= eps) {
+      act++;
+      if (twice) atomicAdd(&resid[u], delta);
+      next[u] = 1;
+    }
+  }
+  return act;
+}
+
+// A self loop's crossings, counted as a sequential run of the reference
+// counts them (the vertex's own residual, read before it is zeroed).
+__device__ __forceinline__ uint32_t self_loops(uint32_t v, uint32_t a, uint32_t d, float r, float delta,
+                                               const uint32_t* __restrict__ nbr_f, uint8_t* next, double eps,
+                                               bool twice) {
+  uint32_t act = 0;
+  float acc = r;
+  for (uint32_t j = a; j < a + d; j++) {
+    if ((nbr_f[j] & 0x3FFFFFFFu) != v) continue;
+    const float prev = acc;
+    acc = __fadd_rn(acc, delta);
+    if ((double)fabsf(acc) >= eps && (double)prev <= eps) {
+      act++;
+      if (twice) acc = __fadd_rn(acc, delta);
+      next[v] = 1;
+    }
+  }
+  return act;
+}
+
+// Update of one active vertex given its new rank and the residual it took
+// (atomically, before): error, rank store, and the pushes (short out-rows
+// here, long ones deferred).
+__device__ __forceinline__ void push_vertex(uint32_t v, float nv, float old, float r, const uint2* rows_f,
+                                            const uint32_t* nbr_f, float* pr, float* resid, uint8_t* next,
+                                            uint32_t* big_v, float* big_d, uint32_t* nbig, const DdParams& p,
+                                            bool twice, double& err, uint32_t& act) {
+  const float fv = (float)p.V;
+  err += (double)fabsf(__fsub_rn(__fdiv_rn(nv, fv), __fdiv_rn(old, fv)));
+  pr[v] = nv;
+  const uint2 row = rows_f[v];
+  if (!row.y) return;  // no pushes (the reference's delta divides by zero here and is never used)
+  const float delta = __fmul_rn(p.damp, __fdiv_rn(r, (float)row.y));
+  act += self_loops(v, row.x, row.y, r, delta, nbr_f, next, p.epsilon, twice);
+  if (row.y <= kMarkThr) {
+    act += push_row(v, row.x, row.y, delta, 0, 1, nbr_f, resid, next, p.epsilon, twice);
+  } else {
+    const uint32_t k = atomicAdd(nbig, 1u);
+    big_v[k] = v;
+    big_d[k] = delta;
+  }
+}
+
+__global__ void __launch_bounds__(kT) dd_push_kernel(uint32_t V, const uint8_t* __restrict__ cur, uint8_t* next,
+                                                     const uint2* __restrict__ rows_f,
+                                                     const uint32_t* __restrict__ nbr_f, float* pr, float* resid,
+                                                     uint32_t* big_v, float* big_d, DdParams p,
+                                                     DdCtl* __restrict__ ctl, uint32_t it) {
+  if (ctl->stop) return;
+  double err = 0.0;
+  uint32_t act = 0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    if (!cur[v]) continue;
+    const float r = atomicExch(&resid[v], 0.0f);
+    const float old = pr[v];
+    const float nv = __fadd_rn(r, old);  // the reference's aResiduals[v] + pageRanks[v]
+    push_vertex(v, nv, old, r, rows_f, nbr_f, pr, resid, next, big_v, big_d, &ctl->nbig[it], p, false, err, act);
+  }
+  block_totals(err, act, &ctl->err[it], &ctl->active[it], &ctl->done_a[it]);
+}
+
+// Pull-push (8): the row sum of current ranks / out-degree, then the pushes.
+struct PullPushPolicy {
+  const uint8_t* cur;
+  uint8_t* next;
+  const uint32_t* nbr;
+  const uint32_t* out_degree;
+  float* pr;
+  float* resid;
+  const uint2* rows_f;
+  const uint32_t* nbr_f;
+  uint32_t* big_v;
+  float* big_d;
+  uint32_t* nbig;
+  DdParams p;
+  double err = 0.0;
+  uint32_t act = 0;
+  __device__ bool want(uint32_t v) const { return cur[v] != 0; }
+  __device__ float start(uint32_t) const { return 0.0f; }
+  __device__ float term(uint32_t j) const {
+    const uint32_t u = nbr[j] & 0x3FFFFFFFu;
+    return __fdiv_rn(*(volatile float*)&pr[u], (float)out_degree[u]);
+  }
+  __device__ void finish(uint32_t v, float s) {
+    const float nv = __fadd_rn(p.base_pr, __fmul_rn(p.damp, s));
+    const float old = pr[v];
+    const float r = atomicExch(&resid[v], 0.0f);
+    push_vertex(v, nv, old, r, rows_f, nbr_f, pr, resid, next, big_v, big_d, nbig, p, true, err, act);
+  }
+};
+
+__global__ void __launch_bounds__(kT) dd_pullpush_kernel(const uint2* __restrict__ rows,
+                                                         const uint32_t* __restrict__ med,
+                                                         const uint32_t* __restrict__ heavy, uint32_t nb_light,
+                                                         uint32_t nb_med, PullPushPolicy pol,
+                                                         DdCtl* __restrict__ ctl, uint32_t it) {
+  if (ctl->stop) return;
+  pol.nbig = &ctl->nbig[it];
+  rows_pass(rows, med, heavy, ctl->n_med, ctl->n_heavy, pol.p.V, nb_light, nb_med, pol);
+  block_totals(pol.err, pol.act, &ctl->err[it], &ctl->active[it], &ctl->done_a[it]);
+}
+
+// The deferred long out-rows (a CTA per row), then the iteration's stop
+// decision by the last block: no crossing anywhere in the iteration.
+__global__ void __launch_bounds__(kT) dd_bigpush_kernel(const uint2* __restrict__ rows_f,
+                                                        const uint32_t* __restrict__ nbr_f, float* resid,
+                                                        uint8_t* next, const uint32_t* __restrict__ big_v,
+                                                        const float* __restrict__ big_d, double eps, bool twice,
+                                                        DdCtl* __restrict__ ctl, uint32_t it) {
+  if (ctl->stop) return;
+  const uint32_t n = ctl->nbig[it];
+  uint32_t act = 0;
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint32_t v = big_v[i];
+    const uint2 r = rows_f[v];
+    act += push_row(v, r.x, r.y, big_d[i], threadIdx.x, blockDim.x, nbr_f, resid, next, eps, twice);
+  }
+  if (block_totals(0.0, act, &ctl->err[it], &ctl->active[it], &ctl->done_b[it])) {
+    if (ld_volatile_u32(&ctl->active[it]) == 0) {
+      ctl->stop_iter = it;
+      ctl->stop = 1;
+    }
+  }
+}
+
+__global__ void dd_init_kernel(uint32_t V, float base_pr, float* __restrict__ pr, uint8_t* __restrict__ cur,
+                               uint8_t* __restrict__ next) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    pr[v] = base_pr;
+    cur[v] = 1;
+    next[v] = 0;
+  }
+}
+
+__global__ void dd_clear_kernel(uint32_t V, uint8_t* __restrict__ next, const DdCtl* __restrict__ ctl) {
+  if (ctl->stop) return;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) next[v] = 0;
+}
+
+__global__ void dd_normalize_kernel(uint32_t V, float* __restrict__ pr) {
+  const float fv = (float)V;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
+    pr[v] = __fdiv_rn(pr[v], fv);
+}
+
+// ---- SPMV ---------------------------------------------------------------------
+
+__global__ void spmv_init_kernel(uint32_t V, const uint32_t* __restrict__ out_degree, float* __restrict__ x,
+                                 float* __restrict__ y) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const uint32_t d = out_degree[v];
+    x[v] = d ? __fdiv_rn(1.0f, (float)d) : 0.001f;
+    y[v] = 0.0f;
+  }
+}
+
+struct SpmvPullPolicy {
+  const uint32_t* nbr;
+  const float* w;  // null: every weight is kSpmvDefaultWeight
+  const float* x;
+  float* y;
+  __device__ bool want(uint32_t) const { return true; }
+  __device__ float start(uint32_t v) const { return y[v]; }
+  __device__ float term(uint32_t j) const {
+    return __fmul_rn(w ? w[j] : 0.0001f, x[nbr[j] & 0x3FFFFFFFu]);
+  }
+  __device__ void finish(uint32_t v, float s) { y[v] = s; }
+};
+
+__global__ void __launch_bounds__(kT) spmv_pull_kernel(const uint2* __restrict__ rows, const uint32_t* __restrict__ med,
+                                                       const uint32_t* __restrict__ heavy, uint32_t nb_light,
+                                                       uint32_t nb_med, SpmvPullPolicy pol,
+                                                       const DdCtl* __restrict__ ctl, uint32_t V) {
+  rows_pass(rows, med, heavy, ctl->n_med, ctl->n_heavy, V, nb_light, nb_med, pol);
+}
+
+// Push: rows of at most kWarpThr out-edges by a thread, longer ones by a warp
+// (order does not matter: float atomics, as the reference's omp atomic).
+__global__ void __launch_bounds__(kT) spmv_push_kernel(uint32_t V, const uint2* __restrict__ rows_f,
+                                                       const uint32_t* __restrict__ nbr_f, const float* __restrict__ w,
+                                                       const float* __restrict__ x, float* __restrict__ y) {
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t base = gw * 32; base < V; base += nw * 32) {
+    const uint32_t v = base + lane_id();
+    uint2 r = make_uint2(0u, 0u);
+    if (v < V) r = rows_f[v];
+    const bool own = v < V && r.y <= kWarpThr;
+    if (own) {
+      const float xv = x[v];
+      for (uint32_t j = r.x; j < r.x + r.y; j++)
+        atomicAdd(&y[nbr_f[j] & 0x3FFFFFFFu], __fmul_rn(w ? w[j] : 0.0001f, xv));
+    }
+    uint32_t longm = __ballot_sync(0xffffffffu, v < V && !own);
+    while (longm) {
+      const uint32_t l = (uint32_t)__ffs(longm) - 1;
+      longm &= longm - 1;
+      const uint32_t vv = base + l;
+      const uint2 rr = make_uint2(__shfl_sync(0xffffffffu, r.x, l), __shfl_sync(0xffffffffu, r.y, l));
+      const float xv = x[vv];
+      for (uint32_t j = rr.x + lane_id(); j < rr.x + rr.y; j += 32)
+        atomicAdd(&y[nbr_f[j] & 0x3FFFFFFFu], __fmul_rn(w ? w[j] : 0.0001f, xv));
+    }
+  }
+}
+
+// ---- sort by rank ---------------------------------------------------------------
+
+__global__ void rank_keys_kernel(uint32_t n, const float* __restrict__ ranks, uint32_t* __restrict__ keys) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    keys[i] = __float2uint_rz(__fadd_rn(__fmul_rn(ranks[i], 1048576.0f), ranks[i] >= 0.0f ? 0.5f : -0.5f));
+}
+
+// ---- host side -------------------------------------------------------------------
+
+int dd_work_get(DevGraph& g, DdWork** out, cudaStream_t s) {
+  DdWork* w = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_dd_mu);
+    for (auto& e : g_dd)
+      if (e.g == &g) w = e.w;
+    if (!w) {
+      w = new DdWork();
+      g_dd.push_back({&g, w});
+    }
+  }
+  const uint32_t V = g.V;
+  if (w->V != V || !w->ctl.p) {
+    OGB_TRY(w->ctl.alloc(sizeof(DdCtl)));
+    OGB_TRY(w->contrib.alloc((size_t)V * 4 + 16));
+    OGB_TRY(w->flags0.alloc((size_t)V + 16));
+    OGB_TRY(w->flags1.alloc((size_t)V + 16));
+    OGB_TRY(w->resid.alloc((size_t)V * 4 + 16));
+    OGB_TRY(w->med.alloc((size_t)V * 4 + 16));
+    OGB_TRY(w->heavy.alloc((size_t)V * 4 + 16));
+    OGB_TRY(w->big_v.alloc((size_t)V * 4 + 16));
+    OGB_TRY(w->big_d.alloc((size_t)V * 4 + 16));
+    OGB_TRY(w->xin.alloc((size_t)V * 4 + 16));
+    w->V = V;
+  }
+  if (!w->h_ctl) OGB_CUDA(cudaMallocHost(&w->h_ctl, sizeof(DdCtl)));
+  if (!w->ev0) {
+    OGB_CUDA(cudaEventCreate(&w->ev0));
+    OGB_CUDA(cudaEventCreate(&w->ev1));
+  }
+  OGB_CUDA(cudaMemsetAsync(w->ctl.p, 0, sizeof(DdCtl), s));
+  // the inverse rows' classes, kept with the graph's build id
+  DdCtl* ctl = w->ctl.as<DdCtl>();
+  const int grid = sm_count() * 8;
+  dd_count_kernel<<<grid, kT, 0, s>>>(V, g.inv.d_rows(), ctl);
+  dd_fill_kernel<<<grid, kT, 0, s>>>(V, g.inv.d_rows(), w->med.as<uint32_t>(), w->heavy.as<uint32_t>(), ctl);
+  OGB_CUDA(cudaGetLastError());
+  *out = w;
+  return OK;
+}
+
+struct Grid3 {
+  uint32_t light, med, heavy;
+  uint32_t total() const { return light + med + heavy; }
+};
+
+Grid3 rows_grid(uint32_t V) {
+  const uint32_t sms = sm_count();
+  Grid3 g;
+  g.light = std::max<uint32_t>(1, std::min<uint32_t>(sms * 8, ceil_div(V, kT)));
+  g.med = sms * 8;
+  g.heavy = sms * 2;
+  return g;
+}
+
+}  // namespace
+
+void dd_work_free(const DevGraph* g) {
+  std::lock_guard<std::mutex> lk(g_dd_mu);
+  for (size_t i = 0; i < g_dd.size(); i++) {
+    if (g_dd[i].g == g) {
+      delete g_dd[i].w;
+      g_dd.erase(g_dd.begin() + (long)i);
+      return;
+    }
+  }
+}
+
+int pagerank_dd_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon, float* ranks, PrResult* res,
+                    cudaStream_t s) {
+  if (mode < PR_DD_PULL || mode > PR_DD_PULLPUSH) return fail(ERR_ARG, "data-driven pagerank: mode %u", mode);
+  if (max_iters > kDdMaxIters) return fail(ERR_ARG, "data-driven pagerank: at most %u iterations", kDdMaxIters);
+  const uint32_t V = g.V;
+  if (V == 0) return fail(ERR_ARG, "pagerank: empty graph");
+  DdWork* w = nullptr;
+  OGB_TRY(dd_work_get(g, &w, s));
+  DdCtl* ctl = w->ctl.as<DdCtl>();
+  DdParams p;
+  p.V = V;
+  p.damp = 0.85f;
+  p.base_pr = 1.0f - p.damp;  // float, as newPageRankStatsGraphCSR (pageRank.c:47-75)
+  p.epsilon = epsilon;
+  const int sms = sm_count();
+  const Grid3 G = rows_grid(V);
+  uint8_t* cur = w->flags0.as<uint8_t>();
+  uint8_t* nxt = w->flags1.as<uint8_t>();
+  float* resid = w->resid.as<float>();
+  OGB_CUDA(cudaEventRecord(w->ev0, s));
+  dd_init_kernel<<<sms * 8, kT, 0, s>>>(V, p.base_pr, ranks, cur, nxt);
+  uint32_t launches = 1;
+  if (mode != PR_DD_PULL) {
+    // (1.0f - damp) * damp, then times the row sum (pageRank.c:2614), in float
+    const float coef = (1.0f - p.damp) * p.damp;
+    ResidPolicy rp{g.inv.d_dst(), g.fwd.d_out_degree(), resid, coef};
+    dd_resid_kernel<<<G.total(), kT, 0, s>>>(g.inv.d_rows(), w->med.as<uint32_t>(), w->heavy.as<uint32_t>(), G.light,
+                                             G.med, rp, ctl, V);
+    launches++;
+  }
+  OGB_CUDA(cudaGetLastError());
+  for (uint32_t it = 0; it < max_iters; it++) {
+    if (mode == PR_DD_PULL) {
+      dd_contrib_kernel<<<sms * 8, kT, 0, s>>>(V, g.fwd.d_out_degree(), ranks, w->contrib.as<float>(), nxt, ctl);
+      PullPolicy pol{cur, nxt, w->contrib.as<float>(), g.inv.d_dst(), ranks, g.fwd.d_rows(), g.fwd.d_dst(),
+                     w->big_v.as<uint32_t>(), &ctl->nbig[it], p};
+      dd_pull_kernel<<<G.total(), kT, 0, s>>>(g.inv.d_rows(), w->med.as<uint32_t>(), w->heavy.as<uint32_t>(),
+                                               G.light, G.med, pol, ctl, it);
+      dd_mark_kernel<<<sms * 2, kT, 0, s>>>(g.fwd.d_rows(), g.fwd.d_dst(), w->big_v.as<uint32_t>(), ctl, it, nxt);
+    } else {
+      dd_clear_kernel<<<sms * 8, kT, 0, s>>>(V, nxt, ctl);
+      if (mode == PR_DD_PUSH) {
+        dd_push_kernel<<<sms * 8, kT, 0, s>>>(V, cur, nxt, g.fwd.d_rows(), g.fwd.d_dst(), ranks, resid,
+                                               w->big_v.as<uint32_t>(), w->big_d.as<float>(), p, ctl, it);
+      } else {
+        PullPushPolicy pol{cur, nxt, g.inv.d_dst(), g.fwd.d_out_degree(), ranks, resid, g.fwd.d_rows(), g.fwd.d_dst(),
+                           w->big_v.as<uint32_t>(), w->big_d.as<float>(), nullptr, p};
+        dd_pullpush_kernel<<<G.total(), kT, 0, s>>>(g.inv.d_rows(), w->med.as<uint32_t>(), w->heavy.as<uint32_t>(),
+                                                     G.light, G.med, pol, ctl, it);
+      }
+      dd_bigpush_kernel<<<sms * 2, kT, 0, s>>>(g.fwd.d_rows(), g.fwd.d_dst(), resid, nxt, w->big_v.as<uint32_t>(),
+                                                w->big_d.as<float>(), epsilon, mode == PR_DD_PULLPUSH, ctl, it);
+    }
+    OGB_CUDA(cudaGetLastError());
+    launches += 3;
+    std::swap(cur, nxt);
+  }
+  dd_normalize_kernel<<<sms * 8, kT, 0, s>>>(V, ranks);
+  OGB_CUDA(cudaGetLastError());
+  OGB_CUDA(cudaEventRecord(w->ev1, s));
+  OGB_CUDA(cudaMemcpyAsync(w->h_ctl, ctl, sizeof(DdCtl), cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  OGB_CUDA(cudaEventElapsedTime(&ms, w->ev0, w->ev1));
+  PrResult r;
+  r.ms = ms;
+  r.launches = launches + 1;
+  if (w->h_ctl->stop) {
+    r.converged = 1;
+    r.iterations = w->h_ctl->stop_iter;
+    r.executed = w->h_ctl->stop_iter + 1;
+  } else {
+    r.iterations = max_iters;
+    r.executed = max_iters;
+  }
+  for (uint32_t i = 0; i < r.executed && i < 1024; i++) {
+    r.err_hist[i] = w->h_ctl->err[i];
+    r.active_hist[i] = w->h_ctl->active[i];
+  }
+  if (r.executed) {
+    r.error_total = w->h_ctl->err[r.executed - 1];
+    r.activeVertices = w->h_ctl->active[r.executed - 1];
+  }
+  if (res) *res = r;
+  return OK;
+}
+
+int spmv_run(DevGraph& g, uint32_t mode, uint32_t iterations, float* x, float* y, double* ms_out, cudaStream_t s) {
+  if (mode > 1) return fail(ERR_ARG, "spmv: mode %u", mode);
+  const uint32_t V = g.V;
+  if (V == 0) return fail(ERR_ARG, "spmv: empty graph");
+  DdWork* w = nullptr;
+  OGB_TRY(dd_work_get(g, &w, s));
+  const int sms = sm_count();
+  spmv_init_kernel<<<sms * 8, kT, 0, s>>>(V, g.fwd.d_out_degree(), x, y);
+  OGB_CUDA(cudaGetLastError());
+  OGB_CUDA(cudaEventRecord(w->ev0, s));
+  if (mode == 0) {
+    const Grid3 G = rows_grid(V);
+    SpmvPullPolicy pol{g.inv.d_dst(), g.weighted ? g.inv.d_w() : nullptr, x, y};
+    for (uint32_t it = 0; it < iterations; it++)
+      spmv_pull_kernel<<<G.total(), kT, 0, s>>>(g.inv.d_rows(), w->med.as<uint32_t>(), w->heavy.as<uint32_t>(),
+                                                 G.light, G.med, pol, w->ctl.as<DdCtl>(), V);
+  } else {
+    for (uint32_t it = 0; it < iterations; it++)
+      spmv_push_kernel<<<sms * 8, kT, 0, s>>>(V, g.fwd.d_rows(), g.fwd.d_dst(), g.weighted ? g.fwd.d_w() : nullptr, x,
+                                               y);
+  }
+  OGB_CUDA(cudaGetLastError());
+  OGB_CUDA(cudaEventRecord(w->ev1, s));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  OGB_CUDA(cudaEventElapsedTime(&ms, w->ev0, w->ev1));
+  if (ms_out) *ms_out = ms;
+  return OK;
+}
+
+int rank_sort(const float* ranks, uint32_t* labels, uint32_t n, cudaStream_t s) {
+  if (n == 0) return OK;
+  static SortWorkspace* ws = new SortWorkspace();
+  DevBuf keys, keys_out, labels_out;
+  OGB_TRY(keys.alloc((size_t)n * 4));
+  OGB_TRY(keys_out.alloc((size_t)n * 4));
+  OGB_TRY(labels_out.alloc((size_t)n * 4));
+  const int grid = (int)std::min<uint32_t>(sm_count() * 8, std::max<uint32_t>(1, ceil_div(n, 256)));
+  rank_keys_kernel<<<grid, 256, 0, s>>>(n, ranks, keys.as<uint32_t>());
+  OGB_CUDA(cudaGetLastError());
+  KV in{keys.as<uint32_t>(), labels, nullptr};
+  KV out{keys_out.as<uint32_t>(), labels_out.as<uint32_t>(), nullptr};
+  OGB_TRY(sort_pairs(in, out, n, *ws, s, 32));
+  OGB_TRY(sort_check(*ws, s));
+  OGB_CUDA(cudaMemcpyAsync(labels, labels_out.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  return OK;
+}
+
+}  // namespace ogb

@@ -236,7 +236,9 @@ struct PrResult {
   uint32_t active_hist[1024];
 };
 
-enum PrMode : uint32_t { PR_PULL = 0, PR_PUSH = 1 };
+// The reference's PULL_PUSH numbers: 0 pull, 1 push, 6 data-driven pull, 7
+// data-driven push, 8 data-driven pull-push.
+enum PrMode : uint32_t { PR_PULL = 0, PR_PUSH = 1, PR_DD_PULL = 6, PR_DD_PUSH = 7, PR_DD_PULLPUSH = 8 };
 
 // PageRank with the reference semantics (pageRank.c:939-1186): unnormalized
 // start at 1-d, stop when no vertex changes by >= epsilon or after
@@ -244,6 +246,19 @@ enum PrMode : uint32_t { PR_PULL = 0, PR_PUSH = 1 };
 // floats; `init` (optional, device) replaces the uniform start.
 int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon, float* ranks,
                  const float* init, PrResult* res, cudaStream_t s);
+
+// Data-driven PageRank (modes PR_DD_*; pageRank.c:2405-2919), same result
+// fields as pagerank_run.  dd.cu.
+int pagerank_dd_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon, float* ranks, PrResult* res,
+                    cudaStream_t s);
+// SPMV (SPMV.c:588-811): mode 0 pull, 1 push; x receives the input vector
+// (1 / out_degree, 0.001 without out-edges), y the output accumulated over
+// `iterations` passes.  Device arrays of V floats.  dd.cu.
+int spmv_run(DevGraph& g, uint32_t mode, uint32_t iterations, float* x, float* y, double* ms, cudaStream_t s);
+// radixSortEdgesByPageRank (reorder.c:165-221) on device arrays: labels
+// stably sorted ascending by (uint32_t)(rank * 2^20 + 0.5f).  dd.cu.
+int rank_sort(const float* ranks, uint32_t* labels, uint32_t n, cudaStream_t s);
+void dd_work_free(const DevGraph* g);
 
 // Row-length thresholds of the PageRank work split (light rows per thread,
 // heavy rows per warp, very heavy rows per CTA of cta_threads threads).

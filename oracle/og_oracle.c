@@ -491,3 +491,238 @@ int orc_generate_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, doubl
     free(perm);
     return 0;
 }
+
+/* ------------------------------------------------ data-driven PageRank -- */
+
+/* Row sum of c[] over in-row [a, a + d) in the GPU kernels' order (the
+ * split of orc_set_gpu_order), or sequentially in CSR order. */
+static float row_sum(const float *c, const uint32_t *nbr, uint32_t a, uint32_t d, int gpu_order)
+{
+    if (gpu_order && d > g_cta_thr)
+    {
+        float tot = 0.0f;
+        for (uint32_t k = 0; k < d; k += g_chunk)
+        {
+            const uint32_t len = (d - k < g_chunk) ? d - k : g_chunk;
+            tot += tree_sum(c, nbr, a + k, len, g_cta_threads);
+        }
+        return tot;
+    }
+    if (gpu_order && d > g_warp_thr) return tree_sum(c, nbr, a, d, 32);
+    float s = 0.0f;
+    for (uint32_t j = a; j < a + d; j++) s += c[nbr[j] & 0x3FFFFFFFu];
+    return s;
+}
+
+/* pageRankDataDrivenPullGraphCSR (pageRank.c:2405-2564, mode 6),
+ * pageRankDataDrivenPushGraphCSR (:2566-2721, mode 7) and
+ * pageRankDataDrivenPullPushGraphCSR (:2723-2919, mode 8), run
+ * sequentially in vertex order (the reference's loops with one thread).
+ * gpu_order (mode 6 only) sums long in-rows in the GPU kernels' order. */
+uint32_t orc_pagerank_dd(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_idx, const uint32_t *f_dst,
+                         const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, int mode,
+                         int gpu_order, uint32_t max_iters, double epsilon, float *pr, uint32_t *iterations_out,
+                         double *error_out, uint32_t *active_hist)
+{
+    const float damp = 0.85f;
+    const float base_pr = 1.0f - damp;
+    uint8_t *cur = malloc((size_t)V + 1), *next = malloc((size_t)V + 1);
+    float *c = malloc((size_t)V * 4 + 4), *res = malloc((size_t)V * 4 + 4);
+    for (uint32_t v = 0; v < V; v++)
+    {
+        pr[v] = base_pr;
+        cur[v] = 1;
+        next[v] = 0;
+    }
+    if (mode != 6)
+    {
+        /* residuals: (1 - d) d * sum over in-neighbours of 1 / out_degree */
+        for (uint32_t v = 0; v < V; v++) c[v] = f_outdeg[v] ? 1.0f / (float)f_outdeg[v] : 0.0f;
+        const float coef = (1.0f - damp) * damp;
+        for (uint32_t v = 0; v < V; v++)
+        {
+            const float s = row_sum(c, i_dst, i_idx[v], i_outdeg[v], gpu_order);
+            res[v] = coef * s;
+        }
+    }
+    uint32_t it, executed = 0;
+    double error_total = 0.0;
+    for (it = 0; it < max_iters; it++)
+    {
+        error_total = 0.0;
+        uint32_t active = 0;
+        if (mode == 6)
+        {
+            for (uint32_t v = 0; v < V; v++) c[v] = f_outdeg[v] ? pr[v] / (float)f_outdeg[v] : 0.0f;
+            for (uint32_t v = 0; v < V; v++)
+            {
+                if (!cur[v]) continue;
+                const float s = row_sum(c, i_dst, i_idx[v], i_outdeg[v], gpu_order);
+                const float scaled = damp * s;
+                const float nv = base_pr + scaled;
+                const float diff = nv - pr[v];
+                const double e = fabs((double)diff);
+                error_total += e / V;
+                if (e >= epsilon)
+                {
+                    pr[v] = nv;
+                    for (uint32_t j = f_idx[v]; j < f_idx[v] + f_outdeg[v]; j++) next[f_dst[j] & 0x3FFFFFFFu] = 1;
+                    active++;
+                }
+            }
+        }
+        else
+        {
+            for (uint32_t v = 0; v < V; v++)
+            {
+                if (!cur[v]) continue;
+                float nv;
+                const float old = pr[v];
+                if (mode == 7)
+                {
+                    nv = res[v] + old;
+                }
+                else
+                {
+                    float s = 0.0f;
+                    for (uint32_t j = i_idx[v]; j < i_idx[v] + i_outdeg[v]; j++)
+                    {
+                        const uint32_t u = i_dst[j] & 0x3FFFFFFFu;
+                        s += pr[u] / (float)f_outdeg[u];
+                    }
+                    const float scaled = damp * s;
+                    nv = base_pr + scaled;
+                }
+                const float a = nv / (float)V, b = old / (float)V;
+                const float diff = a - b;
+                error_total += fabs((double)diff);
+                pr[v] = nv;
+                const uint32_t d = f_outdeg[v];
+                if (d)
+                {
+                    const float q = res[v] / (float)d;
+                    const float delta = damp * q;
+                    for (uint32_t j = f_idx[v]; j < f_idx[v] + d; j++)
+                    {
+                        const uint32_t u = f_dst[j] & 0x3FFFFFFFu;
+                        const float prev = res[u];
+                        res[u] = prev + delta;
+                        const float sum = prev + delta;
+                        if (fabs((double)sum) >= epsilon && (double)prev <= epsilon)
+                        {
+                            active++;
+                            if (mode == 8) res[u] = res[u] + delta;
+                            next[u] = 1;
+                        }
+                    }
+                }
+                res[v] = 0.0f;
+            }
+        }
+        if (active_hist) active_hist[executed] = active;
+        executed++;
+        uint8_t *t = cur;
+        cur = next;
+        next = t;
+        memset(next, 0, V);
+        if (active == 0) break;
+    }
+    for (uint32_t v = 0; v < V; v++) pr[v] = pr[v] / (float)V;
+    if (iterations_out) *iterations_out = it;
+    if (error_out) *error_out = error_total;
+    free(cur);
+    free(next);
+    free(c);
+    free(res);
+    return executed;
+}
+
+/* ------------------------------------------------------------------ SPMV -- */
+
+/* SPMVPullGraphCSR (SPMV.c:616-713, mode 0) and SPMVPushGraphCSR
+ * (:715-810, mode 1), sequential.  w (in the direction the mode reads:
+ * inverse for pull, forward for push) may be NULL: every weight 0.0001.
+ * gpu_order (pull) adds long rows' sums, in the GPU kernels' order, to y
+ * once per iteration. */
+void orc_spmv(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_idx, const uint32_t *f_dst,
+              const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, const float *w, int mode,
+              int gpu_order, uint32_t iters, float *x, float *y)
+{
+    for (uint32_t v = 0; v < V; v++)
+    {
+        x[v] = f_outdeg[v] ? 1.0f / (float)f_outdeg[v] : 0.001f;
+        y[v] = 0.0f;
+    }
+    float *t = NULL;
+    const uint32_t E = V ? (mode == 0 ? i_idx[V - 1] + i_outdeg[V - 1] : f_idx[V - 1] + f_outdeg[V - 1]) : 0;
+    (void)E;
+    if (mode == 0 && gpu_order)
+    {
+        /* the per-edge terms as a gather array for tree_sum: t[j] = w_j * x[src] */
+        uint32_t Et = 0;
+        for (uint32_t v = 0; v < V; v++)
+            if (i_idx[v] + i_outdeg[v] > Et) Et = i_idx[v] + i_outdeg[v];
+        t = malloc((size_t)Et * 4 + 4);
+        uint32_t *ident = malloc((size_t)Et * 4 + 4);
+        for (uint32_t j = 0; j < Et; j++)
+        {
+            const float wj = w ? w[j] : 0.0001f;
+            t[j] = wj * x[i_dst[j] & 0x3FFFFFFFu];
+            ident[j] = j;
+        }
+        for (uint32_t it = 0; it < iters; it++)
+            for (uint32_t v = 0; v < V; v++)
+            {
+                const uint32_t d = i_outdeg[v];
+                if (d > g_warp_thr)
+                    y[v] += row_sum(t, ident, i_idx[v], d, 1);
+                else
+                    for (uint32_t j = i_idx[v]; j < i_idx[v] + d; j++) y[v] += t[j];
+            }
+        free(ident);
+        free(t);
+        return;
+    }
+    for (uint32_t it = 0; it < iters; it++)
+    {
+        if (mode == 0)
+        {
+            for (uint32_t v = 0; v < V; v++)
+                for (uint32_t j = i_idx[v]; j < i_idx[v] + i_outdeg[v]; j++)
+                {
+                    const float wj = w ? w[j] : 0.0001f;
+                    const float p = wj * x[i_dst[j] & 0x3FFFFFFFu];
+                    y[v] += p;
+                }
+        }
+        else
+        {
+            for (uint32_t v = 0; v < V; v++)
+                for (uint32_t j = f_idx[v]; j < f_idx[v] + f_outdeg[v]; j++)
+                {
+                    const float wj = w ? w[j] : 0.0001f;
+                    const float p = wj * x[v];
+                    y[f_dst[j] & 0x3FFFFFFFu] += p;
+                }
+        }
+    }
+}
+
+/* radixSortEdgesByPageRank (reorder.c:165-221): labels stably sorted by the
+ * key (uint32_t)(rank * 2^20 + 0.5f) (FloatToFixed32SORT, fixedPoint.h:33),
+ * in place. */
+void orc_rank_sort(uint32_t n, const float *ranks, uint32_t *labels)
+{
+    uint32_t *key = malloc((size_t)n * 4 + 4), *ok = malloc((size_t)n * 4 + 4), *ol = malloc((size_t)n * 4 + 4);
+    for (uint32_t i = 0; i < n; i++)
+    {
+        const float scaled = ranks[i] * 1048576.0f;
+        const float r = scaled + (ranks[i] >= 0 ? 0.5f : -0.5f);
+        key[i] = r > 0.0f ? (uint32_t)r : 0u;
+    }
+    sort_by_key(n, key, labels, NULL, ok, ol, NULL);
+    memcpy(labels, ol, (size_t)n * 4);
+    free(key);
+    free(ok);
+    free(ol);
+}

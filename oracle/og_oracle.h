@@ -92,4 +92,21 @@ void orc_random_roots(uint32_t seed, uint32_t V, uint32_t avg_degree, const uint
 int orc_generate_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, double a, double b, double c,
                       int permute, uint32_t *src, uint32_t *dst, float *w);
 
+/* Data-driven PageRank (pageRank.c:2405-2919): mode 6 pull, 7 push, 8
+ * pull-push, sequential in vertex order; gpu_order (mode 6) sums long
+ * in-rows in the GPU kernels' order.  Ranks normalized; returns the executed
+ * iterations. */
+uint32_t orc_pagerank_dd(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_idx, const uint32_t *f_dst,
+                         const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, int mode,
+                         int gpu_order, uint32_t max_iters, double epsilon, float *pr, uint32_t *iterations_out,
+                         double *error_out, uint32_t *active_hist);
+
+/* SPMV (SPMV.c:616-810): mode 0 pull, 1 push; w may be NULL (0.0001). */
+void orc_spmv(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_idx, const uint32_t *f_dst,
+              const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, const float *w, int mode,
+              int gpu_order, uint32_t iters, float *x, float *y);
+
+/* radixSortEdgesByPageRank (reorder.c:165-221), in place. */
+void orc_rank_sort(uint32_t n, const float *ranks, uint32_t *labels);
+
 #endif

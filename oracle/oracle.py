@@ -68,6 +68,39 @@ class Oracle:
         d.orc_generate_rmat.argtypes = [u32, u32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_int, vp, vp,
                                         vp]
         d.orc_generate_rmat.restype = C.c_int
+        d.orc_pagerank_dd.argtypes = [u32, vp, vp, vp, vp, vp, vp, C.c_int, C.c_int, u32, C.c_double, vp, vp, vp, vp]
+        d.orc_pagerank_dd.restype = u32
+        d.orc_spmv.argtypes = [u32, vp, vp, vp, vp, vp, vp, vp, C.c_int, C.c_int, u32, vp, vp]
+        d.orc_rank_sort.argtypes = [u32, vp, vp]
+
+    def pagerank_dd(self, g: dict, mode: int, max_iters: int = 100, epsilon: float = 1e-4, gpu_order: bool = False):
+        """Data-driven PageRank (6 pull, 7 push, 8 pull-push), sequential;
+        gpu_order sums long in-rows as the GPU kernels do (mode 6)."""
+        V = g["num_vertices"]
+        ranks = np.empty(V, np.float32)
+        it, err = u32(), C.c_double()
+        ah = np.zeros(max(max_iters, 1), np.uint32)
+        n = self.d.orc_pagerank_dd(V, _p(g["f_outdeg"]), _p(g["f_idx"]), _p(g["f_dst"]), _p(g["i_outdeg"]),
+                                   _p(g["i_idx"]), _p(g["i_dst"]), mode, 1 if gpu_order else 0, max_iters, epsilon,
+                                   _p(ranks), C.byref(it), C.byref(err), _p(ah))
+        return ranks, {"iterations": it.value, "error_total": err.value, "executed": n, "active_hist": ah[:n]}
+
+    def spmv(self, g: dict, mode: int = 0, iters: int = 20, weighted: bool = False, gpu_order: bool = False):
+        """SPMV pull (0) / push (1), sequential; weights from the graph dict
+        (i_w for pull, f_w for push) when weighted, else 0.0001 each."""
+        V = g["num_vertices"]
+        x, y = np.empty(V, np.float32), np.empty(V, np.float32)
+        w = (g["i_w"] if mode == 0 else g["f_w"]) if weighted else None
+        self.d.orc_spmv(V, _p(g["f_outdeg"]), _p(g["f_idx"]), _p(g["f_dst"]), _p(g["i_outdeg"]), _p(g["i_idx"]),
+                        _p(g["i_dst"]), _p(w), mode, 1 if gpu_order else 0, iters, _p(x), _p(y))
+        return x, y
+
+    def rank_sort(self, ranks, labels):
+        """radixSortEdgesByPageRank: the labels sorted by fixed-point rank."""
+        r = np.ascontiguousarray(ranks, np.float32)
+        out = np.ascontiguousarray(labels, np.uint32).copy()
+        self.d.orc_rank_sort(len(out), _p(r), _p(out))
+        return out
 
     def generate_rmat(self, scale: int, edge_factor: int, seed: int, a=0.57, b=0.19, c=0.19, permute=True,
                       weighted=False):

@@ -191,3 +191,82 @@ def test_step_functions_match_reference(og, lib, ref, files):
     assert o[3] == r[3] and np.array_equal(o[4], r[4]) and np.array_equal(o[5], r[5])
     lib.graphCSRFree(g)
     ref.graphCSRFree(rg)
+
+
+@pytest.mark.parametrize("pushpull", [6, 7, 8])
+def test_dd_pagerank_dropin_matches_reference(og, lib, ref, files, pushpull):
+    """pageRankGraphCSR pushpull 6/7/8 against the reference build run with
+    one kernel thread (its data-driven push loses updates when threaded).
+    6: within 1e-6 L1 at the same iteration count; 7/8: the reference's own
+    cross-variant rule (graphTest.c:58-80: fewer than 20 normalized ranks
+    more than 1e-3 apart)."""
+    g, _ = our_graph(og, lib, files["rmat"])
+    rg = ref.build_graph(files["rmat"])
+    a = og.default_arguments(pushpull=pushpull, iterations=60, epsilon=1e-5)
+    st = lib.pageRankGraphCSR(C.byref(a), g)
+    s = st.contents
+    pr = og.as_numpy(s.pageRanks, s.num_vertices, np.float32).astype(np.float64)
+    ours_it = s.iterations
+    lib.freePageRankStats(st)
+    ra = ref.arguments(pushpull=pushpull, iterations=60, epsilon=1e-5)
+    ra.ker_numThreads = 1
+    from oracle.oracle import silenced_stdout
+    with silenced_stdout():
+        rst = ref.pageRankGraphCSR(C.byref(ra), rg)
+    rr = og.as_numpy(rst.contents.pageRanks, rst.contents.num_vertices, np.float32).astype(np.float64)
+    ref_it = rst.contents.iterations
+    ref.freePageRankStats(rst)
+    if pushpull == 6:
+        assert ours_it == ref_it
+        assert float(np.abs(pr - rr).sum()) <= 1e-6
+    else:
+        assert int(np.sum(np.abs(pr - rr) > 1e-3)) < 20
+    lib.graphCSRFree(g)
+    ref.graphCSRFree(rg)
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+@pytest.mark.parametrize("pushpull", [0, 1])
+def test_spmv_dropin_matches_reference(og, lib, libw, ref, refw, files, pushpull, weighted):
+    """SPMVGraphCSR: the input vector equal; the output per vertex within the
+    bound of a reordered float sum (pull sums long rows in another order,
+    push adds with atomics in any order)."""
+    L, R = (libw, refw) if weighted else (lib, ref)
+    path = files["rmat_w"] if weighted else files["rmat"]
+    g, _ = our_graph(og, L, path, weighted=1 if weighted else 0)
+    rg = R.build_graph(path, weighted_file=weighted)
+    a = og.default_arguments(pushpull=pushpull, iterations=5)
+    st = L.SPMVGraphCSR(C.byref(a), g)
+    V = st.contents.num_vertices
+    x, y = og.as_numpy(st.contents.vector_input, V, np.float32), og.as_numpy(st.contents.vector_output, V, np.float32)
+    assert st.contents.iterations == 5
+    L.freeSPMVStats(st)
+    ra = R.arguments(pushpull=pushpull, iterations=5)
+    from oracle.oracle import silenced_stdout
+    with silenced_stdout():
+        rst = R.SPMVGraphCSR(C.byref(ra), rg)
+    rx = og.as_numpy(rst.contents.vector_input, V, np.float32)
+    ry = og.as_numpy(rst.contents.vector_output, V, np.float32).astype(np.float64)
+    R.freeSPMVStats(rst)
+    assert np.array_equal(x, rx)
+    rel = np.abs(y - ry) / np.maximum(np.abs(ry), 1e-30)
+    # a reordered float sum of n positive terms: 2 n 2^-24 relative at worst
+    n = 5 * og.graph_arrays(rg)["i_outdeg"].astype(np.float64)
+    assert np.all(rel <= np.maximum(1e-5, 2.0 * n * 2.0 ** -24)), float(rel.max())
+    L.graphCSRFree(g)
+    R.graphCSRFree(rg)
+
+
+def test_rank_sort_dropin_matches_reference(og, lib, ref):
+    """radixSortEdgesByPageRank on host arrays: labels equal (stable sort by
+    the fixed-point key), returned in place."""
+    rng = np.random.default_rng(3)
+    for n in (1, 1000, 300_000):
+        pr = (rng.random(n) / n).astype(np.float32)
+        pr[: n // 3] = pr[0]  # ties
+        lab = rng.permutation(n).astype(np.uint32)
+        ours, theirs = lab.copy(), lab.copy()
+        p = lib.radixSortEdgesByPageRank(pr.ctypes.data_as(og.f32p), ours.ctypes.data_as(og.u32p), n)
+        assert C.addressof(p.contents) == ours.ctypes.data
+        ref.radixSortEdgesByPageRank(pr.ctypes.data_as(og.f32p), theirs.ctypes.data_as(og.u32p), n)
+        assert np.array_equal(ours, theirs), n

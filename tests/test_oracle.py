@@ -207,3 +207,65 @@ def test_gen_rmat_file_equals_product_file(og, tmp_path):
         s, d, w = og.generate_rmat(11, 16, 5, weighted=weighted)
         og.write_edge_file(p2, s, d, w)
         assert open(p1, "rb").read() == open(p2, "rb").read()
+
+
+@pytest.mark.parametrize("scale,seed", [(10, 3), (11, 8)])
+def test_oracle_dd_and_spmv_match_reference(og, oracle, ref, tmp_path, scale, seed):
+    """Data-driven PageRank 6/7/8 (the reference with one kernel thread:
+    threaded, its push loses updates and is not reproducible), SPMV pull and
+    the sort by rank: bit-exact; SPMV push (omp atomics) within 1e-5."""
+    import ctypes as C
+
+    from oracle.oracle import silenced_stdout
+    s, d, _ = og.generate_rmat(scale, 16, seed)
+    path = str(tmp_path / "g.bin")
+    og.write_edge_file(path, s, d)
+    rg = ref.build_graph(path)
+    ga = og.graph_arrays(rg)
+    V = ga["num_vertices"]
+    for mode in (6, 7, 8):
+        a = ref.arguments(pushpull=mode, iterations=40, epsilon=1e-5)
+        a.ker_numThreads = 1
+        with silenced_stdout():
+            st = ref.pageRankGraphCSR(C.byref(a), rg)
+        rr = og.as_numpy(st.contents.pageRanks, V, np.float32)
+        rit, rerr = st.contents.iterations, st.contents.error_total
+        ref.freePageRankStats(st)
+        orr, oi = oracle.pagerank_dd(ga, mode, 40, 1e-5)
+        assert np.array_equal(rr.view(np.uint32), orr.view(np.uint32)), mode
+        assert rit == oi["iterations"] and rerr == oi["error_total"], mode
+    for mode in (0, 1):
+        a = ref.arguments(pushpull=mode, iterations=4)
+        with silenced_stdout():
+            st = ref.SPMVGraphCSR(C.byref(a), rg)
+        rx, ry = og.as_numpy(st.contents.vector_input, V, np.float32), og.as_numpy(st.contents.vector_output, V,
+                                                                                   np.float32)
+        ref.freeSPMVStats(st)
+        ox, oy = oracle.spmv(ga, mode, 4)
+        assert np.array_equal(rx, ox)
+        if mode == 0:
+            assert np.array_equal(ry.view(np.uint32), oy.view(np.uint32))
+        else:
+            assert float((np.abs(ry - oy) / np.maximum(np.abs(oy), 1e-30)).max()) <= 1e-5
+    pr, _ = oracle.pagerank(ga, 0, 20, 1e-4)
+    lab = np.random.default_rng(seed).permutation(V).astype(np.uint32)
+    theirs = lab.copy()
+    ref.radixSortEdgesByPageRank(pr.ctypes.data_as(og.f32p), theirs.ctypes.data_as(og.u32p), V)
+    assert np.array_equal(theirs, oracle.rank_sort(pr, lab))
+    ref.graphCSRFree(rg)
+
+
+def test_oracle_matches_dd_spmv_fixture(oracle):
+    """tests/golden/dd_spmv_rmat10.npz (made by make_golden_dd.py from the
+    reference's build): data-driven PageRank 6/7/8, SPMV pull and the sort by
+    rank, bit-exact."""
+    z = dict(np.load(os.path.join(GOLDEN, "dd_spmv_rmat10.npz")))
+    V = int(max(z["src"].max(), z["dst"].max())) + 1
+    g = oracle.build(z["src"], z["dst"], V, 0)
+    for mode in (6, 7, 8):
+        r, st = oracle.pagerank_dd(g, mode, 50, 1e-5)
+        assert np.array_equal(r.view(np.uint32), z[f"dd{mode}_ranks"].view(np.uint32)), mode
+        assert st["iterations"] == int(z[f"dd{mode}_stats"][0]) and st["error_total"] == float(z[f"dd{mode}_error"][0])
+    x, y = oracle.spmv(g, 0, 3)
+    assert np.array_equal(x, z["spmv_x"]) and np.array_equal(y.view(np.uint32), z["spmv_y"].view(np.uint32))
+    assert np.array_equal(oracle.rank_sort(z["dd6_ranks"], z["sort_labels_in"]), z["sort_labels_out"])
