@@ -275,6 +275,21 @@ typedef struct ogb_spmv_info
  * Device arrays of V floats. */
 int ogb_spmv(ogb_graph *g, uint32_t mode, uint32_t iterations, float *d_x, float *d_y, ogb_spmv_info *info,
              void *stream);
+/* 1-D partitioned PageRank pull (no counterpart in the reference; its
+ * iteration is pageRank.c:984-1044).  A rank owns the destination vertices
+ * [lo, hi).  range_init: d_ranks = 1 - 0.85 and d_contrib = that /
+ * out_degree on all V.  range_step: one iteration over [lo, hi) with the
+ * whole previous d_contrib; writes d_ranks and d_contrib_next on [lo, hi)
+ * only and adds |change| / V and the count of changes >= epsilon to the
+ * DEVICE scalars *d_err / *d_active (zeroed by the caller).  Each row is
+ * summed in the same order as ogb_pagerank pull at its default thresholds,
+ * so any partition gives the same ranks bit for bit.  range_finish: d_ranks
+ * /= V.  The caller all-gathers d_contrib_next's slices between steps
+ * (opengraph_b200.parallel does this over torch.distributed). */
+int ogb_pagerank_range_init(ogb_graph *g, float *d_ranks, float *d_contrib, void *stream);
+int ogb_pagerank_range_step(ogb_graph *g, uint32_t lo, uint32_t hi, const float *d_contrib, float *d_ranks,
+                            float *d_contrib_next, double epsilon, double *d_err, uint32_t *d_active, void *stream);
+int ogb_pagerank_range_finish(ogb_graph *g, float *d_ranks, void *stream);
 /* radixSortEdgesByPageRank (reorder.c:165-221) on device arrays: d_labels
  * stably sorted in place, ascending by (uint32_t)(rank * 2^20 + 0.5f). */
 int ogb_sort_by_rank(const float *d_ranks, uint32_t *d_labels, uint32_t n, void *stream);

@@ -1812,6 +1812,24 @@ extern "C" int ogb_spmv(ogb_graph* g, uint32_t mode, uint32_t iterations, float*
   return OK;
 }
 
+extern "C" int ogb_pagerank_range_init(ogb_graph* g, float* d_ranks, float* d_contrib, void* stream) {
+  if (!g || !d_ranks || !d_contrib) return fail(ERR_ARG, "null");
+  return pagerank_range_init(g->g, d_ranks, d_contrib, as_stream(stream));
+}
+
+extern "C" int ogb_pagerank_range_step(ogb_graph* g, uint32_t lo, uint32_t hi, const float* d_contrib,
+                                       float* d_ranks, float* d_contrib_next, double epsilon, double* d_err,
+                                       uint32_t* d_active, void* stream) {
+  if (!g || !d_contrib || !d_ranks || !d_contrib_next || !d_err || !d_active) return fail(ERR_ARG, "null");
+  return pagerank_range_step(g->g, lo, hi, d_contrib, d_ranks, d_contrib_next, epsilon, d_err, d_active,
+                             as_stream(stream));
+}
+
+extern "C" int ogb_pagerank_range_finish(ogb_graph* g, float* d_ranks, void* stream) {
+  if (!g || !d_ranks) return fail(ERR_ARG, "null");
+  return pagerank_range_finish(g->g, d_ranks, as_stream(stream));
+}
+
 extern "C" int ogb_sort_by_rank(const float* d_ranks, uint32_t* d_labels, uint32_t n, void* stream) {
   if (n && (!d_ranks || !d_labels)) return fail(ERR_ARG, "null");
   return rank_sort(d_ranks, d_labels, n, as_stream(stream));

@@ -768,4 +768,206 @@ int rank_sort(const float* ranks, uint32_t* labels, uint32_t n, cudaStream_t s) 
   return OK;
 }
 
+
+// ---- one pull iteration over a range of vertices (1-D partitioned PageRank) --
+//
+// A rank of a 1-D partition owns the destination vertices [lo, hi) (their
+// inverse-CSR rows) and holds the whole contrib vector of the previous
+// iteration.  One step: for v in [lo, hi): s = sum of contrib over v's
+// in-row (the order above: the same per-row order as the single-GPU pull
+// kernel, whatever the partition), rank 0.15 + 0.85 s, contrib_next[v] =
+// rank / out_degree (0 without out-edges); |change| / V and the count of
+// changes >= epsilon are added to *err / *active.  The caller all-gathers
+// contrib_next's slices between steps (pageRank.c:984-1044 per iteration).
+
+namespace {
+
+struct RangeWork {
+  uint32_t lo = 0, hi = 0, build = 0;
+  bool ready = false;
+  DevBuf ctl, med, heavy;
+};
+std::mutex g_range_mu;
+std::vector<std::pair<const DevGraph*, RangeWork*>> g_range;
+
+__global__ void range_count_kernel(uint32_t lo, uint32_t hi, const uint2* __restrict__ rows,
+                                   DdCtl* __restrict__ ctl) {
+  uint32_t cm = 0, ch = 0;
+  for (uint32_t v = lo + blockIdx.x * blockDim.x + threadIdx.x; v < hi; v += gridDim.x * blockDim.x) {
+    const uint32_t d = rows[v].y;
+    cm += (d > kWarpThr && d <= kCtaThr);
+    ch += (d > kCtaThr);
+  }
+  warp_atomic_add_total(&ctl->n_med, cm);
+  warp_atomic_add_total(&ctl->n_heavy, ch);
+}
+
+__global__ void range_fill_kernel(uint32_t lo, uint32_t hi, const uint2* __restrict__ rows,
+                                  uint32_t* __restrict__ med, uint32_t* __restrict__ heavy,
+                                  DdCtl* __restrict__ ctl) {
+  for (uint32_t v = lo + blockIdx.x * blockDim.x + threadIdx.x; v < hi; v += gridDim.x * blockDim.x) {
+    const uint32_t d = rows[v].y;
+    if (d > kCtaThr)
+      heavy[atomicAdd(&ctl->cur_heavy, 1u)] = v;
+    else if (d > kWarpThr)
+      med[atomicAdd(&ctl->cur_med, 1u)] = v;
+  }
+}
+
+struct RangePolicy {
+  uint32_t lo;
+  const uint32_t* nbr;
+  const uint32_t* out_degree;
+  const float* contrib;
+  float* pr;
+  float* contrib_next;
+  DdParams p;
+  double err = 0.0;
+  uint32_t act = 0;
+  __device__ bool want(uint32_t) const { return true; }
+  __device__ float start(uint32_t) const { return 0.0f; }
+  __device__ float term(uint32_t j) const { return contrib[nbr[j] & 0x3FFFFFFFu]; }
+  __device__ void finish(uint32_t v, float s) {
+    const float nv = __fadd_rn(p.base_pr, __fmul_rn(p.damp, s));
+    const float prev = pr[v];
+    pr[v] = nv;
+    const uint32_t d = out_degree[v];
+    contrib_next[v] = d ? __fdiv_rn(nv, (float)d) : 0.0f;
+    const double e = fabs((double)__fsub_rn(nv, prev));
+    err += e / (double)p.V;
+    act += (e >= p.epsilon) ? 1u : 0u;
+  }
+};
+
+// rows_pass over [lo, hi): the light blocks walk [lo, hi), the lists hold
+// the range's medium and heavy rows.
+__global__ void __launch_bounds__(kT) range_step_kernel(const uint2* __restrict__ rows, uint32_t lo, uint32_t hi,
+                                                        const uint32_t* __restrict__ med,
+                                                        const uint32_t* __restrict__ heavy, uint32_t nb_light,
+                                                        uint32_t nb_med, RangePolicy pol,
+                                                        const DdCtl* __restrict__ ctl, double* g_err,
+                                                        uint32_t* g_act) {
+  // shift the light rows' vertex numbering to the range: rows_pass walks
+  // [0, n) of the shifted arrays
+  struct Shift {
+    RangePolicy& q;
+    uint32_t lo;
+    __device__ bool want(uint32_t) const { return true; }
+    __device__ float start(uint32_t) const { return 0.0f; }
+    __device__ float term(uint32_t j) const { return q.term(j); }
+    __device__ void finish(uint32_t v, float s) { q.finish(v + lo, s); }
+  };
+  Shift sh{pol, lo};
+  if (blockIdx.x < nb_light) {
+    rows_pass(rows + lo, nullptr, nullptr, 0, 0, hi - lo, nb_light, 0, sh);
+  } else {
+    // medium / heavy lists hold absolute vertex ids: run them unshifted
+    rows_pass(rows, med, heavy, ctl->n_med, ctl->n_heavy, 0, nb_light, nb_med, pol);
+  }
+  double err = pol.err;
+  uint32_t act = pol.act;
+  __shared__ double s_e[kT / 32];
+  __shared__ uint32_t s_a[kT / 32];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    err += __shfl_down_sync(0xffffffffu, err, o);
+    act += __shfl_down_sync(0xffffffffu, act, o);
+  }
+  if (lane_id() == 0) {
+    s_e[threadIdx.x >> 5] = err;
+    s_a[threadIdx.x >> 5] = act;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double e = 0.0;
+    uint32_t a = 0;
+    for (uint32_t w = 0; w < kT / 32; w++) {
+      e += s_e[w];
+      a += s_a[w];
+    }
+    if (e != 0.0) atomicAdd(g_err, e);
+    if (a) atomicAdd(g_act, a);
+  }
+}
+
+__global__ void range_init_kernel(uint32_t V, const uint32_t* __restrict__ out_degree, float base_pr,
+                                  float* __restrict__ pr, float* __restrict__ contrib) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    pr[v] = base_pr;
+    const uint32_t d = out_degree[v];
+    contrib[v] = d ? __fdiv_rn(base_pr, (float)d) : 0.0f;
+  }
+}
+
+}  // namespace
+
+void range_work_free(const DevGraph* g) {
+  std::lock_guard<std::mutex> lk(g_range_mu);
+  for (size_t i = 0; i < g_range.size(); i++) {
+    if (g_range[i].first == g) {
+      delete g_range[i].second;
+      g_range.erase(g_range.begin() + (long)i);
+      return;
+    }
+  }
+}
+
+int pagerank_range_init(DevGraph& g, float* ranks, float* contrib, cudaStream_t s) {
+  if (g.V == 0) return fail(ERR_ARG, "pagerank range: empty graph");
+  const float base = 1.0f - 0.85f;
+  range_init_kernel<<<sm_count() * 8, kT, 0, s>>>(g.V, g.fwd.d_out_degree(), base, ranks, contrib);
+  OGB_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int pagerank_range_step(DevGraph& g, uint32_t lo, uint32_t hi, const float* contrib, float* ranks,
+                        float* contrib_next, double epsilon, double* d_err, uint32_t* d_active, cudaStream_t s) {
+  if (lo > hi || hi > g.V) return fail(ERR_RANGE, "pagerank range [%u, %u) outside [0, %u)", lo, hi, g.V);
+  if (lo == hi) return OK;
+  RangeWork* w = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_range_mu);
+    for (auto& e : g_range)
+      if (e.first == &g) w = e.second;
+    if (!w) {
+      w = new RangeWork();
+      g_range.emplace_back(&g, w);
+    }
+  }
+  DdCtl* ctl = nullptr;
+  if (!w->ready || w->lo != lo || w->hi != hi || w->build != g.build_id) {
+    OGB_TRY(w->ctl.alloc(sizeof(DdCtl)));
+    OGB_TRY(w->med.alloc((size_t)(hi - lo) * 4 + 16));
+    OGB_TRY(w->heavy.alloc((size_t)(hi - lo) * 4 + 16));
+    ctl = w->ctl.as<DdCtl>();
+    OGB_CUDA(cudaMemsetAsync(ctl, 0, sizeof(DdCtl), s));
+    const int grid = sm_count() * 8;
+    range_count_kernel<<<grid, kT, 0, s>>>(lo, hi, g.inv.d_rows(), ctl);
+    range_fill_kernel<<<grid, kT, 0, s>>>(lo, hi, g.inv.d_rows(), w->med.as<uint32_t>(), w->heavy.as<uint32_t>(), ctl);
+    OGB_CUDA(cudaGetLastError());
+    w->lo = lo;
+    w->hi = hi;
+    w->build = g.build_id;
+    w->ready = true;
+  }
+  ctl = w->ctl.as<DdCtl>();
+  DdParams p;
+  p.V = g.V;
+  p.damp = 0.85f;
+  p.base_pr = 1.0f - p.damp;
+  p.epsilon = epsilon;
+  RangePolicy pol{lo, g.inv.d_dst(), g.fwd.d_out_degree(), contrib, ranks, contrib_next, p};
+  const Grid3 G = rows_grid(hi - lo);
+  range_step_kernel<<<G.total(), kT, 0, s>>>(g.inv.d_rows(), lo, hi, w->med.as<uint32_t>(), w->heavy.as<uint32_t>(),
+                                             G.light, G.med, pol, ctl, d_err, d_active);
+  OGB_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int pagerank_range_finish(DevGraph& g, float* ranks, cudaStream_t s) {
+  dd_normalize_kernel<<<sm_count() * 8, kT, 0, s>>>(g.V, ranks);
+  OGB_CUDA(cudaGetLastError());
+  return OK;
+}
+
 }  // namespace ogb

@@ -62,6 +62,7 @@ int sm_count() {
 
 DevGraph::~DevGraph() {
   dd_work_free(this);
+  range_work_free(this);
   bfs_work_free(bfs);
   pr_work_free(pr);
   ms_work_free(ms);

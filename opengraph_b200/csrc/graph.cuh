@@ -259,6 +259,16 @@ int spmv_run(DevGraph& g, uint32_t mode, uint32_t iterations, float* x, float* y
 // stably sorted ascending by (uint32_t)(rank * 2^20 + 0.5f).  dd.cu.
 int rank_sort(const float* ranks, uint32_t* labels, uint32_t n, cudaStream_t s);
 void dd_work_free(const DevGraph* g);
+// One pull PageRank iteration over the destination vertices [lo, hi) (a rank
+// of a 1-D partition): ranks and contrib_next are written on [lo, hi) only;
+// |change| / V and the changes >= epsilon are added to d_err / d_active
+// (device, zeroed by the caller).  init: ranks = 1 - 0.85, contrib = that /
+// out_degree on all V; finish: ranks /= V.  dd.cu.
+int pagerank_range_init(DevGraph& g, float* ranks, float* contrib, cudaStream_t s);
+int pagerank_range_step(DevGraph& g, uint32_t lo, uint32_t hi, const float* contrib, float* ranks,
+                        float* contrib_next, double epsilon, double* d_err, uint32_t* d_active, cudaStream_t s);
+int pagerank_range_finish(DevGraph& g, float* ranks, cudaStream_t s);
+void range_work_free(const DevGraph* g);
 
 // Row-length thresholds of the PageRank work split (light rows per thread,
 // heavy rows per warp, very heavy rows per CTA of cta_threads threads).

@@ -726,3 +726,29 @@ void orc_rank_sort(uint32_t n, const float *ranks, uint32_t *labels)
     free(ok);
     free(ol);
 }
+
+/* One pull PageRank iteration over the destination vertices [lo, hi) of a
+ * 1-D partition (the iteration of pageRank.c:984-1044 restricted to a
+ * range): rows summed as row_sum (gpu_order: the GPU kernels' order),
+ * ranks and contrib_next written on [lo, hi); the range's error and active
+ * count added to *err / *active. */
+void orc_pull_range_step(uint32_t V, const uint32_t *f_outdeg, const uint32_t *i_outdeg, const uint32_t *i_idx,
+                         const uint32_t *i_dst, uint32_t lo, uint32_t hi, const float *contrib, float *pr,
+                         float *contrib_next, double epsilon, int gpu_order, double *err, uint32_t *active)
+{
+    const float damp = 0.85f;
+    const float base_pr = 1.0f - damp;
+    for (uint32_t v = lo; v < hi; v++)
+    {
+        const float s = row_sum(contrib, i_dst, i_idx[v], i_outdeg[v], gpu_order);
+        const float scaled = damp * s;
+        const float nv = base_pr + scaled;
+        const float prev = pr[v];
+        pr[v] = nv;
+        contrib_next[v] = f_outdeg[v] ? nv / (float)f_outdeg[v] : 0.0f;
+        const float diff = nv - prev;
+        const double e = fabs((double)diff);
+        *err += e / V;
+        if (e >= epsilon) (*active)++;
+    }
+}

@@ -106,6 +106,12 @@ void orc_spmv(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_idx, const
               const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, const float *w, int mode,
               int gpu_order, uint32_t iters, float *x, float *y);
 
+/* One pull iteration over the destination range [lo, hi) of a 1-D
+ * partition (pageRank.c:984-1044 restricted to the range). */
+void orc_pull_range_step(uint32_t V, const uint32_t *f_outdeg, const uint32_t *i_outdeg, const uint32_t *i_idx,
+                         const uint32_t *i_dst, uint32_t lo, uint32_t hi, const float *contrib, float *pr,
+                         float *contrib_next, double epsilon, int gpu_order, double *err, uint32_t *active);
+
 /* radixSortEdgesByPageRank (reorder.c:165-221), in place. */
 void orc_rank_sort(uint32_t n, const float *ranks, uint32_t *labels);
 

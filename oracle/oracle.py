@@ -72,6 +72,17 @@ class Oracle:
         d.orc_pagerank_dd.restype = u32
         d.orc_spmv.argtypes = [u32, vp, vp, vp, vp, vp, vp, vp, C.c_int, C.c_int, u32, vp, vp]
         d.orc_rank_sort.argtypes = [u32, vp, vp]
+        d.orc_pull_range_step.argtypes = [u32, vp, vp, vp, vp, u32, u32, vp, vp, vp, C.c_double, C.c_int, vp, vp]
+
+    def pull_range_step(self, g: dict, lo: int, hi: int, contrib, pr, contrib_next, epsilon: float,
+                        gpu_order: bool = True):
+        """One pull iteration over [lo, hi) (numpy float32 arrays of V, in
+        place); returns the range's (error, active)."""
+        err, act = C.c_double(0.0), u32(0)
+        self.d.orc_pull_range_step(g["num_vertices"], _p(g["f_outdeg"]), _p(g["i_outdeg"]), _p(g["i_idx"]),
+                                   _p(g["i_dst"]), lo, hi, _p(contrib), _p(pr), _p(contrib_next), epsilon,
+                                   1 if gpu_order else 0, C.byref(err), C.byref(act))
+        return err.value, act.value
 
     def pagerank_dd(self, g: dict, mode: int, max_iters: int = 100, epsilon: float = 1e-4, gpu_order: bool = False):
         """Data-driven PageRank (6 pull, 7 push, 8 pull-push), sequential;
