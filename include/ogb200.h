@@ -267,6 +267,33 @@ uint32_t topDownStepGraphCSR(struct GraphCSR *graph, struct ArrayQueue *sharedFr
 uint32_t bottomUpStepGraphCSR(struct GraphCSR *graph, struct Bitmap *bitmapCurr,
                               struct Bitmap *bitmapNext, struct BFSStats *stats);
 
+/* ---- BFS DualOrder (GPU) ------------------------------------------------
+ * The DualOrder variants translate the frontier and parents between the
+ * forward and inverse CSRs' vertex orders at direction changes.  Provided for
+ * graphs whose two orders are the same (no reordering); after a
+ * direction-optimized search parents_DualOrder holds the parents as they
+ * stood when the last bottom-up phase ended (sentinels if none ran).
+ * Graphs with reordered labels: message + NULL. */
+/* 00_graph_bench/include/structures/graphCSR.h:36 ; graphCSR.c:250-335 (no -l/-L/-O/-M) */
+struct GraphCSR *graphCSRPreProcessingStepDualOrder(struct Arguments *arguments);
+/* graphCSR.h:37 ; graphCSR.c:337-377 */
+void graphCSRVertexLabelRemappingDualOrder(struct GraphCSR *graphCSR);
+/* 00_graph_bench/include/algorithms/openmp/BFS.h:63 ; BFS.c:1045-1068 */
+struct BFSStats *breadthFirstSearchGraphCSRDualOrder(struct Arguments *arguments, struct GraphCSR *graph);
+/* BFS.h:65 ; BFS.c:1082-1164 */
+struct BFSStats *breadthFirstSearchPullGraphCSRDualOrder(struct Arguments *arguments, struct GraphCSR *graph);
+/* BFS.h:66 ; BFS.c:1178-1267 */
+struct BFSStats *breadthFirstSearchPushGraphCSRDualOrder(struct Arguments *arguments, struct GraphCSR *graph);
+/* BFS.h:67 ; BFS.c:1279-1430 */
+struct BFSStats *breadthFirstSearchDirectionOptimizedGraphCSRDualOrder(struct Arguments *arguments,
+                                                                       struct GraphCSR *graph);
+/* BFS.h:69 ; BFS.c:1442-1490 (the code of topDownStepGraphCSR) */
+uint32_t topDownStepGraphCSRDualOrder(struct GraphCSR *graph, struct ArrayQueue *sharedFrontierQueue,
+                                      struct ArrayQueue **localFrontierQueues, struct BFSStats *stats);
+/* BFS.h:70 ; BFS.c:1505-1562 (the code of bottomUpStepGraphCSR) */
+uint32_t bottomUpStepGraphCSRDualOrder(struct GraphCSR *graph, struct Bitmap *bitmapCurr,
+                                       struct Bitmap *bitmapNext, struct BFSStats *stats);
+
 /* ---- PageRank (GPU) ----------------------------------------------------- */
 
 /* 00_graph_bench/include/algorithms/openmp/pageRank.h:32 ; pageRank.c:47-75 */

@@ -210,6 +210,15 @@ def _api(EL, G):
         ("topDownStepGraphCSR", u32, [Gp, C.POINTER(ArrayQueue), C.POINTER(C.POINTER(ArrayQueue)),
                                       C.POINTER(BFSStats)]),
         ("bottomUpStepGraphCSR", u32, [Gp, C.POINTER(Bitmap), C.POINTER(Bitmap), C.POINTER(BFSStats)]),
+        ("graphCSRPreProcessingStepDualOrder", Gp, [Ap]),
+        ("graphCSRVertexLabelRemappingDualOrder", None, [Gp]),
+        ("breadthFirstSearchGraphCSRDualOrder", C.POINTER(BFSStats), [Ap, Gp]),
+        ("breadthFirstSearchPullGraphCSRDualOrder", C.POINTER(BFSStats), [Ap, Gp]),
+        ("breadthFirstSearchPushGraphCSRDualOrder", C.POINTER(BFSStats), [Ap, Gp]),
+        ("breadthFirstSearchDirectionOptimizedGraphCSRDualOrder", C.POINTER(BFSStats), [Ap, Gp]),
+        ("topDownStepGraphCSRDualOrder", u32, [Gp, C.POINTER(ArrayQueue), C.POINTER(C.POINTER(ArrayQueue)),
+                                               C.POINTER(BFSStats)]),
+        ("bottomUpStepGraphCSRDualOrder", u32, [Gp, C.POINTER(Bitmap), C.POINTER(Bitmap), C.POINTER(BFSStats)]),
         ("newPageRankStatsGraphCSR", C.POINTER(PageRankStats), [Gp]),
         ("freePageRankStats", None, [C.POINTER(PageRankStats)]),
         ("pageRankGraphCSR", C.POINTER(PageRankStats), [Ap, Gp]),

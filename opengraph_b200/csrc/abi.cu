@@ -950,6 +950,34 @@ extern "C" struct GraphCSR* graphCSRPreProcessingStep(struct Arguments* argument
   return h;
 }
 
+// graphCSRVertexLabelRemappingDualOrder (graphCSR.c:337-377): each edge
+// list's inverse-label array maps its vertex ids to the other list's.
+extern "C" void graphCSRVertexLabelRemappingDualOrder(struct GraphCSR* graphCSR) {
+  const uint32_t V = graphCSR->num_vertices;
+  EdgeList* el = graphCSR->sorted_edges_array;
+  EdgeList* iel = graphCSR->inverse_sorted_edges_array ? graphCSR->inverse_sorted_edges_array : el;
+  const uint32_t *lab_el = el->label_array, *lab_iel = iel->label_array;
+  uint32_t *inv_el = el->inverse_label_array, *inv_iel = iel->inverse_label_array;
+  if (!lab_el || !lab_iel || !inv_el || !inv_iel) return;  // lists without labels: nothing to map
+  for (uint32_t v = 0; v < V; v++) inv_el[lab_el[v]] = lab_iel[v];
+  if (graphCSR->inverse_sorted_edges_array)
+    for (uint32_t v = 0; v < V; v++) inv_iel[lab_iel[v]] = lab_el[v];
+}
+
+// graphCSRPreProcessingStepDualOrder (graphCSR.c:250-335): without
+// reordering the same graph as graphCSRPreProcessingStep, then the label
+// remapping.  The reordering stages give the two directions different
+// vertex orders, which the DualOrder searches here do not provide.
+extern "C" struct GraphCSR* graphCSRPreProcessingStepDualOrder(struct Arguments* arguments) {
+  if (arguments->lmode || arguments->lmode_l2 || arguments->lmode_l3 || arguments->mmode) {
+    fprintf(stderr, "ogb200: DualOrder preprocessing with reordering (-l/-L/-O/-M) is not provided\n");
+    exit(1);
+  }
+  GraphCSR* g = graphCSRPreProcessingStep(arguments);
+  graphCSRVertexLabelRemappingDualOrder(g);
+  return g;
+}
+
 extern "C" void graphCSRFree(struct GraphCSR* g) {
   if (!g) return;
   mirror_drop(g);
@@ -1115,7 +1143,7 @@ static int bfs_result_to_host(ogb_graph* dg, uint32_t V, uint32_t levels, int* p
 }
 
 static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, uint32_t mode, const char* title,
-                                   bool bitmap_nf) {
+                                   bool bitmap_nf, bool want_trace = false) {
   const uint32_t V = graph->num_vertices;
   // The reference checks source > V (BFS.c:482); source == V would index
   // past the label array there, so it is rejected here too.
@@ -1161,7 +1189,7 @@ static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, 
     const int tid = omp_get_thread_num(), nth = omp_get_num_threads();
     if (tid == 0) {
       run_status = bfs_run(dg->g, (uint32_t)a->source, mode, dg->d_parents.as<int32_t>(),
-                           dg->d_distances.as<uint32_t>(), &r, !quiet(), bitmap_nf, s);
+                           dg->d_distances.as<uint32_t>(), &r, want_trace || !quiet(), bitmap_nf, s);
       t_search = now_s() - t0;
     }
     if (tid > 0 || nth == 1) {
@@ -1225,6 +1253,93 @@ extern "C" struct BFSStats* breadthFirstSearchPushDirectionOptimizedBitmapGraphC
   return bfs_dropin(a, g, BFS_DO, "Starting BFS PUSH/PULL Bitmap (SOURCE NODE)", true);
 }
 
+// ---- DualOrder (BFS.c:1045-1562, graphCSR.c:250-335) ---------------------
+//
+// The DualOrder variants run top-down steps in the forward CSR's vertex
+// order and bottom-up steps in the inverse CSR's, translating the frontier
+// and the parent array between the two orders through the label maps when
+// the direction changes (syncDualOrderParentArrays, BFS.c:182-211: the
+// parents are copied into parents_DualOrder in the other order and the two
+// pointers swapped, once entering and once leaving a bottom-up phase).
+// Without reordering both orders are the identity (this library's
+// preprocessing builds no other), and then the search is the plain one and
+// the only trace of the translation is parents_DualOrder: after a
+// direction-optimized search it holds the parent array as it stood when the
+// last bottom-up phase ended (the sentinels if no bottom-up step ran); the
+// pull-only and push-only variants never translate and leave it at the
+// sentinels.  distances_DualOrder is never written, as in the reference.
+// Graphs whose two orders differ (built by the reference's reordering) are
+// not provided: message and NULL, which the reference's runner skips.
+
+static bool labels_identity(const GraphCSR* g) {
+  const uint32_t V = g->num_vertices;
+  const uint32_t* arrs[4] = {g->sorted_edges_array ? g->sorted_edges_array->label_array : nullptr,
+                             g->sorted_edges_array ? g->sorted_edges_array->inverse_label_array : nullptr,
+                             g->inverse_sorted_edges_array ? g->inverse_sorted_edges_array->label_array : nullptr,
+                             g->inverse_sorted_edges_array ? g->inverse_sorted_edges_array->inverse_label_array
+                                                           : nullptr};
+  int bad = 0;
+  for (const uint32_t* a : arrs) {
+    if (!a) continue;
+    host_par_for(V, [&](size_t lo, size_t hi) {
+      int b = 0;
+      for (size_t v = lo; v < hi; v++) b |= a[v] != (uint32_t)v;
+      if (b) __atomic_store_n(&bad, 1, __ATOMIC_RELAXED);
+    });
+  }
+  return !bad;
+}
+
+static struct BFSStats* bfs_dropin_dual(struct Arguments* a, struct GraphCSR* graph, uint32_t mode,
+                                        const char* title) {
+  if (!labels_identity(graph)) {
+    say(" -----------------------------------------------------\n");
+    say("| %-51s | \n", "DualOrder BFS on reordered labels not provided");
+    say(" -----------------------------------------------------\n");
+    return nullptr;
+  }
+  BFSStats* st = bfs_dropin(a, graph, mode, title, false, mode == BFS_DO);
+  if (mode != BFS_DO || (uint32_t)a->source >= graph->num_vertices) return st;
+  // the step index of the last bottom-up step: its discoveries have depth
+  // index + 1, and everything found up to then is in the snapshot
+  const BfsResult& r = g_last_bfs;
+  int last_bu = -1;
+  for (size_t i = 0; i < r.levels.size(); i++)
+    if (r.levels[i].direction) last_bu = (int)i;
+  if (last_bu < 0) return st;
+  const uint32_t dmax = (uint32_t)last_bu + 1;
+  const int* par = st->parents;
+  const uint32_t* dist = st->distances;
+  int* dual = st->parents_DualOrder;
+  host_par_for(graph->num_vertices, [&](size_t lo, size_t hi) {
+    for (size_t v = lo; v < hi; v++)
+      if (par[v] >= 0 && dist[v] <= dmax) dual[v] = par[v];
+  });
+  return st;
+}
+
+extern "C" struct BFSStats* breadthFirstSearchPullGraphCSRDualOrder(struct Arguments* a, struct GraphCSR* g) {
+  return bfs_dropin_dual(a, g, BFS_PULL, "Starting BFS DualOrder PULL/BU (SOURCE NODE)");
+}
+extern "C" struct BFSStats* breadthFirstSearchPushGraphCSRDualOrder(struct Arguments* a, struct GraphCSR* g) {
+  return bfs_dropin_dual(a, g, BFS_PUSH, "Starting BFS DualOrder PUSH/TD (SOURCE NODE)");
+}
+extern "C" struct BFSStats* breadthFirstSearchDirectionOptimizedGraphCSRDualOrder(struct Arguments* a,
+                                                                                   struct GraphCSR* g) {
+  return bfs_dropin_dual(a, g, BFS_DO, "Starting BFS DualOrder PUSH/PULL(SOURCE NODE)");
+}
+// breadthFirstSearchGraphCSRDualOrder (BFS.c:1045-1068).
+extern "C" struct BFSStats* breadthFirstSearchGraphCSRDualOrder(struct Arguments* a, struct GraphCSR* g) {
+  switch (a->pushpull) {
+    case 0:
+      return breadthFirstSearchPullGraphCSRDualOrder(a, g);
+    case 1:
+      return breadthFirstSearchPushGraphCSRDualOrder(a, g);
+    default:
+      return breadthFirstSearchDirectionOptimizedGraphCSRDualOrder(a, g);
+  }
+}
+
 // breadthFirstSearchGraphCSR (BFS.c:238-268).
 extern "C" struct BFSStats* breadthFirstSearchGraphCSR(struct Arguments* a, struct GraphCSR* g) {
   switch (a->pushpull) {
@@ -1271,6 +1386,16 @@ extern "C" uint32_t bottomUpStepGraphCSR(struct GraphCSR* graph, struct Bitmap* 
   OGB_MUST(bfs_bu_step_host(dg->g, cur->bitarray, next->bitarray, stats->parents, stats->distances, &nf,
                             lib_stream()));
   return nf;
+}
+
+// The DualOrder steps (BFS.c:1442-1562) are the plain steps' code.
+extern "C" uint32_t topDownStepGraphCSRDualOrder(struct GraphCSR* graph, struct ArrayQueue* sharedFrontierQueue,
+                                                 struct ArrayQueue** localFrontierQueues, struct BFSStats* stats) {
+  return topDownStepGraphCSR(graph, sharedFrontierQueue, localFrontierQueues, stats);
+}
+extern "C" uint32_t bottomUpStepGraphCSRDualOrder(struct GraphCSR* graph, struct Bitmap* bitmapCurr,
+                                                  struct Bitmap* bitmapNext, struct BFSStats* stats) {
+  return bottomUpStepGraphCSR(graph, bitmapCurr, bitmapNext, stats);
 }
 
 // --------------------------------------------------------------- PageRank ---

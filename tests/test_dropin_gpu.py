@@ -270,3 +270,66 @@ def test_rank_sort_dropin_matches_reference(og, lib, ref):
         assert C.addressof(p.contents) == ours.ctypes.data
         ref.radixSortEdgesByPageRank(pr.ctypes.data_as(og.f32p), theirs.ctypes.data_as(og.u32p), n)
         assert np.array_equal(ours, theirs), n
+
+
+def test_dualorder_preprocessing_matches_reference(og, lib, ref, files):
+    """graphCSRPreProcessingStepDualOrder: the same arrays and label maps as
+    the reference's (no reordering)."""
+    a = og.default_arguments(fnameb=files["rmat"], sort=1, dflag=1)
+    lib.initializeMersenneState(C.byref(a.mt19937var), 27491095)
+    g = lib.graphCSRPreProcessingStepDualOrder(C.byref(a))
+    ra = ref.arguments(fnameb=files["rmat"], sort=1, dflag=1)
+    from oracle.oracle import silenced_stdout
+    with silenced_stdout():
+        rg = ref.graphCSRPreProcessingStepDualOrder(C.byref(ra))
+    ours, theirs = og.graph_arrays(g), og.graph_arrays(rg)
+    for k, v in theirs.items():
+        if isinstance(v, np.ndarray):
+            assert np.array_equal(ours[k], v), k
+    V = ours["num_vertices"]
+    for side in ("sorted_edges_array", "inverse_sorted_edges_array"):
+        for lab in ("label_array", "inverse_label_array"):
+            o = og.as_numpy(getattr(getattr(g.contents, side).contents, lab), V, np.uint32)
+            t = og.as_numpy(getattr(getattr(rg.contents, side).contents, lab), V, np.uint32)
+            assert np.array_equal(o, t), (side, lab)
+    lib.graphCSRFree(g)
+    ref.graphCSRFree(rg)
+
+
+@pytest.mark.parametrize("pushpull", [0, 1, 2])
+def test_dualorder_bfs_matches_reference(og, lib, ref, files, pushpull):
+    """breadthFirstSearchGraphCSRDualOrder: distances and counts equal to the
+    reference's; parents valid; parents_DualOrder holds the same set of
+    non-sentinel entries as the reference's (the parents at the end of the
+    last bottom-up phase; the sentinels for pull-only / push-only), each
+    equal to our own parent of that vertex."""
+    from oracle.oracle import silenced_stdout
+    g, _ = our_graph(og, lib, files["rmat"])
+    rg = ref.build_graph(files["rmat"])
+    ga = og.graph_arrays(g)
+    V = ga["num_vertices"]
+    for root in (int(np.argmax(ga["f_outdeg"])), 77, 4000):
+        a = og.default_arguments(source=root, pushpull=pushpull)
+        st = lib.breadthFirstSearchGraphCSRDualOrder(C.byref(a), g)
+        s = st.contents
+        dist, par = og.as_numpy(s.distances, V, np.uint32), og.as_numpy(s.parents, V, np.int32)
+        dual = og.as_numpy(s.parents_DualOrder, V, np.int32)
+        counts = (s.processed_nodes, s.iteration)
+        lib.freeBFSStats(st)
+        ra = ref.arguments(source=root, pushpull=pushpull)
+        with silenced_stdout():
+            rst = ref.breadthFirstSearchGraphCSRDualOrder(C.byref(ra), rg)
+        r = rst.contents
+        rdist = og.as_numpy(r.distances, V, np.uint32)
+        rdual = og.as_numpy(r.parents_DualOrder, V, np.int32)
+        rcounts = (r.processed_nodes, r.iteration)
+        ref.freeBFSStats(rst)
+        assert np.array_equal(dist, rdist), (root, pushpull)
+        assert counts == rcounts
+        assert np.array_equal(dual < 0, rdual < 0), (root, pushpull)
+        assert np.array_equal(dual[dual < 0], rdual[rdual < 0])
+        assert np.array_equal(dual[dual >= 0], par[dual >= 0])
+        from test_parity_gpu import check_parents_full
+        check_parents_full(ga, root, par, dist)
+    lib.graphCSRFree(g)
+    ref.graphCSRFree(rg)
