@@ -267,6 +267,13 @@ uint32_t topDownStepGraphCSR(struct GraphCSR *graph, struct ArrayQueue *sharedFr
 uint32_t bottomUpStepGraphCSR(struct GraphCSR *graph, struct Bitmap *bitmapCurr,
                               struct Bitmap *bitmapNext, struct BFSStats *stats);
 
+/* 00_graph_bench/include/structures/graphCSR.h:39 ; graphCSR.c:439-558.  Host
+ * decode of the .csr file; with a GPU present the device copy used by the
+ * algorithms is built while the file decodes.  Label arrays stay NULL. */
+struct GraphCSR *readFromBinFileGraphCSR(const char *fname);
+/* graphCSR.h:40 ; graphCSR.c:380-437.  Writes fname + ".csr". */
+void writeToBinFileGraphCSR(const char *fname, struct GraphCSR *graph);
+
 /* ---- BFS DualOrder (GPU) ------------------------------------------------
  * The DualOrder variants translate the frontier and parents between the
  * forward and inverse CSRs' vertex orders at direction changes.  Provided for

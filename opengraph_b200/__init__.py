@@ -210,6 +210,8 @@ def _api(EL, G):
         ("topDownStepGraphCSR", u32, [Gp, C.POINTER(ArrayQueue), C.POINTER(C.POINTER(ArrayQueue)),
                                       C.POINTER(BFSStats)]),
         ("bottomUpStepGraphCSR", u32, [Gp, C.POINTER(Bitmap), C.POINTER(Bitmap), C.POINTER(BFSStats)]),
+        ("readFromBinFileGraphCSR", Gp, [C.c_char_p]),
+        ("writeToBinFileGraphCSR", None, [C.c_char_p, Gp]),
         ("graphCSRPreProcessingStepDualOrder", Gp, [Ap]),
         ("graphCSRVertexLabelRemappingDualOrder", None, [Gp]),
         ("breadthFirstSearchGraphCSRDualOrder", C.POINTER(BFSStats), [Ap, Gp]),

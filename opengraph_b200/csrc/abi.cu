@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -141,6 +142,16 @@ static void pool_free(void* p, size_t n) {
     if (_st != ::ogb::OK) die_status(#call, _st); \
   } while (0)
 
+// A CUDA runtime call at the OpenGraph boundary: print and exit on failure.
+#define OGB_CUDA_MUST(call)                                                                  \
+  do {                                                                                       \
+    cudaError_t _e = (call);                                                                 \
+    if (_e != cudaSuccess) {                                                                 \
+      fprintf(stderr, "ogb200: %s failed: %s\n", #call, cudaGetErrorString(_e));              \
+      exit(1);                                                                               \
+    }                                                                                        \
+  } while (0)
+
 // Host <-> device copies of malloc'd (pageable) arrays run through pinned
 // bounce buffers: kBufs chunks in flight on the DMA engine while OpenMP
 // threads move the previous chunk between the bounce buffer and the array.
@@ -228,6 +239,23 @@ static int d2h(void* h, const void* d, size_t n, cudaStream_t s) {
     par_memcpy((char*)h + off, b.h[i], std::min(Bounce::kChunk, n - off));
   }
   return OK;
+}
+
+// Run fn(lo, hi) over [0, n) on the OpenMP host threads (as the reference's
+// own parallel loops).
+template <class F>
+static void host_par_for(size_t n, F&& fn) {
+  if (n < (1u << 16)) {
+    fn((size_t)0, n);
+    return;
+  }
+  const long nb = 256;
+  const size_t chunk = (n + nb - 1) / nb;
+#pragma omp parallel for num_threads(host_threads()) schedule(static)
+  for (long b = 0; b < nb; b++) {
+    const size_t lo = (size_t)b * chunk, hi = std::min(n, lo + chunk);
+    if (lo < hi) fn(lo, hi);
+  }
 }
 
 // ---------------------------------------------------------- device mirror ---
@@ -978,6 +1006,247 @@ extern "C" struct GraphCSR* graphCSRPreProcessingStepDualOrder(struct Arguments*
   return g;
 }
 
+// ---- .csr binary file (graphCSR.c:380-558) ----------------------------------
+// Layout, native (little-endian) order: u32 num_edges, u32 num_vertices,
+// [f32 max_weight in the WEIGHTED layout]; then per vertex the forward
+// out_degree, in_degree, edges_idx and, when the graph has an inverse CSR,
+// the inverse's three; then per edge the forward src, dst[, weight] and the
+// inverse's src, dst[, weight].  The reference moves it one value per
+// fread/fwrite; here host threads encode / decode whole chunks.
+
+namespace {
+constexpr uint32_t kCsrW = OGB200_WEIGHTED ? 1u : 0u;  // weight words per edge record
+constexpr size_t kCsrChunk = size_t(1) << 20;           // records per chunk
+
+inline uint32_t fbits(float x) {
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  return u;
+}
+inline float bitsf(uint32_t u) {
+  float x;
+  memcpy(&x, &u, 4);
+  return x;
+}
+}  // namespace
+
+// writeToBinFileGraphCSR (graphCSR.c:380-437): the file is fname + ".csr".
+extern "C" void writeToBinFileGraphCSR(const char* fname, struct GraphCSR* g) {
+  std::string path = std::string(fname) + ".csr";
+  FILE* f = fopen(path.c_str(), "wb");
+  if (!f) err(1, "open: %s", path.c_str());
+  const uint32_t V = g->num_vertices, E = g->num_edges;
+  const bool inv = g->inverse_vertices != nullptr;
+  uint32_t head[3] = {E, V, 0};
+#if OGB200_WEIGHTED
+  head[2] = fbits(g->max_weight);
+#endif
+  fwrite(head, 4, 2 + kCsrW, f);
+  const size_t vw = inv ? 6 : 3, ew = (2 + kCsrW) * (inv ? 2 : 1);
+  std::vector<uint32_t> buf(kCsrChunk * std::max(vw, ew));
+  const Vertex *fv = g->vertices, *iv = g->inverse_vertices;
+  for (size_t v0 = 0; v0 < V; v0 += kCsrChunk) {
+    const size_t n = std::min<size_t>(kCsrChunk, V - v0);
+    host_par_for(n, [&](size_t lo, size_t hi) {
+      for (size_t i = lo; i < hi; i++) {
+        uint32_t* r = &buf[i * vw];
+        const size_t v = v0 + i;
+        r[0] = fv->out_degree[v];
+        r[1] = fv->in_degree[v];
+        r[2] = fv->edges_idx[v];
+        if (inv) {
+          r[3] = iv->out_degree[v];
+          r[4] = iv->in_degree[v];
+          r[5] = iv->edges_idx[v];
+        }
+      }
+    });
+    fwrite(buf.data(), 4 * vw, n, f);
+  }
+  const EdgeList *fe = g->sorted_edges_array, *ie = g->inverse_sorted_edges_array;
+  for (size_t e0 = 0; e0 < E; e0 += kCsrChunk) {
+    const size_t n = std::min<size_t>(kCsrChunk, E - e0);
+    host_par_for(n, [&](size_t lo, size_t hi) {
+      for (size_t i = lo; i < hi; i++) {
+        uint32_t* r = &buf[i * ew];
+        const size_t e = e0 + i;
+        size_t k = 0;
+        r[k++] = fe->edges_array_src[e];
+        r[k++] = fe->edges_array_dest[e];
+#if OGB200_WEIGHTED
+        r[k++] = fbits(fe->edges_array_weight[e]);
+#endif
+        if (inv) {
+          r[k++] = ie->edges_array_src[e];
+          r[k++] = ie->edges_array_dest[e];
+#if OGB200_WEIGHTED
+          r[k++] = fbits(ie->edges_array_weight[e]);
+#endif
+        }
+      }
+    });
+    fwrite(buf.data(), 4 * ew, n, f);
+  }
+  fclose(f);
+}
+
+namespace {
+// Decode the edge records [e0, e0 + n) into the host lists and, when stage is
+// given, the dst (and weight) words of both directions into the pinned
+// stage laid out as [fwd dst | inv dst | fwd w | inv w] of n words each.
+void csr_decode_edges(const uint32_t* rec, size_t ew, bool inv, size_t e0, size_t n, EdgeList* fe, EdgeList* ie,
+                      uint32_t* stage) {
+  host_par_for(n, [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; i++) {
+      const uint32_t* r = rec + (e0 + i) * ew;
+      const size_t e = e0 + i;
+      size_t k = 0;
+      fe->edges_array_src[e] = r[k++];
+      fe->edges_array_dest[e] = r[k++];
+#if OGB200_WEIGHTED
+      fe->edges_array_weight[e] = bitsf(r[k++]);
+#endif
+      if (inv) {
+        ie->edges_array_src[e] = r[k++];
+        ie->edges_array_dest[e] = r[k++];
+#if OGB200_WEIGHTED
+        ie->edges_array_weight[e] = bitsf(r[k++]);
+#endif
+      }
+      if (stage) {
+        stage[i] = fe->edges_array_dest[e];
+        if (inv) stage[n + i] = ie->edges_array_dest[e];
+#if OGB200_WEIGHTED
+        stage[2 * n + i] = fbits(fe->edges_array_weight[e]);
+        if (inv) stage[3 * n + i] = fbits(ie->edges_array_weight[e]);
+#endif
+      }
+    }
+  });
+}
+}  // namespace
+
+// readFromBinFileGraphCSR (graphCSR.c:439-558).  The file is mapped and
+// decoded by host threads; when a GPU is present the device copy the
+// algorithms use is built on the way: the edge section is decoded chunk by
+// chunk into pinned double buffers whose copies to the device run while the
+// next chunk decodes.  The label arrays stay NULL, as in the reference.  A
+// short file leaves the missing values at zero (the reference's fread does
+// the same).
+extern "C" struct GraphCSR* readFromBinFileGraphCSR(const char* fname) {
+  const int fd = open(fname, O_RDONLY);
+  if (fd < 0) err(1, "open: %s", fname);
+  struct stat sb;
+  if (fstat(fd, &sb) != 0) err(1, "open: %s", fname);
+  const size_t bytes = (size_t)sb.st_size;
+  const uint32_t* map = nullptr;
+  if (bytes) {
+    void* p = mmap(nullptr, bytes, PROT_READ, MAP_PRIVATE, fd, 0);
+    if (p == MAP_FAILED) err(1, "open: %s", fname);
+    map = static_cast<const uint32_t*>(p);
+  }
+  const size_t words = bytes / 4;
+  const size_t hw = 2 + kCsrW;
+  const uint32_t E = words > 0 ? map[0] : 0, V = words > 1 ? map[1] : 0;
+  GraphCSR* h = graphCSRNew(V, E, 1);
+  EdgeList* fe = newEdgeList(E);
+  EdgeList* ie = newEdgeList(E);
+  fe->num_vertices = ie->num_vertices = V;
+#if OGB200_WEIGHTED
+  const float mw = words > 2 ? bitsf(map[2]) : 0.0f;
+  h->max_weight = fe->max_weight = ie->max_weight = mw;
+#endif
+  h->sorted_edges_array = fe;
+  h->inverse_sorted_edges_array = ie;
+  const bool inv = true;  // graphCSRNew(.., 1): the reference reads both directions
+  const size_t vw = 6, ew = (2 + kCsrW) * 2;
+  // vertices (a short file leaves zeros)
+  const size_t vavail = words > hw ? std::min<size_t>(V, (words - hw) / vw) : 0;
+  const uint32_t* vrec = map ? map + hw : nullptr;
+  host_par_for(vavail, [&](size_t lo, size_t hi) {
+    for (size_t v = lo; v < hi; v++) {
+      const uint32_t* r = vrec + v * vw;
+      h->vertices->out_degree[v] = r[0];
+      h->vertices->in_degree[v] = r[1];
+      h->vertices->edges_idx[v] = r[2];
+      h->inverse_vertices->out_degree[v] = r[3];
+      h->inverse_vertices->in_degree[v] = r[4];
+      h->inverse_vertices->edges_idx[v] = r[5];
+    }
+  });
+  const size_t ebase = hw + (size_t)V * vw;
+  const size_t eavail = words > ebase ? std::min<size_t>(E, (words - ebase) / ew) : 0;
+  const uint32_t* erec = map ? map + ebase : nullptr;
+  int ndev = 0;
+  const bool gpu = cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0 && V > 0;
+  if (!gpu) {
+    cudaGetLastError();  // clear the no-device error
+    for (size_t e0 = 0; e0 < eavail; e0 += kCsrChunk)
+      csr_decode_edges(erec, ew, inv, e0, std::min(kCsrChunk, eavail - e0), fe, ie, nullptr);
+  } else {
+    cudaStream_t s = lib_stream();
+    ogb_graph* dg = new ogb_graph();
+    DevGraph& g = dg->g;
+    g.V = V;
+    g.E = E;
+    g.weighted = kCsrW != 0;
+    g.build_id++;
+    for (int dir = 0; dir < 2; dir++) {
+      DevCSR& c = dir ? g.inv : g.fwd;
+      const Vertex* hv = dir ? h->inverse_vertices : h->vertices;
+      OGB_MUST(c.dst.alloc((size_t)E * 4 + 4));
+      if (kCsrW) OGB_MUST(c.w.alloc((size_t)E * 4 + 4));
+      OGB_MUST(c.out_degree.alloc((size_t)V * 4 + 4));
+      OGB_MUST(c.in_degree.alloc((size_t)V * 4 + 4));
+      OGB_MUST(c.edges_idx.alloc((size_t)V * 4 + 4));
+      OGB_MUST(c.rows.alloc((size_t)V * 8 + 8));
+      OGB_MUST(h2d(c.out_degree.p, hv->out_degree, (size_t)V * 4, s));
+      OGB_MUST(h2d(c.in_degree.p, hv->in_degree, (size_t)V * 4, s));
+      OGB_MUST(h2d(c.edges_idx.p, hv->edges_idx, (size_t)V * 4, s));
+      OGB_MUST(csr_pack_rows(c, V, s));
+    }
+    // the device arrays past the file's end stay as the host's: zeros
+    if (eavail < E) {
+      for (DevCSR* c : {&g.fwd, &g.inv}) {
+        OGB_CUDA_MUST(cudaMemsetAsync(c->dst.as<uint32_t>() + eavail, 0, (size_t)(E - eavail) * 4, s));
+        if (kCsrW) OGB_CUDA_MUST(cudaMemsetAsync(c->w.as<uint32_t>() + eavail, 0, (size_t)(E - eavail) * 4, s));
+      }
+    }
+    const size_t per = 2 * (1 + kCsrW);  // staged words per edge
+    uint32_t* stage[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2];
+    for (int k = 0; k < 2; k++) {
+      OGB_CUDA_MUST(cudaMallocHost(&stage[k], kCsrChunk * per * 4));
+      OGB_CUDA_MUST(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+    }
+    size_t chunk = 0;
+    for (size_t e0 = 0; e0 < eavail; e0 += kCsrChunk, chunk++) {
+      const int k = (int)(chunk & 1);
+      const size_t n = std::min(kCsrChunk, eavail - e0);
+      OGB_CUDA_MUST(cudaEventSynchronize(ev[k]));  // this buffer's previous copies are done
+      csr_decode_edges(erec, ew, inv, e0, n, fe, ie, stage[k]);
+      const size_t nb = n * 4;
+      OGB_CUDA_MUST(cudaMemcpyAsync(g.fwd.dst.as<uint32_t>() + e0, stage[k], nb, cudaMemcpyHostToDevice, s));
+      OGB_CUDA_MUST(cudaMemcpyAsync(g.inv.dst.as<uint32_t>() + e0, stage[k] + n, nb, cudaMemcpyHostToDevice, s));
+      if (kCsrW) {
+        OGB_CUDA_MUST(cudaMemcpyAsync(g.fwd.w.as<uint32_t>() + e0, stage[k] + 2 * n, nb, cudaMemcpyHostToDevice, s));
+        OGB_CUDA_MUST(cudaMemcpyAsync(g.inv.w.as<uint32_t>() + e0, stage[k] + 3 * n, nb, cudaMemcpyHostToDevice, s));
+      }
+      OGB_CUDA_MUST(cudaEventRecord(ev[k], s));
+    }
+    OGB_CUDA_MUST(cudaStreamSynchronize(s));
+    for (int k = 0; k < 2; k++) {
+      cudaFreeHost(stage[k]);
+      cudaEventDestroy(ev[k]);
+    }
+    mirror_set(h, dg);
+  }
+  if (map) munmap(const_cast<uint32_t*>(map), bytes);
+  close(fd);
+  graphCSRPrint(h);
+  return h;
+}
+
 extern "C" void graphCSRFree(struct GraphCSR* g) {
   if (!g) return;
   mirror_drop(g);
@@ -990,22 +1259,6 @@ extern "C" void graphCSRFree(struct GraphCSR* g) {
 
 // -------------------------------------------------------------------- BFS ---
 
-// Run fn(lo, hi) over [0, n) on the OpenMP host threads (as the reference's
-// own parallel loops).
-template <class F>
-static void host_par_for(size_t n, F&& fn) {
-  if (n < (1u << 16)) {
-    fn((size_t)0, n);
-    return;
-  }
-  const long nb = 256;
-  const size_t chunk = (n + nb - 1) / nb;
-#pragma omp parallel for num_threads(host_threads()) schedule(static)
-  for (long b = 0; b < nb; b++) {
-    const size_t lo = (size_t)b * chunk, hi = std::min(n, lo + chunk);
-    if (lo < hi) fn(lo, hi);
-  }
-}
 
 // BFSStats with its four arrays allocated but not initialized.
 static BFSStats* bfs_stats_alloc(uint32_t V) {
