@@ -37,6 +37,9 @@ def build(ref: bool = True) -> None:
     targets = ["oracle"]
     if ref and os.path.isdir(REFERENCE_SRC):
         targets.append("ref")
+        # the reference's driver, as shipped and linked to the product library
+        if os.path.exists(os.path.join(HERE, "..", "opengraph_b200", "libogb200.so")):
+            targets.append("driver")
     subprocess.run(["make", "-s", "-C", HERE, "-j8", f"REF={REFERENCE_SRC}", *targets], check=True)
 
 

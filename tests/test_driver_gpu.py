@@ -1,0 +1,118 @@
+"""OpenGraph's own driver (00_graph_bench/src/main/open-graph.c) linked
+against libogb200.so, run like a user of the reference runs it, against the
+same driver built from the unmodified reference objects.
+
+Both binaries are made by oracle/Makefile (target ``driver``): the GPU one
+from the reference's objects with every symbol the library exports made
+local (so each cross-file call -- graphRun.c:323,675,1038 and the others --
+binds to the library), the reference one as shipped.  The test checks that
+the linked driver leaves the hot-path symbols undefined (they come from the
+library), then compares the stdout tables of the two runs: graph size, the
+BFS per-level node counts and processed total (exact), PageRank iteration
+count (exact) and rank sum, SPMV sum."""
+import os
+import re
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(os.path.dirname(HERE), "oracle", "_ref")
+OGB = os.path.join(REF_DIR, "open-graph-ogb")
+REF = os.path.join(REF_DIR, "open-graph-ref")
+
+HOT = ("graphCSRPreProcessingStep", "breadthFirstSearchGraphCSR", "pageRankGraphCSR", "SPMVGraphCSR",
+       "radixSortEdgesByPageRank", "generateRandomRootGraphCSR")
+
+
+def _need():
+    if not (os.path.exists(OGB) and os.path.exists(REF)):
+        pytest.skip("driver binaries (oracle/_ref/open-graph-*) not built")
+
+
+def _run(binary, args):
+    env = dict(os.environ)
+    env.pop("OGB200_QUIET", None)  # the tables are what is compared
+    env["OMP_NUM_THREADS"] = "8"
+    r = subprocess.run([binary, *args], capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, (binary, args, r.stdout[-2000:], r.stderr[-2000:])
+    return r.stdout
+
+
+def _graph_size(out):
+    v = re.search(r"Number of Vertices \(V\)\s*\|\s*\n\|\s*(\d+)", out)
+    e = re.search(r"Number of Edges \(E\)\s*\|\s*\n\|\s*(\d+)", out)
+    return int(v.group(1)), int(e.group(1))
+
+
+def _bfs_rows(out):
+    rows = [(m.group(1), int(m.group(2)), int(m.group(3)))
+            for m in re.finditer(r"^\| (TD|BU) (\d+)\s*\| (\d+)\s*\|", out, re.M)]
+    total = int(re.search(r"^\| No OverHead\s*\| (\d+)", out, re.M).group(1))
+    return rows, total
+
+
+def _pr_final(out):
+    m = re.search(r"\| Iterations \| PR Sum\s*\| Error\s*\| Time \(S\)\s*\|\s*\n -+\n\| (\d+)\s*\| ([0-9.]+)", out)
+    return int(m.group(1)), float(m.group(2))
+
+
+def _spmv_sum(out):
+    m = re.search(r"\| Iterations\s*\| Sum\s*\| Time \(S\)\s*\|\s*\n -+\n\| (\d+)\s*\| ([0-9.]+)", out)
+    return int(m.group(1)), float(m.group(2))
+
+
+@pytest.fixture(scope="module")
+def graph_file(tmp_path_factory, og):
+    s, d, _ = og.generate_rmat(14, 16, 21)
+    path = str(tmp_path_factory.mktemp("drv") / "rmat14.bin")
+    og.write_edge_file(path, s, d)
+    return path, int(np.argmax(np.bincount(s, minlength=int(max(s.max(), d.max())) + 1)))
+
+
+def test_linked_driver_takes_the_hot_path_from_the_library():
+    _need()
+    if not shutil.which("nm"):
+        pytest.skip("nm not available")
+    und = subprocess.run(["nm", "-D", "--undefined-only", OGB], capture_output=True, text=True).stdout
+    for sym in HOT:
+        assert re.search(rf"\bU {sym}$", und, re.M), sym
+    ldd = subprocess.run(["ldd", OGB], capture_output=True, text=True).stdout
+    assert "libogb200.so" in ldd
+
+
+@pytest.mark.parametrize("args", [["-a", "0", "-p", "2"], ["-a", "0", "-p", "0"], ["-a", "0", "-p", "1"],
+                                  ["-k", "-o", "1", "-a", "0", "-p", "2"]],
+                         ids=["bfs-do", "bfs-pull", "bfs-push", "bfs-dedup-sort1"])
+def test_driver_bfs_tables_equal(graph_file, args):
+    _need()
+    path, root = graph_file
+    a = ["-f", path, "-r", str(root), *args]
+    ours, theirs = _run(OGB, a), _run(REF, a)
+    assert _graph_size(ours) == _graph_size(theirs)
+    assert _bfs_rows(ours) == _bfs_rows(theirs)
+    assert "Starting BFS" in ours
+
+
+@pytest.mark.parametrize("p", ["0", "1", "6"])
+def test_driver_pagerank_equal(graph_file, p):
+    """pull, push and data-driven pull: the same iteration count under the
+    reference's stop rule; the rank sums (of normalized ranks) agree to 1e-5
+    (the sum of ranks within 1e-6 L1 of each other moves by less)."""
+    _need()
+    path, _ = graph_file
+    a = ["-f", path, "-a", "1", "-p", p, "-i", "30", "-e", "1e-4"]
+    (oi, osum), (ri, rsum) = _pr_final(_run(OGB, a)), _pr_final(_run(REF, a))
+    assert oi == ri and abs(osum - rsum) <= 1e-5, (p, oi, ri, osum, rsum)
+
+
+def test_driver_spmv_equal(graph_file):
+    _need()
+    path, _ = graph_file
+    a = ["-f", path, "-a", "5", "-p", "0", "-i", "5"]
+    (oi, osum), (ri, rsum) = _spmv_sum(_run(OGB, a)), _spmv_sum(_run(REF, a))
+    assert oi == ri and abs(osum - rsum) <= 1e-3 * max(1.0, abs(rsum))

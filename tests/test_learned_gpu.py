@@ -193,3 +193,53 @@ def test_pr_warm_start(torch_cuda, lib):
     assert it_warm < it_plain, (it_warm, it_plain)
     assert np.abs(plain - warm).sum() < 1e-6
     dg.close()
+
+
+@pytest.mark.slow
+def test_trained_switch_gains_on_held_out_rmat(torch_cuda, lib):
+    """What the trained direction switch gains over the plain alpha/beta rule
+    (BFS.c:520-585), on an RMAT graph no training trace came from (scale 21,
+    generator seed 900; training used seeds 100-131): the same roots searched
+    with both rules, L2 flushed before each search, depths identical; the
+    learned total device time must not exceed the plain one by more than 3 %
+    (run-to-run noise of these timings), and the gain is printed."""
+    import opengraph_b200 as og
+    from opengraph_b200.learned import SWITCH, load_weights
+    torch = torch_cuda
+    sw = load_weights(lib, SWITCH)
+    if sw is None:
+        pytest.skip("no trained switch weights")
+    s, d, _ = og.generate_rmat(21, 16, 900)
+    V = 1 << 21
+    dg = lib.device_graph()
+    dg.build(dev(torch, s), dev(torch, d), V, 0)
+    outdeg = host(dg.view(False).out_degree)
+    rng = np.random.default_rng(77)
+    roots = [int(x) for x in rng.choice(np.nonzero(outdeg > 0)[0], size=32, replace=False)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    par = torch.empty(V, dtype=torch.int32, device="cuda")
+    dist = torch.empty(V, dtype=torch.int32, device="cuda")
+    lib.check(lib.ogb_bfs_set_policy(sw.ctypes.data), "set policy")
+    try:
+        ms = {2: [], 3: []}
+        for rep in range(3):  # interleaved repetitions; the best of each is kept
+            for mode in (2, 3):
+                tot = 0.0
+                for i, r in enumerate(roots):
+                    flush.zero_()
+                    torch.cuda.synchronize()
+                    tot += dg.bfs(r, par, dist, mode=mode)["ms"]
+                    if rep == 0 and i < 8:
+                        dcopy = host(dist).copy()
+                        if mode == 2:
+                            ms.setdefault("depths", []).append(dcopy)
+                        else:
+                            assert np.array_equal(dcopy, ms["depths"][i]), r
+                ms[mode].append(tot)
+        plain, learned = min(ms[2]), min(ms[3])
+        print(f"held-out RMAT-21: plain {plain / len(roots):.4f} ms/search, learned {learned / len(roots):.4f} "
+              f"ms/search ({(plain / learned - 1) * 100:+.1f} %)")
+        assert learned <= plain * 1.03
+    finally:
+        lib.ogb_bfs_set_policy(None)
+        dg.close()
