@@ -425,7 +425,35 @@ def stages(lib, og, g, ts, td, tw, V, E, dev, hbm_peak):
                      "reference_stop_rule_iterations": info["iterations"],
                      "device_ms_run": round(info["ms"], 3),
                      "prepare_ms_once_per_graph": round(prepare_ms, 3)}
+    out["data_driven"] = data_driven(g, V, E, dev, hbm_peak)
     return out
+
+
+def data_driven(g, V, E, dev, hbm_peak, eps=1e-4, max_iterations=PR_MAX):
+    """Data-driven PageRank (pageRank.c:2405-2919) against the plain pull at
+    OpenGraph's default epsilon, each run to the reference's stop rule, device
+    time of the whole run (median of 3 after 2 warm runs); SPMV pull / push
+    per iteration (SPMV.c:588-810, weighted graph) with their byte rooflines:
+    pull 12 E + 16 V (in-edge id, weight, x gather; rows, y read + write),
+    push 16 E + 12 V (out-edge id, weight, y atomic read + write; rows, x)."""
+    import torch
+    ranks = torch.empty(V, dtype=torch.float32, device=dev)
+    res = {"epsilon": eps}
+    for mode, name in ((0, "pull"), (6, "dd_pull"), (7, "dd_push"), (8, "dd_pullpush")):
+        for _ in range(2):
+            g.pagerank(ranks, mode=mode, max_iterations=max_iterations, epsilon=eps)
+        runs = [g.pagerank(ranks, mode=mode, max_iterations=max_iterations, epsilon=eps) for _ in range(3)]
+        ms = statistics.median(r["ms"] for r in runs)
+        res[name] = {"ms": round(ms, 3), "iterations": runs[-1]["iterations"], "launches": runs[-1]["launches"]}
+    res["dd_pull_vs_pull"] = round(res["pull"]["ms"] / res["dd_pull"]["ms"], 2)
+    x = torch.empty(V, dtype=torch.float32, device=dev)
+    y = torch.empty(V, dtype=torch.float32, device=dev)
+    for mode, name, alg in ((0, "spmv_pull", 12 * E + 16 * V), (1, "spmv_push", 16 * E + 12 * V)):
+        g.spmv(x, y, mode=mode, iterations=3)
+        ms = statistics.median(g.spmv(x, y, mode=mode, iterations=20)["ms"] / 20 for _ in range(3))
+        res[name] = {"ms_per_iteration": round(ms, 4), "gteps": round(E / ms / 1e6, 1),
+                     "gbs": round(alg / ms / 1e6, 1), "frac": round(alg / ms / 1e6 / hbm_peak, 4)}
+    return res
 
 
 def batching(lib, og, g, roots, V, E, dev, sweep_ms, extra):
@@ -732,8 +760,11 @@ def run_scale(args):
 def run_case(args):
     """One hot-path kernel family on its own, for profiler captures: `bfs`
     runs --n DO-BFS searches, `pr-pull` / `pr-push` one PageRank run of --n
-    iterations, `build` --n sort + CSR builds, all on the seeded RMAT graph
-    of --scale.  Prints one JSON line with the device times."""
+    iterations, `pr-dd-pull` / `pr-dd-push` / `pr-dd-pullpush` one
+    data-driven PageRank run of at most --n iterations at epsilon 1e-4,
+    `spmv-pull` / `spmv-push` --n SPMV iterations, `build` --n sort + CSR
+    builds, all on the seeded RMAT graph of --scale.  Prints one JSON line
+    with the device times."""
     import torch
     import opengraph_b200 as og
     dev = torch.device("cuda", 0)
@@ -772,6 +803,17 @@ def run_case(args):
                 res.append({"root": r, "ms": round(info["ms"], 4), "algorithmic_bytes": int(nbytes),
                             "reached_out_edges": int(info["reached_out_edges"])})
             out["searches"] = res
+        elif args.case.startswith("spmv"):
+            x = torch.empty(V, dtype=torch.float32, device=dev)
+            y = torch.empty(V, dtype=torch.float32, device=dev)
+            info = g.spmv(x, y, mode=0 if args.case == "spmv-pull" else 1, iterations=args.n)
+            out["ms_per_iteration"] = round(info["ms"] / max(args.n, 1), 4)
+        elif args.case.startswith("pr-dd"):
+            ranks = torch.empty(V, dtype=torch.float32, device=dev)
+            mode = {"pr-dd-pull": 6, "pr-dd-push": 7, "pr-dd-pullpush": 8}[args.case]
+            info = g.pagerank(ranks, mode=mode, max_iterations=args.n, epsilon=1e-4)
+            out["ms"] = round(info["ms"], 3)
+            out["iterations"] = info["iterations"]
         else:
             ranks = torch.empty(V, dtype=torch.float32, device=dev)
             mode = 0 if args.case == "pr-pull" else 1
@@ -790,7 +832,8 @@ def main():
     ap.add_argument("--cpu-roots", type=int, default=8)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-stages", action="store_true")
-    ap.add_argument("--case", default="full", choices=["full", "bfs", "pr-pull", "pr-push", "build", "scale"],
+    ap.add_argument("--case", default="full", choices=["full", "bfs", "pr-pull", "pr-push", "pr-dd-pull", "pr-dd-push",
+                                                     "pr-dd-pullpush", "spmv-pull", "spmv-push", "build", "scale"],
                     help="full = the benchmark line; scale = the plain pipeline on RMAT-26 and ER-24; "
                          "the others run one kernel family for profiling")
     ap.add_argument("--scale", type=int, default=SCALE, help="RMAT scale of a --case run")

@@ -49,6 +49,7 @@
 #include "sort.cuh"
 
 #include <algorithm>
+#include <cstddef>
 #include <mutex>
 #include <vector>
 
@@ -59,7 +60,9 @@ namespace {
 constexpr int kT = 256;
 constexpr uint32_t kWarpThr = 32, kCtaThr = 2048, kChunk = 8192;
 constexpr uint32_t kCtaThreads = kT;
-constexpr uint32_t kMarkThr = 32;       // out-rows longer than this are pushed by a CTA
+constexpr uint32_t kMarkThr = 32;       // out-rows longer than this are deferred to a warp
+constexpr uint32_t kOutBig = 1024;      // deferred out-rows longer than this go by chunks
+constexpr uint32_t kOutChunk = 1024;    // edges per chunk of a long out-row
 constexpr uint32_t kDdMaxIters = 1024;
 
 struct DdCtl {
@@ -67,14 +70,20 @@ struct DdCtl {
   uint32_t active[kDdMaxIters];
   uint32_t done_a[kDdMaxIters];   // blocks of the iteration's first kernel that finished
   uint32_t done_b[kDdMaxIters];   // blocks of its second kernel that finished
-  uint32_t nbig[kDdMaxIters];     // deferred long out-rows of the iteration
   uint32_t stop, stop_iter;
-  uint32_t n_med, n_heavy, cur_med, cur_heavy;
+  uint32_t n_med, n_heavy, cur_med, cur_heavy;  // kept across runs of one graph build
+  uint32_t n_och;                               // chunks of the long out-rows
 };
 
 struct DdWork {
   uint32_t V = 0;
-  DevBuf ctl, contrib, flags0, flags1, resid, med, heavy, big_v, big_d, xin;
+  uint32_t built = 0;  // build id of the graph the row classes belong to
+  bool ready = false;
+  // defer: out-row of v pushed / marked by the deferred-row kernel this
+  // iteration; dvec: its push delta; selfcnt: self loops per vertex; och:
+  // {v, j0, j1} chunks of the out-rows longer than kOutBig
+  DevBuf ctl, contrib, flags0, flags1, resid, med, heavy, defer, dvec, selfcnt, och, xin;
+  uint32_t n_och = 0;
   DdCtl* h_ctl = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   ~DdWork() {
@@ -104,6 +113,33 @@ __global__ void dd_count_kernel(uint32_t V, const uint2* __restrict__ rows, DdCt
   warp_atomic_add_total(&ctl->n_heavy, ch);
 }
 
+// Self loops per vertex (counted once per graph build).
+__global__ void dd_self_kernel(uint32_t E, const uint32_t* __restrict__ src, const uint32_t* __restrict__ dst,
+                               uint32_t* __restrict__ selfcnt) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < E; j += gridDim.x * blockDim.x) {
+    const uint32_t u = src[j] & 0x3FFFFFFFu;
+    if (u == (dst[j] & 0x3FFFFFFFu)) atomicAdd(&selfcnt[u], 1u);
+  }
+}
+
+// Chunk counts of the long out-rows, then the chunks {v, j0, j1} at their
+// scanned offsets.
+__global__ void dd_och_count_kernel(uint32_t V, const uint2* __restrict__ rows_f, uint32_t* __restrict__ nch) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const uint32_t d = rows_f[v].y;
+    nch[v] = d > kOutBig ? (d + kOutChunk - 1) / kOutChunk : 0u;
+  }
+}
+__global__ void dd_och_fill_kernel(uint32_t V, const uint2* __restrict__ rows_f, const uint32_t* __restrict__ off,
+                                   uint4* __restrict__ och) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const uint2 r = rows_f[v];
+    if (r.y <= kOutBig) continue;
+    uint32_t k = off[v];
+    for (uint32_t c = 0; c < r.y; c += kOutChunk, k++) och[k] = make_uint4(v, r.x + c, r.x + min(r.y, c + kOutChunk), 0u);
+  }
+}
+
 __global__ void dd_fill_kernel(uint32_t V, const uint2* __restrict__ rows, uint32_t* __restrict__ med,
                                uint32_t* __restrict__ heavy, DdCtl* __restrict__ ctl) {
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
@@ -120,10 +156,25 @@ __global__ void dd_fill_kernel(uint32_t V, const uint2* __restrict__ rows, uint3
 // Sum of term(j) over the row [a, a + d) by one warp (d <= kCtaThr): lane l
 // adds elements l, l + 32, ... in order, then a butterfly fold; every lane
 // returns the sum.
+// Sequential sum s + term(j0) + term(j0 + step) + ... over [j0, j1), the
+// terms fetched four at a time ahead of their additions (same order).
+template <class Term>
+__device__ __forceinline__ float strided_sum4(float s, uint32_t j0, uint32_t j1, uint32_t step, const Term& term) {
+  uint32_t j = j0;
+  for (; j + 3 * step < j1; j += 4 * step) {
+    const float t0 = term(j), t1 = term(j + step), t2 = term(j + 2 * step), t3 = term(j + 3 * step);
+    s = __fadd_rn(s, t0);
+    s = __fadd_rn(s, t1);
+    s = __fadd_rn(s, t2);
+    s = __fadd_rn(s, t3);
+  }
+  for (; j < j1; j += step) s = __fadd_rn(s, term(j));
+  return s;
+}
+
 template <class Term>
 __device__ __forceinline__ float warp_row_sum(uint32_t a, uint32_t d, const Term& term) {
-  float s = 0.0f;
-  for (uint32_t j = a + lane_id(); j < a + d; j += 32) s = __fadd_rn(s, term(j));
+  float s = strided_sum4(0.0f, a + lane_id(), a + d, 32u, term);
 #pragma unroll
   for (int o = 16; o; o >>= 1) s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
   return s;
@@ -138,8 +189,7 @@ __device__ float cta_row_sum(uint32_t a, uint32_t d, const Term& term, float* s_
   float tot = 0.0f;
   for (uint32_t c = 0; c < d; c += kChunk) {
     const uint32_t len = min(kChunk, d - c);
-    float s = 0.0f;
-    for (uint32_t j = a + c + threadIdx.x; j < a + c + len; j += kCtaThreads) s = __fadd_rn(s, term(j));
+    float s = strided_sum4(0.0f, a + c + threadIdx.x, a + c + len, kCtaThreads, term);
 #pragma unroll
     for (int o = 16; o; o >>= 1) s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
     if (lane_id() == 0) s_part[threadIdx.x >> 5] = s;
@@ -171,8 +221,7 @@ __device__ void rows_pass(const uint2* __restrict__ rows, const uint32_t* __rest
     for (uint32_t v = b * kT + threadIdx.x; v < V; v += nb_light * kT) {
       const uint2 r = rows[v];
       if (r.y > kWarpThr || !pol.want(v)) continue;
-      float s = pol.start(v);
-      for (uint32_t j = r.x; j < r.x + r.y; j++) s = __fadd_rn(s, pol.term(j));
+      const float s = strided_sum4(pol.start(v), r.x, r.x + r.y, 1u, [&](uint32_t j) { return pol.term(j); });
       pol.finish(v, s);
     }
   } else if (b < nb_light + nb_med) {
@@ -238,12 +287,13 @@ struct DdParams {
 
 __global__ void dd_contrib_kernel(uint32_t V, const uint32_t* __restrict__ out_degree, const float* __restrict__ pr,
                                   float* __restrict__ contrib, uint8_t* __restrict__ next,
-                                  const DdCtl* __restrict__ ctl) {
+                                  uint8_t* __restrict__ defer, const DdCtl* __restrict__ ctl) {
   if (ctl->stop) return;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     const uint32_t d = out_degree[v];
     contrib[v] = d ? __fdiv_rn(pr[v], (float)d) : 0.0f;
     next[v] = 0;
+    defer[v] = 0;
   }
 }
 
@@ -255,8 +305,7 @@ struct PullPolicy {
   float* pr;
   const uint2* rows_f;
   const uint32_t* nbr_f;
-  uint32_t* big;
-  uint32_t* nbig;
+  uint8_t* defer;
   DdParams p;
   double err = 0.0;
   uint32_t act = 0;
@@ -275,7 +324,7 @@ struct PullPolicy {
       if (r.y <= kMarkThr) {
         for (uint32_t j = r.x; j < r.x + r.y; j++) next[nbr_f[j] & 0x3FFFFFFFu] = 1;
       } else {
-        big[atomicAdd(nbig, 1u)] = v;
+        defer[v] = 1;
       }
     }
   }
@@ -292,18 +341,6 @@ __global__ void __launch_bounds__(kT) dd_pull_kernel(const uint2* __restrict__ r
       ctl->stop_iter = it;
       ctl->stop = 1;
     }
-  }
-}
-
-// Worklist marks of the out-rows deferred by dd_pull_kernel: a CTA per row.
-__global__ void __launch_bounds__(kT) dd_mark_kernel(const uint2* __restrict__ rows_f,
-                                                     const uint32_t* __restrict__ nbr_f,
-                                                     const uint32_t* __restrict__ big, const DdCtl* __restrict__ ctl,
-                                                     uint32_t it, uint8_t* __restrict__ next) {
-  const uint32_t n = ctl->nbig[it];
-  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
-    const uint2 r = rows_f[big[i]];
-    for (uint32_t j = r.x + threadIdx.x; j < r.x + r.y; j += blockDim.x) next[nbr_f[j] & 0x3FFFFFFFu] = 1;
   }
 }
 
@@ -331,34 +368,65 @@ __global__ void __launch_bounds__(kT) dd_resid_kernel(const uint2* __restrict__ 
   rows_pass(rows, med, heavy, ctl->n_med, ctl->n_heavy, V, nb_light, nb_med, pol);
 }
 
-// The pushes of one vertex's out-row [a, a + d) from `lane0` of `nl` lanes
-// (nl = 1: a thread; nl = blockDim.x: a CTA).  Returns the crossings counted.
-__device__ __forceinline__ uint32_t push_row(uint32_t v, uint32_t a, uint32_t d, float delta, uint32_t lane,
-                                             uint32_t nl, const uint32_t* __restrict__ nbr_f, float* resid,
-                                             uint8_t* next, double eps, bool twice) {
+// One push of delta into resid[u]: the returned old value decides whether u
+// crossed epsilon (before <= eps, after >= eps); pull-push (twice) then adds
+// the delta a second time, as the reference does.
+__device__ __forceinline__ uint32_t push_cross(uint32_t u, float prev, float delta, float* resid, uint8_t* next,
+                                               double eps, bool twice) {
+  if ((double)fabsf(__fadd_rn(prev, delta)) >= eps && (double)prev <= eps) {
+    if (twice) atomicAdd(&resid[u], delta);
+    next[u] = 1;
+    return 1;
+  }
+  return 0;
+}
+
+// The pushes of the out-row range [j0, j1) of v by `nl` lanes from `lane`,
+// four pushes in flight per lane.  A self loop's push is dropped (see the
+// header; self_loops counts it).  Returns the crossings counted.
+__device__ __forceinline__ uint32_t push_range(uint32_t v, uint32_t j0, uint32_t j1, float delta, uint32_t lane,
+                                               uint32_t nl, const uint32_t* __restrict__ nbr_f, float* resid,
+                                               uint8_t* next, double eps, bool twice) {
   uint32_t act = 0;
-  for (uint32_t j = a + lane; j < a + d; j += nl) {
-    const uint32_t u = nbr_f[j] & 0x3FFFFFFFu;
-    if (u == v) continue;  // a self loop's push is dropped (see the header)
-    const float prev = atomicAdd(&resid[u], delta);
-    if ((double)fabsf(__fadd_rn(prev, delta)) >= eps && (double)prev <= eps) {
-      act++;
-      if (twice) atomicAdd(&resid[u], delta);
-      next[u] = 1;
+  for (uint32_t j = j0 + lane; j < j1; j += 4 * nl) {
+    uint32_t u[4];
+    float prev[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint32_t jj = j + k * nl;
+      u[k] = jj < j1 ? (nbr_f[jj] & 0x3FFFFFFFu) : v;
     }
+#pragma unroll
+    for (int k = 0; k < 4; k++) prev[k] = u[k] != v ? atomicAdd(&resid[u[k]], delta) : 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (u[k] != v) act += push_cross(u[k], prev[k], delta, resid, next, eps, twice);
   }
   return act;
 }
 
-// A self loop's crossings, counted as a sequential run of the reference
+// The same, one push at a time (a thread's short out-row in pull-push: a
+// repeated neighbour sees its earlier push and second add, as in a
+// sequential run).
+__device__ __forceinline__ uint32_t push_row_seq(uint32_t v, uint32_t a, uint32_t d, float delta,
+                                                 const uint32_t* __restrict__ nbr_f, float* resid, uint8_t* next,
+                                                 double eps, bool twice) {
+  uint32_t act = 0;
+  for (uint32_t j = a; j < a + d; j++) {
+    const uint32_t u = nbr_f[j] & 0x3FFFFFFFu;
+    if (u == v) continue;
+    act += push_cross(u, atomicAdd(&resid[u], delta), delta, resid, next, eps, twice);
+  }
+  return act;
+}
+
+// A vertex's `ns` self loops, counted as a sequential run of the reference
 // counts them (the vertex's own residual, read before it is zeroed).
-__device__ __forceinline__ uint32_t self_loops(uint32_t v, uint32_t a, uint32_t d, float r, float delta,
-                                               const uint32_t* __restrict__ nbr_f, uint8_t* next, double eps,
-                                               bool twice) {
+__device__ __forceinline__ uint32_t self_loops(uint32_t v, uint32_t ns, float r, float delta, uint8_t* next,
+                                               double eps, bool twice) {
   uint32_t act = 0;
   float acc = r;
-  for (uint32_t j = a; j < a + d; j++) {
-    if ((nbr_f[j] & 0x3FFFFFFFu) != v) continue;
+  for (uint32_t k = 0; k < ns; k++) {
     const float prev = acc;
     acc = __fadd_rn(acc, delta);
     if ((double)fabsf(acc) >= eps && (double)prev <= eps) {
@@ -371,11 +439,11 @@ __device__ __forceinline__ uint32_t self_loops(uint32_t v, uint32_t a, uint32_t 
 }
 
 // Update of one active vertex given its new rank and the residual it took
-// (atomically, before): error, rank store, and the pushes (short out-rows
-// here, long ones deferred).
+// (atomically, before): error, rank store, and the pushes (out-rows of at
+// most kMarkThr edges here, longer ones deferred with their delta).
 __device__ __forceinline__ void push_vertex(uint32_t v, float nv, float old, float r, const uint2* rows_f,
-                                            const uint32_t* nbr_f, float* pr, float* resid, uint8_t* next,
-                                            uint32_t* big_v, float* big_d, uint32_t* nbig, const DdParams& p,
+                                            const uint32_t* nbr_f, const uint32_t* selfcnt, float* pr, float* resid,
+                                            uint8_t* next, uint8_t* defer, float* dvec, const DdParams& p,
                                             bool twice, double& err, uint32_t& act) {
   const float fv = (float)p.V;
   err += (double)fabsf(__fsub_rn(__fdiv_rn(nv, fv), __fdiv_rn(old, fv)));
@@ -383,20 +451,22 @@ __device__ __forceinline__ void push_vertex(uint32_t v, float nv, float old, flo
   const uint2 row = rows_f[v];
   if (!row.y) return;  // no pushes (the reference's delta divides by zero here and is never used)
   const float delta = __fmul_rn(p.damp, __fdiv_rn(r, (float)row.y));
-  act += self_loops(v, row.x, row.y, r, delta, nbr_f, next, p.epsilon, twice);
+  const uint32_t ns = selfcnt[v];
+  if (ns) act += self_loops(v, ns, r, delta, next, p.epsilon, twice);
   if (row.y <= kMarkThr) {
-    act += push_row(v, row.x, row.y, delta, 0, 1, nbr_f, resid, next, p.epsilon, twice);
+    act += twice ? push_row_seq(v, row.x, row.y, delta, nbr_f, resid, next, p.epsilon, true)
+                 : push_range(v, row.x, row.x + row.y, delta, 0, 1, nbr_f, resid, next, p.epsilon, false);
   } else {
-    const uint32_t k = atomicAdd(nbig, 1u);
-    big_v[k] = v;
-    big_d[k] = delta;
+    dvec[v] = delta;
+    defer[v] = 1;
   }
 }
 
 __global__ void __launch_bounds__(kT) dd_push_kernel(uint32_t V, const uint8_t* __restrict__ cur, uint8_t* next,
                                                      const uint2* __restrict__ rows_f,
-                                                     const uint32_t* __restrict__ nbr_f, float* pr, float* resid,
-                                                     uint32_t* big_v, float* big_d, DdParams p,
+                                                     const uint32_t* __restrict__ nbr_f,
+                                                     const uint32_t* __restrict__ selfcnt, float* pr, float* resid,
+                                                     uint8_t* defer, float* dvec, DdParams p,
                                                      DdCtl* __restrict__ ctl, uint32_t it) {
   if (ctl->stop) return;
   double err = 0.0;
@@ -406,7 +476,7 @@ __global__ void __launch_bounds__(kT) dd_push_kernel(uint32_t V, const uint8_t* 
     const float r = atomicExch(&resid[v], 0.0f);
     const float old = pr[v];
     const float nv = __fadd_rn(r, old);  // the reference's aResiduals[v] + pageRanks[v]
-    push_vertex(v, nv, old, r, rows_f, nbr_f, pr, resid, next, big_v, big_d, &ctl->nbig[it], p, false, err, act);
+    push_vertex(v, nv, old, r, rows_f, nbr_f, selfcnt, pr, resid, next, defer, dvec, p, false, err, act);
   }
   block_totals(err, act, &ctl->err[it], &ctl->active[it], &ctl->done_a[it]);
 }
@@ -421,9 +491,9 @@ struct PullPushPolicy {
   float* resid;
   const uint2* rows_f;
   const uint32_t* nbr_f;
-  uint32_t* big_v;
-  float* big_d;
-  uint32_t* nbig;
+  const uint32_t* selfcnt;
+  uint8_t* defer;
+  float* dvec;
   DdParams p;
   double err = 0.0;
   uint32_t act = 0;
@@ -437,7 +507,7 @@ struct PullPushPolicy {
     const float nv = __fadd_rn(p.base_pr, __fmul_rn(p.damp, s));
     const float old = pr[v];
     const float r = atomicExch(&resid[v], 0.0f);
-    push_vertex(v, nv, old, r, rows_f, nbr_f, pr, resid, next, big_v, big_d, nbig, p, true, err, act);
+    push_vertex(v, nv, old, r, rows_f, nbr_f, selfcnt, pr, resid, next, defer, dvec, p, true, err, act);
   }
 };
 
@@ -447,26 +517,52 @@ __global__ void __launch_bounds__(kT) dd_pullpush_kernel(const uint2* __restrict
                                                          uint32_t nb_med, PullPushPolicy pol,
                                                          DdCtl* __restrict__ ctl, uint32_t it) {
   if (ctl->stop) return;
-  pol.nbig = &ctl->nbig[it];
   rows_pass(rows, med, heavy, ctl->n_med, ctl->n_heavy, pol.p.V, nb_light, nb_med, pol);
   block_totals(pol.err, pol.act, &ctl->err[it], &ctl->active[it], &ctl->done_a[it]);
 }
 
-// The deferred long out-rows (a CTA per row), then the iteration's stop
-// decision by the last block: no crossing anywhere in the iteration.
-__global__ void __launch_bounds__(kT) dd_bigpush_kernel(const uint2* __restrict__ rows_f,
-                                                        const uint32_t* __restrict__ nbr_f, float* resid,
-                                                        uint8_t* next, const uint32_t* __restrict__ big_v,
-                                                        const float* __restrict__ big_d, double eps, bool twice,
-                                                        DdCtl* __restrict__ ctl, uint32_t it) {
+// The deferred out-rows of an iteration (defer[v] set): first the chunks of
+// the rows longer than kOutBig, a warp per chunk; then every other deferred
+// row, a warp per row, found by a warp scan of the flags of 32 vertices at a
+// time.  kPush: the pushes of delta dvec[v] (crossings counted, the last
+// block decides the stop); otherwise the worklist marks of the pull.
+template <bool kPush>
+__global__ void __launch_bounds__(kT) dd_defer_kernel(uint32_t V, const uint2* __restrict__ rows_f,
+                                                      const uint32_t* __restrict__ nbr_f,
+                                                      const uint8_t* __restrict__ defer,
+                                                      const float* __restrict__ dvec, const uint4* __restrict__ och,
+                                                      float* resid, uint8_t* next, double eps, bool twice,
+                                                      DdCtl* __restrict__ ctl, uint32_t it) {
   if (ctl->stop) return;
-  const uint32_t n = ctl->nbig[it];
+  const uint32_t lane = lane_id();
+  const uint32_t gw = (blockIdx.x * kT + threadIdx.x) >> 5, nw = (gridDim.x * kT) >> 5;
+  const uint32_t n_och = ctl->n_och;
   uint32_t act = 0;
-  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
-    const uint32_t v = big_v[i];
-    const uint2 r = rows_f[v];
-    act += push_row(v, r.x, r.y, big_d[i], threadIdx.x, blockDim.x, nbr_f, resid, next, eps, twice);
+  for (uint32_t c = gw; c < n_och; c += nw) {
+    const uint4 e = och[c];
+    if (!defer[e.x]) continue;  // warp-uniform
+    if (kPush)
+      act += push_range(e.x, e.y, e.z, dvec[e.x], lane, 32, nbr_f, resid, next, eps, twice);
+    else
+      for (uint32_t j = e.y + lane; j < e.z; j += 32) next[nbr_f[j] & 0x3FFFFFFFu] = 1;
   }
+  for (uint32_t base = gw * 32; base < V; base += nw * 32) {
+    const uint32_t v = base + lane;
+    uint2 r = make_uint2(0u, 0u);
+    if (v < V && defer[v]) r = rows_f[v];
+    uint32_t m = __ballot_sync(0xffffffffu, r.y > 0 && r.y <= kOutBig);
+    while (m) {
+      const uint32_t l = (uint32_t)__ffs(m) - 1;
+      m &= m - 1;
+      const uint32_t vv = base + l;
+      const uint32_t a = __shfl_sync(0xffffffffu, r.x, l), d = __shfl_sync(0xffffffffu, r.y, l);
+      if (kPush)
+        act += push_range(vv, a, a + d, dvec[vv], lane, 32, nbr_f, resid, next, eps, twice);
+      else
+        for (uint32_t j = a + lane; j < a + d; j += 32) next[nbr_f[j] & 0x3FFFFFFFu] = 1;
+    }
+  }
+  if (!kPush) return;
   if (block_totals(0.0, act, &ctl->err[it], &ctl->active[it], &ctl->done_b[it])) {
     if (ld_volatile_u32(&ctl->active[it]) == 0) {
       ctl->stop_iter = it;
@@ -484,9 +580,13 @@ __global__ void dd_init_kernel(uint32_t V, float base_pr, float* __restrict__ pr
   }
 }
 
-__global__ void dd_clear_kernel(uint32_t V, uint8_t* __restrict__ next, const DdCtl* __restrict__ ctl) {
+__global__ void dd_clear_kernel(uint32_t V, uint8_t* __restrict__ next, uint8_t* __restrict__ defer,
+                                const DdCtl* __restrict__ ctl) {
   if (ctl->stop) return;
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) next[v] = 0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    next[v] = 0;
+    defer[v] = 0;
+  }
 }
 
 __global__ void dd_normalize_kernel(uint32_t V, float* __restrict__ pr) {
@@ -526,31 +626,41 @@ __global__ void __launch_bounds__(kT) spmv_pull_kernel(const uint2* __restrict__
   rows_pass(rows, med, heavy, ctl->n_med, ctl->n_heavy, V, nb_light, nb_med, pol);
 }
 
-// Push: rows of at most kWarpThr out-edges by a thread, longer ones by a warp
+// Push: rows of at most kWarpThr out-edges by a thread, rows up to kOutBig
+// by a warp, longer ones in chunks of kOutChunk edges, a warp per chunk
 // (order does not matter: float atomics, as the reference's omp atomic).
+__device__ __forceinline__ float spmv_term(const float* __restrict__ w, uint32_t j, float xv) {
+  return __fmul_rn(w ? w[j] : 0.0001f, xv);
+}
+
 __global__ void __launch_bounds__(kT) spmv_push_kernel(uint32_t V, const uint2* __restrict__ rows_f,
                                                        const uint32_t* __restrict__ nbr_f, const float* __restrict__ w,
-                                                       const float* __restrict__ x, float* __restrict__ y) {
+                                                       const float* __restrict__ x, float* __restrict__ y,
+                                                       const uint4* __restrict__ och, const DdCtl* __restrict__ ctl) {
+  const uint32_t lane = lane_id();
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t n_och = ctl->n_och;
+  for (uint32_t c = gw; c < n_och; c += nw) {
+    const uint4 e = och[c];
+    const float xv = x[e.x];
+    for (uint32_t j = e.y + lane; j < e.z; j += 32) atomicAdd(&y[nbr_f[j] & 0x3FFFFFFFu], spmv_term(w, j, xv));
+  }
   for (uint32_t base = gw * 32; base < V; base += nw * 32) {
-    const uint32_t v = base + lane_id();
+    const uint32_t v = base + lane;
     uint2 r = make_uint2(0u, 0u);
     if (v < V) r = rows_f[v];
-    const bool own = v < V && r.y <= kWarpThr;
-    if (own) {
+    if (r.y && r.y <= kWarpThr) {
       const float xv = x[v];
-      for (uint32_t j = r.x; j < r.x + r.y; j++)
-        atomicAdd(&y[nbr_f[j] & 0x3FFFFFFFu], __fmul_rn(w ? w[j] : 0.0001f, xv));
+      for (uint32_t j = r.x; j < r.x + r.y; j++) atomicAdd(&y[nbr_f[j] & 0x3FFFFFFFu], spmv_term(w, j, xv));
     }
-    uint32_t longm = __ballot_sync(0xffffffffu, v < V && !own);
+    uint32_t longm = __ballot_sync(0xffffffffu, r.y > kWarpThr && r.y <= kOutBig);
     while (longm) {
       const uint32_t l = (uint32_t)__ffs(longm) - 1;
       longm &= longm - 1;
       const uint32_t vv = base + l;
-      const uint2 rr = make_uint2(__shfl_sync(0xffffffffu, r.x, l), __shfl_sync(0xffffffffu, r.y, l));
+      const uint32_t a = __shfl_sync(0xffffffffu, r.x, l), d = __shfl_sync(0xffffffffu, r.y, l);
       const float xv = x[vv];
-      for (uint32_t j = rr.x + lane_id(); j < rr.x + rr.y; j += 32)
-        atomicAdd(&y[nbr_f[j] & 0x3FFFFFFFu], __fmul_rn(w ? w[j] : 0.0001f, xv));
+      for (uint32_t j = a + lane; j < a + d; j += 32) atomicAdd(&y[nbr_f[j] & 0x3FFFFFFFu], spmv_term(w, j, xv));
     }
   }
 }
@@ -584,23 +694,54 @@ int dd_work_get(DevGraph& g, DdWork** out, cudaStream_t s) {
     OGB_TRY(w->resid.alloc((size_t)V * 4 + 16));
     OGB_TRY(w->med.alloc((size_t)V * 4 + 16));
     OGB_TRY(w->heavy.alloc((size_t)V * 4 + 16));
-    OGB_TRY(w->big_v.alloc((size_t)V * 4 + 16));
-    OGB_TRY(w->big_d.alloc((size_t)V * 4 + 16));
+    OGB_TRY(w->defer.alloc((size_t)V + 16));
+    OGB_TRY(w->dvec.alloc((size_t)V * 4 + 16));
+    OGB_TRY(w->selfcnt.alloc((size_t)V * 4 + 16));
     OGB_TRY(w->xin.alloc((size_t)V * 4 + 16));
     w->V = V;
+    w->ready = false;
   }
   if (!w->h_ctl) OGB_CUDA(cudaMallocHost(&w->h_ctl, sizeof(DdCtl)));
   if (!w->ev0) {
     OGB_CUDA(cudaEventCreate(&w->ev0));
     OGB_CUDA(cudaEventCreate(&w->ev1));
   }
-  OGB_CUDA(cudaMemsetAsync(w->ctl.p, 0, sizeof(DdCtl), s));
-  // the inverse rows' classes, kept with the graph's build id
   DdCtl* ctl = w->ctl.as<DdCtl>();
+  if (w->ready && w->built == g.build_id) {
+    // per-run counters only; the row classes and chunk count stay
+    OGB_CUDA(cudaMemsetAsync(w->ctl.p, 0, offsetof(DdCtl, n_med), s));
+    *out = w;
+    return OK;
+  }
+  // once per graph build: the inverse rows' classes, the self loops, and the
+  // chunks of the long out-rows
+  OGB_CUDA(cudaMemsetAsync(w->ctl.p, 0, sizeof(DdCtl), s));
+  OGB_CUDA(cudaMemsetAsync(w->defer.p, 0, (size_t)V + 16, s));
+  OGB_CUDA(cudaMemsetAsync(w->selfcnt.p, 0, (size_t)V * 4 + 16, s));
   const int grid = sm_count() * 8;
   dd_count_kernel<<<grid, kT, 0, s>>>(V, g.inv.d_rows(), ctl);
   dd_fill_kernel<<<grid, kT, 0, s>>>(V, g.inv.d_rows(), w->med.as<uint32_t>(), w->heavy.as<uint32_t>(), ctl);
+  dd_self_kernel<<<grid, kT, 0, s>>>(g.E, g.fwd.d_src(), g.fwd.d_dst(), w->selfcnt.as<uint32_t>());
   OGB_CUDA(cudaGetLastError());
+  DevBuf tmp;
+  OGB_TRY(tmp.alloc(((size_t)V * 2 + 4 + scan_tmp_words(V)) * 4));
+  uint32_t* nch = tmp.as<uint32_t>();
+  uint32_t* off = nch + V + 2;
+  uint32_t* stmp = off + V + 2;
+  dd_och_count_kernel<<<grid, kT, 0, s>>>(V, g.fwd.d_rows(), nch);
+  OGB_CUDA(cudaGetLastError());
+  OGB_TRY(scan_exclusive_u32(nch, off, V, stmp, s));
+  uint32_t total = 0;
+  OGB_CUDA(cudaMemcpyAsync(&total, off + V, 4, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  OGB_TRY(w->och.alloc((size_t)total * 16 + 16));
+  dd_och_fill_kernel<<<grid, kT, 0, s>>>(V, g.fwd.d_rows(), off, w->och.as<uint4>());
+  OGB_CUDA(cudaGetLastError());
+  w->n_och = total;
+  OGB_CUDA(cudaMemcpyAsync(&ctl->n_och, &w->n_och, 4, cudaMemcpyHostToDevice, s));
+  OGB_CUDA(cudaStreamSynchronize(s));  // the host copy source and tmp outlive the copies
+  w->built = g.build_id;
+  w->ready = true;
   *out = w;
   return OK;
 }
@@ -664,26 +805,30 @@ int pagerank_dd_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsil
   }
   OGB_CUDA(cudaGetLastError());
   for (uint32_t it = 0; it < max_iters; it++) {
+    uint8_t* defer = w->defer.as<uint8_t>();
+    float* dvec = w->dvec.as<float>();
+    const uint4* och = w->och.as<uint4>();
     if (mode == PR_DD_PULL) {
-      dd_contrib_kernel<<<sms * 8, kT, 0, s>>>(V, g.fwd.d_out_degree(), ranks, w->contrib.as<float>(), nxt, ctl);
-      PullPolicy pol{cur, nxt, w->contrib.as<float>(), g.inv.d_dst(), ranks, g.fwd.d_rows(), g.fwd.d_dst(),
-                     w->big_v.as<uint32_t>(), &ctl->nbig[it], p};
+      dd_contrib_kernel<<<sms * 8, kT, 0, s>>>(V, g.fwd.d_out_degree(), ranks, w->contrib.as<float>(), nxt, defer,
+                                               ctl);
+      PullPolicy pol{cur, nxt, w->contrib.as<float>(), g.inv.d_dst(), ranks, g.fwd.d_rows(), g.fwd.d_dst(), defer, p};
       dd_pull_kernel<<<G.total(), kT, 0, s>>>(g.inv.d_rows(), w->med.as<uint32_t>(), w->heavy.as<uint32_t>(),
                                                G.light, G.med, pol, ctl, it);
-      dd_mark_kernel<<<sms * 2, kT, 0, s>>>(g.fwd.d_rows(), g.fwd.d_dst(), w->big_v.as<uint32_t>(), ctl, it, nxt);
+      dd_defer_kernel<false><<<sms * 8, kT, 0, s>>>(V, g.fwd.d_rows(), g.fwd.d_dst(), defer, dvec, och, resid, nxt,
+                                                    epsilon, false, ctl, it);
     } else {
-      dd_clear_kernel<<<sms * 8, kT, 0, s>>>(V, nxt, ctl);
+      dd_clear_kernel<<<sms * 8, kT, 0, s>>>(V, nxt, defer, ctl);
       if (mode == PR_DD_PUSH) {
-        dd_push_kernel<<<sms * 8, kT, 0, s>>>(V, cur, nxt, g.fwd.d_rows(), g.fwd.d_dst(), ranks, resid,
-                                               w->big_v.as<uint32_t>(), w->big_d.as<float>(), p, ctl, it);
+        dd_push_kernel<<<sms * 8, kT, 0, s>>>(V, cur, nxt, g.fwd.d_rows(), g.fwd.d_dst(), w->selfcnt.as<uint32_t>(),
+                                               ranks, resid, defer, dvec, p, ctl, it);
       } else {
-        PullPushPolicy pol{cur, nxt, g.inv.d_dst(), g.fwd.d_out_degree(), ranks, resid, g.fwd.d_rows(), g.fwd.d_dst(),
-                           w->big_v.as<uint32_t>(), w->big_d.as<float>(), nullptr, p};
+        PullPushPolicy pol{cur,   nxt,  g.inv.d_dst(), g.fwd.d_out_degree(), ranks, resid, g.fwd.d_rows(),
+                           g.fwd.d_dst(), w->selfcnt.as<uint32_t>(), defer, dvec, p};
         dd_pullpush_kernel<<<G.total(), kT, 0, s>>>(g.inv.d_rows(), w->med.as<uint32_t>(), w->heavy.as<uint32_t>(),
                                                      G.light, G.med, pol, ctl, it);
       }
-      dd_bigpush_kernel<<<sms * 2, kT, 0, s>>>(g.fwd.d_rows(), g.fwd.d_dst(), resid, nxt, w->big_v.as<uint32_t>(),
-                                                w->big_d.as<float>(), epsilon, mode == PR_DD_PULLPUSH, ctl, it);
+      dd_defer_kernel<true><<<sms * 8, kT, 0, s>>>(V, g.fwd.d_rows(), g.fwd.d_dst(), defer, dvec, och, resid, nxt,
+                                                   epsilon, mode == PR_DD_PULLPUSH, ctl, it);
     }
     OGB_CUDA(cudaGetLastError());
     launches += 3;
@@ -738,7 +883,7 @@ int spmv_run(DevGraph& g, uint32_t mode, uint32_t iterations, float* x, float* y
   } else {
     for (uint32_t it = 0; it < iterations; it++)
       spmv_push_kernel<<<sms * 8, kT, 0, s>>>(V, g.fwd.d_rows(), g.fwd.d_dst(), g.weighted ? g.fwd.d_w() : nullptr, x,
-                                               y);
+                                               y, w->och.as<uint4>(), w->ctl.as<DdCtl>());
   }
   OGB_CUDA(cudaGetLastError());
   OGB_CUDA(cudaEventRecord(w->ev1, s));
