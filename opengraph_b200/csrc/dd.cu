@@ -285,6 +285,13 @@ struct DdParams {
 
 // ---- data-driven pull (6) -----------------------------------------------------
 
+// Put u on the next worklist.  Most marks of an iteration hit a vertex that
+// is marked already (RMAT hubs are in-neighbours of many active vertices):
+// the flag is read first, from L1 / L2, and only a clear flag is written.
+__device__ __forceinline__ void mark(uint8_t* next, uint32_t u) {
+  if (!next[u]) next[u] = 1;
+}
+
 __global__ void dd_contrib_kernel(uint32_t V, const uint32_t* __restrict__ out_degree, const float* __restrict__ pr,
                                   float* __restrict__ contrib, uint8_t* __restrict__ next,
                                   uint8_t* __restrict__ defer, const DdCtl* __restrict__ ctl) {
@@ -322,7 +329,16 @@ struct PullPolicy {
       act++;
       const uint2 r = rows_f[v];
       if (r.y <= kMarkThr) {
-        for (uint32_t j = r.x; j < r.x + r.y; j++) next[nbr_f[j] & 0x3FFFFFFFu] = 1;
+        const uint32_t e = r.x + r.y;
+        uint32_t j = r.x;
+        for (; j + 3 < e; j += 4) {  // four neighbour ids in flight
+          const uint32_t u0 = nbr_f[j], u1 = nbr_f[j + 1], u2 = nbr_f[j + 2], u3 = nbr_f[j + 3];
+          mark(next, u0 & 0x3FFFFFFFu);
+          mark(next, u1 & 0x3FFFFFFFu);
+          mark(next, u2 & 0x3FFFFFFFu);
+          mark(next, u3 & 0x3FFFFFFFu);
+        }
+        for (; j < e; j++) mark(next, nbr_f[j] & 0x3FFFFFFFu);
       } else {
         defer[v] = 1;
       }
@@ -383,7 +399,11 @@ __device__ __forceinline__ uint32_t push_cross(uint32_t u, float prev, float del
 
 // The pushes of the out-row range [j0, j1) of v by `nl` lanes from `lane`,
 // four pushes in flight per lane.  A self loop's push is dropped (see the
-// header; self_loops counts it).  Returns the crossings counted.
+// header; self_loops counts it).  Returns the crossings counted.  In
+// pull-push a neighbour repeated within one group of four sees the group's
+// earlier push before that push's second add rather than after it: the adds
+// commute, and a residual that crossed epsilon is above it, so the later
+// push counts no crossing either way.
 __device__ __forceinline__ uint32_t push_range(uint32_t v, uint32_t j0, uint32_t j1, float delta, uint32_t lane,
                                                uint32_t nl, const uint32_t* __restrict__ nbr_f, float* resid,
                                                uint8_t* next, double eps, bool twice) {
@@ -401,21 +421,6 @@ __device__ __forceinline__ uint32_t push_range(uint32_t v, uint32_t j0, uint32_t
 #pragma unroll
     for (int k = 0; k < 4; k++)
       if (u[k] != v) act += push_cross(u[k], prev[k], delta, resid, next, eps, twice);
-  }
-  return act;
-}
-
-// The same, one push at a time (a thread's short out-row in pull-push: a
-// repeated neighbour sees its earlier push and second add, as in a
-// sequential run).
-__device__ __forceinline__ uint32_t push_row_seq(uint32_t v, uint32_t a, uint32_t d, float delta,
-                                                 const uint32_t* __restrict__ nbr_f, float* resid, uint8_t* next,
-                                                 double eps, bool twice) {
-  uint32_t act = 0;
-  for (uint32_t j = a; j < a + d; j++) {
-    const uint32_t u = nbr_f[j] & 0x3FFFFFFFu;
-    if (u == v) continue;
-    act += push_cross(u, atomicAdd(&resid[u], delta), delta, resid, next, eps, twice);
   }
   return act;
 }
@@ -439,23 +444,24 @@ __device__ __forceinline__ uint32_t self_loops(uint32_t v, uint32_t ns, float r,
 }
 
 // Update of one active vertex given its new rank and the residual it took
-// (atomically, before): error, rank store, and the pushes (out-rows of at
+// (atomically, before): error, rank store (and, for pull-push, the rank /
+// out-degree its out-neighbours' pulls read), and the pushes (out-rows of at
 // most kMarkThr edges here, longer ones deferred with their delta).
 __device__ __forceinline__ void push_vertex(uint32_t v, float nv, float old, float r, const uint2* rows_f,
-                                            const uint32_t* nbr_f, const uint32_t* selfcnt, float* pr, float* resid,
-                                            uint8_t* next, uint8_t* defer, float* dvec, const DdParams& p,
-                                            bool twice, double& err, uint32_t& act) {
+                                            const uint32_t* nbr_f, const uint32_t* selfcnt, float* pr, float* contrib,
+                                            float* resid, uint8_t* next, uint8_t* defer, float* dvec,
+                                            const DdParams& p, bool twice, double& err, uint32_t& act) {
   const float fv = (float)p.V;
   err += (double)fabsf(__fsub_rn(__fdiv_rn(nv, fv), __fdiv_rn(old, fv)));
   pr[v] = nv;
   const uint2 row = rows_f[v];
   if (!row.y) return;  // no pushes (the reference's delta divides by zero here and is never used)
+  if (contrib) contrib[v] = __fdiv_rn(nv, (float)row.y);
   const float delta = __fmul_rn(p.damp, __fdiv_rn(r, (float)row.y));
   const uint32_t ns = selfcnt[v];
   if (ns) act += self_loops(v, ns, r, delta, next, p.epsilon, twice);
   if (row.y <= kMarkThr) {
-    act += twice ? push_row_seq(v, row.x, row.y, delta, nbr_f, resid, next, p.epsilon, true)
-                 : push_range(v, row.x, row.x + row.y, delta, 0, 1, nbr_f, resid, next, p.epsilon, false);
+    act += push_range(v, row.x, row.x + row.y, delta, 0, 1, nbr_f, resid, next, p.epsilon, twice);
   } else {
     dvec[v] = delta;
     defer[v] = 1;
@@ -476,17 +482,21 @@ __global__ void __launch_bounds__(kT) dd_push_kernel(uint32_t V, const uint8_t* 
     const float r = atomicExch(&resid[v], 0.0f);
     const float old = pr[v];
     const float nv = __fadd_rn(r, old);  // the reference's aResiduals[v] + pageRanks[v]
-    push_vertex(v, nv, old, r, rows_f, nbr_f, selfcnt, pr, resid, next, defer, dvec, p, false, err, act);
+    push_vertex(v, nv, old, r, rows_f, nbr_f, selfcnt, pr, nullptr, resid, next, defer, dvec, p, false, err, act);
   }
   block_totals(err, act, &ctl->err[it], &ctl->active[it], &ctl->done_a[it]);
 }
 
 // Pull-push (8): the row sum of current ranks / out-degree, then the pushes.
+// contrib[u] holds rank[u] / out_degree[u], rewritten by every rank update
+// (a vertex with in-neighbours' reads racing its update sees the old or the
+// new value, as the reference's reads of pageRanks[u] do), so a term is one
+// gather and no division.
 struct PullPushPolicy {
   const uint8_t* cur;
   uint8_t* next;
   const uint32_t* nbr;
-  const uint32_t* out_degree;
+  float* contrib;
   float* pr;
   float* resid;
   const uint2* rows_f;
@@ -499,15 +509,12 @@ struct PullPushPolicy {
   uint32_t act = 0;
   __device__ bool want(uint32_t v) const { return cur[v] != 0; }
   __device__ float start(uint32_t) const { return 0.0f; }
-  __device__ float term(uint32_t j) const {
-    const uint32_t u = nbr[j] & 0x3FFFFFFFu;
-    return __fdiv_rn(*(volatile float*)&pr[u], (float)out_degree[u]);
-  }
+  __device__ float term(uint32_t j) const { return contrib[nbr[j] & 0x3FFFFFFFu]; }
   __device__ void finish(uint32_t v, float s) {
     const float nv = __fadd_rn(p.base_pr, __fmul_rn(p.damp, s));
     const float old = pr[v];
     const float r = atomicExch(&resid[v], 0.0f);
-    push_vertex(v, nv, old, r, rows_f, nbr_f, selfcnt, pr, resid, next, defer, dvec, p, true, err, act);
+    push_vertex(v, nv, old, r, rows_f, nbr_f, selfcnt, pr, contrib, resid, next, defer, dvec, p, true, err, act);
   }
 };
 
@@ -544,7 +551,7 @@ __global__ void __launch_bounds__(kT) dd_defer_kernel(uint32_t V, const uint2* _
     if (kPush)
       act += push_range(e.x, e.y, e.z, dvec[e.x], lane, 32, nbr_f, resid, next, eps, twice);
     else
-      for (uint32_t j = e.y + lane; j < e.z; j += 32) next[nbr_f[j] & 0x3FFFFFFFu] = 1;
+      for (uint32_t j = e.y + lane; j < e.z; j += 32) mark(next, nbr_f[j] & 0x3FFFFFFFu);
   }
   for (uint32_t base = gw * 32; base < V; base += nw * 32) {
     const uint32_t v = base + lane;
@@ -559,7 +566,7 @@ __global__ void __launch_bounds__(kT) dd_defer_kernel(uint32_t V, const uint2* _
       if (kPush)
         act += push_range(vv, a, a + d, dvec[vv], lane, 32, nbr_f, resid, next, eps, twice);
       else
-        for (uint32_t j = a + lane; j < a + d; j += 32) next[nbr_f[j] & 0x3FFFFFFFu] = 1;
+        for (uint32_t j = a + lane; j < a + d; j += 32) mark(next, nbr_f[j] & 0x3FFFFFFFu);
     }
   }
   if (!kPush) return;
@@ -802,6 +809,11 @@ int pagerank_dd_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsil
     dd_resid_kernel<<<G.total(), kT, 0, s>>>(g.inv.d_rows(), w->med.as<uint32_t>(), w->heavy.as<uint32_t>(), G.light,
                                              G.med, rp, ctl, V);
     launches++;
+    if (mode == PR_DD_PULLPUSH) {  // the starting ranks / out-degree (flags cleared on the way)
+      dd_contrib_kernel<<<sms * 8, kT, 0, s>>>(V, g.fwd.d_out_degree(), ranks, w->contrib.as<float>(), nxt,
+                                               w->defer.as<uint8_t>(), ctl);
+      launches++;
+    }
   }
   OGB_CUDA(cudaGetLastError());
   for (uint32_t it = 0; it < max_iters; it++) {
@@ -822,7 +834,7 @@ int pagerank_dd_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsil
         dd_push_kernel<<<sms * 8, kT, 0, s>>>(V, cur, nxt, g.fwd.d_rows(), g.fwd.d_dst(), w->selfcnt.as<uint32_t>(),
                                                ranks, resid, defer, dvec, p, ctl, it);
       } else {
-        PullPushPolicy pol{cur,   nxt,  g.inv.d_dst(), g.fwd.d_out_degree(), ranks, resid, g.fwd.d_rows(),
+        PullPushPolicy pol{cur,   nxt,  g.inv.d_dst(), w->contrib.as<float>(), ranks, resid, g.fwd.d_rows(),
                            g.fwd.d_dst(), w->selfcnt.as<uint32_t>(), defer, dvec, p};
         dd_pullpush_kernel<<<G.total(), kT, 0, s>>>(g.inv.d_rows(), w->med.as<uint32_t>(), w->heavy.as<uint32_t>(),
                                                      G.light, G.med, pol, ctl, it);
