@@ -113,6 +113,7 @@ struct BfsCtrl {
   uint32_t iteration, processed, td_steps, bu_steps;
   uint32_t nlevels, epoch, overflow, qcount_prev;
   uint32_t ul_cand0;                 // 1: the unvisited list is the graph's cached in-edge list
+  uint32_t ul_fresh;                 // 1: the unvisited list comes from the step just before (all unvisited)
   uint32_t lmax;                     // largest out-degree on the expansion list
   unsigned long long edges_examined;
   unsigned long long fedges;         // out-edges of the current frontier
@@ -145,7 +146,14 @@ struct BfsBufs {
   uint32_t* list[2];
   uint32_t* bm[3];
   uint32_t* ul[2];
-  const uint32_t* cand0;  // vertices with in-edges, in vertex order (the first unvisited list)
+  // Candidate records of the bottom-up steps that walk a list (two 16-byte
+  // words per candidate, in two arrays): the first such step's (every vertex
+  // with in-edges, in vertex order; built once per graph) and the unvisited
+  // lists the steps hand on, rotating.
+  const uint4* cand_a;
+  const uint4* cand_b;
+  uint4* ul_a[2];
+  uint4* ul_b[2];
   uint32_t* offs;
   uint32_t* fstart;
   uint32_t* fdist;
@@ -163,7 +171,8 @@ struct BfsWork {
   uint32_t V = 0, E = 0;
   DevBuf q0, q1, bm0, bm1, bm2, ul0, ul1, state;
   DevBuf offs, fstart, fdist, tile_i0, scan_status;
-  DevBuf cand0;                     // vertices with in-edges (built once per graph)
+  DevBuf cand_a, cand_b;            // records of the vertices with in-edges (built once per graph)
+  DevBuf ul_a0, ul_a1, ul_b0, ul_b1;  // records of the unvisited lists (at most n_cand0 each)
   uint32_t n_cand0 = 0, cand0_build = 0;
   bool cand0_ready = false;
   BfsDevState* h_state = nullptr;   // pinned copy of the header only (up to the trace)
@@ -228,7 +237,12 @@ static BfsBufs make_bufs(DevGraph& g, BfsWork* w) {
   b.bm[2] = w->bm2.as<uint32_t>();
   b.ul[0] = w->ul0.as<uint32_t>();
   b.ul[1] = w->ul1.as<uint32_t>();
-  b.cand0 = w->cand0.as<uint32_t>();
+  b.cand_a = w->cand_a.as<uint4>();
+  b.cand_b = w->cand_b.as<uint4>();
+  b.ul_a[0] = w->ul_a0.as<uint4>();
+  b.ul_a[1] = w->ul_a1.as<uint4>();
+  b.ul_b[0] = w->ul_b0.as<uint4>();
+  b.ul_b[1] = w->ul_b1.as<uint4>();
   b.offs = w->offs.as<uint32_t>();
   b.fstart = w->fstart.as<uint32_t>();
   b.fdist = w->fdist.as<uint32_t>();
@@ -326,9 +340,13 @@ __device__ __forceinline__ void bu_push_list(BuSmem& sm, uint32_t v) { sm.buf[wa
 __device__ __forceinline__ void bu_push_ul(BuSmem& sm, uint32_t v) {
   sm.buf[kBuRound - 1u - warp_atomic_inc(&sm.nul)] = v;
 }
-// Both lists out (offsets reserved together), then the buffer is empty.
-__device__ __forceinline__ void bu_flush(BuSmem& sm, uint32_t* list_out, uint32_t* list_count, uint32_t* ul_out,
-                                         uint32_t* ul_count) {
+// A round's appends out, then the buffer is empty: discoveries (vertices)
+// into list_out, and the records of the unvisited candidates (staged as
+// indices into in_a / in_b) copied into out_a / out_b; the offsets of both
+// are reserved together.
+__device__ __forceinline__ void bu_flush(BuSmem& sm, uint32_t* list_out, uint32_t* list_count,
+                                             const uint4* in_a, const uint4* in_b, uint4* out_a, uint4* out_b,
+                                             uint32_t* ul_count) {
   __syncthreads();
   const uint32_t nl = sm.nlist, nu = sm.nul;
   if (threadIdx.x == 0) {
@@ -340,7 +358,11 @@ __device__ __forceinline__ void bu_flush(BuSmem& sm, uint32_t* list_out, uint32_
   }
   __syncthreads();
   for (uint32_t k = threadIdx.x; k < nl; k += blockDim.x) list_out[sm.base_list + k] = sm.buf[k];
-  for (uint32_t k = threadIdx.x; k < nu; k += blockDim.x) ul_out[sm.base_ul + k] = sm.buf[kBuRound - 1u - k];
+  for (uint32_t k = threadIdx.x; k < nu; k += blockDim.x) {
+    const uint32_t s = sm.buf[kBuRound - 1u - k];
+    out_a[sm.base_ul + k] = in_a[s];
+    out_b[sm.base_ul + k] = in_b[s];
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     sm.nlist = 0;
@@ -348,6 +370,7 @@ __device__ __forceinline__ void bu_flush(BuSmem& sm, uint32_t* list_out, uint32_
   }
   __syncthreads();
 }
+
 // A flat top-down step's appends: each of a CTA's threads expands one list
 // entry of at most kFlatMaxDeg out-edges per pass.
 constexpr uint32_t kFlatMaxDeg = 16;
@@ -872,24 +895,95 @@ __device__ void td_flat_phase(const BfsBufs& b, const uint32_t* list, uint32_t* 
 
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
 constexpr int kBuV = kBuRound / kSearchT;  // candidates per thread per round
-constexpr uint32_t kFirst = 6;             // in-edges probed per candidate before deferral
+constexpr uint32_t kFirst = 6;             // dense step: in-edges probed per candidate before deferral
+constexpr uint32_t kRecN = 4;              // list step: in-neighbours held in a candidate record
 
-// One bottom-up step of the search.  Candidates: every vertex (dense, the
-// first bottom-up step of a search) or the unvisited list.  Each thread
-// takes kBuV candidates at once: parents, then in-edge rows, then the first
-// kFirst in-neighbours of each and their frontier bits, all issued
-// together.  A candidate with more in-edges and no hit yet is deferred to
-// the round's long-row list, which groups of 8 lanes scan 8 in-edges per
-// load (the first hit in CSR order still wins).  Found vertices get their
-// bit in bm_next (a warp's ballot stores a whole word in the dense case) and,
-// with out-edges, a slot in list_next; unfound ones with in-edges go to
-// ul_next (a vertex without in-edges can never be found).  bm_clear is
-// zeroed on the way.
-template <bool kDense>
-__device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t* bm_next, uint32_t* bm_clear,
-                              const uint32_t* ul_cur, uint32_t ul_count, uint32_t* ul_next, uint32_t* list_next,
-                              int32_t* parents, uint32_t* distances, uint32_t dnext, BfsCtl* ctl, BuSmem& sm,
-                              unsigned long long* s_red) {
+// Long in-edge rows of a round (deferred by either kind of step): a group of
+// 8 lanes per row, 16 in-edges per step (two per lane, both loads in flight);
+// the first hit in CSR order wins.  Entry h is row [sm.hj[h], sm.he[h]) of
+// the candidate sm.hv[h]: a vertex (dense step) or the index of its record
+// in rec_a (list step), whose vertex and out-degree are then read from the
+// record.  Rows without a hit go to the unvisited list (as the entry).
+__device__ __forceinline__ void bu_long_rows(const BfsBufs& b, const uint32_t* bm_cur, uint32_t* bm_next,
+                                             const uint4* rec_a, int32_t* parents, uint32_t* distances,
+                                             uint32_t dnext, BuSmem& sm, uint32_t& nf, uint32_t& edges,
+                                             uint32_t& mx, unsigned long long& fed) {
+  const uint32_t lane = lane_id();
+  const uint32_t nh = sm.nheavy;
+  const uint32_t gl = threadIdx.x & 7;
+  const uint32_t gmask = 0xFFu << (lane & 24);
+  for (uint32_t h = threadIdx.x >> 3; h < nh; h += kSearchT / 8) {
+    const uint32_t hv = sm.hv[h], j0 = sm.hj[h], end = sm.he[h];
+    bool hit_row = false;
+    for (uint32_t j = j0; j < end; j += 16) {
+      const uint32_t ja = j + gl, jb = j + 8 + gl;
+      const uint32_t xa = ja < end ? (__ldg(&b.nbr_i[ja]) & 0x3FFFFFFFu) : kInvalid;
+      const uint32_t xb = jb < end ? (__ldg(&b.nbr_i[jb]) & 0x3FFFFFFFu) : kInvalid;
+      const bool bita = xa != kInvalid && ((bm_cur[xa >> 5] >> (xa & 31)) & 1u);
+      const bool bitb = xb != kInvalid && ((bm_cur[xb >> 5] >> (xb & 31)) & 1u);
+      const uint32_t ma = (__ballot_sync(gmask, bita) >> (lane & 24)) & 0xFFu;
+      const uint32_t mb = (__ballot_sync(gmask, bitb) >> (lane & 24)) & 0xFFu;
+      const uint32_t m = ma | (mb << 8);
+      if (m) {
+        const uint32_t first = (uint32_t)__ffs(m) - 1;
+        const uint32_t x = first < 8 ? xa : xb;
+        if (gl == (first & 7u)) {
+          uint32_t v = hv, od;
+          if (rec_a) {
+            const uint4 r = rec_a[hv];
+            v = r.x;
+            od = r.w;
+          } else {
+            od = __ldg(&b.out_degree[v]);
+          }
+          parents[v] = (int32_t)x;
+          distances[v] = dnext;
+          atomicOr(&bm_next[v >> 5], 1u << (v & 31));
+          nf++;
+          edges += j + first + 1 - j0;
+          fed += od;
+          if (od) {
+            bu_push_list(sm, v);
+            mx = max(mx, od);
+          }
+        }
+        hit_row = true;
+        break;
+      }
+    }
+    if (!hit_row && gl == 0) {
+      edges += end - j0;
+      bu_push_ul(sm, hv);
+    }
+  }
+}
+
+// Step totals: nf and the edges examined, packed, the discoveries' out-edges
+// and the largest out-degree put on the list.
+__device__ __forceinline__ void bu_publish(BfsCtl* ctl, uint32_t nf, uint32_t edges, unsigned long long fed,
+                                           uint32_t mx, unsigned long long* s_red) {
+  unsigned long long a = (unsigned long long)nf | ((unsigned long long)edges << 32), c = fed;
+  block_sum2_max(a, c, mx, s_red);
+  if (threadIdx.x == 0) {
+    if ((uint32_t)a) atomicAdd(&ctl->nf, (uint32_t)a);
+    if (a >> 32) atomicAdd(&ctl->edges, a >> 32);
+    if (c) atomicAdd(&ctl->fedges, c);
+    if (mx) atomicMax(&ctl->maxdeg, mx);
+  }
+}
+
+// One bottom-up step over every vertex (the dense-probe mode, and a graph
+// without in-edges).  Each thread takes kBuV vertices at once: parents, then
+// in-edge rows, then the first kFirst in-neighbours of each and their
+// frontier bits, all issued together; longer rows without a hit yet go to
+// the round's long-row list.  A warp's ballot stores a whole word of bm_next;
+// discoveries with out-edges get a slot in list_next.  No unvisited list is
+// written: the dense mode walks every vertex in every step, and in a graph
+// without in-edges nothing is ever found bottom-up.  bm_clear is zeroed on
+// the way.
+__device__ void bu_dense_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t* bm_next, uint32_t* bm_clear,
+                               uint32_t* list_next, int32_t* parents, uint32_t* distances, uint32_t dnext,
+                               BfsCtl* ctl, BuSmem& sm, unsigned long long* s_red) {
   grid_clear(bm_clear, nullptr, b.words);
   if (threadIdx.x == 0) {
     sm.nlist = 0;
@@ -898,11 +992,11 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
   }
   __syncthreads();
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-  const uint32_t count = kDense ? b.V : ul_count;
+  const uint32_t count = b.V;
   uint32_t nf = 0, edges = 0, mx = 0;
   unsigned long long fed = 0;
-  // each CTA takes one contiguous, equal range of candidates (a multiple of
-  // 32, so a dense step's ballot words never straddle two CTAs)
+  // each CTA takes one contiguous, equal range of vertices (a multiple of
+  // 32, so the ballot words never straddle two CTAs)
   const uint32_t per = ((count + gridDim.x - 1) / gridDim.x + 31u) & ~31u;
   const uint32_t lo = min(count, blockIdx.x * per), hi = min(count, lo + per);
   for (uint32_t rbase = lo; rbase < hi; rbase += kBuRound) {
@@ -910,7 +1004,7 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
 #pragma unroll
     for (int k = 0; k < kBuV; k++) {
       const uint32_t idx = rbase + k * kSearchT + threadIdx.x;
-      v[k] = idx < hi ? (kDense ? idx : ul_cur[idx]) : kInvalid;
+      v[k] = idx < hi ? idx : kInvalid;
     }
     // parent and in-row together (a visited candidate's row is not used)
     int32_t pv[kBuV];
@@ -953,7 +1047,6 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
           found = true;
           nf++;
           edges += hit[k] + 1;
-          if (!kDense) atomicOr(&bm_next[v[k] >> 5], 1u << (v[k] & 31));
           const uint32_t od = __ldg(&b.out_degree[v[k]]);
           fed += od;
           if (od) {
@@ -968,73 +1061,123 @@ __device__ void bu_step_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t
           sm.he[h] = row[k].x + row[k].y;
         } else {
           edges += row[k].y;
-          bu_push_ul(sm, v[k]);
         }
       }
-      if (kDense) {
-        const uint32_t word = __ballot_sync(0xffffffffu, found);
-        const uint32_t base = rbase + k * kSearchT + warp * 32;
-        if (lane == 0 && base < hi) bm_next[base >> 5] = word;
+      const uint32_t word = __ballot_sync(0xffffffffu, found);
+      const uint32_t base = rbase + k * kSearchT + warp * 32;
+      if (lane == 0 && base < hi) bm_next[base >> 5] = word;
+    }
+    __syncthreads();
+    bu_long_rows(b, bm_cur, bm_next, nullptr, parents, distances, dnext, sm, nf, edges, mx, fed);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      sm.nheavy = 0;
+      sm.nul = 0;  // long rows without a hit: no unvisited list in this mode
+    }
+    bu_flush(sm, list_next, &ctl->lnext, nullptr, nullptr, nullptr, nullptr, &ctl->ul_size);
+  }
+  bu_publish(ctl, nf, edges, fed, mx, s_red);
+}
+
+// A record's k-th in-neighbour.
+__device__ __forceinline__ uint32_t rec_nbr(const uint4& q, int m) {
+  return m == 0 ? q.x : (m == 1 ? q.y : (m == 2 ? q.z : q.w));
+}
+
+// One bottom-up step over a list of candidate records: the first such step
+// of a search walks the graph's vertices with in-edges (a vertex without one
+// can never be found bottom-up), later ones the unvisited list the step
+// before wrote.  A record is two 16-byte words in two arrays, A = {vertex,
+// first in-edge, in-degree, out-degree} and B = the row's first kRecN
+// in-neighbours (kInvalid past its end), so a warp reads 32 candidates with
+// two contiguous 512-byte loads; the frontier bits of the first in-neighbours
+// follow directly, instead of list entry, row, neighbour ids and bits as four
+// dependent, scattered loads.  Each CTA takes one contiguous, equal range of
+// records, each thread kBuV of them per round.  The parents are read only
+// when the list may hold visited vertices (check_parents: the first list, or
+// a list that top-down steps have run after); a list written by the step just
+// before holds unvisited vertices only.  Rows longer than kRecN without a hit
+// go to the round's long-row list.  Unfound candidates' records are copied
+// into out_a / out_b, the next step's list.  bm_clear is zeroed on the way.
+__device__ void bu_rec_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t* bm_next, uint32_t* bm_clear,
+                             const uint4* in_a, const uint4* in_b, uint32_t count, bool check_parents,
+                             uint4* out_a, uint4* out_b, uint32_t* list_next, int32_t* parents,
+                             uint32_t* distances, uint32_t dnext, BfsCtl* ctl, BuSmem& sm,
+                             unsigned long long* s_red) {
+  grid_clear(bm_clear, nullptr, b.words);
+  if (threadIdx.x == 0) {
+    sm.nlist = 0;
+    sm.nul = 0;
+    sm.nheavy = 0;
+  }
+  __syncthreads();
+  uint32_t nf = 0, edges = 0, mx = 0;
+  unsigned long long fed = 0;
+  const uint32_t per = ((count + gridDim.x - 1) / gridDim.x + 31u) & ~31u;
+  const uint32_t lo = min(count, blockIdx.x * per), hi = min(count, lo + per);
+  for (uint32_t rbase = lo; rbase < hi; rbase += kBuRound) {
+    uint4 ra[kBuV], rb[kBuV];
+#pragma unroll
+    for (int k = 0; k < kBuV; k++) {
+      const uint32_t idx = rbase + k * kSearchT + threadIdx.x;
+      if (idx < hi) {
+        ra[k] = in_a[idx];
+        rb[k] = in_b[idx];
+      } else {
+        ra[k] = make_uint4(0u, 0u, 0u, 0u);  // in-degree 0: no candidate
+        rb[k] = make_uint4(kInvalid, kInvalid, kInvalid, kInvalid);
+      }
+    }
+    int32_t pv[kBuV];
+#pragma unroll
+    for (int k = 0; k < kBuV; k++) pv[k] = (check_parents && ra[k].z) ? parents[ra[k].x] : -1;
+    uint32_t hit[kBuV], par[kBuV];
+#pragma unroll
+    for (int k = 0; k < kBuV; k++) {
+      hit[k] = kRecN;
+      par[k] = 0;
+#pragma unroll
+      for (int m = (int)kRecN - 1; m >= 0; m--) {
+        const uint32_t x = rec_nbr(rb[k], m);
+        if (x != kInvalid && ((bm_cur[x >> 5] >> (x & 31)) & 1u)) {
+          hit[k] = (uint32_t)m;
+          par[k] = x;
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kBuV; k++) {
+      const uint32_t v = ra[k].x, start = ra[k].y, deg = ra[k].z, od = ra[k].w;
+      if (deg == 0 || pv[k] >= 0) continue;  // no candidate, or visited
+      if (hit[k] < kRecN) {
+        parents[v] = (int32_t)par[k];
+        distances[v] = dnext;
+        nf++;
+        edges += hit[k] + 1;
+        atomicOr(&bm_next[v >> 5], 1u << (v & 31));
+        fed += od;
+        if (od) {
+          bu_push_list(sm, v);
+          mx = max(mx, od);
+        }
+      } else if (deg > kRecN) {
+        edges += kRecN;
+        const uint32_t h = warp_atomic_inc(&sm.nheavy);
+        sm.hv[h] = rbase + k * kSearchT + threadIdx.x;
+        sm.hj[h] = start + kRecN;
+        sm.he[h] = start + deg;
+      } else {
+        edges += deg;
+        bu_push_ul(sm, rbase + k * kSearchT + threadIdx.x);
       }
     }
     __syncthreads();
-    // long rows: a group of 8 lanes per row, 16 in-edges per step (two per
-    // lane, both loads in flight); the first hit in CSR order wins
-    const uint32_t nh = sm.nheavy;
-    const uint32_t gl = threadIdx.x & 7;
-    const uint32_t gmask = 0xFFu << (lane & 24);
-    for (uint32_t h = threadIdx.x >> 3; h < nh; h += kSearchT / 8) {
-      const uint32_t hv = sm.hv[h], j0 = sm.hj[h], end = sm.he[h];
-      bool hit_row = false;
-      for (uint32_t j = j0; j < end; j += 16) {
-        const uint32_t ja = j + gl, jb = j + 8 + gl;
-        const uint32_t xa = ja < end ? (__ldg(&b.nbr_i[ja]) & 0x3FFFFFFFu) : kInvalid;
-        const uint32_t xb = jb < end ? (__ldg(&b.nbr_i[jb]) & 0x3FFFFFFFu) : kInvalid;
-        const bool bita = xa != kInvalid && ((bm_cur[xa >> 5] >> (xa & 31)) & 1u);
-        const bool bitb = xb != kInvalid && ((bm_cur[xb >> 5] >> (xb & 31)) & 1u);
-        const uint32_t ma = (__ballot_sync(gmask, bita) >> (lane & 24)) & 0xFFu;
-        const uint32_t mb = (__ballot_sync(gmask, bitb) >> (lane & 24)) & 0xFFu;
-        const uint32_t m = ma | (mb << 8);
-        if (m) {
-          const uint32_t first = (uint32_t)__ffs(m) - 1;
-          const uint32_t x = first < 8 ? xa : xb;
-          if (gl == (first & 7u)) {
-            parents[hv] = (int32_t)x;
-            distances[hv] = dnext;
-            atomicOr(&bm_next[hv >> 5], 1u << (hv & 31));
-            nf++;
-            edges += j + first + 1 - j0;
-            const uint32_t od = __ldg(&b.out_degree[hv]);
-            fed += od;
-            if (od) {
-              bu_push_list(sm, hv);
-              mx = max(mx, od);
-            }
-          }
-          hit_row = true;
-          break;
-        }
-      }
-      if (!hit_row && gl == 0) {
-        edges += end - j0;
-        bu_push_ul(sm, hv);
-      }
-    }
+    bu_long_rows(b, bm_cur, bm_next, in_a, parents, distances, dnext, sm, nf, edges, mx, fed);
     __syncthreads();
     if (threadIdx.x == 0) sm.nheavy = 0;
-    bu_flush(sm, list_next, &ctl->lnext, ul_next, &ctl->ul_size);
+    bu_flush(sm, list_next, &ctl->lnext, in_a, in_b, out_a, out_b, &ctl->ul_size);
   }
-  {
-    // nf and the edges examined, packed, and the discoveries' out-edges
-    unsigned long long a = (unsigned long long)nf | ((unsigned long long)edges << 32), c = fed;
-    block_sum2_max(a, c, mx, s_red);
-    if (threadIdx.x == 0) {
-      if ((uint32_t)a) atomicAdd(&ctl->nf, (uint32_t)a);
-      if (a >> 32) atomicAdd(&ctl->edges, a >> 32);
-      if (c) atomicAdd(&ctl->fedges, c);
-      if (mx) atomicMax(&ctl->maxdeg, mx);
-    }
-  }
+  bu_publish(ctl, nf, edges, fed, mx, s_red);
 }
 
 // ---- bottom-up of the host-state step (depth read from the parent) --------
@@ -1239,6 +1382,7 @@ __device__ void ctrl_finish_td(BfsCtrl& c, uint32_t total_edges, const BfsCtl& k
   c.bm_r = c.bm_w;
   c.bm_w = r;
   c.td_steps++;
+  c.ul_fresh = 0;  // the unvisited list may now hold vertices this step visited
   ctrl_level(c, st, leader, 0, c.qcount, total_edges, t0);
 }
 
@@ -1251,6 +1395,7 @@ __device__ void ctrl_finish_bu(BfsCtrl& c, const BfsCtl& k, BfsDevState* st, boo
   c.ul_size = k.ul_size;
   c.ul_valid = c.mode == BFS_PULL_DENSE ? 0u : 1u;  // that mode walks every vertex in every step
   c.ul_cand0 = 0;
+  c.ul_fresh = 1;
   c.par_ul ^= 1u;
   c.qcount = k.nf;
   c.lsize = k.lnext;
@@ -1470,13 +1615,16 @@ __global__ void __launch_bounds__(kSearchT, 4) bfsk_search(BfsBufs b, BfsDevStat
       p++;
     } else {
       if (leader) zero_ctl(&ctl[(p + 1) % 3]);
-      if (!S.ul_valid)
-        bu_step_phase<true>(b, b.bm[S.bm_r], b.bm[S.bm_w], b.bm[S.bm_c], nullptr, 0, b.ul[S.par_ul ^ 1u],
-                            b.list[S.par_l ^ 1u], parents, distances, dnext, &ctl[p % 3], sm.bu, s_red);
-      else
-        bu_step_phase<false>(b, b.bm[S.bm_r], b.bm[S.bm_w], b.bm[S.bm_c], S.ul_cand0 ? b.cand0 : b.ul[S.par_ul],
-                             S.ul_size, b.ul[S.par_ul ^ 1u], b.list[S.par_l ^ 1u], parents, distances, dnext,
-                             &ctl[p % 3], sm.bu, s_red);
+      if (!S.ul_valid) {
+        bu_dense_phase(b, b.bm[S.bm_r], b.bm[S.bm_w], b.bm[S.bm_c], b.list[S.par_l ^ 1u], parents, distances, dnext,
+                       &ctl[p % 3], sm.bu, s_red);
+      } else {
+        const bool c0 = S.ul_cand0 != 0;
+        bu_rec_phase(b, b.bm[S.bm_r], b.bm[S.bm_w], b.bm[S.bm_c], c0 ? b.cand_a : b.ul_a[S.par_ul],
+                     c0 ? b.cand_b : b.ul_b[S.par_ul], S.ul_size, c0 || !S.ul_fresh, b.ul_a[S.par_ul ^ 1u],
+                     b.ul_b[S.par_ul ^ 1u], b.list[S.par_l ^ 1u], parents, distances, dnext, &ctl[p % 3], sm.bu,
+                     s_red);
+      }
       if (!grid_sync(&st->bar, &st->err, &s_ok)) break;
       if (threadIdx.x == 0) {
         BfsCtl k;
@@ -1572,19 +1720,33 @@ __global__ void bfsk_cand_flags(const uint2* __restrict__ rows_i, uint32_t V, ui
     flags[v] = rows_i[v].y ? 1u : 0u;
 }
 
-__global__ void bfsk_cand_scatter(const uint2* __restrict__ rows_i, uint32_t V, const uint32_t* __restrict__ pos,
-                                  uint32_t* __restrict__ cand) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
-    if (rows_i[v].y) cand[pos[v]] = v;
+// The record of every vertex with in-edges at its place in vertex order
+// (pos: exclusive scan of the flags): A = {vertex, first in-edge, in-degree,
+// out-degree}, B = its first kRecN in-neighbours (ids without the mask bits;
+// kInvalid past the row's end).
+__global__ void bfsk_cand_records(const uint2* __restrict__ rows_i, const uint32_t* __restrict__ nbr_i,
+                                  const uint32_t* __restrict__ out_degree, uint32_t V,
+                                  const uint32_t* __restrict__ pos, uint4* __restrict__ rec_a,
+                                  uint4* __restrict__ rec_b) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const uint2 row = rows_i[v];
+    if (!row.y) continue;
+    uint32_t n[kRecN];
+#pragma unroll
+    for (uint32_t m = 0; m < kRecN; m++) n[m] = m < row.y ? (nbr_i[row.x + m] & 0x3FFFFFFFu) : kInvalid;
+    const uint32_t p = pos[v];
+    rec_a[p] = make_uint4(v, row.x, row.y, out_degree[v]);
+    rec_b[p] = make_uint4(n[0], n[1], n[2], n[3]);
+  }
 }
 
-// The graph's vertices with in-edges, in vertex order, once per build: the
-// first bottom-up step's candidates (about half the vertices of an RMAT
-// graph have no in-edge).
+// The records of the graph's vertices with in-edges, in vertex order, once
+// per build: the first list bottom-up step's candidates (about half the
+// vertices of an RMAT graph have no in-edge).  The unvisited lists the steps
+// hand on hold at most as many records.
 static int bfs_cand0(DevGraph& g, BfsWork* w, cudaStream_t s) {
   if (w->cand0_ready && w->cand0_build == g.build_id) return OK;
   const uint32_t V = g.V;
-  OGB_TRY(w->cand0.alloc((size_t)V * 4 + 16));
   // scratch from the search's own V-sized buffers (free outside a search)
   uint32_t* flags = w->fstart.as<uint32_t>();
   uint32_t* pos = w->offs.as<uint32_t>();      // V + 1 words
@@ -1592,11 +1754,19 @@ static int bfs_cand0(DevGraph& g, BfsWork* w, cudaStream_t s) {
   const int grid = sm_count() * 8;
   bfsk_cand_flags<<<grid, 256, 0, s>>>(g.inv.d_rows(), V, flags);
   OGB_TRY(scan_exclusive_u32(flags, pos, V, tmp, s));
-  bfsk_cand_scatter<<<grid, 256, 0, s>>>(g.inv.d_rows(), V, pos, w->cand0.as<uint32_t>());
-  OGB_CUDA(cudaGetLastError());
   uint32_t n = 0;
   OGB_CUDA(cudaMemcpyAsync(&n, pos + V, 4, cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaStreamSynchronize(s));
+  const size_t bytes = (size_t)n * 16 + 16;
+  OGB_TRY(w->cand_a.alloc(bytes));
+  OGB_TRY(w->cand_b.alloc(bytes));
+  OGB_TRY(w->ul_a0.alloc(bytes));
+  OGB_TRY(w->ul_a1.alloc(bytes));
+  OGB_TRY(w->ul_b0.alloc(bytes));
+  OGB_TRY(w->ul_b1.alloc(bytes));
+  bfsk_cand_records<<<grid, 256, 0, s>>>(g.inv.d_rows(), g.inv.d_dst(), g.fwd.d_out_degree(), V, pos,
+                                         w->cand_a.as<uint4>(), w->cand_b.as<uint4>());
+  OGB_CUDA(cudaGetLastError());
   w->n_cand0 = n;
   w->cand0_build = g.build_id;
   w->cand0_ready = true;
@@ -1619,7 +1789,6 @@ int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t 
   if (mode == BFS_LEARNED && !bfs_policy_weights()) return fail(ERR_ARG, "bfs: no learned switch installed");
   BfsWork* w = nullptr;
   OGB_TRY(bfs_work_get(g, &w));
-  BfsBufs b = make_bufs(g, w);
   BfsDevState* st = w->state.as<BfsDevState>();
   if (!w->search_grid) {
     int nb = 0;
@@ -1627,12 +1796,12 @@ int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t 
     if (nb < 1) return fail(ERR_CUDA, "bfs: search kernel does not fit on an SM");
     w->search_grid = nb * sm_count();
   }
+  OGB_TRY(bfs_cand0(g, w, s));
+  BfsBufs b = make_bufs(g, w);  // after bfs_cand0: it (re)allocates the record buffers
   if (mode != BFS_LEARNED) {  // the network is read only by the learned switch
     b.policy = nullptr;
     b.policy_tail = nullptr;
   }
-  OGB_TRY(bfs_cand0(g, w, s));
-  b.cand0 = w->cand0.as<uint32_t>();
   bfsk_init<<<sm_count() * 8, 256, 0, s>>>(b, st, root, parents, distances, mode, bu_entry_nf_frontier ? 1u : 0u,
                                             g.E, w->epoch, w->n_cand0);
   DevBuf d_roots;
