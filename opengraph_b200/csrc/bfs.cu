@@ -899,35 +899,49 @@ constexpr uint32_t kFirst = 6;             // dense step: in-edges probed per ca
 constexpr uint32_t kRecN = 4;              // list step: in-neighbours held in a candidate record
 
 // Long in-edge rows of a round (deferred by either kind of step): a group of
-// 8 lanes per row, 16 in-edges per step (two per lane, both loads in flight);
-// the first hit in CSR order wins.  Entry h is row [sm.hj[h], sm.he[h]) of
-// the candidate sm.hv[h]: a vertex (dense step) or the index of its record
-// in rec_a (list step), whose vertex and out-degree are then read from the
-// record.  Rows without a hit go to the unvisited list (as the entry).
+// 4 lanes per row, 8 in-edges per step (two per lane, both loads in flight,
+// then all frontier probes), 64 groups per CTA; the first hit in CSR order
+// wins.  Entry h is row [sm.hj[h], sm.he[h]) of the candidate sm.hv[h]: a
+// vertex (dense step) or the index of its record in rec_a (list step), whose
+// vertex and out-degree are then read from the record.  Rows without a hit go
+// to the unvisited list (as the entry).
+constexpr uint32_t kLongLanes = 4;
+constexpr uint32_t kLongLoads = 2;
+constexpr uint32_t kLongStep = kLongLanes * kLongLoads;
 __device__ __forceinline__ void bu_long_rows(const BfsBufs& b, const uint32_t* bm_cur, uint32_t* bm_next,
                                              const uint4* rec_a, int32_t* parents, uint32_t* distances,
                                              uint32_t dnext, BuSmem& sm, uint32_t& nf, uint32_t& edges,
                                              uint32_t& mx, unsigned long long& fed) {
   const uint32_t lane = lane_id();
   const uint32_t nh = sm.nheavy;
-  const uint32_t gl = threadIdx.x & 7;
-  const uint32_t gmask = 0xFFu << (lane & 24);
-  for (uint32_t h = threadIdx.x >> 3; h < nh; h += kSearchT / 8) {
+  const uint32_t gl = threadIdx.x & (kLongLanes - 1);
+  const uint32_t gshift = lane & ~(kLongLanes - 1);
+  const uint32_t gmask = ((1u << kLongLanes) - 1u) << gshift;
+  for (uint32_t h = threadIdx.x / kLongLanes; h < nh; h += kSearchT / kLongLanes) {
     const uint32_t hv = sm.hv[h], j0 = sm.hj[h], end = sm.he[h];
     bool hit_row = false;
-    for (uint32_t j = j0; j < end; j += 16) {
-      const uint32_t ja = j + gl, jb = j + 8 + gl;
-      const uint32_t xa = ja < end ? (__ldg(&b.nbr_i[ja]) & 0x3FFFFFFFu) : kInvalid;
-      const uint32_t xb = jb < end ? (__ldg(&b.nbr_i[jb]) & 0x3FFFFFFFu) : kInvalid;
-      const bool bita = xa != kInvalid && ((bm_cur[xa >> 5] >> (xa & 31)) & 1u);
-      const bool bitb = xb != kInvalid && ((bm_cur[xb >> 5] >> (xb & 31)) & 1u);
-      const uint32_t ma = (__ballot_sync(gmask, bita) >> (lane & 24)) & 0xFFu;
-      const uint32_t mb = (__ballot_sync(gmask, bitb) >> (lane & 24)) & 0xFFu;
-      const uint32_t m = ma | (mb << 8);
+    for (uint32_t j = j0; j < end; j += kLongStep) {
+      uint32_t x[kLongLoads];
+#pragma unroll
+      for (uint32_t q = 0; q < kLongLoads; q++) {
+        const uint32_t jq = j + q * kLongLanes + gl;
+        x[q] = jq < end ? (__ldg(&b.nbr_i[jq]) & 0x3FFFFFFFu) : kInvalid;
+      }
+      bool bit[kLongLoads];
+#pragma unroll
+      for (uint32_t q = 0; q < kLongLoads; q++) bit[q] = x[q] != kInvalid && ((bm_cur[x[q] >> 5] >> (x[q] & 31)) & 1u);
+      // bit (q * kLongLanes + group lane) of m <-> in-edge j + that index
+      uint32_t m = 0;
+#pragma unroll
+      for (uint32_t q = 0; q < kLongLoads; q++)
+        m |= ((__ballot_sync(gmask, bit[q]) >> gshift) & ((1u << kLongLanes) - 1u)) << (q * kLongLanes);
       if (m) {
         const uint32_t first = (uint32_t)__ffs(m) - 1;
-        const uint32_t x = first < 8 ? xa : xb;
-        if (gl == (first & 7u)) {
+        if (gl == (first & (kLongLanes - 1))) {
+          uint32_t u = x[0];
+#pragma unroll
+          for (uint32_t q = 1; q < kLongLoads; q++)
+            if (first / kLongLanes == q) u = x[q];
           uint32_t v = hv, od;
           if (rec_a) {
             const uint4 r = rec_a[hv];
@@ -936,7 +950,7 @@ __device__ __forceinline__ void bu_long_rows(const BfsBufs& b, const uint32_t* b
           } else {
             od = __ldg(&b.out_degree[v]);
           }
-          parents[v] = (int32_t)x;
+          parents[v] = (int32_t)u;
           distances[v] = dnext;
           atomicOr(&bm_next[v >> 5], 1u << (v & 31));
           nf++;

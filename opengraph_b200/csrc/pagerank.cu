@@ -64,6 +64,8 @@ constexpr uint32_t kWarpSmemWords = kStage + 3 * kTab + 1;  // stage + table of 
 constexpr size_t kPullDynSmem = (size_t)(kPullThreads / 32) * kWarpSmemWords * 4;
 constexpr uint32_t kHotLimit = 0;    // renumbered sources whose contrib a pull CTA stages in shared memory
 constexpr uint32_t kPrChunk = 8192;  // edges per chunk of a very heavy row
+constexpr uint32_t kPushHubDeg = 256;  // push: destinations with more in-edges are hubs
+constexpr uint32_t kHubChunk = 1024;   // push: in-edges of a hub summed by one warp
 
 // Row-length thresholds of the work split (settable; the GPU-order mode of
 // the oracle takes the same values).
@@ -111,6 +113,13 @@ struct PrWork {
   DevBuf vfirst, vcount, done;         // per chunked vertex: first chunk, chunk count, finished chunks
   DevBuf partials;                     // float per chunk
   uint32_t n_warp = 0, n_cta = 0, n_chunks = 0;
+  // push: the pushes into each hub (in-degree > kPushHubDeg) are summed over
+  // the hub's in-row and applied once per chunk; the other out-edges scatter
+  // from a filtered copy of the forward CSR
+  uint32_t push_build = 0;
+  bool push_ready = false;
+  DevBuf rows_fp, nbr_fp, hub_items;   // filtered rows {start, count}, their neighbours; hub chunks {v, j0, j1, 0}
+  uint32_t n_hub_items = 0;
   PrCtl* h_ctl = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   ~PrWork() {
@@ -574,15 +583,113 @@ __global__ void pr_rl_copy_kernel(uint32_t V, const uint2* __restrict__ rows, co
 }
 
 
-// Push scatter: contrib of each source added to its out-neighbours, split by
-// out-degree like the pull gather (chunks scatter their edge range).
+// ---------------------------------------------------------------- push ------
+//
+// Push adds c[v] into next[u] for every out-edge v -> u (pageRank.c:1117-1134:
+// one float atomic per edge).  On RMAT graphs a few destinations take most of
+// those adds (RMAT-22: the 32 K with most in-edges take 54 % of them, the
+// largest 161 K), and float atomics on one address serialize at its L2 slice.
+// So the adds into every hub -- a destination with more than kPushHubDeg
+// in-edges -- are combined first: a warp sums, for a chunk of kHubChunk of the
+// hub's pushers (its in-row lists exactly the sources that push into it), the
+// values they push, and applies the sum with one atomic.  Every other out-edge
+// is scattered with its own atomic from a filtered copy of the forward CSR
+// (built once per graph).  The set of additions is the reference's; only their
+// order differs, which the reference's own atomics leave open as well.
+
+// Per source: out-edges whose destination is not a hub (a warp per row).
+__global__ void pr_push_count_kernel(uint32_t V, const uint2* __restrict__ rows_f, const uint32_t* __restrict__ nbr_f,
+                                     const uint2* __restrict__ rows_i, uint32_t hub_deg, uint32_t* __restrict__ cnt) {
+  const uint32_t lane = lane_id();
+  const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
+  for (uint32_t v = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); v < V; v += nwarps) {
+    const uint2 r = rows_f[v];
+    uint32_t c = 0;
+    for (uint32_t j = lane; j < r.y; j += 32) c += rows_i[nbr_f[r.x + j] & 0x3FFFFFFFu].y <= hub_deg ? 1u : 0u;
+    c = __reduce_add_sync(0xffffffffu, c);
+    if (lane == 0) cnt[v] = c;
+  }
+}
+
+// The filtered forward CSR: each row's non-hub out-neighbours, in order.
+__global__ void pr_push_filter_kernel(uint32_t V, const uint2* __restrict__ rows_f, const uint32_t* __restrict__ nbr_f,
+                                      const uint2* __restrict__ rows_i, uint32_t hub_deg,
+                                      const uint32_t* __restrict__ off, uint2* __restrict__ rows_fp,
+                                      uint32_t* __restrict__ nbr_fp) {
+  const uint32_t lane = lane_id();
+  const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
+  for (uint32_t v = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); v < V; v += nwarps) {
+    const uint2 r = rows_f[v];
+    uint32_t base = off[v];
+    if (lane == 0) rows_fp[v] = make_uint2(base, off[v + 1] - base);
+    for (uint32_t j0 = 0; j0 < r.y; j0 += 32) {
+      const uint32_t j = j0 + lane;
+      uint32_t x = 0;
+      bool keep = false;
+      if (j < r.y) {
+        x = nbr_f[r.x + j];
+        keep = rows_i[x & 0x3FFFFFFFu].y <= hub_deg;
+      }
+      const uint32_t m = __ballot_sync(0xffffffffu, keep);
+      if (keep) nbr_fp[base + __popc(m & lanemask_lt())] = x;
+      base += __popc(m);
+    }
+  }
+}
+
+// Hub chunks per vertex, then their table {hub, first in-edge, end, 0}.
+__global__ void pr_hub_count_kernel(uint32_t V, const uint2* __restrict__ rows_i, uint32_t hub_deg,
+                                    uint32_t* __restrict__ cnt) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const uint32_t d = rows_i[v].y;
+    cnt[v] = d > hub_deg ? (d + kHubChunk - 1) / kHubChunk : 0u;
+  }
+}
+__global__ void pr_hub_fill_kernel(uint32_t V, const uint2* __restrict__ rows_i, uint32_t hub_deg,
+                                   const uint32_t* __restrict__ pos, uint4* __restrict__ items) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const uint2 r = rows_i[v];
+    if (r.y <= hub_deg) continue;
+    uint32_t k = pos[v];
+    for (uint32_t c = 0; c < r.y; c += kHubChunk, k++) items[k] = make_uint4(v, r.x + c, r.x + min(r.y, c + kHubChunk), 0u);
+  }
+}
+
+// Push scatter, four kinds of blocks: hub chunks (a warp per chunk: the
+// chunk's pushers' contribs summed, four gathers in flight per lane, one
+// atomic), then the filtered rows split by out-degree like the pull gather
+// (chunks of very long rows, a warp per long row, a thread per short row),
+// one atomic per edge.
 __global__ void __launch_bounds__(kPrThreads) pr_push_scatter_kernel(
+    uint32_t nb_hub, const uint4* __restrict__ hub_items, uint32_t n_hub_items, const uint32_t* __restrict__ nbr_i,
     uint32_t nb_chunk, uint32_t nb_warp, const uint32_t* __restrict__ heavy, uint32_t n_warp,
     const PrChunkItem* __restrict__ chunks, uint32_t n_chunks, uint32_t V, uint32_t warp_thr,
     const uint2* __restrict__ rows, const uint32_t* __restrict__ nbr, const float* __restrict__ contrib,
     float* __restrict__ next, const PrCtl* __restrict__ ctl) {
   if (ctl->stop) return;
-  const uint32_t b = blockIdx.x;
+  uint32_t b = blockIdx.x;
+  if (b < nb_hub) {
+    const uint32_t lane = lane_id();
+    const uint32_t wstride = nb_hub * (kPrThreads / 32);
+    for (uint32_t t = b * (kPrThreads / 32) + (threadIdx.x >> 5); t < n_hub_items; t += wstride) {
+      const uint4 it = hub_items[t];
+      float sum = 0.0f;
+      for (uint32_t j = it.y + lane; j < it.z; j += 4 * 32) {
+        uint32_t x[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) x[k] = (j + k * 32 < it.z) ? (__ldg(&nbr_i[j + k * 32]) & 0x3FFFFFFFu) : 0u;
+        float cx[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) cx[k] = (j + k * 32 < it.z) ? __ldg(&contrib[x[k]]) : 0.0f;
+#pragma unroll
+        for (int k = 0; k < 4; k++) sum += cx[k];
+      }
+      sum = warp_fold(sum);
+      if (lane == 0) atomicAdd(&next[it.x], sum);
+    }
+    return;
+  }
+  b -= nb_hub;
   if (b < nb_chunk) {
     for (uint32_t g = b; g < n_chunks; g += nb_chunk) {
       const PrChunkItem ci = chunks[g];
@@ -600,7 +707,7 @@ __global__ void __launch_bounds__(kPrThreads) pr_push_scatter_kernel(
     }
   } else {
     const uint32_t lb = b - nb_chunk - nb_warp;
-    const uint32_t nlb = gridDim.x - nb_chunk - nb_warp;
+    const uint32_t nlb = gridDim.x - nb_hub - nb_chunk - nb_warp;
     for (uint32_t v = lb * kPrThreads + threadIdx.x; v < V; v += nlb * kPrThreads) {
       const uint2 row = rows[v];
       if (row.y > warp_thr) continue;
@@ -647,10 +754,10 @@ __global__ void pr_normalize_kernel(uint32_t V, float* __restrict__ pr) {
 // Heavy lists and the chunk table of one direction (built once per graph,
 // direction and thresholds; the only host round trips of PageRank).
 // Pull lists refer to the renumbered layout (rows_rl), push lists to the
-// forward CSR.
+// filtered forward CSR (rows_fp).
 static int pr_build_lists(DevGraph& g, PrWork* w, bool pull, cudaStream_t s) {
   const uint32_t V = g.V;
-  const uint2* rows = pull ? w->rows_rl.as<uint2>() : g.fwd.d_rows();
+  const uint2* rows = pull ? w->rows_rl.as<uint2>() : w->rows_fp.as<uint2>();
   uint32_t* cnt = w->ctl.as<uint32_t>() + sizeof(PrCtl) / 4;  // scratch words after the control block
   OGB_CUDA(cudaMemsetAsync(cnt, 0, 16, s));
   const int grid = sm_count() * 8;
@@ -767,6 +874,41 @@ static int pr_build_relabel(DevGraph& g, PrWork* w, cudaStream_t s) {
   return OK;
 }
 
+// Push preparation (once per graph): the filtered forward CSR without the
+// out-edges into hubs, and the hub chunk table.
+static int pr_build_push(DevGraph& g, PrWork* w, cudaStream_t s) {
+  const uint32_t V = g.V;
+  const size_t Vp = ((size_t)V + 8) & ~(size_t)3;  // words per V + 1 array, padded
+  DevBuf tmp;
+  OGB_TRY(tmp.alloc((Vp * 2 + scan_tmp_words(V)) * 4));
+  uint32_t* cnt = tmp.as<uint32_t>();
+  uint32_t* pos = cnt + Vp;
+  uint32_t* scan_tmp = pos + Vp;
+  const int grid = sm_count() * 8;
+  pr_push_count_kernel<<<grid, 256, 0, s>>>(V, g.fwd.d_rows(), g.fwd.d_dst(), g.inv.d_rows(), kPushHubDeg, cnt);
+  OGB_CUDA(cudaGetLastError());
+  OGB_TRY(scan_exclusive_u32(cnt, pos, V, scan_tmp, s));
+  uint32_t n_fp = 0;
+  OGB_CUDA(cudaMemcpyAsync(&n_fp, pos + V, 4, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  OGB_TRY(w->rows_fp.alloc((size_t)V * 8 + 16));
+  OGB_TRY(w->nbr_fp.alloc((size_t)n_fp * 4 + 16));
+  pr_push_filter_kernel<<<grid, 256, 0, s>>>(V, g.fwd.d_rows(), g.fwd.d_dst(), g.inv.d_rows(), kPushHubDeg, pos,
+                                             w->rows_fp.as<uint2>(), w->nbr_fp.as<uint32_t>());
+  pr_hub_count_kernel<<<grid, 256, 0, s>>>(V, g.inv.d_rows(), kPushHubDeg, cnt);
+  OGB_CUDA(cudaGetLastError());
+  OGB_TRY(scan_exclusive_u32(cnt, pos, V, scan_tmp, s));
+  uint32_t n_items = 0;
+  OGB_CUDA(cudaMemcpyAsync(&n_items, pos + V, 4, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaStreamSynchronize(s));
+  OGB_TRY(w->hub_items.alloc((size_t)n_items * 16 + 16));
+  pr_hub_fill_kernel<<<grid, 256, 0, s>>>(V, g.inv.d_rows(), kPushHubDeg, pos, w->hub_items.as<uint4>());
+  OGB_CUDA(cudaGetLastError());
+  OGB_CUDA(cudaStreamSynchronize(s));  // before the scratch is released
+  w->n_hub_items = n_items;
+  return OK;
+}
+
 static int pr_work_get(DevGraph& g, bool pull, PrWork** out, cudaStream_t s) {
   if (!g.pr) g.pr = new PrWork();
   PrWork* w = g.pr;
@@ -792,6 +934,12 @@ static int pr_work_get(DevGraph& g, bool pull, PrWork** out, cudaStream_t s) {
     w->rl_build = g.build_id;
     w->rl_warp = g_warp_thr;
     w->rl_cta = g_cta_thr;
+    w->listed_pull = -1;
+  }
+  if (!pull && (!w->push_ready || w->push_build != g.build_id)) {
+    OGB_TRY(pr_build_push(g, w, s));
+    w->push_ready = true;
+    w->push_build = g.build_id;
     w->listed_pull = -1;
   }
   if (w->listed_pull != want || w->listed_warp != g_warp_thr || w->listed_cta != g_cta_thr ||
@@ -838,9 +986,11 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
   const uint32_t nb_chunk = w->n_chunks ? std::min<uint32_t>(sms * 4, w->n_chunks) : 0;
   const uint32_t nb_warp = w->n_warp ? std::max<uint32_t>(1, std::min<uint32_t>(sms * 8, ceil_div(w->n_warp, T / 32))) : 0;
   const uint32_t nb_light = std::max<uint32_t>(1, std::min<uint32_t>(sms * 8, ceil_div(V, T)));
-  const uint32_t grid = nb_chunk + nb_warp + nb_light;
-  const uint2* rows = pull ? g.inv.d_rows() : g.fwd.d_rows();
-  const uint32_t* nbr = pull ? g.inv.d_dst() : g.fwd.d_dst();
+  const uint32_t nb_hub = (!pull && w->n_hub_items)
+                              ? std::min<uint32_t>(sms * 4, ceil_div(w->n_hub_items, T / 32)) : 0;
+  const uint32_t grid = nb_hub + nb_chunk + nb_warp + nb_light;
+  const uint2* rows = pull ? g.inv.d_rows() : w->rows_fp.as<uint2>();
+  const uint32_t* nbr = pull ? g.inv.d_dst() : w->nbr_fp.as<uint32_t>();
   const uint32_t* heavy = w->heavy.as<uint32_t>();
   const PrChunkItem* chunks = w->chunks.as<PrChunkItem>();
 
@@ -853,7 +1003,8 @@ int pagerank_run(DevGraph& g, uint32_t mode, uint32_t max_iters, double epsilon,
           w->n_units, w->med_off.as<uint32_t>(), w->med_v.as<uint32_t>(), w->med_base, w->nbr_rl.as<uint32_t>(),
           g.fwd.d_out_degree(), perm, c_cur, c_nxt, ranks, p, d_ctl, it);
     } else {
-      pr_push_scatter_kernel<<<grid, T, 0, s>>>(nb_chunk, nb_warp, heavy, w->n_warp, chunks, w->n_chunks, V,
+      pr_push_scatter_kernel<<<grid, T, 0, s>>>(nb_hub, w->hub_items.as<uint4>(), w->n_hub_items, g.inv.d_dst(),
+                                                 nb_chunk, nb_warp, heavy, w->n_warp, chunks, w->n_chunks, V,
                                                  g_warp_thr, rows, nbr, c_cur, nxt, d_ctl);
       pr_push_update_kernel<<<sms * 8, T, 0, s>>>(V, g.fwd.d_out_degree(), nxt, c_nxt, ranks, p, d_ctl, it);
     }

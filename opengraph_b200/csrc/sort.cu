@@ -151,8 +151,23 @@ __global__ void __launch_bounds__(256) digit_scan_kernel(const uint32_t* __restr
   base[blockIdx.x * 256 + threadIdx.x] = e;
 }
 
+__device__ __forceinline__ void cp_async_u32(uint32_t* dst_smem, const uint32_t* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// One pass over one tile.  Only the keys pass through registers: once the
+// tile-local digit prefix is known, each payload element is copied from
+// global memory straight into its slot of the digit-ordered stage by an
+// asynchronous copy, and those copies land while the look-back runs; the
+// kernel holds no payload registers.  Keys and payloads are then written out
+// run by run (consecutive threads, consecutive addresses).  Shared memory: a
+// stage per array (32 KB unweighted: four CTAs per SM; 48 KB weighted: three).
 template <bool HAS_P1>
-__global__ void __launch_bounds__(kSortThreads, 3)
+__global__ void __launch_bounds__(kSortThreads, HAS_P1 ? 3 : 4)
 onesweep_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ p0in,
                 const uint32_t* __restrict__ p1in, uint32_t* __restrict__ kout,
                 uint32_t* __restrict__ p0out, uint32_t* __restrict__ p1out, uint32_t n,
@@ -176,28 +191,22 @@ onesweep_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ p
   const uint32_t tile = s_tile;
   const uint64_t tile_base = (uint64_t)tile * kTile;
   const uint64_t warp_base = tile_base + (uint64_t)warp * 32 * kSortItems;
+  // this warp's items: [0, wn) of kSortItems * 32, addressed from per-warp bases
+  const uint32_t wn = n > warp_base ? (uint32_t)min((uint64_t)kSortItems * 32, (uint64_t)n - warp_base) : 0u;
+  const uint32_t* kw = kin + warp_base;
 
-  uint32_t key[kSortItems], p0[kSortItems], p1[kSortItems], pos[kSortItems];
+  uint32_t key[kSortItems], pos[kSortItems];
 #pragma unroll
   for (int i = 0; i < kSortItems; i++) {
-    const uint64_t idx = warp_base + (uint64_t)i * 32 + lane;
-    if (idx < n) {
-      key[i] = kin[idx];
-      p0[i] = p0in[idx];
-      if (HAS_P1) p1[i] = p1in[idx];
-    } else {
-      key[i] = 0xFFFFFFFFu;
-      p0[i] = 0;
-      p1[i] = 0;
-    }
+    const uint32_t o = (uint32_t)i * 32 + lane;
+    key[i] = o < wn ? kw[o] : 0xFFFFFFFFu;
   }
 
   // Stable warp-level ranking: order within the warp is (item, lane).
   uint32_t* wh = s_whist[warp];
 #pragma unroll
   for (int i = 0; i < kSortItems; i++) {
-    const uint64_t idx = warp_base + (uint64_t)i * 32 + lane;
-    const uint32_t d = (idx < n) ? ((key[i] >> shift) & mask) : 256u;
+    const uint32_t d = ((uint32_t)i * 32 + lane < wn) ? ((key[i] >> shift) & mask) : 256u;
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     uint32_t before = (d < 256) ? wh[d] : 0u;
     __syncwarp();
@@ -221,6 +230,25 @@ onesweep_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ p
   if (live) st_volatile_u64(my_status, (tile == 0 ? kFlagInc : kFlagAgg) | cnt);
   const uint32_t local_start = block_exclusive_scan_256(cnt, s_warp);
   s_local_start[tid] = local_start;
+  __syncthreads();
+
+  // Stage slots (digit order within the tile): keys staged, payloads copied
+  // into their slots asynchronously.
+  {
+    const uint32_t* p0w = p0in + warp_base;
+    const uint32_t* p1w = HAS_P1 ? p1in + warp_base : nullptr;
+#pragma unroll
+    for (int i = 0; i < kSortItems; i++) {
+      const uint32_t o = (uint32_t)i * 32 + lane;
+      if (o < wn) {
+        const uint32_t d = (key[i] >> shift) & mask;
+        const uint32_t p = s_local_start[d] + s_whist[warp][d] + pos[i];
+        s_k[p] = key[i];
+        cp_async_u32(&s_p0[p], p0w + o);
+        if (HAS_P1) cp_async_u32(&s_p1[p], p1w + o);
+      }
+    }
+  }
 
   // Decoupled look-back over earlier tiles for this digit.
   uint32_t excl = 0;
@@ -243,21 +271,8 @@ onesweep_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ p
     }
     st_volatile_u64(my_status, kFlagInc | (unsigned long long)(excl + cnt));
   }
-  s_global_start[tid] = digit_base[tid] + excl - s_local_start[tid];
-  __syncthreads();
-
-  // Stage the tile in digit order.
-#pragma unroll
-  for (int i = 0; i < kSortItems; i++) {
-    const uint64_t idx = warp_base + (uint64_t)i * 32 + lane;
-    if (idx < n) {
-      const uint32_t d = (key[i] >> shift) & mask;
-      const uint32_t p = s_local_start[d] + s_whist[warp][d] + pos[i];
-      s_k[p] = key[i];
-      s_p0[p] = p0[i];
-      if (HAS_P1) s_p1[p] = p1[i];
-    }
-  }
+  s_global_start[tid] = digit_base[tid] + excl - local_start;
+  cp_async_commit_wait_all();
   __syncthreads();
 
   const uint32_t valid = (uint32_t)min((uint64_t)kTile, (uint64_t)n - tile_base);
@@ -354,7 +369,7 @@ static int sort_impl(const KV& in, const KV& out, uint64_t n, bool lex, uint32_t
     return OK;
   }
   const uint64_t tiles = (n + kTile - 1) / kTile;
-  const size_t dyn_smem = (size_t)(has_p1 ? 3 : 2) * kTile * sizeof(uint32_t);
+  const size_t dyn_smem = (size_t)(has_p1 ? 3 : 2) * kTile * sizeof(uint32_t);  // a stage per array
   static bool attr_set = false;
   if (!attr_set) {
     OGB_CUDA(cudaFuncSetAttribute(onesweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * kTile * 4));
