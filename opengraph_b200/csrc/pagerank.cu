@@ -587,8 +587,9 @@ __global__ void pr_rl_copy_kernel(uint32_t V, const uint2* __restrict__ rows, co
 //
 // Push adds c[v] into next[u] for every out-edge v -> u (pageRank.c:1117-1134:
 // one float atomic per edge).  On RMAT graphs a few destinations take most of
-// those adds (RMAT-22: the 32 K with most in-edges take 54 % of them, the
-// largest 161 K), and float atomics on one address serialize at its L2 slice.
+// those adds (RMAT-22: the 35,443 with more than 256 in-edges take 56 % of
+// them, the largest 161 K), and float atomics on one address serialize at its
+// L2 slice.
 // So the adds into every hub -- a destination with more than kPushHubDeg
 // in-edges -- are combined first: a warp sums, for a chunk of kHubChunk of the
 // hub's pushers (its in-row lists exactly the sources that push into it), the
@@ -597,43 +598,30 @@ __global__ void pr_rl_copy_kernel(uint32_t V, const uint2* __restrict__ rows, co
 // (built once per graph).  The set of additions is the reference's; only their
 // order differs, which the reference's own atomics leave open as well.
 
-// Per source: out-edges whose destination is not a hub (a warp per row).
-__global__ void pr_push_count_kernel(uint32_t V, const uint2* __restrict__ rows_f, const uint32_t* __restrict__ nbr_f,
-                                     const uint2* __restrict__ rows_i, uint32_t hub_deg, uint32_t* __restrict__ cnt) {
-  const uint32_t lane = lane_id();
-  const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
-  for (uint32_t v = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); v < V; v += nwarps) {
-    const uint2 r = rows_f[v];
-    uint32_t c = 0;
-    for (uint32_t j = lane; j < r.y; j += 32) c += rows_i[nbr_f[r.x + j] & 0x3FFFFFFFu].y <= hub_deg ? 1u : 0u;
-    c = __reduce_add_sync(0xffffffffu, c);
-    if (lane == 0) cnt[v] = c;
-  }
+// The filtered forward CSR is a stable compaction of the forward edge array:
+// a flag per edge (its destination is not a hub), an exclusive scan of the
+// flags, then each kept edge moves to its scanned position and each row's
+// start is the scan at the row's first edge.  Edge-parallel, so the rows of
+// the sources with most out-edges cost no more than any others.
+__global__ void pr_push_flag_kernel(uint32_t E, const uint32_t* __restrict__ nbr_f, const uint2* __restrict__ rows_i,
+                                    uint32_t hub_deg, uint32_t* __restrict__ flag) {
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x)
+    flag[e] = rows_i[nbr_f[e] & 0x3FFFFFFFu].y <= hub_deg ? 1u : 0u;
 }
 
-// The filtered forward CSR: each row's non-hub out-neighbours, in order.
-__global__ void pr_push_filter_kernel(uint32_t V, const uint2* __restrict__ rows_f, const uint32_t* __restrict__ nbr_f,
-                                      const uint2* __restrict__ rows_i, uint32_t hub_deg,
-                                      const uint32_t* __restrict__ off, uint2* __restrict__ rows_fp,
-                                      uint32_t* __restrict__ nbr_fp) {
-  const uint32_t lane = lane_id();
-  const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
-  for (uint32_t v = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); v < V; v += nwarps) {
+__global__ void pr_push_compact_kernel(uint32_t E, const uint32_t* __restrict__ nbr_f, const uint32_t* __restrict__ flag,
+                                       const uint32_t* __restrict__ pos, uint32_t* __restrict__ nbr_fp) {
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x)
+    if (flag[e]) nbr_fp[pos[e]] = nbr_f[e];
+}
+
+__global__ void pr_push_rows_kernel(uint32_t V, const uint2* __restrict__ rows_f, const uint32_t* __restrict__ pos,
+                                    uint2* __restrict__ rows_fp) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     const uint2 r = rows_f[v];
-    uint32_t base = off[v];
-    if (lane == 0) rows_fp[v] = make_uint2(base, off[v + 1] - base);
-    for (uint32_t j0 = 0; j0 < r.y; j0 += 32) {
-      const uint32_t j = j0 + lane;
-      uint32_t x = 0;
-      bool keep = false;
-      if (j < r.y) {
-        x = nbr_f[r.x + j];
-        keep = rows_i[x & 0x3FFFFFFFu].y <= hub_deg;
-      }
-      const uint32_t m = __ballot_sync(0xffffffffu, keep);
-      if (keep) nbr_fp[base + __popc(m & lanemask_lt())] = x;
-      base += __popc(m);
-    }
+    // a row without edges may sit anywhere (its edges_idx is 0): it keeps none
+    const uint32_t a = r.y ? pos[r.x] : 0u;
+    rows_fp[v] = make_uint2(a, r.y ? pos[r.x + r.y] - a : 0u);
   }
 }
 
@@ -877,27 +865,29 @@ static int pr_build_relabel(DevGraph& g, PrWork* w, cudaStream_t s) {
 // Push preparation (once per graph): the filtered forward CSR without the
 // out-edges into hubs, and the hub chunk table.
 static int pr_build_push(DevGraph& g, PrWork* w, cudaStream_t s) {
-  const uint32_t V = g.V;
-  const size_t Vp = ((size_t)V + 8) & ~(size_t)3;  // words per V + 1 array, padded
+  const uint32_t V = g.V, E = g.E;
+  const size_t Ep = ((size_t)E + 8) & ~(size_t)3;  // words per E + 1 array, padded
+  const size_t Vp = ((size_t)V + 8) & ~(size_t)3;
   DevBuf tmp;
-  OGB_TRY(tmp.alloc((Vp * 2 + scan_tmp_words(V)) * 4));
-  uint32_t* cnt = tmp.as<uint32_t>();
-  uint32_t* pos = cnt + Vp;
-  uint32_t* scan_tmp = pos + Vp;
+  OGB_TRY(tmp.alloc((2 * std::max(Ep, Vp) + scan_tmp_words(std::max(E, V))) * 4));
+  uint32_t* flag = tmp.as<uint32_t>();
+  uint32_t* pos = flag + std::max(Ep, Vp);
+  uint32_t* scan_tmp = pos + std::max(Ep, Vp);
   const int grid = sm_count() * 8;
-  pr_push_count_kernel<<<grid, 256, 0, s>>>(V, g.fwd.d_rows(), g.fwd.d_dst(), g.inv.d_rows(), kPushHubDeg, cnt);
+  pr_push_flag_kernel<<<grid, 256, 0, s>>>(E, g.fwd.d_dst(), g.inv.d_rows(), kPushHubDeg, flag);
   OGB_CUDA(cudaGetLastError());
-  OGB_TRY(scan_exclusive_u32(cnt, pos, V, scan_tmp, s));
+  OGB_TRY(scan_exclusive_u32(flag, pos, E, scan_tmp, s));
   uint32_t n_fp = 0;
-  OGB_CUDA(cudaMemcpyAsync(&n_fp, pos + V, 4, cudaMemcpyDeviceToHost, s));
+  OGB_CUDA(cudaMemcpyAsync(&n_fp, pos + E, 4, cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaStreamSynchronize(s));
   OGB_TRY(w->rows_fp.alloc((size_t)V * 8 + 16));
   OGB_TRY(w->nbr_fp.alloc((size_t)n_fp * 4 + 16));
-  pr_push_filter_kernel<<<grid, 256, 0, s>>>(V, g.fwd.d_rows(), g.fwd.d_dst(), g.inv.d_rows(), kPushHubDeg, pos,
-                                             w->rows_fp.as<uint2>(), w->nbr_fp.as<uint32_t>());
-  pr_hub_count_kernel<<<grid, 256, 0, s>>>(V, g.inv.d_rows(), kPushHubDeg, cnt);
+  pr_push_compact_kernel<<<grid, 256, 0, s>>>(E, g.fwd.d_dst(), flag, pos, w->nbr_fp.as<uint32_t>());
+  pr_push_rows_kernel<<<grid, 256, 0, s>>>(V, g.fwd.d_rows(), pos, w->rows_fp.as<uint2>());
+  // hub chunks (flag / pos reused as V + 1 arrays)
+  pr_hub_count_kernel<<<grid, 256, 0, s>>>(V, g.inv.d_rows(), kPushHubDeg, flag);
   OGB_CUDA(cudaGetLastError());
-  OGB_TRY(scan_exclusive_u32(cnt, pos, V, scan_tmp, s));
+  OGB_TRY(scan_exclusive_u32(flag, pos, V, scan_tmp, s));
   uint32_t n_items = 0;
   OGB_CUDA(cudaMemcpyAsync(&n_items, pos + V, 4, cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaStreamSynchronize(s));
