@@ -466,9 +466,16 @@ def batching(lib, og, g, roots, V, E, dev, sweep_ms, extra):
     depth = torch.empty(V * 64, dtype=torch.int16, device=dev)
     for _ in range(2):
         g.msbfs(roots, depth)
-    ms = min(g.msbfs(roots, depth)["ms"] for _ in range(3))
-    out["msbfs_64_roots"] = {"ms": round(ms, 3), "sequential_64_searches_ms": round(sweep_ms, 3),
-                             "speedup": round(sweep_ms / ms, 2)}
+    runs = [g.msbfs(roots, depth) for _ in range(3)]
+    best = min(runs, key=lambda r: r["ms"])
+    ms, init_ms = best["ms"], best["init_ms"]
+    # like the single searches (whose output initialisation precedes their
+    # timed region), `ms` is the search; init_ms (depth fill, word clears,
+    # roots) is reported beside it and in the second ratio
+    out["msbfs_64_roots"] = {"ms": round(ms, 3), "init_ms": round(init_ms, 3),
+                             "sequential_64_searches_ms": round(sweep_ms, 3),
+                             "speedup": round(sweep_ms / ms, 2),
+                             "speedup_with_init": round(sweep_ms / (ms + init_ms), 2)}
     del depth
     rng = np.random.default_rng(5)
     seeds = [int(x) for x in rng.choice(V, size=32, replace=False)]

@@ -175,7 +175,11 @@ typedef struct ogb_msbfs_info
     uint32_t launches;
     uint64_t reached_pairs;    /* (vertex, lane) pairs reached, roots too */
     uint64_t edges_examined;
-    double ms;                 /* device time of the batch                */
+    double ms;                 /* device time of the levels (the search)  */
+    double init_ms;            /* device time of the initialisation before
+                                  it: depth fill, per-vertex words cleared,
+                                  roots set (as the single-root search's
+                                  initialisation precedes its timed part) */
 } ogb_msbfs_info;
 int ogb_msbfs(ogb_graph *g, const uint32_t *roots, uint32_t nroots, uint16_t *d_depths, ogb_msbfs_info *info,
               void *stream);

@@ -129,7 +129,8 @@ class BfsInfo(C.Structure):
 
 class MsBfsInfo(C.Structure):
     _fields_ = [("levels", u32), ("push_levels", u32), ("pull_levels", u32), ("launches", u32),
-                ("reached_pairs", C.c_uint64), ("edges_examined", C.c_uint64), ("ms", C.c_double)]
+                ("reached_pairs", C.c_uint64), ("edges_examined", C.c_uint64), ("ms", C.c_double),
+                ("init_ms", C.c_double)]
 
 
 class PprBatchInfo(C.Structure):

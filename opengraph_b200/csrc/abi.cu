@@ -2023,6 +2023,7 @@ extern "C" int ogb_msbfs(ogb_graph* g, const uint32_t* roots, uint32_t nroots, u
     info->reached_pairs = r.reached;
     info->edges_examined = r.edges_examined;
     info->ms = r.ms;
+    info->init_ms = r.init_ms;
   }
   return OK;
 }

@@ -139,7 +139,8 @@ struct MsResult {
   uint32_t levels = 0, push_levels = 0, pull_levels = 0, launches = 0;
   unsigned long long reached = 0;         // (vertex, lane) pairs reached, roots included
   unsigned long long edges_examined = 0;  // edges read by the levels
-  double ms = 0.0;                        // device time
+  double ms = 0.0;                        // device time of the levels
+  double init_ms = 0.0;                   // device time of the initialisation before them
 };
 // Up to 64 BFS searches at once, one lane per root; depth[v * 64 + lane] =
 // depth of v in that lane's search, 0xFFFF when unreached (V * 64 u16).
