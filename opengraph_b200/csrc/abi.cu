@@ -1441,8 +1441,9 @@ static struct BFSStats* bfs_dropin(struct Arguments* a, struct GraphCSR* graph, 
   {
     const int tid = omp_get_thread_num(), nth = omp_get_num_threads();
     if (tid == 0) {
+      // (the reference's stats need no reached-vertex count)
       run_status = bfs_run(dg->g, (uint32_t)a->source, mode, dg->d_parents.as<int32_t>(),
-                           dg->d_distances.as<uint32_t>(), &r, want_trace || !quiet(), bitmap_nf, s);
+                           dg->d_distances.as<uint32_t>(), &r, want_trace || !quiet(), bitmap_nf, s, false);
       t_search = now_s() - t0;
     }
     if (tid > 0 || nth == 1) {

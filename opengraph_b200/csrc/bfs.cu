@@ -340,10 +340,10 @@ __device__ __forceinline__ void bu_push_list(BuSmem& sm, uint32_t v) { sm.buf[wa
 __device__ __forceinline__ void bu_push_ul(BuSmem& sm, uint32_t v) {
   sm.buf[kBuRound - 1u - warp_atomic_inc(&sm.nul)] = v;
 }
-// A round's appends out, then the buffer is empty: discoveries (vertices)
-// into list_out, and the records of the unvisited candidates (staged as
-// indices into in_a / in_b) copied into out_a / out_b; the offsets of both
-// are reserved together.
+// A round's appends out, then the buffer and the long-row list are empty:
+// discoveries (vertices) into list_out, and the records of the unvisited
+// candidates (staged as indices into in_a / in_b) copied into out_a /
+// out_b; the offsets of both are reserved together.
 __device__ __forceinline__ void bu_flush(BuSmem& sm, uint32_t* list_out, uint32_t* list_count,
                                              const uint4* in_a, const uint4* in_b, uint4* out_a, uint4* out_b,
                                              uint32_t* ul_count) {
@@ -367,6 +367,7 @@ __device__ __forceinline__ void bu_flush(BuSmem& sm, uint32_t* list_out, uint32_
   if (threadIdx.x == 0) {
     sm.nlist = 0;
     sm.nul = 0;
+    sm.nheavy = 0;  // the round's long rows were all read before the first barrier above
   }
   __syncthreads();
 }
@@ -1187,8 +1188,7 @@ __device__ void bu_rec_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t*
     }
     __syncthreads();
     bu_long_rows(b, bm_cur, bm_next, in_a, parents, distances, dnext, sm, nf, edges, mx, fed);
-    __syncthreads();
-    if (threadIdx.x == 0) sm.nheavy = 0;
+    // the flush's first barrier ends the long rows (it also clears their count)
     bu_flush(sm, list_next, &ctl->lnext, in_a, in_b, out_a, out_b, &ctl->ul_size);
   }
   bu_publish(ctl, nf, edges, fed, mx, s_red);
@@ -1788,12 +1788,14 @@ static int bfs_cand0(DevGraph& g, BfsWork* w, cudaStream_t s) {
 }
 
 int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_t* distances, BfsResult* res,
-            bool want_trace, bool bu_entry_nf_frontier, cudaStream_t s) {
-  return bfs_run_roots(g, &root, 1, mode, parents, distances, res, want_trace, bu_entry_nf_frontier, s);
+            bool want_trace, bool bu_entry_nf_frontier, cudaStream_t s, bool want_reached) {
+  return bfs_run_roots(g, &root, 1, mode, parents, distances, res, want_trace, bu_entry_nf_frontier, s,
+                       want_reached);
 }
 
 int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t mode, int32_t* parents,
-                  uint32_t* distances, BfsResult* res, bool want_trace, bool bu_entry_nf_frontier, cudaStream_t s) {
+                  uint32_t* distances, BfsResult* res, bool want_trace, bool bu_entry_nf_frontier, cudaStream_t s,
+                  bool want_reached) {
   const uint32_t V = g.V;
   if (nroots == 0) return fail(ERR_ARG, "bfs: no root");
   for (uint32_t i = 0; i < nroots; i++)
@@ -1830,8 +1832,10 @@ int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t 
   OGB_CUDA(cudaLaunchCooperativeKernel((void*)bfsk_search, dim3(w->search_grid), dim3(kSearchT), args, 0, s));
   OGB_CUDA(cudaEventRecord(w->ev_stop, s));
   OGB_CUDA(cudaMemsetAsync(&st->aux, 0, sizeof(BfsCtl), s));
-  bfsk_reached<<<sm_count() * 8, 256, 0, s>>>(b, st);
-  OGB_CUDA(cudaGetLastError());
+  if (want_reached) {
+    bfsk_reached<<<sm_count() * 8, 256, 0, s>>>(b, st);
+    OGB_CUDA(cudaGetLastError());
+  }
   OGB_CUDA(cudaMemcpyAsync(w->h_state, w->state.p, offsetof(BfsDevState, trace), cudaMemcpyDeviceToHost, s));
   OGB_CUDA(cudaStreamSynchronize(s));
   float total_ms = 0.f;

@@ -125,14 +125,16 @@ struct BfsSwitchState {
 // arrays of V entries.  bu_entry_nf selects the nf value at the start of a
 // bottom-up phase: 0 as the array-queue DO-BFS (BFS.c:550-551), or the
 // frontier size as the bitmap DO-BFS.  want_trace: also copy the per-step
-// trace and switch inputs back into res.
+// trace and switch inputs back into res.  want_reached: count the reached
+// vertices and their out-edges into res (one more pass over V).
 int bfs_run(DevGraph& g, uint32_t root, uint32_t mode, int32_t* parents, uint32_t* distances,
-            BfsResult* res, bool want_trace, bool bu_entry_nf_frontier, cudaStream_t s);
+            BfsResult* res, bool want_trace, bool bu_entry_nf_frontier, cudaStream_t s, bool want_reached = true);
 // The same from several roots at once (host array): on a disjoint union of
 // graphs with one root each, every vertex gets its depth from its own
 // graph's root.  The switch state covers the whole union.
 int bfs_run_roots(DevGraph& g, const uint32_t* roots, uint32_t nroots, uint32_t mode, int32_t* parents,
-                  uint32_t* distances, BfsResult* res, bool want_trace, bool bu_entry_nf_frontier, cudaStream_t s);
+                  uint32_t* distances, BfsResult* res, bool want_trace, bool bu_entry_nf_frontier, cudaStream_t s,
+                  bool want_reached = true);
 
 // ---- multi-source BFS (batch.cu) -------------------------------------------
 struct MsResult {

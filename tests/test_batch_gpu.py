@@ -154,7 +154,11 @@ def small_batch(og, n, seed):
     return nv, eoff, srcs, dsts
 
 
-def test_batch_equals_single_graphs(torch_cuda, lib):
+def test_batch_equals_single_graphs(torch_cuda, lib, oracle):
+    """Every graph of a 24-graph batch: BFS and PageRank equal the
+    single-graph path bit for bit, and the oracle (the reference's
+    restatement): BFS depths exact, PageRank within 1e-6 L1 of the
+    reference's summation order at the executed iteration count."""
     import opengraph_b200 as og
     torch = torch_cuda
     nv, eoff, srcs, dsts = small_batch(og, 24, 0)
@@ -190,6 +194,13 @@ def test_batch_equals_single_graphs(torch_cuda, lib):
         assert per[i]["iterations"] == info["iterations"], i
         assert np.array_equal(branks[lo:hi].view(np.uint32), host(r1, np.float32).view(np.uint32)), i
         assert abs(per[i]["error_total"] - info["error_total"]) <= 1e-12 + 1e-9 * abs(info["error_total"]), i
+        # against the oracle
+        gi = oracle.build(srcs[i], dsts[i], V, 0)
+        _, odist, _ = oracle.bfs(gi, roots[i], 2)
+        assert np.array_equal(bdist[lo:hi].astype(np.uint32), odist), i
+        er, _ = oracle.pagerank(gi, 0, per[i]["executed"], 0.0)
+        l1 = float(np.abs(branks[lo:hi].astype(np.float64) - er).sum())
+        assert l1 <= 1e-6, (i, l1)
         dg.close()
     assert binfo["reached"] == reached
     # the same call again replays the captured graph
