@@ -36,7 +36,7 @@ extern "C" {
 
 /* ---- structs (layout-identical to OpenGraph) --------------------------- */
 
-/* 00_graph_bench/include/utils/mt19937.h:38-44 (unsigned long words). */
+/* 00_graph_bench/include/utils/mt19937.h:56-60 (unsigned long words). */
 typedef struct mt19937_stateStruct
 {
     unsigned long mt[624];
@@ -342,11 +342,11 @@ struct SPMVStats *SPMVPushGraphCSR(struct Arguments *arguments, struct GraphCSR 
 
 /* ---- roots and RNG ------------------------------------------------------ */
 
-/* 00_graph_bench/include/utils/mt19937.h:47-57 ; mt19937.c:54-114 */
+/* 00_graph_bench/include/utils/mt19937.h:62-69 ; mt19937.c:54-114 */
 void initializeMersenneState(mt19937state *m, unsigned long seed);
 unsigned long generateRandInt(mt19937state *m);
 float generateRandFloat(mt19937state *m);
-/* 00_graph_bench/include/utils/graphRun.h ; graphRun.c:537-556 */
+/* 00_graph_bench/include/utils/graphRun.h:27 ; graphRun.c:537-556 */
 uint32_t generateRandomRootGraphCSR(mt19937state *mt19937var, struct GraphCSR *graph);
 
 #ifdef __cplusplus
