@@ -830,6 +830,67 @@ def run_case(args):
     print(json.dumps(out), flush=True)
 
 
+def run_bfs_partitioned(args):
+    """--case bfs-part: --n DO-BFS searches of the seeded RMAT graph of
+    --scale, each one search partitioned over all ranks of the job (1-D
+    vertex ranges, one process per GPU, NCCL for the exchange of next
+    bytes; opengraph_b200.parallel).  Each search is timed with CUDA events
+    between barriers, and the slowest rank's time is reported.  Prints one
+    JSON line (rank 0)."""
+    import datetime
+
+    import torch
+    import torch.distributed as tdist
+    import opengraph_b200 as og
+    from opengraph_b200.parallel import DeviceBfsRangeStep, bfs_partitioned, edge_balanced_ranges
+    ws, rank, local = dist_env()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if ws > 1:
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    lib = og.load(True)
+    lib.quiet(True)
+    s, d, w = og.generate_rmat(args.scale, EDGE_FACTOR, SEED, weighted=True)
+    V, E = 1 << args.scale, len(s)
+    g = lib.device_graph()
+    g.build(torch.from_numpy(s.view(np.int32)).to(dev), torch.from_numpy(d.view(np.int32)).to(dev), V, 0,
+            weight=torch.from_numpy(w).to(dev))
+    torch.cuda.synchronize()
+    vf, vi = g.view(False), g.view(True)
+    E = vf.num_edges  # after the build's duplicate / self-loop removal: the switch's mu
+    outdeg = vf.out_degree.cpu().numpy().view(np.uint32).astype(np.int64)
+    ranges = edge_balanced_ranges(vi.out_degree.cpu().numpy().view(np.uint32), ws)
+    rng = np.random.default_rng(1000)
+    roots = [int(x) for x in rng.choice(np.nonzero(outdeg > 0)[0], size=args.n + 1, replace=False)]
+    step = DeviceBfsRangeStep(g)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    res = []
+    for k, r in enumerate(roots):
+        if ws > 1:
+            tdist.barrier()
+        torch.cuda.synchronize()
+        start.record()
+        par, dep, st = bfs_partitioned(step, V, E, ranges, rank, ws, r, dev, dist=tdist if ws > 1 else None)
+        stop.record()
+        torch.cuda.synchronize()
+        ms = torch.tensor([start.elapsed_time(stop)], dtype=torch.float64, device=dev)
+        if ws > 1:
+            tdist.all_reduce(ms, op=tdist.ReduceOp.MAX)
+        if k == 0:
+            continue  # warm-up search
+        reached_out = int(outdeg[par.cpu().numpy() >= 0].sum())
+        t = float(ms.item())
+        res.append({"root": r, "ms": round(t, 4), "steps": len(st.directions), "bu_steps": st.bu_steps,
+                    "gteps": round(reached_out / (t * 1e6), 2)})
+    g.close()
+    if rank == 0:
+        print(json.dumps({"case": "bfs-part", "scale": args.scale, "V": V, "E": E, "n_gpus": ws,
+                          "ranges": [list(x) for x in ranges], "searches": res,
+                          "note": "timed per search: barrier, CUDA events, max over ranks"}), flush=True)
+    if ws > 1:
+        tdist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -840,8 +901,9 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-stages", action="store_true")
     ap.add_argument("--case", default="full", choices=["full", "bfs", "pr-pull", "pr-push", "pr-dd-pull", "pr-dd-push",
-                                                     "pr-dd-pullpush", "spmv-pull", "spmv-push", "build", "scale"],
+                                                     "pr-dd-pullpush", "spmv-pull", "spmv-push", "build", "scale", "bfs-part"],
                     help="full = the benchmark line; scale = the plain pipeline on RMAT-26 and ER-24; "
+                         "bfs-part = one DO-BFS partitioned over all ranks; "
                          "the others run one kernel family for profiling")
     ap.add_argument("--scale", type=int, default=SCALE, help="RMAT scale of a --case run")
     ap.add_argument("--n", type=int, default=3, help="searches / iterations / builds of a --case run")
@@ -849,6 +911,8 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.case == "scale":
         run_scale(args)
+    elif args.case == "bfs-part":
+        run_bfs_partitioned(args)
     elif args.case != "full":
         run_case(args)
     elif args.impl == "reference":

@@ -294,6 +294,45 @@ int ogb_pagerank_range_init(ogb_graph *g, float *d_ranks, float *d_contrib, void
 int ogb_pagerank_range_step(ogb_graph *g, uint32_t lo, uint32_t hi, const float *d_contrib, float *d_ranks,
                             float *d_contrib_next, double epsilon, double *d_err, uint32_t *d_active, void *stream);
 int ogb_pagerank_range_finish(ogb_graph *g, float *d_ranks, void *stream);
+/* 1-D partitioned direction-optimizing BFS (no counterpart in the
+ * reference; its loop is BFS.c:476-626).  A rank owns the vertices [lo, hi):
+ * their parents and depths (d_parents, d_dist: V entries, written on
+ * [lo, hi) only), their out-rows for top-down steps and in-rows for
+ * bottom-up steps.  d_frontier, d_next and d_visited are V bytes (0/1) and
+ * d_cand V int32, the same on every rank.
+ * bfs_range_init: d_frontier = d_visited = {root}; d_cand = 0x7F7F7F7F
+ * everywhere (it is so again after every step); d_parents / d_dist on
+ * [lo, hi) as the reference initialises them (BFS.c:58-74: -out_degree, or
+ * -1 without out-edges; depth 0; the root its own parent); d_counts =
+ * {1, out_degree(root), 0, 0} (the first frontier's size and mf,
+ * BFS.c:511).
+ * A step at depth `depth` (1 for the first) in `direction` (0 top-down,
+ * 1 bottom-up) is bfs_range_expand, an all-reduce by the caller across the
+ * ranks (top-down: MIN over d_cand; bottom-up: MAX over d_next), then
+ * bfs_range_settle; d_next is then the next frontier.
+ * expand zeroes d_counts (4 u64, device).  Top-down: d_cand[w] =
+ * min(d_cand[w], u) for every unvisited
+ * out-neighbour w of an owned frontier vertex u.  Bottom-up: d_next zeroed;
+ * each owned unvisited vertex takes its first in-neighbour in the frontier,
+ * in CSR order, as parent (BFS.c:703-754), sets its d_next byte and adds
+ * itself to d_counts[0] and its examined in-edges to d_counts[2].
+ * settle: top-down, d_next[v] = (d_cand[v] != 0x7F7F7F7F), and each owned
+ * such vertex takes d_cand[v] as parent (its smallest frontier
+ * in-neighbour) and the depth, adding itself to d_counts[0] and
+ * max(out_degree, 1) to d_counts[1] (the mf of BFS.c:675), and d_cand is
+ * reset to 0x7F7F7F7F; both
+ * directions: d_visited |= d_next.  d_counts[3] != 0 reports an overflow of
+ * the library's step queue (sized for the worst case).  Neither call
+ * synchronizes its stream.  opengraph_b200.parallel holds the direction
+ * switch of BFS.c:546-587. */
+int ogb_bfs_range_init(ogb_graph *g, uint32_t lo, uint32_t hi, uint32_t root, int32_t *d_parents, uint32_t *d_dist,
+                       uint8_t *d_frontier, uint8_t *d_visited, int32_t *d_cand, uint64_t *d_counts, void *stream);
+int ogb_bfs_range_expand(ogb_graph *g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth,
+                         const uint8_t *d_frontier, const uint8_t *d_visited, uint8_t *d_next, int32_t *d_cand,
+                         int32_t *d_parents, uint32_t *d_dist, uint64_t *d_counts, void *stream);
+int ogb_bfs_range_settle(ogb_graph *g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth,
+                         int32_t *d_cand, uint8_t *d_next, uint8_t *d_visited, int32_t *d_parents,
+                         uint32_t *d_dist, uint64_t *d_counts, void *stream);
 /* radixSortEdgesByPageRank (reorder.c:165-221) on device arrays: d_labels
  * stably sorted in place, ascending by (uint32_t)(rank * 2^20 + 0.5f). */
 int ogb_sort_by_rank(const float *d_ranks, uint32_t *d_labels, uint32_t n, void *stream);

@@ -278,6 +278,9 @@ _DEVICE_API = [
     ("ogb_pagerank_range_init", C.c_int, [vp, vp, vp, vp]),
     ("ogb_pagerank_range_step", C.c_int, [vp, u32, u32, vp, vp, vp, C.c_double, vp, vp, vp]),
     ("ogb_pagerank_range_finish", C.c_int, [vp, vp, vp]),
+    ("ogb_bfs_range_init", C.c_int, [vp, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp]),
+    ("ogb_bfs_range_expand", C.c_int, [vp, u32, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp]),
+    ("ogb_bfs_range_settle", C.c_int, [vp, u32, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp]),
     ("ogb_pagerank_set_bins", None, [u32, u32]),
     ("ogb_pagerank_pull_noalloc", C.c_int, [u32, vp, vp, vp, vp, u32, C.c_double, vp, vp, vp]),
     ("ogb_pagerank_get_bins", None, [u32p, u32p, u32p, u32p]),

@@ -2210,6 +2210,32 @@ extern "C" int ogb_pagerank_range_finish(ogb_graph* g, float* d_ranks, void* str
   return pagerank_range_finish(g->g, d_ranks, as_stream(stream));
 }
 
+extern "C" int ogb_bfs_range_init(ogb_graph* g, uint32_t lo, uint32_t hi, uint32_t root, int32_t* d_parents,
+                                  uint32_t* d_dist, uint8_t* d_frontier, uint8_t* d_visited, int32_t* d_cand,
+                                  uint64_t* d_counts, void* stream) {
+  if (!g || !d_parents || !d_dist || !d_frontier || !d_visited || !d_cand || !d_counts) return fail(ERR_ARG, "null");
+  return bfs_range_init(g->g, lo, hi, root, d_parents, d_dist, d_frontier, d_visited, d_cand,
+                        reinterpret_cast<unsigned long long*>(d_counts), as_stream(stream));
+}
+
+extern "C" int ogb_bfs_range_expand(ogb_graph* g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth,
+                                    const uint8_t* d_frontier, const uint8_t* d_visited, uint8_t* d_next,
+                                    int32_t* d_cand, int32_t* d_parents, uint32_t* d_dist, uint64_t* d_counts,
+                                    void* stream) {
+  if (!g || !d_frontier || !d_visited || !d_next || !d_cand || !d_parents || !d_dist || !d_counts)
+    return fail(ERR_ARG, "null");
+  return bfs_range_expand(g->g, lo, hi, direction, depth, d_frontier, d_visited, d_next, d_cand, d_parents, d_dist,
+                          reinterpret_cast<unsigned long long*>(d_counts), as_stream(stream));
+}
+
+extern "C" int ogb_bfs_range_settle(ogb_graph* g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth,
+                                    int32_t* d_cand, uint8_t* d_next, uint8_t* d_visited, int32_t* d_parents,
+                                    uint32_t* d_dist, uint64_t* d_counts, void* stream) {
+  if (!g || !d_cand || !d_next || !d_visited || !d_parents || !d_dist || !d_counts) return fail(ERR_ARG, "null");
+  return bfs_range_settle(g->g, lo, hi, direction, depth, d_cand, d_next, d_visited, d_parents, d_dist,
+                          reinterpret_cast<unsigned long long*>(d_counts), as_stream(stream));
+}
+
 extern "C" int ogb_sort_by_rank(const float* d_ranks, uint32_t* d_labels, uint32_t n, void* stream) {
   if (n && (!d_ranks || !d_labels)) return fail(ERR_ARG, "null");
   return rank_sort(d_ranks, d_labels, n, as_stream(stream));

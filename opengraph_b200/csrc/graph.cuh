@@ -53,6 +53,7 @@ struct DevGraph {
   SortWorkspace sort_ws;
   DevBuf input_src, input_dst, input_w;  // staging of host uploads
   DevBuf err;                            // u32 error word of the build kernels
+  DevBuf range_q;                        // scratch of the partitioned BFS steps (bfs_range.cu)
   uint32_t build_id = 0;  // bumped whenever the edges change (caches key on it)
   BfsWork* bfs = nullptr;
   PrWork* pr = nullptr;
@@ -272,6 +273,16 @@ int pagerank_range_step(DevGraph& g, uint32_t lo, uint32_t hi, const float* cont
                         float* contrib_next, double epsilon, double* d_err, uint32_t* d_active, cudaStream_t s);
 int pagerank_range_finish(DevGraph& g, float* ranks, cudaStream_t s);
 void range_work_free(const DevGraph* g);
+// One rank's share of a 1-D partitioned DO-BFS over the vertices [lo, hi)
+// (ogb_bfs_range_* in ogb200_device.h).  bfs_range.cu.
+int bfs_range_init(DevGraph& g, uint32_t lo, uint32_t hi, uint32_t root, int32_t* parents, uint32_t* dist,
+                   uint8_t* frontier, uint8_t* visited, int32_t* cand, unsigned long long* counts, cudaStream_t s);
+int bfs_range_expand(DevGraph& g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth,
+                     const uint8_t* frontier, const uint8_t* visited, uint8_t* next, int32_t* cand,
+                     int32_t* parents, uint32_t* dist, unsigned long long* counts, cudaStream_t s);
+int bfs_range_settle(DevGraph& g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth, int32_t* cand,
+                     uint8_t* next, uint8_t* visited, int32_t* parents, uint32_t* dist, unsigned long long* counts,
+                     cudaStream_t s);
 
 // Row-length thresholds of the PageRank work split (light rows per thread,
 // heavy rows per warp, very heavy rows per CTA of cta_threads threads).

@@ -1,5 +1,8 @@
-"""1-D partitioned PageRank pull over several GPUs (one process per GPU).
+"""1-D partitioned PageRank pull and direction-optimizing BFS over several
+GPUs (one process per GPU).
 
+PageRank pull
+-------------
 The reference runs one shared-memory pull loop (pageRank.c:984-1044).  Here
 each rank owns a contiguous range of destination vertices -- their
 inverse-CSR rows -- chosen so that every range holds about the same number of
@@ -21,6 +24,35 @@ the ranks do not depend on the partition; the collectives run on whatever
 backend the process group has (NCCL between GPUs).  The step object is
 passed in, so the partition and exchange logic can also be exercised with
 another implementation of the same three calls.
+
+Direction-optimizing BFS
+------------------------
+The reference runs one shared-memory loop (BFS.c:476-626).  Here each rank
+owns a contiguous vertex range (edge-balanced by in-degree, as above): their
+parents and depths, their out-rows for top-down steps and their in-rows for
+bottom-up steps.  Every rank keeps the frontier and the visited set as one
+byte per vertex over all V.  One step:
+
+1. expand (the library's kernels): top-down, every unvisited out-neighbour
+   w of an owned frontier vertex u gets cand[w] = min(cand[w], u);
+   bottom-up, each owned unvisited vertex takes its first in-neighbour in
+   the frontier as parent and sets its next byte;
+2. the exchange: top-down a min all-reduce of cand (4 V bytes), bottom-up a
+   max all-reduce of the next bytes (V bytes);
+3. settle: top-down, the vertices with a cand form the next frontier, and
+   each owner gives its own their parent (cand: the smallest frontier
+   in-neighbour) and depth and counts them and the reference's mf; then
+   visited |= next;
+4. a sum all-reduce of the step's counts, from which every rank takes the
+   same direction decision (the switch of BFS.c:546-587: mu, mf, nf with
+   alpha 15 and beta 18, in the reference's u32 arithmetic).
+
+Depths, the step count and every step's direction equal the single-GPU
+search's (and the reference's); bottom-up parents are the reference's too
+(the first frontier in-neighbour in CSR order), top-down parents the
+smallest frontier in-neighbour (the reference's are whichever frontier
+vertex wins a race); neither depends on the partition.  At the end the owned
+slices of parents and depths are all-gathered.
 """
 from __future__ import annotations
 
@@ -136,3 +168,132 @@ def pagerank_pull_partitioned(step, V: int, ranges, rank: int, world: int, max_i
     step.finish(ranks)
     return ranks, PartitionResult(iterations=it, executed=executed, error_total=err, active=act,
                                   ranges=list(ranges))
+
+
+class DeviceBfsRangeStep:
+    """The library's CUDA kernels as one rank's BFS step (device tensors)."""
+
+    def __init__(self, dg, stream=None):
+        self.dg = dg
+        self.lib = dg.lib
+        self.stream = stream
+
+    def init(self, lo, hi, root, parents, dist, frontier, visited, cand, counts):
+        self.lib.check(self.lib.ogb_bfs_range_init(self.dg.handle, int(lo), int(hi), int(root), _ptr(parents),
+                                                   _ptr(dist), _ptr(frontier), _ptr(visited), _ptr(cand),
+                                                   _ptr(counts), _stream(self.stream)), "ogb_bfs_range_init")
+
+    def expand(self, lo, hi, direction, depth, frontier, visited, nxt, cand, parents, dist, counts):
+        self.lib.check(self.lib.ogb_bfs_range_expand(self.dg.handle, int(lo), int(hi), int(direction), int(depth),
+                                                     _ptr(frontier), _ptr(visited), _ptr(nxt), _ptr(cand),
+                                                     _ptr(parents), _ptr(dist), _ptr(counts), _stream(self.stream)),
+                       "ogb_bfs_range_expand")
+
+    def settle(self, lo, hi, direction, depth, cand, nxt, visited, parents, dist, counts):
+        self.lib.check(self.lib.ogb_bfs_range_settle(self.dg.handle, int(lo), int(hi), int(direction), int(depth),
+                                                     _ptr(cand), _ptr(nxt), _ptr(visited), _ptr(parents),
+                                                     _ptr(dist), _ptr(counts), _stream(self.stream)),
+                       "ogb_bfs_range_settle")
+
+
+@dataclass
+class BfsPartitionResult:
+    iteration: int        # BFSStats.iteration: steps + 1
+    processed_nodes: int  # BFSStats.processed_nodes: vertices reached, root included
+    td_steps: int
+    bu_steps: int
+    directions: list      # per step: 0 top-down, 1 bottom-up
+    edges_examined: int   # in-edges read by the bottom-up steps, all ranks
+    ranges: list
+
+
+_U32 = 0xFFFFFFFF
+
+
+def bfs_partitioned(step, V: int, E: int, ranges, rank: int, world: int, root: int, device, mode: int = 2,
+                    bu_entry_nf_frontier: bool = False, dist=None, group=None):
+    """Run the partitioned BFS on this rank; returns (parents, depths as
+    int32 tensors of V, the whole vectors on every rank; BfsPartitionResult).
+    mode 0 bottom-up only, 1 top-down only, 2 direction-optimizing;
+    bu_entry_nf_frontier starts a bottom-up run with nf = the frontier size
+    (the bitmap variant) instead of 0.  ``dist`` is torch.distributed (None
+    for a single process: world must be 1)."""
+    import torch
+    if world > 1 and dist is None:
+        raise ValueError("world > 1 needs torch.distributed")
+    if mode not in (0, 1, 2):
+        raise ValueError("mode: 0 bottom-up, 1 top-down, 2 direction-optimizing")
+    if not 0 <= root < V:
+        raise ValueError(f"root {root} out of range (V={V})")
+    lo, hi = ranges[rank]
+    parents = torch.empty(V, dtype=torch.int32, device=device)
+    depths = torch.empty(V, dtype=torch.int32, device=device)
+    frontier = torch.empty(V, dtype=torch.uint8, device=device)
+    nxt = torch.empty(V, dtype=torch.uint8, device=device)
+    visited = torch.empty(V, dtype=torch.uint8, device=device)
+    cand = torch.empty(V, dtype=torch.int32, device=device)
+    counts = torch.zeros(4, dtype=torch.int64, device=device)
+    step.init(lo, hi, root, parents, depths, frontier, visited, cand, counts)
+    mf = int(counts[1].item()) & _U32
+    mu = E & _U32
+    alpha, beta = 15, 18
+    qn, nf = 1, 0
+    iteration = processed = 1
+    td = bu = 0
+    dirs = []
+    examined = 0
+
+    def run(direction):
+        nonlocal frontier, nxt, examined
+        depth = len(dirs) + 1
+        step.expand(lo, hi, direction, depth, frontier, visited, nxt, cand, parents, depths, counts)
+        if world > 1:
+            if direction == 0:
+                dist.all_reduce(cand, op=dist.ReduceOp.MIN, group=group)
+            else:
+                dist.all_reduce(nxt, op=dist.ReduceOp.MAX, group=group)
+        step.settle(lo, hi, direction, depth, cand, nxt, visited, parents, depths, counts)
+        if world > 1:
+            dist.all_reduce(counts, group=group)
+        c = [int(x) for x in counts.tolist()]
+        if c[3]:
+            raise RuntimeError("partitioned bfs: a step queue overflowed")
+        frontier, nxt = nxt, frontier
+        dirs.append(direction)
+        examined += c[2]
+        return c
+
+    while qn > 0:
+        if mode == 0 or (mode == 2 and mf > mu // alpha):
+            nf = qn if bu_entry_nf_frontier else 0
+            while True:
+                nf_prev = nf
+                nf = run(1)[0]
+                iteration += 1
+                processed += nf
+                bu += 1
+                if not (nf > 0 if mode == 0 else (nf > nf_prev or nf > V // beta)):
+                    break
+            qn = nf
+            mf = 1
+        else:
+            mu = (mu - mf) & _U32
+            c = run(0)
+            mf = c[1] & _U32
+            qn = c[0]
+            iteration += 1
+            processed += qn
+            td += 1
+
+    if world > 1:
+        maxlen = max(h - l for l, h in ranges)
+        for t in (parents, depths):
+            send = torch.zeros(maxlen, dtype=t.dtype, device=device)
+            send[: hi - lo] = t[lo:hi]
+            recv = [torch.zeros(maxlen, dtype=t.dtype, device=device) for _ in range(world)]
+            dist.all_gather(recv, send, group=group)
+            for r, (l, h) in enumerate(ranges):
+                t[l:h] = recv[r][: h - l]
+    return parents, depths, BfsPartitionResult(iteration=iteration, processed_nodes=processed, td_steps=td,
+                                               bu_steps=bu, directions=dirs, edges_examined=examined,
+                                               ranges=list(ranges))

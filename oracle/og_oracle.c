@@ -752,3 +752,94 @@ void orc_pull_range_step(uint32_t V, const uint32_t *f_outdeg, const uint32_t *i
         if (e >= epsilon) (*active)++;
     }
 }
+
+/* ------------------------------------------------- partitioned DO-BFS -- */
+
+#define ORC_NO_CAND 0x7F7F7F7F /* cand of a vertex no frontier vertex reached */
+
+/* The first in-neighbour of v in the frontier, in CSR order; -1 if none.
+ * *examined grows by the in-edges read (BFS.c:736-748's early break). */
+static int64_t first_frontier_in(const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, uint32_t v,
+                                 const uint8_t *frontier, uint64_t *examined)
+{
+    for (uint32_t j = i_idx[v]; j < i_idx[v] + i_outdeg[v]; j++)
+    {
+        const uint32_t u = i_dst[j] & 0x3FFFFFFFu;
+        if (frontier[u])
+        {
+            *examined += j + 1 - i_idx[v];
+            return u;
+        }
+    }
+    *examined += i_outdeg[v];
+    return -1;
+}
+
+void orc_bfs_range_init(uint32_t V, const uint32_t *f_outdeg, uint32_t lo, uint32_t hi, uint32_t root,
+                        int32_t *parents, uint32_t *dist, uint8_t *frontier, uint8_t *visited, int32_t *cand)
+{
+    for (uint32_t v = 0; v < V; v++) cand[v] = ORC_NO_CAND;
+    for (uint32_t v = lo; v < hi; v++)
+    {
+        parents[v] = f_outdeg[v] ? -(int32_t)f_outdeg[v] : -1;
+        dist[v] = 0;
+    }
+    if (root >= lo && root < hi) parents[root] = (int32_t)root;
+    memset(frontier, 0, V);
+    memset(visited, 0, V);
+    frontier[root] = 1;
+    visited[root] = 1;
+}
+
+void orc_bfs_range_expand(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_idx, const uint32_t *f_dst,
+                          const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, uint32_t lo,
+                          uint32_t hi, int direction, uint32_t depth, const uint8_t *frontier, const uint8_t *visited,
+                          uint8_t *next, int32_t *cand, int32_t *parents, uint32_t *dist, uint64_t *counts)
+{
+    memset(counts, 0, 4 * sizeof(uint64_t));
+    if (direction != 0) memset(next, 0, V);
+    for (uint32_t v = lo; v < hi; v++)
+    {
+        if (direction == 0)
+        {
+            if (!frontier[v]) continue;
+            for (uint32_t j = f_idx[v]; j < f_idx[v] + f_outdeg[v]; j++)
+            {
+                const uint32_t w = f_dst[j] & 0x3FFFFFFFu;
+                if (!visited[w] && (int32_t)v < cand[w]) cand[w] = (int32_t)v;
+            }
+        }
+        else
+        {
+            if (visited[v]) continue;
+            const int64_t p = first_frontier_in(i_outdeg, i_idx, i_dst, v, frontier, &counts[2]);
+            if (p < 0) continue;
+            parents[v] = (int32_t)p;
+            dist[v] = depth;
+            next[v] = 1;
+            counts[0]++;
+        }
+    }
+}
+
+void orc_bfs_range_settle(uint32_t V, const uint32_t *f_outdeg, uint32_t lo, uint32_t hi, int direction,
+                          uint32_t depth, int32_t *cand, uint8_t *next, uint8_t *visited, int32_t *parents,
+                          uint32_t *dist, uint64_t *counts)
+{
+    for (uint32_t v = 0; v < V; v++)
+    {
+        if (direction == 0)
+        {
+            next[v] = cand[v] != ORC_NO_CAND;
+            if (next[v] && v >= lo && v < hi)
+            {
+                parents[v] = cand[v];
+                dist[v] = depth;
+                counts[0]++;
+                counts[1] += f_outdeg[v] ? f_outdeg[v] : 1u;
+            }
+            cand[v] = ORC_NO_CAND;
+        }
+        if (next[v]) visited[v] = 1;
+    }
+}

@@ -112,6 +112,29 @@ void orc_pull_range_step(uint32_t V, const uint32_t *f_outdeg, const uint32_t *i
                          const uint32_t *i_dst, uint32_t lo, uint32_t hi, const float *contrib, float *pr,
                          float *contrib_next, double epsilon, int gpu_order, double *err, uint32_t *active);
 
+/* One rank's share of a 1-D partitioned DO-BFS step over the owned
+ * vertices [lo, hi) (the steps of BFS.c:639-687 and BFS.c:703-754
+ * restricted to the range); frontier, next and visited are V bytes, cand
+ * V int32.  init: parents / dist on [lo, hi) as BFS.c:58-74; frontier =
+ * visited = {root}; cand = 0x7F7F7F7F (and again after every step).
+ * expand: counts zeroed; top-down, cand[w] = min(cand[w], u) over the
+ * unvisited out-neighbours w of
+ * owned frontier vertices u; bottom-up, next zeroed, each owned unvisited
+ * vertex takes its first frontier in-neighbour in CSR order (counts[0]
+ * found, counts[2] in-edges examined).  settle (after the exchange: MIN of
+ * cand, or MAX of next): top-down, next = cand set, the owned such vertices
+ * take cand as parent (counts[0] found, counts[1] sum of
+ * max(out_degree, 1), the mf of BFS.c:675), cand reset; visited |= next. */
+void orc_bfs_range_init(uint32_t V, const uint32_t *f_outdeg, uint32_t lo, uint32_t hi, uint32_t root,
+                        int32_t *parents, uint32_t *dist, uint8_t *frontier, uint8_t *visited, int32_t *cand);
+void orc_bfs_range_expand(uint32_t V, const uint32_t *f_outdeg, const uint32_t *f_idx, const uint32_t *f_dst,
+                          const uint32_t *i_outdeg, const uint32_t *i_idx, const uint32_t *i_dst, uint32_t lo,
+                          uint32_t hi, int direction, uint32_t depth, const uint8_t *frontier, const uint8_t *visited,
+                          uint8_t *next, int32_t *cand, int32_t *parents, uint32_t *dist, uint64_t *counts);
+void orc_bfs_range_settle(uint32_t V, const uint32_t *f_outdeg, uint32_t lo, uint32_t hi, int direction,
+                          uint32_t depth, int32_t *cand, uint8_t *next, uint8_t *visited, int32_t *parents,
+                          uint32_t *dist, uint64_t *counts);
+
 /* radixSortEdgesByPageRank (reorder.c:165-221), in place. */
 void orc_rank_sort(uint32_t n, const float *ranks, uint32_t *labels);
 

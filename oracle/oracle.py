@@ -76,6 +76,10 @@ class Oracle:
         d.orc_spmv.argtypes = [u32, vp, vp, vp, vp, vp, vp, vp, C.c_int, C.c_int, u32, vp, vp]
         d.orc_rank_sort.argtypes = [u32, vp, vp]
         d.orc_pull_range_step.argtypes = [u32, vp, vp, vp, vp, u32, u32, vp, vp, vp, C.c_double, C.c_int, vp, vp]
+        d.orc_bfs_range_init.argtypes = [u32, vp, u32, u32, u32, vp, vp, vp, vp, vp]
+        d.orc_bfs_range_expand.argtypes = [u32, vp, vp, vp, vp, vp, vp, u32, u32, C.c_int, u32, vp, vp, vp, vp, vp,
+                                           vp, vp]
+        d.orc_bfs_range_settle.argtypes = [u32, vp, u32, u32, C.c_int, u32, vp, vp, vp, vp, vp, vp]
 
     def pull_range_step(self, g: dict, lo: int, hi: int, contrib, pr, contrib_next, epsilon: float,
                         gpu_order: bool = True):
@@ -86,6 +90,24 @@ class Oracle:
                                    _p(g["i_dst"]), lo, hi, _p(contrib), _p(pr), _p(contrib_next), epsilon,
                                    1 if gpu_order else 0, C.byref(err), C.byref(act))
         return err.value, act.value
+
+    def bfs_range_init(self, g: dict, lo: int, hi: int, root: int, parents, dist, frontier, visited, cand) -> int:
+        """One rank's initialisation of the partitioned DO-BFS (numpy arrays
+        of V, in place); returns the root's out-degree (the first mf)."""
+        self.d.orc_bfs_range_init(g["num_vertices"], _p(g["f_outdeg"]), lo, hi, root, _p(parents), _p(dist),
+                                  _p(frontier), _p(visited), _p(cand))
+        return int(g["f_outdeg"][root])
+
+    def bfs_range_expand(self, g: dict, lo: int, hi: int, direction: int, depth: int, frontier, visited, nxt,
+                         cand, parents, dist, counts) -> None:
+        self.d.orc_bfs_range_expand(g["num_vertices"], _p(g["f_outdeg"]), _p(g["f_idx"]), _p(g["f_dst"]),
+                                    _p(g["i_outdeg"]), _p(g["i_idx"]), _p(g["i_dst"]), lo, hi, direction, depth,
+                                    _p(frontier), _p(visited), _p(nxt), _p(cand), _p(parents), _p(dist), _p(counts))
+
+    def bfs_range_settle(self, g: dict, lo: int, hi: int, direction: int, depth: int, cand, nxt, visited,
+                         parents, dist, counts) -> None:
+        self.d.orc_bfs_range_settle(g["num_vertices"], _p(g["f_outdeg"]), lo, hi, direction, depth, _p(cand),
+                                    _p(nxt), _p(visited), _p(parents), _p(dist), _p(counts))
 
     def pagerank_dd(self, g: dict, mode: int, max_iters: int = 100, epsilon: float = 1e-4, gpu_order: bool = False):
         """Data-driven PageRank (6 pull, 7 push, 8 pull-push), sequential;
