@@ -294,6 +294,23 @@ int ogb_pagerank_range_init(ogb_graph *g, float *d_ranks, float *d_contrib, void
 int ogb_pagerank_range_step(ogb_graph *g, uint32_t lo, uint32_t hi, const float *d_contrib, float *d_ranks,
                             float *d_contrib_next, double epsilon, double *d_err, uint32_t *d_active, void *stream);
 int ogb_pagerank_range_finish(ogb_graph *g, float *d_ranks, void *stream);
+/* Graph build across several GPUs (no counterpart in the reference, which
+ * sorts one edge list: radixsort.c:46-335, graphCSR.c:107-248).  Ranks own
+ * the vertex ranges [bounds[r], bounds[r+1]) (bounds: nparts + 1 ascending
+ * HOST values from 0; nparts <= 64).  ogb_partition_edges splits a rank's
+ * edge-list shard (device arrays of E, d_w may be NULL): every edge goes to
+ * its source's owner and, when that is another rank, to its destination's
+ * owner.  d_out_* (capacity 2 E) receive, per owner in rank order, first the
+ * edges it owns by source then those it owns by destination only, each in
+ * shard order; counts (HOST, nparts) the edges per owner.  After an
+ * all-to-all of these segments, ogb_graph_build on the received edges (in
+ * sender order, with the global V) gives every owned vertex the out-row and
+ * in-row, in the same order, of the graph of the whole edge list (the
+ * shards concatenated in rank order).  ERR_RANGE if an id is >= bounds[nparts].
+ * Synchronizes the stream. */
+int ogb_partition_edges(const uint32_t *d_src, const uint32_t *d_dst, const float *d_w, uint32_t E,
+                        const uint32_t *bounds, uint32_t nparts, uint32_t *d_out_src, uint32_t *d_out_dst,
+                        float *d_out_w, uint32_t *counts, void *stream);
 /* 1-D partitioned direction-optimizing BFS (no counterpart in the
  * reference; its loop is BFS.c:476-626).  A rank owns the vertices [lo, hi):
  * their parents and depths (d_parents, d_dist: V entries, written on
@@ -304,8 +321,10 @@ int ogb_pagerank_range_finish(ogb_graph *g, float *d_ranks, void *stream);
  * everywhere (it is so again after every step); d_parents / d_dist on
  * [lo, hi) as the reference initialises them (BFS.c:58-74: -out_degree, or
  * -1 without out-edges; depth 0; the root its own parent); d_counts =
- * {1, out_degree(root), 0, 0} (the first frontier's size and mf,
- * BFS.c:511).
+ * {1, out_degree(root), 0, 0} on the rank that owns the root and zeros on
+ * the others (summed over the ranks: the first frontier's size and mf,
+ * BFS.c:511).  g may hold the whole graph or, built from
+ * ogb_partition_edges' output, only the rows of the owned vertices.
  * A step at depth `depth` (1 for the first) in `direction` (0 top-down,
  * 1 bottom-up) is bfs_range_expand, an all-reduce by the caller across the
  * ranks (top-down: MIN over d_cand; bottom-up: MAX over d_next), then

@@ -19,8 +19,8 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(ROOT, "include")
 
-CUDA_SOURCES = ["graph.cu", "sort.cu", "scan.cu", "bfs.cu", "bfs_range.cu", "pagerank.cu", "compact.cu", "noalloc.cu",
-                "batch.cu", "mlp.cu", "dd.cu"]
+CUDA_SOURCES = ["graph.cu", "sort.cu", "scan.cu", "bfs.cu", "bfs_range.cu", "partition.cu", "pagerank.cu", "compact.cu",
+                "noalloc.cu", "batch.cu", "mlp.cu", "dd.cu"]
 LAYOUT_SOURCES = ["abi.cu"]  # compiled once per struct layout
 CXX_SOURCES = ["generate.cpp"]
 

@@ -2210,6 +2210,13 @@ extern "C" int ogb_pagerank_range_finish(ogb_graph* g, float* d_ranks, void* str
   return pagerank_range_finish(g->g, d_ranks, as_stream(stream));
 }
 
+extern "C" int ogb_partition_edges(const uint32_t* d_src, const uint32_t* d_dst, const float* d_w, uint32_t E,
+                                   const uint32_t* bounds, uint32_t nparts, uint32_t* d_out_src, uint32_t* d_out_dst,
+                                   float* d_out_w, uint32_t* counts, void* stream) {
+  return partition_edges(d_src, d_dst, d_w, E, bounds, nparts, d_out_src, d_out_dst, d_out_w, counts,
+                         as_stream(stream));
+}
+
 extern "C" int ogb_bfs_range_init(ogb_graph* g, uint32_t lo, uint32_t hi, uint32_t root, int32_t* d_parents,
                                   uint32_t* d_dist, uint8_t* d_frontier, uint8_t* d_visited, int32_t* d_cand,
                                   uint64_t* d_counts, void* stream) {

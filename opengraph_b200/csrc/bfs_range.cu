@@ -334,10 +334,14 @@ int bfs_range_init(DevGraph& g, uint32_t lo, uint32_t hi, uint32_t root, int32_t
                    uint8_t* frontier, uint8_t* visited, int32_t* cand, unsigned long long* counts, cudaStream_t s) {
   OGB_TRY(range_check(g, lo, hi, 0));
   if (root >= g.V) return fail(ERR_ARG, "bfs range: root %u out of range (V=%u)", root, g.V);
-  // counts = {1, out_degree(root), 0, 0}: the first frontier and its mf (BFS.c:511)
+  // counts = {1, out_degree(root), 0, 0} on the root's owner, zeros elsewhere:
+  // summed over the ranks, the first frontier and its mf (BFS.c:511).  Only
+  // the owner's out-row of the root is whole when the graph is partitioned.
   OGB_CUDA(cudaMemsetAsync(counts, 0, 32, s));
-  OGB_CUDA(cudaMemsetAsync(counts, 1, 1, s));
-  OGB_CUDA(cudaMemcpyAsync(counts + 1, g.fwd.d_out_degree() + root, 4, cudaMemcpyDeviceToDevice, s));
+  if (root >= lo && root < hi) {
+    OGB_CUDA(cudaMemsetAsync(counts, 1, 1, s));
+    OGB_CUDA(cudaMemcpyAsync(counts + 1, g.fwd.d_out_degree() + root, 4, cudaMemcpyDeviceToDevice, s));
+  }
   OGB_CUDA(cudaMemsetAsync(frontier, 0, g.V, s));
   OGB_CUDA(cudaMemsetAsync(visited, 0, g.V, s));
   OGB_CUDA(cudaMemsetAsync(frontier + root, 1, 1, s));

@@ -273,6 +273,14 @@ int pagerank_range_step(DevGraph& g, uint32_t lo, uint32_t hi, const float* cont
                         float* contrib_next, double epsilon, double* d_err, uint32_t* d_active, cudaStream_t s);
 int pagerank_range_finish(DevGraph& g, float* ranks, cudaStream_t s);
 void range_work_free(const DevGraph* g);
+// Stable split of an edge-list shard by vertex owner (ranges
+// [bounds[r], bounds[r+1]), bounds on the host): each edge to its source's
+// owner and, if another, to its destination's owner; out_* hold up to 2 E
+// edges, grouped by owner in rank order; counts (host) the edges per owner.
+// partition.cu.
+int partition_edges(const uint32_t* src, const uint32_t* dst, const float* w, uint32_t E, const uint32_t* bounds,
+                    uint32_t nparts, uint32_t* out_src, uint32_t* out_dst, float* out_w, uint32_t* counts,
+                    cudaStream_t s);
 // One rank's share of a 1-D partitioned DO-BFS over the vertices [lo, hi)
 // (ogb_bfs_range_* in ogb200_device.h).  bfs_range.cu.
 int bfs_range_init(DevGraph& g, uint32_t lo, uint32_t hi, uint32_t root, int32_t* parents, uint32_t* dist,

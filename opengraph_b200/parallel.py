@@ -25,6 +25,18 @@ backend the process group has (NCCL between GPUs).  The step object is
 passed in, so the partition and exchange logic can also be exercised with
 another implementation of the same three calls.
 
+Graph build
+-----------
+``exchange_edges`` turns each rank's shard of the edge list (the shards in
+rank order form the whole list) into the edges its graph needs: every edge
+goes to the owner of its source and to the owner of its destination (the
+library's stable split, ``ogb_partition_edges``, then an all-to-all).  The
+graph a rank builds from them (``partitioned_device_graph``) holds, for each
+vertex it owns, the out-row and in-row of the whole graph in the same order,
+which is all the partitioned PageRank and BFS steps read; each edge is
+stored on at most two ranks.  With the whole graph on every rank instead,
+the same steps give the same results.
+
 Direction-optimizing BFS
 ------------------------
 The reference runs one shared-memory loop (BFS.c:476-626).  Here each rank
@@ -59,6 +71,8 @@ from __future__ import annotations
 from dataclasses import dataclass
 
 import numpy as np
+
+import ctypes as C
 
 from . import _ptr, _stream
 
@@ -148,6 +162,8 @@ def pagerank_pull_partitioned(step, V: int, ranges, rank: int, world: int, max_i
         for r, (l, h) in enumerate(ranges):
             dst[l:h] = recv[r][: h - l]
 
+    # the owners' contribs: with a partitioned graph only they have whole out-degrees
+    gather_slices(contrib, contrib)
     it = executed = 0
     err = 0.0
     act = 0
@@ -234,6 +250,8 @@ def bfs_partitioned(step, V: int, E: int, ranges, rank: int, world: int, root: i
     cand = torch.empty(V, dtype=torch.int32, device=device)
     counts = torch.zeros(4, dtype=torch.int64, device=device)
     step.init(lo, hi, root, parents, depths, frontier, visited, cand, counts)
+    if world > 1:
+        dist.all_reduce(counts, group=group)  # the root's owner holds its out-degree
     mf = int(counts[1].item()) & _U32
     mu = E & _U32
     alpha, beta = 15, 18
@@ -297,3 +315,87 @@ def bfs_partitioned(step, V: int, E: int, ranges, rank: int, world: int, root: i
     return parents, depths, BfsPartitionResult(iteration=iteration, processed_nodes=processed, td_steps=td,
                                                bu_steps=bu, directions=dirs, edges_examined=examined,
                                                ranges=list(ranges))
+
+
+def shard_ranges(dst, V: int, world: int, dist=None, group=None) -> list[tuple[int, int]]:
+    """edge_balanced_ranges of the whole graph's in-degrees, from this rank's
+    shard of destination ids (a V-entry count summed over the ranks).
+    Duplicate edges and self loops count as they stand."""
+    import torch
+    deg = torch.bincount(dst.long(), minlength=V)[:V].to(torch.int64)
+    if world > 1:
+        dist.all_reduce(deg, group=group)
+    return edge_balanced_ranges(deg.cpu().numpy(), world)
+
+
+def owner_bounds(ranges) -> list[int]:
+    """[lo_0, lo_1, ..., hi_last]: the ranges as the partition kernel takes them."""
+    return [int(lo) for lo, _ in ranges] + [int(ranges[-1][1])]
+
+
+class DeviceEdgeSplit:
+    """The library's stable split of an edge shard by owner (device tensors)."""
+
+    def __init__(self, lib, stream=None):
+        self.lib = lib
+        self.stream = stream
+
+    def split(self, src, dst, w, bounds):
+        """Returns (out_src, out_dst, out_w or None, counts per owner)."""
+        import torch
+        E = int(src.numel())
+        n = len(bounds) - 1
+        cap = max(2 * E, 1)
+        out_src = torch.empty(cap, dtype=src.dtype, device=src.device)
+        out_dst = torch.empty(cap, dtype=dst.dtype, device=dst.device)
+        out_w = torch.empty(cap, dtype=torch.float32, device=src.device) if w is not None else None
+        b = (C.c_uint32 * (n + 1))(*bounds)
+        cnt = (C.c_uint32 * n)()
+        self.lib.check(self.lib.ogb_partition_edges(_ptr(src), _ptr(dst), _ptr(w), E, b, n, _ptr(out_src),
+                                                    _ptr(out_dst), _ptr(out_w), cnt, _stream(self.stream)),
+                       "ogb_partition_edges")
+        return out_src, out_dst, out_w, [int(x) for x in cnt]
+
+
+def exchange_edges(split, src, dst, w, ranges, rank: int, world: int, dist=None, group=None):
+    """This rank's shard (src, dst[, w]) in, the edges this rank's graph needs
+    out: (src, dst, w or None, total edges of all shards).  ``split`` is a
+    DeviceEdgeSplit (or another implementation of ``split``); the received
+    segments are in sender order."""
+    import torch
+    if world > 1 and dist is None:
+        raise ValueError("world > 1 needs torch.distributed")
+    out_src, out_dst, out_w, counts = split.split(src, dst, w, owner_bounds(ranges))
+    n_total = torch.tensor([int(src.numel())], dtype=torch.int64, device=src.device)
+    if world == 1:
+        n = counts[0]
+        return out_src[:n], out_dst[:n], (out_w[:n] if out_w is not None else None), int(n_total.item())
+    send_n = torch.tensor(counts, dtype=torch.int64, device=src.device)
+    recv_n = torch.empty(world, dtype=torch.int64, device=src.device)
+    dist.all_to_all_single(recv_n, send_n, group=group)
+    rc = [int(x) for x in recv_n.tolist()]
+    sent = sum(counts)
+
+    def a2a(t):
+        x = t[:sent].contiguous()
+        if x.dtype == torch.uint32:  # 32-bit ids cross as int32 (not every backend takes uint32)
+            x = x.view(torch.int32)
+        r = torch.empty(sum(rc), dtype=x.dtype, device=t.device)
+        dist.all_to_all_single(r, x, output_split_sizes=rc, input_split_sizes=counts, group=group)
+        return r.view(t.dtype)
+
+    rs, rd = a2a(out_src), a2a(out_dst)
+    rw = a2a(out_w) if out_w is not None else None
+    dist.all_reduce(n_total, group=group)
+    return rs, rd, rw, int(n_total.item())
+
+
+def partitioned_device_graph(lib, src, dst, w, V: int, ranges, rank: int, world: int, sort_type: int = 0,
+                             dist=None, group=None, stream=None):
+    """Build this rank's part of a graph split by ``ranges`` from this rank's
+    shard of the edge list (device tensors).  Returns (DeviceGraph, total
+    edges E of the whole graph: the DO-BFS switch's mu)."""
+    s, d, ww, E = exchange_edges(DeviceEdgeSplit(lib, stream), src, dst, w, ranges, rank, world, dist, group)
+    dg = lib.device_graph()
+    dg.build(s, d, V, sort_type, weight=ww, stream=stream)
+    return dg, E

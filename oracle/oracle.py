@@ -109,6 +109,30 @@ class Oracle:
         self.d.orc_bfs_range_settle(g["num_vertices"], _p(g["f_outdeg"]), lo, hi, direction, depth, _p(cand),
                                     _p(nxt), _p(visited), _p(parents), _p(dist), _p(counts))
 
+    @staticmethod
+    def partition_edges(src, dst, w, bounds):
+        """Stable split of an edge shard by vertex owner (owner r holds
+        [bounds[r], bounds[r+1])): per owner in rank order, the edges it owns
+        by source, then those it owns by destination only, each in shard
+        order.  Returns (src, dst, w or None, counts per owner).  The
+        graph-build exchange of a 1-D partition; the reference builds one
+        graph in one process (graphCSR.c:107-248)."""
+        b = np.asarray(bounds, np.int64)
+        s64, d64 = np.asarray(src, np.int64), np.asarray(dst, np.int64)
+        if len(s64) and max(int(s64.max()), int(d64.max())) >= b[-1]:
+            raise ValueError("partition: a vertex id is past the last range")
+        os_ = np.searchsorted(b, s64, side="right") - 1
+        od = np.searchsorted(b, d64, side="right") - 1
+        idx, counts = [], []
+        for r in range(len(b) - 1):
+            a = np.nonzero(os_ == r)[0]
+            c = np.nonzero((od == r) & (os_ != r))[0]
+            idx.append(a)
+            idx.append(c)
+            counts.append(len(a) + len(c))
+        k = np.concatenate(idx) if idx else np.zeros(0, np.int64)
+        return (np.asarray(src)[k], np.asarray(dst)[k], (np.asarray(w)[k] if w is not None else None), counts)
+
     def pagerank_dd(self, g: dict, mode: int, max_iters: int = 100, epsilon: float = 1e-4, gpu_order: bool = False):
         """Data-driven PageRank (6 pull, 7 push, 8 pull-push), sequential;
         gpu_order sums long in-rows as the GPU kernels do (mode 6)."""

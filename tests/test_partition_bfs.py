@@ -44,6 +44,17 @@ class ThreadDist:
         self.bar.wait()
         t.copy_(acc)
 
+    def all_to_all_single(self, out, t, output_split_sizes=None, input_split_sizes=None, group=None):
+        import torch
+        r = self.local.rank
+        ins = input_split_sizes or [t.numel() // self.world] * self.world
+        starts = [sum(ins[:k]) for k in range(self.world)]
+        self.slots[r] = [t[starts[k]: starts[k] + ins[k]].clone() for k in range(self.world)]
+        self.bar.wait()
+        got = [self.slots[k][r] for k in range(self.world)]
+        self.bar.wait()
+        out.copy_(torch.cat(got) if got else out)
+
     def all_gather(self, out, t, group=None):
         self.slots[self.local.rank] = t.clone()
         self.bar.wait()
@@ -84,7 +95,7 @@ class OracleBfsRangeStep:
     def init(self, lo, hi, root, parents, dist, frontier, visited, cand, counts):
         od = self.o.bfs_range_init(self.g, lo, hi, root, parents.numpy(), dist.numpy().view(np.uint32),
                                    frontier.numpy(), visited.numpy(), cand.numpy())
-        counts.numpy()[:] = [1, od, 0, 0]
+        counts.numpy()[:] = [1, od, 0, 0] if lo <= root < hi else [0, 0, 0, 0]
 
     def expand(self, lo, hi, direction, depth, frontier, visited, nxt, cand, parents, dist, counts):
         self.o.bfs_range_expand(self.g, lo, hi, direction, depth, frontier.numpy(), visited.numpy(), nxt.numpy(),
