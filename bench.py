@@ -831,62 +831,90 @@ def run_case(args):
 
 
 def run_bfs_partitioned(args):
-    """--case bfs-part: --n DO-BFS searches of the seeded RMAT graph of
-    --scale, each one search partitioned over all ranks of the job (1-D
-    vertex ranges, one process per GPU, NCCL for the exchange of next
-    bytes; opengraph_b200.parallel).  Each search is timed with CUDA events
-    between barriers, and the slowest rank's time is reported.  Prints one
-    JSON line (rank 0)."""
+    """--case bfs-part: the graph and the search partitioned over all ranks of
+    the job (1-D vertex ranges, one process per GPU, NCCL; opengraph_b200.
+    parallel).  Each rank starts from its shard of the seeded RMAT edge list
+    of --scale and builds its part of the graph (split by owner, all-to-all,
+    local sort + CSR: `build_ms`); then --n DO-BFS searches, each one search
+    over all ranks.  Every phase is timed with CUDA events between barriers
+    and the slowest rank's time is reported.  Also the split kernel alone on
+    the rank's shard into 8 owners (`split`).  Prints one JSON line (rank 0)."""
     import datetime
 
     import torch
     import torch.distributed as tdist
     import opengraph_b200 as og
-    from opengraph_b200.parallel import DeviceBfsRangeStep, bfs_partitioned, edge_balanced_ranges
+    from opengraph_b200.parallel import (DeviceBfsRangeStep, DeviceEdgeSplit, bfs_partitioned, partitioned_device_graph,
+                                         shard_ranges)
     ws, rank, local = dist_env()
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    dist = tdist if ws > 1 else None
     if ws > 1:
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     lib = og.load(True)
     lib.quiet(True)
     s, d, w = og.generate_rmat(args.scale, EDGE_FACTOR, SEED, weighted=True)
     V, E = 1 << args.scale, len(s)
-    g = lib.device_graph()
-    g.build(torch.from_numpy(s.view(np.int32)).to(dev), torch.from_numpy(d.view(np.int32)).to(dev), V, 0,
-            weight=torch.from_numpy(w).to(dev))
-    torch.cuda.synchronize()
-    vf, vi = g.view(False), g.view(True)
-    E = vf.num_edges  # after the build's duplicate / self-loop removal: the switch's mu
-    outdeg = vf.out_degree.cpu().numpy().view(np.uint32).astype(np.int64)
-    ranges = edge_balanced_ranges(vi.out_degree.cpu().numpy().view(np.uint32), ws)
-    rng = np.random.default_rng(1000)
-    roots = [int(x) for x in rng.choice(np.nonzero(outdeg > 0)[0], size=args.n + 1, replace=False)]
-    step = DeviceBfsRangeStep(g)
+    a, b = E * rank // ws, E * (rank + 1) // ws
+    ts = torch.from_numpy(s[a:b].view(np.int32)).to(dev)
+    td = torch.from_numpy(d[a:b].view(np.int32)).to(dev)
+    tw = torch.from_numpy(w[a:b]).to(dev)
+    del s, d, w
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    res = []
-    for k, r in enumerate(roots):
+
+    def timed(fn):
         if ws > 1:
             tdist.barrier()
         torch.cuda.synchronize()
         start.record()
-        par, dep, st = bfs_partitioned(step, V, E, ranges, rank, ws, r, dev, dist=tdist if ws > 1 else None)
+        out = fn()
         stop.record()
         torch.cuda.synchronize()
-        ms = torch.tensor([start.elapsed_time(stop)], dtype=torch.float64, device=dev)
+        t = torch.tensor([start.elapsed_time(stop)], dtype=torch.float64, device=dev)
         if ws > 1:
-            tdist.all_reduce(ms, op=tdist.ReduceOp.MAX)
+            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        return out, float(t.item())
+
+    ranges = shard_ranges(td, V, ws, dist)
+    # the split alone, 8 owners (after one untimed call)
+    b8 = [V * k // 8 for k in range(9)]
+    splitter = DeviceEdgeSplit(lib)
+    splitter.split(ts, td, tw, b8)
+    sp, split_ms = timed(lambda: splitter.split(ts, td, tw, b8))
+    split_bytes = 12 * int(ts.numel()) + 12 * sum(sp[3])
+    del sp
+    (g, Eg), build_ms = timed(lambda: partitioned_device_graph(lib, ts, td, tw, V, ranges, rank, ws, dist=dist))
+    vf = g.view(False)
+    lo, hi = ranges[rank]
+    outdeg = np.zeros(V, np.int64)
+    outdeg[lo:hi] = vf.out_degree.cpu().numpy().view(np.uint32)[lo:hi]
+    if ws > 1:
+        od = torch.from_numpy(outdeg).to(dev)
+        tdist.all_reduce(od)
+        outdeg = od.cpu().numpy()
+    rng = np.random.default_rng(1000)
+    roots = [int(x) for x in rng.choice(np.nonzero(outdeg > 0)[0], size=args.n + 1, replace=False)]
+    step = DeviceBfsRangeStep(g)
+    res = []
+    for k, r in enumerate(roots):
+        (par, dep, st), t = timed(lambda: bfs_partitioned(step, V, Eg, ranges, rank, ws, r, dev, dist=dist))
         if k == 0:
             continue  # warm-up search
         reached_out = int(outdeg[par.cpu().numpy() >= 0].sum())
-        t = float(ms.item())
         res.append({"root": r, "ms": round(t, 4), "steps": len(st.directions), "bu_steps": st.bu_steps,
                     "gteps": round(reached_out / (t * 1e6), 2)})
     g.close()
     if rank == 0:
         print(json.dumps({"case": "bfs-part", "scale": args.scale, "V": V, "E": E, "n_gpus": ws,
-                          "ranges": [list(x) for x in ranges], "searches": res,
-                          "note": "timed per search: barrier, CUDA events, max over ranks"}), flush=True)
+                          "ranges": [list(x) for x in ranges], "edges_per_rank": int(vf.num_edges),
+                          "build_ms": round(build_ms, 3),
+                          "split": {"owners": 8, "edges": int(ts.numel()), "ms": round(split_ms, 3),
+                                    "algorithmic_bytes": split_bytes,
+                                    "gbs": round(split_bytes / (split_ms * 1e6), 1)},
+                          "searches": res,
+                          "note": "each phase timed with CUDA events between barriers, max over ranks"}),
+              flush=True)
     if ws > 1:
         tdist.destroy_process_group()
 
