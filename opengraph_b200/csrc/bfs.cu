@@ -85,6 +85,9 @@ constexpr int kSearchT = 256;          // threads per CTA of the persistent sear
 constexpr int kMaxTrace = 16384;    // steps whose trace and switch inputs are kept
 constexpr uint32_t kAlpha = 15, kBeta = 18;
 constexpr uint32_t kBuRound = 1024;    // vertices per CTA round of a bottom-up step
+constexpr uint32_t kBuSub = 2;         // list step: load/probe passes of kBuRound records per round,
+                                       // before one long-row phase and one flush
+constexpr uint32_t kBuCap = kBuSub * kBuRound;  // appends and long rows a round can hold
 
 struct BfsCtl {
   uint32_t qnext;            // logical size of the next frontier
@@ -327,18 +330,18 @@ struct TdSmemHost : TdSmem {
   BlockAppend<kExpTile> q_all;
 };
 // Bottom-up: a round's appends and its deferred long in-edge rows.  A round
-// appends each of its at most kBuRound candidates to at most one list, so
+// appends each of its at most kBuCap candidates to at most one list, so
 // the new frontier list fills one buffer from the front and the unvisited
 // list from the back.
 struct BuSmem {
   uint32_t nlist, nul, base_list, base_ul;
-  uint32_t buf[kBuRound];
+  uint32_t buf[kBuCap];
   uint32_t nheavy;
-  uint32_t hv[kBuRound], hj[kBuRound], he[kBuRound];
+  uint32_t hv[kBuCap];
 };
 __device__ __forceinline__ void bu_push_list(BuSmem& sm, uint32_t v) { sm.buf[warp_atomic_inc(&sm.nlist)] = v; }
 __device__ __forceinline__ void bu_push_ul(BuSmem& sm, uint32_t v) {
-  sm.buf[kBuRound - 1u - warp_atomic_inc(&sm.nul)] = v;
+  sm.buf[kBuCap - 1u - warp_atomic_inc(&sm.nul)] = v;
 }
 // A round's appends out, then the buffer and the long-row list are empty:
 // discoveries (vertices) into list_out, and the records of the unvisited
@@ -359,7 +362,7 @@ __device__ __forceinline__ void bu_flush(BuSmem& sm, uint32_t* list_out, uint32_
   __syncthreads();
   for (uint32_t k = threadIdx.x; k < nl; k += blockDim.x) list_out[sm.base_list + k] = sm.buf[k];
   for (uint32_t k = threadIdx.x; k < nu; k += blockDim.x) {
-    const uint32_t s = sm.buf[kBuRound - 1u - k];
+    const uint32_t s = sm.buf[kBuCap - 1u - k];
     out_a[sm.base_ul + k] = in_a[s];
     out_b[sm.base_ul + k] = in_b[s];
   }
@@ -902,10 +905,11 @@ constexpr uint32_t kRecN = 4;              // list step: in-neighbours held in a
 // Long in-edge rows of a round (deferred by either kind of step): a group of
 // 4 lanes per row, 8 in-edges per step (two per lane, both loads in flight,
 // then all frontier probes), 64 groups per CTA; the first hit in CSR order
-// wins.  Entry h is row [sm.hj[h], sm.he[h]) of the candidate sm.hv[h]: a
-// vertex (dense step) or the index of its record in rec_a (list step), whose
-// vertex and out-degree are then read from the record.  Rows without a hit go
-// to the unvisited list (as the entry).
+// wins.  Entry h is the candidate sm.hv[h]: the index of its record in rec_a
+// (list step), whose vertex, in-row and out-degree are read back from the
+// record, or a vertex (dense step), whose in-row is read back from rows_i;
+// the row is scanned from past the in-edges the step already probed.  Rows
+// without a hit go to the unvisited list (as the entry).
 constexpr uint32_t kLongLanes = 4;
 constexpr uint32_t kLongLoads = 2;
 constexpr uint32_t kLongStep = kLongLanes * kLongLoads;
@@ -919,7 +923,21 @@ __device__ __forceinline__ void bu_long_rows(const BfsBufs& b, const uint32_t* b
   const uint32_t gshift = lane & ~(kLongLanes - 1);
   const uint32_t gmask = ((1u << kLongLanes) - 1u) << gshift;
   for (uint32_t h = threadIdx.x / kLongLanes; h < nh; h += kSearchT / kLongLanes) {
-    const uint32_t hv = sm.hv[h], j0 = sm.hj[h], end = sm.he[h];
+    const uint32_t hv = sm.hv[h];
+    uint32_t j0, end, v, od;
+    if (rec_a) {
+      const uint4 r = rec_a[hv];
+      v = r.x;
+      od = r.w;
+      j0 = r.y + kRecN;
+      end = r.y + r.z;
+    } else {
+      const uint2 rr = __ldg(&b.rows_i[hv]);
+      v = hv;
+      od = 0;  // read on a hit
+      j0 = rr.x + kFirst;
+      end = rr.x + rr.y;
+    }
     bool hit_row = false;
     for (uint32_t j = j0; j < end; j += kLongStep) {
       uint32_t x[kLongLoads];
@@ -943,14 +961,7 @@ __device__ __forceinline__ void bu_long_rows(const BfsBufs& b, const uint32_t* b
 #pragma unroll
           for (uint32_t q = 1; q < kLongLoads; q++)
             if (first / kLongLanes == q) u = x[q];
-          uint32_t v = hv, od;
-          if (rec_a) {
-            const uint4 r = rec_a[hv];
-            v = r.x;
-            od = r.w;
-          } else {
-            od = __ldg(&b.out_degree[v]);
-          }
+          if (!rec_a) od = __ldg(&b.out_degree[v]);
           parents[v] = (int32_t)u;
           distances[v] = dnext;
           atomicOr(&bm_next[v >> 5], 1u << (v & 31));
@@ -1072,8 +1083,6 @@ __device__ void bu_dense_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_
           edges += kFirst;
           const uint32_t h = warp_atomic_inc(&sm.nheavy);
           sm.hv[h] = v[k];
-          sm.hj[h] = row[k].x + kFirst;
-          sm.he[h] = row[k].x + row[k].y;
         } else {
           edges += row[k].y;
         }
@@ -1108,7 +1117,8 @@ __device__ __forceinline__ uint32_t rec_nbr(const uint4& q, int m) {
 // two contiguous 512-byte loads; the frontier bits of the first in-neighbours
 // follow directly, instead of list entry, row, neighbour ids and bits as four
 // dependent, scattered loads.  Each CTA takes one contiguous, equal range of
-// records, each thread kBuV of them per round.  The parents are read only
+// records; a round is kBuSub passes of kBuV records per thread (loads, probes,
+// appends), then one long-row phase and one flush for all of them.  The parents are read only
 // when the list may hold visited vertices (check_parents: the first list, or
 // a list that top-down steps have run after); a list written by the step just
 // before holds unvisited vertices only.  Rows longer than kRecN without a hit
@@ -1130,60 +1140,62 @@ __device__ void bu_rec_phase(const BfsBufs& b, const uint32_t* bm_cur, uint32_t*
   unsigned long long fed = 0;
   const uint32_t per = ((count + gridDim.x - 1) / gridDim.x + 31u) & ~31u;
   const uint32_t lo = min(count, blockIdx.x * per), hi = min(count, lo + per);
-  for (uint32_t rbase = lo; rbase < hi; rbase += kBuRound) {
-    uint4 ra[kBuV], rb[kBuV];
+  for (uint32_t rbase0 = lo; rbase0 < hi; rbase0 += kBuCap) {
+#pragma unroll 1
+    for (uint32_t sub = 0; sub < kBuSub; sub++) {
+      const uint32_t rbase = rbase0 + sub * kBuRound;
+      uint4 ra[kBuV], rb[kBuV];
 #pragma unroll
-    for (int k = 0; k < kBuV; k++) {
-      const uint32_t idx = rbase + k * kSearchT + threadIdx.x;
-      if (idx < hi) {
-        ra[k] = in_a[idx];
-        rb[k] = in_b[idx];
-      } else {
-        ra[k] = make_uint4(0u, 0u, 0u, 0u);  // in-degree 0: no candidate
-        rb[k] = make_uint4(kInvalid, kInvalid, kInvalid, kInvalid);
-      }
-    }
-    int32_t pv[kBuV];
-#pragma unroll
-    for (int k = 0; k < kBuV; k++) pv[k] = (check_parents && ra[k].z) ? parents[ra[k].x] : -1;
-    uint32_t hit[kBuV], par[kBuV];
-#pragma unroll
-    for (int k = 0; k < kBuV; k++) {
-      hit[k] = kRecN;
-      par[k] = 0;
-#pragma unroll
-      for (int m = (int)kRecN - 1; m >= 0; m--) {
-        const uint32_t x = rec_nbr(rb[k], m);
-        if (x != kInvalid && ((bm_cur[x >> 5] >> (x & 31)) & 1u)) {
-          hit[k] = (uint32_t)m;
-          par[k] = x;
+      for (int k = 0; k < kBuV; k++) {
+        const uint32_t idx = rbase + k * kSearchT + threadIdx.x;
+        if (idx < hi) {
+          ra[k] = in_a[idx];
+          rb[k] = in_b[idx];
+        } else {
+          ra[k] = make_uint4(0u, 0u, 0u, 0u);  // in-degree 0: no candidate
+          rb[k] = make_uint4(kInvalid, kInvalid, kInvalid, kInvalid);
         }
       }
-    }
+      int32_t pv[kBuV];
 #pragma unroll
-    for (int k = 0; k < kBuV; k++) {
-      const uint32_t v = ra[k].x, start = ra[k].y, deg = ra[k].z, od = ra[k].w;
-      if (deg == 0 || pv[k] >= 0) continue;  // no candidate, or visited
-      if (hit[k] < kRecN) {
-        parents[v] = (int32_t)par[k];
-        distances[v] = dnext;
-        nf++;
-        edges += hit[k] + 1;
-        atomicOr(&bm_next[v >> 5], 1u << (v & 31));
-        fed += od;
-        if (od) {
-          bu_push_list(sm, v);
-          mx = max(mx, od);
+      for (int k = 0; k < kBuV; k++) pv[k] = (check_parents && ra[k].z) ? parents[ra[k].x] : -1;
+      uint32_t hit[kBuV], par[kBuV];
+#pragma unroll
+      for (int k = 0; k < kBuV; k++) {
+        hit[k] = kRecN;
+        par[k] = 0;
+#pragma unroll
+        for (int m = (int)kRecN - 1; m >= 0; m--) {
+          const uint32_t x = rec_nbr(rb[k], m);
+          if (x != kInvalid && ((bm_cur[x >> 5] >> (x & 31)) & 1u)) {
+            hit[k] = (uint32_t)m;
+            par[k] = x;
+          }
         }
-      } else if (deg > kRecN) {
-        edges += kRecN;
-        const uint32_t h = warp_atomic_inc(&sm.nheavy);
-        sm.hv[h] = rbase + k * kSearchT + threadIdx.x;
-        sm.hj[h] = start + kRecN;
-        sm.he[h] = start + deg;
-      } else {
-        edges += deg;
-        bu_push_ul(sm, rbase + k * kSearchT + threadIdx.x);
+      }
+#pragma unroll
+      for (int k = 0; k < kBuV; k++) {
+        const uint32_t v = ra[k].x, deg = ra[k].z, od = ra[k].w;
+        if (deg == 0 || pv[k] >= 0) continue;  // no candidate, or visited
+        if (hit[k] < kRecN) {
+          parents[v] = (int32_t)par[k];
+          distances[v] = dnext;
+          nf++;
+          edges += hit[k] + 1;
+          atomicOr(&bm_next[v >> 5], 1u << (v & 31));
+          fed += od;
+          if (od) {
+            bu_push_list(sm, v);
+            mx = max(mx, od);
+          }
+        } else if (deg > kRecN) {
+          edges += kRecN;
+          const uint32_t h = warp_atomic_inc(&sm.nheavy);
+          sm.hv[h] = rbase + k * kSearchT + threadIdx.x;
+        } else {
+          edges += deg;
+          bu_push_ul(sm, rbase + k * kSearchT + threadIdx.x);
+        }
       }
     }
     __syncthreads();
