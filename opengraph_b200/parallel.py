@@ -25,6 +25,14 @@ backend the process group has (NCCL between GPUs).  The step object is
 passed in, so the partition and exchange logic can also be exercised with
 another implementation of the same three calls.
 
+Batched work
+------------
+Multi-source BFS roots, personalized-PageRank seeds and small graphs are
+independent units: ``replicas`` gives each rank a contiguous share, runs the
+library's batched kernels on it against its own copy of the graph, and
+all-gathers the result rows in unit order (``msbfs_replicas``,
+``ppr_replicas``).  There is no exchange inside the work.
+
 Graph build
 -----------
 ``exchange_edges`` turns each rank's shard of the edge list (the shards in
@@ -399,3 +407,70 @@ def partitioned_device_graph(lib, src, dst, w, V: int, ranges, rank: int, world:
     dg = lib.device_graph()
     dg.build(s, d, V, sort_type, weight=ww, stream=stream)
     return dg, E
+
+
+def split_units(n: int, rank: int, world: int) -> tuple[int, int]:
+    """This rank's contiguous share [a, b) of n independent units."""
+    return n * rank // world, n * (rank + 1) // world
+
+
+def replicas(run, units, rank: int, world: int, dist=None, group=None):
+    """Independent units (roots, seeds, graphs) split across the ranks: this
+    rank runs ``run(its units)``, which returns a tensor with one row per
+    unit; every rank gets the rows of all units, in unit order (an all-gather
+    of the shares, padded to the largest)."""
+    import torch
+    if world > 1 and dist is None:
+        raise ValueError("world > 1 needs torch.distributed")
+    units = list(units)
+    n = len(units)
+    a, b = split_units(n, rank, world)
+    local = run(units[a:b])
+    if local.shape[0] != b - a:
+        raise ValueError(f"run returned {local.shape[0]} rows for {b - a} units")
+    if world == 1:
+        return local
+    sizes = [split_units(n, r, world)[1] - split_units(n, r, world)[0] for r in range(world)]
+    pad = torch.zeros((max(sizes),) + tuple(local.shape[1:]), dtype=local.dtype, device=local.device)
+    pad[: b - a] = local
+    recv = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(recv, pad, group=group)
+    return torch.cat([recv[r][: sizes[r]] for r in range(world)])
+
+
+def msbfs_replicas(dg, roots, rank: int, world: int, dist=None, group=None, stream=None):
+    """Depths of many single-source searches (one row per root, V uint16
+    entries, 0xFFFF unreached), the roots split across the ranks and run 64
+    at a time by the library's multi-source BFS (``ogb_msbfs``) on each rank's
+    copy of the graph."""
+    import torch
+
+    def run(rs):
+        V = dg.view(False).num_vertices
+        out = torch.empty((len(rs), V), dtype=torch.int16, device="cuda")
+        depths = torch.empty(V * 64, dtype=torch.int16, device="cuda")
+        for i in range(0, len(rs), 64):
+            chunk = rs[i: i + 64]
+            dg.msbfs(chunk, depths, stream=stream)
+            out[i: i + len(chunk)] = depths.view(V, 64)[:, : len(chunk)].t()
+        return out
+    return replicas(run, roots, rank, world, dist, group)
+
+
+def ppr_replicas(dg, seeds, rank: int, world: int, max_iterations: int = 20, epsilon: float = 0.0, dist=None,
+                 group=None, stream=None):
+    """Personalized PageRank vectors (one row per seed, V float32), the seeds
+    split across the ranks and run 32 at a time by the library's batched PPR
+    (``ogb_ppr``) on each rank's copy of the graph."""
+    import torch
+
+    def run(ss):
+        V = dg.view(False).num_vertices
+        out = torch.empty((len(ss), V), dtype=torch.float32, device="cuda")
+        ranks = torch.empty(V * 32, dtype=torch.float32, device="cuda")
+        for i in range(0, len(ss), 32):
+            chunk = ss[i: i + 32]
+            dg.ppr(chunk, ranks, max_iterations=max_iterations, epsilon=epsilon, stream=stream)
+            out[i: i + len(chunk)] = ranks.view(V, 32)[:, : len(chunk)].t()
+        return out
+    return replicas(run, seeds, rank, world, dist, group)
