@@ -294,6 +294,15 @@ int ogb_pagerank_range_init(ogb_graph *g, float *d_ranks, float *d_contrib, void
 int ogb_pagerank_range_step(ogb_graph *g, uint32_t lo, uint32_t hi, const float *d_contrib, float *d_ranks,
                             float *d_contrib_next, double epsilon, double *d_err, uint32_t *d_active, void *stream);
 int ogb_pagerank_range_finish(ogb_graph *g, float *d_ranks, void *stream);
+/* range_step with the all-gather fused in: d_peers is a DEVICE array of
+ * npeers addresses of V-float buffers (the ranks' next-contrib buffers,
+ * e.g. symmetric memory mapped over NVLink; this rank's own may be among
+ * them); every contrib of [lo, hi) is stored into each of them as it is
+ * computed, then ordered by a system-scope fence, so the caller needs only a
+ * barrier across the ranks before the next step reads them. */
+int ogb_pagerank_range_step_peers(ogb_graph *g, uint32_t lo, uint32_t hi, const float *d_contrib, float *d_ranks,
+                                  float *d_contrib_next, const uint64_t *d_peers, uint32_t npeers, double epsilon,
+                                  double *d_err, uint32_t *d_active, void *stream);
 /* Graph build across several GPUs (no counterpart in the reference, which
  * sorts one edge list: radixsort.c:46-335, graphCSR.c:107-248).  Ranks own
  * the vertex ranges [bounds[r], bounds[r+1]) (bounds: nparts + 1 ascending

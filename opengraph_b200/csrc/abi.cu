@@ -2217,6 +2217,16 @@ extern "C" int ogb_pagerank_range_step(ogb_graph* g, uint32_t lo, uint32_t hi, c
                              as_stream(stream));
 }
 
+extern "C" int ogb_pagerank_range_step_peers(ogb_graph* g, uint32_t lo, uint32_t hi, const float* d_contrib,
+                                             float* d_ranks, float* d_contrib_next, const uint64_t* d_peers,
+                                             uint32_t npeers, double epsilon, double* d_err, uint32_t* d_active,
+                                             void* stream) {
+  if (!g || !d_contrib || !d_ranks || !d_contrib_next || !d_err || !d_active || (npeers && !d_peers))
+    return fail(ERR_ARG, "null");
+  return pagerank_range_step(g->g, lo, hi, d_contrib, d_ranks, d_contrib_next, epsilon, d_err, d_active,
+                             as_stream(stream), reinterpret_cast<float* const*>(d_peers), npeers);
+}
+
 extern "C" int ogb_pagerank_range_finish(ogb_graph* g, float* d_ranks, void* stream) {
   if (!g || !d_ranks) return fail(ERR_ARG, "null");
   return pagerank_range_finish(g->g, d_ranks, as_stream(stream));

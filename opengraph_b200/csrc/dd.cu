@@ -935,7 +935,11 @@ int rank_sort(const float* ranks, uint32_t* labels, uint32_t n, cudaStream_t s) 
 // kernel, whatever the partition), rank 0.15 + 0.85 s, contrib_next[v] =
 // rank / out_degree (0 without out-edges); |change| / V and the count of
 // changes >= epsilon are added to *err / *active.  The caller all-gathers
-// contrib_next's slices between steps (pageRank.c:984-1044 per iteration).
+// contrib_next's slices between steps (pageRank.c:984-1044 per iteration),
+// or passes the other ranks' contrib_next buffers as peers: the step then
+// stores each owned contrib into every one of them as it is computed (the
+// all-gather fused into the step: over NVLink when the peers are other
+// GPUs' memory), and the caller only needs a barrier between steps.
 
 namespace {
 
@@ -979,6 +983,8 @@ struct RangePolicy {
   float* pr;
   float* contrib_next;
   DdParams p;
+  float* const* peers = nullptr;  // fused exchange: contrib_next also stored into each of these
+  uint32_t npeers = 0;
   double err = 0.0;
   uint32_t act = 0;
   __device__ bool want(uint32_t) const { return true; }
@@ -989,7 +995,9 @@ struct RangePolicy {
     const float prev = pr[v];
     pr[v] = nv;
     const uint32_t d = out_degree[v];
-    contrib_next[v] = d ? __fdiv_rn(nv, (float)d) : 0.0f;
+    const float c = d ? __fdiv_rn(nv, (float)d) : 0.0f;
+    contrib_next[v] = c;
+    for (uint32_t k = 0; k < npeers; k++) peers[k][v] = c;
     const double e = fabs((double)__fsub_rn(nv, prev));
     err += e / (double)p.V;
     act += (e >= p.epsilon) ? 1u : 0u;
@@ -1021,6 +1029,9 @@ __global__ void __launch_bounds__(kT) range_step_kernel(const uint2* __restrict_
     // medium / heavy lists hold absolute vertex ids: run them unshifted
     rows_pass(rows, med, heavy, ctl->n_med, ctl->n_heavy, 0, nb_light, nb_med, pol);
   }
+  // peer stores (other GPUs' memory over NVLink) ordered before anything
+  // this thread does after the step, the caller's barrier included
+  if (pol.npeers) __threadfence_system();
   double err = pol.err;
   uint32_t act = pol.act;
   __shared__ double s_e[kT / 32];
@@ -1078,8 +1089,10 @@ int pagerank_range_init(DevGraph& g, float* ranks, float* contrib, cudaStream_t 
 }
 
 int pagerank_range_step(DevGraph& g, uint32_t lo, uint32_t hi, const float* contrib, float* ranks,
-                        float* contrib_next, double epsilon, double* d_err, uint32_t* d_active, cudaStream_t s) {
+                        float* contrib_next, double epsilon, double* d_err, uint32_t* d_active, cudaStream_t s,
+                        float* const* peers, uint32_t npeers) {
   if (lo > hi || hi > g.V) return fail(ERR_RANGE, "pagerank range [%u, %u) outside [0, %u)", lo, hi, g.V);
+  if (npeers && !peers) return fail(ERR_ARG, "pagerank range: %u peers without their addresses", npeers);
   if (lo == hi) return OK;
   RangeWork* w = nullptr;
   {
@@ -1113,7 +1126,7 @@ int pagerank_range_step(DevGraph& g, uint32_t lo, uint32_t hi, const float* cont
   p.damp = 0.85f;
   p.base_pr = 1.0f - p.damp;
   p.epsilon = epsilon;
-  RangePolicy pol{lo, g.inv.d_dst(), g.fwd.d_out_degree(), contrib, ranks, contrib_next, p};
+  RangePolicy pol{lo, g.inv.d_dst(), g.fwd.d_out_degree(), contrib, ranks, contrib_next, p, peers, npeers};
   const Grid3 G = rows_grid(hi - lo);
   range_step_kernel<<<G.total(), kT, 0, s>>>(g.inv.d_rows(), lo, hi, w->med.as<uint32_t>(), w->heavy.as<uint32_t>(),
                                              G.light, G.med, pol, ctl, d_err, d_active);

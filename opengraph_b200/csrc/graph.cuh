@@ -269,8 +269,11 @@ void dd_work_free(const DevGraph* g);
 // (device, zeroed by the caller).  init: ranks = 1 - 0.85, contrib = that /
 // out_degree on all V; finish: ranks /= V.  dd.cu.
 int pagerank_range_init(DevGraph& g, float* ranks, float* contrib, cudaStream_t s);
+// peers (device array of npeers buffers of V floats, optional): contrib_next
+// on [lo, hi) is also stored into each of them.
 int pagerank_range_step(DevGraph& g, uint32_t lo, uint32_t hi, const float* contrib, float* ranks,
-                        float* contrib_next, double epsilon, double* d_err, uint32_t* d_active, cudaStream_t s);
+                        float* contrib_next, double epsilon, double* d_err, uint32_t* d_active, cudaStream_t s,
+                        float* const* peers = nullptr, uint32_t npeers = 0);
 int pagerank_range_finish(DevGraph& g, float* ranks, cudaStream_t s);
 void range_work_free(const DevGraph* g);
 // Stable split of an edge-list shard by vertex owner (ranges

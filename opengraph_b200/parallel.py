@@ -117,14 +117,23 @@ class DeviceRangeStep:
         self.lib.check(self.lib.ogb_pagerank_range_init(self.dg.handle, _ptr(ranks), _ptr(contrib),
                                                         _stream(self.stream)), "ogb_pagerank_range_init")
 
-    def step(self, lo, hi, contrib, ranks, contrib_next, epsilon) -> tuple[float, int]:
-        """One iteration over [lo, hi); returns the range's (error, active)."""
+    def step(self, lo, hi, contrib, ranks, contrib_next, epsilon, peers=None) -> tuple[float, int]:
+        """One iteration over [lo, hi); returns the range's (error, active).
+        peers: a device int64 tensor of buffer addresses that also receive
+        contrib_next on [lo, hi) (the fused exchange)."""
         self.err.zero_()
         self.act.zero_()
-        self.lib.check(self.lib.ogb_pagerank_range_step(self.dg.handle, int(lo), int(hi), _ptr(contrib), _ptr(ranks),
-                                                        _ptr(contrib_next), float(epsilon), _ptr(self.err),
-                                                        _ptr(self.act), _stream(self.stream)),
-                       "ogb_pagerank_range_step")
+        if peers is None:
+            self.lib.check(self.lib.ogb_pagerank_range_step(self.dg.handle, int(lo), int(hi), _ptr(contrib),
+                                                            _ptr(ranks), _ptr(contrib_next), float(epsilon),
+                                                            _ptr(self.err), _ptr(self.act), _stream(self.stream)),
+                           "ogb_pagerank_range_step")
+        else:
+            self.lib.check(self.lib.ogb_pagerank_range_step_peers(self.dg.handle, int(lo), int(hi), _ptr(contrib),
+                                                                  _ptr(ranks), _ptr(contrib_next), _ptr(peers),
+                                                                  int(peers.numel()), float(epsilon), _ptr(self.err),
+                                                                  _ptr(self.act), _stream(self.stream)),
+                           "ogb_pagerank_range_step_peers")
         return float(self.err.item()), int(self.act.item())
 
     def finish(self, ranks):
@@ -141,19 +150,48 @@ class PartitionResult:
     ranges: list
 
 
+class PeerContribs:
+    """The fused exchange of the partitioned pull: the two next-contrib
+    buffers in symmetric memory (torch.distributed._symmetric_memory), mapped
+    on every rank, so a range step stores each owned contrib into every
+    rank's copy over NVLink (``ogb_pagerank_range_step_peers``) instead of an
+    all-gather after it."""
+
+    def __init__(self, V: int, device, group=None):
+        import torch
+        import torch.distributed as tdist
+        import torch.distributed._symmetric_memory as symm
+        g = group if group is not None else tdist.group.WORLD
+        self.bufs = [symm.empty(V, dtype=torch.float32, device=device) for _ in range(2)]
+        self.handles = [symm.rendezvous(b, g.group_name) for b in self.bufs]
+        self.peers = [torch.tensor([int(x) for x in h.buffer_ptrs], dtype=torch.int64, device=device)
+                      for h in self.handles]
+
+    def barrier(self, k: int):
+        self.handles[k].barrier()
+
+
 def pagerank_pull_partitioned(step, V: int, ranges, rank: int, world: int, max_iterations: int, epsilon: float,
-                              device, dist=None, group=None):
+                              device, dist=None, group=None, fused: bool = False):
     """Run the partitioned pull on this rank; returns (the whole normalized
     rank vector on every rank, PartitionResult).  ``dist`` is
-    torch.distributed (None for a single process: world must be 1)."""
+    torch.distributed (None for a single process: world must be 1).  fused:
+    the contrib exchange inside the range step (peer stores into symmetric
+    memory, then a barrier) instead of an all-gather after it; GPUs with a
+    process group only."""
     import torch
     if world > 1 and dist is None:
         raise ValueError("world > 1 needs torch.distributed")
     lo, hi = ranges[rank]
     maxlen = max(h - l for l, h in ranges)
     ranks = torch.empty(V, dtype=torch.float32, device=device)
-    contrib = torch.empty(V, dtype=torch.float32, device=device)
-    contrib_next = torch.empty(V, dtype=torch.float32, device=device)
+    peer = PeerContribs(V, device, group) if fused else None
+    if peer is not None:
+        contrib, contrib_next = peer.bufs
+        which = 1  # the buffer contrib_next is
+    else:
+        contrib = torch.empty(V, dtype=torch.float32, device=device)
+        contrib_next = torch.empty(V, dtype=torch.float32, device=device)
     step.init(ranks, contrib)
     send = torch.zeros(maxlen, dtype=torch.float32, device=device)
     recv = [torch.zeros(maxlen, dtype=torch.float32, device=device) for _ in range(world)]
@@ -176,12 +214,19 @@ def pagerank_pull_partitioned(step, V: int, ranges, rank: int, world: int, max_i
     err = 0.0
     act = 0
     for it in range(max_iterations):
-        err, act = step.step(lo, hi, contrib, ranks, contrib_next, epsilon)
+        if peer is not None:
+            err, act = step.step(lo, hi, contrib, ranks, contrib_next, epsilon, peers=peer.peers[which])
+        else:
+            err, act = step.step(lo, hi, contrib, ranks, contrib_next, epsilon)
         if world > 1:
             tot = torch.tensor([err, float(act)], dtype=torch.float64, device=device)
             dist.all_reduce(tot, group=group)
             err, act = float(tot[0].item()), int(round(float(tot[1].item())))
-        gather_slices(contrib_next, contrib_next)
+        if peer is not None:
+            peer.barrier(which)  # every rank's stores into every copy are done
+            which ^= 1
+        else:
+            gather_slices(contrib_next, contrib_next)
         contrib, contrib_next = contrib_next, contrib
         executed = it + 1
         if act == 0:
