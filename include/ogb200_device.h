@@ -361,6 +361,28 @@ int ogb_bfs_range_expand(ogb_graph *g, uint32_t lo, uint32_t hi, uint32_t direct
 int ogb_bfs_range_settle(ogb_graph *g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth,
                          int32_t *d_cand, uint8_t *d_next, uint8_t *d_visited, int32_t *d_parents,
                          uint32_t *d_dist, uint64_t *d_counts, void *stream);
+/* The same search with the exchange fused into the steps (no all-reduce of
+ * cand or next).  d_cand and the two next buffers are memory every rank maps
+ * (e.g. symmetric memory over NVLink), 4-byte aligned; d_cand_peers /
+ * d_next_peers are DEVICE arrays of every rank's address of them (rank
+ * order), d_bounds a DEVICE array of the nparts + 1 range bounds.  A step:
+ * ogb_bfs_range_expand_peers (top-down: each candidate goes straight to the
+ * cand array of its vertex's owner by atomicMin; bottom-up: as
+ * ogb_bfs_range_expand, zeroing only the owned next bytes), then for a
+ * top-down step a barrier across the ranks, then ogb_bfs_range_claim_peers
+ * (top-down: the owned vertices with a candidate are reached -- parent =
+ * the smallest frontier in-neighbour, depth, d_counts -- and d_cand is put
+ * back; both: the owned next bytes are stored into every rank's next
+ * buffer), a barrier, and ogb_bfs_range_settle with direction 1 (visited |=
+ * next).  Both calls end with a system-scope fence; the caller's barrier
+ * must order them across the GPUs. */
+int ogb_bfs_range_expand_peers(ogb_graph *g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth,
+                               const uint8_t *d_frontier, const uint8_t *d_visited, uint8_t *d_next,
+                               const uint64_t *d_cand_peers, const uint32_t *d_bounds, uint32_t nparts,
+                               int32_t *d_parents, uint32_t *d_dist, uint64_t *d_counts, void *stream);
+int ogb_bfs_range_claim_peers(ogb_graph *g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth,
+                              int32_t *d_cand, uint8_t *d_next, const uint64_t *d_next_peers, uint32_t npeers,
+                              int32_t *d_parents, uint32_t *d_dist, uint64_t *d_counts, void *stream);
 /* radixSortEdgesByPageRank (reorder.c:165-221) on device arrays: d_labels
  * stably sorted in place, ascending by (uint32_t)(rank * 2^20 + 0.5f). */
 int ogb_sort_by_rank(const float *d_ranks, uint32_t *d_labels, uint32_t n, void *stream);

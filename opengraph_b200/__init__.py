@@ -280,6 +280,8 @@ _DEVICE_API = [
     ("ogb_pagerank_range_finish", C.c_int, [vp, vp, vp]),
     ("ogb_pagerank_range_step_peers", C.c_int, [vp, u32, u32, vp, vp, vp, vp, u32, C.c_double, vp, vp, vp]),
     ("ogb_partition_edges", C.c_int, [vp, vp, vp, u32, vp, u32, vp, vp, vp, vp, vp]),
+    ("ogb_bfs_range_expand_peers", C.c_int, [vp, u32, u32, u32, u32, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp]),
+    ("ogb_bfs_range_claim_peers", C.c_int, [vp, u32, u32, u32, u32, vp, vp, vp, u32, vp, vp, vp, vp]),
     ("ogb_bfs_range_init", C.c_int, [vp, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp]),
     ("ogb_bfs_range_expand", C.c_int, [vp, u32, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp]),
     ("ogb_bfs_range_settle", C.c_int, [vp, u32, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp]),

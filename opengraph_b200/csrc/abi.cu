@@ -2265,6 +2265,27 @@ extern "C" int ogb_bfs_range_settle(ogb_graph* g, uint32_t lo, uint32_t hi, uint
                           reinterpret_cast<unsigned long long*>(d_counts), as_stream(stream));
 }
 
+extern "C" int ogb_bfs_range_expand_peers(ogb_graph* g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth,
+                                          const uint8_t* d_frontier, const uint8_t* d_visited, uint8_t* d_next,
+                                          const uint64_t* d_cand_peers, const uint32_t* d_bounds, uint32_t nparts,
+                                          int32_t* d_parents, uint32_t* d_dist, uint64_t* d_counts, void* stream) {
+  if (!g || !d_frontier || !d_visited || !d_next || !d_cand_peers || !d_bounds || !d_parents || !d_dist || !d_counts)
+    return fail(ERR_ARG, "null");
+  return bfs_range_expand_peers(g->g, lo, hi, direction, depth, d_frontier, d_visited, d_next,
+                                reinterpret_cast<int32_t* const*>(d_cand_peers), d_bounds, nparts, d_parents, d_dist,
+                                reinterpret_cast<unsigned long long*>(d_counts), as_stream(stream));
+}
+
+extern "C" int ogb_bfs_range_claim_peers(ogb_graph* g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth,
+                                         int32_t* d_cand, uint8_t* d_next, const uint64_t* d_next_peers,
+                                         uint32_t npeers, int32_t* d_parents, uint32_t* d_dist, uint64_t* d_counts,
+                                         void* stream) {
+  if (!g || !d_cand || !d_next || !d_next_peers || !d_parents || !d_dist || !d_counts) return fail(ERR_ARG, "null");
+  return bfs_range_claim_peers(g->g, lo, hi, direction, depth, d_cand, d_next,
+                               reinterpret_cast<uint8_t* const*>(d_next_peers), npeers, d_parents, d_dist,
+                               reinterpret_cast<unsigned long long*>(d_counts), as_stream(stream));
+}
+
 extern "C" int ogb_sort_by_rank(const float* d_ranks, uint32_t* d_labels, uint32_t n, void* stream) {
   if (n && (!d_ranks || !d_labels)) return fail(ERR_ARG, "null");
   return rank_sort(d_ranks, d_labels, n, as_stream(stream));

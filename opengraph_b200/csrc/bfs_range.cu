@@ -36,6 +36,17 @@
 //
 // The scans over vertex bytes read 4 bytes at a time when the buffers are
 // 4-byte aligned (and cand 16-byte aligned), else one at a time.
+//
+// Fused exchange (bfs_range_expand_peers / bfs_range_claim_peers), with the
+// cand array and two alternating next buffers in memory every rank maps (for
+// example symmetric memory over NVLink): a top-down expand sends each
+// candidate straight to the cand array of w's owner (remote atomicMin); after
+// a barrier each owner claims its vertices from its own cand, writes its
+// owned next bytes and stores them into every rank's next buffer; after a
+// second barrier each rank merges visited |= next (bfs_range_settle with
+// direction 1).  A bottom-up step zeroes only its owned next bytes, finds its
+// parents as above, and broadcasts its owned next bytes the same way.  No
+// all-reduce of cand or next: each byte crosses the links once per reader.
 #include "graph.cuh"
 
 #include <algorithm>
@@ -92,19 +103,41 @@ __global__ void bfsr_init_kernel(uint32_t lo, uint32_t hi, uint32_t root, const 
   }
 }
 
+// Where a top-down step's candidate for w goes: this rank's cand array, or
+// (fused exchange) the cand array of w's owner, mapped from another GPU.
+struct CandLocal {
+  int32_t* cand;
+  __device__ __forceinline__ int32_t* at(uint32_t w) const { return cand + w; }
+  static constexpr bool kPeers = false;
+};
+struct CandPeers {
+  int32_t* const* cand;     // per rank: its cand array (V entries)
+  const uint32_t* bounds;   // owner ranges: rank r owns [bounds[r], bounds[r + 1])
+  uint32_t nparts;
+  __device__ __forceinline__ int32_t* at(uint32_t w) const {
+    uint32_t lo = 0, hi = nparts;  // the owner is in [lo, hi)
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (w >= __ldg(&bounds[mid])) lo = mid; else hi = mid;
+    }
+    return cand[lo] + w;
+  }
+  static constexpr bool kPeers = true;
+};
+
 // Top-down, the owned frontier vertices: short rows by their thread, longer
 // rows queued in chunks.
-template <bool kVec>
+template <bool kVec, class T>
 __global__ void bfsr_td_kernel(uint32_t V, uint32_t lo, uint32_t hi, const uint8_t* __restrict__ frontier,
                                const uint8_t* __restrict__ visited, const uint2* __restrict__ rows,
-                               const uint32_t* __restrict__ nbr, int32_t* __restrict__ cand, RangeQueue* q,
+                               const uint32_t* __restrict__ nbr, T cand, RangeQueue* q,
                                uint32_t qcap, unsigned long long* __restrict__ counts) {
   for_bytes<kVec, true>(frontier, lo, hi, V, [&](uint32_t u) {
     const uint2 r = rows[u];
     if (r.y <= kThreadRow) {
       for (uint32_t j = r.x; j < r.x + r.y; j++) {
         const uint32_t w = __ldg(&nbr[j]) & 0x3FFFFFFFu;
-        if (!visited[w]) atomicMin(&cand[w], (int32_t)u);  // result unused: a reduction, no round trip
+        if (!visited[w]) atomicMin(cand.at(w), (int32_t)u);  // result unused: a reduction, no round trip
       }
     } else {
       const uint32_t nc = (r.y + kRowChunk - 1) / kRowChunk;
@@ -117,11 +150,13 @@ __global__ void bfsr_td_kernel(uint32_t V, uint32_t lo, uint32_t hi, const uint8
         q->item[k0 + k] = make_uint4(u, r.x + k * kRowChunk, r.x + min(r.y, (k + 1) * kRowChunk), 0u);
     }
   });
+  if (T::kPeers) __threadfence_system();  // the remote atomics before the caller's barrier
 }
 
 // Top-down, the queued chunks: a warp per chunk, lanes strided over its edges.
+template <class T>
 __global__ void bfsr_td_rows_kernel(const uint8_t* __restrict__ visited, const uint32_t* __restrict__ nbr,
-                                    int32_t* __restrict__ cand, const RangeQueue* q, uint32_t qcap) {
+                                    T cand, const RangeQueue* q, uint32_t qcap) {
   const uint32_t lane = lane_id();
   const uint32_t gw = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   const uint32_t nw = gridDim.x * (blockDim.x / 32);
@@ -130,9 +165,10 @@ __global__ void bfsr_td_rows_kernel(const uint8_t* __restrict__ visited, const u
     const uint4 it = q->item[t];
     for (uint32_t j = it.y + lane; j < it.z; j += 32) {
       const uint32_t w = __ldg(&nbr[j]) & 0x3FFFFFFFu;
-      if (!visited[w]) atomicMin(&cand[w], (int32_t)it.x);
+      if (!visited[w]) atomicMin(cand.at(w), (int32_t)it.x);
     }
   }
+  if (T::kPeers) __threadfence_system();
 }
 
 // The first in-neighbour of a vertex in the frontier, in CSR order of its
@@ -308,6 +344,52 @@ __global__ void bfsr_settle_kernel(uint32_t V, uint32_t lo, uint32_t hi, uint32_
   }
 }
 
+// Fused exchange, top-down: the owned vertices with a candidate (in this
+// rank's cand, which every rank's expand fed) are reached: parent, depth,
+// counts; their next bytes are written (0 or 1 over the whole owned range)
+// and cand is put back to kNoCand.
+__global__ void bfsr_claim_owned_kernel(uint32_t lo, uint32_t hi, uint32_t depth, int32_t* __restrict__ cand,
+                                        uint8_t* __restrict__ next, const uint32_t* __restrict__ out_degree,
+                                        int32_t* __restrict__ parents, uint32_t* __restrict__ dist,
+                                        unsigned long long* __restrict__ counts) {
+  uint32_t found = 0;
+  unsigned long long mf = 0;
+  for (uint32_t v = lo + blockIdx.x * blockDim.x + threadIdx.x; v < hi; v += gridDim.x * blockDim.x) {
+    const int32_t c = cand[v];
+    const uint32_t nx = settle_td_vertex(v, c, lo, hi, depth, out_degree, parents, dist, found, mf);
+    next[v] = (uint8_t)nx;
+    if (nx) cand[v] = kNoCand;
+  }
+  warp_atomic_add_total64(&counts[0], found);
+  const uint32_t active = __activemask();
+  unsigned long long t = mf;
+  for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(active, t, o);
+  if ((int)lane_id() == __ffs(active) - 1 && t) atomicAdd(&counts[1], t);
+}
+
+// Fused exchange: this rank's next bytes of its owned range [lo, hi) copied
+// into every rank's next buffer (peer stores; 4 bytes at a time inside the
+// range, single bytes on its ragged ends, so no other owner's byte is
+// written), then ordered before the caller's barrier.
+__global__ void bfsr_broadcast_kernel(uint32_t lo, uint32_t hi, const uint8_t* __restrict__ src,
+                                      uint8_t* const* __restrict__ peers, uint32_t npeers) {
+  const uint32_t a = (lo + 3) & ~3u, b = hi & ~3u;  // whole words [a, b)
+  const uint32_t stride = gridDim.x * blockDim.x, tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a < b) {
+    for (uint32_t w = a / 4 + tid; w < b / 4; w += stride) {
+      const uint32_t x = reinterpret_cast<const uint32_t*>(src)[w];
+      for (uint32_t p = 0; p < npeers; p++) reinterpret_cast<uint32_t*>(peers[p])[w] = x;
+    }
+  }
+  // the ends: [lo, min(a, hi)) and [max(b, a, lo), hi)
+  const uint32_t e0 = min(a, hi), e1 = max(max(b, a), lo);
+  for (uint32_t v = lo + tid; v < e0; v += stride)
+    for (uint32_t p = 0; p < npeers; p++) peers[p][v] = src[v];
+  for (uint32_t v = e1 + tid; v < hi; v += stride)
+    for (uint32_t p = 0; p < npeers; p++) peers[p][v] = src[v];
+  __threadfence_system();
+}
+
 bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
 
 }  // namespace
@@ -327,6 +409,21 @@ static int range_queue(DevGraph& g, RangeQueue** q, uint32_t* cap) {
 static int range_check(const DevGraph& g, uint32_t lo, uint32_t hi, uint32_t direction) {
   if (lo > hi || hi > g.V) return fail(ERR_ARG, "bfs range: [%u, %u) is not inside [0, %u)", lo, hi, g.V);
   if (direction > 1) return fail(ERR_ARG, "bfs range: direction %u (0 top-down, 1 bottom-up)", direction);
+  return OK;
+}
+
+template <class T>
+static int launch_td(DevGraph& g, uint32_t lo, uint32_t hi, const uint8_t* frontier, const uint8_t* visited, T cand,
+                     RangeQueue* q, uint32_t cap, unsigned long long* counts, bool vec, cudaStream_t s) {
+  const int grid = sm_count() * 8;
+  if (vec)
+    bfsr_td_kernel<true, T><<<grid, 256, 0, s>>>(g.V, lo, hi, frontier, visited, g.fwd.d_rows(), g.fwd.d_dst(), cand,
+                                                 q, cap, counts);
+  else
+    bfsr_td_kernel<false, T><<<grid, 256, 0, s>>>(g.V, lo, hi, frontier, visited, g.fwd.d_rows(), g.fwd.d_dst(),
+                                                  cand, q, cap, counts);
+  bfsr_td_rows_kernel<T><<<grid, 256, 0, s>>>(visited, g.fwd.d_dst(), cand, q, cap);
+  OGB_CUDA(cudaGetLastError());
   return OK;
 }
 
@@ -376,14 +473,54 @@ int bfs_range_expand(DevGraph& g, uint32_t lo, uint32_t hi, uint32_t direction, 
                                                  g.inv.d_dst(), parents, dist, next, counts, q, cap);
     bfsr_bu_long_kernel<<<grid, 256, 0, s>>>(frontier, depth, g.inv.d_dst(), parents, dist, next, counts, q, cap);
   } else {
-    if (vec)
-      bfsr_td_kernel<true><<<grid, 256, 0, s>>>(g.V, lo, hi, frontier, visited, g.fwd.d_rows(), g.fwd.d_dst(), cand,
-                                                q, cap, counts);
-    else
-      bfsr_td_kernel<false><<<grid, 256, 0, s>>>(g.V, lo, hi, frontier, visited, g.fwd.d_rows(), g.fwd.d_dst(),
-                                                 cand, q, cap, counts);
-    bfsr_td_rows_kernel<<<grid, 256, 0, s>>>(visited, g.fwd.d_dst(), cand, q, cap);
+    OGB_TRY(launch_td(g, lo, hi, frontier, visited, CandLocal{cand}, q, cap, counts, vec, s));
   }
+  OGB_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int bfs_range_expand_peers(DevGraph& g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth,
+                           const uint8_t* frontier, const uint8_t* visited, uint8_t* next, int32_t* const* cand_peers,
+                           const uint32_t* bounds, uint32_t nparts, int32_t* parents, uint32_t* dist,
+                           unsigned long long* counts, cudaStream_t s) {
+  OGB_TRY(range_check(g, lo, hi, direction));
+  if (nparts < 1 || !cand_peers || !bounds) return fail(ERR_ARG, "bfs range: no peers");
+  OGB_CUDA(cudaMemsetAsync(counts, 0, 32, s));
+  if (direction == 1 && hi > lo) OGB_CUDA(cudaMemsetAsync(next + lo, 0, hi - lo, s));  // only the owned bytes
+  if (hi == lo) return OK;
+  RangeQueue* q = nullptr;
+  uint32_t cap = 0;
+  OGB_TRY(range_queue(g, &q, &cap));
+  OGB_CUDA(cudaMemsetAsync(q, 0, 16, s));
+  const bool vec = aligned(frontier, 4) && aligned(visited, 4);
+  const int grid = sm_count() * 8;
+  if (direction == 1) {
+    if (vec)
+      bfsr_bu_kernel<true><<<grid, 256, 0, s>>>(g.V, lo, hi, frontier, visited, depth, g.inv.d_rows(),
+                                                g.inv.d_dst(), parents, dist, next, counts, q, cap);
+    else
+      bfsr_bu_kernel<false><<<grid, 256, 0, s>>>(g.V, lo, hi, frontier, visited, depth, g.inv.d_rows(),
+                                                 g.inv.d_dst(), parents, dist, next, counts, q, cap);
+    bfsr_bu_long_kernel<<<grid, 256, 0, s>>>(frontier, depth, g.inv.d_dst(), parents, dist, next, counts, q, cap);
+  } else {
+    OGB_TRY(launch_td(g, lo, hi, frontier, visited, CandPeers{cand_peers, bounds, nparts}, q, cap, counts, vec, s));
+  }
+  OGB_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int bfs_range_claim_peers(DevGraph& g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth, int32_t* cand,
+                          uint8_t* next, uint8_t* const* next_peers, uint32_t npeers, int32_t* parents,
+                          uint32_t* dist, unsigned long long* counts, cudaStream_t s) {
+  OGB_TRY(range_check(g, lo, hi, direction));
+  if (npeers < 1 || !next_peers) return fail(ERR_ARG, "bfs range: no peers");
+  if (!aligned(next, 4)) return fail(ERR_ARG, "bfs range: next buffers must be 4-byte aligned");
+  if (hi == lo) return OK;
+  const int grid = sm_count() * 8;
+  if (direction == 0)
+    bfsr_claim_owned_kernel<<<grid, 256, 0, s>>>(lo, hi, depth, cand, next, g.fwd.d_out_degree(), parents, dist,
+                                                 counts);
+  bfsr_broadcast_kernel<<<grid, 256, 0, s>>>(lo, hi, next, next_peers, npeers);
   OGB_CUDA(cudaGetLastError());
   return OK;
 }

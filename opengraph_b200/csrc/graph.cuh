@@ -291,6 +291,13 @@ int bfs_range_init(DevGraph& g, uint32_t lo, uint32_t hi, uint32_t root, int32_t
 int bfs_range_expand(DevGraph& g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth,
                      const uint8_t* frontier, const uint8_t* visited, uint8_t* next, int32_t* cand,
                      int32_t* parents, uint32_t* dist, unsigned long long* counts, cudaStream_t s);
+int bfs_range_expand_peers(DevGraph& g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth,
+                           const uint8_t* frontier, const uint8_t* visited, uint8_t* next, int32_t* const* cand_peers,
+                           const uint32_t* bounds, uint32_t nparts, int32_t* parents, uint32_t* dist,
+                           unsigned long long* counts, cudaStream_t s);
+int bfs_range_claim_peers(DevGraph& g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth, int32_t* cand,
+                          uint8_t* next, uint8_t* const* next_peers, uint32_t npeers, int32_t* parents,
+                          uint32_t* dist, unsigned long long* counts, cudaStream_t s);
 int bfs_range_settle(DevGraph& g, uint32_t lo, uint32_t hi, uint32_t direction, uint32_t depth, int32_t* cand,
                      uint8_t* next, uint8_t* visited, int32_t* parents, uint32_t* dist, unsigned long long* counts,
                      cudaStream_t s);

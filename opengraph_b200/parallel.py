@@ -67,6 +67,12 @@ byte per vertex over all V.  One step:
    same direction decision (the switch of BFS.c:546-587: mu, mf, nf with
    alpha 15 and beta 18, in the reference's u32 arithmetic).
 
+With ``peers`` (SymmetricBfsBuffers) the exchange is fused into the steps:
+a top-down expand sends each candidate to its owner's cand array (remote
+atomicMin over NVLink), the owner claims and stores its next bytes into
+every rank's buffer, and barriers replace the two all-reduces of cand and
+next; only the four counters are still all-reduced.
+
 Depths, the step count and every step's direction equal the single-GPU
 search's (and the reference's); bottom-up parents are the reference's too
 (the first frontier in-neighbour in CSR order), top-down parents the
@@ -264,6 +270,44 @@ class DeviceBfsRangeStep:
                                                      _ptr(dist), _ptr(counts), _stream(self.stream)),
                        "ogb_bfs_range_settle")
 
+    def expand_peers(self, lo, hi, direction, depth, frontier, visited, nxt, cand_peers, bounds, parents, dist,
+                     counts):
+        self.lib.check(self.lib.ogb_bfs_range_expand_peers(self.dg.handle, int(lo), int(hi), int(direction),
+                                                           int(depth), _ptr(frontier), _ptr(visited), _ptr(nxt),
+                                                           _ptr(cand_peers), _ptr(bounds), int(bounds.numel()) - 1,
+                                                           _ptr(parents), _ptr(dist), _ptr(counts),
+                                                           _stream(self.stream)), "ogb_bfs_range_expand_peers")
+
+    def claim_peers(self, lo, hi, direction, depth, cand, nxt, next_peers, parents, dist, counts):
+        self.lib.check(self.lib.ogb_bfs_range_claim_peers(self.dg.handle, int(lo), int(hi), int(direction),
+                                                          int(depth), _ptr(cand), _ptr(nxt), _ptr(next_peers),
+                                                          int(next_peers.numel()), _ptr(parents), _ptr(dist),
+                                                          _ptr(counts), _stream(self.stream)),
+                       "ogb_bfs_range_claim_peers")
+
+
+class SymmetricBfsBuffers:
+    """The fused exchange of the partitioned BFS: this rank's cand array and
+    two alternating next buffers in symmetric memory
+    (torch.distributed._symmetric_memory), every rank's addresses of them,
+    and the owner bounds, as ``bfs_partitioned(..., peers=...)`` takes them."""
+
+    def __init__(self, V: int, ranges, device, group=None):
+        import torch
+        import torch.distributed as tdist
+        import torch.distributed._symmetric_memory as symm
+        g = group if group is not None else tdist.group.WORLD
+        self.cand = symm.empty(V, dtype=torch.int32, device=device)
+        self.next = [symm.empty(V, dtype=torch.uint8, device=device) for _ in range(2)]
+        bufs = [self.cand, self.next[0], self.next[1]]
+        self.handles = [symm.rendezvous(b, g.group_name) for b in bufs]
+        ptrs = [torch.tensor([int(x) for x in h.buffer_ptrs], dtype=torch.int64, device=device) for h in self.handles]
+        self.cand_peers, self.next_peers = ptrs[0], ptrs[1:]
+        self.bounds = torch.tensor(owner_bounds(ranges), dtype=torch.int32, device=device)
+
+    def barrier(self):
+        self.handles[0].barrier()
+
 
 @dataclass
 class BfsPartitionResult:
@@ -280,13 +324,17 @@ _U32 = 0xFFFFFFFF
 
 
 def bfs_partitioned(step, V: int, E: int, ranges, rank: int, world: int, root: int, device, mode: int = 2,
-                    bu_entry_nf_frontier: bool = False, dist=None, group=None):
+                    bu_entry_nf_frontier: bool = False, dist=None, group=None, peers=None):
     """Run the partitioned BFS on this rank; returns (parents, depths as
     int32 tensors of V, the whole vectors on every rank; BfsPartitionResult).
     mode 0 bottom-up only, 1 top-down only, 2 direction-optimizing;
     bu_entry_nf_frontier starts a bottom-up run with nf = the frontier size
     (the bitmap variant) instead of 0.  ``dist`` is torch.distributed (None
-    for a single process: world must be 1)."""
+    for a single process: world must be 1).  peers: the fused exchange's
+    buffers (SymmetricBfsBuffers: cand, next[2], cand_peers, next_peers[2],
+    bounds, barrier()); the steps then send candidates and next bytes
+    straight to the ranks that need them, with barriers instead of the
+    all-reduces of cand and next."""
     import torch
     if world > 1 and dist is None:
         raise ValueError("world > 1 needs torch.distributed")
@@ -297,12 +345,18 @@ def bfs_partitioned(step, V: int, E: int, ranges, rank: int, world: int, root: i
     lo, hi = ranges[rank]
     parents = torch.empty(V, dtype=torch.int32, device=device)
     depths = torch.empty(V, dtype=torch.int32, device=device)
-    frontier = torch.empty(V, dtype=torch.uint8, device=device)
-    nxt = torch.empty(V, dtype=torch.uint8, device=device)
     visited = torch.empty(V, dtype=torch.uint8, device=device)
-    cand = torch.empty(V, dtype=torch.int32, device=device)
     counts = torch.zeros(4, dtype=torch.int64, device=device)
+    which = 0  # fused exchange: the next buffer that holds the frontier
+    if peers is None:
+        frontier = torch.empty(V, dtype=torch.uint8, device=device)
+        nxt = torch.empty(V, dtype=torch.uint8, device=device)
+        cand = torch.empty(V, dtype=torch.int32, device=device)
+    else:
+        frontier, nxt, cand = peers.next[0], peers.next[1], peers.cand
     step.init(lo, hi, root, parents, depths, frontier, visited, cand, counts)
+    if peers is not None:
+        peers.barrier()  # every rank's cand and frontier set before any rank writes into them
     if world > 1:
         dist.all_reduce(counts, group=group)  # the root's owner holds its out-degree
     mf = int(counts[1].item()) & _U32
@@ -315,15 +369,26 @@ def bfs_partitioned(step, V: int, E: int, ranges, rank: int, world: int, root: i
     examined = 0
 
     def run(direction):
-        nonlocal frontier, nxt, examined
+        nonlocal frontier, nxt, examined, which
         depth = len(dirs) + 1
-        step.expand(lo, hi, direction, depth, frontier, visited, nxt, cand, parents, depths, counts)
-        if world > 1:
+        if peers is None:
+            step.expand(lo, hi, direction, depth, frontier, visited, nxt, cand, parents, depths, counts)
+            if world > 1:
+                if direction == 0:
+                    dist.all_reduce(cand, op=dist.ReduceOp.MIN, group=group)
+                else:
+                    dist.all_reduce(nxt, op=dist.ReduceOp.MAX, group=group)
+            step.settle(lo, hi, direction, depth, cand, nxt, visited, parents, depths, counts)
+        else:
+            step.expand_peers(lo, hi, direction, depth, frontier, visited, nxt, peers.cand_peers, peers.bounds,
+                              parents, depths, counts)
             if direction == 0:
-                dist.all_reduce(cand, op=dist.ReduceOp.MIN, group=group)
-            else:
-                dist.all_reduce(nxt, op=dist.ReduceOp.MAX, group=group)
-        step.settle(lo, hi, direction, depth, cand, nxt, visited, parents, depths, counts)
+                peers.barrier()  # every candidate is in its owner's cand
+            step.claim_peers(lo, hi, direction, depth, cand, nxt, peers.next_peers[which ^ 1], parents, depths,
+                             counts)
+            peers.barrier()  # every owner's next bytes are in every rank's buffer
+            step.settle(lo, hi, 1, depth, cand, nxt, visited, parents, depths, counts)  # visited |= next
+            which ^= 1
         if world > 1:
             dist.all_reduce(counts, group=group)
         c = [int(x) for x in counts.tolist()]

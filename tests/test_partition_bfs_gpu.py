@@ -95,3 +95,83 @@ def test_range_calls_reject_bad_arguments(torch_cuda, lib, graphs):
     with pytest.raises(Exception):
         step.settle(0, V, 2, 1, i[2], b[2], b[1], i[0], i[1], c)  # direction
     dg.close()
+
+
+@pytest.mark.parametrize("kind,kw", [("rmat", dict(scale=14, ef=16, seed=3)), ("star", dict(n=20_000, seed=4)),
+                                     ("grid", dict(side=80, p=0.01, seed=2)), ("chain", dict(n=600))])
+def test_fused_exchange_equals_oracle(torch_cuda, lib, oracle, graphs, kind, kw):
+    """ogb_bfs_range_expand_peers / _claim_peers: candidates sent to their
+    owner's cand array by atomicMin, owners storing their next bytes into
+    every rank's buffer, barriers instead of the all-reduces; each rank a
+    thread with its own graph copy, the ranks' buffers local to this GPU."""
+    from test_partition_bfs_fused import PeerSet
+    torch = torch_cuda
+    s, d, _, V = graphs(kind, **kw)
+    g = oracle.build(s, d, V, 0)
+    E = g["num_edges"]
+    gs = _device_graphs(torch, lib, s, d, V, 3)
+    try:
+        for world in (1, 2, 3):
+            ranges = edge_balanced_ranges(g["i_outdeg"], world)
+            for root in _roots(g, 2):
+                for mode in (2, 0, 1):
+                    ps = PeerSet(V, ranges, world, "cuda")
+                    outs = run_threads(world, lambda r, dd: bfs_partitioned(DeviceBfsRangeStep(gs[r]), V, E, ranges,
+                                                                            r, world, root, "cuda", mode=mode,
+                                                                            dist=dd, peers=ps.view(r)))
+                    for par, dep, res in outs:
+                        check_against_oracle(oracle, g, root, mode, False, host(par, np.int32), host(dep, np.int32),
+                                             res)
+    finally:
+        for dg in gs:
+            dg.close()
+
+
+def _symm_worker(rank, out_path, port):
+    import datetime
+    import os
+
+    import torch
+    import torch.distributed as tdist
+
+    import opengraph_b200 as og
+    from conftest import graph_edges
+    from oracle.oracle import Oracle
+    from opengraph_b200.parallel import SymmetricBfsBuffers
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    tdist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
+                             device_id=torch.device("cuda", 0))
+    try:
+        lib = og.load(False)
+        lib.quiet(True)
+        o = Oracle()
+        s, d, _, V = graph_edges("rmat", scale=13, ef=16, seed=2)
+        g = o.build(s, d, V, 0)
+        dg = lib.device_graph()
+        dg.build(dev(torch, s), dev(torch, d), V, 0)
+        peers = SymmetricBfsBuffers(V, [(0, V)], "cuda")
+        ok = 1
+        for root in _roots(g, 2):
+            par, dep, res = bfs_partitioned(DeviceBfsRangeStep(dg), V, g["num_edges"], [(0, V)], 0, 1, root, "cuda",
+                                            dist=tdist, peers=peers)
+            check_against_oracle(o, g, root, 2, False, host(par, np.int32), host(dep, np.int32), res)
+        np.save(out_path, np.array([ok]))
+        dg.close()
+    finally:
+        tdist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+def test_fused_exchange_through_symmetric_memory(torch_cuda, tmp_path):
+    """bfs_partitioned(peers=SymmetricBfsBuffers(...)): cand and the next
+    buffers in torch's symmetric memory; one rank of an NCCL group here."""
+    import socket
+
+    import torch.multiprocessing as mp
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    out = str(tmp_path / "symm_bfs.npy")
+    mp.spawn(_symm_worker, args=(out, port), nprocs=1, join=True)
+    assert np.load(out).tolist() == [1]
