@@ -1,5 +1,6 @@
-"""1-D partitioned PageRank pull and direction-optimizing BFS over several
-GPUs (one process per GPU).
+"""Work over several GPUs (one process per GPU): the graph build from
+edge-list shards, the 1-D partitioned PageRank pull and direction-optimizing
+BFS, and replicas of the batched work.
 
 PageRank pull
 -------------
@@ -23,7 +24,10 @@ which sums every row in the same order as the single-GPU pull kernel, so
 the ranks do not depend on the partition; the collectives run on whatever
 backend the process group has (NCCL between GPUs).  The step object is
 passed in, so the partition and exchange logic can also be exercised with
-another implementation of the same three calls.
+another implementation of the same three calls.  With ``fused=True`` the
+all-gather moves into the step: the next-contrib buffers live in symmetric
+memory (``PeerContribs``) and the range kernel stores each contrib it
+computes into every rank's copy, so an iteration ends with a barrier.
 
 Batched work
 ------------
@@ -82,11 +86,10 @@ slices of parents and depths are all-gathered.
 """
 from __future__ import annotations
 
+import ctypes as C
 from dataclasses import dataclass
 
 import numpy as np
-
-import ctypes as C
 
 from . import _ptr, _stream
 
