@@ -838,20 +838,25 @@ def run_bfs_partitioned(args):
     local sort + CSR: `build_ms`); then --n DO-BFS searches, each one search
     over all ranks.  Every phase is timed with CUDA events between barriers
     and the slowest rank's time is reported.  Also the split kernel alone on
-    the rank's shard into 8 owners (`split`).  Prints one JSON line (rank 0)."""
+    the rank's shard into 8 owners (`split`).  --fused: the searches' exchange
+    fused into the steps (symmetric memory) instead of the all-reduces.
+    Prints one JSON line (rank 0)."""
     import datetime
 
     import torch
     import torch.distributed as tdist
     import opengraph_b200 as og
-    from opengraph_b200.parallel import (DeviceBfsRangeStep, DeviceEdgeSplit, bfs_partitioned, partitioned_device_graph,
-                                         shard_ranges)
+    from opengraph_b200.parallel import (DeviceBfsRangeStep, DeviceEdgeSplit, SymmetricBfsBuffers, bfs_partitioned,
+                                         partitioned_device_graph, shard_ranges)
     ws, rank, local = dist_env()
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     dist = tdist if ws > 1 else None
-    if ws > 1:
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    if ws > 1 or args.fused:  # the fused exchange's symmetric memory needs a process group, even of one
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29531")
+        tdist.init_process_group("nccl", rank=rank, world_size=ws, timeout=datetime.timedelta(seconds=120),
+                                 device_id=dev)
     lib = og.load(True)
     lib.quiet(True)
     s, d, w = og.generate_rmat(args.scale, EDGE_FACTOR, SEED, weighted=True)
@@ -896,9 +901,11 @@ def run_bfs_partitioned(args):
     rng = np.random.default_rng(1000)
     roots = [int(x) for x in rng.choice(np.nonzero(outdeg > 0)[0], size=args.n + 1, replace=False)]
     step = DeviceBfsRangeStep(g)
+    peers = SymmetricBfsBuffers(V, ranges, dev) if args.fused else None
     res = []
     for k, r in enumerate(roots):
-        (par, dep, st), t = timed(lambda: bfs_partitioned(step, V, Eg, ranges, rank, ws, r, dev, dist=dist))
+        (par, dep, st), t = timed(lambda: bfs_partitioned(step, V, Eg, ranges, rank, ws, r, dev, dist=dist,
+                                                          peers=peers))
         if k == 0:
             continue  # warm-up search
         reached_out = int(outdeg[par.cpu().numpy() >= 0].sum())
@@ -907,6 +914,7 @@ def run_bfs_partitioned(args):
     g.close()
     if rank == 0:
         print(json.dumps({"case": "bfs-part", "scale": args.scale, "V": V, "E": E, "n_gpus": ws,
+                          "exchange": "fused (symmetric memory)" if args.fused else "all-reduce",
                           "ranges": [list(x) for x in ranges], "edges_per_rank": int(vf.num_edges),
                           "build_ms": round(build_ms, 3),
                           "split": {"owners": 8, "edges": int(ts.numel()), "ms": round(split_ms, 3),
@@ -915,7 +923,8 @@ def run_bfs_partitioned(args):
                           "searches": res,
                           "note": "each phase timed with CUDA events between barriers, max over ranks"}),
               flush=True)
-    if ws > 1:
+    del peers
+    if tdist.is_initialized():
         tdist.destroy_process_group()
 
 
@@ -935,6 +944,7 @@ def main():
                          "the others run one kernel family for profiling")
     ap.add_argument("--scale", type=int, default=SCALE, help="RMAT scale of a --case run")
     ap.add_argument("--n", type=int, default=3, help="searches / iterations / builds of a --case run")
+    ap.add_argument("--fused", action="store_true", help="bfs-part: the exchange fused into the steps")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.case == "scale":
