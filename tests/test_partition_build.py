@@ -156,3 +156,41 @@ def test_two_ranks_gloo_build_and_search(tmp_path):
     import torch.multiprocessing as mp
     mp.spawn(_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
     assert all((tmp_path / f"ok{r}.npy").exists() for r in range(2))
+
+
+def test_owned_rows_exact_for_random_shards_and_cuts(oracle):
+    """Property: for random edge lists (duplicates and self loops included),
+    random shard sizes and random owner cut points (empty ranges included),
+    every rank's graph built from the exchanged edges holds the whole
+    graph's out-rows and in-rows of its vertices, in order, for sort types 0
+    and 1, with and without weights."""
+    from hypothesis import given, settings, strategies as st
+
+    @settings(max_examples=60, deadline=None)
+    @given(st.integers(1, 40), st.integers(0, 160), st.integers(1, 5), st.integers(0, 2**31 - 1),
+           st.sampled_from([0, 1]), st.booleans())
+    def check(V, E, world, seed, sort_type, weighted):
+        import torch
+        rng = np.random.default_rng(seed)
+        s = rng.integers(0, V, E).astype(np.uint32)
+        d = rng.integers(0, V, E).astype(np.uint32)
+        w = rng.uniform(1, 9, E).astype(np.float32) if weighted else None
+        cuts = np.sort(rng.integers(0, V + 1, world - 1))
+        bounds = [0] + [int(c) for c in cuts] + [V]
+        ranges = [(bounds[r], bounds[r + 1]) for r in range(world)]
+        whole = oracle.build(s, d, V, sort_type, w=w)
+        sc = np.sort(rng.integers(0, E + 1, world - 1))
+        sb = [0] + [int(c) for c in sc] + [E]
+        t = lambda a: None if a is None else torch.from_numpy(np.ascontiguousarray(a))  # noqa: E731
+
+        def body(r, dd):
+            a, b = sb[r], sb[r + 1]
+            rs, rd, rw, n = exchange_edges(OracleEdgeSplit(oracle), t(s[a:b]), t(d[a:b]),
+                                           t(w[a:b]) if w is not None else None, ranges, r, world, dd)
+            return oracle.build(rs.numpy(), rd.numpy(), V, sort_type, w=None if rw is None else rw.numpy()), n
+
+        for r, (g, n) in enumerate(run_threads(world, body)):
+            assert n == E
+            check_rows(whole, g, *ranges[r])
+
+    check()
