@@ -144,3 +144,35 @@ def test_fused_exchange_more_ranks_than_vertices(oracle):
                                                             ranges, r, 6, root, "cpu", dist=dd, peers=ps.view(r)))
         for par, dep, res in outs:
             check_against_oracle(oracle, g, root, 2, False, par.numpy(), dep.numpy(), res)
+
+
+def test_random_graphs_and_cuts_both_exchanges(oracle):
+    """Property: on random small graphs (duplicates and self loops
+    included) with random owner cut points (empty ranges included), random
+    roots and all three modes, the partitioned search with either exchange
+    matches the oracle's single search."""
+    from hypothesis import given, settings, strategies as st
+
+    @settings(max_examples=40, deadline=None)
+    @given(st.integers(2, 48), st.integers(0, 200), st.integers(1, 4), st.integers(0, 2**31 - 1),
+           st.sampled_from([0, 1, 2]), st.booleans())
+    def check(V, E, world, seed, mode, fused):
+        rng = np.random.default_rng(seed)
+        s = rng.integers(0, V, E).astype(np.uint32)
+        d = rng.integers(0, V, E).astype(np.uint32)
+        g = oracle.build(s, d, V, 0)
+        cuts = np.sort(rng.integers(0, V + 1, world - 1))
+        bounds = [0] + [int(c) for c in cuts] + [V]
+        ranges = [(bounds[r], bounds[r + 1]) for r in range(world)]
+        root = int(rng.integers(0, V))
+        ps = PeerSet(V, ranges, world, "cpu") if fused else None
+
+        def body(r, dd):
+            step = NumpyFusedStep(oracle, g, ps, r) if fused else OracleBfsRangeStep(oracle, g)
+            return bfs_partitioned(step, V, g["num_edges"], ranges, r, world, root, "cpu", mode=mode, dist=dd,
+                                   peers=ps.view(r) if fused else None)
+
+        for par, dep, res in run_threads(world, body):
+            check_against_oracle(oracle, g, root, mode, False, par.numpy(), dep.numpy(), res)
+
+    check()
