@@ -112,3 +112,34 @@ def test_two_ranks_gloo_equal_single_rank(oracle, tmp_path):
         res = np.load(str(tmp_path / f"res{r}.npy"))
         assert np.array_equal(got.view(np.uint32), er.view(np.uint32)), r
         assert int(res[0]) == ei["iterations"] and int(res[1]) == ei["executed"], r
+
+
+def test_random_graphs_and_cuts_bit_exact(oracle):
+    """Property: random small graphs (duplicates, self loops, vertices
+    without in- or out-edges), random owner cut points (empty ranges
+    included), 1-4 thread-ranks: the partitioned pull equals the
+    single-process oracle bit for bit, iteration count included."""
+    from hypothesis import given, settings, strategies as st
+
+    from test_partition_bfs import run_threads
+    oracle.set_gpu_order()
+
+    @settings(max_examples=30, deadline=None)
+    @given(st.integers(2, 60), st.integers(1, 300), st.integers(1, 4), st.integers(0, 2**31 - 1))
+    def check(V, E, world, seed):
+        rng = np.random.default_rng(seed)
+        s = rng.integers(0, V, E).astype(np.uint32)
+        d = rng.integers(0, V, E).astype(np.uint32)
+        g = oracle.build(s, d, V, 0)
+        cuts = np.sort(rng.integers(0, V + 1, world - 1))
+        bounds = [0] + [int(c) for c in cuts] + [V]
+        ranges = [(bounds[r], bounds[r + 1]) for r in range(world)]
+        want, info = oracle.pagerank(g, 2, 50, 1e-7)
+        outs = run_threads(world, lambda r, dd: pagerank_pull_partitioned(OracleRangeStep(oracle, g), V, ranges, r,
+                                                                          world, 50, 1e-7, "cpu",
+                                                                          dist=dd if world > 1 else None))
+        for ranks, res in outs:
+            assert np.array_equal(ranks.numpy().view(np.uint32), want.view(np.uint32))
+            assert res.iterations == info["iterations"] and res.executed == info["executed"]
+
+    check()
