@@ -269,3 +269,41 @@ def test_oracle_matches_dd_spmv_fixture(oracle):
     x, y = oracle.spmv(g, 0, 3)
     assert np.array_equal(x, z["spmv_x"]) and np.array_equal(y.view(np.uint32), z["spmv_y"].view(np.uint32))
     assert np.array_equal(oracle.rank_sort(z["dd6_ranks"], z["sort_labels_in"]), z["sort_labels_out"])
+
+
+def test_oracle_matches_reference_live_random(og, oracle, ref, tmp_path):
+    """Property: on random small edge lists (duplicates, self loops and
+    vertices without edges included), every sort type, random roots and all
+    three BFS modes, the oracle's CSR arrays, BFS depths and stats and
+    PageRank pull ranks equal the reference's own build and search."""
+    from hypothesis import given, settings, strategies as st
+
+    @settings(max_examples=25, deadline=None)
+    @given(st.integers(2, 80), st.integers(1, 400), st.sampled_from([0, 1, 2, 3]), st.integers(0, 2**31 - 1))
+    def check(V, E, sort, seed):
+        rng = np.random.default_rng(seed)
+        s = rng.integers(0, V, E).astype(np.uint32)
+        d = rng.integers(0, V, E).astype(np.uint32)
+        path = str(tmp_path / f"r{seed}.bin")
+        og.write_edge_file(path, s, d)
+        rg = ref.build_graph(path, sort=sort)
+        try:
+            ga = og.graph_arrays(rg)
+            g = oracle.build(s, d, ga["num_vertices"], sort)
+            for k, v in g.items():
+                if isinstance(v, np.ndarray):
+                    assert np.array_equal(v, ga[k]), k
+            for root in {int(rng.integers(0, ga["num_vertices"])), int(np.argmax(ga["f_outdeg"]))}:
+                for mode in (0, 1, 2):
+                    rp, rd, rs = ref.bfs(rg, root, mode)
+                    op, od, os_ = oracle.bfs(g, root, mode)
+                    assert np.array_equal(rd, od), (root, mode)
+                    assert (rs["processed_nodes"], rs["iteration"]) == (os_["processed_nodes"], os_["iteration"])
+            rr, rs = ref.pagerank(rg, 0, 20, 1e-6)
+            orr, os_ = oracle.pagerank(g, 0, 20, 1e-6)
+            assert np.array_equal(rr.view(np.uint32), orr.view(np.uint32))
+            assert rs["iterations"] == os_["iterations"]
+        finally:
+            ref.graphCSRFree(rg)
+
+    check()
